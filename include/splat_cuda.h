@@ -1,0 +1,209 @@
+/*
+ * splat_cuda.h — C ABI of the B200 (sm_100a) Gaussian-splat tile rasterizer.
+ *
+ * This is the boundary a `cuda` backend of farmerchris/splat binds over FFI.
+ * It replaces the body of `Renderer::render` (src/render/mod.rs:86-97) for a
+ * scene bound at construction (`render::create`, src/render/mod.rs:115-121):
+ *
+ *   reference                                   replaced by
+ *   ------------------------------------------  -----------------------------
+ *   CpuTiled::new / GpuRenderer::new            splat_cuda_create
+ *     (src/render/cpu.rs:82-91, gpu.rs:510-707)
+ *   Renderer::render                            splat_cuda_render
+ *     (src/render/mod.rs:89-96; cpu.rs:109-222)
+ *   Renderer::render + term::downsample         splat_cuda_render with
+ *     (src/app.rs:203-206, src/term.rs:74-99)     downsample > 1
+ *   Renderer::name (src/render/mod.rs:87)       splat_cuda_backend_name
+ *   drop(Box<dyn Renderer>)                     splat_cuda_destroy
+ *   anyhow error text (src/bench.rs:147)        splat_cuda_last_error
+ *
+ * All entry points return a splat_status and never abort the process. A
+ * handle is used by one thread at a time (the reference trait is Send, not
+ * Sync, and render takes &mut self). Every call makes the handle's device
+ * current; all device work runs on the handle's stream.
+ *
+ * Layouts follow the reference's Scene (src/scene.rs:11-28): glam Vec3 is
+ * three packed f32, so `Vec<Vec3>` / `Vec<[f32; 6]>` can be passed as plain
+ * float pointers.
+ */
+#ifndef SPLAT_CUDA_H
+#define SPLAT_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SPLAT_CUDA_ABI_VERSION 1
+
+typedef enum splat_status {
+  SPLAT_OK = 0,
+  SPLAT_ERR_INVALID_ARG = 1,   /* null pointer, bad size, frame > MAX_DIM, ... */
+  SPLAT_ERR_OOM = 2,           /* device or pinned-host allocation failed */
+  SPLAT_ERR_CAPACITY = 3,      /* more (splat, tile) pairs than the pair limit */
+  SPLAT_ERR_DEVICE = 4,        /* CUDA error (text in splat_cuda_last_error) */
+  SPLAT_ERR_TIMEOUT = 5,       /* a bounded device-side wait gave up */
+  SPLAT_ERR_UNSUPPORTED = 6    /* option or precision not available */
+} splat_status;
+
+/* Largest output width or height (src/render/mod.rs:31-33). */
+#define SPLAT_MAX_DIM 16384u
+/* Screen tile edge in pixels (src/render/cpu.rs:34). */
+#define SPLAT_TILE 16u
+
+/* Scene parameter storage. */
+#define SPLAT_PRECISION_FP32 0u /* activated f32 params + precomputed cov3d */
+#define SPLAT_PRECISION_FP16 1u /* f32 positions; f16 scales/rotations/opacity/SH */
+
+/*
+ * A scene, as the reference's Scene holds it (activated parameters).
+ *
+ * FP32 (precision = SPLAT_PRECISION_FP32): positions, opacities, colors,
+ * cov3d and, for sh_degree > 0, sh_rest are read; scales/rotations and the
+ * f16 fields are ignored.
+ *   positions  n*3  world-space means                       (scene.rs:13)
+ *   opacities  n    sigmoid-activated, in [0, 1]             (scene.rs:18)
+ *   colors     n*3  SH_C0 * f_dc + 0.5                       (scene.rs:20)
+ *   cov3d      n*6  xx, xy, xz, yy, yz, zz                   (scene.rs:26)
+ *   sh_rest    n*rest*3, rest = (deg+1)^2 - 1, splat-major, coefficient
+ *              (3DGS basis order, sh.rs:39-64), then RGB   (scene.rs:23)
+ *
+ * FP16 (precision = SPLAT_PRECISION_FP16): positions stay f32; scales_f16
+ * (n*3, linear, exp-activated), rotations_f16 (n*4 unit quaternion x,y,z,w),
+ * opacities_f16 (n) and sh_f16 (n*(rest+1)*3: the base colour first, then the
+ * rest coefficients, RGB innermost) are IEEE binary16 bit patterns. The 3D
+ * covariance is then formed on the device from scale and rotation.
+ */
+typedef struct splat_scene_desc {
+  uint64_t n;
+  uint32_t sh_degree;  /* 0..3 */
+  uint32_t precision;  /* SPLAT_PRECISION_* */
+  const float* positions;
+  const float* opacities;
+  const float* colors;
+  const float* cov3d;
+  const float* sh_rest;
+  const uint16_t* scales_f16;
+  const uint16_t* rotations_f16;
+  const uint16_t* opacities_f16;
+  const uint16_t* sh_f16;
+} splat_scene_desc;
+
+/* A resolved camera pose (src/camera.rs:161-170): camera space is x right,
+ * y down, z forward; fov_y in radians. */
+typedef struct splat_view_desc {
+  float eye[3];
+  float right[3];
+  float down[3];
+  float forward[3];
+  float fov_y;
+  float near_plane;
+} splat_view_desc;
+
+/* RenderStats (src/render/mod.rs:72-83). For this tiled backend `overlaps`
+ * counts (splat, tile) pairs. Stage times are device times from CUDA events
+ * (project = projection + SH + pair emission, sort = radix sort + tile ranges,
+ * raster = blend + downsample); total_ms is host wall time of the call. */
+typedef struct splat_render_stats {
+  uint64_t visible;
+  uint64_t overlaps;
+  double project_ms;
+  double sort_ms;
+  double raster_ms;
+  double total_ms;
+} splat_render_stats;
+
+typedef struct splat_cuda_handle splat_cuda_handle;
+
+/* ABI version of the loaded library (SPLAT_CUDA_ABI_VERSION). */
+int splat_cuda_abi_version(void);
+
+/* "cuda" (Renderer::name, src/render/mod.rs:87). */
+const char* splat_cuda_backend_name(void);
+
+/* Binds a scene to a new renderer on `device` (a CUDA ordinal) and uploads it
+ * once. Replaces CpuTiled::new (src/render/cpu.rs:82-91) and
+ * GpuRenderer::new (src/render/gpu.rs:510-707). On failure *out is NULL and
+ * the status says why (no global error text is kept for a NULL handle; see
+ * splat_cuda_create_error). */
+int splat_cuda_create(const splat_scene_desc* scene, int device, splat_cuda_handle** out);
+
+/* Text of the last splat_cuda_create failure on this thread. */
+const char* splat_cuda_create_error(void);
+
+/* Renders `view` at width x height over background bg (linear RGB) and writes
+ * the u8 RGB frame, row-major, to host memory rgb_out (Frame::pixels,
+ * src/render/mod.rs:43-49). With downsample = f > 1 the frame is box-filtered
+ * by f on the device exactly as term::downsample does (src/term.rs:74-99):
+ * the output is floor(w/f) x floor(h/f) pixels. downsample 0 means 1.
+ * out_bytes must be at least floor(w/f)*floor(h/f)*3. width or height 0 gives
+ * an empty frame and zeroed stats (src/render/cpu.rs:120-122). width or
+ * height above SPLAT_MAX_DIM is rejected (src/render/mod.rs:35-41). Pair
+ * buffers grow and the frame is re-rendered when a view needs more (splat,
+ * tile) pairs than allocated (the reference's grow-and-retry,
+ * src/render/gpu.rs:1040-1056). Blocks until the frame is in rgb_out.
+ * Replaces Renderer::render (src/render/mod.rs:89-96). */
+int splat_cuda_render(splat_cuda_handle* h, const splat_view_desc* view, uint32_t width, uint32_t height,
+                      const float bg[3], uint32_t downsample, uint8_t* rgb_out, size_t out_bytes,
+                      splat_render_stats* stats);
+
+/* As splat_cuda_render, but the frame goes to DEVICE memory dev_out (on the
+ * handle's device) and the call only enqueues work on the handle's stream: it
+ * does not wait for the GPU. Call splat_cuda_finish before using the stats;
+ * it reports whether the frame overflowed the pair buffers, in which case the
+ * buffers have been grown and the frame must be enqueued again. */
+int splat_cuda_render_device(splat_cuda_handle* h, const splat_view_desc* view, uint32_t width, uint32_t height,
+                             const float bg[3], uint32_t downsample, uint8_t* dev_out, size_t out_bytes);
+
+/* Waits for the frames enqueued by splat_cuda_render_device, fills the stats
+ * of the last one and reports whether it overflowed the pair buffers
+ * (*regrown = 1: the buffers have been grown; enqueue the frame again). */
+int splat_cuda_finish(splat_cuda_handle* h, splat_render_stats* stats, int* regrown);
+
+/* Uses `stream` (a cudaStream_t on the handle's device; NULL restores the
+ * handle's own stream) for all later work of this handle. */
+int splat_cuda_set_stream(splat_cuda_handle* h, void* stream);
+/* The cudaStream_t the handle currently launches on. */
+void* splat_cuda_get_stream(splat_cuda_handle* h);
+
+/* Renderer options. */
+#define SPLAT_OPT_EXACT_BLEND 1u   /* 1: blend with the reference cpu backend's
+                                      exact f32 arithmetic (polynomial exp,
+                                      unfused multiply-adds); 0 (default): FMA
+                                      and the hardware exp2 */
+#define SPLAT_OPT_PAIR_CAPACITY 2u /* set the pair-buffer capacity (pairs) */
+#define SPLAT_OPT_STAGE_EVENTS 3u  /* 1 (default): time stages with CUDA events */
+#define SPLAT_OPT_DEBUG_CAPTURE 4u /* 1: keep per-splat projections for
+                                      splat_cuda_debug_dump (costs n*44 bytes) */
+int splat_cuda_set_option(splat_cuda_handle* h, uint32_t option, uint64_t value);
+int splat_cuda_get_option(splat_cuda_handle* h, uint32_t option, uint64_t* value);
+
+/*
+ * Intermediate buffers of the last completed render, for the oracle checks
+ * (the bit-exact key/range gate). Any output pointer may be NULL.
+ *   proj      n*8 floats per splat: x, y, ext_x, ext_y, depth, conic a, b, c
+ *   visible   n bytes: 1 if the splat survived culling
+ *   color     n*3 floats: the clamped view-dependent colour of visible splats
+ *   keys      sorted (tile << 32 | depth bits) keys, up to key_capacity
+ *   values    sorted splat indices, up to key_capacity
+ *   ranges    per tile [begin, end) as 2 u32, tiles_x*tiles_y*2 entries
+ *             (range_capacity entries at most)
+ *   n_pairs   the pair count
+ */
+int splat_cuda_debug_dump(splat_cuda_handle* h, float* proj, uint8_t* visible, float* color, uint64_t* keys,
+                          uint32_t* values, uint64_t key_capacity, uint32_t* ranges, uint64_t range_capacity,
+                          uint64_t* n_pairs);
+
+/* Frees the handle and its device memory. NULL is ignored. */
+int splat_cuda_destroy(splat_cuda_handle* h);
+
+/* Text describing the last failure on this handle ("" if none). */
+const char* splat_cuda_last_error(const splat_cuda_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SPLAT_CUDA_H */

@@ -1,0 +1,104 @@
+"""ctypes binding of ``libsplat_cuda.so`` (the C ABI in ``include/splat_cuda.h``).
+
+The library is loaded from this package directory. If it is missing the
+import fails loudly: there is no fallback renderer behind this module.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libsplat_cuda.so")
+
+SPLAT_OK = 0
+SPLAT_ERR_INVALID_ARG = 1
+SPLAT_ERR_OOM = 2
+SPLAT_ERR_CAPACITY = 3
+SPLAT_ERR_DEVICE = 4
+SPLAT_ERR_TIMEOUT = 5
+SPLAT_ERR_UNSUPPORTED = 6
+
+SPLAT_PRECISION_FP32 = 0
+SPLAT_PRECISION_FP16 = 1
+
+SPLAT_OPT_EXACT_BLEND = 1
+SPLAT_OPT_PAIR_CAPACITY = 2
+SPLAT_OPT_STAGE_EVENTS = 3
+SPLAT_OPT_DEBUG_CAPTURE = 4
+
+_STATUS_NAMES = {0: "OK", 1: "INVALID_ARG", 2: "OOM", 3: "CAPACITY", 4: "DEVICE", 5: "TIMEOUT", 6: "UNSUPPORTED"}
+
+# Every symbol include/splat_cuda.h declares.
+EXPORTS = [
+    "splat_cuda_abi_version", "splat_cuda_backend_name", "splat_cuda_create", "splat_cuda_create_error",
+    "splat_cuda_render", "splat_cuda_render_device", "splat_cuda_finish", "splat_cuda_set_stream",
+    "splat_cuda_get_stream", "splat_cuda_set_option", "splat_cuda_get_option", "splat_cuda_debug_dump",
+    "splat_cuda_destroy", "splat_cuda_last_error",
+]
+
+
+class SplatError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{_STATUS_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+class SceneDesc(ctypes.Structure):
+    _fields_ = [
+        ("n", ctypes.c_uint64), ("sh_degree", ctypes.c_uint32), ("precision", ctypes.c_uint32),
+        ("positions", ctypes.c_void_p), ("opacities", ctypes.c_void_p), ("colors", ctypes.c_void_p),
+        ("cov3d", ctypes.c_void_p), ("sh_rest", ctypes.c_void_p), ("scales_f16", ctypes.c_void_p),
+        ("rotations_f16", ctypes.c_void_p), ("opacities_f16", ctypes.c_void_p), ("sh_f16", ctypes.c_void_p),
+    ]
+
+
+class ViewDesc(ctypes.Structure):
+    _fields_ = [("eye", ctypes.c_float * 3), ("right", ctypes.c_float * 3), ("down", ctypes.c_float * 3),
+                ("forward", ctypes.c_float * 3), ("fov_y", ctypes.c_float), ("near_plane", ctypes.c_float)]
+
+
+class RenderStatsC(ctypes.Structure):
+    _fields_ = [("visible", ctypes.c_uint64), ("overlaps", ctypes.c_uint64), ("project_ms", ctypes.c_double),
+                ("sort_ms", ctypes.c_double), ("raster_ms", ctypes.c_double), ("total_ms", ctypes.c_double)]
+
+
+_lib = None
+
+
+def lib():
+    """The loaded library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with `python -m splat_b200.build` "
+                              "(the CUDA backend has no fallback)")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, u32, u64, f32p = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64, ctypes.POINTER(ctypes.c_float)
+        L.splat_cuda_abi_version.restype = ctypes.c_int
+        L.splat_cuda_backend_name.restype = ctypes.c_char_p
+        L.splat_cuda_create.argtypes = [ctypes.POINTER(SceneDesc), ctypes.c_int, ctypes.POINTER(vp)]
+        L.splat_cuda_create_error.restype = ctypes.c_char_p
+        L.splat_cuda_render.argtypes = [vp, ctypes.POINTER(ViewDesc), u32, u32, f32p, u32, vp, ctypes.c_size_t,
+                                        ctypes.POINTER(RenderStatsC)]
+        L.splat_cuda_render_device.argtypes = [vp, ctypes.POINTER(ViewDesc), u32, u32, f32p, u32, vp,
+                                               ctypes.c_size_t]
+        L.splat_cuda_finish.argtypes = [vp, ctypes.POINTER(RenderStatsC), ctypes.POINTER(ctypes.c_int)]
+        L.splat_cuda_set_stream.argtypes = [vp, vp]
+        L.splat_cuda_get_stream.argtypes = [vp]
+        L.splat_cuda_get_stream.restype = vp
+        L.splat_cuda_set_option.argtypes = [vp, u32, u64]
+        L.splat_cuda_get_option.argtypes = [vp, u32, ctypes.POINTER(u64)]
+        L.splat_cuda_debug_dump.argtypes = [vp, vp, vp, vp, vp, vp, u64, vp, u64, ctypes.POINTER(u64)]
+        L.splat_cuda_destroy.argtypes = [vp]
+        L.splat_cuda_last_error.argtypes = [vp]
+        L.splat_cuda_last_error.restype = ctypes.c_char_p
+        _lib = L
+    return _lib
+
+
+def check(rc: int, handle=None, what: str = ""):
+    if rc != SPLAT_OK:
+        msg = lib().splat_cuda_last_error(handle).decode() if handle else ""
+        raise SplatError(rc, f"{what}: {msg}" if what else msg)

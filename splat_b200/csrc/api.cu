@@ -1,0 +1,554 @@
+// C ABI of the B200 rasterizer (include/splat_cuda.h): scene upload, buffer
+// management, the per-frame launch sequence and the host<->device boundary.
+//
+// One frame is: clear the frame state -> project (a) -> scan + emit pairs (b)
+// -> digit histogram, pass schedule, onesweep passes (c) -> tile ranges (c)
+// -> blend + downsample (d) -> one device-to-host copy of the frame and the
+// frame state. The host never waits in the middle of a frame; pair counts
+// that exceed the allocated capacity are detected from the frame state after
+// the frame, the buffers grow and the frame is rendered again (the
+// reference's grow-and-retry, src/render/gpu.rs:1040-1056).
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/splat_cuda.h"
+#include "common.cuh"
+
+#define SPLAT_API extern "C" __attribute__((visibility("default")))
+
+using namespace splat;
+
+struct splat_cuda_handle {
+  int device = 0;
+  int num_sms = 148;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  uint64_t n = 0;
+  uint32_t sh_degree = 0;
+  uint32_t precision = SPLAT_PRECISION_FP32;
+  // scene (device)
+  float4* pos_op = nullptr;
+  float4* cov_a = nullptr;
+  float4* cov_b = nullptr;
+  float* color = nullptr;
+  float* sh = nullptr;
+  // per-splat frame buffers
+  Record* rec = nullptr;
+  BinInfo* bin = nullptr;
+  unsigned long long* emit_desc = nullptr;
+  // pair buffers
+  uint64_t cap = 0;
+  uint64_t* keys[2] = {nullptr, nullptr};
+  uint32_t* vals[2] = {nullptr, nullptr};
+  uint32_t* lookback = nullptr;
+  uint64_t lb_parts = 0;
+  // per-size buffers
+  uint2* ranges = nullptr;
+  uint64_t ranges_cap = 0;  // tiles
+  uint8_t* out_dev = nullptr;
+  size_t out_cap = 0;
+  uint8_t* full_dev = nullptr;
+  size_t full_cap = 0;
+  // frame state
+  DevState* st = nullptr;
+  DevState* st_host = nullptr;  // pinned
+  uint8_t* stage = nullptr;     // pinned staging for pageable outputs
+  size_t stage_cap = 0;
+  // debug capture
+  float* dbg_proj = nullptr;
+  float* dbg_color = nullptr;
+  bool debug_capture = false;
+  // options
+  bool exact = false;
+  bool stage_events = true;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  // last frame
+  FrameParams last_fp{};
+  bool have_frame = false;
+  uint32_t last_digits = 0;
+  std::string err;
+};
+
+namespace {
+
+thread_local std::string g_create_error;
+
+int fail(splat_cuda_handle* h, int code, const std::string& msg) {
+  if (h) h->err = msg;
+  return code;
+}
+
+int cuda_fail(splat_cuda_handle* h, cudaError_t e, const char* what) {
+  const int code = (e == cudaErrorMemoryAllocation) ? SPLAT_ERR_OOM : SPLAT_ERR_DEVICE;
+  return fail(h, code, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(expr, what)                            \
+  do {                                            \
+    cudaError_t e_ = (expr);                      \
+    if (e_ != cudaSuccess) return cuda_fail(h, e_, what); \
+  } while (0)
+
+template <class T> void dfree(T*& p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+
+uint32_t bits_for(uint64_t v) {  // bits needed to hold values < v
+  uint32_t b = 0;
+  while (b < 64 && (1ull << b) < v) b++;
+  return b;
+}
+
+int ensure_pairs(splat_cuda_handle* h, uint64_t cap) {
+  if (cap <= h->cap) return SPLAT_OK;
+  if (cap > kMaxPairs) return fail(h, SPLAT_ERR_CAPACITY, "more than 2^30 - 1 gaussian/tile pairs");
+  for (int b = 0; b < 2; b++) {
+    dfree(h->keys[b]);
+    dfree(h->vals[b]);
+  }
+  dfree(h->lookback);
+  h->cap = 0;
+  for (int b = 0; b < 2; b++) {
+    CK(cudaMalloc(&h->keys[b], cap * sizeof(uint64_t)), "cudaMalloc keys");
+    CK(cudaMalloc(&h->vals[b], cap * sizeof(uint32_t)), "cudaMalloc values");
+  }
+  h->lb_parts = (cap + kSortPart - 1) / kSortPart;
+  CK(cudaMalloc(&h->lookback, (size_t)kMaxDigits * h->lb_parts * 256 * sizeof(uint32_t)), "cudaMalloc lookback");
+  h->cap = cap;
+  return SPLAT_OK;
+}
+
+int ensure_size(splat_cuda_handle* h, uint64_t tiles, size_t out_bytes, size_t full_bytes) {
+  if (tiles > h->ranges_cap) {
+    dfree(h->ranges);
+    CK(cudaMalloc(&h->ranges, tiles * sizeof(uint2)), "cudaMalloc ranges");
+    h->ranges_cap = tiles;
+  }
+  if (out_bytes > h->out_cap) {
+    dfree(h->out_dev);
+    CK(cudaMalloc(&h->out_dev, out_bytes), "cudaMalloc frame");
+    h->out_cap = out_bytes;
+  }
+  if (full_bytes > h->full_cap) {
+    dfree(h->full_dev);
+    CK(cudaMalloc(&h->full_dev, full_bytes), "cudaMalloc full-resolution frame");
+    h->full_cap = full_bytes;
+  }
+  return SPLAT_OK;
+}
+
+// ProjectCtx::new (src/render/mod.rs:169-196) with View::rotation/focal
+// (src/camera.rs:172-181), in f32 exactly as the reference computes it.
+FrameParams make_params(const splat_view_desc& v, uint32_t w, uint32_t hgt, const float bg[3], uint32_t f) {
+  FrameParams p{};
+  for (int c = 0; c < 3; c++) {
+    p.rot[c] = v.right[c];
+    p.rot[3 + c] = v.down[c];
+    p.rot[6 + c] = v.forward[c];
+    p.eye[c] = v.eye[c];
+    p.bg[c] = bg[c];
+  }
+  p.focal = ((float)hgt * 0.5f) / std::tan(v.fov_y * 0.5f);
+  const float fw = (float)w, fh = (float)hgt;
+  auto lim = [&](float half) {
+    const float l = 1.3f * (half / p.focal);
+    return std::isfinite(l) ? l : 0.0f;
+  };
+  p.cx = fw * 0.5f;
+  p.cy = fh * 0.5f;
+  p.width = fw;
+  p.height = fh;
+  p.near_plane = v.near_plane;
+  p.lim_x = lim(fw * 0.5f);
+  p.lim_y = lim(fh * 0.5f);
+  p.w = w;
+  p.h = hgt;
+  p.tiles_x = (w + kTile - 1) / kTile;
+  p.tiles_y = (hgt + kTile - 1) / kTile;
+  p.downsample = f;
+  p.out_w = w / f;
+  p.out_h = hgt / f;
+  return p;
+}
+
+bool is_pinned_host(const void* p) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+// Enqueues one frame into dev_out (no host synchronisation).
+int enqueue_frame(splat_cuda_handle* h, const FrameParams& fp, uint8_t* dev_out) {
+  const uint64_t tiles = (uint64_t)fp.tiles_x * fp.tiles_y;
+  const size_t full_bytes = (fp.downsample > 1 && kTile % fp.downsample != 0) ? (size_t)fp.w * fp.h * 3 : 0;
+  int rc = ensure_size(h, tiles, 0, full_bytes);
+  if (rc) return rc;
+  cudaStream_t s = h->stream;
+  CK(cudaMemsetAsync(h->st, 0, sizeof(DevState), s), "clear frame state");
+  CK(cudaMemsetAsync(h->ranges, 0, tiles * sizeof(uint2), s), "clear ranges");
+  const uint32_t key_bits = 32 + bits_for(tiles);
+  const uint32_t digits = (key_bits + 7) / 8;
+  h->last_digits = digits;
+  if (h->n) {
+    CK(cudaMemsetAsync(h->emit_desc, 0, ((h->n + 511) / 512) * sizeof(unsigned long long), s), "clear scan");
+    CK(cudaMemsetAsync(h->lookback, 0, (size_t)digits * h->lb_parts * 256 * sizeof(uint32_t), s), "clear lookback");
+  }
+  if (h->stage_events) CK(cudaEventRecord(h->ev[0], s), "event");
+  if (h->n) {
+    SceneDev sd{h->pos_op, h->cov_a, h->cov_b, h->color, h->sh, h->n, h->sh_degree};
+    CK(launch_project(fp, sd, h->rec, h->bin, h->debug_capture ? h->dbg_proj : nullptr,
+                      h->debug_capture ? h->dbg_color : nullptr, h->st, s),
+       "project kernel");
+    CK(launch_emit(fp, h->bin, h->n, h->emit_desc, h->keys[0], h->vals[0], h->cap, h->st, s), "emit kernel");
+  }
+  if (h->stage_events) CK(cudaEventRecord(h->ev[1], s), "event");
+  if (h->n) {
+    CK(launch_sort(key_bits, h->cap, h->keys[0], h->vals[0], h->keys[1], h->vals[1], h->lookback, h->lb_parts, h->st,
+                   h->num_sms, s),
+       "sort kernels");
+    CK(launch_ranges(h->cap, h->keys, h->ranges, h->st, h->num_sms, s), "ranges kernel");
+  }
+  if (h->stage_events) CK(cudaEventRecord(h->ev[2], s), "event");
+  const uint32_t* vals[2] = {h->vals[0], h->vals[1]};
+  CK(launch_blend(fp, h->rec, vals, h->ranges, h->st, h->exact, dev_out, h->full_dev, s), "blend kernel");
+  if (h->stage_events) CK(cudaEventRecord(h->ev[3], s), "event");
+  CK(cudaMemcpyAsync(h->st_host, h->st, sizeof(DevState), cudaMemcpyDeviceToHost, s), "copy frame state");
+  h->last_fp = fp;
+  return SPLAT_OK;
+}
+
+// Waits for the enqueued frame and interprets its state.
+int finish_frame(splat_cuda_handle* h, splat_render_stats* stats, int* regrown) {
+  *regrown = 0;
+  CK(cudaStreamSynchronize(h->stream), "frame");
+  const DevState& st = *h->st_host;
+  if (st.error & (kErrEmitTimeout | kErrSortTimeout))
+    return fail(h, SPLAT_ERR_TIMEOUT, "a device-side look-back wait gave up");
+  if (st.error & kErrSortRange) return fail(h, SPLAT_ERR_DEVICE, "sort produced an out-of-range position");
+  if (stats) {
+    stats->visible = st.visible;
+    stats->overlaps = st.total_pairs;
+    if (h->stage_events) {
+      float a = 0, b = 0, c = 0;
+      cudaEventElapsedTime(&a, h->ev[0], h->ev[1]);
+      cudaEventElapsedTime(&b, h->ev[1], h->ev[2]);
+      cudaEventElapsedTime(&c, h->ev[2], h->ev[3]);
+      stats->project_ms = a;
+      stats->sort_ms = b;
+      stats->raster_ms = c;
+    }
+  }
+  if (st.total_pairs > h->cap) {
+    const uint64_t want = std::max<uint64_t>(st.total_pairs + st.total_pairs / 4, h->cap + 1);
+    int rc = ensure_pairs(h, std::min<uint64_t>(want, std::max<uint64_t>(st.total_pairs, kMaxPairs)));
+    if (rc) return rc;
+    *regrown = 1;
+  }
+  h->have_frame = true;
+  return SPLAT_OK;
+}
+
+int check_frame_args(splat_cuda_handle* h, const splat_view_desc* view, uint32_t w, uint32_t hgt, const float* bg,
+                     uint32_t f, size_t out_bytes, const void* out) {
+  if (!h) return SPLAT_ERR_INVALID_ARG;
+  if (!view || !bg) return fail(h, SPLAT_ERR_INVALID_ARG, "null view or background");
+  if (w > SPLAT_MAX_DIM || hgt > SPLAT_MAX_DIM)
+    return fail(h, SPLAT_ERR_INVALID_ARG,
+                "frame " + std::to_string(w) + "x" + std::to_string(hgt) + " exceeds the 16384 pixel limit");
+  if (f == 0) f = 1;
+  const size_t need = (size_t)(w / f) * (hgt / f) * 3;
+  if (need && (!out || out_bytes < need))
+    return fail(h, SPLAT_ERR_INVALID_ARG, "output buffer smaller than floor(w/f)*floor(h/f)*3 bytes");
+  return SPLAT_OK;
+}
+
+}  // namespace
+
+SPLAT_API int splat_cuda_abi_version(void) { return SPLAT_CUDA_ABI_VERSION; }
+
+SPLAT_API const char* splat_cuda_backend_name(void) { return "cuda"; }
+
+SPLAT_API const char* splat_cuda_create_error(void) { return g_create_error.c_str(); }
+
+SPLAT_API int splat_cuda_create(const splat_scene_desc* d, int device, splat_cuda_handle** out) {
+  g_create_error.clear();
+  if (!out) return SPLAT_ERR_INVALID_ARG;
+  *out = nullptr;
+  if (!d) {
+    g_create_error = "null scene";
+    return SPLAT_ERR_INVALID_ARG;
+  }
+  if (d->sh_degree > 3) {
+    g_create_error = "sh_degree must be 0..3";
+    return SPLAT_ERR_INVALID_ARG;
+  }
+  if (d->precision != SPLAT_PRECISION_FP32) {
+    g_create_error = "only FP32 scene storage is available in this build";
+    return SPLAT_ERR_UNSUPPORTED;
+  }
+  if (d->n > 0xFFFFFFFFull) {
+    g_create_error = "more than 2^32 - 1 gaussians";
+    return SPLAT_ERR_INVALID_ARG;
+  }
+  const uint64_t n = d->n;
+  if (n && (!d->positions || !d->opacities || !d->colors || !d->cov3d || (d->sh_degree && !d->sh_rest))) {
+    g_create_error = "null scene array";
+    return SPLAT_ERR_INVALID_ARG;
+  }
+  auto* h = new splat_cuda_handle();
+  auto bail = [&](int rc) {
+    g_create_error = h->err;
+    splat_cuda_destroy(h);
+    return rc;
+  };
+  h->device = device;
+  h->n = n;
+  h->sh_degree = d->sh_degree;
+  h->precision = d->precision;
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) return bail(cuda_fail(h, e, "cudaSetDevice"));
+  e = cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, device);
+  if (e != cudaSuccess) return bail(cuda_fail(h, e, "device attributes"));
+  if ((e = cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking)) != cudaSuccess)
+    return bail(cuda_fail(h, e, "cudaStreamCreate"));
+  h->stream = h->own_stream;
+  for (auto& ev : h->ev)
+    if ((e = cudaEventCreate(&ev)) != cudaSuccess) return bail(cuda_fail(h, e, "cudaEventCreate"));
+  if ((e = cudaMalloc(&h->st, sizeof(DevState))) != cudaSuccess) return bail(cuda_fail(h, e, "cudaMalloc state"));
+  if ((e = cudaMallocHost(&h->st_host, sizeof(DevState))) != cudaSuccess)
+    return bail(cuda_fail(h, e, "cudaMallocHost state"));
+  std::memset(h->st_host, 0, sizeof(DevState));
+
+  if (n) {
+    // Upload in the device layout: float4 (pos, opacity), float4 + float4 for
+    // the covariance (with k = sqrt(2 ln(opacity / ALPHA_MIN)), the bbox
+    // radius the reference's cpu backend also precomputes, cpu.rs:384-388),
+    // colour and SH as planes of n floats for coalesced loads.
+    const uint32_t rest = d->sh_degree ? (d->sh_degree + 1) * (d->sh_degree + 1) - 1 : 0;
+    std::vector<float4> a(n), b(n), c(n);
+    for (uint64_t i = 0; i < n; i++) {
+      const float* p = d->positions + 3 * i;
+      const float o = d->opacities[i];
+      a[i] = make_float4(p[0], p[1], p[2], o);
+      const float* cv = d->cov3d + 6 * i;
+      b[i] = make_float4(cv[0], cv[1], cv[2], cv[3]);
+      const float k = o < kAlphaMin ? 0.0f : std::sqrt(2.0f * std::log(o / kAlphaMin));
+      c[i] = make_float4(cv[4], cv[5], k, 0.0f);
+    }
+    std::vector<float> col(3 * n);
+    for (uint64_t i = 0; i < n; i++)
+      for (int ch = 0; ch < 3; ch++) col[ch * n + i] = d->colors[3 * i + ch];
+    auto up = [&](void** dst, const void* src, size_t bytes, const char* what) -> int {
+      cudaError_t er = cudaMalloc(dst, bytes);
+      if (er != cudaSuccess) return cuda_fail(h, er, what);
+      er = cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice);
+      if (er != cudaSuccess) return cuda_fail(h, er, what);
+      return SPLAT_OK;
+    };
+    int rc;
+    if ((rc = up((void**)&h->pos_op, a.data(), n * sizeof(float4), "upload positions"))) return bail(rc);
+    if ((rc = up((void**)&h->cov_a, b.data(), n * sizeof(float4), "upload covariance"))) return bail(rc);
+    if ((rc = up((void**)&h->cov_b, c.data(), n * sizeof(float4), "upload covariance"))) return bail(rc);
+    if ((rc = up((void**)&h->color, col.data(), 3 * n * sizeof(float), "upload colours"))) return bail(rc);
+    if (rest) {
+      std::vector<float> sh((size_t)rest * 3 * n);
+      for (uint64_t i = 0; i < n; i++)
+        for (uint32_t k = 0; k < rest * 3; k++) sh[(size_t)k * n + i] = d->sh_rest[i * rest * 3 + k];
+      if ((rc = up((void**)&h->sh, sh.data(), sh.size() * sizeof(float), "upload SH"))) return bail(rc);
+    }
+    if ((e = cudaMalloc(&h->rec, n * sizeof(Record))) != cudaSuccess) return bail(cuda_fail(h, e, "cudaMalloc records"));
+    if ((e = cudaMalloc(&h->bin, n * sizeof(BinInfo))) != cudaSuccess) return bail(cuda_fail(h, e, "cudaMalloc bins"));
+    if ((e = cudaMalloc(&h->emit_desc, ((n + 511) / 512) * sizeof(unsigned long long))) != cudaSuccess)
+      return bail(cuda_fail(h, e, "cudaMalloc scan"));
+  }
+  int rc = ensure_pairs(h, std::max<uint64_t>(4 * n, 1u << 16));
+  if (rc) return bail(rc);
+  *out = h;
+  return SPLAT_OK;
+}
+
+SPLAT_API int splat_cuda_render_device(splat_cuda_handle* h, const splat_view_desc* view, uint32_t width,
+                                       uint32_t height, const float bg[3], uint32_t downsample, uint8_t* dev_out,
+                                       size_t out_bytes) {
+  int rc = check_frame_args(h, view, width, height, bg, downsample, out_bytes, dev_out);
+  if (rc) return rc;
+  if (width == 0 || height == 0) return SPLAT_OK;
+  CK(cudaSetDevice(h->device), "cudaSetDevice");
+  const uint32_t f = downsample ? downsample : 1;
+  return enqueue_frame(h, make_params(*view, width, height, bg, f), dev_out);
+}
+
+SPLAT_API int splat_cuda_finish(splat_cuda_handle* h, splat_render_stats* stats, int* regrown) {
+  if (!h) return SPLAT_ERR_INVALID_ARG;
+  int dummy = 0;
+  if (!regrown) regrown = &dummy;
+  if (stats) std::memset(stats, 0, sizeof(*stats));
+  CK(cudaSetDevice(h->device), "cudaSetDevice");
+  return finish_frame(h, stats, regrown);
+}
+
+SPLAT_API int splat_cuda_render(splat_cuda_handle* h, const splat_view_desc* view, uint32_t width, uint32_t height,
+                                const float bg[3], uint32_t downsample, uint8_t* rgb_out, size_t out_bytes,
+                                splat_render_stats* stats) {
+  const auto t0 = std::chrono::steady_clock::now();
+  if (stats) std::memset(stats, 0, sizeof(*stats));
+  int rc = check_frame_args(h, view, width, height, bg, downsample, out_bytes, rgb_out);
+  if (rc) return rc;
+  if (width == 0 || height == 0) return SPLAT_OK;
+  CK(cudaSetDevice(h->device), "cudaSetDevice");
+  const uint32_t f = downsample ? downsample : 1;
+  const FrameParams fp = make_params(*view, width, height, bg, f);
+  const size_t bytes = (size_t)fp.out_w * fp.out_h * 3;
+  if ((rc = ensure_size(h, 0, bytes, 0))) return rc;
+  const bool direct = bytes && is_pinned_host(rgb_out);
+  if (!direct && bytes > h->stage_cap) {
+    if (h->stage) cudaFreeHost(h->stage);
+    h->stage = nullptr;
+    h->stage_cap = 0;
+    CK(cudaMallocHost(&h->stage, bytes), "cudaMallocHost staging");
+    h->stage_cap = bytes;
+  }
+  for (int attempt = 0; attempt < 8; attempt++) {
+    if ((rc = enqueue_frame(h, fp, h->out_dev))) return rc;
+    if (bytes)
+      CK(cudaMemcpyAsync(direct ? rgb_out : h->stage, h->out_dev, bytes, cudaMemcpyDeviceToHost, h->stream),
+         "copy frame");
+    int regrown = 0;
+    if ((rc = finish_frame(h, stats, &regrown))) return rc;
+    if (!regrown) {
+      if (!direct && bytes) std::memcpy(rgb_out, h->stage, bytes);
+      if (stats)
+        stats->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+      return SPLAT_OK;
+    }
+  }
+  return fail(h, SPLAT_ERR_CAPACITY, "pair buffers kept overflowing");
+}
+
+SPLAT_API int splat_cuda_set_stream(splat_cuda_handle* h, void* stream) {
+  if (!h) return SPLAT_ERR_INVALID_ARG;
+  h->stream = stream ? (cudaStream_t)stream : h->own_stream;
+  return SPLAT_OK;
+}
+
+SPLAT_API void* splat_cuda_get_stream(splat_cuda_handle* h) { return h ? (void*)h->stream : nullptr; }
+
+SPLAT_API int splat_cuda_set_option(splat_cuda_handle* h, uint32_t option, uint64_t value) {
+  if (!h) return SPLAT_ERR_INVALID_ARG;
+  CK(cudaSetDevice(h->device), "cudaSetDevice");
+  switch (option) {
+    case SPLAT_OPT_EXACT_BLEND:
+      h->exact = value != 0;
+      return SPLAT_OK;
+    case SPLAT_OPT_PAIR_CAPACITY: {
+      if (value == 0 || value > kMaxPairs) return fail(h, SPLAT_ERR_INVALID_ARG, "pair capacity out of range");
+      // Shrinking is allowed: reallocate at exactly `value`.
+      for (int b = 0; b < 2; b++) {
+        dfree(h->keys[b]);
+        dfree(h->vals[b]);
+      }
+      dfree(h->lookback);
+      h->cap = 0;
+      return ensure_pairs(h, value);
+    }
+    case SPLAT_OPT_STAGE_EVENTS:
+      h->stage_events = value != 0;
+      return SPLAT_OK;
+    case SPLAT_OPT_DEBUG_CAPTURE: {
+      h->debug_capture = value != 0;
+      if (h->debug_capture && h->n && !h->dbg_proj) {
+        CK(cudaMalloc(&h->dbg_proj, h->n * 8 * sizeof(float)), "cudaMalloc debug");
+        CK(cudaMalloc(&h->dbg_color, h->n * 3 * sizeof(float)), "cudaMalloc debug");
+      }
+      return SPLAT_OK;
+    }
+    default:
+      return fail(h, SPLAT_ERR_UNSUPPORTED, "unknown option");
+  }
+}
+
+SPLAT_API int splat_cuda_get_option(splat_cuda_handle* h, uint32_t option, uint64_t* value) {
+  if (!h || !value) return SPLAT_ERR_INVALID_ARG;
+  switch (option) {
+    case SPLAT_OPT_EXACT_BLEND: *value = h->exact; return SPLAT_OK;
+    case SPLAT_OPT_PAIR_CAPACITY: *value = h->cap; return SPLAT_OK;
+    case SPLAT_OPT_STAGE_EVENTS: *value = h->stage_events; return SPLAT_OK;
+    case SPLAT_OPT_DEBUG_CAPTURE: *value = h->debug_capture; return SPLAT_OK;
+    default: return fail(h, SPLAT_ERR_UNSUPPORTED, "unknown option");
+  }
+}
+
+SPLAT_API int splat_cuda_debug_dump(splat_cuda_handle* h, float* proj, uint8_t* visible, float* color,
+                                    uint64_t* keys, uint32_t* values, uint64_t key_capacity, uint32_t* ranges,
+                                    uint64_t range_capacity, uint64_t* n_pairs) {
+  if (!h) return SPLAT_ERR_INVALID_ARG;
+  if (!h->have_frame) return fail(h, SPLAT_ERR_INVALID_ARG, "no frame rendered yet");
+  CK(cudaSetDevice(h->device), "cudaSetDevice");
+  CK(cudaStreamSynchronize(h->stream), "sync");
+  const DevState& st = *h->st_host;
+  const uint64_t P = std::min<uint64_t>(st.total_pairs, h->cap);
+  if (n_pairs) *n_pairs = P;
+  if ((proj || visible || color) && !h->dbg_proj)
+    return fail(h, SPLAT_ERR_INVALID_ARG, "enable SPLAT_OPT_DEBUG_CAPTURE before rendering");
+  if (proj) CK(cudaMemcpy(proj, h->dbg_proj, h->n * 8 * sizeof(float), cudaMemcpyDeviceToHost), "dump");
+  if (color) CK(cudaMemcpy(color, h->dbg_color, h->n * 3 * sizeof(float), cudaMemcpyDeviceToHost), "dump");
+  if (visible) {
+    std::vector<BinInfo> bin(h->n);
+    CK(cudaMemcpy(bin.data(), h->bin, h->n * sizeof(BinInfo), cudaMemcpyDeviceToHost), "dump");
+    for (uint64_t i = 0; i < h->n; i++) visible[i] = bin[i].rect_lo != kCulled;
+  }
+  const int sel = st.final_sel;
+  const uint64_t m = std::min(P, key_capacity);
+  if (keys && m) CK(cudaMemcpy(keys, h->keys[sel], m * 8, cudaMemcpyDeviceToHost), "dump");
+  if (values && m) CK(cudaMemcpy(values, h->vals[sel], m * 4, cudaMemcpyDeviceToHost), "dump");
+  if (ranges) {
+    const uint64_t tiles = (uint64_t)h->last_fp.tiles_x * h->last_fp.tiles_y;
+    const uint64_t r = std::min<uint64_t>(tiles * 2, range_capacity);
+    if (r) CK(cudaMemcpy(ranges, h->ranges, r * 4, cudaMemcpyDeviceToHost), "dump");
+  }
+  return SPLAT_OK;
+}
+
+SPLAT_API int splat_cuda_destroy(splat_cuda_handle* h) {
+  if (!h) return SPLAT_OK;
+  cudaSetDevice(h->device);
+  if (h->own_stream) cudaStreamSynchronize(h->own_stream);
+  if (h->stream && h->stream != h->own_stream) cudaStreamSynchronize(h->stream);
+  dfree(h->pos_op);
+  dfree(h->cov_a);
+  dfree(h->cov_b);
+  dfree(h->color);
+  dfree(h->sh);
+  dfree(h->rec);
+  dfree(h->bin);
+  dfree(h->emit_desc);
+  for (int b = 0; b < 2; b++) {
+    dfree(h->keys[b]);
+    dfree(h->vals[b]);
+  }
+  dfree(h->lookback);
+  dfree(h->ranges);
+  dfree(h->out_dev);
+  dfree(h->full_dev);
+  dfree(h->st);
+  dfree(h->dbg_proj);
+  dfree(h->dbg_color);
+  if (h->st_host) cudaFreeHost(h->st_host);
+  if (h->stage) cudaFreeHost(h->stage);
+  for (auto& ev : h->ev)
+    if (ev) cudaEventDestroy(ev);
+  if (h->own_stream) cudaStreamDestroy(h->own_stream);
+  delete h;
+  return SPLAT_OK;
+}
+
+SPLAT_API const char* splat_cuda_last_error(const splat_cuda_handle* h) { return h ? h->err.c_str() : ""; }

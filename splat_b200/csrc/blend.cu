@@ -1,0 +1,242 @@
+// Kernel (d): per-tile front-to-back blend with the terminal box-filter
+// downsample fused in.
+//
+// One CTA per 16x16 tile, one pixel per thread; each warp covers an 8x4 block
+// of the tile so a splat whose pixel bbox misses the block is skipped by the
+// whole warp. The tile's depth-sorted splat list is walked in batches of 256:
+// the CTA gathers the batch's 48-byte records into shared memory (one per
+// thread, coalesced index loads), then every pixel blends the batch front to
+// back. A pixel stops once its transmittance drops below T_MIN; the CTA stops
+// when a block vote finds no live pixel (the reference stops a tile when all
+// its row masks are empty, src/render/cpu.rs:693-702).
+//
+// Per pixel and splat the arithmetic is that of raster_tile
+// (src/render/cpu.rs:638-703): power = (-a/2 dx^2 + -c/2 dy^2) + (-b dy) dx
+// inside the splat's pixel bbox, alpha = min(opacity * exp(power), 0.99),
+// masked by power <= 0 and alpha >= 1/255, C += colour * alpha * T,
+// T *= 1 - alpha. EXACT = true evaluates it with the reference's x86 f32
+// semantics (unfused multiply-adds, the polynomial exp_neg of
+// src/render/simd.rs:315-331), which reproduces the cpu backend's image bit
+// for bit; EXACT = false uses FMA and the hardware exp2 (the default).
+// The result is quantised with to_u8 (src/render/mod.rs:282-285) and, for a
+// downsample factor f dividing 16, averaged over f x f blocks in shared
+// memory with term::downsample's truncating integer division
+// (src/term.rs:74-99); other factors go through a full-resolution scratch
+// frame and k_downsample.
+#include "common.cuh"
+
+namespace splat {
+namespace {
+
+constexpr float kLog2e = 1.44269504088896340736f;
+
+// src/render/simd.rs:315-331 with the portable F4's unfused mul_add.
+__device__ __forceinline__ float exp_neg_exact(float xin) {
+  const float C1 = 0.6933594f;
+  const float C2 = -2.1219444e-4f;
+  const float x = fmaxf(xin, -87.0f);
+  const float n = rintf(__fmul_rn(x, kLog2e));
+  const float f = __fsub_rn(__fsub_rn(x, __fmul_rn(n, C1)), __fmul_rn(n, C2));
+  float p = 1.9875691e-4f;
+  p = __fadd_rn(1.3981999e-3f, __fmul_rn(p, f));
+  p = __fadd_rn(8.333452e-3f, __fmul_rn(p, f));
+  p = __fadd_rn(4.1665796e-2f, __fmul_rn(p, f));
+  p = __fadd_rn(1.6666665e-1f, __fmul_rn(p, f));
+  p = __fadd_rn(0.5f, __fmul_rn(p, f));
+  const float f2 = __fmul_rn(f, f);
+  const float r = __fadd_rn(__fadd_rn(f, 1.0f), __fmul_rn(p, f2));
+  return __fmul_rn(r, __int_as_float(((int)n + 127) << 23));
+}
+
+__device__ __forceinline__ float ex2_approx(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// to_u8 (src/render/mod.rs:282-285)
+__device__ __forceinline__ uint32_t to_u8(float v) {
+  const float c = v < 0.0f ? 0.0f : (v > 1.0f ? 1.0f : v);  // f32::clamp; NaN passes
+  const float q = __fadd_rn(__fmul_rn(c, 255.0f), 0.5f);
+  if (!(q > 0.0f)) return 0u;
+  if (q >= 255.0f) return 255u;
+  return (uint32_t)q;
+}
+
+template <bool EXACT>
+__global__ void __launch_bounds__(256) k_blend(FrameParams fp, const Record* __restrict__ rec,
+                                               const uint32_t* __restrict__ v0, const uint32_t* __restrict__ v1,
+                                               const uint2* __restrict__ ranges, const DevState* st,
+                                               uint8_t* __restrict__ out, uint8_t* __restrict__ full) {
+  __shared__ float4 s_r0[256];
+  __shared__ float4 s_r1[256];
+  __shared__ float4 s_r2[256];
+  __shared__ uint32_t s_px[256];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint32_t tile = blockIdx.x;
+  const uint32_t tx = tile % fp.tiles_x, ty = tile / fp.tiles_x;
+  const uint32_t ox = tx * kTile, oy = ty * kTile;
+  const uint32_t lx = (warp & 1) * 8 + (lane & 7), ly = (warp >> 1) * 4 + (lane >> 3);
+  const uint32_t px = ox + lx, py = oy + ly;
+  const bool inside = px < fp.w && py < fp.h;
+  const uint32_t* __restrict__ vals = st->final_sel ? v1 : v0;
+  const uint2 range = ranges[tile];
+  const uint32_t begin = range.x, end = range.y > range.x ? range.y : range.x;
+
+  // Pixel-centre terms in the reference's association:
+  // dx = lane + ((g*4) + ((ox + 0.5) - x)), dy = ((oy + ly) + 0.5) - y.
+  const float fx05 = __fadd_rn((float)ox, 0.5f);
+  const float gbase = (float)(lx & ~3u), lanef = (float)(lx & 3u);
+  const float rowc = __fadd_rn(__fadd_rn((float)oy, (float)ly), 0.5f);
+  const float pxc = (float)px + 0.5f, pyc = (float)py + 0.5f;
+
+  float T = 1.0f, cr = 0.0f, cg = 0.0f, cb = 0.0f;
+  bool done = !inside;
+  for (uint32_t start = begin; start < end; start += 256) {
+    const uint32_t idx = start + tid;
+    if (idx < end) {
+      const Record r = rec[vals[idx]];
+      float4 a = r.r0, b = r.r1;
+      if (!EXACT) {  // pre-scale the conic terms by log2(e) for exp2
+        a.z *= kLog2e;
+        a.w *= kLog2e;
+        b.x *= kLog2e;
+      }
+      s_r0[tid] = a;
+      s_r1[tid] = b;
+      s_r2[tid] = r.r2;
+    }
+    __syncthreads();
+    const uint32_t cnt = min(256u, end - start);
+    if (!done) {
+      for (uint32_t j = 0; j < cnt; j++) {
+        const float4 r2 = s_r2[j];
+        const uint32_t bx = __float_as_uint(r2.y), by = __float_as_uint(r2.z);
+        if (px < (bx & 0xFFFFu) || px >= (bx >> 16) || py < (by & 0xFFFFu) || py >= (by >> 16)) continue;
+        const float4 r0 = s_r0[j];
+        const float4 r1 = s_r1[j];
+        float pw, alpha;
+        if (EXACT) {
+          const float cx0 = __fsub_rn(fx05, r0.x);
+          const float dx = __fadd_rn(lanef, __fadd_rn(gbase, cx0));
+          const float qx = __fmul_rn(__fmul_rn(dx, dx), r0.z);
+          const float dy = __fsub_rn(rowc, r0.y);
+          const float qy = __fmul_rn(__fmul_rn(r1.x, dy), dy);
+          const float bdy = __fmul_rn(r0.w, dy);
+          pw = __fadd_rn(__fadd_rn(qx, qy), __fmul_rn(bdy, dx));
+          alpha = fminf(__fmul_rn(exp_neg_exact(pw), r1.y), kAlphaMax);
+        } else {
+          const float dx = pxc - r0.x;
+          const float dy = pyc - r0.y;
+          pw = fmaf(r0.z * dx, dx, fmaf(r1.x * dy, dy, (r0.w * dy) * dx));
+          alpha = fminf(ex2_approx(pw) * r1.y, kAlphaMax);
+        }
+        if (!(pw <= 0.0f && alpha >= kAlphaMin)) continue;
+        if (EXACT) {
+          const float w = __fmul_rn(alpha, T);
+          cr = __fadd_rn(cr, __fmul_rn(r1.z, w));
+          cg = __fadd_rn(cg, __fmul_rn(r1.w, w));
+          cb = __fadd_rn(cb, __fmul_rn(r2.x, w));
+          T = __fmul_rn(T, __fsub_rn(1.0f, alpha));
+        } else {
+          const float w = alpha * T;
+          cr = fmaf(r1.z, w, cr);
+          cg = fmaf(r1.w, w, cg);
+          cb = fmaf(r2.x, w, cb);
+          T = T * (1.0f - alpha);
+        }
+        if (T < kTMin) {
+          done = true;
+          break;
+        }
+      }
+    }
+    if (__syncthreads_count(!done) == 0) break;
+  }
+
+  // C + T * bg, quantised (the reference adds unfused: c + (t * bg)).
+  const uint32_t qr = to_u8(__fadd_rn(cr, __fmul_rn(T, fp.bg[0])));
+  const uint32_t qg = to_u8(__fadd_rn(cg, __fmul_rn(T, fp.bg[1])));
+  const uint32_t qb = to_u8(__fadd_rn(cb, __fmul_rn(T, fp.bg[2])));
+  const uint32_t f = fp.downsample;
+  if (f == 1) {
+    if (inside) {
+      uint8_t* o = out + ((size_t)py * fp.w + px) * 3;
+      o[0] = (uint8_t)qr;
+      o[1] = (uint8_t)qg;
+      o[2] = (uint8_t)qb;
+    }
+    return;
+  }
+  if (kTile % f != 0) {  // factor 3 etc.: full-resolution scratch, then k_downsample
+    if (inside) {
+      uint8_t* o = full + ((size_t)py * fp.w + px) * 3;
+      o[0] = (uint8_t)qr;
+      o[1] = (uint8_t)qg;
+      o[2] = (uint8_t)qb;
+    }
+    return;
+  }
+  s_px[ly * kTile + lx] = qr | (qg << 8) | (qb << 16);
+  __syncthreads();
+  const uint32_t per = kTile / f;  // output pixels per tile edge
+  if ((uint32_t)tid < per * per) {
+    const uint32_t bxl = tid % per, byl = tid / per;
+    const uint32_t obx = ox / f + bxl, oby = oy / f + byl;
+    if (obx < fp.out_w && oby < fp.out_h) {
+      uint32_t acc[3] = {0u, 0u, 0u};
+      for (uint32_t sy = 0; sy < f; sy++)
+        for (uint32_t sx = 0; sx < f; sx++) {
+          const uint32_t p = s_px[(byl * f + sy) * kTile + bxl * f + sx];
+          acc[0] += p & 255u;
+          acc[1] += (p >> 8) & 255u;
+          acc[2] += (p >> 16) & 255u;
+        }
+      const uint32_t nn = f * f;
+      uint8_t* o = out + ((size_t)oby * fp.out_w + obx) * 3;
+      o[0] = (uint8_t)(acc[0] / nn);
+      o[1] = (uint8_t)(acc[1] / nn);
+      o[2] = (uint8_t)(acc[2] / nn);
+    }
+  }
+}
+
+// term::downsample (src/term.rs:74-99) for factors that do not divide the tile.
+__global__ void k_downsample(FrameParams fp, const uint8_t* __restrict__ full, uint8_t* __restrict__ out) {
+  const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+  if (x >= fp.out_w || y >= fp.out_h) return;
+  const uint32_t f = fp.downsample;
+  uint32_t acc[3] = {0u, 0u, 0u};
+  for (uint32_t sy = 0; sy < f; sy++) {
+    const uint8_t* row = full + ((size_t)(y * f + sy) * fp.w + x * f) * 3;
+    for (uint32_t sx = 0; sx < f; sx++) {
+      acc[0] += row[3 * sx];
+      acc[1] += row[3 * sx + 1];
+      acc[2] += row[3 * sx + 2];
+    }
+  }
+  const uint32_t nn = f * f;
+  uint8_t* o = out + ((size_t)y * fp.out_w + x) * 3;
+  o[0] = (uint8_t)(acc[0] / nn);
+  o[1] = (uint8_t)(acc[1] / nn);
+  o[2] = (uint8_t)(acc[2] / nn);
+}
+
+}  // namespace
+
+cudaError_t launch_blend(const FrameParams& fp, const Record* rec, const uint32_t* const* vals, const uint2* ranges,
+                         const DevState* st, bool exact, uint8_t* out, uint8_t* full_scratch, cudaStream_t stream) {
+  const unsigned tiles = fp.tiles_x * fp.tiles_y;
+  if (tiles == 0) return cudaSuccess;
+  if (exact)
+    k_blend<true><<<tiles, 256, 0, stream>>>(fp, rec, vals[0], vals[1], ranges, st, out, full_scratch);
+  else
+    k_blend<false><<<tiles, 256, 0, stream>>>(fp, rec, vals[0], vals[1], ranges, st, out, full_scratch);
+  if (fp.downsample > 1 && kTile % fp.downsample != 0 && fp.out_w > 0 && fp.out_h > 0) {
+    dim3 grid((fp.out_w + 127) / 128, fp.out_h);
+    k_downsample<<<grid, 128, 0, stream>>>(fp, full_scratch, out);
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace splat

@@ -1,0 +1,220 @@
+// Kernel (a): fused EWA projection, culling and SH colour, one thread per
+// splat. Follows `project` (src/render/mod.rs:199-272, equal bit for bit to
+// project_fast/project4 of src/render/cpu.rs:419-566) and `sh::eval_rest`
+// (src/sh.rs:39-64) operation by operation. This translation unit is built
+// with --fmad=false and IEEE division/sqrt, so every result is the correctly
+// rounded f32 of the same expression tree the reference evaluates on x86
+// (no fused multiply-adds): the projected splats equal the oracle's bit for
+// bit. The kernel also emits each visible splat's tile rectangle (pixel_bbox,
+// src/render/cpu.rs:94-102 and the tile loop of cpu.rs:262-276), its pair
+// count and depth bits for the binning scan.
+#include "common.cuh"
+
+namespace splat {
+namespace {
+
+// src/sh.rs:5-22
+constexpr float kShC1 = 0.4886025f;
+constexpr float kShC2_0 = 1.0925485f, kShC2_1 = -1.0925485f, kShC2_2 = 0.31539157f, kShC2_3 = -1.0925485f,
+                kShC2_4 = 0.54627424f;
+constexpr float kShC3_0 = -0.5900436f, kShC3_1 = 2.8906114f, kShC3_2 = -0.4570458f, kShC3_3 = 0.37317633f,
+                kShC3_4 = -0.4570458f, kShC3_5 = 1.4453057f, kShC3_6 = -0.5900436f;
+
+// `x as u32` of a float: saturating, NaN -> 0.
+__device__ __forceinline__ uint32_t sat_u32(float v) {
+  if (!(v > 0.0f)) return 0u;
+  if (v >= 4294967296.0f) return 0xFFFFFFFFu;
+  return (uint32_t)v;
+}
+
+// f32::clamp (NaN passes through).
+__device__ __forceinline__ float rclamp(float v, float lo, float hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+// SH coefficient `coef`, channel `ch` of splat i (planar layout).
+template <int DEG>
+__device__ __forceinline__ void eval_sh(const float* __restrict__ sh, uint64_t n, uint64_t i, float x, float y, float z,
+                                        float c[3]) {
+  if constexpr (DEG >= 1) {
+    auto R = [&](int coef, int ch) { return __ldg(sh + (uint64_t)(coef * 3 + ch) * n + i); };
+    float r[3];
+#pragma unroll
+    for (int ch = 0; ch < 3; ch++) {
+      float v = kShC1 * (((-y) * R(0, ch) + z * R(1, ch)) - x * R(2, ch));
+      r[ch] = v;
+    }
+    if constexpr (DEG >= 2) {
+      float xx = x * x, yy = y * y, zz = z * z;
+      float xy = x * y, yz = y * z, xz = x * z;
+      float b3 = kShC2_0 * xy, b4 = kShC2_1 * yz, b5 = kShC2_2 * ((2.0f * zz - xx) - yy), b6 = kShC2_3 * xz,
+            b7 = kShC2_4 * (xx - yy);
+#pragma unroll
+      for (int ch = 0; ch < 3; ch++) {
+        float s = b3 * R(3, ch);
+        s = s + b4 * R(4, ch);
+        s = s + b5 * R(5, ch);
+        s = s + b6 * R(6, ch);
+        s = s + b7 * R(7, ch);
+        r[ch] = r[ch] + s;
+      }
+      if constexpr (DEG >= 3) {
+        float b8 = (kShC3_0 * y) * (3.0f * xx - yy);
+        float b9 = (kShC3_1 * xy) * z;
+        float b10 = (kShC3_2 * y) * ((4.0f * zz - xx) - yy);
+        float b11 = (kShC3_3 * z) * ((2.0f * zz - 3.0f * xx) - 3.0f * yy);
+        float b12 = (kShC3_4 * x) * ((4.0f * zz - xx) - yy);
+        float b13 = (kShC3_5 * z) * (xx - yy);
+        float b14 = (kShC3_6 * x) * (xx - 3.0f * yy);
+#pragma unroll
+        for (int ch = 0; ch < 3; ch++) {
+          float u = b8 * R(8, ch);
+          u = u + b9 * R(9, ch);
+          u = u + b10 * R(10, ch);
+          u = u + b11 * R(11, ch);
+          u = u + b12 * R(12, ch);
+          u = u + b13 * R(13, ch);
+          u = u + b14 * R(14, ch);
+          r[ch] = r[ch] + u;
+        }
+      }
+    }
+#pragma unroll
+    for (int ch = 0; ch < 3; ch++) c[ch] = c[ch] + r[ch];
+  }
+}
+
+template <int DEG>
+__global__ void __launch_bounds__(256) k_project(FrameParams fp, SceneDev s, Record* __restrict__ rec,
+                                                 BinInfo* __restrict__ bin, float* __restrict__ dbg_proj,
+                                                 float* __restrict__ dbg_color, DevState* st) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  bool vis = false;
+  if (i < s.n) {
+    const float4 po = __ldg(&s.pos_op[i]);
+    BinInfo b{kCulled, 0u, 0u, 0u};
+    float out_x = 0.f, out_y = 0.f, out_ex = 0.f, out_ey = 0.f, out_depth = 0.f, c0 = 0.f, c1 = 0.f, c2 = 0.f;
+    float col[3] = {0.f, 0.f, 0.f};
+    const float opacity = po.w;
+    do {
+      if (opacity < kAlphaMin) break;
+      // t = rot * (p - eye), glam Mat3::mul_vec3 order.
+      const float dx = po.x - fp.eye[0], dy = po.y - fp.eye[1], dz = po.z - fp.eye[2];
+      const float tx_ = (fp.rot[0] * dx + fp.rot[1] * dy) + fp.rot[2] * dz;
+      const float ty_ = (fp.rot[3] * dx + fp.rot[4] * dy) + fp.rot[5] * dz;
+      const float tz = (fp.rot[6] * dx + fp.rot[7] * dy) + fp.rot[8] * dz;
+      if (!(tz > fp.near_plane)) break;
+      const float inv_z = 1.0f / tz;
+      const float x = ((fp.focal * tx_) * inv_z) + fp.cx;
+      const float y = ((fp.focal * ty_) * inv_z) + fp.cy;
+      // Jacobian at the clamped mean; rows of T = J R are rot^T * j.
+      const float jx = rclamp(tx_ * inv_z, -fp.lim_x, fp.lim_x);
+      const float jy = rclamp(ty_ * inv_z, -fp.lim_y, fp.lim_y);
+      const float f = fp.focal * inv_z;
+      const float j0z = (-f) * jx, j1z = (-f) * jy;
+      const float t0x = (fp.rot[0] * f + fp.rot[3] * 0.0f) + fp.rot[6] * j0z;
+      const float t0y = (fp.rot[1] * f + fp.rot[4] * 0.0f) + fp.rot[7] * j0z;
+      const float t0z = (fp.rot[2] * f + fp.rot[5] * 0.0f) + fp.rot[8] * j0z;
+      const float t1x = (fp.rot[0] * 0.0f + fp.rot[3] * f) + fp.rot[6] * j1z;
+      const float t1y = (fp.rot[1] * 0.0f + fp.rot[4] * f) + fp.rot[7] * j1z;
+      const float t1z = (fp.rot[2] * 0.0f + fp.rot[5] * f) + fp.rot[8] * j1z;
+      const float4 ca = __ldg(&s.cov_a[i]);
+      const float4 cb = __ldg(&s.cov_b[i]);
+      const float cxx = ca.x, cxy = ca.y, cxz = ca.z, cyy = ca.w, cyz = cb.x, czz = cb.y;
+      const float s0x = (cxx * t0x + cxy * t0y) + cxz * t0z;
+      const float s0y = (cxy * t0x + cyy * t0y) + cyz * t0z;
+      const float s0z = (cxz * t0x + cyz * t0y) + czz * t0z;
+      const float s1x = (cxx * t1x + cxy * t1y) + cxz * t1z;
+      const float s1y = (cxy * t1x + cyy * t1y) + cyz * t1z;
+      const float s1z = (cxz * t1x + cyz * t1y) + czz * t1z;
+      const float a = ((t0x * s0x + t0y * s0y) + t0z * s0z) + kDilation;
+      const float bb = (t1x * s0x + t1y * s0y) + t1z * s0z;
+      const float cc = ((t1x * s1x + t1y * s1y) + t1z * s1z) + kDilation;
+      const float det = a * cc - bb * bb;
+      if (!(det > 0.0f)) break;
+      const float inv_det = 1.0f / det;
+      const float k = cb.z;  // sqrt(2 ln(opacity / ALPHA_MIN)), precomputed at upload
+      const float ext_x = k * sqrtf(a);
+      const float ext_y = k * sqrtf(cc);
+      if (x + ext_x <= 0.0f || x - ext_x >= fp.width || y + ext_y <= 0.0f || y - ext_y >= fp.height) break;
+      col[0] = __ldg(s.color + i);
+      col[1] = __ldg(s.color + s.n + i);
+      col[2] = __ldg(s.color + 2 * s.n + i);
+      if constexpr (DEG > 0) {
+        // normalize_or_zero(p - eye)
+        const float len = sqrtf((dx * dx + dy * dy) + dz * dz);
+        const float rcp = 1.0f / len;
+        float nx = 0.f, ny = 0.f, nz = 0.f;
+        if (isfinite(rcp) && rcp > 0.0f) {
+          nx = dx * rcp;
+          ny = dy * rcp;
+          nz = dz * rcp;
+        }
+        eval_sh<DEG>(s.sh, s.n, i, nx, ny, nz, col);
+      }
+      col[0] = fmaxf(col[0], 0.0f);
+      col[1] = fmaxf(col[1], 0.0f);
+      col[2] = fmaxf(col[2], 0.0f);
+      if (!(isfinite(x) && isfinite(y) && isfinite(ext_x) && isfinite(ext_y))) break;
+      c0 = cc * inv_det;
+      c1 = (-bb) * inv_det;
+      c2 = a * inv_det;
+      // pixel_bbox (src/render/cpu.rs:96-102)
+      const uint32_t x0 = sat_u32(fmaxf(floorf(x - ext_x), 0.0f));
+      const uint32_t y0 = sat_u32(fmaxf(floorf(y - ext_y), 0.0f));
+      const uint32_t x1 = min(sat_u32(fmaxf(ceilf(x + ext_x), 0.0f)), fp.w);
+      const uint32_t y1 = min(sat_u32(fmaxf(ceilf(y + ext_y), 0.0f)), fp.h);
+      const uint32_t bx0 = min(x0, x1), by0 = min(y0, y1);
+      Record r;
+      r.r0 = make_float4(x, y, -0.5f * c0, -c1);
+      r.r1 = make_float4(-0.5f * c2, opacity, col[0], col[1]);
+      r.r2 = make_float4(col[2], __uint_as_float(bx0 | (x1 << 16)), __uint_as_float(by0 | (y1 << 16)), tz);
+      rec[i] = r;
+      b.depth_bits = __float_as_uint(tz);
+      if (bx0 < x1 && by0 < y1) {
+        const uint32_t tx0 = bx0 / kTile, ty0 = by0 / kTile;
+        const uint32_t tx1 = (x1 + kTile - 1) / kTile, ty1 = (y1 + kTile - 1) / kTile;
+        b.rect_lo = tx0 | (ty0 << 16);
+        b.rect_hi = tx1 | (ty1 << 16);
+        b.count = (tx1 - tx0) * (ty1 - ty0);
+      } else {
+        b.rect_lo = 0u;  // visible, but its bbox holds no pixel: no pairs
+        b.rect_hi = 0u;
+        b.count = 0u;
+      }
+      vis = true;
+      out_x = x;
+      out_y = y;
+      out_ex = ext_x;
+      out_ey = ext_y;
+      out_depth = tz;
+    } while (false);
+    bin[i] = b;
+    if (dbg_proj) {
+      float* d = dbg_proj + 8 * i;
+      d[0] = out_x; d[1] = out_y; d[2] = out_ex; d[3] = out_ey; d[4] = out_depth; d[5] = c0; d[6] = c1; d[7] = c2;
+    }
+    if (dbg_color) {
+      dbg_color[3 * i] = vis ? col[0] : 0.f;
+      dbg_color[3 * i + 1] = vis ? col[1] : 0.f;
+      dbg_color[3 * i + 2] = vis ? col[2] : 0.f;
+    }
+  }
+  const int nvis = __syncthreads_count(vis);
+  if (threadIdx.x == 0 && nvis) atomicAdd(&st->visible, (unsigned)nvis);
+}
+
+}  // namespace
+
+cudaError_t launch_project(const FrameParams& fp, const SceneDev& s, Record* rec, BinInfo* bin, float* dbg_proj,
+                           float* dbg_color, DevState* st, cudaStream_t stream) {
+  if (s.n == 0) return cudaSuccess;
+  const unsigned grid = (unsigned)((s.n + 255) / 256);
+  switch (s.sh_degree) {
+    case 0: k_project<0><<<grid, 256, 0, stream>>>(fp, s, rec, bin, dbg_proj, dbg_color, st); break;
+    case 1: k_project<1><<<grid, 256, 0, stream>>>(fp, s, rec, bin, dbg_proj, dbg_color, st); break;
+    case 2: k_project<2><<<grid, 256, 0, stream>>>(fp, s, rec, bin, dbg_proj, dbg_color, st); break;
+    default: k_project<3><<<grid, 256, 0, stream>>>(fp, s, rec, bin, dbg_proj, dbg_color, st); break;
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace splat

@@ -1,0 +1,240 @@
+"""The renderer interface of farmerchris/splat (``src/render/mod.rs``) over the
+sm_100a backend's C ABI.
+
+``Renderer``, ``Frame``, ``RenderStats``, ``Backend`` and ``create`` keep the
+reference's names, argument meaning and error behaviour: ``render`` resizes
+the caller's frame and fills it (``mod.rs:86-97``); frames above
+``MAX_DIM`` are rejected with the reference's "pixel limit" message
+(``mod.rs:35-41``); a zero-sized frame returns default stats
+(``cpu.rs:120-122``); backend creation fails with an error, not a crash
+(``mod.rs:115-134``).
+"""
+
+from __future__ import annotations
+
+import ctypes
+import enum
+from abc import ABC, abstractmethod
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _native as N
+from .camera import View
+from .scene import Scene
+
+# src/render/mod.rs:23-33
+DILATION = np.float32(0.3)
+ALPHA_MIN = np.float32(1.0 / 255.0)
+ALPHA_MAX = np.float32(0.99)
+T_MIN = np.float32(1e-4)
+MAX_DIM = 16384
+TILE = 16  # src/render/cpu.rs:34
+
+
+def _pixel_count(width: int, height: int) -> int:
+    if width > MAX_DIM or height > MAX_DIM:
+        raise ValueError(f"frame {width}x{height} exceeds the {MAX_DIM} pixel limit")
+    return width * height
+
+
+class Frame:
+    """8-bit RGB image, row-major (``mod.rs:43-70``); ``pixels`` is (h, w, 3) u8."""
+
+    def __init__(self, width: int = 0, height: int = 0):
+        _pixel_count(width, height)
+        self.width = width
+        self.height = height
+        self.pixels = np.zeros((height, width, 3), np.uint8)
+
+    def resize(self, width: int, height: int):
+        _pixel_count(width, height)
+        self.width, self.height = width, height
+        if self.pixels.shape != (height, width, 3):
+            self.pixels = np.zeros((height, width, 3), np.uint8)
+
+    def get(self, x: int, y: int):
+        return self.pixels[y, x].tolist()
+
+
+@dataclass
+class RenderStats:
+    """``RenderStats`` (``mod.rs:72-83``); ``overlaps`` = (splat, tile) pairs."""
+
+    visible: int = 0
+    overlaps: int = 0
+    project_ms: float = 0.0
+    sort_ms: float = 0.0
+    raster_ms: float = 0.0
+    total_ms: float = 0.0
+
+    @staticmethod
+    def from_c(s: N.RenderStatsC) -> "RenderStats":
+        return RenderStats(int(s.visible), int(s.overlaps), s.project_ms, s.sort_ms, s.raster_ms, s.total_ms)
+
+
+class Renderer(ABC):
+    """A rasterizer backend bound to one scene (``mod.rs:85-97``)."""
+
+    @abstractmethod
+    def name(self) -> str: ...
+
+    @abstractmethod
+    def render(self, view: View, width: int, height: int, background, frame: Frame) -> RenderStats: ...
+
+
+class Backend(enum.Enum):
+    """Backends of this package. The reference's ``cpu``/``cpu-naive``/``gpu``
+    backends are its own Rust/wgpu code and are not part of this package."""
+
+    CUDA = "cuda"
+
+    @staticmethod
+    def all():
+        return [Backend.CUDA]
+
+
+def _view_desc(view: View) -> N.ViewDesc:
+    v = N.ViewDesc()
+    a = view.to_array()
+    for i in range(3):
+        v.eye[i], v.right[i], v.down[i], v.forward[i] = a[i], a[3 + i], a[6 + i], a[9 + i]
+    v.fov_y, v.near_plane = a[12], a[13]
+    return v
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+class CudaRenderer(Renderer):
+    """The sm_100a backend: uploads the scene once, renders views on `device`."""
+
+    def __init__(self, scene: Scene, device: int = 0):
+        L = N.lib()
+        n = len(scene)
+        self._keep = [_f32(scene.positions), _f32(scene.opacities), _f32(scene.colors), _f32(scene.cov3d),
+                      _f32(scene.sh_rest.reshape(n, -1) if scene.sh_degree > 0 else np.zeros(1, np.float32))]
+        d = N.SceneDesc()
+        d.n = n
+        d.sh_degree = scene.sh_degree
+        d.precision = N.SPLAT_PRECISION_FP32
+        d.positions, d.opacities, d.colors, d.cov3d, d.sh_rest = [a.ctypes.data for a in self._keep]
+        h = ctypes.c_void_p()
+        rc = L.splat_cuda_create(ctypes.byref(d), device, ctypes.byref(h))
+        if rc != N.SPLAT_OK:
+            raise N.SplatError(rc, L.splat_cuda_create_error().decode())
+        self._keep = None  # the scene lives on the device now
+        self._h = h
+        self.n = n
+        self.device = device
+
+    # --- Renderer ---------------------------------------------------------
+    def name(self) -> str:
+        return N.lib().splat_cuda_backend_name().decode()
+
+    def render(self, view: View, width: int, height: int, background=(0.0, 0.0, 0.0), frame: Frame = None,
+               downsample: int = 1) -> RenderStats:
+        """Render into `frame` (resized to the output size). With
+        downsample f > 1 the frame is term::downsample'd by f on the device
+        and `frame` becomes floor(w/f) x floor(h/f)."""
+        f = max(int(downsample), 1)
+        if frame is None:
+            frame = Frame()
+        _pixel_count(width, height)
+        frame.resize(width // f, height // f)
+        bg = _f32(background)
+        st = N.RenderStatsC()
+        rc = N.lib().splat_cuda_render(self._h, ctypes.byref(_view_desc(view)), width, height,
+                                       bg.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), f,
+                                       frame.pixels.ctypes.data, frame.pixels.nbytes, ctypes.byref(st))
+        N.check(rc, self._h, "render")
+        return RenderStats.from_c(st)
+
+    # --- device-side entry points --------------------------------------------
+    def render_into(self, view: View, width: int, height: int, background, out_ptr: int, out_bytes: int,
+                    downsample: int = 1) -> RenderStats:
+        """Render into caller-owned HOST memory at `out_ptr` (e.g. a pinned
+        torch tensor's data_ptr()); blocks until the frame is there."""
+        bg = _f32(background)
+        st = N.RenderStatsC()
+        rc = N.lib().splat_cuda_render(self._h, ctypes.byref(_view_desc(view)), width, height,
+                                       bg.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), max(int(downsample), 1),
+                                       out_ptr, out_bytes, ctypes.byref(st))
+        N.check(rc, self._h, "render")
+        return RenderStats.from_c(st)
+
+    def render_device(self, view: View, width: int, height: int, background, dev_ptr: int, out_bytes: int,
+                      downsample: int = 1):
+        """Enqueue a frame into DEVICE memory `dev_ptr` on this renderer's
+        stream; no host synchronisation (pair with `finish`)."""
+        bg = _f32(background)
+        rc = N.lib().splat_cuda_render_device(self._h, ctypes.byref(_view_desc(view)), width, height,
+                                              bg.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                              max(int(downsample), 1), dev_ptr, out_bytes)
+        N.check(rc, self._h, "render_device")
+
+    def finish(self):
+        """Wait for enqueued frames; returns (stats of the last, regrown)."""
+        st = N.RenderStatsC()
+        regrown = ctypes.c_int(0)
+        N.check(N.lib().splat_cuda_finish(self._h, ctypes.byref(st), ctypes.byref(regrown)), self._h, "finish")
+        return RenderStats.from_c(st), bool(regrown.value)
+
+    def set_stream(self, stream_ptr: int):
+        N.check(N.lib().splat_cuda_set_stream(self._h, stream_ptr or None), self._h, "set_stream")
+
+    def stream(self) -> int:
+        return N.lib().splat_cuda_get_stream(self._h) or 0
+
+    def set_option(self, option: int, value: int):
+        N.check(N.lib().splat_cuda_set_option(self._h, option, int(value)), self._h, "set_option")
+
+    def get_option(self, option: int) -> int:
+        v = ctypes.c_uint64(0)
+        N.check(N.lib().splat_cuda_get_option(self._h, option, ctypes.byref(v)), self._h, "get_option")
+        return int(v.value)
+
+    def set_exact(self, exact: bool):
+        """Blend with the reference cpu backend's exact f32 arithmetic."""
+        self.set_option(N.SPLAT_OPT_EXACT_BLEND, int(exact))
+
+    def debug_dump(self, width: int, height: int):
+        """Intermediate buffers of the last frame (needs SPLAT_OPT_DEBUG_CAPTURE):
+        dict with proj (n, 8), visible (n,), color (n, 3), keys, values, ranges."""
+        L = N.lib()
+        n = self.n
+        proj = np.zeros((n, 8), np.float32)
+        vis = np.zeros(n, np.uint8)
+        col = np.zeros((n, 3), np.float32)
+        npairs = ctypes.c_uint64(0)
+        tiles = ((width + TILE - 1) // TILE) * ((height + TILE - 1) // TILE)
+        ranges = np.zeros((tiles, 2), np.uint32)
+        N.check(L.splat_cuda_debug_dump(self._h, None, None, None, None, None, 0, None, 0, ctypes.byref(npairs)),
+                self._h, "debug_dump")
+        p = int(npairs.value)
+        keys = np.zeros(max(p, 1), np.uint64)
+        vals = np.zeros(max(p, 1), np.uint32)
+        N.check(L.splat_cuda_debug_dump(self._h, proj.ctypes.data, vis.ctypes.data, col.ctypes.data,
+                                        keys.ctypes.data, vals.ctypes.data, p, ranges.ctypes.data, ranges.size,
+                                        ctypes.byref(npairs)), self._h, "debug_dump")
+        return {"proj": proj, "visible": vis.astype(bool), "color": col, "keys": keys[:p], "values": vals[:p],
+                "ranges": ranges}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            N.lib().splat_cuda_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def create(backend: Backend, scene: Scene, device: int = 0) -> Renderer:
+    """``render::create`` (``mod.rs:115-121``)."""
+    if backend == Backend.CUDA:
+        return CudaRenderer(scene, device)
+    raise ValueError(f"unknown backend {backend!r}")
