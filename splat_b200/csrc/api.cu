@@ -215,7 +215,7 @@ int enqueue_frame(splat_cuda_handle* h, const FrameParams& fp, uint8_t* dev_out)
     CK(launch_sort(key_bits, h->cap, h->keys[0], h->vals[0], h->keys[1], h->vals[1], h->lookback, h->lb_parts, h->st,
                    h->num_sms, s),
        "sort kernels");
-    CK(launch_ranges(h->cap, h->keys, h->ranges, h->st, h->num_sms, s), "ranges kernel");
+    CK(launch_ranges(h->cap, h->keys, h->ranges, (uint32_t)tiles, h->st, h->num_sms, s), "ranges kernel");
   }
   if (h->stage_events) CK(cudaEventRecord(h->ev[2], s), "event");
   const uint32_t* vals[2] = {h->vals[0], h->vals[1]};

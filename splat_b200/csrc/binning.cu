@@ -78,7 +78,7 @@ __global__ void __launch_bounds__(kEmitThreads) k_emit(uint32_t tiles_x, const B
           uint32_t spins = 0;
           d = ld_volatile(&desc[idx]);
           while ((d >> 62) == 0ull) {
-            if (++spins > kSpinLimit) {
+            if (++spins > kSpinLimit || ((spins & 1023u) == 0u && (*(volatile uint32_t*)&st->error & kErrEmitTimeout))) {
               atomicOr(&st->error, kErrEmitTimeout);
               d = kFlagInc;
               break;

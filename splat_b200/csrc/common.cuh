@@ -25,7 +25,7 @@ constexpr uint64_t kMaxPairs = (1ull << 30) - 1;
 // Bounded spin of every device-side wait (decoupled look-back). A wait that
 // runs out sets an error bit and the kernel carries on without writing out of
 // bounds; the host turns the bit into SPLAT_ERR_TIMEOUT.
-constexpr uint32_t kSpinLimit = 1u << 24;
+constexpr uint32_t kSpinLimit = 1u << 20;
 
 enum ErrorBits : uint32_t {
   kErrEmitTimeout = 1u,
@@ -99,8 +99,8 @@ cudaError_t launch_emit(const FrameParams& fp, const BinInfo* bin, uint64_t n, u
 cudaError_t launch_sort(uint32_t key_bits, uint64_t cap, uint64_t* keys0, uint32_t* vals0, uint64_t* keys1,
                         uint32_t* vals1, uint32_t* lookback, uint64_t lookback_parts, DevState* st,
                         int num_sms, cudaStream_t stream);
-cudaError_t launch_ranges(uint64_t cap, uint64_t* const* keys, uint2* ranges, DevState* st, int num_sms,
-                          cudaStream_t stream);
+cudaError_t launch_ranges(uint64_t cap, uint64_t* const* keys, uint2* ranges, uint32_t tiles, DevState* st,
+                          int num_sms, cudaStream_t stream);
 cudaError_t launch_blend(const FrameParams& fp, const Record* rec, const uint32_t* const* vals, const uint2* ranges,
                          const DevState* st, bool exact, uint8_t* out, uint8_t* full_scratch, cudaStream_t stream);
 

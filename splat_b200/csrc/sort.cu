@@ -151,7 +151,8 @@ __global__ void __launch_bounds__(kSortThreads, 2) k_onesweep(int d, uint64_t ca
         uint32_t v = *(const volatile uint32_t*)q;
         uint32_t spins = 0;
         while ((v >> 30) == 0u) {
-          if (++spins > kSpinLimit) {
+          // Give up at the bound, or at once after another wait gave up.
+          if (++spins > kSpinLimit || ((spins & 1023u) == 0u && (*(volatile uint32_t*)&st->error & kErrSortTimeout))) {
             atomicOr(&st->error, kErrSortTimeout);
             v = kLbInc;
             break;
@@ -186,11 +187,12 @@ __global__ void __launch_bounds__(kSortThreads, 2) k_onesweep(int d, uint64_t ca
 }
 
 __global__ void __launch_bounds__(256) k_ranges(uint64_t cap, const uint64_t* k0, const uint64_t* k1,
-                                                uint2* __restrict__ ranges, const DevState* st) {
+                                                uint2* __restrict__ ranges, uint32_t tiles, const DevState* st) {
   const uint64_t* __restrict__ keys = st->final_sel ? k1 : k0;
   const uint64_t P = pair_count(st, cap);
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < P; i += (uint64_t)gridDim.x * blockDim.x) {
     const uint32_t t = (uint32_t)(keys[i] >> 32);
+    if (t >= tiles) continue;
     if (i == 0 || (uint32_t)(keys[i - 1] >> 32) != t) ranges[t].x = (uint32_t)i;
     if (i + 1 == P || (uint32_t)(keys[i + 1] >> 32) != t) ranges[t].y = (uint32_t)(i + 1);
   }
@@ -211,9 +213,9 @@ cudaError_t launch_sort(uint32_t key_bits, uint64_t cap, uint64_t* keys0, uint32
   return cudaGetLastError();
 }
 
-cudaError_t launch_ranges(uint64_t cap, uint64_t* const* keys, uint2* ranges, DevState* st, int num_sms,
-                          cudaStream_t stream) {
-  k_ranges<<<num_sms * 4, 256, 0, stream>>>(cap, keys[0], keys[1], ranges, st);
+cudaError_t launch_ranges(uint64_t cap, uint64_t* const* keys, uint2* ranges, uint32_t tiles, DevState* st,
+                          int num_sms, cudaStream_t stream) {
+  k_ranges<<<num_sms * 4, 256, 0, stream>>>(cap, keys[0], keys[1], ranges, tiles, st);
   return cudaGetLastError();
 }
 
