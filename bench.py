@@ -52,6 +52,8 @@ def parse():
     p.add_argument("--splats", type=int, default=N_SPLATS)
     p.add_argument("--cpu-sample-s", type=float, default=15.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--profile", action="store_true",
+                   help="render --warmup then --steps frames and exit (a short command for ncu captures)")
     return p.parse_args()
 
 
@@ -226,6 +228,15 @@ def run_ours(args):
         if world > 1:
             torch.distributed.barrier()
         torch.cuda.synchronize()
+
+    if args.profile:
+        for i in range(args.steps):
+            r.render_device(views[i % len(views)], W, H, (0, 0, 0), out.data_ptr(), nbytes)
+            s, _ = r.finish()
+        if rank == 0:
+            print(json.dumps({"profile_frames": args.steps, "visible": s.visible, "pairs": s.overlaps}), flush=True)
+        r.close()
+        return
 
     # Timed region: K frames enqueued back to back on the renderer's stream.
     K = args.steps
