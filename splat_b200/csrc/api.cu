@@ -1,10 +1,10 @@
 // C ABI of the B200 rasterizer (include/splat_cuda.h): scene upload, buffer
 // management, the per-frame launch sequence and the host<->device boundary.
 //
-// One frame is: clear the frame state -> project (a) -> scan + emit pairs (b)
-// -> digit histogram, pass schedule, onesweep passes (c) -> tile ranges (c)
-// -> blend + downsample (d) -> one device-to-host copy of the frame and the
-// frame state. The host never waits in the middle of a frame; pair counts
+// One frame is: clear the frame state -> project + compact visible splats (a)
+// -> depth sort of the visible splats (c) -> scan + emit pairs in depth order
+// (b) -> tile sort of the pairs and tile ranges (c) -> blend + downsample (d)
+// -> one device-to-host copy of the frame and the frame state. The host never waits in the middle of a frame; pair counts
 // that exceed the allocated capacity are detected from the frame state after
 // the frame, the buffers grow and the frame is rendered again (the
 // reference's grow-and-retry, src/render/gpu.rs:1040-1056).
@@ -40,13 +40,16 @@ struct splat_cuda_handle {
   // per-splat frame buffers
   Record* rec = nullptr;
   BinInfo* bin = nullptr;
-  unsigned long long* emit_desc = nullptr;
+  unsigned long long* desc_project = nullptr;  // scan descriptors, one per partition
+  unsigned long long* desc_emit = nullptr;
+  uint64_t* depth_words[2] = {nullptr, nullptr};
+  uint32_t* lb_depth = nullptr;  // look-back words of the depth sort
+  uint64_t lb_depth_parts = 0;
   // pair buffers
   uint64_t cap = 0;
-  uint64_t* keys[2] = {nullptr, nullptr};
-  uint32_t* vals[2] = {nullptr, nullptr};
-  uint32_t* lookback = nullptr;
-  uint64_t lb_parts = 0;
+  uint64_t* pairs[2] = {nullptr, nullptr};
+  uint32_t* lb_tile = nullptr;  // look-back words of the tile sort
+  uint64_t lb_tile_parts = 0;
   // per-size buffers
   uint2* ranges = nullptr;
   uint64_t ranges_cap = 0;  // tiles
@@ -70,7 +73,6 @@ struct splat_cuda_handle {
   // last frame
   FrameParams last_fp{};
   bool have_frame = false;
-  uint32_t last_digits = 0;
   std::string err;
 };
 
@@ -105,21 +107,19 @@ uint32_t bits_for(uint64_t v) {  // bits needed to hold values < v
   return b;
 }
 
+void free_pairs(splat_cuda_handle* h) {
+  for (int b = 0; b < 2; b++) dfree(h->pairs[b]);
+  dfree(h->lb_tile);
+  h->cap = 0;
+}
+
 int ensure_pairs(splat_cuda_handle* h, uint64_t cap) {
   if (cap <= h->cap) return SPLAT_OK;
   if (cap > kMaxPairs) return fail(h, SPLAT_ERR_CAPACITY, "more than 2^30 - 1 gaussian/tile pairs");
-  for (int b = 0; b < 2; b++) {
-    dfree(h->keys[b]);
-    dfree(h->vals[b]);
-  }
-  dfree(h->lookback);
-  h->cap = 0;
-  for (int b = 0; b < 2; b++) {
-    CK(cudaMalloc(&h->keys[b], cap * sizeof(uint64_t)), "cudaMalloc keys");
-    CK(cudaMalloc(&h->vals[b], cap * sizeof(uint32_t)), "cudaMalloc values");
-  }
-  h->lb_parts = (cap + kSortPart - 1) / kSortPart;
-  CK(cudaMalloc(&h->lookback, (size_t)kMaxDigits * h->lb_parts * 256 * sizeof(uint32_t)), "cudaMalloc lookback");
+  free_pairs(h);
+  for (int b = 0; b < 2; b++) CK(cudaMalloc(&h->pairs[b], cap * sizeof(uint64_t)), "cudaMalloc pairs");
+  h->lb_tile_parts = (cap + kSortPart - 1) / kSortPart;
+  CK(cudaMalloc(&h->lb_tile, (size_t)kMaxPasses * h->lb_tile_parts * 256 * sizeof(uint32_t)), "cudaMalloc lookback");
   h->cap = cap;
   return SPLAT_OK;
 }
@@ -193,33 +193,40 @@ int enqueue_frame(splat_cuda_handle* h, const FrameParams& fp, uint8_t* dev_out)
   int rc = ensure_size(h, tiles, 0, full_bytes);
   if (rc) return rc;
   cudaStream_t s = h->stream;
+  const int tile_digits = (int)((bits_for(tiles) + 7) / 8);
   CK(cudaMemsetAsync(h->st, 0, sizeof(DevState), s), "clear frame state");
   CK(cudaMemsetAsync(h->ranges, 0, tiles * sizeof(uint2), s), "clear ranges");
-  const uint32_t key_bits = 32 + bits_for(tiles);
-  const uint32_t digits = (key_bits + 7) / 8;
-  h->last_digits = digits;
   if (h->n) {
-    CK(cudaMemsetAsync(h->emit_desc, 0, ((h->n + 511) / 512) * sizeof(unsigned long long), s), "clear scan");
-    CK(cudaMemsetAsync(h->lookback, 0, (size_t)digits * h->lb_parts * 256 * sizeof(uint32_t), s), "clear lookback");
+    const size_t nd = ((h->n + kScanThreads - 1) / kScanThreads) * sizeof(unsigned long long);
+    CK(cudaMemsetAsync(h->desc_project, 0, nd, s), "clear scan");
+    CK(cudaMemsetAsync(h->desc_emit, 0, nd, s), "clear scan");
+    CK(cudaMemsetAsync(h->lb_depth, 0, (size_t)kMaxPasses * h->lb_depth_parts * 256 * sizeof(uint32_t), s),
+       "clear lookback");
+    if (tile_digits)
+      CK(cudaMemsetAsync(h->lb_tile, 0, (size_t)tile_digits * h->lb_tile_parts * 256 * sizeof(uint32_t), s),
+         "clear lookback");
   }
   if (h->stage_events) CK(cudaEventRecord(h->ev[0], s), "event");
   if (h->n) {
     SceneDev sd{h->pos_op, h->cov_a, h->cov_b, h->color, h->sh, h->n, h->sh_degree};
-    CK(launch_project(fp, sd, h->rec, h->bin, h->debug_capture ? h->dbg_proj : nullptr,
-                      h->debug_capture ? h->dbg_color : nullptr, h->st, s),
+    CK(launch_project(fp, sd, h->rec, h->bin, h->desc_project, h->depth_words[0],
+                      h->debug_capture ? h->dbg_proj : nullptr, h->debug_capture ? h->dbg_color : nullptr, h->st, s),
        "project kernel");
-    CK(launch_emit(fp, h->bin, h->n, h->emit_desc, h->keys[0], h->vals[0], h->cap, h->st, s), "emit kernel");
   }
   if (h->stage_events) CK(cudaEventRecord(h->ev[1], s), "event");
   if (h->n) {
-    CK(launch_sort(key_bits, h->cap, h->keys[0], h->vals[0], h->keys[1], h->vals[1], h->lookback, h->lb_parts, h->st,
-                   h->num_sms, s),
-       "sort kernels");
-    CK(launch_ranges(h->cap, h->keys, h->ranges, (uint32_t)tiles, h->st, h->num_sms, s), "ranges kernel");
+    DevState* st = h->st;
+    CK(launch_sort(&st->depth, &st->visible, h->n, 0, kMaxPasses, h->depth_words[0], h->depth_words[1], h->lb_depth,
+                   h->lb_depth_parts, st, h->num_sms, s),
+       "depth sort");
+    CK(launch_emit(fp, h->bin, h->n, h->desc_emit, h->depth_words, h->pairs[0], h->cap, st, s), "emit kernel");
+    CK(launch_sort(&st->tile, &st->total_pairs, h->cap, 0, tile_digits, h->pairs[0], h->pairs[1], h->lb_tile,
+                   h->lb_tile_parts, st, h->num_sms, s),
+       "tile sort");
+    CK(launch_ranges(h->cap, h->pairs, h->ranges, (uint32_t)tiles, st, h->num_sms, s), "ranges kernel");
   }
   if (h->stage_events) CK(cudaEventRecord(h->ev[2], s), "event");
-  const uint32_t* vals[2] = {h->vals[0], h->vals[1]};
-  CK(launch_blend(fp, h->rec, vals, h->ranges, h->st, h->exact, dev_out, h->full_dev, s), "blend kernel");
+  CK(launch_blend(fp, h->rec, h->pairs, h->ranges, h->st, h->exact, dev_out, h->full_dev, s), "blend kernel");
   if (h->stage_events) CK(cudaEventRecord(h->ev[3], s), "event");
   CK(cudaMemcpyAsync(h->st_host, h->st, sizeof(DevState), cudaMemcpyDeviceToHost, s), "copy frame state");
   h->last_fp = fp;
@@ -367,8 +374,15 @@ SPLAT_API int splat_cuda_create(const splat_scene_desc* d, int device, splat_cud
     }
     if ((e = cudaMalloc(&h->rec, n * sizeof(Record))) != cudaSuccess) return bail(cuda_fail(h, e, "cudaMalloc records"));
     if ((e = cudaMalloc(&h->bin, n * sizeof(BinInfo))) != cudaSuccess) return bail(cuda_fail(h, e, "cudaMalloc bins"));
-    if ((e = cudaMalloc(&h->emit_desc, ((n + 511) / 512) * sizeof(unsigned long long))) != cudaSuccess)
-      return bail(cuda_fail(h, e, "cudaMalloc scan"));
+    const size_t nd = ((n + kScanThreads - 1) / kScanThreads) * sizeof(unsigned long long);
+    if ((e = cudaMalloc(&h->desc_project, nd)) != cudaSuccess) return bail(cuda_fail(h, e, "cudaMalloc scan"));
+    if ((e = cudaMalloc(&h->desc_emit, nd)) != cudaSuccess) return bail(cuda_fail(h, e, "cudaMalloc scan"));
+    for (int b = 0; b < 2; b++)
+      if ((e = cudaMalloc(&h->depth_words[b], n * sizeof(uint64_t))) != cudaSuccess)
+        return bail(cuda_fail(h, e, "cudaMalloc depth words"));
+    h->lb_depth_parts = (n + kSortPart - 1) / kSortPart;
+    if ((e = cudaMalloc(&h->lb_depth, (size_t)kMaxPasses * h->lb_depth_parts * 256 * sizeof(uint32_t))) != cudaSuccess)
+      return bail(cuda_fail(h, e, "cudaMalloc lookback"));
   }
   int rc = ensure_pairs(h, std::max<uint64_t>(4 * n, 1u << 16));
   if (rc) return bail(rc);
@@ -452,12 +466,7 @@ SPLAT_API int splat_cuda_set_option(splat_cuda_handle* h, uint32_t option, uint6
     case SPLAT_OPT_PAIR_CAPACITY: {
       if (value == 0 || value > kMaxPairs) return fail(h, SPLAT_ERR_INVALID_ARG, "pair capacity out of range");
       // Shrinking is allowed: reallocate at exactly `value`.
-      for (int b = 0; b < 2; b++) {
-        dfree(h->keys[b]);
-        dfree(h->vals[b]);
-      }
-      dfree(h->lookback);
-      h->cap = 0;
+      free_pairs(h);
       return ensure_pairs(h, value);
     }
     case SPLAT_OPT_STAGE_EVENTS:
@@ -497,19 +506,29 @@ SPLAT_API int splat_cuda_debug_dump(splat_cuda_handle* h, float* proj, uint8_t* 
   const DevState& st = *h->st_host;
   const uint64_t P = std::min<uint64_t>(st.total_pairs, h->cap);
   if (n_pairs) *n_pairs = P;
-  if ((proj || visible || color) && !h->dbg_proj)
+  if ((proj || color) && !h->dbg_proj)
     return fail(h, SPLAT_ERR_INVALID_ARG, "enable SPLAT_OPT_DEBUG_CAPTURE before rendering");
   if (proj) CK(cudaMemcpy(proj, h->dbg_proj, h->n * 8 * sizeof(float), cudaMemcpyDeviceToHost), "dump");
   if (color) CK(cudaMemcpy(color, h->dbg_color, h->n * 3 * sizeof(float), cudaMemcpyDeviceToHost), "dump");
-  if (visible) {
-    std::vector<BinInfo> bin(h->n);
-    CK(cudaMemcpy(bin.data(), h->bin, h->n * sizeof(BinInfo), cudaMemcpyDeviceToHost), "dump");
-    for (uint64_t i = 0; i < h->n; i++) visible[i] = bin[i].rect_lo != kCulled;
+  std::vector<BinInfo> bin;
+  if (visible || keys) {
+    bin.resize(h->n);
+    if (h->n) CK(cudaMemcpy(bin.data(), h->bin, h->n * sizeof(BinInfo), cudaMemcpyDeviceToHost), "dump");
   }
-  const int sel = st.final_sel;
+  if (visible)
+    for (uint64_t i = 0; i < h->n; i++) visible[i] = bin[i].rect_lo != kCulled;
   const uint64_t m = std::min(P, key_capacity);
-  if (keys && m) CK(cudaMemcpy(keys, h->keys[sel], m * 8, cudaMemcpyDeviceToHost), "dump");
-  if (values && m) CK(cudaMemcpy(values, h->vals[sel], m * 4, cudaMemcpyDeviceToHost), "dump");
+  if ((keys || values) && m) {
+    // Pairs are (tile << 32 | splat); the reference's key of a pair is
+    // (tile << 32 | depth bits of its splat).
+    std::vector<uint64_t> pw(m);
+    CK(cudaMemcpy(pw.data(), h->pairs[st.tile.final_sel], m * 8, cudaMemcpyDeviceToHost), "dump");
+    for (uint64_t p = 0; p < m; p++) {
+      const uint32_t splat = (uint32_t)pw[p];
+      if (values) values[p] = splat;
+      if (keys) keys[p] = (pw[p] & 0xFFFFFFFF00000000ull) | (splat < h->n ? bin[splat].depth_bits : 0u);
+    }
+  }
   if (ranges) {
     const uint64_t tiles = (uint64_t)h->last_fp.tiles_x * h->last_fp.tiles_y;
     const uint64_t r = std::min<uint64_t>(tiles * 2, range_capacity);
@@ -530,12 +549,11 @@ SPLAT_API int splat_cuda_destroy(splat_cuda_handle* h) {
   dfree(h->sh);
   dfree(h->rec);
   dfree(h->bin);
-  dfree(h->emit_desc);
-  for (int b = 0; b < 2; b++) {
-    dfree(h->keys[b]);
-    dfree(h->vals[b]);
-  }
-  dfree(h->lookback);
+  dfree(h->desc_project);
+  dfree(h->desc_emit);
+  for (int b = 0; b < 2; b++) dfree(h->depth_words[b]);
+  dfree(h->lb_depth);
+  free_pairs(h);
   dfree(h->ranges);
   dfree(h->out_dev);
   dfree(h->full_dev);

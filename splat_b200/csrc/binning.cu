@@ -1,46 +1,54 @@
 // Kernel (b): device-wide exclusive scan of the per-splat pair counts with
-// warp shuffles and a decoupled look-back (single pass; each CTA takes its
-// partition from a ticket so every predecessor is already resident), fused
-// with the pair emission: each visible splat writes one 64-bit key
-// (tile << 32 | depth bits) and its splat index per tile of its pixel bbox,
-// row-major (ty, then tx) as the reference's `emit` does
-// (src/render/cpu.rs:251-277). Offsets come from the scan in splat-index
-// order, so pairs are laid out in index order and a stable sort by key gives
-// the reference's (tile, depth, scene index) order (src/render/naive.rs:
-// 306-308, src/render/cpu.rs:396-414).
+// warp shuffles and a decoupled look-back, fused with the pair emission.
+//
+// The scan runs over the visible splats in depth order (the output of the
+// depth sort: words depth bits << 32 | splat index, ties in splat-index
+// order). Each visible splat duplicates into one pair per tile of its pixel
+// bbox, row-major (ty, then tx) as the reference's `emit` does
+// (src/render/cpu.rs:251-277); a pair is the 64-bit word tile << 32 | splat.
+// Pairs are therefore laid out in (depth, splat index) order, and the stable
+// tile sort that follows yields the reference's per-tile blending order:
+// by depth, ties by scene index (src/render/naive.rs:306-308,
+// src/render/cpu.rs:396-414). The reference's sort key of a pair,
+// tile << 32 | depth bits, is recovered exactly from the pair's tile and its
+// splat's depth bits.
+//
+// Expansion is warp-cooperative: a warp's pairs are written 32 at a time,
+// each lane locating its pair's splat by a binary search over the warp's
+// inclusive counts, so one large splat does not serialise its warp.
 #include "common.cuh"
+#include "lookback.cuh"
 
 namespace splat {
 namespace {
 
-constexpr int kEmitThreads = 512;
-constexpr int kEmitWarps = kEmitThreads / 32;
+constexpr int kWarps = kScanThreads / 32;
 
-__device__ __forceinline__ unsigned long long ld_volatile(const unsigned long long* p) {
-  return *(const volatile unsigned long long*)p;
-}
-__device__ __forceinline__ void st_volatile(unsigned long long* p, unsigned long long v) {
-  *(volatile unsigned long long*)p = v;
-}
-
-__global__ void __launch_bounds__(kEmitThreads) k_emit(uint32_t tiles_x, const BinInfo* __restrict__ bin, uint64_t n,
-                                                       unsigned long long* desc, uint64_t* __restrict__ keys,
-                                                       uint32_t* __restrict__ vals, uint64_t cap, DevState* st) {
+__global__ void __launch_bounds__(kScanThreads) k_emit(uint32_t tiles_x, const BinInfo* __restrict__ bin,
+                                                       unsigned long long* desc, const uint64_t* dw0,
+                                                       const uint64_t* dw1, uint64_t* __restrict__ pairs,
+                                                       uint64_t cap, DevState* st) {
   __shared__ uint32_t s_part;
-  __shared__ uint32_t s_warp[kEmitWarps];
-  __shared__ unsigned long long s_excl;
+  __shared__ uint32_t s_warp[kWarps];
+  __shared__ unsigned long long s_base;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint64_t V = *(const volatile unsigned long long*)&st->visible;
+  const uint64_t nparts = (V + kScanThreads - 1) / kScanThreads;
   if (tid == 0) s_part = atomicAdd(&st->emit_ticket, 1u);
   __syncthreads();
   const uint32_t part = s_part;
-  const uint64_t nparts = (n + kEmitThreads - 1) / kEmitThreads;
-  const uint64_t i = (uint64_t)part * kEmitThreads + tid;
-  BinInfo b{kCulled, 0u, 0u, 0u};
-  if (i < n) b = bin[i];
-  const uint32_t cnt = (b.rect_lo != kCulled) ? b.count : 0u;
-
-  // Block-wide exclusive scan of the counts.
-  uint32_t x = cnt;
+  if (part >= nparts) return;  // uniform across the block
+  const uint64_t* __restrict__ dsorted = st->depth.final_sel ? dw1 : dw0;
+  const uint64_t q = (uint64_t)part * kScanThreads + tid;
+  uint32_t idx = 0, cnt = 0, rect_lo = 0, rect_hi = 0;
+  if (q < V) {
+    idx = (uint32_t)dsorted[q];
+    const BinInfo b = bin[idx];
+    cnt = b.count;
+    rect_lo = b.rect_lo;
+    rect_hi = b.rect_hi;
+  }
+  uint32_t x = cnt;  // inclusive prefix within the warp
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
     const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
@@ -49,87 +57,62 @@ __global__ void __launch_bounds__(kEmitThreads) k_emit(uint32_t tiles_x, const B
   if (lane == 31) s_warp[warp] = x;
   __syncthreads();
   if (warp == 0) {
-    uint32_t w = lane < kEmitWarps ? s_warp[lane] : 0u;
+    const uint32_t c = lane < kWarps ? s_warp[lane] : 0u;
+    uint32_t w = c;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
       if (lane >= o) w += y;
     }
-    if (lane < kEmitWarps) s_warp[lane] = w;  // inclusive per warp
-  }
-  __syncthreads();
-  const uint32_t warp_excl = warp ? s_warp[warp - 1] : 0u;
-  const uint32_t local_excl = warp_excl + x - cnt;
-  const unsigned long long block_total = s_warp[kEmitWarps - 1];
-
-  // Decoupled look-back over the partition descriptors (warp 0).
-  if (warp == 0) {
-    unsigned long long excl = 0;
-    if (part == 0) {
-      if (lane == 0) st_volatile(&desc[0], kFlagInc | block_total);
-    } else {
-      if (lane == 0) st_volatile(&desc[part], kFlagAgg | block_total);
-      long long j = (long long)part - 1;
-      bool done = false;
-      while (!done) {
-        const long long idx = j - lane;
-        unsigned long long d = kFlagInc;  // before partition 0: an inclusive zero
-        if (idx >= 0) {
-          uint32_t spins = 0;
-          d = ld_volatile(&desc[idx]);
-          while ((d >> 62) == 0ull) {
-            if (++spins > kSpinLimit || ((spins & 1023u) == 0u && (*(volatile uint32_t*)&st->error & kErrEmitTimeout))) {
-              atomicOr(&st->error, kErrEmitTimeout);
-              d = kFlagInc;
-              break;
-            }
-            __nanosleep(20);
-            d = ld_volatile(&desc[idx]);
-          }
-        }
-        const unsigned inc = __ballot_sync(0xffffffffu, (d >> 62) == 2ull);
-        unsigned long long v = d & kValMask;
-        if (inc) {
-          const int first = __ffs(inc) - 1;
-          if (lane > first) v = 0;
-          done = true;
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        excl += v;
-        j -= 32;
-      }
-      if (lane == 0) st_volatile(&desc[part], kFlagInc | (excl + block_total));
-    }
+    const uint32_t total = __shfl_sync(0xffffffffu, w, 31);
+    if (lane < kWarps) s_warp[lane] = w - c;  // exclusive per warp
+    const unsigned long long base = lookback_exclusive(desc, part, total, st, kErrEmitTimeout);
     if (lane == 0) {
-      s_excl = excl;
-      if ((uint64_t)part == nparts - 1) st->total_pairs = excl + block_total;
+      s_base = base;
+      if ((uint64_t)part == nparts - 1) st->total_pairs = base + total;
     }
   }
   __syncthreads();
 
-  if (cnt) {
-    uint64_t off = s_excl + local_excl;
-    const uint32_t tx0 = b.rect_lo & 0xFFFFu, ty0 = b.rect_lo >> 16;
-    const uint32_t tx1 = b.rect_hi & 0xFFFFu, ty1 = b.rect_hi >> 16;
-    const uint64_t lo = b.depth_bits;
-    for (uint32_t ty = ty0; ty < ty1 && off < cap; ty++) {
-      for (uint32_t tx = tx0; tx < tx1; tx++, off++) {
-        if (off >= cap) break;
-        keys[off] = ((uint64_t)(ty * tiles_x + tx) << 32) | lo;
-        vals[off] = (uint32_t)i;
-      }
+  const uint64_t warp_base = s_base + s_warp[warp];
+  const uint32_t warp_total = __shfl_sync(0xffffffffu, x, 31);
+  const uint32_t my_excl = x - cnt;
+  for (uint32_t c0 = 0; c0 < warp_total; c0 += 32) {
+    const uint32_t k = c0 + lane;
+    // owner = number of lanes whose inclusive count is <= k
+    uint32_t pos = 0;
+#pragma unroll
+    for (uint32_t s = 16; s > 0; s >>= 1) {
+      const uint32_t xv = __shfl_sync(0xffffffffu, x, pos + s - 1);
+      if (xv <= k) pos += s;
+    }
+    const uint32_t owner = pos < 32 ? pos : 31;
+    const uint32_t o_lo = __shfl_sync(0xffffffffu, rect_lo, owner);
+    const uint32_t o_hi = __shfl_sync(0xffffffffu, rect_hi, owner);
+    const uint32_t o_ex = __shfl_sync(0xffffffffu, my_excl, owner);
+    const uint32_t o_id = __shfl_sync(0xffffffffu, idx, owner);
+    if (k < warp_total) {
+      const uint32_t tx0 = o_lo & 0xFFFFu, ty0 = o_lo >> 16, tx1 = o_hi & 0xFFFFu;
+      const uint32_t wdt = tx1 - tx0;
+      const uint32_t local = k - o_ex;
+      const uint32_t row = local / wdt;
+      const uint32_t tile = (ty0 + row) * tiles_x + tx0 + (local - row * wdt);
+      const uint64_t off = warp_base + k;
+      if (off < cap) pairs[off] = ((uint64_t)tile << 32) | o_id;
     }
   }
 }
 
 }  // namespace
 
-cudaError_t launch_emit(const FrameParams& fp, const BinInfo* bin, uint64_t n, unsigned long long* emit_desc,
-                        uint64_t* keys, uint32_t* vals, uint64_t cap, DevState* st, cudaStream_t stream) {
+cudaError_t launch_emit(const FrameParams& fp, const BinInfo* bin, uint64_t n, unsigned long long* scan_desc,
+                        uint64_t* const* depth_words, uint64_t* pairs, uint64_t cap, DevState* st,
+                        cudaStream_t stream) {
   if (n == 0) return cudaSuccess;
-  const unsigned grid = (unsigned)((n + kEmitThreads - 1) / kEmitThreads);
-  k_emit<<<grid, kEmitThreads, 0, stream>>>(fp.tiles_x, bin, n, emit_desc, keys, vals, cap, st);
+  // Enough CTAs for every splat being visible; CTAs past the visible count return at once.
+  const unsigned grid = (unsigned)((n + kScanThreads - 1) / kScanThreads);
+  k_emit<<<grid, kScanThreads, 0, stream>>>(fp.tiles_x, bin, scan_desc, depth_words[0], depth_words[1], pairs, cap,
+                                            st);
   return cudaGetLastError();
 }
 

@@ -5,8 +5,10 @@
 // of the tile so a splat whose pixel bbox misses the block is skipped by the
 // whole warp. The tile's depth-sorted splat list is walked in batches of 256:
 // the CTA gathers the batch's 48-byte records into shared memory (one per
-// thread, coalesced index loads), then every pixel blends the batch front to
-// back. A pixel stops once its transmittance drops below T_MIN; the CTA stops
+// thread, coalesced index loads, the next batch's gather in flight while the
+// current one blends), storing each splat's bbox as a row/column bit mask so
+// the per-pixel bbox test is one AND and one compare; then every pixel blends
+// the batch front to back. A pixel stops once its transmittance drops below T_MIN; the CTA stops
 // when a block vote finds no live pixel (the reference stops a tile when all
 // its row masks are empty, src/render/cpu.rs:693-702).
 //
@@ -65,12 +67,17 @@ __device__ __forceinline__ uint32_t to_u8(float v) {
 
 template <bool EXACT>
 __global__ void __launch_bounds__(256) k_blend(FrameParams fp, const Record* __restrict__ rec,
-                                               const uint32_t* __restrict__ v0, const uint32_t* __restrict__ v1,
+                                               const uint64_t* __restrict__ p0, const uint64_t* __restrict__ p1,
                                                const uint2* __restrict__ ranges, const DevState* st,
                                                uint8_t* __restrict__ out, uint8_t* __restrict__ full) {
-  __shared__ float4 s_r0[256];
-  __shared__ float4 s_r1[256];
-  __shared__ float4 s_r2[256];
+  // Per batch entry: the splat's pixel bbox clipped to this tile as a bit
+  // mask (columns in bits 0-15, rows in bits 16-31), then its geometry and
+  // colour. The default path stores the centre relative to the tile's first
+  // pixel centre and the conic pre-scaled by log2(e) for exp2.
+  __shared__ uint32_t s_mask[256];
+  __shared__ float4 s_a[256];  // x, y, -a/2, -b   (scaled / shifted when !EXACT)
+  __shared__ float4 s_b[256];  // -c/2, opacity, red, green
+  __shared__ float s_c[256];   // blue
   __shared__ uint32_t s_px[256];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const uint32_t tile = blockIdx.x;
@@ -79,71 +86,92 @@ __global__ void __launch_bounds__(256) k_blend(FrameParams fp, const Record* __r
   const uint32_t lx = (warp & 1) * 8 + (lane & 7), ly = (warp >> 1) * 4 + (lane >> 3);
   const uint32_t px = ox + lx, py = oy + ly;
   const bool inside = px < fp.w && py < fp.h;
-  const uint32_t* __restrict__ vals = st->final_sel ? v1 : v0;
+  const uint32_t mybits = (1u << lx) | (1u << (16 + ly));
+  const uint64_t* __restrict__ pairs = st->tile.final_sel ? p1 : p0;
   const uint2 range = ranges[tile];
   const uint32_t begin = range.x, end = range.y > range.x ? range.y : range.x;
 
-  // Pixel-centre terms in the reference's association:
-  // dx = lane + ((g*4) + ((ox + 0.5) - x)), dy = ((oy + ly) + 0.5) - y.
+  // EXACT: dx = lane + ((g*4) + ((ox + 0.5) - x)), dy = ((oy + ly) + 0.5) - y
+  // in the reference's association (src/render/cpu.rs:658-671).
   const float fx05 = __fadd_rn((float)ox, 0.5f);
   const float gbase = (float)(lx & ~3u), lanef = (float)(lx & 3u);
   const float rowc = __fadd_rn(__fadd_rn((float)oy, (float)ly), 0.5f);
-  const float pxc = (float)px + 0.5f, pyc = (float)py + 0.5f;
+  const float lxf = (float)lx, lyf = (float)ly;
+  const float ox05 = (float)ox + 0.5f, oy05 = (float)oy + 0.5f;
 
   float T = 1.0f, cr = 0.0f, cg = 0.0f, cb = 0.0f;
   bool done = !inside;
+
+  // The next batch's record is gathered into registers while the current
+  // batch is blended.
+  Record nr;
+  bool has = false;
+  if (begin + tid < end) {
+    nr = rec[(uint32_t)pairs[begin + tid]];
+    has = true;
+  }
   for (uint32_t start = begin; start < end; start += 256) {
-    const uint32_t idx = start + tid;
-    if (idx < end) {
-      const Record r = rec[vals[idx]];
-      float4 a = r.r0, b = r.r1;
-      if (!EXACT) {  // pre-scale the conic terms by log2(e) for exp2
+    if (has) {
+      const uint32_t bx = __float_as_uint(nr.r2.y), by = __float_as_uint(nr.r2.z);
+      const int x0 = min(max((int)(bx & 0xFFFFu) - (int)ox, 0), 16), x1 = min(max((int)(bx >> 16) - (int)ox, 0), 16);
+      const int y0 = min(max((int)(by & 0xFFFFu) - (int)oy, 0), 16), y1 = min(max((int)(by >> 16) - (int)oy, 0), 16);
+      const uint32_t xb = ((1u << x1) - 1u) & ~((1u << x0) - 1u);
+      const uint32_t yb = ((1u << y1) - 1u) & ~((1u << y0) - 1u);
+      s_mask[tid] = xb | (yb << 16);
+      float4 a = nr.r0, b = nr.r1;
+      if (!EXACT) {
+        a.x -= ox05;
+        a.y -= oy05;
         a.z *= kLog2e;
         a.w *= kLog2e;
         b.x *= kLog2e;
       }
-      s_r0[tid] = a;
-      s_r1[tid] = b;
-      s_r2[tid] = r.r2;
+      s_a[tid] = a;
+      s_b[tid] = b;
+      s_c[tid] = nr.r2.x;
     }
     __syncthreads();
+    const uint32_t nxt = start + 256 + tid;
+    has = nxt < end;
+    if (has) nr = rec[(uint32_t)pairs[nxt]];
     const uint32_t cnt = min(256u, end - start);
     if (!done) {
       for (uint32_t j = 0; j < cnt; j++) {
-        const float4 r2 = s_r2[j];
-        const uint32_t bx = __float_as_uint(r2.y), by = __float_as_uint(r2.z);
-        if (px < (bx & 0xFFFFu) || px >= (bx >> 16) || py < (by & 0xFFFFu) || py >= (by >> 16)) continue;
-        const float4 r0 = s_r0[j];
-        const float4 r1 = s_r1[j];
+        if ((s_mask[j] & mybits) != mybits) continue;
+        const float4 a = s_a[j];
+        const float4 b = s_b[j];
         float pw, alpha;
         if (EXACT) {
-          const float cx0 = __fsub_rn(fx05, r0.x);
+          const float cx0 = __fsub_rn(fx05, a.x);
           const float dx = __fadd_rn(lanef, __fadd_rn(gbase, cx0));
-          const float qx = __fmul_rn(__fmul_rn(dx, dx), r0.z);
-          const float dy = __fsub_rn(rowc, r0.y);
-          const float qy = __fmul_rn(__fmul_rn(r1.x, dy), dy);
-          const float bdy = __fmul_rn(r0.w, dy);
+          const float qx = __fmul_rn(__fmul_rn(dx, dx), a.z);
+          const float dy = __fsub_rn(rowc, a.y);
+          const float qy = __fmul_rn(__fmul_rn(b.x, dy), dy);
+          const float bdy = __fmul_rn(a.w, dy);
           pw = __fadd_rn(__fadd_rn(qx, qy), __fmul_rn(bdy, dx));
-          alpha = fminf(__fmul_rn(exp_neg_exact(pw), r1.y), kAlphaMax);
+          if (!(pw <= 0.0f)) continue;
+          alpha = fminf(__fmul_rn(exp_neg_exact(pw), b.y), kAlphaMax);
         } else {
-          const float dx = pxc - r0.x;
-          const float dy = pyc - r0.y;
-          pw = fmaf(r0.z * dx, dx, fmaf(r1.x * dy, dy, (r0.w * dy) * dx));
-          alpha = fminf(ex2_approx(pw) * r1.y, kAlphaMax);
+          const float dx = lxf - a.x;
+          const float dy = lyf - a.y;
+          pw = fmaf(dx, fmaf(a.z, dx, a.w * dy), (b.x * dy) * dy);
+          if (!(pw <= 0.0f)) continue;
+          alpha = fminf(ex2_approx(pw) * b.y, kAlphaMax);
         }
-        if (!(pw <= 0.0f && alpha >= kAlphaMin)) continue;
+        if (!(alpha >= kAlphaMin)) continue;
+        const float blue = s_c[j];
         if (EXACT) {
           const float w = __fmul_rn(alpha, T);
-          cr = __fadd_rn(cr, __fmul_rn(r1.z, w));
-          cg = __fadd_rn(cg, __fmul_rn(r1.w, w));
-          cb = __fadd_rn(cb, __fmul_rn(r2.x, w));
+          cr = __fadd_rn(cr, __fmul_rn(b.z, w));
+          cg = __fadd_rn(cg, __fmul_rn(b.w, w));
+          cb = __fadd_rn(cb, __fmul_rn(blue, w));
           T = __fmul_rn(T, __fsub_rn(1.0f, alpha));
         } else {
           const float w = alpha * T;
-          cr = fmaf(r1.z, w, cr);
-          cg = fmaf(r1.w, w, cg);
-          cb = fmaf(r2.x, w, cb);
-          T = T * (1.0f - alpha);
+          cr = fmaf(b.z, w, cr);
+          cg = fmaf(b.w, w, cg);
+          cb = fmaf(blue, w, cb);
+          T = T - w;
         }
         if (T < kTMin) {
           done = true;
@@ -224,14 +252,14 @@ __global__ void k_downsample(FrameParams fp, const uint8_t* __restrict__ full, u
 
 }  // namespace
 
-cudaError_t launch_blend(const FrameParams& fp, const Record* rec, const uint32_t* const* vals, const uint2* ranges,
+cudaError_t launch_blend(const FrameParams& fp, const Record* rec, uint64_t* const* pairs, const uint2* ranges,
                          const DevState* st, bool exact, uint8_t* out, uint8_t* full_scratch, cudaStream_t stream) {
   const unsigned tiles = fp.tiles_x * fp.tiles_y;
   if (tiles == 0) return cudaSuccess;
   if (exact)
-    k_blend<true><<<tiles, 256, 0, stream>>>(fp, rec, vals[0], vals[1], ranges, st, out, full_scratch);
+    k_blend<true><<<tiles, 256, 0, stream>>>(fp, rec, pairs[0], pairs[1], ranges, st, out, full_scratch);
   else
-    k_blend<false><<<tiles, 256, 0, stream>>>(fp, rec, vals[0], vals[1], ranges, st, out, full_scratch);
+    k_blend<false><<<tiles, 256, 0, stream>>>(fp, rec, pairs[0], pairs[1], ranges, st, out, full_scratch);
   if (fp.downsample > 1 && kTile % fp.downsample != 0 && fp.out_w > 0 && fp.out_h > 0) {
     dim3 grid((fp.out_w + 127) / 128, fp.out_h);
     k_downsample<<<grid, 128, 0, stream>>>(fp, full_scratch, out);

@@ -71,42 +71,58 @@ struct __align__(16) BinInfo {
   uint32_t rect_lo, rect_hi, depth_bits, count;
 };
 
-constexpr int kMaxDigits = 8;
+constexpr int kMaxPasses = 4;  // 8-bit digits of a 32-bit sort field
+
+// One stable LSD sort of 64-bit words on (part of) their upper 32 bits.
+struct SortState {
+  unsigned int ticket[kMaxPasses];
+  int pass_src[kMaxPasses];  // per digit pass: source buffer (0/1) or -1 to skip
+  int final_sel;             // buffer holding the sorted words
+  unsigned int pad[3];
+  unsigned int hist[kMaxPasses][256];  // digit histograms, then exclusive starts
+};
 
 // Frame state in device memory, cleared at the start of every frame.
 struct DevState {
+  unsigned long long visible;      // splats that survived culling
   unsigned long long total_pairs;  // sum of per-splat pair counts (may exceed capacity)
-  unsigned int visible;
   unsigned int error;
+  unsigned int project_ticket;
   unsigned int emit_ticket;
-  unsigned int sort_ticket[kMaxDigits];
-  int pass_src[kMaxDigits];        // per digit pass: source buffer (0/1) or -1 to skip
-  int final_sel;                   // buffer holding the sorted pairs
   unsigned int pad[5];
-  unsigned int hist[kMaxDigits][256];  // digit histograms, then exclusive starts
+  SortState depth;  // visible splats by depth: words (depth bits << 32 | splat)
+  SortState tile;   // pairs by tile: words (tile << 32 | splat), already in depth order
 };
 
-// Decoupled look-back descriptor flags (emit scan: 64-bit words).
+// Decoupled look-back descriptor flags (scans: 64-bit words).
 constexpr unsigned long long kFlagAgg = 1ull << 62;
 constexpr unsigned long long kFlagInc = 2ull << 62;
 constexpr unsigned long long kValMask = (1ull << 62) - 1;
 
 // Launchers (each returns the cudaGetLastError of its launches).
-cudaError_t launch_project(const FrameParams& fp, const SceneDev& s, Record* rec, BinInfo* bin, float* dbg_proj,
-                           float* dbg_color, DevState* st, cudaStream_t stream);
-cudaError_t launch_emit(const FrameParams& fp, const BinInfo* bin, uint64_t n, unsigned long long* emit_desc,
-                        uint64_t* keys, uint32_t* vals, uint64_t cap, DevState* st, cudaStream_t stream);
-cudaError_t launch_sort(uint32_t key_bits, uint64_t cap, uint64_t* keys0, uint32_t* vals0, uint64_t* keys1,
-                        uint32_t* vals1, uint32_t* lookback, uint64_t lookback_parts, DevState* st,
-                        int num_sms, cudaStream_t stream);
-cudaError_t launch_ranges(uint64_t cap, uint64_t* const* keys, uint2* ranges, uint32_t tiles, DevState* st,
+// (a) projection + compaction of visible splats into depth words.
+cudaError_t launch_project(const FrameParams& fp, const SceneDev& s, Record* rec, BinInfo* bin,
+                           unsigned long long* scan_desc, uint64_t* depth_words, float* dbg_proj, float* dbg_color,
+                           DevState* st, cudaStream_t stream);
+// (b) pair emission over the depth-sorted splats.
+cudaError_t launch_emit(const FrameParams& fp, const BinInfo* bin, uint64_t n, unsigned long long* scan_desc,
+                        uint64_t* const* depth_words, uint64_t* pairs, uint64_t cap, DevState* st,
+                        cudaStream_t stream);
+// (c) stable LSD sort of words[0] (ping-pong with words[1]) on `digits` 8-bit
+// digits starting at bit 32 + 8 * first_digit.
+cudaError_t launch_sort(SortState* ss, const unsigned long long* count, uint64_t cap, int first_digit, int digits,
+                        uint64_t* words0, uint64_t* words1, uint32_t* lookback, uint64_t lookback_parts,
+                        DevState* st, int num_sms, cudaStream_t stream);
+cudaError_t launch_ranges(uint64_t cap, uint64_t* const* pairs, uint2* ranges, uint32_t tiles, DevState* st,
                           int num_sms, cudaStream_t stream);
-cudaError_t launch_blend(const FrameParams& fp, const Record* rec, const uint32_t* const* vals, const uint2* ranges,
+// (d) blend + downsample.
+cudaError_t launch_blend(const FrameParams& fp, const Record* rec, uint64_t* const* pairs, const uint2* ranges,
                          const DevState* st, bool exact, uint8_t* out, uint8_t* full_scratch, cudaStream_t stream);
 
 // Partition size (pairs) of one onesweep CTA.
 constexpr int kSortThreads = 256;
 constexpr int kSortItems = 16;
+constexpr int kScanThreads = 256;  // splats per projection / emission partition
 constexpr int kSortPart = kSortThreads * kSortItems;
 
 }  // namespace splat

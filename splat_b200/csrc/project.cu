@@ -7,8 +7,12 @@
 // (no fused multiply-adds): the projected splats equal the oracle's bit for
 // bit. The kernel also emits each visible splat's tile rectangle (pixel_bbox,
 // src/render/cpu.rs:94-102 and the tile loop of cpu.rs:262-276), its pair
-// count and depth bits for the binning scan.
+// count and depth bits for the binning scan, and compacts the visible splats,
+// in index order, into 64-bit depth words (depth bits << 32 | splat index)
+// for the depth sort: a block-wide ballot scan plus a decoupled look-back over
+// ticketed partitions.
 #include "common.cuh"
+#include "lookback.cuh"
 
 namespace splat {
 namespace {
@@ -83,11 +87,21 @@ __device__ __forceinline__ void eval_sh(const float* __restrict__ sh, uint64_t n
 }
 
 template <int DEG>
-__global__ void __launch_bounds__(256) k_project(FrameParams fp, SceneDev s, Record* __restrict__ rec,
-                                                 BinInfo* __restrict__ bin, float* __restrict__ dbg_proj,
-                                                 float* __restrict__ dbg_color, DevState* st) {
-  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(kScanThreads) k_project(FrameParams fp, SceneDev s, Record* __restrict__ rec,
+                                                          BinInfo* __restrict__ bin, unsigned long long* desc,
+                                                          uint64_t* __restrict__ depth_words,
+                                                          float* __restrict__ dbg_proj, float* __restrict__ dbg_color,
+                                                          DevState* st) {
+  __shared__ uint32_t s_part;
+  __shared__ uint32_t s_warp[kScanThreads / 32];
+  __shared__ unsigned long long s_base;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) s_part = atomicAdd(&st->project_ticket, 1u);
+  __syncthreads();
+  const uint32_t part = s_part;
+  const uint64_t i = (uint64_t)part * kScanThreads + tid;
   bool vis = false;
+  uint32_t depth_bits = 0;
   if (i < s.n) {
     const float4 po = __ldg(&s.pos_op[i]);
     BinInfo b{kCulled, 0u, 0u, 0u};
@@ -169,6 +183,7 @@ __global__ void __launch_bounds__(256) k_project(FrameParams fp, SceneDev s, Rec
       r.r2 = make_float4(col[2], __uint_as_float(bx0 | (x1 << 16)), __uint_as_float(by0 | (y1 << 16)), tz);
       rec[i] = r;
       b.depth_bits = __float_as_uint(tz);
+      depth_bits = b.depth_bits;
       if (bx0 < x1 && by0 < y1) {
         const uint32_t tx0 = bx0 / kTile, ty0 = by0 / kTile;
         const uint32_t tx1 = (x1 + kTile - 1) / kTile, ty1 = (y1 + kTile - 1) / kTile;
@@ -198,22 +213,50 @@ __global__ void __launch_bounds__(256) k_project(FrameParams fp, SceneDev s, Rec
       dbg_color[3 * i + 2] = vis ? col[2] : 0.f;
     }
   }
-  const int nvis = __syncthreads_count(vis);
-  if (threadIdx.x == 0 && nvis) atomicAdd(&st->visible, (unsigned)nvis);
+  // Compact the visible splats in index order: ballot within warps, a scan
+  // over the warps, then the look-back across partitions.
+  const uint32_t vmask = __ballot_sync(0xffffffffu, vis);
+  if (lane == 0) s_warp[warp] = __popc(vmask);
+  __syncthreads();
+  if (warp == 0) {
+    const uint32_t c = lane < kScanThreads / 32 ? s_warp[lane] : 0u;
+    uint32_t x = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    const uint32_t total = __shfl_sync(0xffffffffu, x, 31);
+    if (lane < kScanThreads / 32) s_warp[lane] = x - c;
+    const unsigned long long base = lookback_exclusive(desc, part, total, st, kErrEmitTimeout);
+    if (lane == 0) {
+      s_base = base;
+      if ((uint64_t)part == gridDim.x - 1ull) st->visible = base + total;
+    }
+  }
+  __syncthreads();
+  if (vis) {
+    const uint64_t off = s_base + s_warp[warp] + __popc(vmask & ((1u << lane) - 1u));
+    depth_words[off] = ((uint64_t)depth_bits << 32) | i;
+  }
 }
 
 }  // namespace
 
-cudaError_t launch_project(const FrameParams& fp, const SceneDev& s, Record* rec, BinInfo* bin, float* dbg_proj,
-                           float* dbg_color, DevState* st, cudaStream_t stream) {
+cudaError_t launch_project(const FrameParams& fp, const SceneDev& s, Record* rec, BinInfo* bin,
+                           unsigned long long* scan_desc, uint64_t* depth_words, float* dbg_proj, float* dbg_color,
+                           DevState* st, cudaStream_t stream) {
   if (s.n == 0) return cudaSuccess;
-  const unsigned grid = (unsigned)((s.n + 255) / 256);
+  const unsigned grid = (unsigned)((s.n + kScanThreads - 1) / kScanThreads);
+#define SPLAT_PROJECT(D) \
+  k_project<D><<<grid, kScanThreads, 0, stream>>>(fp, s, rec, bin, scan_desc, depth_words, dbg_proj, dbg_color, st)
   switch (s.sh_degree) {
-    case 0: k_project<0><<<grid, 256, 0, stream>>>(fp, s, rec, bin, dbg_proj, dbg_color, st); break;
-    case 1: k_project<1><<<grid, 256, 0, stream>>>(fp, s, rec, bin, dbg_proj, dbg_color, st); break;
-    case 2: k_project<2><<<grid, 256, 0, stream>>>(fp, s, rec, bin, dbg_proj, dbg_color, st); break;
-    default: k_project<3><<<grid, 256, 0, stream>>>(fp, s, rec, bin, dbg_proj, dbg_color, st); break;
+    case 0: SPLAT_PROJECT(0); break;
+    case 1: SPLAT_PROJECT(1); break;
+    case 2: SPLAT_PROJECT(2); break;
+    default: SPLAT_PROJECT(3); break;
   }
+#undef SPLAT_PROJECT
   return cudaGetLastError();
 }
 

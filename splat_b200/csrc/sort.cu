@@ -1,18 +1,20 @@
-// Kernel (c): onesweep LSD radix sort of the (tile << 32 | depth bits) keys
-// with their splat-index values, plus the tile-range kernel.
+// Kernel (c): onesweep LSD radix sort plus the tile-range kernel.
 //
 // The reference sorts each tile's bucket stably by depth (radix::sort_hi32,
 // src/render/radix.rs:13-57, after a counting sort by tile, cpu.rs:149-199)
-// and breaks depth ties by scene index (fix_ties, cpu.rs:396-414). Here one
-// stable LSD sort over the whole key does both: pairs arrive in splat-index
-// order, so equal keys keep index order. Digits are 8 bits; one histogram
-// pass counts every digit up front, a digit shared by all keys is skipped
-// (as sort_hi32 does, radix.rs:389-393), and each remaining digit is one
-// onesweep pass: a CTA ranks its 4096-key partition stably with warp
-// match-any, publishes per-digit counts, resolves its global offsets by a
-// decoupled look-back over earlier partitions (bounded spin), and scatters.
+// and breaks depth ties by scene index (fix_ties, cpu.rs:396-414). Here two
+// stable LSD sorts of 64-bit words produce the same order: the visible splats
+// by depth (words depth bits << 32 | splat, built in splat-index order, so
+// ties keep index order), then, after emission in that order, the pairs by
+// tile (words tile << 32 | splat). Only the upper 32 bits are digits: 8-bit
+// digits, one histogram kernel counts every digit of a sort up front, and a
+// digit shared by all words is skipped (as sort_hi32 does, radix.rs:389-393).
+// Each remaining digit is one onesweep pass: a CTA ranks its 4096-word
+// partition stably with warp match-any, publishes its per-digit counts,
+// resolves its global offsets by a decoupled look-back over the earlier
+// partitions (bounded spin) and scatters.
 // Tile ranges ([begin, end) per tile) come from neighbour compares over the
-// sorted keys, as the reference's `ranges_main` does (tiles.wgsl:83-101).
+// sorted pairs, as the reference's `ranges_main` does (tiles.wgsl:83-101).
 #include "common.cuh"
 
 namespace splat {
@@ -23,37 +25,49 @@ constexpr uint32_t kLbAgg = 1u << 30;
 constexpr uint32_t kLbInc = 2u << 30;
 constexpr uint32_t kLbMask = (1u << 30) - 1;
 
-__device__ __forceinline__ uint64_t pair_count(const DevState* st, uint64_t cap) {
-  const unsigned long long t = *(const volatile unsigned long long*)&st->total_pairs;
+__device__ __forceinline__ uint64_t sort_count(const unsigned long long* count, uint64_t cap) {
+  const unsigned long long t = *(const volatile unsigned long long*)count;
   return t < cap ? t : cap;
 }
 
-__global__ void __launch_bounds__(256) k_hist(const uint64_t* __restrict__ keys, uint64_t cap, int digits,
-                                              DevState* st) {
-  __shared__ uint32_t h[kMaxDigits][256];
-  for (int t = threadIdx.x; t < kMaxDigits * 256; t += blockDim.x) (&h[0][0])[t] = 0u;
+// Histograms of `digits` 8-bit digits (from bit 32 + 8 * first_digit) of the
+// words, with warp-aggregated shared-memory atomics (peers found by match-any).
+__global__ void __launch_bounds__(256) k_hist(const uint64_t* __restrict__ words, const unsigned long long* count,
+                                              uint64_t cap, int first_digit, int digits, SortState* ss) {
+  __shared__ uint32_t h[kMaxPasses][256];
+  for (int t = threadIdx.x; t < kMaxPasses * 256; t += blockDim.x) (&h[0][0])[t] = 0u;
   __syncthreads();
-  const uint64_t P = pair_count(st, cap);
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < P; i += (uint64_t)gridDim.x * blockDim.x) {
-    const uint64_t k = keys[i];
-    for (int d = 0; d < digits; d++) atomicAdd(&h[d][(k >> (8 * d)) & 255u], 1u);
+  const uint64_t n = sort_count(count, cap);
+  const int lane = threadIdx.x & 31;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  // Whole warps iterate together so match-any sees every lane.
+  for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n; base += stride) {
+    const uint64_t i = base + lane;
+    const bool valid = i < n;
+    const uint32_t hi = valid ? (uint32_t)(words[i] >> 32) : 0u;
+    for (int d = 0; d < digits; d++) {
+      const uint32_t dig = valid ? (hi >> (8 * (first_digit + d))) & 255u : 256u;
+      const uint32_t peers = __match_any_sync(0xffffffffu, dig);
+      if (valid && lane == 31 - __clz(peers)) atomicAdd(&h[d][dig], (uint32_t)__popc(peers));
+    }
   }
   __syncthreads();
   for (int t = threadIdx.x; t < digits * 256; t += blockDim.x) {
     const uint32_t v = (&h[0][0])[t];
-    if (v) atomicAdd(&(&st->hist[0][0])[t], v);
+    if (v) atomicAdd(&(&ss->hist[0][0])[t], v);
   }
 }
 
 // One CTA: exclusive scans of the digit histograms and the pass schedule.
-__global__ void __launch_bounds__(256) k_hist_scan(uint64_t cap, int digits, DevState* st) {
+__global__ void __launch_bounds__(256) k_hist_scan(SortState* ss, const unsigned long long* count, uint64_t cap,
+                                                   int digits) {
   __shared__ uint32_t s_warp[8];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const uint64_t P = pair_count(st, cap);
+  const uint64_t n = sort_count(count, cap);
   int parity = 0;
   for (int d = 0; d < digits; d++) {
-    const uint32_t v = st->hist[d][tid];
-    const int trivial = __syncthreads_or((uint64_t)v == P);
+    const uint32_t v = ss->hist[d][tid];
+    const int trivial = __syncthreads_or((uint64_t)v == n);
     uint32_t x = v;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -64,54 +78,50 @@ __global__ void __launch_bounds__(256) k_hist_scan(uint64_t cap, int digits, Dev
     __syncthreads();
     uint32_t base = 0;
     for (int w = 0; w < warp; w++) base += s_warp[w];
-    st->hist[d][tid] = base + x - v;
+    ss->hist[d][tid] = base + x - v;
     __syncthreads();
-    if (tid == 0) st->pass_src[d] = trivial ? -1 : parity;
+    if (tid == 0) ss->pass_src[d] = trivial ? -1 : parity;
     if (!trivial) parity ^= 1;
   }
   if (tid == 0) {
-    for (int d = digits; d < kMaxDigits; d++) st->pass_src[d] = -1;
-    st->final_sel = parity;
+    for (int d = digits; d < kMaxPasses; d++) ss->pass_src[d] = -1;
+    ss->final_sel = parity;
   }
 }
 
-__global__ void __launch_bounds__(kSortThreads, 2) k_onesweep(int d, uint64_t cap, uint64_t* k0, uint32_t* v0,
-                                                              uint64_t* k1, uint32_t* v1, uint32_t* lb, DevState* st) {
+__global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(SortState* ss, const unsigned long long* count,
+                                                              uint64_t cap, int pass, int shift, uint64_t* w0,
+                                                              uint64_t* w1, uint32_t* lb, DevState* st) {
   __shared__ uint32_t s_whist[kWarps][256];
   __shared__ uint32_t s_gbase[256];
   __shared__ uint32_t s_part;
-  const int src = st->pass_src[d];
+  const int src = ss->pass_src[pass];
   if (src < 0) return;
-  const uint64_t* __restrict__ kin = src ? k1 : k0;
-  const uint32_t* __restrict__ vin = src ? v1 : v0;
-  uint64_t* __restrict__ kout = src ? k0 : k1;
-  uint32_t* __restrict__ vout = src ? v0 : v1;
-  const uint64_t P = pair_count(st, cap);
-  const uint32_t nparts = (uint32_t)((P + kSortPart - 1) / kSortPart);
-  const int shift = 8 * d;
+  const uint64_t* __restrict__ in = src ? w1 : w0;
+  uint64_t* __restrict__ out = src ? w0 : w1;
+  const uint64_t n = sort_count(count, cap);
+  const uint32_t nparts = (uint32_t)((n + kSortPart - 1) / kSortPart);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const uint32_t lt_mask = (1u << lane) - 1u;
 
   for (;;) {
-    if (tid == 0) s_part = atomicAdd(&st->sort_ticket[d], 1u);
+    if (tid == 0) s_part = atomicAdd(&ss->ticket[pass], 1u);
 #pragma unroll
     for (int w = 0; w < kWarps; w++) s_whist[w][tid] = 0u;
     __syncthreads();
     const uint32_t part = s_part;
     if (part >= nparts) break;
 
-    // Load this warp's 16 x 32 keys (warp-striped, coalesced) and rank them
-    // stably per digit: item (j, lane) is key base + 32 j + lane.
+    // This warp's 16 x 32 words (warp-striped, coalesced), ranked stably per
+    // digit: item (j, lane) is word base + 32 j + lane.
     const uint64_t base = (uint64_t)part * kSortPart + (uint64_t)warp * (kSortItems * 32);
     uint64_t key[kSortItems];
-    uint32_t val[kSortItems];
-    uint32_t dr[kSortItems];  // rank << 8 | digit, or 0xFFFFFFFF when past the end
+    uint32_t dr[kSortItems];  // rank << 8 | digit, or 0xFFFFFFFF past the end
 #pragma unroll
     for (int j = 0; j < kSortItems; j++) {
       const uint64_t idx = base + (uint64_t)j * 32 + lane;
-      const bool valid = idx < P;
-      key[j] = valid ? kin[idx] : 0ull;
-      val[j] = valid ? vin[idx] : 0u;
+      const bool valid = idx < n;
+      key[j] = valid ? in[idx] : 0ull;
       dr[j] = valid ? (uint32_t)((key[j] >> shift) & 255u) : 0xFFFFFFFFu;
     }
 #pragma unroll
@@ -166,7 +176,7 @@ __global__ void __launch_bounds__(kSortThreads, 2) k_onesweep(int d, uint64_t ca
       }
       *(volatile uint32_t*)my = kLbInc | (prefix + running);
     }
-    s_gbase[tid] = st->hist[d][tid] + prefix;
+    s_gbase[tid] = ss->hist[pass][tid] + prefix;
     __syncthreads();
 
 #pragma unroll
@@ -174,48 +184,46 @@ __global__ void __launch_bounds__(kSortThreads, 2) k_onesweep(int d, uint64_t ca
       if (dr[j] != 0xFFFFFFFFu) {
         const uint32_t dig = dr[j] & 255u;
         const uint64_t pos = (uint64_t)s_gbase[dig] + s_whist[warp][dig] + (dr[j] >> 8);
-        if (pos < P) {
-          kout[pos] = key[j];
-          vout[pos] = val[j];
-        } else {
+        if (pos < n)
+          out[pos] = key[j];
+        else
           atomicOr(&st->error, kErrSortRange);
-        }
       }
     }
     __syncthreads();
   }
 }
 
-__global__ void __launch_bounds__(256) k_ranges(uint64_t cap, const uint64_t* k0, const uint64_t* k1,
+__global__ void __launch_bounds__(256) k_ranges(uint64_t cap, const uint64_t* p0, const uint64_t* p1,
                                                 uint2* __restrict__ ranges, uint32_t tiles, const DevState* st) {
-  const uint64_t* __restrict__ keys = st->final_sel ? k1 : k0;
-  const uint64_t P = pair_count(st, cap);
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < P; i += (uint64_t)gridDim.x * blockDim.x) {
-    const uint32_t t = (uint32_t)(keys[i] >> 32);
+  const uint64_t* __restrict__ pairs = st->tile.final_sel ? p1 : p0;
+  const uint64_t n = sort_count(&st->total_pairs, cap);
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t t = (uint32_t)(pairs[i] >> 32);
     if (t >= tiles) continue;
-    if (i == 0 || (uint32_t)(keys[i - 1] >> 32) != t) ranges[t].x = (uint32_t)i;
-    if (i + 1 == P || (uint32_t)(keys[i + 1] >> 32) != t) ranges[t].y = (uint32_t)(i + 1);
+    if (i == 0 || (uint32_t)(pairs[i - 1] >> 32) != t) ranges[t].x = (uint32_t)i;
+    if (i + 1 == n || (uint32_t)(pairs[i + 1] >> 32) != t) ranges[t].y = (uint32_t)(i + 1);
   }
 }
 
 }  // namespace
 
-cudaError_t launch_sort(uint32_t key_bits, uint64_t cap, uint64_t* keys0, uint32_t* vals0, uint64_t* keys1,
-                        uint32_t* vals1, uint32_t* lookback, uint64_t lookback_parts, DevState* st, int num_sms,
-                        cudaStream_t stream) {
-  const int digits = (int)((key_bits + 7) / 8);
-  k_hist<<<num_sms * 4, 256, 0, stream>>>(keys0, cap, digits, st);
-  k_hist_scan<<<1, 256, 0, stream>>>(cap, digits, st);
+cudaError_t launch_sort(SortState* ss, const unsigned long long* count, uint64_t cap, int first_digit, int digits,
+                        uint64_t* words0, uint64_t* words1, uint32_t* lookback, uint64_t lookback_parts,
+                        DevState* st, int num_sms, cudaStream_t stream) {
+  if (digits <= 0) return cudaSuccess;
+  k_hist<<<num_sms * 4, 256, 0, stream>>>(words0, count, cap, first_digit, digits, ss);
+  k_hist_scan<<<1, 256, 0, stream>>>(ss, count, cap, digits);
   for (int d = 0; d < digits; d++) {
-    k_onesweep<<<num_sms * 2, kSortThreads, 0, stream>>>(d, cap, keys0, vals0, keys1, vals1,
-                                                        lookback + (uint64_t)d * lookback_parts * 256, st);
+    k_onesweep<<<num_sms * 3, kSortThreads, 0, stream>>>(ss, count, cap, d, 32 + 8 * (first_digit + d), words0,
+                                                        words1, lookback + (uint64_t)d * lookback_parts * 256, st);
   }
   return cudaGetLastError();
 }
 
-cudaError_t launch_ranges(uint64_t cap, uint64_t* const* keys, uint2* ranges, uint32_t tiles, DevState* st,
+cudaError_t launch_ranges(uint64_t cap, uint64_t* const* pairs, uint2* ranges, uint32_t tiles, DevState* st,
                           int num_sms, cudaStream_t stream) {
-  k_ranges<<<num_sms * 4, 256, 0, stream>>>(cap, keys[0], keys[1], ranges, tiles, st);
+  k_ranges<<<num_sms * 4, 256, 0, stream>>>(cap, pairs[0], pairs[1], ranges, tiles, st);
   return cudaGetLastError();
 }
 
