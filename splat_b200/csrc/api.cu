@@ -40,8 +40,7 @@ struct splat_cuda_handle {
   // per-splat frame buffers
   Record* rec = nullptr;
   BinInfo* bin = nullptr;
-  unsigned long long* desc_project = nullptr;  // scan descriptors, one per partition
-  unsigned long long* desc_emit = nullptr;
+  unsigned long long* desc_emit = nullptr;  // scan descriptors, one per partition
   uint64_t* depth_words[2] = {nullptr, nullptr};
   uint32_t* lb_depth = nullptr;  // look-back words of the depth sort
   uint64_t lb_depth_parts = 0;
@@ -52,6 +51,7 @@ struct splat_cuda_handle {
   uint64_t lb_tile_parts = 0;
   // per-size buffers
   uint2* ranges = nullptr;
+  uint32_t* tile_counts = nullptr;
   uint64_t ranges_cap = 0;  // tiles
   uint8_t* out_dev = nullptr;
   size_t out_cap = 0;
@@ -127,7 +127,9 @@ int ensure_pairs(splat_cuda_handle* h, uint64_t cap) {
 int ensure_size(splat_cuda_handle* h, uint64_t tiles, size_t out_bytes, size_t full_bytes) {
   if (tiles > h->ranges_cap) {
     dfree(h->ranges);
+    dfree(h->tile_counts);
     CK(cudaMalloc(&h->ranges, tiles * sizeof(uint2)), "cudaMalloc ranges");
+    CK(cudaMalloc(&h->tile_counts, tiles * sizeof(uint32_t)), "cudaMalloc tile counts");
     h->ranges_cap = tiles;
   }
   if (out_bytes > h->out_cap) {
@@ -195,10 +197,9 @@ int enqueue_frame(splat_cuda_handle* h, const FrameParams& fp, uint8_t* dev_out)
   cudaStream_t s = h->stream;
   const int tile_digits = (int)((bits_for(tiles) + 7) / 8);
   CK(cudaMemsetAsync(h->st, 0, sizeof(DevState), s), "clear frame state");
-  CK(cudaMemsetAsync(h->ranges, 0, tiles * sizeof(uint2), s), "clear ranges");
+  CK(cudaMemsetAsync(h->tile_counts, 0, tiles * sizeof(uint32_t), s), "clear tile counts");
   if (h->n) {
     const size_t nd = ((h->n + kScanThreads - 1) / kScanThreads) * sizeof(unsigned long long);
-    CK(cudaMemsetAsync(h->desc_project, 0, nd, s), "clear scan");
     CK(cudaMemsetAsync(h->desc_emit, 0, nd, s), "clear scan");
     CK(cudaMemsetAsync(h->lb_depth, 0, (size_t)kMaxPasses * h->lb_depth_parts * 256 * sizeof(uint32_t), s),
        "clear lookback");
@@ -209,21 +210,26 @@ int enqueue_frame(splat_cuda_handle* h, const FrameParams& fp, uint8_t* dev_out)
   if (h->stage_events) CK(cudaEventRecord(h->ev[0], s), "event");
   if (h->n) {
     SceneDev sd{h->pos_op, h->cov_a, h->cov_b, h->color, h->sh, h->n, h->sh_degree};
-    CK(launch_project(fp, sd, h->rec, h->bin, h->desc_project, h->depth_words[0],
-                      h->debug_capture ? h->dbg_proj : nullptr, h->debug_capture ? h->dbg_color : nullptr, h->st, s),
+    CK(launch_project(fp, sd, h->rec, h->bin, h->depth_words[0], h->debug_capture ? h->dbg_proj : nullptr,
+                      h->debug_capture ? h->dbg_color : nullptr, h->st, s),
        "project kernel");
   }
   if (h->stage_events) CK(cudaEventRecord(h->ev[1], s), "event");
   if (h->n) {
     DevState* st = h->st;
-    CK(launch_sort(&st->depth, &st->visible, h->n, 0, kMaxPasses, h->depth_words[0], h->depth_words[1], h->lb_depth,
+    CK(launch_depth_schedule(st, h->n, s), "depth schedule");
+    CK(launch_sort(&st->depth, nullptr, h->n, kMaxPasses, h->depth_words[0], h->depth_words[1], h->lb_depth,
                    h->lb_depth_parts, st, h->num_sms, s),
        "depth sort");
-    CK(launch_emit(fp, h->bin, h->n, h->desc_emit, h->depth_words, h->pairs[0], h->cap, st, s), "emit kernel");
-    CK(launch_sort(&st->tile, &st->total_pairs, h->cap, 0, tile_digits, h->pairs[0], h->pairs[1], h->lb_tile,
+    CK(launch_emit(fp, h->bin, h->n, h->desc_emit, h->depth_words, h->pairs[0], h->cap, h->tile_counts, st, s),
+       "emit kernel");
+  }
+  CK(launch_tile_prep(h->tile_counts, (uint32_t)tiles, h->ranges, h->st, s), "tile ranges");
+  if (h->n) {
+    DevState* st = h->st;
+    CK(launch_sort(&st->tile, &st->total_pairs, h->cap, tile_digits, h->pairs[0], h->pairs[1], h->lb_tile,
                    h->lb_tile_parts, st, h->num_sms, s),
        "tile sort");
-    CK(launch_ranges(h->cap, h->pairs, h->ranges, (uint32_t)tiles, st, h->num_sms, s), "ranges kernel");
   }
   if (h->stage_events) CK(cudaEventRecord(h->ev[2], s), "event");
   CK(launch_blend(fp, h->rec, h->pairs, h->ranges, h->st, h->exact, dev_out, h->full_dev, s), "blend kernel");
@@ -240,7 +246,8 @@ int finish_frame(splat_cuda_handle* h, splat_render_stats* stats, int* regrown) 
   const DevState& st = *h->st_host;
   if (st.error & (kErrEmitTimeout | kErrSortTimeout))
     return fail(h, SPLAT_ERR_TIMEOUT, "a device-side look-back wait gave up");
-  if (st.error & kErrSortRange) return fail(h, SPLAT_ERR_DEVICE, "sort produced an out-of-range position");
+  if ((st.error & kErrSortRange) && st.total_pairs <= h->cap)
+    return fail(h, SPLAT_ERR_DEVICE, "sort produced an out-of-range position");
   if (stats) {
     stats->visible = st.visible;
     stats->overlaps = st.total_pairs;
@@ -375,7 +382,6 @@ SPLAT_API int splat_cuda_create(const splat_scene_desc* d, int device, splat_cud
     if ((e = cudaMalloc(&h->rec, n * sizeof(Record))) != cudaSuccess) return bail(cuda_fail(h, e, "cudaMalloc records"));
     if ((e = cudaMalloc(&h->bin, n * sizeof(BinInfo))) != cudaSuccess) return bail(cuda_fail(h, e, "cudaMalloc bins"));
     const size_t nd = ((n + kScanThreads - 1) / kScanThreads) * sizeof(unsigned long long);
-    if ((e = cudaMalloc(&h->desc_project, nd)) != cudaSuccess) return bail(cuda_fail(h, e, "cudaMalloc scan"));
     if ((e = cudaMalloc(&h->desc_emit, nd)) != cudaSuccess) return bail(cuda_fail(h, e, "cudaMalloc scan"));
     for (int b = 0; b < 2; b++)
       if ((e = cudaMalloc(&h->depth_words[b], n * sizeof(uint64_t))) != cudaSuccess)
@@ -549,12 +555,12 @@ SPLAT_API int splat_cuda_destroy(splat_cuda_handle* h) {
   dfree(h->sh);
   dfree(h->rec);
   dfree(h->bin);
-  dfree(h->desc_project);
   dfree(h->desc_emit);
   for (int b = 0; b < 2; b++) dfree(h->depth_words[b]);
   dfree(h->lb_depth);
   free_pairs(h);
   dfree(h->ranges);
+  dfree(h->tile_counts);
   dfree(h->out_dev);
   dfree(h->full_dev);
   dfree(h->st);

@@ -1,10 +1,10 @@
 // Kernel (b): device-wide exclusive scan of the per-splat pair counts with
 // warp shuffles and a decoupled look-back, fused with the pair emission.
 //
-// The scan runs over the visible splats in depth order (the output of the
-// depth sort: words depth bits << 32 | splat index, ties in splat-index
-// order). Each visible splat duplicates into one pair per tile of its pixel
-// bbox, row-major (ty, then tx) as the reference's `emit` does
+// The scan runs over the visible splats in depth order (the first `visible`
+// words of the depth sort's output: depth bits << 32 | splat index, ties in
+// splat-index order). Each visible splat duplicates into one pair per tile of
+// its pixel bbox, row-major (ty, then tx) as the reference's `emit` does
 // (src/render/cpu.rs:251-277); a pair is the 64-bit word tile << 32 | splat.
 // Pairs are therefore laid out in (depth, splat index) order, and the stable
 // tile sort that follows yields the reference's per-tile blending order:
@@ -13,9 +13,12 @@
 // tile << 32 | depth bits, is recovered exactly from the pair's tile and its
 // splat's depth bits.
 //
-// Expansion is warp-cooperative: a warp's pairs are written 32 at a time,
-// each lane locating its pair's splat by a binary search over the warp's
-// inclusive counts, so one large splat does not serialise its warp.
+// A CTA scans 1024 splats (4 rounds of 32 per warp, their gathers in flight
+// together). Expansion is warp-cooperative: a round's pairs are written 32 at
+// a time, each lane locating its pair's splat by a binary search over the
+// round's inclusive counts, so one large splat does not serialise its warp.
+// Every written pair also bumps its tile's pair count, from which the tile
+// ranges and the tile sort's digit histograms are derived.
 #include "common.cuh"
 #include "lookback.cuh"
 
@@ -23,38 +26,56 @@ namespace splat {
 namespace {
 
 constexpr int kWarps = kScanThreads / 32;
+constexpr int kRounds = 4;
+constexpr int kEmitPart = kScanThreads * kRounds;
 
 __global__ void __launch_bounds__(kScanThreads) k_emit(uint32_t tiles_x, const BinInfo* __restrict__ bin,
                                                        unsigned long long* desc, const uint64_t* dw0,
                                                        const uint64_t* dw1, uint64_t* __restrict__ pairs,
-                                                       uint64_t cap, DevState* st) {
+                                                       uint64_t cap, uint32_t* __restrict__ tile_counts,
+                                                       DevState* st) {
   __shared__ uint32_t s_part;
   __shared__ uint32_t s_warp[kWarps];
   __shared__ unsigned long long s_base;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const uint64_t V = *(const volatile unsigned long long*)&st->visible;
-  const uint64_t nparts = (V + kScanThreads - 1) / kScanThreads;
+  const uint64_t nparts = (V + kEmitPart - 1) / kEmitPart;
   if (tid == 0) s_part = atomicAdd(&st->emit_ticket, 1u);
   __syncthreads();
   const uint32_t part = s_part;
   if (part >= nparts) return;  // uniform across the block
   const uint64_t* __restrict__ dsorted = st->depth.final_sel ? dw1 : dw0;
-  const uint64_t q = (uint64_t)part * kScanThreads + tid;
-  uint32_t idx = 0, cnt = 0, rect_lo = 0, rect_hi = 0;
-  if (q < V) {
-    idx = (uint32_t)dsorted[q];
-    const BinInfo b = bin[idx];
-    cnt = b.count;
-    rect_lo = b.rect_lo;
-    rect_hi = b.rect_hi;
-  }
-  uint32_t x = cnt;  // inclusive prefix within the warp
+  const uint64_t wbase = (uint64_t)part * kEmitPart + (uint64_t)warp * (32 * kRounds);
+  uint32_t idx[kRounds], cnt[kRounds], lo[kRounds], hi[kRounds], incl[kRounds];
 #pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-    if (lane >= o) x += y;
+  for (int r = 0; r < kRounds; r++) {
+    const uint64_t q = wbase + (uint64_t)r * 32 + lane;
+    idx[r] = q < V ? (uint32_t)dsorted[q] : 0xFFFFFFFFu;
   }
-  if (lane == 31) s_warp[warp] = x;
+#pragma unroll
+  for (int r = 0; r < kRounds; r++) {
+    cnt[r] = 0u;
+    lo[r] = hi[r] = 0u;
+    if (idx[r] != 0xFFFFFFFFu) {
+      const BinInfo b = bin[idx[r]];
+      cnt[r] = b.count;
+      lo[r] = b.rect_lo;
+      hi[r] = b.rect_hi;
+    }
+  }
+  uint32_t warp_total = 0;
+#pragma unroll
+  for (int r = 0; r < kRounds; r++) {
+    uint32_t x = cnt[r];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    incl[r] = x;
+    warp_total += __shfl_sync(0xffffffffu, x, 31);
+  }
+  if (lane == 0) s_warp[warp] = warp_total;
   __syncthreads();
   if (warp == 0) {
     const uint32_t c = lane < kWarps ? s_warp[lane] : 0u;
@@ -74,45 +95,53 @@ __global__ void __launch_bounds__(kScanThreads) k_emit(uint32_t tiles_x, const B
   }
   __syncthreads();
 
-  const uint64_t warp_base = s_base + s_warp[warp];
-  const uint32_t warp_total = __shfl_sync(0xffffffffu, x, 31);
-  const uint32_t my_excl = x - cnt;
-  for (uint32_t c0 = 0; c0 < warp_total; c0 += 32) {
-    const uint32_t k = c0 + lane;
-    // owner = number of lanes whose inclusive count is <= k
-    uint32_t pos = 0;
+  uint64_t round_base = s_base + s_warp[warp];
 #pragma unroll
-    for (uint32_t s = 16; s > 0; s >>= 1) {
-      const uint32_t xv = __shfl_sync(0xffffffffu, x, pos + s - 1);
-      if (xv <= k) pos += s;
+  for (int r = 0; r < kRounds; r++) {
+    const uint32_t x = incl[r];
+    const uint32_t round_total = __shfl_sync(0xffffffffu, x, 31);
+    const uint32_t my_excl = x - cnt[r];
+    for (uint32_t c0 = 0; c0 < round_total; c0 += 32) {
+      const uint32_t k = c0 + lane;
+      // owner = number of lanes whose inclusive count is <= k
+      uint32_t pos = 0;
+#pragma unroll
+      for (uint32_t s = 16; s > 0; s >>= 1) {
+        const uint32_t xv = __shfl_sync(0xffffffffu, x, pos + s - 1);
+        if (xv <= k) pos += s;
+      }
+      const uint32_t owner = pos < 32 ? pos : 31;
+      const uint32_t o_lo = __shfl_sync(0xffffffffu, lo[r], owner);
+      const uint32_t o_hi = __shfl_sync(0xffffffffu, hi[r], owner);
+      const uint32_t o_ex = __shfl_sync(0xffffffffu, my_excl, owner);
+      const uint32_t o_id = __shfl_sync(0xffffffffu, idx[r], owner);
+      if (k < round_total) {
+        const uint32_t tx0 = o_lo & 0xFFFFu, ty0 = o_lo >> 16, tx1 = o_hi & 0xFFFFu;
+        const uint32_t wdt = tx1 - tx0;
+        const uint32_t local = k - o_ex;
+        const uint32_t row = local / wdt;
+        const uint32_t tile = (ty0 + row) * tiles_x + tx0 + (local - row * wdt);
+        const uint64_t off = round_base + k;
+        if (off < cap) {
+          pairs[off] = ((uint64_t)tile << 32) | o_id;
+          atomicAdd(&tile_counts[tile], 1u);
+        }
+      }
     }
-    const uint32_t owner = pos < 32 ? pos : 31;
-    const uint32_t o_lo = __shfl_sync(0xffffffffu, rect_lo, owner);
-    const uint32_t o_hi = __shfl_sync(0xffffffffu, rect_hi, owner);
-    const uint32_t o_ex = __shfl_sync(0xffffffffu, my_excl, owner);
-    const uint32_t o_id = __shfl_sync(0xffffffffu, idx, owner);
-    if (k < warp_total) {
-      const uint32_t tx0 = o_lo & 0xFFFFu, ty0 = o_lo >> 16, tx1 = o_hi & 0xFFFFu;
-      const uint32_t wdt = tx1 - tx0;
-      const uint32_t local = k - o_ex;
-      const uint32_t row = local / wdt;
-      const uint32_t tile = (ty0 + row) * tiles_x + tx0 + (local - row * wdt);
-      const uint64_t off = warp_base + k;
-      if (off < cap) pairs[off] = ((uint64_t)tile << 32) | o_id;
-    }
+    round_base += round_total;
   }
 }
 
 }  // namespace
 
 cudaError_t launch_emit(const FrameParams& fp, const BinInfo* bin, uint64_t n, unsigned long long* scan_desc,
-                        uint64_t* const* depth_words, uint64_t* pairs, uint64_t cap, DevState* st,
-                        cudaStream_t stream) {
+                        uint64_t* const* depth_words, uint64_t* pairs, uint64_t cap, uint32_t* tile_counts,
+                        DevState* st, cudaStream_t stream) {
   if (n == 0) return cudaSuccess;
   // Enough CTAs for every splat being visible; CTAs past the visible count return at once.
-  const unsigned grid = (unsigned)((n + kScanThreads - 1) / kScanThreads);
+  const unsigned grid = (unsigned)((n + kEmitPart - 1) / kEmitPart);
   k_emit<<<grid, kScanThreads, 0, stream>>>(fp.tiles_x, bin, scan_desc, depth_words[0], depth_words[1], pairs, cap,
-                                            st);
+                                            tile_counts, st);
   return cudaGetLastError();
 }
 

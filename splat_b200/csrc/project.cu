@@ -7,12 +7,14 @@
 // (no fused multiply-adds): the projected splats equal the oracle's bit for
 // bit. The kernel also emits each visible splat's tile rectangle (pixel_bbox,
 // src/render/cpu.rs:94-102 and the tile loop of cpu.rs:262-276), its pair
-// count and depth bits for the binning scan, and compacts the visible splats,
-// in index order, into 64-bit depth words (depth bits << 32 | splat index)
-// for the depth sort: a block-wide ballot scan plus a decoupled look-back over
-// ticketed partitions.
+// count and depth bits for the binning scan, and the 64-bit depth word
+// (depth bits << 32 | splat index) of every splat for the depth sort, a
+// culled splat with depth bits 0xFFFFFFFF so it sorts after every visible one
+// (visible depths are finite and positive, so their bit patterns order like
+// the floats and stay below 0x7F800000). The four 8-bit digit histograms of
+// the depth bits are counted here too, so the depth sort needs no histogram
+// pass of its own.
 #include "common.cuh"
-#include "lookback.cuh"
 
 namespace splat {
 namespace {
@@ -88,20 +90,16 @@ __device__ __forceinline__ void eval_sh(const float* __restrict__ sh, uint64_t n
 
 template <int DEG>
 __global__ void __launch_bounds__(kScanThreads) k_project(FrameParams fp, SceneDev s, Record* __restrict__ rec,
-                                                          BinInfo* __restrict__ bin, unsigned long long* desc,
-                                                          uint64_t* __restrict__ depth_words,
+                                                          BinInfo* __restrict__ bin, uint64_t* __restrict__ depth_words,
                                                           float* __restrict__ dbg_proj, float* __restrict__ dbg_color,
                                                           DevState* st) {
-  __shared__ uint32_t s_part;
-  __shared__ uint32_t s_warp[kScanThreads / 32];
-  __shared__ unsigned long long s_base;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  if (tid == 0) s_part = atomicAdd(&st->project_ticket, 1u);
+  __shared__ uint32_t s_hist[kMaxPasses][256];
+  const int tid = threadIdx.x;
+  for (int t = tid; t < kMaxPasses * 256; t += kScanThreads) (&s_hist[0][0])[t] = 0u;
   __syncthreads();
-  const uint32_t part = s_part;
-  const uint64_t i = (uint64_t)part * kScanThreads + tid;
+  const uint64_t i = (uint64_t)blockIdx.x * kScanThreads + tid;
   bool vis = false;
-  uint32_t depth_bits = 0;
+  uint32_t depth_bits = 0xFFFFFFFFu;
   if (i < s.n) {
     const float4 po = __ldg(&s.pos_op[i]);
     BinInfo b{kCulled, 0u, 0u, 0u};
@@ -213,43 +211,27 @@ __global__ void __launch_bounds__(kScanThreads) k_project(FrameParams fp, SceneD
       dbg_color[3 * i + 2] = vis ? col[2] : 0.f;
     }
   }
-  // Compact the visible splats in index order: ballot within warps, a scan
-  // over the warps, then the look-back across partitions.
-  const uint32_t vmask = __ballot_sync(0xffffffffu, vis);
-  if (lane == 0) s_warp[warp] = __popc(vmask);
-  __syncthreads();
-  if (warp == 0) {
-    const uint32_t c = lane < kScanThreads / 32 ? s_warp[lane] : 0u;
-    uint32_t x = c;
+  if (i < s.n) {
+    depth_words[i] = ((uint64_t)depth_bits << 32) | i;
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-      if (lane >= o) x += y;
-    }
-    const uint32_t total = __shfl_sync(0xffffffffu, x, 31);
-    if (lane < kScanThreads / 32) s_warp[lane] = x - c;
-    const unsigned long long base = lookback_exclusive(desc, part, total, st, kErrEmitTimeout);
-    if (lane == 0) {
-      s_base = base;
-      if ((uint64_t)part == gridDim.x - 1ull) st->visible = base + total;
-    }
+    for (int d = 0; d < kMaxPasses; d++) atomicAdd(&s_hist[d][(depth_bits >> (8 * d)) & 255u], 1u);
   }
-  __syncthreads();
-  if (vis) {
-    const uint64_t off = s_base + s_warp[warp] + __popc(vmask & ((1u << lane) - 1u));
-    depth_words[off] = ((uint64_t)depth_bits << 32) | i;
+  const int nvis = __syncthreads_count(vis);
+  if (tid == 0 && nvis) atomicAdd(&st->visible, (unsigned long long)nvis);
+  for (int t = tid; t < kMaxPasses * 256; t += kScanThreads) {
+    const uint32_t v = (&s_hist[0][0])[t];
+    if (v) atomicAdd(&(&st->depth.hist[0][0])[t], v);
   }
 }
 
 }  // namespace
 
-cudaError_t launch_project(const FrameParams& fp, const SceneDev& s, Record* rec, BinInfo* bin,
-                           unsigned long long* scan_desc, uint64_t* depth_words, float* dbg_proj, float* dbg_color,
-                           DevState* st, cudaStream_t stream) {
+cudaError_t launch_project(const FrameParams& fp, const SceneDev& s, Record* rec, BinInfo* bin, uint64_t* depth_words,
+                           float* dbg_proj, float* dbg_color, DevState* st, cudaStream_t stream) {
   if (s.n == 0) return cudaSuccess;
   const unsigned grid = (unsigned)((s.n + kScanThreads - 1) / kScanThreads);
 #define SPLAT_PROJECT(D) \
-  k_project<D><<<grid, kScanThreads, 0, stream>>>(fp, s, rec, bin, scan_desc, depth_words, dbg_proj, dbg_color, st)
+  k_project<D><<<grid, kScanThreads, 0, stream>>>(fp, s, rec, bin, depth_words, dbg_proj, dbg_color, st)
   switch (s.sh_degree) {
     case 0: SPLAT_PROJECT(0); break;
     case 1: SPLAT_PROJECT(1); break;
