@@ -65,6 +65,49 @@ __device__ __forceinline__ uint32_t to_u8(float v) {
   return (uint32_t)q;
 }
 
+// One splat's contribution test at this pixel: returns alpha, or 0 when the
+// splat does not contribute (outside the bbox, power > 0, alpha < 1/255).
+template <bool EXACT>
+__device__ __forceinline__ float splat_alpha(uint32_t m, uint32_t mybits, const float4& a, const float4& b,
+                                             float fx05, float gbase, float lanef, float rowc, float lxf, float lyf) {
+  float pw, alpha;
+  if (EXACT) {
+    const float cx0 = __fsub_rn(fx05, a.x);
+    const float dx = __fadd_rn(lanef, __fadd_rn(gbase, cx0));
+    const float qx = __fmul_rn(__fmul_rn(dx, dx), a.z);
+    const float dy = __fsub_rn(rowc, a.y);
+    const float qy = __fmul_rn(__fmul_rn(b.x, dy), dy);
+    const float bdy = __fmul_rn(a.w, dy);
+    pw = __fadd_rn(__fadd_rn(qx, qy), __fmul_rn(bdy, dx));
+    alpha = fminf(__fmul_rn(exp_neg_exact(pw), b.y), kAlphaMax);
+  } else {
+    const float dx = lxf - a.x;
+    const float dy = lyf - a.y;
+    pw = fmaf(dx, fmaf(a.z, dx, a.w * dy), (b.x * dy) * dy);
+    alpha = fminf(ex2_approx(pw) * b.y, kAlphaMax);
+  }
+  const bool on = ((m & mybits) == mybits) && (pw <= 0.0f) && (alpha >= kAlphaMin);
+  return on ? alpha : 0.0f;
+}
+
+template <bool EXACT>
+__device__ __forceinline__ void accumulate(float alpha, const float4& b, float blue, float& T, float& cr, float& cg,
+                                           float& cb) {
+  if (EXACT) {
+    const float w = __fmul_rn(alpha, T);
+    cr = __fadd_rn(cr, __fmul_rn(b.z, w));
+    cg = __fadd_rn(cg, __fmul_rn(b.w, w));
+    cb = __fadd_rn(cb, __fmul_rn(blue, w));
+    T = __fmul_rn(T, __fsub_rn(1.0f, alpha));
+  } else {
+    const float w = alpha * T;
+    cr = fmaf(b.z, w, cr);
+    cg = fmaf(b.w, w, cg);
+    cb = fmaf(blue, w, cb);
+    T = T - w;
+  }
+}
+
 template <bool EXACT>
 __global__ void __launch_bounds__(256) k_blend(FrameParams fp, const Record* __restrict__ rec,
                                                const uint64_t* __restrict__ p0, const uint64_t* __restrict__ p1,
@@ -73,20 +116,26 @@ __global__ void __launch_bounds__(256) k_blend(FrameParams fp, const Record* __r
   // Per batch entry: the splat's pixel bbox clipped to this tile as a bit
   // mask (columns in bits 0-15, rows in bits 16-31), then its geometry and
   // colour. The default path stores the centre relative to the tile's first
-  // pixel centre and the conic pre-scaled by log2(e) for exp2.
+  // pixel centre and the conic pre-scaled by log2(e) for exp2. Each warp
+  // then lists the entries whose bbox meets its 8x4 block and walks only
+  // those, two at a time (the second splat's alpha is computed while the
+  // first one's is being accumulated).
   __shared__ uint32_t s_mask[256];
   __shared__ float4 s_a[256];  // x, y, -a/2, -b   (scaled / shifted when !EXACT)
   __shared__ float4 s_b[256];  // -c/2, opacity, red, green
   __shared__ float s_c[256];   // blue
+  __shared__ uint8_t s_list[8][256];
   __shared__ uint32_t s_px[256];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const uint32_t tile = blockIdx.x;
   const uint32_t tx = tile % fp.tiles_x, ty = tile / fp.tiles_x;
   const uint32_t ox = tx * kTile, oy = ty * kTile;
-  const uint32_t lx = (warp & 1) * 8 + (lane & 7), ly = (warp >> 1) * 4 + (lane >> 3);
+  const uint32_t wx = (warp & 1) * 8, wy = (warp >> 1) * 4;
+  const uint32_t lx = wx + (lane & 7), ly = wy + (lane >> 3);
   const uint32_t px = ox + lx, py = oy + ly;
   const bool inside = px < fp.w && py < fp.h;
   const uint32_t mybits = (1u << lx) | (1u << (16 + ly));
+  const uint32_t wxbits = 0xFFu << wx, wybits = 0xFu << (16 + wy);
   const uint64_t* __restrict__ pairs = st->tile.final_sel ? p1 : p0;
   const uint2 range = ranges[tile];
   const uint32_t begin = range.x, end = range.y > range.x ? range.y : range.x;
@@ -135,47 +184,49 @@ __global__ void __launch_bounds__(256) k_blend(FrameParams fp, const Record* __r
     has = nxt < end;
     if (has) nr = rec[(uint32_t)pairs[nxt]];
     const uint32_t cnt = min(256u, end - start);
+    // This warp's list of batch entries whose bbox meets its block.
+    uint32_t len = 0;
+    if (__any_sync(0xffffffffu, !done)) {
+      for (uint32_t c0 = 0; c0 < cnt; c0 += 32) {
+        const uint32_t e = c0 + lane;
+        const uint32_t m = e < cnt ? s_mask[e] : 0u;
+        const bool hit = (m & wxbits) && (m & wybits);
+        const uint32_t bal = __ballot_sync(0xffffffffu, hit);
+        if (hit) s_list[warp][len + __popc(bal & ((1u << lane) - 1u))] = (uint8_t)e;
+        len += __popc(bal);
+      }
+      __syncwarp();
+    }
     if (!done) {
-      for (uint32_t j = 0; j < cnt; j++) {
-        if ((s_mask[j] & mybits) != mybits) continue;
-        const float4 a = s_a[j];
-        const float4 b = s_b[j];
-        float pw, alpha;
-        if (EXACT) {
-          const float cx0 = __fsub_rn(fx05, a.x);
-          const float dx = __fadd_rn(lanef, __fadd_rn(gbase, cx0));
-          const float qx = __fmul_rn(__fmul_rn(dx, dx), a.z);
-          const float dy = __fsub_rn(rowc, a.y);
-          const float qy = __fmul_rn(__fmul_rn(b.x, dy), dy);
-          const float bdy = __fmul_rn(a.w, dy);
-          pw = __fadd_rn(__fadd_rn(qx, qy), __fmul_rn(bdy, dx));
-          if (!(pw <= 0.0f)) continue;
-          alpha = fminf(__fmul_rn(exp_neg_exact(pw), b.y), kAlphaMax);
-        } else {
-          const float dx = lxf - a.x;
-          const float dy = lyf - a.y;
-          pw = fmaf(dx, fmaf(a.z, dx, a.w * dy), (b.x * dy) * dy);
-          if (!(pw <= 0.0f)) continue;
-          alpha = fminf(ex2_approx(pw) * b.y, kAlphaMax);
+      uint32_t k = 0;
+      for (; k + 1 < len; k += 2) {
+        const uint32_t j0 = s_list[warp][k], j1 = s_list[warp][k + 1];
+        const float4 a0 = s_a[j0], b0 = s_b[j0];
+        const float4 a1 = s_a[j1], b1 = s_b[j1];
+        const float al0 = splat_alpha<EXACT>(s_mask[j0], mybits, a0, b0, fx05, gbase, lanef, rowc, lxf, lyf);
+        const float al1 = splat_alpha<EXACT>(s_mask[j1], mybits, a1, b1, fx05, gbase, lanef, rowc, lxf, lyf);
+        if (al0 > 0.0f) {
+          accumulate<EXACT>(al0, b0, s_c[j0], T, cr, cg, cb);
+          if (T < kTMin) {
+            done = true;
+            break;
+          }
         }
-        if (!(alpha >= kAlphaMin)) continue;
-        const float blue = s_c[j];
-        if (EXACT) {
-          const float w = __fmul_rn(alpha, T);
-          cr = __fadd_rn(cr, __fmul_rn(b.z, w));
-          cg = __fadd_rn(cg, __fmul_rn(b.w, w));
-          cb = __fadd_rn(cb, __fmul_rn(blue, w));
-          T = __fmul_rn(T, __fsub_rn(1.0f, alpha));
-        } else {
-          const float w = alpha * T;
-          cr = fmaf(b.z, w, cr);
-          cg = fmaf(b.w, w, cg);
-          cb = fmaf(blue, w, cb);
-          T = T - w;
+        if (al1 > 0.0f) {
+          accumulate<EXACT>(al1, b1, s_c[j1], T, cr, cg, cb);
+          if (T < kTMin) {
+            done = true;
+            break;
+          }
         }
-        if (T < kTMin) {
-          done = true;
-          break;
+      }
+      if (!done && k < len) {
+        const uint32_t j0 = s_list[warp][k];
+        const float4 a0 = s_a[j0], b0 = s_b[j0];
+        const float al0 = splat_alpha<EXACT>(s_mask[j0], mybits, a0, b0, fx05, gbase, lanef, rowc, lxf, lyf);
+        if (al0 > 0.0f) {
+          accumulate<EXACT>(al0, b0, s_c[j0], T, cr, cg, cb);
+          if (T < kTMin) done = true;
         }
       }
     }
