@@ -14,9 +14,9 @@
 // splat's depth bits.
 //
 // A CTA scans 1024 splats (4 rounds of 32 per warp, their gathers in flight
-// together). Expansion is warp-cooperative: a round's pairs are written 32 at
-// a time, each lane locating its pair's splat by a binary search over the
-// round's inclusive counts, so one large splat does not serialise its warp.
+// together). A lane writes its own splat's pairs when there are at most 32;
+// a larger splat is expanded by its whole warp, so one large splat does not
+// serialise its warp.
 // Every written pair also bumps its tile's pair count, from which the tile
 // ranges and the tile sort's digit histograms are derived.
 #include "common.cuh"
@@ -95,35 +95,46 @@ __global__ void __launch_bounds__(kScanThreads) k_emit(uint32_t tiles_x, const B
   }
   __syncthreads();
 
+  // Splats with at most kLanePairs pairs are written by their own lane,
+  // stepping through the tile rectangle row-major; larger ones by the whole
+  // warp, 32 pairs at a time.
+  constexpr uint32_t kLanePairs = 32;
   uint64_t round_base = s_base + s_warp[warp];
 #pragma unroll
   for (int r = 0; r < kRounds; r++) {
     const uint32_t x = incl[r];
     const uint32_t round_total = __shfl_sync(0xffffffffu, x, 31);
     const uint32_t my_excl = x - cnt[r];
-    for (uint32_t c0 = 0; c0 < round_total; c0 += 32) {
-      const uint32_t k = c0 + lane;
-      // owner = number of lanes whose inclusive count is <= k
-      uint32_t pos = 0;
-#pragma unroll
-      for (uint32_t s = 16; s > 0; s >>= 1) {
-        const uint32_t xv = __shfl_sync(0xffffffffu, x, pos + s - 1);
-        if (xv <= k) pos += s;
-      }
-      const uint32_t owner = pos < 32 ? pos : 31;
-      const uint32_t o_lo = __shfl_sync(0xffffffffu, lo[r], owner);
-      const uint32_t o_hi = __shfl_sync(0xffffffffu, hi[r], owner);
-      const uint32_t o_ex = __shfl_sync(0xffffffffu, my_excl, owner);
-      const uint32_t o_id = __shfl_sync(0xffffffffu, idx[r], owner);
-      if (k < round_total) {
-        const uint32_t tx0 = o_lo & 0xFFFFu, ty0 = o_lo >> 16, tx1 = o_hi & 0xFFFFu;
-        const uint32_t wdt = tx1 - tx0;
-        const uint32_t local = k - o_ex;
-        const uint32_t row = local / wdt;
-        const uint32_t tile = (ty0 + row) * tiles_x + tx0 + (local - row * wdt);
-        const uint64_t off = round_base + k;
+    const uint32_t tx0 = lo[r] & 0xFFFFu, ty0 = lo[r] >> 16, tx1 = hi[r] & 0xFFFFu;
+    if (cnt[r] <= kLanePairs) {
+      uint64_t off = round_base + my_excl;
+      uint32_t tx = tx0, ty = ty0;
+      for (uint32_t p = 0; p < cnt[r]; p++, off++) {
+        const uint32_t tile = ty * tiles_x + tx;
         if (off < cap) {
-          pairs[off] = ((uint64_t)tile << 32) | o_id;
+          pairs[off] = ((uint64_t)tile << 32) | idx[r];
+          atomicAdd(&tile_counts[tile], 1u);
+        }
+        if (++tx == tx1) {
+          tx = tx0;
+          ty++;
+        }
+      }
+    }
+    uint32_t big = __ballot_sync(0xffffffffu, cnt[r] > kLanePairs);
+    while (big) {
+      const int L = __ffs(big) - 1;
+      big &= big - 1u;
+      const uint32_t b_lo = __shfl_sync(0xffffffffu, lo[r], L), b_hi = __shfl_sync(0xffffffffu, hi[r], L);
+      const uint32_t b_cnt = __shfl_sync(0xffffffffu, cnt[r], L), b_ex = __shfl_sync(0xffffffffu, my_excl, L);
+      const uint32_t b_id = __shfl_sync(0xffffffffu, idx[r], L);
+      const uint32_t btx0 = b_lo & 0xFFFFu, bty0 = b_lo >> 16, wdt = (b_hi & 0xFFFFu) - btx0;
+      for (uint32_t k = lane; k < b_cnt; k += 32) {
+        const uint32_t row = k / wdt;
+        const uint32_t tile = (bty0 + row) * tiles_x + btx0 + (k - row * wdt);
+        const uint64_t off = round_base + b_ex + k;
+        if (off < cap) {
+          pairs[off] = ((uint64_t)tile << 32) | b_id;
           atomicAdd(&tile_counts[tile], 1u);
         }
       }

@@ -86,7 +86,12 @@ __device__ __forceinline__ float splat_alpha(uint32_t m, uint32_t mybits, const 
     pw = fmaf(dx, fmaf(a.z, dx, a.w * dy), (b.x * dy) * dy);
     alpha = fminf(ex2_approx(pw) * b.y, kAlphaMax);
   }
-  const bool on = ((m & mybits) == mybits) && (pw <= 0.0f) && (alpha >= kAlphaMin);
+  // A pixel outside the splat's bbox is at least half a pixel beyond the
+  // ellipse on which opacity * exp(power) = 1/255 (the bbox is the k-sigma
+  // extent rounded outwards and pixels are sampled at their centres), so the
+  // alpha test alone excludes it in the default path; the exact path also
+  // tests the bbox, as the reference does.
+  const bool on = (pw <= 0.0f) && (alpha >= kAlphaMin) && (!EXACT || (m & mybits) == mybits);
   return on ? alpha : 0.0f;
 }
 
