@@ -51,7 +51,6 @@ struct splat_cuda_handle {
   uint64_t lb_tile_parts = 0;
   // per-size buffers
   uint2* ranges = nullptr;
-  uint32_t* tile_counts = nullptr;
   uint64_t ranges_cap = 0;  // tiles
   uint8_t* out_dev = nullptr;
   size_t out_cap = 0;
@@ -127,9 +126,7 @@ int ensure_pairs(splat_cuda_handle* h, uint64_t cap) {
 int ensure_size(splat_cuda_handle* h, uint64_t tiles, size_t out_bytes, size_t full_bytes) {
   if (tiles > h->ranges_cap) {
     dfree(h->ranges);
-    dfree(h->tile_counts);
     CK(cudaMalloc(&h->ranges, tiles * sizeof(uint2)), "cudaMalloc ranges");
-    CK(cudaMalloc(&h->tile_counts, tiles * sizeof(uint32_t)), "cudaMalloc tile counts");
     h->ranges_cap = tiles;
   }
   if (out_bytes > h->out_cap) {
@@ -197,7 +194,7 @@ int enqueue_frame(splat_cuda_handle* h, const FrameParams& fp, uint8_t* dev_out)
   cudaStream_t s = h->stream;
   const int tile_digits = (int)((bits_for(tiles) + 7) / 8);
   CK(cudaMemsetAsync(h->st, 0, sizeof(DevState), s), "clear frame state");
-  CK(cudaMemsetAsync(h->tile_counts, 0, tiles * sizeof(uint32_t), s), "clear tile counts");
+  CK(cudaMemsetAsync(h->ranges, 0, tiles * sizeof(uint2), s), "clear ranges");
   if (h->n) {
     const size_t nd = ((h->n + kScanThreads - 1) / kScanThreads) * sizeof(unsigned long long);
     CK(cudaMemsetAsync(h->desc_emit, 0, nd, s), "clear scan");
@@ -221,15 +218,13 @@ int enqueue_frame(splat_cuda_handle* h, const FrameParams& fp, uint8_t* dev_out)
     CK(launch_sort(&st->depth, nullptr, h->n, kMaxPasses, h->depth_words[0], h->depth_words[1], h->lb_depth,
                    h->lb_depth_parts, st, h->num_sms, s),
        "depth sort");
-    CK(launch_emit(fp, h->bin, h->n, h->desc_emit, h->depth_words, h->pairs[0], h->cap, h->tile_counts, st, s),
+    CK(launch_emit(fp, tile_digits, h->bin, h->n, h->desc_emit, h->depth_words, h->pairs[0], h->cap, st, s),
        "emit kernel");
-  }
-  CK(launch_tile_prep(h->tile_counts, (uint32_t)tiles, h->ranges, h->st, s), "tile ranges");
-  if (h->n) {
-    DevState* st = h->st;
+    CK(launch_tile_schedule(st, h->cap, tile_digits, s), "tile schedule");
     CK(launch_sort(&st->tile, &st->total_pairs, h->cap, tile_digits, h->pairs[0], h->pairs[1], h->lb_tile,
                    h->lb_tile_parts, st, h->num_sms, s),
        "tile sort");
+    CK(launch_ranges(h->cap, h->pairs, h->ranges, (uint32_t)tiles, st, h->num_sms, s), "ranges");
   }
   if (h->stage_events) CK(cudaEventRecord(h->ev[2], s), "event");
   CK(launch_blend(fp, h->rec, h->pairs, h->ranges, h->st, h->exact, dev_out, h->full_dev, s), "blend kernel");
@@ -560,7 +555,6 @@ SPLAT_API int splat_cuda_destroy(splat_cuda_handle* h) {
   dfree(h->lb_depth);
   free_pairs(h);
   dfree(h->ranges);
-  dfree(h->tile_counts);
   dfree(h->out_dev);
   dfree(h->full_dev);
   dfree(h->st);

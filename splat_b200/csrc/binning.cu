@@ -14,11 +14,12 @@
 // splat's depth bits.
 //
 // A CTA scans 1024 splats (4 rounds of 32 per warp, their gathers in flight
-// together). A lane writes its own splat's pairs when there are at most 32;
-// a larger splat is expanded by its whole warp, so one large splat does not
-// serialise its warp.
-// Every written pair also bumps its tile's pair count, from which the tile
-// ranges and the tile sort's digit histograms are derived.
+// together). A lane expands its own splat when it has at most 32 pairs; a
+// larger splat is expanded by its whole warp, so one large splat does not
+// serialise its warp. Pairs are staged in shared memory at their offset in
+// the CTA's contiguous output range and then written out coalesced, and the
+// tile sort's digit histograms are counted from the staged pairs (pairs past
+// the staging buffer go straight to global memory and are counted there).
 #include "common.cuh"
 #include "lookback.cuh"
 
@@ -29,18 +30,27 @@ constexpr int kWarps = kScanThreads / 32;
 constexpr int kRounds = 4;
 constexpr int kEmitPart = kScanThreads * kRounds;
 
-__global__ void __launch_bounds__(kScanThreads) k_emit(uint32_t tiles_x, const BinInfo* __restrict__ bin,
-                                                       unsigned long long* desc, const uint64_t* dw0,
-                                                       const uint64_t* dw1, uint64_t* __restrict__ pairs,
-                                                       uint64_t cap, uint32_t* __restrict__ tile_counts,
-                                                       DevState* st) {
+constexpr uint32_t kStage = 4096;  // staged pairs per CTA (32 KB)
+
+__device__ __forceinline__ void count_digits(uint32_t (*hist)[256], uint32_t tile, int digits) {
+  for (int d = 0; d < digits; d++) atomicAdd(&hist[d][(tile >> (8 * d)) & 255u], 1u);
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_emit(uint32_t tiles_x, int tile_digits,
+                                                       const BinInfo* __restrict__ bin, unsigned long long* desc,
+                                                       const uint64_t* dw0, const uint64_t* dw1,
+                                                       uint64_t* __restrict__ pairs, uint64_t cap, DevState* st) {
   __shared__ uint32_t s_part;
   __shared__ uint32_t s_warp[kWarps];
   __shared__ unsigned long long s_base;
+  __shared__ uint32_t s_total;
+  __shared__ uint32_t s_hist[kMaxPasses][256];
+  __shared__ uint64_t s_stage[kStage];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const uint64_t V = *(const volatile unsigned long long*)&st->visible;
   const uint64_t nparts = (V + kEmitPart - 1) / kEmitPart;
   if (tid == 0) s_part = atomicAdd(&st->emit_ticket, 1u);
+  for (int t = tid; t < kMaxPasses * 256; t += kScanThreads) (&s_hist[0][0])[t] = 0u;
   __syncthreads();
   const uint32_t part = s_part;
   if (part >= nparts) return;  // uniform across the block
@@ -90,31 +100,36 @@ __global__ void __launch_bounds__(kScanThreads) k_emit(uint32_t tiles_x, const B
     const unsigned long long base = lookback_exclusive(desc, part, total, st, kErrEmitTimeout);
     if (lane == 0) {
       s_base = base;
+      s_total = total;
       if ((uint64_t)part == nparts - 1) st->total_pairs = base + total;
     }
   }
   __syncthreads();
 
-  // Splats with at most kLanePairs pairs are written by their own lane,
-  // stepping through the tile rectangle row-major; larger ones by the whole
-  // warp, 32 pairs at a time.
+  // Expansion into the staging buffer: local offset = offset in this CTA's range.
+  const uint64_t cta_base = s_base;
+  auto put = [&](uint32_t local, uint32_t tile, uint32_t splat) {
+    const uint64_t word = ((uint64_t)tile << 32) | splat;
+    if (local < kStage) {
+      s_stage[local] = word;
+    } else if (cta_base + local < cap) {
+      pairs[cta_base + local] = word;
+      count_digits(s_hist, tile, tile_digits);
+    }
+  };
   constexpr uint32_t kLanePairs = 32;
-  uint64_t round_base = s_base + s_warp[warp];
+  uint32_t round_local = s_warp[warp];
 #pragma unroll
   for (int r = 0; r < kRounds; r++) {
     const uint32_t x = incl[r];
     const uint32_t round_total = __shfl_sync(0xffffffffu, x, 31);
     const uint32_t my_excl = x - cnt[r];
-    const uint32_t tx0 = lo[r] & 0xFFFFu, ty0 = lo[r] >> 16, tx1 = hi[r] & 0xFFFFu;
     if (cnt[r] <= kLanePairs) {
-      uint64_t off = round_base + my_excl;
+      const uint32_t tx0 = lo[r] & 0xFFFFu, ty0 = lo[r] >> 16, tx1 = hi[r] & 0xFFFFu;
+      uint32_t local = round_local + my_excl;
       uint32_t tx = tx0, ty = ty0;
-      for (uint32_t p = 0; p < cnt[r]; p++, off++) {
-        const uint32_t tile = ty * tiles_x + tx;
-        if (off < cap) {
-          pairs[off] = ((uint64_t)tile << 32) | idx[r];
-          atomicAdd(&tile_counts[tile], 1u);
-        }
+      for (uint32_t p = 0; p < cnt[r]; p++, local++) {
+        put(local, ty * tiles_x + tx, idx[r]);
         if (++tx == tx1) {
           tx = tx0;
           ty++;
@@ -131,28 +146,38 @@ __global__ void __launch_bounds__(kScanThreads) k_emit(uint32_t tiles_x, const B
       const uint32_t btx0 = b_lo & 0xFFFFu, bty0 = b_lo >> 16, wdt = (b_hi & 0xFFFFu) - btx0;
       for (uint32_t k = lane; k < b_cnt; k += 32) {
         const uint32_t row = k / wdt;
-        const uint32_t tile = (bty0 + row) * tiles_x + btx0 + (k - row * wdt);
-        const uint64_t off = round_base + b_ex + k;
-        if (off < cap) {
-          pairs[off] = ((uint64_t)tile << 32) | b_id;
-          atomicAdd(&tile_counts[tile], 1u);
-        }
+        put(round_local + b_ex + k, (bty0 + row) * tiles_x + btx0 + (k - row * wdt), b_id);
       }
     }
-    round_base += round_total;
+    round_local += round_total;
+  }
+  __syncthreads();
+  // Coalesced write-out of the staged pairs, counting their tile digits.
+  const uint32_t staged = min(s_total, kStage);
+  for (uint32_t l = tid; l < staged; l += kScanThreads) {
+    if (cta_base + l < cap) {
+      const uint64_t word = s_stage[l];
+      pairs[cta_base + l] = word;
+      count_digits(s_hist, (uint32_t)(word >> 32), tile_digits);
+    }
+  }
+  __syncthreads();
+  for (int t = tid; t < tile_digits * 256; t += kScanThreads) {
+    const uint32_t v = (&s_hist[0][0])[t];
+    if (v) atomicAdd(&(&st->tile.hist[0][0])[t], v);
   }
 }
 
 }  // namespace
 
-cudaError_t launch_emit(const FrameParams& fp, const BinInfo* bin, uint64_t n, unsigned long long* scan_desc,
-                        uint64_t* const* depth_words, uint64_t* pairs, uint64_t cap, uint32_t* tile_counts,
+cudaError_t launch_emit(const FrameParams& fp, int tile_digits, const BinInfo* bin, uint64_t n,
+                        unsigned long long* scan_desc, uint64_t* const* depth_words, uint64_t* pairs, uint64_t cap,
                         DevState* st, cudaStream_t stream) {
   if (n == 0) return cudaSuccess;
   // Enough CTAs for every splat being visible; CTAs past the visible count return at once.
   const unsigned grid = (unsigned)((n + kEmitPart - 1) / kEmitPart);
-  k_emit<<<grid, kScanThreads, 0, stream>>>(fp.tiles_x, bin, scan_desc, depth_words[0], depth_words[1], pairs, cap,
-                                            tile_counts, st);
+  k_emit<<<grid, kScanThreads, 0, stream>>>(fp.tiles_x, tile_digits, bin, scan_desc, depth_words[0], depth_words[1],
+                                            pairs, cap, st);
   return cudaGetLastError();
 }
 

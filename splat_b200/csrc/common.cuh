@@ -103,9 +103,10 @@ constexpr unsigned long long kValMask = (1ull << 62) - 1;
 // (a) projection; a depth word per splat and the depth-digit histograms.
 cudaError_t launch_project(const FrameParams& fp, const SceneDev& s, Record* rec, BinInfo* bin, uint64_t* depth_words,
                            float* dbg_proj, float* dbg_color, DevState* st, cudaStream_t stream);
-// (b) pair emission over the depth-sorted visible splats; counts pairs per tile.
-cudaError_t launch_emit(const FrameParams& fp, const BinInfo* bin, uint64_t n, unsigned long long* scan_desc,
-                        uint64_t* const* depth_words, uint64_t* pairs, uint64_t cap, uint32_t* tile_counts,
+// (b) pair emission over the depth-sorted visible splats; counts the tile
+// sort's digit histograms.
+cudaError_t launch_emit(const FrameParams& fp, int tile_digits, const BinInfo* bin, uint64_t n,
+                        unsigned long long* scan_desc, uint64_t* const* depth_words, uint64_t* pairs, uint64_t cap,
                         DevState* st, cudaStream_t stream);
 // (c) stable LSD sort of words[0] (ping-pong with words[1]) on `digits` 8-bit
 // digits from bit 32, whose schedule is already in ss; count may be null
@@ -113,11 +114,14 @@ cudaError_t launch_emit(const FrameParams& fp, const BinInfo* bin, uint64_t n, u
 cudaError_t launch_sort(SortState* ss, const unsigned long long* count, uint64_t cap, int digits, uint64_t* words0,
                         uint64_t* words1, uint32_t* lookback, uint64_t lookback_parts, DevState* st, int num_sms,
                         cudaStream_t stream);
-// (c) the depth sort's pass schedule (its histograms come from the projection).
+// (c) pass schedules (exclusive digit starts, skipped digits) of the depth
+// sort (histograms from the projection, all n words) and of the tile sort
+// (histograms from the emission, total_pairs words capped at cap).
 cudaError_t launch_depth_schedule(DevState* st, uint64_t n, cudaStream_t stream);
-// (c) tile ranges and the tile sort's digit histograms from the per-tile pair counts.
-cudaError_t launch_tile_prep(const uint32_t* tile_counts, uint32_t tiles, uint2* ranges, DevState* st,
-                             cudaStream_t stream);
+cudaError_t launch_tile_schedule(DevState* st, uint64_t cap, int digits, cudaStream_t stream);
+// (c) per-tile [begin, end) ranges from the tile-sorted pairs (ranges zeroed first).
+cudaError_t launch_ranges(uint64_t cap, uint64_t* const* pairs, uint2* ranges, uint32_t tiles, DevState* st,
+                          int num_sms, cudaStream_t stream);
 // (d) blend + downsample.
 cudaError_t launch_blend(const FrameParams& fp, const Record* rec, uint64_t* const* pairs, const uint2* ranges,
                          const DevState* st, bool exact, uint8_t* out, uint8_t* full_scratch, cudaStream_t stream);

@@ -71,56 +71,21 @@ __global__ void __launch_bounds__(256) k_hist_scan(SortState* ss, const unsigned
   schedule_passes(ss, sort_count(count, cap), digits);
 }
 
-// Tile ranges and the tile sort's digit histograms from the per-tile pair
-// counts (one CTA): ranges are the exclusive scan of the counts ([0, 0) for
-// an empty tile, as the reference's neighbour compare leaves it), the digit
-// histograms weigh each tile's digits by its count.
-__global__ void __launch_bounds__(256) k_tile_prep(const uint32_t* __restrict__ counts, uint32_t tiles,
-                                                   uint2* __restrict__ ranges, int digits, DevState* st) {
-  __shared__ uint32_t s_hist[kMaxPasses][256];
-  __shared__ uint32_t s_warp[8];
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  for (int t = tid; t < kMaxPasses * 256; t += 256) (&s_hist[0][0])[t] = 0u;
-  __syncthreads();
-  uint32_t running = 0;
-  for (uint32_t b0 = 0; b0 < tiles; b0 += 256 * 4) {
-    uint32_t c[4], sum = 0;
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
-      const uint32_t t = b0 + tid * 4 + k;
-      c[k] = t < tiles ? counts[t] : 0u;
-      sum += c[k];
+// Per-tile [begin, end) from neighbour compares over the tile-sorted pairs
+// (tiles.wgsl:83-101); empty tiles keep the zeroed [0, 0).
+__global__ void __launch_bounds__(256) k_ranges(uint64_t cap, const uint64_t* p0, const uint64_t* p1,
+                                                uint2* __restrict__ ranges, uint32_t tiles, const DevState* st) {
+  const uint64_t* __restrict__ pairs = st->tile.final_sel ? p1 : p0;
+  const uint64_t n = sort_count(&st->total_pairs, cap);
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t t = (uint32_t)(pairs[i] >> 32);
+    const uint32_t tn = i + 1 < n ? (uint32_t)(pairs[i + 1] >> 32) : 0xFFFFFFFFu;
+    if (i == 0 && t < tiles) ranges[t].x = 0u;
+    if (tn != t) {
+      if (t < tiles) ranges[t].y = (uint32_t)(i + 1);
+      if (tn < tiles) ranges[tn].x = (uint32_t)(i + 1);
     }
-    uint32_t x = sum;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-      if (lane >= o) x += y;
-    }
-    if (lane == 31) s_warp[warp] = x;
-    __syncthreads();
-    uint32_t base = running, chunk = 0;
-    for (int w = 0; w < 8; w++) {
-      if (w < warp) base += s_warp[w];
-      chunk += s_warp[w];
-    }
-    uint32_t start = base + x - sum;
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
-      const uint32_t t = b0 + tid * 4 + k;
-      if (t < tiles) {
-        ranges[t] = c[k] ? make_uint2(start, start + c[k]) : make_uint2(0u, 0u);
-        if (c[k])
-          for (int d = 0; d < digits; d++) atomicAdd(&s_hist[d][(t >> (8 * d)) & 255u], c[k]);
-      }
-      start += c[k];
-    }
-    running += chunk;
-    __syncthreads();
   }
-  for (int t = tid; t < digits * 256; t += 256) st->tile.hist[t >> 8][t & 255] = (&s_hist[0][0])[t];
-  __syncthreads();
-  schedule_passes(&st->tile, running, digits);
 }
 
 __global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(SortState* ss, const unsigned long long* count,
@@ -207,26 +172,37 @@ __global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(SortState* ss, con
       if (lane >= o) x += y;
     }
     if (lane == 31) s_wsum[warp] = x;
+    // Look back kLookAhead predecessors per step (independent loads), summing
+    // aggregates up to and including the nearest inclusive prefix.
     uint32_t prefix = 0;
     if (part != 0) {
+      constexpr int kLookAhead = 8;
       long long j = (long long)part - 1;
-      while (j >= 0) {
-        const uint32_t* q = lb + (uint64_t)j * 256 + tid;
-        uint32_t v = *(const volatile uint32_t*)q;
-        uint32_t spins = 0;
-        while ((v >> 30) == 0u) {
-          // Give up at the bound, or at once after another wait gave up.
-          if (++spins > kSpinLimit || ((spins & 1023u) == 0u && (*(volatile uint32_t*)&st->error & kErrSortTimeout))) {
-            atomicOr(&st->error, kErrSortTimeout);
-            v = kLbInc;
-            break;
+      bool found = false;
+      while (!found && j >= 0) {
+        uint32_t v[kLookAhead];
+#pragma unroll
+        for (int k = 0; k < kLookAhead; k++)
+          v[k] = (j - k >= 0) ? *(const volatile uint32_t*)(lb + (uint64_t)(j - k) * 256 + tid) : kLbInc;
+#pragma unroll
+        for (int k = 0; k < kLookAhead; k++) {
+          if (found) break;
+          uint32_t spins = 0;
+          while ((v[k] >> 30) == 0u) {
+            // Give up at the bound, or at once after another wait gave up.
+            if (++spins > kSpinLimit ||
+                ((spins & 1023u) == 0u && (*(volatile uint32_t*)&st->error & kErrSortTimeout))) {
+              atomicOr(&st->error, kErrSortTimeout);
+              v[k] = kLbInc;
+              break;
+            }
+            __nanosleep(20);
+            v[k] = *(const volatile uint32_t*)(lb + (uint64_t)(j - k) * 256 + tid);
           }
-          __nanosleep(20);
-          v = *(const volatile uint32_t*)q;
+          prefix += v[k] & kLbMask;
+          if ((v[k] >> 30) == 2u) found = true;
         }
-        prefix += v & kLbMask;
-        if ((v >> 30) == 2u) break;
-        j--;
+        j -= kLookAhead;
       }
       *(volatile uint32_t*)my = kLbInc | (prefix + running);
     }
@@ -279,11 +255,14 @@ cudaError_t launch_depth_schedule(DevState* st, uint64_t n, cudaStream_t stream)
   return cudaGetLastError();
 }
 
-cudaError_t launch_tile_prep(const uint32_t* tile_counts, uint32_t tiles, uint2* ranges, DevState* st,
-                             cudaStream_t stream) {
-  uint32_t bits = 0;
-  while (bits < 32 && (1u << bits) < tiles) bits++;
-  k_tile_prep<<<1, 256, 0, stream>>>(tile_counts, tiles, ranges, (int)((bits + 7) / 8), st);
+cudaError_t launch_tile_schedule(DevState* st, uint64_t cap, int digits, cudaStream_t stream) {
+  k_hist_scan<<<1, 256, 0, stream>>>(&st->tile, &st->total_pairs, cap, digits);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ranges(uint64_t cap, uint64_t* const* pairs, uint2* ranges, uint32_t tiles, DevState* st,
+                          int num_sms, cudaStream_t stream) {
+  k_ranges<<<num_sms * 8, 256, 0, stream>>>(cap, pairs[0], pairs[1], ranges, tiles, st);
   return cudaGetLastError();
 }
 
