@@ -151,8 +151,9 @@ __global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(SortState* ss, con
     }
     __syncthreads();
 
-    // Thread `tid` owns digit tid: warp offsets, block count, look-back, and
-    // the digit's run start inside the partition (a block scan of counts).
+    // Thread `tid` owns digit tid: warp offsets, the block count (published
+    // at once as this partition's aggregate) and the digit's run start inside
+    // the partition (a block scan of the counts).
     uint32_t running = 0;
 #pragma unroll
     for (int w = 0; w < kWarps; w++) {
@@ -161,10 +162,7 @@ __global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(SortState* ss, con
       running += t;
     }
     uint32_t* my = lb + (uint64_t)part * 256 + tid;
-    if (part == 0)
-      *(volatile uint32_t*)my = kLbInc | running;
-    else
-      *(volatile uint32_t*)my = kLbAgg | running;
+    *(volatile uint32_t*)my = (part == 0 ? kLbInc : kLbAgg) | running;
     uint32_t x = running;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -172,11 +170,29 @@ __global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(SortState* ss, con
       if (lane >= o) x += y;
     }
     if (lane == 31) s_wsum[warp] = x;
+    __syncthreads();
+    uint32_t wb = 0;
+    for (int w = 0; w < warp; w++) wb += s_wsum[w];
+    s_lbase[tid] = wb + x - running;
+    __syncthreads();
+
+    // Place the words in shared memory in partition order (this needs only
+    // the partition's own counts), freeing their registers for the look-back.
+#pragma unroll
+    for (int j = 0; j < kSortItems; j++) {
+      if (dr[j] != 0xFFFFFFFFu) {
+        const uint32_t dig = dr[j] & 255u;
+        s_keys[s_lbase[dig] + s_whist[warp][dig] + (dr[j] >> 8)] = key[j];
+      }
+    }
+
     // Look back kLookAhead predecessors per step (independent loads), summing
-    // aggregates up to and including the nearest inclusive prefix.
+    // aggregates up to and including the nearest inclusive prefix. When a
+    // whole wave of partitions starts together, partition p resolves after
+    // about p / (2 kLookAhead) load round trips.
     uint32_t prefix = 0;
     if (part != 0) {
-      constexpr int kLookAhead = 8;
+      constexpr int kLookAhead = 32;
       long long j = (long long)part - 1;
       bool found = false;
       while (!found && j >= 0) {
@@ -186,43 +202,28 @@ __global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(SortState* ss, con
           v[k] = (j - k >= 0) ? *(const volatile uint32_t*)(lb + (uint64_t)(j - k) * 256 + tid) : kLbInc;
 #pragma unroll
         for (int k = 0; k < kLookAhead; k++) {
-          if (found) break;
-          uint32_t spins = 0;
-          while ((v[k] >> 30) == 0u) {
-            // Give up at the bound, or at once after another wait gave up.
-            if (++spins > kSpinLimit ||
-                ((spins & 1023u) == 0u && (*(volatile uint32_t*)&st->error & kErrSortTimeout))) {
-              atomicOr(&st->error, kErrSortTimeout);
-              v[k] = kLbInc;
-              break;
+          if (!found) {
+            uint32_t spins = 0;
+            while ((v[k] >> 30) == 0u) {
+              // Give up at the bound, or at once after another wait gave up.
+              if (++spins > kSpinLimit ||
+                  ((spins & 1023u) == 0u && (*(volatile uint32_t*)&st->error & kErrSortTimeout))) {
+                atomicOr(&st->error, kErrSortTimeout);
+                v[k] = kLbInc;
+                break;
+              }
+              __nanosleep(20);
+              v[k] = *(const volatile uint32_t*)(lb + (uint64_t)(j - k) * 256 + tid);
             }
-            __nanosleep(20);
-            v[k] = *(const volatile uint32_t*)(lb + (uint64_t)(j - k) * 256 + tid);
+            prefix += v[k] & kLbMask;
+            if ((v[k] >> 30) == 2u) found = true;
           }
-          prefix += v[k] & kLbMask;
-          if ((v[k] >> 30) == 2u) found = true;
         }
         j -= kLookAhead;
       }
       *(volatile uint32_t*)my = kLbInc | (prefix + running);
     }
-    __syncthreads();
-    uint32_t wb = 0;
-    for (int w = 0; w < warp; w++) wb += s_wsum[w];
-    const uint32_t lbase = wb + x - running;
-    s_lbase[tid] = lbase;
     s_gbase[tid] = ss->hist[pass][tid] + prefix;
-    __syncthreads();
-
-    // Place the words in shared memory in partition order, then write them
-    // out in that order: runs of one digit land on consecutive addresses.
-#pragma unroll
-    for (int j = 0; j < kSortItems; j++) {
-      if (dr[j] != 0xFFFFFFFFu) {
-        const uint32_t dig = dr[j] & 255u;
-        s_keys[s_lbase[dig] + s_whist[warp][dig] + (dr[j] >> 8)] = key[j];
-      }
-    }
     __syncthreads();
     for (uint32_t l = tid; l < pcount; l += kSortThreads) {
       const uint64_t k = s_keys[l];
