@@ -27,10 +27,10 @@ SOURCES = {
     "api.cu": [],
     "project.cu": ["--fmad=false"],
     "binning.cu": [],
-    "sort.cu": [],
     "blend.cu": [],
 }
-HEADERS = [os.path.join(CSRC, "common.cuh"), os.path.join(ROOT, "include", "splat_cuda.h")]
+HEADERS = [os.path.join(CSRC, "common.cuh"), os.path.join(CSRC, "tilesort.cuh"),
+           os.path.join(ROOT, "include", "splat_cuda.h")]
 
 
 def _stale(target: str, deps) -> bool:

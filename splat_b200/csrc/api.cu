@@ -1,10 +1,10 @@
 // C ABI of the B200 rasterizer (include/splat_cuda.h): scene upload, buffer
 // management, the per-frame launch sequence and the host<->device boundary.
 //
-// One frame is: clear the frame state -> project + compact visible splats (a)
-// -> depth sort of the visible splats (c) -> scan + emit pairs in depth order
-// (b) -> tile sort of the pairs and tile ranges (c) -> blend + downsample (d)
-// -> one device-to-host copy of the frame and the frame state. The host never waits in the middle of a frame; pair counts
+// One frame is: clear the frame state -> project (a) -> bin pairs into
+// per-tile buckets: count, scans, ranges, scatter, sort of long tiles (b, c)
+// -> per-tile depth sort + blend + downsample (c, d) -> one device-to-host
+// copy of the frame and the frame state. The host never waits in the middle of a frame; pair counts
 // that exceed the allocated capacity are detected from the frame state after
 // the frame, the buffers grow and the frame is rendered again (the
 // reference's grow-and-retry, src/render/gpu.rs:1040-1056).
@@ -40,18 +40,16 @@ struct splat_cuda_handle {
   // per-splat frame buffers
   Record* rec = nullptr;
   BinInfo* bin = nullptr;
-  unsigned long long* desc_emit = nullptr;  // scan descriptors, one per partition
-  uint64_t* depth_words[2] = {nullptr, nullptr};
-  uint32_t* lb_depth = nullptr;  // look-back words of the depth sort
-  uint64_t lb_depth_parts = 0;
-  // pair buffers
+  // pair buffers: per-tile buckets and the long-tile sort's scratch
   uint64_t cap = 0;
   uint64_t* pairs[2] = {nullptr, nullptr};
-  uint32_t* lb_tile = nullptr;  // look-back words of the tile sort
-  uint64_t lb_tile_parts = 0;
   // per-size buffers
   uint2* ranges = nullptr;
-  uint64_t ranges_cap = 0;  // tiles
+  uint32_t* counts = nullptr;     // bin_rows x tiles
+  uint32_t* totals = nullptr;     // tiles
+  uint32_t* long_list = nullptr;  // tiles
+  uint64_t ranges_cap = 0;        // tiles
+  size_t max_smem = 48 * 1024;
   uint8_t* out_dev = nullptr;
   size_t out_cap = 0;
   uint8_t* full_dev = nullptr;
@@ -108,7 +106,6 @@ uint32_t bits_for(uint64_t v) {  // bits needed to hold values < v
 
 void free_pairs(splat_cuda_handle* h) {
   for (int b = 0; b < 2; b++) dfree(h->pairs[b]);
-  dfree(h->lb_tile);
   h->cap = 0;
 }
 
@@ -117,8 +114,6 @@ int ensure_pairs(splat_cuda_handle* h, uint64_t cap) {
   if (cap > kMaxPairs) return fail(h, SPLAT_ERR_CAPACITY, "more than 2^30 - 1 gaussian/tile pairs");
   free_pairs(h);
   for (int b = 0; b < 2; b++) CK(cudaMalloc(&h->pairs[b], cap * sizeof(uint64_t)), "cudaMalloc pairs");
-  h->lb_tile_parts = (cap + kSortPart - 1) / kSortPart;
-  CK(cudaMalloc(&h->lb_tile, (size_t)kMaxPasses * h->lb_tile_parts * 256 * sizeof(uint32_t)), "cudaMalloc lookback");
   h->cap = cap;
   return SPLAT_OK;
 }
@@ -126,7 +121,14 @@ int ensure_pairs(splat_cuda_handle* h, uint64_t cap) {
 int ensure_size(splat_cuda_handle* h, uint64_t tiles, size_t out_bytes, size_t full_bytes) {
   if (tiles > h->ranges_cap) {
     dfree(h->ranges);
+    dfree(h->counts);
+    dfree(h->totals);
+    dfree(h->long_list);
+    h->ranges_cap = 0;
     CK(cudaMalloc(&h->ranges, tiles * sizeof(uint2)), "cudaMalloc ranges");
+    CK(cudaMalloc(&h->counts, (size_t)bin_rows(h->num_sms) * tiles * sizeof(uint32_t)), "cudaMalloc counts");
+    CK(cudaMalloc(&h->totals, tiles * sizeof(uint32_t)), "cudaMalloc totals");
+    CK(cudaMalloc(&h->long_list, tiles * sizeof(uint32_t)), "cudaMalloc long tiles");
     h->ranges_cap = tiles;
   }
   if (out_bytes > h->out_cap) {
@@ -192,42 +194,21 @@ int enqueue_frame(splat_cuda_handle* h, const FrameParams& fp, uint8_t* dev_out)
   int rc = ensure_size(h, tiles, 0, full_bytes);
   if (rc) return rc;
   cudaStream_t s = h->stream;
-  const int tile_digits = (int)((bits_for(tiles) + 7) / 8);
   CK(cudaMemsetAsync(h->st, 0, sizeof(DevState), s), "clear frame state");
-  CK(cudaMemsetAsync(h->ranges, 0, tiles * sizeof(uint2), s), "clear ranges");
-  if (h->n) {
-    const size_t nd = ((h->n + kScanThreads - 1) / kScanThreads) * sizeof(unsigned long long);
-    CK(cudaMemsetAsync(h->desc_emit, 0, nd, s), "clear scan");
-    CK(cudaMemsetAsync(h->lb_depth, 0, (size_t)kMaxPasses * h->lb_depth_parts * 256 * sizeof(uint32_t), s),
-       "clear lookback");
-    if (tile_digits)
-      CK(cudaMemsetAsync(h->lb_tile, 0, (size_t)tile_digits * h->lb_tile_parts * 256 * sizeof(uint32_t), s),
-         "clear lookback");
-  }
   if (h->stage_events) CK(cudaEventRecord(h->ev[0], s), "event");
   if (h->n) {
     SceneDev sd{h->pos_op, h->cov_a, h->cov_b, h->color, h->sh, h->n, h->sh_degree};
-    CK(launch_project(fp, sd, h->rec, h->bin, h->depth_words[0], h->debug_capture ? h->dbg_proj : nullptr,
+    CK(launch_project(fp, sd, h->rec, h->bin, h->debug_capture ? h->dbg_proj : nullptr,
                       h->debug_capture ? h->dbg_color : nullptr, h->st, s),
        "project kernel");
   }
   if (h->stage_events) CK(cudaEventRecord(h->ev[1], s), "event");
-  if (h->n) {
-    DevState* st = h->st;
-    CK(launch_depth_schedule(st, h->n, s), "depth schedule");
-    CK(launch_sort(&st->depth, nullptr, h->n, kMaxPasses, h->depth_words[0], h->depth_words[1], h->lb_depth,
-                   h->lb_depth_parts, st, h->num_sms, s),
-       "depth sort");
-    CK(launch_emit(fp, tile_digits, h->bin, h->n, h->desc_emit, h->depth_words, h->pairs[0], h->cap, st, s),
-       "emit kernel");
-    CK(launch_tile_schedule(st, h->cap, tile_digits, s), "tile schedule");
-    CK(launch_sort(&st->tile, &st->total_pairs, h->cap, tile_digits, h->pairs[0], h->pairs[1], h->lb_tile,
-                   h->lb_tile_parts, st, h->num_sms, s),
-       "tile sort");
-    CK(launch_ranges(h->cap, h->pairs, h->ranges, (uint32_t)tiles, st, h->num_sms, s), "ranges");
-  }
+  CK(launch_binning(fp, h->bin, h->n, h->counts, h->totals, h->ranges, h->long_list, h->pairs[0], h->pairs[1], h->cap,
+                    h->st, h->num_sms, h->max_smem, s),
+     "binning kernels");
   if (h->stage_events) CK(cudaEventRecord(h->ev[2], s), "event");
-  CK(launch_blend(fp, h->rec, h->pairs, h->ranges, h->st, h->exact, dev_out, h->full_dev, s), "blend kernel");
+  CK(launch_blend(fp, h->rec, h->pairs[0], h->ranges, h->exact, h->debug_capture, dev_out, h->full_dev, s),
+     "blend kernel");
   if (h->stage_events) CK(cudaEventRecord(h->ev[3], s), "event");
   CK(cudaMemcpyAsync(h->st_host, h->st, sizeof(DevState), cudaMemcpyDeviceToHost, s), "copy frame state");
   h->last_fp = fp;
@@ -239,10 +220,6 @@ int finish_frame(splat_cuda_handle* h, splat_render_stats* stats, int* regrown) 
   *regrown = 0;
   CK(cudaStreamSynchronize(h->stream), "frame");
   const DevState& st = *h->st_host;
-  if (st.error & (kErrEmitTimeout | kErrSortTimeout))
-    return fail(h, SPLAT_ERR_TIMEOUT, "a device-side look-back wait gave up");
-  if ((st.error & kErrSortRange) && st.total_pairs <= h->cap)
-    return fail(h, SPLAT_ERR_DEVICE, "sort produced an out-of-range position");
   if (stats) {
     stats->visible = st.visible;
     stats->overlaps = st.total_pairs;
@@ -327,6 +304,10 @@ SPLAT_API int splat_cuda_create(const splat_scene_desc* d, int device, splat_cud
   if (e != cudaSuccess) return bail(cuda_fail(h, e, "cudaSetDevice"));
   e = cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, device);
   if (e != cudaSuccess) return bail(cuda_fail(h, e, "device attributes"));
+  int optin = 0;
+  e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+  if (e != cudaSuccess) return bail(cuda_fail(h, e, "device attributes"));
+  h->max_smem = (size_t)optin;
   if ((e = cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking)) != cudaSuccess)
     return bail(cuda_fail(h, e, "cudaStreamCreate"));
   h->stream = h->own_stream;
@@ -376,14 +357,7 @@ SPLAT_API int splat_cuda_create(const splat_scene_desc* d, int device, splat_cud
     }
     if ((e = cudaMalloc(&h->rec, n * sizeof(Record))) != cudaSuccess) return bail(cuda_fail(h, e, "cudaMalloc records"));
     if ((e = cudaMalloc(&h->bin, n * sizeof(BinInfo))) != cudaSuccess) return bail(cuda_fail(h, e, "cudaMalloc bins"));
-    const size_t nd = ((n + kScanThreads - 1) / kScanThreads) * sizeof(unsigned long long);
-    if ((e = cudaMalloc(&h->desc_emit, nd)) != cudaSuccess) return bail(cuda_fail(h, e, "cudaMalloc scan"));
-    for (int b = 0; b < 2; b++)
-      if ((e = cudaMalloc(&h->depth_words[b], n * sizeof(uint64_t))) != cudaSuccess)
-        return bail(cuda_fail(h, e, "cudaMalloc depth words"));
-    h->lb_depth_parts = (n + kSortPart - 1) / kSortPart;
-    if ((e = cudaMalloc(&h->lb_depth, (size_t)kMaxPasses * h->lb_depth_parts * 256 * sizeof(uint32_t))) != cudaSuccess)
-      return bail(cuda_fail(h, e, "cudaMalloc lookback"));
+
   }
   int rc = ensure_pairs(h, std::max<uint64_t>(4 * n, 1u << 16));
   if (rc) return bail(rc);
@@ -520,15 +494,19 @@ SPLAT_API int splat_cuda_debug_dump(splat_cuda_handle* h, float* proj, uint8_t* 
     for (uint64_t i = 0; i < h->n; i++) visible[i] = bin[i].rect_lo != kCulled;
   const uint64_t m = std::min(P, key_capacity);
   if ((keys || values) && m) {
-    // Pairs are (tile << 32 | splat); the reference's key of a pair is
-    // (tile << 32 | depth bits of its splat).
+    // The buckets hold each tile's pairs (depth bits << 32 | splat) in blend
+    // order when debug capture is on; the reference's key of a pair is
+    // tile << 32 | depth bits.
+    const uint64_t tiles = (uint64_t)h->last_fp.tiles_x * h->last_fp.tiles_y;
     std::vector<uint64_t> pw(m);
-    CK(cudaMemcpy(pw.data(), h->pairs[st.tile.final_sel], m * 8, cudaMemcpyDeviceToHost), "dump");
-    for (uint64_t p = 0; p < m; p++) {
-      const uint32_t splat = (uint32_t)pw[p];
-      if (values) values[p] = splat;
-      if (keys) keys[p] = (pw[p] & 0xFFFFFFFF00000000ull) | (splat < h->n ? bin[splat].depth_bits : 0u);
-    }
+    std::vector<uint2> rg(tiles);
+    CK(cudaMemcpy(pw.data(), h->pairs[0], m * 8, cudaMemcpyDeviceToHost), "dump");
+    CK(cudaMemcpy(rg.data(), h->ranges, tiles * sizeof(uint2), cudaMemcpyDeviceToHost), "dump");
+    for (uint64_t t = 0; t < tiles; t++)
+      for (uint64_t p = rg[t].x; p < rg[t].y && p < m; p++) {
+        if (values) values[p] = (uint32_t)pw[p];
+        if (keys) keys[p] = (t << 32) | (pw[p] >> 32);
+      }
   }
   if (ranges) {
     const uint64_t tiles = (uint64_t)h->last_fp.tiles_x * h->last_fp.tiles_y;
@@ -550,11 +528,11 @@ SPLAT_API int splat_cuda_destroy(splat_cuda_handle* h) {
   dfree(h->sh);
   dfree(h->rec);
   dfree(h->bin);
-  dfree(h->desc_emit);
-  for (int b = 0; b < 2; b++) dfree(h->depth_words[b]);
-  dfree(h->lb_depth);
   free_pairs(h);
   dfree(h->ranges);
+  dfree(h->counts);
+  dfree(h->totals);
+  dfree(h->long_list);
   dfree(h->out_dev);
   dfree(h->full_dev);
   dfree(h->st);

@@ -1,183 +1,338 @@
-// Kernel (b): device-wide exclusive scan of the per-splat pair counts with
-// warp shuffles and a decoupled look-back, fused with the pair emission.
+// Kernel (b): binning of (splat, tile) pairs into per-tile buckets, and the
+// sort of tiles too long to sort inside the blend CTA.
 //
-// The scan runs over the visible splats in depth order (the first `visible`
-// words of the depth sort's output: depth bits << 32 | splat index, ties in
-// splat-index order). Each visible splat duplicates into one pair per tile of
-// its pixel bbox, row-major (ty, then tx) as the reference's `emit` does
-// (src/render/cpu.rs:251-277); a pair is the 64-bit word tile << 32 | splat.
-// Pairs are therefore laid out in (depth, splat index) order, and the stable
-// tile sort that follows yields the reference's per-tile blending order:
-// by depth, ties by scene index (src/render/naive.rs:306-308,
-// src/render/cpu.rs:396-414). The reference's sort key of a pair,
-// tile << 32 | depth bits, is recovered exactly from the pair's tile and its
-// splat's depth bits.
+// Every visible splat duplicates into one pair per tile of its pixel bbox
+// (src/render/cpu.rs:251-277). The reference buckets pairs with a counting
+// sort by tile (cpu.rs:149-199): per-group tile histograms, a prefix over
+// (tile, group), then a scatter. The same scheme here, with CTAs as groups:
 //
-// A CTA scans 1024 splats (4 rounds of 32 per warp, their gathers in flight
-// together). A lane expands its own splat when it has at most 32 pairs; a
-// larger splat is expanded by its whole warp, so one large splat does not
-// serialise its warp. Pairs are staged in shared memory at their offset in
-// the CTA's contiguous output range and then written out coalesced, and the
-// tile sort's digit histograms are counted from the staged pairs (pairs past
-// the staging buffer go straight to global memory and are counted there).
+//  k_bin_count    each CTA counts the pairs of its slice of splats per tile
+//                 in shared memory and writes its row of the count matrix;
+//  k_bin_colscan  per tile, an exclusive scan of the counts down the rows;
+//  k_bin_tilescan an exclusive scan of the tile totals: the tile ranges
+//                 ([begin, end); [0, 0) for an empty tile) and the list of
+//                 tiles longer than the blend CTA sorts itself;
+//  k_bin_scatter  each CTA writes its pairs at its row's offsets, positions
+//                 handed out by shared-memory atomics.
+//
+// A pair is the word depth bits << 32 | splat index. Order inside a bucket is
+// whatever the atomics produced; the per-tile depth sort that follows (in the
+// blend CTA, or k_sort_long for long tiles) restores the reference's order.
 #include "common.cuh"
-#include "lookback.cuh"
+#include "tilesort.cuh"
 
 namespace splat {
 namespace {
 
-constexpr int kWarps = kScanThreads / 32;
-constexpr int kRounds = 4;
-constexpr int kEmitPart = kScanThreads * kRounds;
+constexpr int kBinThreads = 512;
 
-constexpr uint32_t kStage = 4096;  // staged pairs per CTA (32 KB)
-
-__device__ __forceinline__ void count_digits(uint32_t (*hist)[256], uint32_t tile, int digits) {
-  for (int d = 0; d < digits; d++) atomicAdd(&hist[d][(tile >> (8 * d)) & 255u], 1u);
-}
-
-__global__ void __launch_bounds__(kScanThreads) k_emit(uint32_t tiles_x, int tile_digits,
-                                                       const BinInfo* __restrict__ bin, unsigned long long* desc,
-                                                       const uint64_t* dw0, const uint64_t* dw1,
-                                                       uint64_t* __restrict__ pairs, uint64_t cap, DevState* st) {
-  __shared__ uint32_t s_part;
-  __shared__ uint32_t s_warp[kWarps];
-  __shared__ unsigned long long s_base;
-  __shared__ uint32_t s_total;
-  __shared__ uint32_t s_hist[kMaxPasses][256];
-  __shared__ uint64_t s_stage[kStage];
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const uint64_t V = *(const volatile unsigned long long*)&st->visible;
-  const uint64_t nparts = (V + kEmitPart - 1) / kEmitPart;
-  if (tid == 0) s_part = atomicAdd(&st->emit_ticket, 1u);
-  for (int t = tid; t < kMaxPasses * 256; t += kScanThreads) (&s_hist[0][0])[t] = 0u;
-  __syncthreads();
-  const uint32_t part = s_part;
-  if (part >= nparts) return;  // uniform across the block
-  const uint64_t* __restrict__ dsorted = st->depth.final_sel ? dw1 : dw0;
-  const uint64_t wbase = (uint64_t)part * kEmitPart + (uint64_t)warp * (32 * kRounds);
-  uint32_t idx[kRounds], cnt[kRounds], lo[kRounds], hi[kRounds], incl[kRounds];
-#pragma unroll
-  for (int r = 0; r < kRounds; r++) {
-    const uint64_t q = wbase + (uint64_t)r * 32 + lane;
-    idx[r] = q < V ? (uint32_t)dsorted[q] : 0xFFFFFFFFu;
-  }
-#pragma unroll
-  for (int r = 0; r < kRounds; r++) {
-    cnt[r] = 0u;
-    lo[r] = hi[r] = 0u;
-    if (idx[r] != 0xFFFFFFFFu) {
-      const BinInfo b = bin[idx[r]];
-      cnt[r] = b.count;
-      lo[r] = b.rect_lo;
-      hi[r] = b.rect_hi;
-    }
-  }
-  uint32_t warp_total = 0;
-#pragma unroll
-  for (int r = 0; r < kRounds; r++) {
-    uint32_t x = cnt[r];
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-      if (lane >= o) x += y;
-    }
-    incl[r] = x;
-    warp_total += __shfl_sync(0xffffffffu, x, 31);
-  }
-  if (lane == 0) s_warp[warp] = warp_total;
-  __syncthreads();
-  if (warp == 0) {
-    const uint32_t c = lane < kWarps ? s_warp[lane] : 0u;
-    uint32_t w = c;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
-      if (lane >= o) w += y;
-    }
-    const uint32_t total = __shfl_sync(0xffffffffu, w, 31);
-    if (lane < kWarps) s_warp[lane] = w - c;  // exclusive per warp
-    const unsigned long long base = lookback_exclusive(desc, part, total, st, kErrEmitTimeout);
-    if (lane == 0) {
-      s_base = base;
-      s_total = total;
-      if ((uint64_t)part == nparts - 1) st->total_pairs = base + total;
-    }
-  }
-  __syncthreads();
-
-  // Expansion into the staging buffer: local offset = offset in this CTA's range.
-  const uint64_t cta_base = s_base;
-  auto put = [&](uint32_t local, uint32_t tile, uint32_t splat) {
-    const uint64_t word = ((uint64_t)tile << 32) | splat;
-    if (local < kStage) {
-      s_stage[local] = word;
-    } else if (cta_base + local < cap) {
-      pairs[cta_base + local] = word;
-      count_digits(s_hist, tile, tile_digits);
-    }
-  };
-  constexpr uint32_t kLanePairs = 32;
-  uint32_t round_local = s_warp[warp];
-#pragma unroll
-  for (int r = 0; r < kRounds; r++) {
-    const uint32_t x = incl[r];
-    const uint32_t round_total = __shfl_sync(0xffffffffu, x, 31);
-    const uint32_t my_excl = x - cnt[r];
-    if (cnt[r] <= kLanePairs) {
-      const uint32_t tx0 = lo[r] & 0xFFFFu, ty0 = lo[r] >> 16, tx1 = hi[r] & 0xFFFFu;
-      uint32_t local = round_local + my_excl;
+// Calls f(tile, splat, depth bits) for every pair of the splats [s0, s1): a
+// lane expands its own splat when it has at most 32 pairs, larger splats are
+// expanded by the whole warp.
+template <class F>
+__device__ __forceinline__ void for_each_pair(const BinInfo* __restrict__ bin, uint64_t s0, uint64_t s1,
+                                              uint32_t tiles_x, F&& f) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int kWarpsPerCta = kBinThreads / 32;
+  for (uint64_t wb = s0 + (uint64_t)warp * 32; wb < s1; wb += (uint64_t)kWarpsPerCta * 32) {
+    const uint64_t i = wb + lane;
+    BinInfo b{kCulled, 0u, 0u, 0u};
+    if (i < s1) b = bin[i];
+    const uint32_t cnt = b.rect_lo != kCulled ? b.count : 0u;
+    if (cnt <= 32) {
+      const uint32_t tx0 = b.rect_lo & 0xFFFFu, ty0 = b.rect_lo >> 16, tx1 = b.rect_hi & 0xFFFFu;
       uint32_t tx = tx0, ty = ty0;
-      for (uint32_t p = 0; p < cnt[r]; p++, local++) {
-        put(local, ty * tiles_x + tx, idx[r]);
+      for (uint32_t p = 0; p < cnt; p++) {
+        f(ty * tiles_x + tx, (uint32_t)i, b.depth_bits);
         if (++tx == tx1) {
           tx = tx0;
           ty++;
         }
       }
     }
-    uint32_t big = __ballot_sync(0xffffffffu, cnt[r] > kLanePairs);
+    uint32_t big = __ballot_sync(0xffffffffu, cnt > 32);
     while (big) {
       const int L = __ffs(big) - 1;
       big &= big - 1u;
-      const uint32_t b_lo = __shfl_sync(0xffffffffu, lo[r], L), b_hi = __shfl_sync(0xffffffffu, hi[r], L);
-      const uint32_t b_cnt = __shfl_sync(0xffffffffu, cnt[r], L), b_ex = __shfl_sync(0xffffffffu, my_excl, L);
-      const uint32_t b_id = __shfl_sync(0xffffffffu, idx[r], L);
-      const uint32_t btx0 = b_lo & 0xFFFFu, bty0 = b_lo >> 16, wdt = (b_hi & 0xFFFFu) - btx0;
+      const uint32_t b_lo = __shfl_sync(0xffffffffu, b.rect_lo, L), b_hi = __shfl_sync(0xffffffffu, b.rect_hi, L);
+      const uint32_t b_cnt = __shfl_sync(0xffffffffu, cnt, L), b_d = __shfl_sync(0xffffffffu, b.depth_bits, L);
+      const uint32_t b_i = __shfl_sync(0xffffffffu, (uint32_t)i, L);
+      const uint32_t tx0 = b_lo & 0xFFFFu, ty0 = b_lo >> 16, wdt = (b_hi & 0xFFFFu) - tx0;
       for (uint32_t k = lane; k < b_cnt; k += 32) {
         const uint32_t row = k / wdt;
-        put(round_local + b_ex + k, (bty0 + row) * tiles_x + btx0 + (k - row * wdt), b_id);
+        f((ty0 + row) * tiles_x + tx0 + (k - row * wdt), b_i, b_d);
       }
     }
-    round_local += round_total;
   }
-  __syncthreads();
-  // Coalesced write-out of the staged pairs, counting their tile digits.
-  const uint32_t staged = min(s_total, kStage);
-  for (uint32_t l = tid; l < staged; l += kScanThreads) {
-    if (cta_base + l < cap) {
-      const uint64_t word = s_stage[l];
-      pairs[cta_base + l] = word;
-      count_digits(s_hist, (uint32_t)(word >> 32), tile_digits);
+}
+
+// SMEM: the CTA's row lives in shared memory (tiles * 4 bytes); otherwise the
+// CTA counts straight into its global row (zeroed beforehand).
+template <bool SMEM>
+__global__ void __launch_bounds__(kBinThreads) k_bin_count(const BinInfo* __restrict__ bin, uint64_t n,
+                                                           uint64_t per_cta, uint32_t tiles_x, uint32_t tiles,
+                                                           uint32_t* __restrict__ counts) {
+  extern __shared__ uint32_t s_row[];
+  uint32_t* row = counts + (uint64_t)blockIdx.x * tiles;
+  if (SMEM) {
+    for (uint32_t t = threadIdx.x; t < tiles; t += kBinThreads) s_row[t] = 0u;
+    __syncthreads();
+  }
+  const uint64_t s0 = min(n, (uint64_t)blockIdx.x * per_cta), s1 = min(n, s0 + per_cta);
+  for_each_pair(bin, s0, s1, tiles_x, [&](uint32_t t, uint32_t, uint32_t) {
+    if (SMEM)
+      atomicAdd(&s_row[t], 1u);
+    else
+      atomicAdd(&row[t], 1u);
+  });
+  if (SMEM) {
+    __syncthreads();
+    for (uint32_t t = threadIdx.x; t < tiles; t += kBinThreads) row[t] = s_row[t];
+  }
+}
+
+// Per tile: exclusive scan of the counts down the rows; the tile's total.
+__global__ void __launch_bounds__(256) k_bin_colscan(uint32_t* __restrict__ counts, uint32_t rows, uint32_t tiles,
+                                                     uint32_t* __restrict__ totals) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= tiles) return;
+  uint32_t running = 0;
+  uint32_t r = 0;
+  for (; r + 4 <= rows; r += 4) {
+    uint32_t v[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) v[k] = counts[(uint64_t)(r + k) * tiles + t];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      counts[(uint64_t)(r + k) * tiles + t] = running;
+      running += v[k];
     }
   }
-  __syncthreads();
-  for (int t = tid; t < tile_digits * 256; t += kScanThreads) {
-    const uint32_t v = (&s_hist[0][0])[t];
-    if (v) atomicAdd(&(&st->tile.hist[0][0])[t], v);
+  for (; r < rows; r++) {
+    const uint32_t v = counts[(uint64_t)r * tiles + t];
+    counts[(uint64_t)r * tiles + t] = running;
+    running += v;
+  }
+  totals[t] = running;
+}
+
+// One CTA: exclusive scan of the tile totals -> ranges, total pairs, long tiles.
+__global__ void __launch_bounds__(1024) k_bin_tilescan(const uint32_t* __restrict__ totals, uint32_t tiles,
+                                                       uint64_t cap, uint2* __restrict__ ranges, uint32_t long_min,
+                                                       uint32_t* __restrict__ long_list, DevState* st) {
+  __shared__ unsigned long long s_warp[32];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  unsigned long long running = 0;
+  for (uint32_t b0 = 0; b0 < tiles; b0 += 1024 * 4) {
+    uint32_t c[4];
+    unsigned long long sum = 0;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const uint32_t t = b0 + tid * 4 + k;
+      c[k] = t < tiles ? totals[t] : 0u;
+      sum += c[k];
+    }
+    unsigned long long x = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) s_warp[warp] = x;
+    __syncthreads();
+    unsigned long long base = running, chunk = 0;
+    for (int w = 0; w < 32; w++) {
+      if (w < warp) base += s_warp[w];
+      chunk += s_warp[w];
+    }
+    unsigned long long start = base + x - sum;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const uint32_t t = b0 + tid * 4 + k;
+      if (t < tiles) {
+        // Ranges are clamped to the pair capacity: past it the frame is
+        // incomplete and rendered again with larger buffers, and nothing
+        // reads beyond the buffers meanwhile.
+        const uint32_t s = (uint32_t)min(start, (unsigned long long)cap);
+        const uint32_t e = (uint32_t)min(start + c[k], (unsigned long long)cap);
+        ranges[t] = e > s ? make_uint2(s, e) : make_uint2(0u, 0u);
+        if (c[k] > long_min) long_list[atomicAdd(&st->long_tiles, 1u)] = t;
+      }
+      start += c[k];
+    }
+    running += chunk;
+    __syncthreads();
+  }
+  if (tid == 0) st->total_pairs = running;
+}
+
+template <bool SMEM>
+__global__ void __launch_bounds__(kBinThreads) k_bin_scatter(const BinInfo* __restrict__ bin, uint64_t n,
+                                                             uint64_t per_cta, uint32_t tiles_x, uint32_t tiles,
+                                                             uint32_t* __restrict__ counts,
+                                                             const uint2* __restrict__ ranges,
+                                                             uint64_t* __restrict__ pairs, uint64_t cap) {
+  extern __shared__ uint32_t s_row[];
+  uint32_t* row = counts + (uint64_t)blockIdx.x * tiles;
+  if (SMEM) {
+    for (uint32_t t = threadIdx.x; t < tiles; t += kBinThreads) s_row[t] = ranges[t].x + row[t];
+    __syncthreads();
+  }
+  const uint64_t s0 = min(n, (uint64_t)blockIdx.x * per_cta), s1 = min(n, s0 + per_cta);
+  for_each_pair(bin, s0, s1, tiles_x, [&](uint32_t t, uint32_t i, uint32_t depth_bits) {
+    uint64_t pos;
+    if (SMEM)
+      pos = atomicAdd(&s_row[t], 1u);
+    else
+      pos = (uint64_t)ranges[t].x + atomicAdd(&row[t], 1u);
+    if (pos < cap) pairs[pos] = ((uint64_t)depth_bits << 32) | i;
+  });
+}
+
+// Sorts the pairs of each tile longer than the blend CTA's capacity, in
+// global memory (the pair buffer and the second pair buffer as ping-pong),
+// one CTA per tile: each pass of the tile sort runs over chunks of kLongChunk
+// words staged through shared memory, digit starts carried across chunks.
+constexpr int kLongChunk = 4096;
+
+struct LongSmem {
+  TileSortSmem t;
+  uint32_t run[256];  // running start of each digit across chunks
+  uint32_t key[kLongChunk];
+};
+
+__global__ void __launch_bounds__(kTileThreads) k_sort_long(const uint2* __restrict__ ranges,
+                                                            const uint32_t* __restrict__ long_list,
+                                                            uint64_t* __restrict__ w0, uint64_t* __restrict__ w1,
+                                                            uint64_t cap, const DevState* st) {
+  __shared__ LongSmem sm;
+  constexpr int kChunks = kLongChunk / (32 * kTileWarps);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t nlong = *(const volatile uint32_t*)&st->long_tiles;
+  for (uint32_t li = blockIdx.x; li < nlong; li += gridDim.x) {
+    const uint2 r = ranges[long_list[li]];  // within the capacity (k_bin_tilescan)
+    const uint32_t b = r.x, n = r.y - r.x;
+    uint32_t a = 0xFFFFFFFFu, o = 0u;
+    for (uint32_t e = tid; e < n; e += kTileThreads) {
+      const uint32_t k = (uint32_t)(w0[b + e] >> 32);
+      a &= k;
+      o |= k;
+    }
+    uint32_t and_all, or_all;
+    block_and_or(a, o, sm.t, and_all, or_all);
+    const uint32_t vary = and_all ^ or_all;
+    uint64_t* src = w0 + b;
+    uint64_t* dst = w1 + b;
+    for (int d = 0; d < 4; d++) {
+      const int shift = 32 + 8 * d;
+      if (((vary >> (8 * d)) & 255u) == 0u) continue;
+      // Digit starts over the whole tile.
+      clear_counts(sm.t);
+      __syncthreads();
+      for (uint32_t e = tid; e < n; e += kTileThreads) atomicAdd(&sm.t.wh[warp][(src[e] >> shift) & 255u], 1u);
+      __syncthreads();
+      digit_offsets(sm.t);
+      sm.run[tid] = sm.t.dstart[tid];
+      __syncthreads();
+      // Stable scatter, chunk by chunk in order.
+      for (uint32_t c0 = 0; c0 < n; c0 += kLongChunk) {
+        const uint32_t cn = min((uint32_t)kLongChunk, n - c0);
+        for (uint32_t e = tid; e < cn; e += kTileThreads) sm.key[e] = (uint32_t)(src[c0 + e] >> 32);
+        clear_counts(sm.t);
+        __syncthreads();
+        const uint32_t seg = (cn + kTileWarps - 1) / kTileWarps;
+        const uint32_t seg0 = min(cn, (uint32_t)warp * seg), seg1 = min(cn, seg0 + seg);
+        uint32_t k[kChunks], dr[kChunks];
+        warp_rank<kChunks>(sm.key, seg0, seg1, 8 * d, sm.t, k, dr);
+        __syncthreads();
+        // Exclusive per-warp offsets per digit; the chunk's count per digit.
+        uint32_t running = 0;
+#pragma unroll
+        for (int w = 0; w < kTileWarps; w++) {
+          const uint32_t t = sm.t.wh[w][tid];
+          sm.t.wh[w][tid] = running;
+          running += t;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int c = 0; c < kChunks; c++) {
+          if (dr[c] != 0xFFFFFFFFu) {
+            const uint32_t dig = dr[c] & 255u;
+            dst[sm.run[dig] + sm.t.wh[warp][dig] + (dr[c] >> 8)] = src[c0 + seg0 + (uint32_t)c * 32 + lane];
+          }
+        }
+        __syncthreads();
+        sm.run[tid] += running;
+        __syncthreads();
+      }
+      uint64_t* t = src;
+      src = dst;
+      dst = t;
+    }
+    if (src != w0 + b) {
+      for (uint32_t e = tid; e < n; e += kTileThreads) w0[b + e] = src[e];
+    }
+    __syncthreads();
+    // fix_ties: runs of equal depth ordered by splat index.
+    for (uint32_t e = tid + 1; e < n; e += kTileThreads) {
+      const uint32_t kk = (uint32_t)(w0[b + e] >> 32);
+      if (kk == (uint32_t)(w0[b + e - 1] >> 32) && (e == 1 || (uint32_t)(w0[b + e - 2] >> 32) != kk)) {
+        uint32_t r1 = e + 1;
+        while (r1 < n && (uint32_t)(w0[b + r1] >> 32) == kk) r1++;
+        for (uint32_t i = e; i < r1; i++) {  // insertion sort of [e-1, r1) by splat index
+          const uint64_t x = w0[b + i];
+          uint32_t j = i;
+          while (j > e - 1 && (uint32_t)w0[b + j - 1] > (uint32_t)x) {
+            w0[b + j] = w0[b + j - 1];
+            j--;
+          }
+          w0[b + j] = x;
+        }
+      }
+    }
+    __syncthreads();
   }
 }
 
 }  // namespace
 
-cudaError_t launch_emit(const FrameParams& fp, int tile_digits, const BinInfo* bin, uint64_t n,
-                        unsigned long long* scan_desc, uint64_t* const* depth_words, uint64_t* pairs, uint64_t cap,
-                        DevState* st, cudaStream_t stream) {
-  if (n == 0) return cudaSuccess;
-  // Enough CTAs for every splat being visible; CTAs past the visible count return at once.
-  const unsigned grid = (unsigned)((n + kEmitPart - 1) / kEmitPart);
-  k_emit<<<grid, kScanThreads, 0, stream>>>(fp.tiles_x, tile_digits, bin, scan_desc, depth_words[0], depth_words[1],
-                                            pairs, cap, st);
+uint32_t bin_rows(int num_sms) { return 2u * (uint32_t)num_sms; }
+
+cudaError_t launch_binning(const FrameParams& fp, const BinInfo* bin, uint64_t n, uint32_t* counts, uint32_t* totals,
+                           uint2* ranges, uint32_t* long_list, uint64_t* pairs, uint64_t* pairs_alt, uint64_t cap,
+                           DevState* st, int num_sms, size_t max_smem, cudaStream_t stream) {
+  const uint32_t tiles = fp.tiles_x * fp.tiles_y;
+  const uint32_t rows = bin_rows(num_sms);
+  const uint64_t per_cta = n ? (n + rows - 1) / rows : 1;
+  const size_t smem = (size_t)tiles * sizeof(uint32_t);
+  const bool use_smem = smem <= max_smem;
+  cudaError_t e = cudaSuccess;
+  if (n) {
+    if (use_smem) {
+      if ((e = cudaFuncSetAttribute(k_bin_count<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
+        return e;
+      k_bin_count<true><<<rows, kBinThreads, smem, stream>>>(bin, n, per_cta, fp.tiles_x, tiles, counts);
+    } else {
+      if ((e = cudaMemsetAsync(counts, 0, (size_t)rows * tiles * sizeof(uint32_t), stream))) return e;
+      k_bin_count<false><<<rows, kBinThreads, 0, stream>>>(bin, n, per_cta, fp.tiles_x, tiles, counts);
+    }
+    k_bin_colscan<<<(tiles + 255) / 256, 256, 0, stream>>>(counts, rows, tiles, totals);
+  } else {
+    if ((e = cudaMemsetAsync(totals, 0, (size_t)tiles * sizeof(uint32_t), stream))) return e;
+  }
+  k_bin_tilescan<<<1, 1024, 0, stream>>>(totals, tiles, cap, ranges, kBlendSortCap, long_list, st);
+  if (n) {
+    if (use_smem) {
+      if ((e = cudaFuncSetAttribute(k_bin_scatter<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
+        return e;
+      k_bin_scatter<true><<<rows, kBinThreads, smem, stream>>>(bin, n, per_cta, fp.tiles_x, tiles, counts, ranges,
+                                                               pairs, cap);
+    } else {
+      k_bin_scatter<false><<<rows, kBinThreads, 0, stream>>>(bin, n, per_cta, fp.tiles_x, tiles, counts, ranges,
+                                                             pairs, cap);
+    }
+    k_sort_long<<<num_sms, kTileThreads, 0, stream>>>(ranges, long_list, pairs, pairs_alt, cap, st);
+  }
   return cudaGetLastError();
 }
 

@@ -19,19 +19,8 @@ constexpr uint32_t kTilePixels = kTile * kTile;
 // Marks a culled splat in BinInfo::rect_lo.
 constexpr uint32_t kCulled = 0xFFFFFFFFu;
 
-// Largest pair count the sort's 30-bit look-back words can carry.
+// Largest pair capacity (pair offsets and tile ranges are 32-bit).
 constexpr uint64_t kMaxPairs = (1ull << 30) - 1;
-
-// Bounded spin of every device-side wait (decoupled look-back). A wait that
-// runs out sets an error bit and the kernel carries on without writing out of
-// bounds; the host turns the bit into SPLAT_ERR_TIMEOUT.
-constexpr uint32_t kSpinLimit = 1u << 20;
-
-enum ErrorBits : uint32_t {
-  kErrEmitTimeout = 1u,
-  kErrSortTimeout = 2u,
-  kErrSortRange = 4u,
-};
 
 // Per-frame constants (ProjectCtx, src/render/mod.rs:155-196) plus grid sizes.
 struct FrameParams {
@@ -66,70 +55,38 @@ struct __align__(16) Record {
 
 // Per-splat binning input written by the projection: the tile rectangle of
 // its pixel bbox (tx0 | ty0 << 16, tx1 | ty1 << 16), depth bits, pair count.
-// rect_lo == kCulled marks a culled splat.
+// rect_lo == kCulled marks a culled splat; a visible splat whose bbox holds
+// no pixel has count 0.
 struct __align__(16) BinInfo {
   uint32_t rect_lo, rect_hi, depth_bits, count;
 };
 
-constexpr int kMaxPasses = 4;  // 8-bit digits of a 32-bit sort field
-
-// One stable LSD sort of 64-bit words on (part of) their upper 32 bits.
-struct SortState {
-  unsigned int ticket[kMaxPasses];
-  int pass_src[kMaxPasses];  // per digit pass: source buffer (0/1) or -1 to skip
-  int final_sel;             // buffer holding the sorted words
-  unsigned int pad[3];
-  unsigned int hist[kMaxPasses][256];  // digit histograms, then exclusive starts
-};
+// Pairs a blend CTA sorts in shared memory; longer tiles are sorted by
+// k_sort_long before the blend.
+constexpr uint32_t kBlendSortCap = 2048;
 
 // Frame state in device memory, cleared at the start of every frame.
 struct DevState {
   unsigned long long visible;      // splats that survived culling
-  unsigned long long total_pairs;  // sum of per-splat pair counts (may exceed capacity)
+  unsigned long long total_pairs;  // (splat, tile) pairs, may exceed the capacity
   unsigned int error;
-  unsigned int project_ticket;
-  unsigned int emit_ticket;
-  unsigned int pad[5];
-  SortState depth;  // visible splats by depth: words (depth bits << 32 | splat)
-  SortState tile;   // pairs by tile: words (tile << 32 | splat), already in depth order
+  unsigned int long_tiles;         // tiles with more than kBlendSortCap pairs
+  unsigned int pad[2];
 };
 
-// Decoupled look-back descriptor flags (scans: 64-bit words).
-constexpr unsigned long long kFlagAgg = 1ull << 62;
-constexpr unsigned long long kFlagInc = 2ull << 62;
-constexpr unsigned long long kValMask = (1ull << 62) - 1;
-
 // Launchers (each returns the cudaGetLastError of its launches).
-// (a) projection; a depth word per splat and the depth-digit histograms.
-cudaError_t launch_project(const FrameParams& fp, const SceneDev& s, Record* rec, BinInfo* bin, uint64_t* depth_words,
-                           float* dbg_proj, float* dbg_color, DevState* st, cudaStream_t stream);
-// (b) pair emission over the depth-sorted visible splats; counts the tile
-// sort's digit histograms.
-cudaError_t launch_emit(const FrameParams& fp, int tile_digits, const BinInfo* bin, uint64_t n,
-                        unsigned long long* scan_desc, uint64_t* const* depth_words, uint64_t* pairs, uint64_t cap,
-                        DevState* st, cudaStream_t stream);
-// (c) stable LSD sort of words[0] (ping-pong with words[1]) on `digits` 8-bit
-// digits from bit 32, whose schedule is already in ss; count may be null
-// (then cap words are sorted).
-cudaError_t launch_sort(SortState* ss, const unsigned long long* count, uint64_t cap, int digits, uint64_t* words0,
-                        uint64_t* words1, uint32_t* lookback, uint64_t lookback_parts, DevState* st, int num_sms,
-                        cudaStream_t stream);
-// (c) pass schedules (exclusive digit starts, skipped digits) of the depth
-// sort (histograms from the projection, all n words) and of the tile sort
-// (histograms from the emission, total_pairs words capped at cap).
-cudaError_t launch_depth_schedule(DevState* st, uint64_t n, cudaStream_t stream);
-cudaError_t launch_tile_schedule(DevState* st, uint64_t cap, int digits, cudaStream_t stream);
-// (c) per-tile [begin, end) ranges from the tile-sorted pairs (ranges zeroed first).
-cudaError_t launch_ranges(uint64_t cap, uint64_t* const* pairs, uint2* ranges, uint32_t tiles, DevState* st,
-                          int num_sms, cudaStream_t stream);
-// (d) blend + downsample.
-cudaError_t launch_blend(const FrameParams& fp, const Record* rec, uint64_t* const* pairs, const uint2* ranges,
-                         const DevState* st, bool exact, uint8_t* out, uint8_t* full_scratch, cudaStream_t stream);
-
-// Partition size (pairs) of one onesweep CTA.
-constexpr int kSortThreads = 256;
-constexpr int kSortItems = 16;
-constexpr int kScanThreads = 256;  // splats per projection / emission partition
-constexpr int kSortPart = kSortThreads * kSortItems;
+// (a) projection: records, tile rectangles and pair counts, visible count.
+cudaError_t launch_project(const FrameParams& fp, const SceneDev& s, Record* rec, BinInfo* bin, float* dbg_proj,
+                           float* dbg_color, DevState* st, cudaStream_t stream);
+// (b) binning into per-tile buckets (count matrix of bin_rows() x tiles,
+// tile totals, ranges, the long-tile list) and the sort of long tiles.
+uint32_t bin_rows(int num_sms);
+cudaError_t launch_binning(const FrameParams& fp, const BinInfo* bin, uint64_t n, uint32_t* counts, uint32_t* totals,
+                           uint2* ranges, uint32_t* long_list, uint64_t* pairs, uint64_t* pairs_alt, uint64_t cap,
+                           DevState* st, int num_sms, size_t max_smem, cudaStream_t stream);
+// (d) per-tile depth sort + blend + downsample. writeback: store each tile's
+// sorted pairs back into `pairs` (for the debug dump).
+cudaError_t launch_blend(const FrameParams& fp, const Record* rec, uint64_t* pairs, const uint2* ranges, bool exact,
+                         bool writeback, uint8_t* out, uint8_t* full_scratch, cudaStream_t stream);
 
 }  // namespace splat

@@ -7,13 +7,7 @@
 // (no fused multiply-adds): the projected splats equal the oracle's bit for
 // bit. The kernel also emits each visible splat's tile rectangle (pixel_bbox,
 // src/render/cpu.rs:94-102 and the tile loop of cpu.rs:262-276), its pair
-// count and depth bits for the binning scan, and the 64-bit depth word
-// (depth bits << 32 | splat index) of every splat for the depth sort, a
-// culled splat with depth bits 0xFFFFFFFF so it sorts after every visible one
-// (visible depths are finite and positive, so their bit patterns order like
-// the floats and stay below 0x7F800000). The four 8-bit digit histograms of
-// the depth bits are counted here too, so the depth sort needs no histogram
-// pass of its own.
+// count and depth bits for the binning, and counts the visible splats.
 #include "common.cuh"
 
 namespace splat {
@@ -89,17 +83,12 @@ __device__ __forceinline__ void eval_sh(const float* __restrict__ sh, uint64_t n
 }
 
 template <int DEG>
-__global__ void __launch_bounds__(kScanThreads) k_project(FrameParams fp, SceneDev s, Record* __restrict__ rec,
-                                                          BinInfo* __restrict__ bin, uint64_t* __restrict__ depth_words,
-                                                          float* __restrict__ dbg_proj, float* __restrict__ dbg_color,
-                                                          DevState* st) {
-  __shared__ uint32_t s_hist[kMaxPasses][256];
+__global__ void __launch_bounds__(256) k_project(FrameParams fp, SceneDev s, Record* __restrict__ rec,
+                                                 BinInfo* __restrict__ bin, float* __restrict__ dbg_proj,
+                                                 float* __restrict__ dbg_color, DevState* st) {
   const int tid = threadIdx.x;
-  for (int t = tid; t < kMaxPasses * 256; t += kScanThreads) (&s_hist[0][0])[t] = 0u;
-  __syncthreads();
-  const uint64_t i = (uint64_t)blockIdx.x * kScanThreads + tid;
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + tid;
   bool vis = false;
-  uint32_t depth_bits = 0xFFFFFFFFu;
   if (i < s.n) {
     const float4 po = __ldg(&s.pos_op[i]);
     BinInfo b{kCulled, 0u, 0u, 0u};
@@ -181,7 +170,6 @@ __global__ void __launch_bounds__(kScanThreads) k_project(FrameParams fp, SceneD
       r.r2 = make_float4(col[2], __uint_as_float(bx0 | (x1 << 16)), __uint_as_float(by0 | (y1 << 16)), tz);
       rec[i] = r;
       b.depth_bits = __float_as_uint(tz);
-      depth_bits = b.depth_bits;
       if (bx0 < x1 && by0 < y1) {
         const uint32_t tx0 = bx0 / kTile, ty0 = by0 / kTile;
         const uint32_t tx1 = (x1 + kTile - 1) / kTile, ty1 = (y1 + kTile - 1) / kTile;
@@ -211,27 +199,17 @@ __global__ void __launch_bounds__(kScanThreads) k_project(FrameParams fp, SceneD
       dbg_color[3 * i + 2] = vis ? col[2] : 0.f;
     }
   }
-  if (i < s.n) {
-    depth_words[i] = ((uint64_t)depth_bits << 32) | i;
-#pragma unroll
-    for (int d = 0; d < kMaxPasses; d++) atomicAdd(&s_hist[d][(depth_bits >> (8 * d)) & 255u], 1u);
-  }
   const int nvis = __syncthreads_count(vis);
   if (tid == 0 && nvis) atomicAdd(&st->visible, (unsigned long long)nvis);
-  for (int t = tid; t < kMaxPasses * 256; t += kScanThreads) {
-    const uint32_t v = (&s_hist[0][0])[t];
-    if (v) atomicAdd(&(&st->depth.hist[0][0])[t], v);
-  }
 }
 
 }  // namespace
 
-cudaError_t launch_project(const FrameParams& fp, const SceneDev& s, Record* rec, BinInfo* bin, uint64_t* depth_words,
-                           float* dbg_proj, float* dbg_color, DevState* st, cudaStream_t stream) {
+cudaError_t launch_project(const FrameParams& fp, const SceneDev& s, Record* rec, BinInfo* bin, float* dbg_proj,
+                           float* dbg_color, DevState* st, cudaStream_t stream) {
   if (s.n == 0) return cudaSuccess;
-  const unsigned grid = (unsigned)((s.n + kScanThreads - 1) / kScanThreads);
-#define SPLAT_PROJECT(D) \
-  k_project<D><<<grid, kScanThreads, 0, stream>>>(fp, s, rec, bin, depth_words, dbg_proj, dbg_color, st)
+  const unsigned grid = (unsigned)((s.n + 255) / 256);
+#define SPLAT_PROJECT(D) k_project<D><<<grid, 256, 0, stream>>>(fp, s, rec, bin, dbg_proj, dbg_color, st)
   switch (s.sh_degree) {
     case 0: SPLAT_PROJECT(0); break;
     case 1: SPLAT_PROJECT(1); break;
