@@ -47,6 +47,7 @@ struct splat_cuda_handle {
   uint2* ranges = nullptr;
   uint32_t* counts = nullptr;     // bin_rows x tiles
   uint32_t* totals = nullptr;     // tiles
+  uint32_t* mid_list = nullptr;   // tiles
   uint32_t* long_list = nullptr;  // tiles
   uint64_t ranges_cap = 0;        // tiles
   size_t max_smem = 48 * 1024;
@@ -123,11 +124,13 @@ int ensure_size(splat_cuda_handle* h, uint64_t tiles, size_t out_bytes, size_t f
     dfree(h->ranges);
     dfree(h->counts);
     dfree(h->totals);
+    dfree(h->mid_list);
     dfree(h->long_list);
     h->ranges_cap = 0;
     CK(cudaMalloc(&h->ranges, tiles * sizeof(uint2)), "cudaMalloc ranges");
     CK(cudaMalloc(&h->counts, (size_t)bin_rows(h->num_sms) * tiles * sizeof(uint32_t)), "cudaMalloc counts");
     CK(cudaMalloc(&h->totals, tiles * sizeof(uint32_t)), "cudaMalloc totals");
+    CK(cudaMalloc(&h->mid_list, tiles * sizeof(uint32_t)), "cudaMalloc mid tiles");
     CK(cudaMalloc(&h->long_list, tiles * sizeof(uint32_t)), "cudaMalloc long tiles");
     h->ranges_cap = tiles;
   }
@@ -203,12 +206,11 @@ int enqueue_frame(splat_cuda_handle* h, const FrameParams& fp, uint8_t* dev_out)
        "project kernel");
   }
   if (h->stage_events) CK(cudaEventRecord(h->ev[1], s), "event");
-  CK(launch_binning(fp, h->bin, h->n, h->counts, h->totals, h->ranges, h->long_list, h->pairs[0], h->pairs[1], h->cap,
-                    h->st, h->num_sms, h->max_smem, s),
+  CK(launch_binning(fp, h->bin, h->n, h->counts, h->totals, h->ranges, h->mid_list, h->long_list, h->pairs[0],
+                    h->pairs[1], h->cap, h->st, h->num_sms, h->max_smem, s),
      "binning kernels");
   if (h->stage_events) CK(cudaEventRecord(h->ev[2], s), "event");
-  CK(launch_blend(fp, h->rec, h->pairs[0], h->ranges, h->exact, h->debug_capture, dev_out, h->full_dev, s),
-     "blend kernel");
+  CK(launch_blend(fp, h->rec, h->pairs[0], h->ranges, h->exact, dev_out, h->full_dev, s), "blend kernel");
   if (h->stage_events) CK(cudaEventRecord(h->ev[3], s), "event");
   CK(cudaMemcpyAsync(h->st_host, h->st, sizeof(DevState), cudaMemcpyDeviceToHost, s), "copy frame state");
   h->last_fp = fp;
@@ -495,8 +497,7 @@ SPLAT_API int splat_cuda_debug_dump(splat_cuda_handle* h, float* proj, uint8_t* 
   const uint64_t m = std::min(P, key_capacity);
   if ((keys || values) && m) {
     // The buckets hold each tile's pairs (depth bits << 32 | splat) in blend
-    // order when debug capture is on; the reference's key of a pair is
-    // tile << 32 | depth bits.
+    // order; the reference's key of a pair is tile << 32 | depth bits.
     const uint64_t tiles = (uint64_t)h->last_fp.tiles_x * h->last_fp.tiles_y;
     std::vector<uint64_t> pw(m);
     std::vector<uint2> rg(tiles);
@@ -532,6 +533,7 @@ SPLAT_API int splat_cuda_destroy(splat_cuda_handle* h) {
   dfree(h->ranges);
   dfree(h->counts);
   dfree(h->totals);
+  dfree(h->mid_list);
   dfree(h->long_list);
   dfree(h->out_dev);
   dfree(h->full_dev);

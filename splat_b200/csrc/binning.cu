@@ -92,33 +92,41 @@ __global__ void __launch_bounds__(kBinThreads) k_bin_count(const BinInfo* __rest
 }
 
 // Per tile: exclusive scan of the counts down the rows; the tile's total.
+// A CTA takes 32 tiles; its 8 warps each scan a contiguous eighth of the rows
+// (a warp reads 32 adjacent tiles of a row: coalesced), then the segment sums
+// are combined and the rows rewritten with exclusive offsets.
 __global__ void __launch_bounds__(256) k_bin_colscan(uint32_t* __restrict__ counts, uint32_t rows, uint32_t tiles,
                                                      uint32_t* __restrict__ totals) {
-  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= tiles) return;
-  uint32_t running = 0;
-  uint32_t r = 0;
-  for (; r + 4 <= rows; r += 4) {
-    uint32_t v[4];
-#pragma unroll
-    for (int k = 0; k < 4; k++) v[k] = counts[(uint64_t)(r + k) * tiles + t];
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
-      counts[(uint64_t)(r + k) * tiles + t] = running;
-      running += v[k];
+  __shared__ uint32_t s_seg[8][32];
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t t = blockIdx.x * 32 + lane;
+  const uint32_t per = (rows + 7) / 8;
+  const uint32_t r0 = min(rows, warp * per), r1 = min(rows, r0 + per);
+  uint32_t sum = 0;
+  if (t < tiles)
+    for (uint32_t r = r0; r < r1; r++) sum += counts[(uint64_t)r * tiles + t];
+  s_seg[warp][lane] = sum;
+  __syncthreads();
+  uint32_t run = 0, total = 0;
+  for (uint32_t w = 0; w < 8; w++) {
+    if (w < warp) run += s_seg[w][lane];
+    total += s_seg[w][lane];
+  }
+  if (t < tiles) {
+    for (uint32_t r = r0; r < r1; r++) {
+      const uint32_t v = counts[(uint64_t)r * tiles + t];
+      counts[(uint64_t)r * tiles + t] = run;
+      run += v;
     }
+    if (warp == 0) totals[t] = total;
   }
-  for (; r < rows; r++) {
-    const uint32_t v = counts[(uint64_t)r * tiles + t];
-    counts[(uint64_t)r * tiles + t] = running;
-    running += v;
-  }
-  totals[t] = running;
 }
 
-// One CTA: exclusive scan of the tile totals -> ranges, total pairs, long tiles.
+// One CTA: exclusive scan of the tile totals -> ranges, total pairs, and the
+// lists of tiles sorted by a whole CTA (mid) or in chunks (long).
 __global__ void __launch_bounds__(1024) k_bin_tilescan(const uint32_t* __restrict__ totals, uint32_t tiles,
-                                                       uint64_t cap, uint2* __restrict__ ranges, uint32_t long_min,
+                                                       uint64_t cap, uint2* __restrict__ ranges,
+                                                       uint32_t* __restrict__ mid_list,
                                                        uint32_t* __restrict__ long_list, DevState* st) {
   __shared__ unsigned long long s_warp[32];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -156,7 +164,11 @@ __global__ void __launch_bounds__(1024) k_bin_tilescan(const uint32_t* __restric
         const uint32_t s = (uint32_t)min(start, (unsigned long long)cap);
         const uint32_t e = (uint32_t)min(start + c[k], (unsigned long long)cap);
         ranges[t] = e > s ? make_uint2(s, e) : make_uint2(0u, 0u);
-        if (c[k] > long_min) long_list[atomicAdd(&st->long_tiles, 1u)] = t;
+        const uint32_t len = e > s ? e - s : 0u;
+        if (len > kMidSortCap)
+          long_list[atomicAdd(&st->long_tiles, 1u)] = t;
+        else if (len > kWarpSortCap)
+          mid_list[atomicAdd(&st->mid_tiles, 1u)] = t;
       }
       start += c[k];
     }
@@ -189,7 +201,50 @@ __global__ void __launch_bounds__(kBinThreads) k_bin_scatter(const BinInfo* __re
   });
 }
 
-// Sorts the pairs of each tile longer than the blend CTA's capacity, in
+// Tiles of at most kWarpSortCap pairs: one warp per tile.
+__global__ void __launch_bounds__(256) k_sort_small(const uint2* __restrict__ ranges, uint32_t tiles,
+                                                    uint64_t* __restrict__ pairs) {
+  __shared__ uint64_t s_scratch[8][kWarpSortCap];
+  __shared__ uint32_t s_counts[8][256];
+  const uint32_t warp = threadIdx.x >> 5;
+  const uint32_t tile = blockIdx.x * 8 + warp;
+  if (tile >= tiles) return;
+  const uint2 r = ranges[tile];
+  const uint32_t n = r.y - r.x;
+  if (n < 2 || n > kWarpSortCap) return;
+  warp_sort_tile(pairs + r.x, n, s_scratch[warp], s_counts[warp]);
+}
+
+// Tiles of (kWarpSortCap, kMidSortCap] pairs: one CTA per tile, in shared memory.
+struct MidSmem {
+  uint32_t key[2][kMidSortCap];
+  uint32_t val[2][kMidSortCap];
+  TileSortSmem t;
+};
+
+__global__ void __launch_bounds__(kTileThreads) k_sort_mid(const uint2* __restrict__ ranges,
+                                                           const uint32_t* __restrict__ mid_list,
+                                                           uint64_t* __restrict__ pairs, const DevState* st) {
+  extern __shared__ __align__(16) unsigned char s_raw[];
+  MidSmem& sm = *reinterpret_cast<MidSmem*>(s_raw);
+  const uint32_t nmid = *(const volatile uint32_t*)&st->mid_tiles;
+  for (uint32_t li = blockIdx.x; li < nmid; li += gridDim.x) {
+    const uint2 r = ranges[mid_list[li]];
+    const uint32_t n = r.y - r.x;
+    for (uint32_t e = threadIdx.x; e < n; e += kTileThreads) {
+      const uint64_t w = pairs[r.x + e];
+      sm.key[0][e] = (uint32_t)(w >> 32);
+      sm.val[0][e] = (uint32_t)w;
+    }
+    __syncthreads();
+    const int fin = smem_sort<kMidSortCap>(sm.key, sm.val, n, sm.t);
+    for (uint32_t e = threadIdx.x; e < n; e += kTileThreads)
+      pairs[r.x + e] = ((uint64_t)sm.key[fin][e] << 32) | sm.val[fin][e];
+    __syncthreads();
+  }
+}
+
+// Sorts the pairs of each tile longer than kMidSortCap, in
 // global memory (the pair buffer and the second pair buffer as ping-pong),
 // one CTA per tile: each pass of the tile sort runs over chunks of kLongChunk
 // words staged through shared memory, digit starts carried across chunks.
@@ -299,8 +354,9 @@ __global__ void __launch_bounds__(kTileThreads) k_sort_long(const uint2* __restr
 uint32_t bin_rows(int num_sms) { return 2u * (uint32_t)num_sms; }
 
 cudaError_t launch_binning(const FrameParams& fp, const BinInfo* bin, uint64_t n, uint32_t* counts, uint32_t* totals,
-                           uint2* ranges, uint32_t* long_list, uint64_t* pairs, uint64_t* pairs_alt, uint64_t cap,
-                           DevState* st, int num_sms, size_t max_smem, cudaStream_t stream) {
+                           uint2* ranges, uint32_t* mid_list, uint32_t* long_list, uint64_t* pairs,
+                           uint64_t* pairs_alt, uint64_t cap, DevState* st, int num_sms, size_t max_smem,
+                           cudaStream_t stream) {
   const uint32_t tiles = fp.tiles_x * fp.tiles_y;
   const uint32_t rows = bin_rows(num_sms);
   const uint64_t per_cta = n ? (n + rows - 1) / rows : 1;
@@ -316,11 +372,11 @@ cudaError_t launch_binning(const FrameParams& fp, const BinInfo* bin, uint64_t n
       if ((e = cudaMemsetAsync(counts, 0, (size_t)rows * tiles * sizeof(uint32_t), stream))) return e;
       k_bin_count<false><<<rows, kBinThreads, 0, stream>>>(bin, n, per_cta, fp.tiles_x, tiles, counts);
     }
-    k_bin_colscan<<<(tiles + 255) / 256, 256, 0, stream>>>(counts, rows, tiles, totals);
+    k_bin_colscan<<<(tiles + 31) / 32, 256, 0, stream>>>(counts, rows, tiles, totals);
   } else {
     if ((e = cudaMemsetAsync(totals, 0, (size_t)tiles * sizeof(uint32_t), stream))) return e;
   }
-  k_bin_tilescan<<<1, 1024, 0, stream>>>(totals, tiles, cap, ranges, kBlendSortCap, long_list, st);
+  k_bin_tilescan<<<1, 1024, 0, stream>>>(totals, tiles, cap, ranges, mid_list, long_list, st);
   if (n) {
     if (use_smem) {
       if ((e = cudaFuncSetAttribute(k_bin_scatter<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
@@ -331,6 +387,10 @@ cudaError_t launch_binning(const FrameParams& fp, const BinInfo* bin, uint64_t n
       k_bin_scatter<false><<<rows, kBinThreads, 0, stream>>>(bin, n, per_cta, fp.tiles_x, tiles, counts, ranges,
                                                              pairs, cap);
     }
+    k_sort_small<<<(tiles + 7) / 8, 256, 0, stream>>>(ranges, tiles, pairs);
+    const int mid_smem = (int)sizeof(MidSmem);
+    if ((e = cudaFuncSetAttribute(k_sort_mid, cudaFuncAttributeMaxDynamicSharedMemorySize, mid_smem))) return e;
+    k_sort_mid<<<num_sms * 3, kTileThreads, mid_smem, stream>>>(ranges, mid_list, pairs, st);
     k_sort_long<<<num_sms, kTileThreads, 0, stream>>>(ranges, long_list, pairs, pairs_alt, cap, st);
   }
   return cudaGetLastError();

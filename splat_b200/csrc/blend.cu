@@ -1,10 +1,8 @@
-// Kernel (d): per-tile depth sort and front-to-back blend with the terminal
-// box-filter downsample fused in.
+// Kernel (d): per-tile front-to-back blend with the terminal box-filter
+// downsample fused in.
 //
-// One CTA per 16x16 tile, one pixel per thread. The CTA first sorts its
-// tile's pairs by depth in shared memory (tilesort.cuh; tiles longer than
-// kBlendSortCap arrive sorted by k_sort_long), as the reference's per-tile
-// sort runs fused with its blend (src/render/cpu.rs:202-214); each warp covers an 8x4 block
+// One CTA per 16x16 tile, one pixel per thread, over the tile's pairs in
+// depth order (sorted per tile by the binning stage); each warp covers an 8x4 block
 // of the tile so a splat whose pixel bbox misses the block is skipped by the
 // whole warp. The tile's depth-sorted splat list is walked in batches of 256:
 // the CTA gathers the batch's 48-byte records into shared memory (one per
@@ -29,7 +27,6 @@
 // (src/term.rs:74-99); other factors go through a full-resolution scratch
 // frame and k_downsample.
 #include "common.cuh"
-#include "tilesort.cuh"
 
 namespace splat {
 namespace {
@@ -119,10 +116,8 @@ __device__ __forceinline__ void accumulate(float alpha, const float4& b, float b
 
 template <bool EXACT>
 __global__ void __launch_bounds__(256) k_blend(FrameParams fp, const Record* __restrict__ rec,
-                                               uint64_t* __restrict__ pairs, const uint2* __restrict__ ranges,
-                                               bool writeback, uint8_t* __restrict__ out, uint8_t* __restrict__ full) {
-  // Shared memory: the tile sort's key and value buffers (ping-pong); once
-  // the tile is sorted the key buffers hold the batch staging instead.
+                                               const uint64_t* __restrict__ pairs, const uint2* __restrict__ ranges,
+                                               uint8_t* __restrict__ out, uint8_t* __restrict__ full) {
   // Per batch entry: the splat's pixel bbox clipped to this tile as a bit
   // mask (columns in bits 0-15, rows in bits 16-31), its geometry and colour.
   // The default path stores the centre relative to the tile's first pixel
@@ -130,16 +125,12 @@ __global__ void __launch_bounds__(256) k_blend(FrameParams fp, const Record* __r
   // the entries whose bbox meets its 8x4 block and walks only those, two at a
   // time (the second splat's alpha is computed while the first one's is being
   // accumulated).
-  __shared__ __align__(16) uint32_t s_keys[2][kBlendSortCap];
-  __shared__ __align__(16) uint32_t s_vals[2][kBlendSortCap];
-  __shared__ TileSortSmem s_ts;
+  __shared__ float4 s_a[256];  // x, y, -a/2, -b
+  __shared__ float4 s_b[256];  // -c/2, opacity, red, green
+  __shared__ uint32_t s_mask[256];
+  __shared__ float s_c[256];  // blue
+  __shared__ uint8_t s_list[8][256];
   __shared__ uint32_t s_px[256];
-  float4* s_a = reinterpret_cast<float4*>(&s_keys[0][0]);      // 256 x 16 B: x, y, -a/2, -b
-  float4* s_b = s_a + 256;                                      // -c/2, opacity, red, green
-  uint32_t* s_mask = reinterpret_cast<uint32_t*>(s_b + 256);    // 256 x 4 B
-  float* s_c = reinterpret_cast<float*>(s_mask + 256);          // blue
-  uint8_t (*s_list)[256] = reinterpret_cast<uint8_t (*)[256]>(s_c + 256);  // 8 x 256 B
-  static_assert(sizeof(s_keys) >= 256 * (16 + 16 + 4 + 4) + 8 * 256, "batch staging must fit the key buffers");
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const uint32_t tile = blockIdx.x;
@@ -153,24 +144,7 @@ __global__ void __launch_bounds__(256) k_blend(FrameParams fp, const Record* __r
   const uint32_t wxbits = 0xFFu << wx, wybits = 0xFu << (16 + wy);
   const uint2 range = ranges[tile];
   const uint32_t begin = range.x, n = range.y > range.x ? range.y - range.x : 0u;
-
-  // Depth order of the tile's splats (radix::sort_hi32 + fix_ties).
-  const bool in_smem = n <= kBlendSortCap;
-  int fin = 0;
-  if (n && in_smem) {
-    for (uint32_t e = tid; e < n; e += 256) {
-      const uint64_t w = pairs[begin + e];
-      s_keys[0][e] = (uint32_t)(w >> 32);
-      s_vals[0][e] = (uint32_t)w;
-    }
-    __syncthreads();
-    fin = smem_sort<kBlendSortCap>(s_keys, s_vals, n, s_ts);
-    if (writeback)
-      for (uint32_t e = tid; e < n; e += 256) pairs[begin + e] = ((uint64_t)s_keys[fin][e] << 32) | s_vals[fin][e];
-    __syncthreads();
-  }
-  const uint32_t* sorted = s_vals[fin];
-  auto splat_at = [&](uint32_t p) -> uint32_t { return in_smem ? sorted[p] : (uint32_t)pairs[begin + p]; };
+  auto splat_at = [&](uint32_t p) -> uint32_t { return (uint32_t)pairs[begin + p]; };
 
   // EXACT: dx = lane + ((g*4) + ((ox + 0.5) - x)), dy = ((oy + ly) + 0.5) - y
   // in the reference's association (src/render/cpu.rs:658-671).
@@ -335,14 +309,14 @@ __global__ void k_downsample(FrameParams fp, const uint8_t* __restrict__ full, u
 
 }  // namespace
 
-cudaError_t launch_blend(const FrameParams& fp, const Record* rec, uint64_t* pairs, const uint2* ranges, bool exact,
-                         bool writeback, uint8_t* out, uint8_t* full_scratch, cudaStream_t stream) {
+cudaError_t launch_blend(const FrameParams& fp, const Record* rec, const uint64_t* pairs, const uint2* ranges,
+                         bool exact, uint8_t* out, uint8_t* full_scratch, cudaStream_t stream) {
   const unsigned tiles = fp.tiles_x * fp.tiles_y;
   if (tiles == 0) return cudaSuccess;
   if (exact)
-    k_blend<true><<<tiles, 256, 0, stream>>>(fp, rec, pairs, ranges, writeback, out, full_scratch);
+    k_blend<true><<<tiles, 256, 0, stream>>>(fp, rec, pairs, ranges, out, full_scratch);
   else
-    k_blend<false><<<tiles, 256, 0, stream>>>(fp, rec, pairs, ranges, writeback, out, full_scratch);
+    k_blend<false><<<tiles, 256, 0, stream>>>(fp, rec, pairs, ranges, out, full_scratch);
   if (fp.downsample > 1 && kTile % fp.downsample != 0 && fp.out_w > 0 && fp.out_h > 0) {
     dim3 grid((fp.out_w + 127) / 128, fp.out_h);
     k_downsample<<<grid, 128, 0, stream>>>(fp, full_scratch, out);

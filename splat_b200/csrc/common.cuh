@@ -61,17 +61,19 @@ struct __align__(16) BinInfo {
   uint32_t rect_lo, rect_hi, depth_bits, count;
 };
 
-// Pairs a blend CTA sorts in shared memory; longer tiles are sorted by
-// k_sort_long before the blend.
-constexpr uint32_t kBlendSortCap = 2048;
+// Per-tile depth sort sizes: tiles up to kWarpSortCap pairs are sorted by one
+// warp, up to kMidSortCap by one CTA in shared memory, longer ones in chunks.
+constexpr uint32_t kWarpSortCap = 512;
+constexpr uint32_t kMidSortCap = 4096;
 
 // Frame state in device memory, cleared at the start of every frame.
 struct DevState {
   unsigned long long visible;      // splats that survived culling
   unsigned long long total_pairs;  // (splat, tile) pairs, may exceed the capacity
   unsigned int error;
-  unsigned int long_tiles;         // tiles with more than kBlendSortCap pairs
-  unsigned int pad[2];
+  unsigned int mid_tiles;          // tiles with (kWarpSortCap, kMidSortCap] pairs
+  unsigned int long_tiles;         // tiles with more than kMidSortCap pairs
+  unsigned int pad;
 };
 
 // Launchers (each returns the cudaGetLastError of its launches).
@@ -79,14 +81,14 @@ struct DevState {
 cudaError_t launch_project(const FrameParams& fp, const SceneDev& s, Record* rec, BinInfo* bin, float* dbg_proj,
                            float* dbg_color, DevState* st, cudaStream_t stream);
 // (b) binning into per-tile buckets (count matrix of bin_rows() x tiles,
-// tile totals, ranges, the long-tile list) and the sort of long tiles.
+// tile totals, ranges, mid/long tile lists) and (c) the per-tile depth sorts.
 uint32_t bin_rows(int num_sms);
 cudaError_t launch_binning(const FrameParams& fp, const BinInfo* bin, uint64_t n, uint32_t* counts, uint32_t* totals,
-                           uint2* ranges, uint32_t* long_list, uint64_t* pairs, uint64_t* pairs_alt, uint64_t cap,
-                           DevState* st, int num_sms, size_t max_smem, cudaStream_t stream);
-// (d) per-tile depth sort + blend + downsample. writeback: store each tile's
-// sorted pairs back into `pairs` (for the debug dump).
-cudaError_t launch_blend(const FrameParams& fp, const Record* rec, uint64_t* pairs, const uint2* ranges, bool exact,
-                         bool writeback, uint8_t* out, uint8_t* full_scratch, cudaStream_t stream);
+                           uint2* ranges, uint32_t* mid_list, uint32_t* long_list, uint64_t* pairs,
+                           uint64_t* pairs_alt, uint64_t cap, DevState* st, int num_sms, size_t max_smem,
+                           cudaStream_t stream);
+// (d) blend + downsample over the depth-sorted buckets.
+cudaError_t launch_blend(const FrameParams& fp, const Record* rec, const uint64_t* pairs, const uint2* ranges,
+                         bool exact, uint8_t* out, uint8_t* full_scratch, cudaStream_t stream);
 
 }  // namespace splat

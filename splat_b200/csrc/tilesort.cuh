@@ -176,4 +176,122 @@ __device__ int smem_sort(uint32_t (*key)[kCap], uint32_t (*val)[kCap], uint32_t 
   return cur;
 }
 
+// Warp-level sort of one tile's n <= kWarpSortCap words (depth bits << 32 |
+// splat index) in place in global memory: the elements live in registers,
+// warp-striped (element j*32 + lane), each pass ranks them stably with
+// ballots, places them in `scratch` (kWarpSortCap words of shared memory) and
+// reads them back striped; fix_ties runs on the final scratch copy.
+__device__ __forceinline__ void warp_sort_tile(uint64_t* __restrict__ words, uint32_t n, uint64_t* scratch,
+                                               uint32_t* counts) {
+  constexpr int kM = kWarpSortCap / 32;
+  const int lane = threadIdx.x & 31;
+  const uint32_t lt = (1u << lane) - 1u;
+  uint64_t w[kM];
+  uint32_t a = 0xFFFFFFFFu, o = 0u;
+#pragma unroll
+  for (int j = 0; j < kM; j++) {
+    const uint32_t e = (uint32_t)j * 32 + lane;
+    w[j] = e < n ? words[e] : ~0ull;
+    if (e < n) {
+      a &= (uint32_t)(w[j] >> 32);
+      o |= (uint32_t)(w[j] >> 32);
+    }
+  }
+#pragma unroll
+  for (int s = 16; s > 0; s >>= 1) {
+    a &= __shfl_xor_sync(0xffffffffu, a, s);
+    o |= __shfl_xor_sync(0xffffffffu, o, s);
+  }
+  const uint32_t vary = a ^ o;
+  const int m = (int)((n + 31) / 32);
+  for (int d = 0; d < 4; d++) {
+    const int shift = 32 + 8 * d;
+    if (((vary >> (8 * d)) & 255u) == 0u) continue;
+#pragma unroll
+    for (int b = 0; b < 8; b++) counts[b * 32 + lane] = 0u;
+    __syncwarp();
+    uint32_t dr[kM];
+#pragma unroll
+    for (int j = 0; j < kM; j++) {
+      if (j < m) {
+        const uint32_t e = (uint32_t)j * 32 + lane;
+        const bool valid = e < n;
+        const uint32_t dig = (uint32_t)(w[j] >> shift) & 255u;
+        uint32_t peers = __ballot_sync(0xffffffffu, valid);
+#pragma unroll
+        for (int b = 0; b < 8; b++) {
+          const bool bit = (dig >> b) & 1u;
+          const uint32_t bal = __ballot_sync(0xffffffffu, bit);
+          peers &= bit ? bal : ~bal;
+        }
+        const uint32_t cnt = valid ? counts[dig] : 0u;
+        __syncwarp();
+        dr[j] = 0xFFFFFFFFu;
+        if (valid) {
+          dr[j] = ((cnt + __popc(peers & lt)) << 8) | dig;
+          if (lane == 31 - __clz(peers)) counts[dig] = cnt + __popc(peers);
+        }
+        __syncwarp();
+      }
+    }
+    // Exclusive scan of the 256 digit counts (8 per lane, then across lanes).
+    uint32_t c[8], sum = 0;
+#pragma unroll
+    for (int b = 0; b < 8; b++) {
+      c[b] = counts[lane * 8 + b];
+      sum += c[b];
+    }
+    uint32_t x = sum;
+#pragma unroll
+    for (int s = 1; s < 32; s <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, x, s);
+      if (lane >= s) x += y;
+    }
+    uint32_t run = x - sum;
+    __syncwarp();
+#pragma unroll
+    for (int b = 0; b < 8; b++) {
+      counts[lane * 8 + b] = run;
+      run += c[b];
+    }
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < kM; j++)
+      if (j < m && dr[j] != 0xFFFFFFFFu) scratch[counts[dr[j] & 255u] + (dr[j] >> 8)] = w[j];
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < kM; j++) {
+      const uint32_t e = (uint32_t)j * 32 + lane;
+      if (e < n) w[j] = scratch[e];
+    }
+    __syncwarp();
+  }
+#pragma unroll
+  for (int j = 0; j < kM; j++) {
+    const uint32_t e = (uint32_t)j * 32 + lane;
+    if (e < n) scratch[e] = w[j];
+  }
+  __syncwarp();
+  // fix_ties: runs of equal depth ordered by splat index.
+  for (uint32_t e = lane + 1; e < n; e += 32) {
+    const uint32_t kk = (uint32_t)(scratch[e] >> 32);
+    if (kk == (uint32_t)(scratch[e - 1] >> 32) && (e == 1 || (uint32_t)(scratch[e - 2] >> 32) != kk)) {
+      uint32_t r1 = e + 1;
+      while (r1 < n && (uint32_t)(scratch[r1] >> 32) == kk) r1++;
+      for (uint32_t i = e; i < r1; i++) {
+        const uint64_t v = scratch[i];
+        uint32_t j = i;
+        while (j > e - 1 && (uint32_t)scratch[j - 1] > (uint32_t)v) {
+          scratch[j] = scratch[j - 1];
+          j--;
+        }
+        scratch[j] = v;
+      }
+    }
+  }
+  __syncwarp();
+  for (uint32_t e = lane; e < n; e += 32) words[e] = scratch[e];
+  __syncwarp();
+}
+
 }  // namespace splat
