@@ -202,7 +202,7 @@ __global__ void __launch_bounds__(kBinThreads) k_bin_scatter(const BinInfo* __re
 }
 
 // Tiles of at most kWarpSortCap pairs: one warp per tile.
-__global__ void __launch_bounds__(256) k_sort_small(const uint2* __restrict__ ranges, uint32_t tiles,
+__global__ void __launch_bounds__(256, 3) k_sort_small(const uint2* __restrict__ ranges, uint32_t tiles,
                                                     uint64_t* __restrict__ pairs) {
   __shared__ uint64_t s_scratch[8][kWarpSortCap];
   __shared__ uint32_t s_counts[8][256];
@@ -217,8 +217,8 @@ __global__ void __launch_bounds__(256) k_sort_small(const uint2* __restrict__ ra
 
 // Tiles of (kWarpSortCap, kMidSortCap] pairs: one CTA per tile, in shared memory.
 struct MidSmem {
+  uint64_t words[kMidSortCap];
   uint32_t key[2][kMidSortCap];
-  uint32_t val[2][kMidSortCap];
   TileSortSmem t;
 };
 
@@ -231,15 +231,10 @@ __global__ void __launch_bounds__(kTileThreads) k_sort_mid(const uint2* __restri
   for (uint32_t li = blockIdx.x; li < nmid; li += gridDim.x) {
     const uint2 r = ranges[mid_list[li]];
     const uint32_t n = r.y - r.x;
-    for (uint32_t e = threadIdx.x; e < n; e += kTileThreads) {
-      const uint64_t w = pairs[r.x + e];
-      sm.key[0][e] = (uint32_t)(w >> 32);
-      sm.val[0][e] = (uint32_t)w;
-    }
+    for (uint32_t e = threadIdx.x; e < n; e += kTileThreads) sm.words[e] = pairs[r.x + e];
     __syncthreads();
-    const int fin = smem_sort<kMidSortCap>(sm.key, sm.val, n, sm.t);
-    for (uint32_t e = threadIdx.x; e < n; e += kTileThreads)
-      pairs[r.x + e] = ((uint64_t)sm.key[fin][e] << 32) | sm.val[fin][e];
+    const int fin = smem_sort<kMidSortCap>(sm.key, sm.words, n, sm.t);
+    for (uint32_t e = threadIdx.x; e < n; e += kTileThreads) pairs[r.x + e] = sm.words[sm.key[fin][e] & 0xFFFFu];
     __syncthreads();
   }
 }

@@ -1,14 +1,14 @@
 // Per-tile depth sort: the reference's per-tile radix::sort_hi32 followed by
-// fix_ties (src/render/cpu.rs:208-210, radix.rs:13-57, cpu.rs:396-414),
-// run by one CTA of kTileThreads threads.
+// fix_ties (src/render/cpu.rs:208-210, radix.rs:13-57, cpu.rs:396-414), by
+// one warp (short tiles) or one CTA of kTileThreads threads.
 //
 // A tile's pairs arrive in arbitrary order (they are bucketed with shared-
-// memory atomics). Each pair is the word depth bits << 32 | splat index; the
-// key is the depth bits (a positive float's bit pattern orders like the
-// float). A stable LSD radix sort over the 8-bit digits that are not shared by
-// every key of the tile orders the pairs by depth; runs of equal depth are
-// then ordered by splat index, which makes the result independent of the
-// bucketing order: exactly the reference's (depth, scene index) order.
+// memory atomics). Each pair is the word depth bits << 32 | splat index. A
+// stable LSD radix sort on a 16-bit monotone quantisation of the depth (two
+// 8-bit passes) orders the pairs up to runs of equal quantised depth; each
+// run is then ordered by the full word, i.e. by depth and, within equal
+// depth, by splat index. The result is independent of the bucketing order:
+// exactly the reference's (depth, scene index) order.
 //
 // Ranking is stable per pass: each warp ranks a contiguous segment of the
 // elements 32 at a time (lanes with equal digits found by ballots over the
@@ -54,36 +54,88 @@ __device__ __forceinline__ void block_and_or(uint32_t a, uint32_t o, TileSortSme
   __syncthreads();
 }
 
-// Stable ranks of up to 32 * kChunks elements per warp (a contiguous segment
-// [seg0, seg1) of key[]), digit at `shift`. Fills sm.wh with per-warp counts,
-// returns per-chunk (rank << 8 | digit) in dr[] (0xFFFFFFFF past the end).
+// Sort key of a pair: its depth quantised to 16 bits over the tile's depth
+// range, q = min(65535, (d - dmin) * (65535 / (dmax - dmin))), truncated.
+// Every step is monotone (IEEE subtraction, multiplication by a positive
+// factor, truncation), so d1 <= d2 implies q1 <= q2: a stable sort on q
+// followed by ordering each run of equal q by the full word (depth bits,
+// splat index) gives exactly the (depth, scene index) order.
+struct DepthQuant {
+  float dmin, scale;
+  __device__ __forceinline__ uint32_t operator()(uint64_t word) const {
+    const float d = __uint_as_float((uint32_t)(word >> 32));
+    const float q = (d - dmin) * scale;
+    return q >= 65535.0f ? 65535u : (uint32_t)q;  // d >= dmin, so q >= 0
+  }
+};
+
+__device__ __forceinline__ DepthQuant make_quant(uint32_t min_bits, uint32_t max_bits) {
+  const float dmin = __uint_as_float(min_bits), dmax = __uint_as_float(max_bits);
+  const float range = dmax - dmin;
+  return DepthQuant{dmin, range > 0.0f ? 65535.0f / range : 0.0f};
+}
+
+// Orders each run of items with equal quantised key by their full word
+// (insertion sort by the run's first thread; runs are short except for
+// degenerate depth distributions). q(item) gives the quantised key, w(item)
+// the 64-bit word (depth bits, splat index) the run is ordered by.
+template <class Item, class Q, class W>
+__device__ __forceinline__ void sort_runs(Item* items, uint32_t n, uint32_t tid, uint32_t nthreads, Q&& q, W&& w) {
+  for (uint32_t e = tid + 1; e < n; e += nthreads) {
+    const uint32_t qq = q(items[e]);
+    if (qq == q(items[e - 1]) && (e == 1 || q(items[e - 2]) != qq)) {
+      uint32_t r1 = e + 1;
+      while (r1 < n && q(items[r1]) == qq) r1++;
+      for (uint32_t i = e; i < r1; i++) {
+        const Item x = items[i];
+        const uint64_t wx = w(x);
+        uint32_t j = i;
+        while (j > e - 1 && w(items[j - 1]) > wx) {
+          items[j] = items[j - 1];
+          j--;
+        }
+        items[j] = x;
+      }
+    }
+  }
+}
+
+// Stable ranks of the elements key[seg0, seg1) of one warp, 32 at a time,
+// digit at `shift` (lanes holding the same digit found by ballots over its
+// bits). Fills sm.wh[warp] with the warp's digit counts and returns per chunk
+// (rank << 8 | digit) in dr[] (0xFFFFFFFF past the end); only the chunks that
+// hold elements are ranked.
 template <int kChunks>
 __device__ __forceinline__ void warp_rank(const uint32_t* key, uint32_t seg0, uint32_t seg1, int shift,
                                           TileSortSmem& sm, uint32_t (&k)[kChunks], uint32_t (&dr)[kChunks]) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t lt = (1u << lane) - 1u;
+  const uint32_t nch = (seg1 - seg0 + 31) / 32;
 #pragma unroll
   for (int c = 0; c < kChunks; c++) {
-    const uint32_t e = seg0 + (uint32_t)c * 32 + lane;
-    const bool valid = e < seg1;
-    k[c] = valid ? key[e] : 0u;
-    const uint32_t dig = (k[c] >> shift) & 255u;
-    uint32_t peers = __ballot_sync(0xffffffffu, valid);
-#pragma unroll
-    for (int b = 0; b < 8; b++) {
-      const bool bit = (dig >> b) & 1u;
-      const uint32_t bal = __ballot_sync(0xffffffffu, bit);
-      peers &= bit ? bal : ~bal;
-    }
-    uint32_t cnt = 0;
-    if (valid) cnt = sm.wh[warp][dig];
-    __syncwarp();
     dr[c] = 0xFFFFFFFFu;
-    if (valid) {
-      dr[c] = ((cnt + __popc(peers & lt)) << 8) | dig;
-      if (lane == 31 - __clz(peers)) sm.wh[warp][dig] = cnt + __popc(peers);
+    k[c] = 0u;
+    if ((uint32_t)c < nch) {
+      const uint32_t e = seg0 + (uint32_t)c * 32 + lane;
+      const bool valid = e < seg1;
+      k[c] = valid ? key[e] : 0u;
+      const uint32_t dig = (k[c] >> shift) & 255u;
+      uint32_t peers = __ballot_sync(0xffffffffu, valid);
+#pragma unroll
+      for (int b = 0; b < 8; b++) {
+        const bool bit = (dig >> b) & 1u;
+        const uint32_t bal = __ballot_sync(0xffffffffu, bit);
+        peers &= bit ? bal : ~bal;
+      }
+      uint32_t cnt = 0;
+      if (valid) cnt = sm.wh[warp][dig];
+      __syncwarp();
+      if (valid) {
+        dr[c] = ((cnt + __popc(peers & lt)) << 8) | dig;
+        if (lane == 31 - __clz(peers)) sm.wh[warp][dig] = cnt + __popc(peers);
+      }
+      __syncwarp();
     }
-    __syncwarp();
   }
 }
 
@@ -116,24 +168,58 @@ __device__ __forceinline__ void clear_counts(TileSortSmem& sm) {
   for (int w = 0; w < kTileWarps; w++) sm.wh[w][threadIdx.x] = 0u;
 }
 
-// In-shared-memory sort of n <= kCap (key, value) pairs held in key[0]/val[0];
-// returns the buffer index (0/1) holding the result.
+// CTA sort of one tile's n <= kCap words in shared memory: key[0][e] =
+// quantised depth << 16 | e (e the word's slot in words[]); two passes on the
+// quantised depth (digits at bits 16 and 24), then runs of equal quantised
+// depth ordered by word. Returns the key buffer holding the order; its low 16
+// bits index words[].
 template <int kCap>
-__device__ int smem_sort(uint32_t (*key)[kCap], uint32_t (*val)[kCap], uint32_t n, TileSortSmem& sm) {
+__device__ int smem_sort(uint32_t (*key)[kCap], const uint64_t* words, uint32_t n, TileSortSmem& sm) {
+  static_assert(kCap <= 65536, "slots are 16-bit");
   constexpr int kChunks = kCap / (32 * kTileWarps);
-  uint32_t a = 0xFFFFFFFFu, o = 0u;
+  uint32_t a = 0xFFFFFFFFu, o = 0u, mn = 0xFFFFFFFFu, mx = 0u;
   for (uint32_t e = threadIdx.x; e < n; e += kTileThreads) {
-    a &= key[0][e];
-    o |= key[0][e];
+    const uint32_t b = (uint32_t)(words[e] >> 32);
+    mn = min(mn, b);
+    mx = max(mx, b);
+  }
+  // block min / max of the depth bits (positive floats order like their bits)
+  {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int s2 = 16; s2 > 0; s2 >>= 1) {
+      mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, s2));
+      mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, s2));
+    }
+    if (lane == 0) {
+      sm.red[0][warp] = mn;
+      sm.red[1][warp] = mx;
+    }
+    __syncthreads();
+    mn = 0xFFFFFFFFu;
+    mx = 0u;
+#pragma unroll
+    for (int w = 0; w < kTileWarps; w++) {
+      mn = min(mn, sm.red[0][w]);
+      mx = max(mx, sm.red[1][w]);
+    }
+    __syncthreads();
+  }
+  const DepthQuant quant = make_quant(mn, mx);
+  for (uint32_t e = threadIdx.x; e < n; e += kTileThreads) {
+    const uint32_t k2 = (quant(words[e]) << 16) | e;
+    key[0][e] = k2;
+    a &= k2;
+    o |= k2;
   }
   uint32_t and_all, or_all;
   block_and_or(a, o, sm, and_all, or_all);
   const uint32_t vary = and_all ^ or_all;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
   const uint32_t seg = (n + kTileWarps - 1) / kTileWarps;
   const uint32_t seg0 = min(n, (uint32_t)warp * seg), seg1 = min(n, seg0 + seg);
   int cur = 0;
-  for (int d = 0; d < 4; d++) {
+  for (int d = 2; d < 4; d++) {
     const int shift = 8 * d;
     if (((vary >> shift) & 255u) == 0u) continue;
     clear_counts(sm);
@@ -143,80 +229,78 @@ __device__ int smem_sort(uint32_t (*key)[kCap], uint32_t (*val)[kCap], uint32_t 
     __syncthreads();
     digit_offsets(sm);
 #pragma unroll
-    for (int c = 0; c < kChunks; c++) {
-      if (dr[c] != 0xFFFFFFFFu) {
-        const uint32_t dig = dr[c] & 255u;
-        const uint32_t pos = sm.dstart[dig] + sm.wh[warp][dig] + (dr[c] >> 8);
-        key[cur ^ 1][pos] = k[c];
-        val[cur ^ 1][pos] = val[cur][seg0 + (uint32_t)c * 32 + lane];
-      }
-    }
+    for (int c = 0; c < kChunks; c++)
+      if (dr[c] != 0xFFFFFFFFu) key[cur ^ 1][sm.dstart[dr[c] & 255u] + sm.wh[warp][dr[c] & 255u] + (dr[c] >> 8)] = k[c];
     __syncthreads();
     cur ^= 1;
   }
-  // fix_ties: within runs of equal depth, order by splat index.
-  for (uint32_t e = threadIdx.x + 1; e < n; e += kTileThreads) {
-    const uint32_t kk = key[cur][e];
-    if (kk == key[cur][e - 1] && (e == 1 || key[cur][e - 2] != kk)) {
-      uint32_t r1 = e + 1;
-      while (r1 < n && key[cur][r1] == kk) r1++;
-      uint32_t* v = val[cur];
-      for (uint32_t i = e; i < r1; i++) {  // insertion sort of v[e-1, r1)
-        const uint32_t x = v[i];
-        uint32_t j = i;
-        while (j > e - 1 && v[j - 1] > x) {
-          v[j] = v[j - 1];
-          j--;
-        }
-        v[j] = x;
-      }
-    }
-  }
+  // Runs of equal quantised depth, ordered by the full word: sort the slots.
+  sort_runs(
+      key[cur], n, threadIdx.x, kTileThreads, [](uint32_t k2) { return k2 >> 16; },
+      [&](uint32_t k2) { return words[k2 & 0xFFFFu]; });
   __syncthreads();
   return cur;
 }
 
-// Warp-level sort of one tile's n <= kWarpSortCap words (depth bits << 32 |
-// splat index) in place in global memory: the elements live in registers,
-// warp-striped (element j*32 + lane), each pass ranks them stably with
-// ballots, places them in `scratch` (kWarpSortCap words of shared memory) and
-// reads them back striped; fix_ties runs on the final scratch copy.
+// Warp sort of one tile's n <= kWarpSortCap words in place in global memory.
+// The words live in registers, warp-striped (element j*32 + lane); each of
+// the two passes on the quantised depth ranks them stably with ballots,
+// places them in `scratch` (kWarpSortCap words of shared memory) and reads
+// them back striped; runs of equal quantised depth are then ordered by word.
 __device__ __forceinline__ void warp_sort_tile(uint64_t* __restrict__ words, uint32_t n, uint64_t* scratch,
                                                uint32_t* counts) {
   constexpr int kM = kWarpSortCap / 32;
   const int lane = threadIdx.x & 31;
   const uint32_t lt = (1u << lane) - 1u;
+  const int m = (int)((n + 31) / 32);
   uint64_t w[kM];
+  uint32_t mn = 0xFFFFFFFFu, mx = 0u;
+#pragma unroll
+  for (int j = 0; j < kM; j++) {
+    const uint32_t e = (uint32_t)j * 32 + lane;
+    w[j] = 0ull;
+    if (j < m && e < n) {
+      w[j] = words[e];
+      mn = min(mn, (uint32_t)(w[j] >> 32));
+      mx = max(mx, (uint32_t)(w[j] >> 32));
+    }
+  }
+#pragma unroll
+  for (int s2 = 16; s2 > 0; s2 >>= 1) {
+    mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, s2));
+    mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, s2));
+  }
+  const DepthQuant quant = make_quant(mn, mx);
   uint32_t a = 0xFFFFFFFFu, o = 0u;
 #pragma unroll
   for (int j = 0; j < kM; j++) {
     const uint32_t e = (uint32_t)j * 32 + lane;
-    w[j] = e < n ? words[e] : ~0ull;
-    if (e < n) {
-      a &= (uint32_t)(w[j] >> 32);
-      o |= (uint32_t)(w[j] >> 32);
+    if (j < m && e < n) {
+      const uint32_t q = quant(w[j]);
+      a &= q;
+      o |= q;
     }
   }
 #pragma unroll
-  for (int s = 16; s > 0; s >>= 1) {
-    a &= __shfl_xor_sync(0xffffffffu, a, s);
-    o |= __shfl_xor_sync(0xffffffffu, o, s);
+  for (int s2 = 16; s2 > 0; s2 >>= 1) {
+    a &= __shfl_xor_sync(0xffffffffu, a, s2);
+    o |= __shfl_xor_sync(0xffffffffu, o, s2);
   }
   const uint32_t vary = a ^ o;
-  const int m = (int)((n + 31) / 32);
-  for (int d = 0; d < 4; d++) {
-    const int shift = 32 + 8 * d;
-    if (((vary >> (8 * d)) & 255u) == 0u) continue;
+  for (int d = 0; d < 2; d++) {
+    const int shift = 8 * d;
+    if (((vary >> shift) & 255u) == 0u) continue;
 #pragma unroll
     for (int b = 0; b < 8; b++) counts[b * 32 + lane] = 0u;
     __syncwarp();
     uint32_t dr[kM];
 #pragma unroll
     for (int j = 0; j < kM; j++) {
+      dr[j] = 0xFFFFFFFFu;
       if (j < m) {
         const uint32_t e = (uint32_t)j * 32 + lane;
         const bool valid = e < n;
-        const uint32_t dig = (uint32_t)(w[j] >> shift) & 255u;
+        const uint32_t dig = (quant(w[j]) >> shift) & 255u;
         uint32_t peers = __ballot_sync(0xffffffffu, valid);
 #pragma unroll
         for (int b = 0; b < 8; b++) {
@@ -226,7 +310,6 @@ __device__ __forceinline__ void warp_sort_tile(uint64_t* __restrict__ words, uin
         }
         const uint32_t cnt = valid ? counts[dig] : 0u;
         __syncwarp();
-        dr[j] = 0xFFFFFFFFu;
         if (valid) {
           dr[j] = ((cnt + __popc(peers & lt)) << 8) | dig;
           if (lane == 31 - __clz(peers)) counts[dig] = cnt + __popc(peers);
@@ -243,9 +326,9 @@ __device__ __forceinline__ void warp_sort_tile(uint64_t* __restrict__ words, uin
     }
     uint32_t x = sum;
 #pragma unroll
-    for (int s = 1; s < 32; s <<= 1) {
-      const uint32_t y = __shfl_up_sync(0xffffffffu, x, s);
-      if (lane >= s) x += y;
+    for (int s2 = 1; s2 < 32; s2 <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, x, s2);
+      if (lane >= s2) x += y;
     }
     uint32_t run = x - sum;
     __syncwarp();
@@ -257,38 +340,23 @@ __device__ __forceinline__ void warp_sort_tile(uint64_t* __restrict__ words, uin
     __syncwarp();
 #pragma unroll
     for (int j = 0; j < kM; j++)
-      if (j < m && dr[j] != 0xFFFFFFFFu) scratch[counts[dr[j] & 255u] + (dr[j] >> 8)] = w[j];
+      if (dr[j] != 0xFFFFFFFFu) scratch[counts[dr[j] & 255u] + (dr[j] >> 8)] = w[j];
     __syncwarp();
 #pragma unroll
     for (int j = 0; j < kM; j++) {
       const uint32_t e = (uint32_t)j * 32 + lane;
-      if (e < n) w[j] = scratch[e];
+      if (j < m && e < n) w[j] = scratch[e];
     }
     __syncwarp();
   }
 #pragma unroll
   for (int j = 0; j < kM; j++) {
     const uint32_t e = (uint32_t)j * 32 + lane;
-    if (e < n) scratch[e] = w[j];
+    if (j < m && e < n) scratch[e] = w[j];
   }
   __syncwarp();
-  // fix_ties: runs of equal depth ordered by splat index.
-  for (uint32_t e = lane + 1; e < n; e += 32) {
-    const uint32_t kk = (uint32_t)(scratch[e] >> 32);
-    if (kk == (uint32_t)(scratch[e - 1] >> 32) && (e == 1 || (uint32_t)(scratch[e - 2] >> 32) != kk)) {
-      uint32_t r1 = e + 1;
-      while (r1 < n && (uint32_t)(scratch[r1] >> 32) == kk) r1++;
-      for (uint32_t i = e; i < r1; i++) {
-        const uint64_t v = scratch[i];
-        uint32_t j = i;
-        while (j > e - 1 && (uint32_t)scratch[j - 1] > (uint32_t)v) {
-          scratch[j] = scratch[j - 1];
-          j--;
-        }
-        scratch[j] = v;
-      }
-    }
-  }
+  sort_runs(
+      scratch, n, lane, 32, [&](uint64_t x) { return quant(x); }, [](uint64_t x) { return x; });
   __syncwarp();
   for (uint32_t e = lane; e < n; e += 32) words[e] = scratch[e];
   __syncwarp();
