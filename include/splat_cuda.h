@@ -196,6 +196,25 @@ int splat_cuda_debug_dump(splat_cuda_handle* h, float* proj, uint8_t* visible, f
                           uint32_t* values, uint64_t key_capacity, uint32_t* ranges, uint64_t range_capacity,
                           uint64_t* n_pairs);
 
+/*
+ * Sorts one tile's pairs in place, for callers that cannot allocate device
+ * memory (a host whose device memory belongs to another allocator, or code
+ * that must not allocate while it runs). No counterpart in the reference: it
+ * is the renderer's long-tile sort with its ping-pong buffer moved into a
+ * static device array, so the call allocates nothing.
+ *   words   DEVICE pointer to n words (depth bits << 32 | splat index), on the
+ *           current device; on return they are ordered by depth, equal depths
+ *           by splat index (the order the blend consumes).
+ *   n       at most 1048576 (1 << 20) words; more is rejected with
+ *           SPLAT_ERR_INVALID_ARG before anything is launched.
+ *   stream  cudaStream_t to launch on (NULL: the legacy default stream).
+ * The call only enqueues work. Every GPU that loads the library holds the
+ * 8 MiB scratch array until the process exits; all calls on a device share
+ * it, so calls whose work overlaps on the GPU race and must not be issued.
+ * The first call on each device looks the array up (cudaGetSymbolAddress);
+ * make that first call before any stream capture. No error text is kept. */
+int splat_cuda_sort_tile_noalloc(uint64_t* words, uint32_t n, void* stream);
+
 /* Frees the handle and its device memory. NULL is ignored. */
 int splat_cuda_destroy(splat_cuda_handle* h);
 

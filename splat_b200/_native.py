@@ -35,7 +35,7 @@ EXPORTS = [
     "splat_cuda_abi_version", "splat_cuda_backend_name", "splat_cuda_create", "splat_cuda_create_error",
     "splat_cuda_render", "splat_cuda_render_device", "splat_cuda_finish", "splat_cuda_set_stream",
     "splat_cuda_get_stream", "splat_cuda_set_option", "splat_cuda_get_option", "splat_cuda_debug_dump",
-    "splat_cuda_destroy", "splat_cuda_last_error",
+    "splat_cuda_destroy", "splat_cuda_last_error", "splat_cuda_sort_tile_noalloc",
 ]
 
 
@@ -92,6 +92,7 @@ def lib():
         L.splat_cuda_get_option.argtypes = [vp, u32, ctypes.POINTER(u64)]
         L.splat_cuda_debug_dump.argtypes = [vp, vp, vp, vp, vp, vp, u64, vp, u64, ctypes.POINTER(u64)]
         L.splat_cuda_destroy.argtypes = [vp]
+        L.splat_cuda_sort_tile_noalloc.argtypes = [vp, u32, vp]
         L.splat_cuda_last_error.argtypes = [vp]
         L.splat_cuda_last_error.restype = ctypes.c_char_p
         _lib = L

@@ -28,6 +28,7 @@ SOURCES = {
     "project.cu": ["--fmad=false"],
     "binning.cu": [],
     "blend.cu": [],
+    "noalloc.cu": [],
 }
 HEADERS = [os.path.join(CSRC, "common.cuh"), os.path.join(CSRC, "tilesort.cuh"),
            os.path.join(ROOT, "include", "splat_cuda.h")]
