@@ -1,9 +1,14 @@
 """Benchmark of the sm_100a splat rasterizer on the reference's headline workload.
 
-Workload: 1.2M anisotropic degree-3 SH gaussians (seeded synthetic clusters,
-fp32), rendered at 1920x1080 with 16x16 tiles over the reference bench's
-orbit (src/bench.rs:38-111: distance 12, FOV 50 deg, yaw step 2 pi / 40,
-pitch 0.4 sin(0.1 i)). A step is one frame.
+Workloads (--config):
+  plain  1.2M anisotropic degree-3 SH gaussians (seeded synthetic clusters,
+         fp32), 1920x1080, 16x16 tiles, over the reference bench's orbit
+         (src/bench.rs:38-111: distance 12, FOV 50 deg, yaw step 2 pi / 40,
+         pitch 0.4 sin(0.1 i)). The default.
+  fp16   the same scene with scales, rotations, opacities and SH stored as
+         FP16 (positions f32), 3840x2160; the per-frame error against the
+         FP64 naive rasterizer is stated for the first frames.
+A step is one frame.
 
   value  frames/s with the scene resident in HBM and the frame written to
          device memory (CUDA events on the renderer's stream, max over ranks)
@@ -34,13 +39,20 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "frames/s at 1920x1080, 1.2M SH3 splats"
-WORKLOAD = "1.2M SH-degree-3 gaussians (64 seeded clusters), 1920x1080, 16x16 tiles, 40-view orbit"
 N_SPLATS = 1_200_000
-W, H = 1920, 1080
 ORBIT = 40
-S_IN = 232  # bytes per splat read by the projection (fp32 pos, opacity, colour, cov3d, 45 SH)
 S_REC = 48  # bytes per projected-splat record
+S_BIN = 16  # bytes per splat of tile rectangle, depth bits and pair count
+CONFIGS = {
+    "plain": {"metric": "frames/s at 1920x1080, 1.2M SH3 splats", "w": 1920, "h": 1080, "precision": "fp32",
+              "s_in": 232,  # f32 position, opacity, colour, cov3d, 45 SH coefficients
+              "workload": "1.2M SH-degree-3 gaussians (64 seeded clusters), 1920x1080, 16x16 tiles, 40-view orbit"},
+    "fp16": {"metric": "frames/s at 3840x2160, 1.2M SH3 splats, FP16 storage", "w": 3840, "h": 2160,
+             "precision": "fp16",
+             "s_in": 124,  # f32 position; f16 scale, rotation, opacity, 48 SH coefficients
+             "workload": "1.2M SH-degree-3 gaussians (64 seeded clusters) stored in FP16, 3840x2160, 16x16 tiles, "
+                         "40-view orbit"},
+}
 
 
 def parse():
@@ -49,6 +61,9 @@ def parse():
     p.add_argument("--steps", type=int, default=4000)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--config", default="plain", choices=sorted(CONFIGS))
+    p.add_argument("--error-frames", type=int, default=2,
+                   help="fp16: frames whose error against the FP64 naive rasterizer is stated")
     p.add_argument("--splats", type=int, default=N_SPLATS)
     p.add_argument("--cpu-sample-s", type=float, default=15.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -114,13 +129,18 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(rows)}
 
 
-def make_workload(n):
+def make_workload(n, cfg):
+    """Scene (a Scene, or its HalfScene for the FP16 workload), the oracle's
+    f32 form of what the device holds, and the orbit views."""
     from splat_b200 import synth
 
     scene = synth.cluster_scene(n, seed=0x5EED0001, sh_degree=3)
     cam = synth.orbit_camera(scene)
     home, warm, timed = synth.orbit_views(cam, ORBIT, 5)
-    return scene, home, warm, timed
+    if cfg["precision"] == "fp16":
+        half = scene.to_fp16()
+        return half, half.decoded_scene(), scene, home, warm, timed
+    return scene, scene, scene, home, warm, timed
 
 
 def measured_peaks():
@@ -132,20 +152,20 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
-def cpu_baseline(scene, views, sample_s, threads=0):
+def cpu_baseline(scene, views, w, h, sample_s, threads=0):
     """The reference's `cpu` backend (oracle restatement), all host threads,
     over a bounded sample of the orbit."""
     from oracle import oracle as O
 
     cpu = O.CpuTiled(scene, threads=threads)
-    out = np.zeros((H, W, 3), np.uint8)
-    cpu.render(views[0], W, H, (0, 0, 0), out)  # warm-up
+    out = np.zeros((h, w, 3), np.uint8)
+    cpu.render(views[0], w, h, (0, 0, 0), out)  # warm-up
     times = []
     t_end = time.perf_counter() + sample_s
     i = 0
     while time.perf_counter() < t_end or i < 2:
         t0 = time.perf_counter()
-        cpu.render(views[i % len(views)], W, H, (0, 0, 0), out)
+        cpu.render(views[i % len(views)], w, h, (0, 0, 0), out)
         times.append(time.perf_counter() - t0)
         i += 1
     threads_used = cpu.threads
@@ -157,10 +177,12 @@ def run_reference(args):
     rank, world, _ = dist_env()
     if world > 1 and rank != 0:
         return
-    scene, home, warm, timed = make_workload(args.splats)
+    cfg = CONFIGS[args.config]
+    W, H = cfg["w"], cfg["h"]
+    _, f32_scene, _, home, warm, timed = make_workload(args.splats, cfg)
     from oracle import oracle as O
 
-    cpu = O.CpuTiled(scene, threads=0)
+    cpu = O.CpuTiled(f32_scene, threads=0)
     out = np.zeros((H, W, 3), np.uint8)
     for i in range(args.warmup):
         cpu.render(warm[i % len(warm)], W, H, (0, 0, 0), out)
@@ -178,15 +200,35 @@ def run_reference(args):
     threads = cpu.threads
     cpu.close()
     line = {
-        "impl": "reference", "metric": METRIC, "value": fps, "unit": "frames/s", "n_gpus": 0, "steps": len(times),
-        "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "splats": args.splats, "width": W, "height": H},
+        "impl": "reference", "metric": cfg["metric"], "value": fps, "unit": "frames/s", "n_gpus": 0,
+        "steps": len(times), "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": cfg["workload"], "splats": args.splats, "width": W, "height": H},
         "cpu_baseline": {"value": fps, "unit": "frames/s", "cores": threads, "kind": "port",
-                         "sample": f"{len(times)} frames of the orbit (full 1920x1080 frames)"},
+                         "sample": f"{len(times)} frames of the orbit (full {W}x{H} frames)"},
         "e2e": {"value": fps, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def fp64_errors(device_frames, source_scene, decoded_scene, views, w, h):
+    """Per-frame error of the device frames against the FP64 naive
+    rasterizer, run on the decoded FP16 values and on the f32 source."""
+    from oracle import oracle as O
+
+    def as_dict(sc):
+        return {"positions": sc.positions, "scales": sc.scales, "rotations": sc.rotations,
+                "opacities": sc.opacities, "colors": sc.colors, "sh_rest": sc.sh_rest, "sh_degree": sc.sh_degree}
+
+    rows = []
+    for i, (img, v) in enumerate(zip(device_frames, views)):
+        row = {"frame": i}
+        for key, sc in (("decoded_fp16", decoded_scene), ("f32_source", source_scene)):
+            ref, _, _ = O.render_naive_f64(as_dict(sc), v, w, h)
+            row[key] = {"psnr_db": O.psnr(img, ref),
+                        "max_abs": int(np.max(np.abs(img.astype(int) - ref.astype(int))))}
+        rows.append(row)
+    return rows
 
 
 def run_ours(args):
@@ -203,20 +245,22 @@ def run_ours(args):
     else:
         torch.cuda.set_device(0)
     dev = torch.cuda.current_device()
+    cfg = CONFIGS[args.config]
+    W, H = cfg["w"], cfg["h"]
 
     from splat_b200 import _native as Nat
     from splat_b200.render import CudaRenderer
 
-    scene, home, warm, timed = make_workload(args.splats)
+    stored, f32_scene, source, home, warm, timed = make_workload(args.splats, cfg)
     views = timed[rank::world] if world > 1 else timed
     if not views:
         views = timed
-    r = CudaRenderer(scene, device=dev)
+    r = CudaRenderer(stored, device=dev)
     stream = torch.cuda.ExternalStream(r.stream())
     out = torch.empty(W * H * 3, dtype=torch.uint8, device=dev)
     nbytes = out.numel()
 
-    # Home frame (PSNR frame) and warm-up; capacity growth settles here.
+    # Home frame and warm-up; capacity growth settles here.
     for v in [home] + warm[: max(args.warmup, 3)]:
         while True:
             r.render_device(v, W, H, (0, 0, 0), out.data_ptr(), nbytes)
@@ -242,6 +286,7 @@ def run_ours(args):
     K = args.steps
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier()
+    launches0 = r.get_option(Nat.SPLAT_OPT_KERNEL_LAUNCHES)
     with Clocks(dev) as clk:
         start.record(stream)
         for i in range(K):
@@ -249,6 +294,7 @@ def run_ours(args):
         end.record(stream)
         st_last, regrown = r.finish()
         barrier()
+    launches = (r.get_option(Nat.SPLAT_OPT_KERNEL_LAUNCHES) - launches0) % (1 << 32)
     assert not regrown, "pair buffers overflowed inside the timed region"
     ms = start.elapsed_time(end)
     t = torch.tensor([ms], device=dev)
@@ -288,14 +334,27 @@ def run_ours(args):
         torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
     e2e = frames_total / float(te.item())
 
+    errors = None
+    if rank == 0 and cfg["precision"] == "fp16" and args.error_frames > 0:
+        frames = []
+        for v in views[: args.error_frames]:
+            r.render_into(v, W, H, (0, 0, 0), host.data_ptr(), host.numel())
+            frames.append(host.numpy().reshape(H, W, 3).copy())
+        errors = fp64_errors(frames, source, f32_scene, views[: args.error_frames], W, H)
+
     if rank == 0:
         peak, peak_kind = measured_peaks()
-        digits = 6  # 32 depth bits + 13 tile bits at 1920x1080 / 16x16
+        N = args.splats
         tiles = ((W + 15) // 16) * ((H + 15) // 16)
+        # Algorithmic bytes per frame and stage:
+        #   project: scene read once, tile rectangle per splat and record per visible splat written
+        #   sort:    rectangles read by the count and scatter passes, pair words written by the
+        #            scatter, read and written once by the per-tile sort
+        #   raster:  pair words read, one record gathered per pair, ranges, u8 frame written
         bytes_stage = {
-            "project": args.splats * S_IN + V * (S_REC + 16) + P * 12,
-            "sort": P * 8 + digits * P * 24 + P * 8,
-            "raster": P * (4 + S_REC) + tiles * 8 + W * H * 3,
+            "project": N * cfg["s_in"] + N * S_BIN + V * S_REC,
+            "sort": 2 * N * S_BIN + P * 8 + 2 * P * 8,
+            "raster": P * (8 + S_REC) + tiles * 8 + W * H * 3,
         }
         times = {"project": stage["project_ms"], "sort": stage["sort_ms"], "raster": stage["raster_ms"]}
         dom = max(times, key=times.get)
@@ -304,34 +363,39 @@ def run_ours(args):
         prof = os.path.join(ROOT, "profiles", "traffic.json")
         if os.path.exists(prof):
             try:
-                traffic = json.load(open(prof)).get(dom)
+                traffic = json.load(open(prof)).get(args.config, {}).get(dom)
             except Exception:
                 traffic = None
         cpu = None
         if not args.no_cpu_baseline:
-            fps, cores, frames = cpu_baseline(scene, timed, args.cpu_sample_s)
+            fps, cores, frames = cpu_baseline(f32_scene, timed, W, H, args.cpu_sample_s)
             cpu = {"value": fps, "unit": "frames/s", "cores": cores, "kind": "port",
-                   "sample": f"{frames} full 1920x1080 frames of the orbit (~{args.cpu_sample_s:.0f} s)"}
-        launches_per_frame = 4 + digits + 2  # project, emit, hist, hist_scan, passes, ranges, blend
+                   "sample": f"{frames} full {W}x{H} frames of the orbit (~{args.cpu_sample_s:.0f} s)"}
         line = {
-            "metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world, "steps": K,
+            "metric": cfg["metric"], "value": value, "unit": "frames/s", "n_gpus": world, "steps": K,
             "warmup": args.warmup, "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "splats": args.splats, "width": W, "height": H, "tile": 16,
-                       "visible": V, "pairs": P, "parallelism": f"view-parallel x{world}",
-                       "l2": "inputs larger than L2 (scene 288 MB > 126 MB)"},
+            "config": {"workload": cfg["workload"], "splats": N, "width": W, "height": H, "tile": 16,
+                       "storage": cfg["precision"], "visible": V, "pairs": P,
+                       "parallelism": f"view-parallel x{world}",
+                       "l2": f"inputs larger than L2 (scene {N * cfg['s_in'] / 1e6:.0f} MB > 126 MB)"},
             "gsplat_tiles_per_s": P * value / world / 1e9,
             "stages_ms": stage,
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind},
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "algorithmic_bytes": bytes_stage[dom]},
             "frame_hbm": {"bytes": sum(bytes_stage.values()),
                           "achieved_gbs": sum(bytes_stage.values()) * value / world / 1e9},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e, "unit": "frames/s", "h2d_bytes_per_step": 56,
-                    "d2h_bytes_per_step": W * H * 3 + 9216},
+                    "d2h_bytes_per_step": W * H * 3 + 32,
+                    "note": "input per step: the 56-byte view, passed as kernel parameters (the scene stays "
+                            "resident); output: the u8 frame into pinned host memory plus the 32-byte frame state"},
             "clocks": clk.summary(),
-            "gpu_launches": launches_per_frame * K,
+            "gpu_launches": launches,
         }
+        if errors is not None:
+            line["error_vs_fp64_naive"] = errors
         print(json.dumps(line), flush=True)
     r.close()
     if world > 1:

@@ -177,6 +177,12 @@ void* splat_cuda_get_stream(splat_cuda_handle* h);
 #define SPLAT_OPT_STAGE_EVENTS 3u  /* 1 (default): time stages with CUDA events */
 #define SPLAT_OPT_DEBUG_CAPTURE 4u /* 1: keep per-splat projections for
                                       splat_cuda_debug_dump (costs n*44 bytes) */
+#define SPLAT_OPT_FP64_CONICS 5u   /* read-only: splats of the last completed
+                                      frame whose 2D covariance determinant fell
+                                      below 1e-6 and was recomputed in FP64
+                                      (FP16 scenes; 0 otherwise) */
+#define SPLAT_OPT_KERNEL_LAUNCHES 6u /* kernels this handle has launched
+                                        (set to reset the count) */
 int splat_cuda_set_option(splat_cuda_handle* h, uint32_t option, uint64_t value);
 int splat_cuda_get_option(splat_cuda_handle* h, uint32_t option, uint64_t* value);
 

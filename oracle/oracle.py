@@ -40,6 +40,8 @@ def lib():
         L = ctypes.CDLL(LIB_PATH)
         L.oracle_project.argtypes = [ctypes.c_uint64, ctypes.c_uint32] + [_f32p] * 6 + [
             ctypes.c_uint32, ctypes.c_uint32, _f32p, _u8p]
+        L.oracle_project_det.argtypes = [ctypes.c_uint64, ctypes.c_uint32] + [_f32p] * 6 + [
+            ctypes.c_uint32, ctypes.c_uint32, _f32p]
         L.oracle_project_ctx.argtypes = [_f32p, ctypes.c_uint32, ctypes.c_uint32, _f32p]
         L.oracle_eval_rest.argtypes = [ctypes.c_uint32, _f32p, _f32p, _f32p]
         L.oracle_covariance.argtypes = [_f32p, _f32p, _f32p]
@@ -105,6 +107,16 @@ def project(scene, view, w, h):
     v = _view(view)
     lib().oracle_project(n, scene.sh_degree, *ptrs, _p(v, _f32p), w, h, _p(out, _f32p), _p(vis, _u8p))
     return out, vis.astype(bool)
+
+
+def project_det(scene, view, w, h):
+    """The f32 2D covariance determinant project() computes per splat (+inf
+    where the splat is culled before it)."""
+    n = len(scene.opacities)
+    keep, ptrs = _scene_ptrs(scene)
+    det = np.zeros(n, np.float32)
+    lib().oracle_project_det(n, scene.sh_degree, *ptrs, _p(_view(view), _f32p), w, h, _p(det, _f32p))
+    return det
 
 
 def project_ctx(view, w, h):

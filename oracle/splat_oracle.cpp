@@ -34,6 +34,7 @@
 #include <memory>
 #include <mutex>
 #include <thread>
+#include <limits>
 #include <vector>
 
 namespace {
@@ -228,7 +229,10 @@ template <class T> struct SplatIn {
 // src/render/mod.rs:199-272 (project); identical results to project_fast and
 // project4 (src/render/cpu.rs:419-566, pinned bit for bit by cpu.rs:763-804).
 // `k_pre` >= 0 substitutes the precomputed bounding radius (cpu.rs:384-388).
-template <class T> bool project(const SplatIn<T>& s, const Ctx<T>& ctx, Splat2D<T>* out, T k_pre = T(-1)) {
+// `det_out` (optional) receives the 2D covariance determinant when the
+// projection gets that far.
+template <class T>
+bool project(const SplatIn<T>& s, const Ctx<T>& ctx, Splat2D<T>* out, T k_pre = T(-1), T* det_out = nullptr) {
   const T amin = T(ALPHA_MIN);
   T opacity = s.opacity;
   if (opacity < amin) return false;
@@ -255,6 +259,7 @@ template <class T> bool project(const SplatIn<T>& s, const Ctx<T>& ctx, Splat2D<
   T b = dot(t1, s0);
   T cc = dot(t1, sigma(t1)) + T(DILATION);
   T det = a * cc - b * b;
+  if (det_out) *det_out = det;
   if (!(det > T(0))) return false;
   T inv_det = T(1) / det;
   T k = k_pre >= T(0) ? k_pre : std::sqrt(T(2) * std::log(opacity / amin));
@@ -936,6 +941,20 @@ void oracle_project(uint64_t n, uint32_t degree, const float* pos, const float* 
     } else {
       std::memset(o, 0, 48);
     }
+  }
+}
+
+// The 2D covariance determinant project() computes per splat (+inf where the
+// splat is culled before it), for locating near-singular conics.
+void oracle_project_det(uint64_t n, uint32_t degree, const float* pos, const float* opac, const float* col,
+                        const float* cov, const float* rest, const float* view, uint32_t w, uint32_t h,
+                        float* det) {
+  SceneF s = scene_from(n, degree, pos, opac, col, cov, rest);
+  Ctx<float> ctx = make_ctx(view_from(view), w, h);
+  for (size_t i = 0; i < n; i++) {
+    Splat2D<float> p;
+    det[i] = std::numeric_limits<float>::infinity();
+    project(s.at(i), ctx, &p, -1.0f, &det[i]);
   }
 }
 

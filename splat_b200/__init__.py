@@ -10,10 +10,10 @@ and scene (``src/scene.rs``) over that ABI.
 from .camera import MAX_PITCH, OrbitCamera, UpAxis, View, to_radians
 from .render import (ALPHA_MAX, ALPHA_MIN, DILATION, MAX_DIM, T_MIN, TILE, Backend, CudaRenderer, Frame,
                      RenderStats, Renderer, create)
-from .scene import SH_C0, Scene, coeffs_for_degree, covariance, degree_from_rest_count
+from .scene import SH_C0, HalfScene, Scene, coeffs_for_degree, covariance, degree_from_rest_count
 
 __all__ = [
     "MAX_PITCH", "OrbitCamera", "UpAxis", "View", "to_radians", "ALPHA_MAX", "ALPHA_MIN", "DILATION", "MAX_DIM",
-    "T_MIN", "TILE", "Backend", "CudaRenderer", "Frame", "RenderStats", "Renderer", "create", "SH_C0", "Scene",
+    "T_MIN", "TILE", "Backend", "CudaRenderer", "Frame", "RenderStats", "Renderer", "create", "SH_C0", "HalfScene", "Scene",
     "coeffs_for_degree", "covariance", "degree_from_rest_count",
 ]

@@ -27,6 +27,8 @@ SPLAT_OPT_EXACT_BLEND = 1
 SPLAT_OPT_PAIR_CAPACITY = 2
 SPLAT_OPT_STAGE_EVENTS = 3
 SPLAT_OPT_DEBUG_CAPTURE = 4
+SPLAT_OPT_FP64_CONICS = 5
+SPLAT_OPT_KERNEL_LAUNCHES = 6
 
 _STATUS_NAMES = {0: "OK", 1: "INVALID_ARG", 2: "OOM", 3: "CAPACITY", 4: "DEVICE", 5: "TIMEOUT", 6: "UNSUPPORTED"}
 

@@ -37,6 +37,9 @@ struct splat_cuda_handle {
   float4* cov_b = nullptr;
   float* color = nullptr;
   float* sh = nullptr;
+  float4* pos_k = nullptr;   // FP16 storage: x, y, z, k
+  uint4* geom16 = nullptr;   // FP16 storage: scale, rotation, opacity halves
+  uint16_t* sh16 = nullptr;  // FP16 storage: base colour + SH planes
   // per-splat frame buffers
   Record* rec = nullptr;
   BinInfo* bin = nullptr;
@@ -67,6 +70,7 @@ struct splat_cuda_handle {
   // options
   bool exact = false;
   bool stage_events = true;
+  uint32_t launches = 0;  // kernels this handle has launched (wraps at 2^32)
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   // last frame
   FrameParams last_fp{};
@@ -94,15 +98,34 @@ int cuda_fail(splat_cuda_handle* h, cudaError_t e, const char* what) {
     if (e_ != cudaSuccess) return cuda_fail(h, e_, what); \
   } while (0)
 
+// IEEE binary16 bit pattern to binary32 (exact: every half is a float).
+float half_bits_to_float(uint16_t b) {
+  const uint32_t sign = (uint32_t)(b >> 15) << 31;
+  const uint32_t e = (b >> 10) & 31u, m = b & 1023u;
+  uint32_t bits;
+  if (e == 31u) {
+    bits = sign | 0x7F800000u | (m << 13);  // inf / NaN
+  } else if (e != 0u) {
+    bits = sign | ((e + 112u) << 23) | (m << 13);  // rebias 15 -> 127
+  } else if (m == 0u) {
+    bits = sign;  // signed zero
+  } else {  // subnormal half: m * 2^-24, normal as a float
+    int ex = -1;
+    uint32_t mm = m;
+    do {
+      mm <<= 1;
+      ex++;
+    } while (!(mm & 1024u));
+    bits = sign | ((uint32_t)(112 - ex) << 23) | ((mm & 1023u) << 13);
+  }
+  float f;
+  std::memcpy(&f, &bits, 4);
+  return f;
+}
+
 template <class T> void dfree(T*& p) {
   if (p) cudaFree(p);
   p = nullptr;
-}
-
-uint32_t bits_for(uint64_t v) {  // bits needed to hold values < v
-  uint32_t b = 0;
-  while (b < 64 && (1ull << b) < v) b++;
-  return b;
 }
 
 void free_pairs(splat_cuda_handle* h) {
@@ -200,17 +223,19 @@ int enqueue_frame(splat_cuda_handle* h, const FrameParams& fp, uint8_t* dev_out)
   CK(cudaMemsetAsync(h->st, 0, sizeof(DevState), s), "clear frame state");
   if (h->stage_events) CK(cudaEventRecord(h->ev[0], s), "event");
   if (h->n) {
-    SceneDev sd{h->pos_op, h->cov_a, h->cov_b, h->color, h->sh, h->n, h->sh_degree};
+    SceneDev sd{h->pos_op, h->cov_a, h->cov_b, h->color, h->sh, h->pos_k, h->geom16, h->sh16, h->n, h->sh_degree,
+                h->precision == SPLAT_PRECISION_FP16 ? 1u : 0u};
     CK(launch_project(fp, sd, h->rec, h->bin, h->debug_capture ? h->dbg_proj : nullptr,
-                      h->debug_capture ? h->dbg_color : nullptr, h->st, s),
+                      h->debug_capture ? h->dbg_color : nullptr, h->st, s, &h->launches),
        "project kernel");
   }
   if (h->stage_events) CK(cudaEventRecord(h->ev[1], s), "event");
   CK(launch_binning(fp, h->bin, h->n, h->counts, h->totals, h->ranges, h->mid_list, h->long_list, h->pairs[0],
-                    h->pairs[1], h->cap, h->st, h->num_sms, h->max_smem, s),
+                    h->pairs[1], h->cap, h->st, h->num_sms, h->max_smem, s, &h->launches),
      "binning kernels");
   if (h->stage_events) CK(cudaEventRecord(h->ev[2], s), "event");
-  CK(launch_blend(fp, h->rec, h->pairs[0], h->ranges, h->exact, dev_out, h->full_dev, s), "blend kernel");
+  CK(launch_blend(fp, h->rec, h->pairs[0], h->ranges, h->exact, dev_out, h->full_dev, s, &h->launches),
+     "blend kernel");
   if (h->stage_events) CK(cudaEventRecord(h->ev[3], s), "event");
   CK(cudaMemcpyAsync(h->st_host, h->st, sizeof(DevState), cudaMemcpyDeviceToHost, s), "copy frame state");
   h->last_fp = fp;
@@ -279,8 +304,8 @@ SPLAT_API int splat_cuda_create(const splat_scene_desc* d, int device, splat_cud
     g_create_error = "sh_degree must be 0..3";
     return SPLAT_ERR_INVALID_ARG;
   }
-  if (d->precision != SPLAT_PRECISION_FP32) {
-    g_create_error = "only FP32 scene storage is available in this build";
+  if (d->precision != SPLAT_PRECISION_FP32 && d->precision != SPLAT_PRECISION_FP16) {
+    g_create_error = "unknown scene precision";
     return SPLAT_ERR_UNSUPPORTED;
   }
   if (d->n > 0xFFFFFFFFull) {
@@ -288,8 +313,13 @@ SPLAT_API int splat_cuda_create(const splat_scene_desc* d, int device, splat_cud
     return SPLAT_ERR_INVALID_ARG;
   }
   const uint64_t n = d->n;
-  if (n && (!d->positions || !d->opacities || !d->colors || !d->cov3d || (d->sh_degree && !d->sh_rest))) {
+  const bool f16 = d->precision == SPLAT_PRECISION_FP16;
+  if (n && !f16 && (!d->positions || !d->opacities || !d->colors || !d->cov3d || (d->sh_degree && !d->sh_rest))) {
     g_create_error = "null scene array";
+    return SPLAT_ERR_INVALID_ARG;
+  }
+  if (n && f16 && (!d->positions || !d->scales_f16 || !d->rotations_f16 || !d->opacities_f16 || !d->sh_f16)) {
+    g_create_error = "null FP16 scene array";
     return SPLAT_ERR_INVALID_ARG;
   }
   auto* h = new splat_cuda_handle();
@@ -320,7 +350,41 @@ SPLAT_API int splat_cuda_create(const splat_scene_desc* d, int device, splat_cud
     return bail(cuda_fail(h, e, "cudaMallocHost state"));
   std::memset(h->st_host, 0, sizeof(DevState));
 
-  if (n) {
+  if (n && f16) {
+    // FP16 layout, 128 bytes per splat: float4 (pos, k); 8 halves (scale xyz,
+    // rotation xyzw, opacity) as one uint4; base colour and SH as planes of n
+    // halves. k is computed from the decoded opacity as in the FP32 layout.
+    const uint32_t planes = d->sh_degree ? (d->sh_degree + 1) * (d->sh_degree + 1) * 3 : 3;
+    std::vector<float4> pk(n);
+    std::vector<uint4> g(n);
+    for (uint64_t i = 0; i < n; i++) {
+      const float* p = d->positions + 3 * i;
+      const uint16_t* sc = d->scales_f16 + 3 * i;
+      const uint16_t* q = d->rotations_f16 + 4 * i;
+      const uint16_t ob = d->opacities_f16[i];
+      const float o = std::fmin(std::fmax(half_bits_to_float(ob), 0.0f), 1.0f);  // as the device clamps it
+      const float k = o < kAlphaMin ? 0.0f : std::sqrt(2.0f * std::log(o / kAlphaMin));
+      pk[i] = make_float4(p[0], p[1], p[2], k);
+      g[i] = make_uint4(sc[0] | ((uint32_t)sc[1] << 16), sc[2] | ((uint32_t)q[0] << 16), q[1] | ((uint32_t)q[2] << 16),
+                        q[3] | ((uint32_t)ob << 16));
+    }
+    std::vector<uint16_t> sh((size_t)planes * n);
+    for (uint64_t i = 0; i < n; i++)
+      for (uint32_t k = 0; k < planes; k++) sh[(size_t)k * n + i] = d->sh_f16[i * planes + k];
+    auto up = [&](void** dst, const void* src, size_t bytes, const char* what) -> int {
+      cudaError_t er = cudaMalloc(dst, bytes);
+      if (er != cudaSuccess) return cuda_fail(h, er, what);
+      er = cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice);
+      if (er != cudaSuccess) return cuda_fail(h, er, what);
+      return SPLAT_OK;
+    };
+    int rc;
+    if ((rc = up((void**)&h->pos_k, pk.data(), n * sizeof(float4), "upload positions"))) return bail(rc);
+    if ((rc = up((void**)&h->geom16, g.data(), n * sizeof(uint4), "upload FP16 geometry"))) return bail(rc);
+    if ((rc = up((void**)&h->sh16, sh.data(), sh.size() * sizeof(uint16_t), "upload FP16 SH"))) return bail(rc);
+    if ((e = cudaMalloc(&h->rec, n * sizeof(Record))) != cudaSuccess) return bail(cuda_fail(h, e, "cudaMalloc records"));
+    if ((e = cudaMalloc(&h->bin, n * sizeof(BinInfo))) != cudaSuccess) return bail(cuda_fail(h, e, "cudaMalloc bins"));
+  } else if (n) {
     // Upload in the device layout: float4 (pos, opacity), float4 + float4 for
     // the covariance (with k = sqrt(2 ln(opacity / ALPHA_MIN)), the bbox
     // radius the reference's cpu backend also precomputes, cpu.rs:384-388),
@@ -449,6 +513,11 @@ SPLAT_API int splat_cuda_set_option(splat_cuda_handle* h, uint32_t option, uint6
     case SPLAT_OPT_STAGE_EVENTS:
       h->stage_events = value != 0;
       return SPLAT_OK;
+    case SPLAT_OPT_FP64_CONICS:
+      return fail(h, SPLAT_ERR_INVALID_ARG, "SPLAT_OPT_FP64_CONICS is read-only");
+    case SPLAT_OPT_KERNEL_LAUNCHES:
+      h->launches = (uint32_t)value;
+      return SPLAT_OK;
     case SPLAT_OPT_DEBUG_CAPTURE: {
       h->debug_capture = value != 0;
       if (h->debug_capture && h->n && !h->dbg_proj) {
@@ -469,6 +538,8 @@ SPLAT_API int splat_cuda_get_option(splat_cuda_handle* h, uint32_t option, uint6
     case SPLAT_OPT_PAIR_CAPACITY: *value = h->cap; return SPLAT_OK;
     case SPLAT_OPT_STAGE_EVENTS: *value = h->stage_events; return SPLAT_OK;
     case SPLAT_OPT_DEBUG_CAPTURE: *value = h->debug_capture; return SPLAT_OK;
+    case SPLAT_OPT_FP64_CONICS: *value = h->have_frame ? h->st_host->fp64_conics : 0; return SPLAT_OK;
+    case SPLAT_OPT_KERNEL_LAUNCHES: *value = h->launches; return SPLAT_OK;
     default: return fail(h, SPLAT_ERR_UNSUPPORTED, "unknown option");
   }
 }
@@ -527,6 +598,9 @@ SPLAT_API int splat_cuda_destroy(splat_cuda_handle* h) {
   dfree(h->cov_b);
   dfree(h->color);
   dfree(h->sh);
+  dfree(h->pos_k);
+  dfree(h->geom16);
+  dfree(h->sh16);
   dfree(h->rec);
   dfree(h->bin);
   free_pairs(h);

@@ -351,7 +351,7 @@ uint32_t bin_rows(int num_sms) { return 2u * (uint32_t)num_sms; }
 cudaError_t launch_binning(const FrameParams& fp, const BinInfo* bin, uint64_t n, uint32_t* counts, uint32_t* totals,
                            uint2* ranges, uint32_t* mid_list, uint32_t* long_list, uint64_t* pairs,
                            uint64_t* pairs_alt, uint64_t cap, DevState* st, int num_sms, size_t max_smem,
-                           cudaStream_t stream) {
+                           cudaStream_t stream, uint32_t* launches) {
   const uint32_t tiles = fp.tiles_x * fp.tiles_y;
   const uint32_t rows = bin_rows(num_sms);
   const uint64_t per_cta = n ? (n + rows - 1) / rows : 1;
@@ -368,10 +368,12 @@ cudaError_t launch_binning(const FrameParams& fp, const BinInfo* bin, uint64_t n
       k_bin_count<false><<<rows, kBinThreads, 0, stream>>>(bin, n, per_cta, fp.tiles_x, tiles, counts);
     }
     k_bin_colscan<<<(tiles + 31) / 32, 256, 0, stream>>>(counts, rows, tiles, totals);
+    *launches += 2;
   } else {
     if ((e = cudaMemsetAsync(totals, 0, (size_t)tiles * sizeof(uint32_t), stream))) return e;
   }
   k_bin_tilescan<<<1, 1024, 0, stream>>>(totals, tiles, cap, ranges, mid_list, long_list, st);
+  *launches += 1;
   if (n) {
     if (use_smem) {
       if ((e = cudaFuncSetAttribute(k_bin_scatter<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
@@ -387,6 +389,7 @@ cudaError_t launch_binning(const FrameParams& fp, const BinInfo* bin, uint64_t n
     if ((e = cudaFuncSetAttribute(k_sort_mid, cudaFuncAttributeMaxDynamicSharedMemorySize, mid_smem))) return e;
     k_sort_mid<<<num_sms * 3, kTileThreads, mid_smem, stream>>>(ranges, mid_list, pairs, st);
     k_sort_long<<<num_sms, kTileThreads, 0, stream>>>(ranges, long_list, pairs, pairs_alt, cap, st);
+    *launches += 4;  // scatter, small, mid, long
   }
   return cudaGetLastError();
 }

@@ -310,16 +310,18 @@ __global__ void k_downsample(FrameParams fp, const uint8_t* __restrict__ full, u
 }  // namespace
 
 cudaError_t launch_blend(const FrameParams& fp, const Record* rec, const uint64_t* pairs, const uint2* ranges,
-                         bool exact, uint8_t* out, uint8_t* full_scratch, cudaStream_t stream) {
+                         bool exact, uint8_t* out, uint8_t* full_scratch, cudaStream_t stream, uint32_t* launches) {
   const unsigned tiles = fp.tiles_x * fp.tiles_y;
   if (tiles == 0) return cudaSuccess;
   if (exact)
     k_blend<true><<<tiles, 256, 0, stream>>>(fp, rec, pairs, ranges, out, full_scratch);
   else
     k_blend<false><<<tiles, 256, 0, stream>>>(fp, rec, pairs, ranges, out, full_scratch);
+  *launches += 1;
   if (fp.downsample > 1 && kTile % fp.downsample != 0 && fp.out_w > 0 && fp.out_h > 0) {
     dim3 grid((fp.out_w + 127) / 128, fp.out_h);
     k_downsample<<<grid, 128, 0, stream>>>(fp, full_scratch, out);
+    *launches += 1;
   }
   return cudaGetLastError();
 }

@@ -8,6 +8,8 @@
 // bit. The kernel also emits each visible splat's tile rectangle (pixel_bbox,
 // src/render/cpu.rs:94-102 and the tile loop of cpu.rs:262-276), its pair
 // count and depth bits for the binning, and counts the visible splats.
+#include <cuda_fp16.h>
+
 #include "common.cuh"
 
 namespace splat {
@@ -30,12 +32,11 @@ __device__ __forceinline__ uint32_t sat_u32(float v) {
 // f32::clamp (NaN passes through).
 __device__ __forceinline__ float rclamp(float v, float lo, float hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
-// SH coefficient `coef`, channel `ch` of splat i (planar layout).
-template <int DEG>
-__device__ __forceinline__ void eval_sh(const float* __restrict__ sh, uint64_t n, uint64_t i, float x, float y, float z,
-                                        float c[3]) {
+// sh::eval_rest added to c; R(coef, ch) loads rest coefficient `coef`,
+// channel `ch` of the splat.
+template <int DEG, class Load>
+__device__ __forceinline__ void eval_sh(Load&& R, float x, float y, float z, float c[3]) {
   if constexpr (DEG >= 1) {
-    auto R = [&](int coef, int ch) { return __ldg(sh + (uint64_t)(coef * 3 + ch) * n + i); };
     float r[3];
 #pragma unroll
     for (int ch = 0; ch < 3; ch++) {
@@ -82,23 +83,97 @@ __device__ __forceinline__ void eval_sh(const float* __restrict__ sh, uint64_t n
   }
 }
 
-template <int DEG>
+__device__ __forceinline__ float h2f(uint32_t bits16) { return __half2float(__ushort_as_half((unsigned short)bits16)); }
+
+// Scene::finalize's quaternion normalisation (src/scene.rs:164-171; glam's
+// SSE2 Quat::length sums (x^2 + z^2) + (y^2 + w^2)) and covariance's
+// R S S^T R^T in glam's Mat3 operation order (src/scene.rs:261-270).
+template <class T>
+__device__ __forceinline__ void covariance_from(const T s[3], T qx, T qy, T qz, T qw, T c[6]) {
+  const T len = sqrt((qx * qx + qz * qz) + (qy * qy + qw * qw));
+  if (isfinite(len) && len > T(1e-12)) {
+    qx = qx / len;
+    qy = qy / len;
+    qz = qz / len;
+    qw = qw / len;
+  } else {
+    qx = qy = qz = T(0);
+    qw = T(1);
+  }
+  const T x2 = qx + qx, y2 = qy + qy, z2 = qz + qz;
+  const T xx = qx * x2, xy = qx * y2, xz = qx * z2, yy = qy * y2, yz = qy * z2, zz = qz * z2;
+  const T wx = qw * x2, wy = qw * y2, wz = qw * z2;
+  const T r[3][3] = {{T(1) - (yy + zz), xy + wz, xz - wy},   // column 0
+                     {xy - wz, T(1) - (xx + zz), yz + wx},   // column 1
+                     {xz + wy, yz - wx, T(1) - (xx + yy)}};  // column 2
+  T m[3][3];  // columns of R * diag(s): c0*v.x + c1*v.y + c2*v.z with v = (s0,0,0), ...
+  for (int j = 0; j < 3; j++)
+    for (int k = 0; k < 3; k++) {
+      const T v0 = j == 0 ? s[0] : T(0), v1 = j == 1 ? s[1] : T(0), v2 = j == 2 ? s[2] : T(0);
+      m[j][k] = (r[0][k] * v0 + r[1][k] * v1) + r[2][k] * v2;
+    }
+  T o[3][3];  // columns of m * m^T; column j of m^T is row j of m
+  for (int j = 0; j < 3; j++)
+    for (int k = 0; k < 3; k++) o[j][k] = (m[0][k] * m[0][j] + m[1][k] * m[1][j]) + m[2][k] * m[2][j];
+  c[0] = o[0][0];
+  c[1] = o[1][0];
+  c[2] = o[2][0];
+  c[3] = o[1][1];
+  c[4] = o[2][1];
+  c[5] = o[2][2];
+}
+
+template <class T>
+__device__ __forceinline__ void conic_terms(const T c[6], T t0x, T t0y, T t0z, T t1x, T t1y, T t1z, T& a, T& bb,
+                                            T& cc) {
+  const T s0x = (c[0] * t0x + c[1] * t0y) + c[2] * t0z;
+  const T s0y = (c[1] * t0x + c[3] * t0y) + c[4] * t0z;
+  const T s0z = (c[2] * t0x + c[4] * t0y) + c[5] * t0z;
+  const T s1x = (c[0] * t1x + c[1] * t1y) + c[2] * t1z;
+  const T s1y = (c[1] * t1x + c[3] * t1y) + c[4] * t1z;
+  const T s1z = (c[2] * t1x + c[4] * t1y) + c[5] * t1z;
+  a = ((t0x * s0x + t0y * s0y) + t0z * s0z) + T(kDilation);
+  bb = (t1x * s0x + t1y * s0y) + t1z * s0z;
+  cc = ((t1x * s1x + t1y * s1y) + t1z * s1z) + T(kDilation);
+}
+
+// F16: the scene is stored in FP16 (positions FP32); the 3D covariance is
+// formed here in FP32, and a 2D covariance whose FP32 determinant falls below
+// kFp64DetBelow is recomputed in FP64.
+template <int DEG, bool F16>
 __global__ void __launch_bounds__(256) k_project(FrameParams fp, SceneDev s, Record* __restrict__ rec,
                                                  BinInfo* __restrict__ bin, float* __restrict__ dbg_proj,
                                                  float* __restrict__ dbg_color, DevState* st) {
   const int tid = threadIdx.x;
   const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + tid;
   bool vis = false;
+  bool used_fp64 = false;
   if (i < s.n) {
-    const float4 po = __ldg(&s.pos_op[i]);
+    float px, py, pz, opacity, k;
+    uint4 g16 = make_uint4(0, 0, 0, 0);
+    if (F16) {
+      const float4 pk = __ldg(&s.pos_k[i]);
+      px = pk.x;
+      py = pk.y;
+      pz = pk.z;
+      k = pk.w;
+      g16 = __ldg(&s.geom16[i]);
+      opacity = fminf(fmaxf(h2f(g16.w >> 16), 0.0f), 1.0f);  // Scene::finalize's clamp; NaN -> 0
+    } else {
+      const float4 po = __ldg(&s.pos_op[i]);
+      px = po.x;
+      py = po.y;
+      pz = po.z;
+      opacity = po.w;
+      k = 0.0f;
+    }
     BinInfo b{kCulled, 0u, 0u, 0u};
     float out_x = 0.f, out_y = 0.f, out_ex = 0.f, out_ey = 0.f, out_depth = 0.f, c0 = 0.f, c1 = 0.f, c2 = 0.f;
     float col[3] = {0.f, 0.f, 0.f};
-    const float opacity = po.w;
     do {
       if (opacity < kAlphaMin) break;
       // t = rot * (p - eye), glam Mat3::mul_vec3 order.
-      const float dx = po.x - fp.eye[0], dy = po.y - fp.eye[1], dz = po.z - fp.eye[2];
+      const float dx = px - fp.eye[0], dy = py - fp.eye[1], dz = pz - fp.eye[2];
       const float tx_ = (fp.rot[0] * dx + fp.rot[1] * dy) + fp.rot[2] * dz;
       const float ty_ = (fp.rot[3] * dx + fp.rot[4] * dy) + fp.rot[5] * dz;
       const float tz = (fp.rot[6] * dx + fp.rot[7] * dy) + fp.rot[8] * dz;
@@ -117,28 +192,65 @@ __global__ void __launch_bounds__(256) k_project(FrameParams fp, SceneDev s, Rec
       const float t1x = (fp.rot[0] * 0.0f + fp.rot[3] * f) + fp.rot[6] * j1z;
       const float t1y = (fp.rot[1] * 0.0f + fp.rot[4] * f) + fp.rot[7] * j1z;
       const float t1z = (fp.rot[2] * 0.0f + fp.rot[5] * f) + fp.rot[8] * j1z;
-      const float4 ca = __ldg(&s.cov_a[i]);
-      const float4 cb = __ldg(&s.cov_b[i]);
-      const float cxx = ca.x, cxy = ca.y, cxz = ca.z, cyy = ca.w, cyz = cb.x, czz = cb.y;
-      const float s0x = (cxx * t0x + cxy * t0y) + cxz * t0z;
-      const float s0y = (cxy * t0x + cyy * t0y) + cyz * t0z;
-      const float s0z = (cxz * t0x + cyz * t0y) + czz * t0z;
-      const float s1x = (cxx * t1x + cxy * t1y) + cxz * t1z;
-      const float s1y = (cxy * t1x + cyy * t1y) + cyz * t1z;
-      const float s1z = (cxz * t1x + cyz * t1y) + czz * t1z;
-      const float a = ((t0x * s0x + t0y * s0y) + t0z * s0z) + kDilation;
-      const float bb = (t1x * s0x + t1y * s0y) + t1z * s0z;
-      const float cc = ((t1x * s1x + t1y * s1y) + t1z * s1z) + kDilation;
-      const float det = a * cc - bb * bb;
-      if (!(det > 0.0f)) break;
-      const float inv_det = 1.0f / det;
-      const float k = cb.z;  // sqrt(2 ln(opacity / ALPHA_MIN)), precomputed at upload
+      float cov[6];
+      float sc[3], q[4];
+      if (F16) {
+        sc[0] = h2f(g16.x & 0xFFFFu);
+        sc[1] = h2f(g16.x >> 16);
+        sc[2] = h2f(g16.y & 0xFFFFu);
+        q[0] = h2f(g16.y >> 16);
+        q[1] = h2f(g16.z & 0xFFFFu);
+        q[2] = h2f(g16.z >> 16);
+        q[3] = h2f(g16.w & 0xFFFFu);
+        covariance_from<float>(sc, q[0], q[1], q[2], q[3], cov);
+      } else {
+        const float4 ca = __ldg(&s.cov_a[i]);
+        const float4 cb = __ldg(&s.cov_b[i]);
+        cov[0] = ca.x;
+        cov[1] = ca.y;
+        cov[2] = ca.z;
+        cov[3] = ca.w;
+        cov[4] = cb.x;
+        cov[5] = cb.y;
+        k = cb.z;  // sqrt(2 ln(opacity / ALPHA_MIN)), precomputed at upload
+      }
+      float a, bb, cc;
+      conic_terms<float>(cov, t0x, t0y, t0z, t1x, t1y, t1z, a, bb, cc);
+      float det = a * cc - bb * bb;
+      float inv_det = 0.0f;
+      bool conic_done = false;
+      if (F16 && !(det >= kFp64DetBelow)) {
+        // Near-singular: the 2D covariance and its inverse in FP64.
+        double scd[3] = {sc[0], sc[1], sc[2]}, cd[6];
+        covariance_from<double>(scd, (double)q[0], (double)q[1], (double)q[2], (double)q[3], cd);
+        double ad, bd, ccd;
+        conic_terms<double>(cd, t0x, t0y, t0z, t1x, t1y, t1z, ad, bd, ccd);
+        const double detd = ad * ccd - bd * bd;
+        if (!(detd > 0.0)) break;
+        const double inv = 1.0 / detd;
+        c0 = (float)(ccd * inv);
+        c1 = (float)(-bd * inv);
+        c2 = (float)(ad * inv);
+        a = (float)ad;
+        cc = (float)ccd;
+        conic_done = true;
+        used_fp64 = true;
+      } else {
+        if (!(det > 0.0f)) break;
+        inv_det = 1.0f / det;
+      }
       const float ext_x = k * sqrtf(a);
       const float ext_y = k * sqrtf(cc);
       if (x + ext_x <= 0.0f || x - ext_x >= fp.width || y + ext_y <= 0.0f || y - ext_y >= fp.height) break;
-      col[0] = __ldg(s.color + i);
-      col[1] = __ldg(s.color + s.n + i);
-      col[2] = __ldg(s.color + 2 * s.n + i);
+      if (F16) {
+        col[0] = h2f(__ldg(s.sh16 + i));
+        col[1] = h2f(__ldg(s.sh16 + s.n + i));
+        col[2] = h2f(__ldg(s.sh16 + 2 * s.n + i));
+      } else {
+        col[0] = __ldg(s.color + i);
+        col[1] = __ldg(s.color + s.n + i);
+        col[2] = __ldg(s.color + 2 * s.n + i);
+      }
       if constexpr (DEG > 0) {
         // normalize_or_zero(p - eye)
         const float len = sqrtf((dx * dx + dy * dy) + dz * dz);
@@ -149,15 +261,22 @@ __global__ void __launch_bounds__(256) k_project(FrameParams fp, SceneDev s, Rec
           ny = dy * rcp;
           nz = dz * rcp;
         }
-        eval_sh<DEG>(s.sh, s.n, i, nx, ny, nz, col);
+        if (F16)
+          eval_sh<DEG>([&](int coef, int ch) { return h2f(__ldg(s.sh16 + (uint64_t)((coef + 1) * 3 + ch) * s.n + i)); },
+                       nx, ny, nz, col);
+        else
+          eval_sh<DEG>([&](int coef, int ch) { return __ldg(s.sh + (uint64_t)(coef * 3 + ch) * s.n + i); }, nx, ny,
+                       nz, col);
       }
       col[0] = fmaxf(col[0], 0.0f);
       col[1] = fmaxf(col[1], 0.0f);
       col[2] = fmaxf(col[2], 0.0f);
       if (!(isfinite(x) && isfinite(y) && isfinite(ext_x) && isfinite(ext_y))) break;
-      c0 = cc * inv_det;
-      c1 = (-bb) * inv_det;
-      c2 = a * inv_det;
+      if (!conic_done) {
+        c0 = cc * inv_det;
+        c1 = (-bb) * inv_det;
+        c2 = a * inv_det;
+      }
       // pixel_bbox (src/render/cpu.rs:96-102)
       const uint32_t x0 = sat_u32(fmaxf(floorf(x - ext_x), 0.0f));
       const uint32_t y0 = sat_u32(fmaxf(floorf(y - ext_y), 0.0f));
@@ -201,15 +320,26 @@ __global__ void __launch_bounds__(256) k_project(FrameParams fp, SceneDev s, Rec
   }
   const int nvis = __syncthreads_count(vis);
   if (tid == 0 && nvis) atomicAdd(&st->visible, (unsigned long long)nvis);
+  if (F16) {
+    const int n64 = __syncthreads_count(used_fp64);
+    if (tid == 0 && n64) atomicAdd(&st->fp64_conics, (unsigned)n64);
+  }
 }
 
 }  // namespace
 
 cudaError_t launch_project(const FrameParams& fp, const SceneDev& s, Record* rec, BinInfo* bin, float* dbg_proj,
-                           float* dbg_color, DevState* st, cudaStream_t stream) {
+                           float* dbg_color, DevState* st, cudaStream_t stream, uint32_t* launches) {
   if (s.n == 0) return cudaSuccess;
+  *launches += 1;
   const unsigned grid = (unsigned)((s.n + 255) / 256);
-#define SPLAT_PROJECT(D) k_project<D><<<grid, 256, 0, stream>>>(fp, s, rec, bin, dbg_proj, dbg_color, st)
+#define SPLAT_PROJECT(D)                                                                          \
+  do {                                                                                            \
+    if (s.fp16)                                                                                   \
+      k_project<D, true><<<grid, 256, 0, stream>>>(fp, s, rec, bin, dbg_proj, dbg_color, st);     \
+    else                                                                                          \
+      k_project<D, false><<<grid, 256, 0, stream>>>(fp, s, rec, bin, dbg_proj, dbg_color, st);    \
+  } while (0)
   switch (s.sh_degree) {
     case 0: SPLAT_PROJECT(0); break;
     case 1: SPLAT_PROJECT(1); break;

@@ -21,7 +21,7 @@ import numpy as np
 
 from . import _native as N
 from .camera import View
-from .scene import Scene
+from .scene import HalfScene, Scene
 
 # src/render/mod.rs:23-33
 DILATION = np.float32(0.3)
@@ -110,16 +110,25 @@ def _f32(a):
 class CudaRenderer(Renderer):
     """The sm_100a backend: uploads the scene once, renders views on `device`."""
 
-    def __init__(self, scene: Scene, device: int = 0):
+    def __init__(self, scene, device: int = 0):
+        """`scene`: a finalized Scene (FP32 storage) or a HalfScene (FP16
+        storage of scales, rotations, opacities and SH)."""
         L = N.lib()
         n = len(scene)
-        self._keep = [_f32(scene.positions), _f32(scene.opacities), _f32(scene.colors), _f32(scene.cov3d),
-                      _f32(scene.sh_rest.reshape(n, -1) if scene.sh_degree > 0 else np.zeros(1, np.float32))]
         d = N.SceneDesc()
         d.n = n
         d.sh_degree = scene.sh_degree
-        d.precision = N.SPLAT_PRECISION_FP32
-        d.positions, d.opacities, d.colors, d.cov3d, d.sh_rest = [a.ctypes.data for a in self._keep]
+        if isinstance(scene, HalfScene):
+            self._keep = [_f32(scene.positions), scene.scales, scene.rotations, scene.opacities, scene.sh]
+            d.precision = N.SPLAT_PRECISION_FP16
+            d.positions, d.scales_f16, d.rotations_f16, d.opacities_f16, d.sh_f16 = [
+                a.ctypes.data for a in self._keep]
+        else:
+            self._keep = [_f32(scene.positions), _f32(scene.opacities), _f32(scene.colors), _f32(scene.cov3d),
+                          _f32(scene.sh_rest.reshape(n, -1) if scene.sh_degree > 0 else np.zeros(1, np.float32))]
+            d.precision = N.SPLAT_PRECISION_FP32
+            d.positions, d.opacities, d.colors, d.cov3d, d.sh_rest = [a.ctypes.data for a in self._keep]
+        self.precision = d.precision
         h = ctypes.c_void_p()
         rc = L.splat_cuda_create(ctypes.byref(d), device, ctypes.byref(h))
         if rc != N.SPLAT_OK:
@@ -198,6 +207,11 @@ class CudaRenderer(Renderer):
     def set_exact(self, exact: bool):
         """Blend with the reference cpu backend's exact f32 arithmetic."""
         self.set_option(N.SPLAT_OPT_EXACT_BLEND, int(exact))
+
+    def fp64_conics(self) -> int:
+        """Splats of the last completed frame whose 2D covariance was inverted
+        in FP64 (FP16 scenes: determinant below 1e-6 in FP32)."""
+        return self.get_option(N.SPLAT_OPT_FP64_CONICS)
 
     def debug_dump(self, width: int, height: int):
         """Intermediate buffers of the last frame (needs SPLAT_OPT_DEBUG_CAPTURE):

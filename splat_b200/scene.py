@@ -142,3 +142,68 @@ class Scene:
 
         radius = f32(min(pct(0.9), f32(2.0) * pct(0.5)))
         return center, (radius if radius > f32(1e-6) else f32(1.0))
+
+    def to_fp16(self) -> "HalfScene":
+        """This scene with scales, rotations, opacities, base colours and SH
+        stored as IEEE binary16 (round to nearest even); positions stay f32."""
+        self._flush()
+        return HalfScene.from_scene(self)
+
+
+def _half_bits(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a, np.float32).astype(np.float16)).view(np.uint16)
+
+
+class HalfScene:
+    """FP16 parameter storage of a finalized scene: f32 positions (12 B), f16
+    scales (6 B), rotations x, y, z, w (8 B), opacity (2 B) and base colour +
+    SH rest, RGB innermost ((rest + 1) * 3 halves): 124 bytes per degree-3
+    splat against 232 for the f32 scene. The device forms the 3D covariance
+    from the decoded scale and rotation."""
+
+    def __init__(self, positions, scales, rotations, opacities, sh, sh_degree: int):
+        self.positions = np.ascontiguousarray(positions, np.float32)
+        self.scales = np.ascontiguousarray(scales, np.uint16)
+        self.rotations = np.ascontiguousarray(rotations, np.uint16)
+        self.opacities = np.ascontiguousarray(opacities, np.uint16)
+        self.sh = np.ascontiguousarray(sh, np.uint16)  # n x (rest + 1) x 3
+        self.sh_degree = int(sh_degree)
+
+    @classmethod
+    def from_scene(cls, s: Scene) -> "HalfScene":
+        n = len(s)
+        per = s.rest_per_splat()
+        sh = np.concatenate([np.asarray(s.colors, np.float32).reshape(n, 1, 3),
+                             np.asarray(s.sh_rest, np.float32).reshape(n, per, 3)], axis=1)
+        return cls(s.positions, _half_bits(s.scales), _half_bits(s.rotations), _half_bits(s.opacities),
+                   _half_bits(sh), s.sh_degree)
+
+    def __len__(self):
+        return len(self.positions)
+
+    def decoded(self) -> dict:
+        """The stored values widened back to f32 (exact), as arrays named like
+        Scene's: positions, scales, rotations (x, y, z, w; as stored, not
+        renormalised), opacities, colors, sh_rest, sh_degree."""
+        n = len(self)
+        h = lambda a: a.view(np.float16).astype(np.float32)  # noqa: E731
+        sh = h(self.sh).reshape(n, -1, 3)
+        return {"positions": self.positions, "scales": h(self.scales).reshape(n, 3),
+                "rotations": h(self.rotations).reshape(n, 4), "opacities": h(self.opacities).reshape(n),
+                "colors": np.ascontiguousarray(sh[:, 0, :]), "sh_rest": np.ascontiguousarray(sh[:, 1:, :]),
+                "sh_degree": self.sh_degree}
+
+    def decoded_scene(self) -> Scene:
+        """The decoded values as a finalized f32 Scene: rotation normalisation,
+        opacity clamp and covariance exactly as the device applies them to
+        the stored halves."""
+        d = self.decoded()
+        s = Scene()
+        s.positions = d["positions"].copy()
+        s.scales = d["scales"]
+        s.rotations = d["rotations"]
+        s.opacities = d["opacities"]
+        s.colors = d["colors"]
+        s.sh_degree = self.sh_degree
+        s.sh_rest = d["sh_rest"]
+        return s.finalize()

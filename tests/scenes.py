@@ -175,3 +175,20 @@ def splats(items) -> Scene:
 
 def empty() -> Scene:
     return Scene().finalize()
+
+
+def needles(n=20_000, seed=5, length=4.0, thickness=1e-4) -> Scene:
+    """Long, thin splats close to the camera at the origin looking along +z:
+    their projected 2D covariances are nearly rank one with entries ~1e7, so
+    the f32 determinant a*c - b^2 cancels and some fall below 1e-6 (the FP16
+    storage path's FP64 conic case)."""
+    rng = np.random.default_rng(seed)
+    s = Scene()
+    z = rng.uniform(0.5, 3.0, n)
+    xy = rng.uniform(-0.6, 0.6, (n, 2)) * z[:, None]
+    s.positions = np.stack([xy[:, 0], xy[:, 1], z], 1).astype(np.float32)
+    s.scales = np.tile(np.array([length, thickness, thickness], np.float32), (n, 1))
+    s.rotations = rng.normal(size=(n, 4)).astype(np.float32)
+    s.opacities = rng.uniform(0.3, 1.0, n).astype(np.float32)
+    s.colors = rng.uniform(0.0, 1.0, (n, 3)).astype(np.float32)
+    return s.finalize()

@@ -135,3 +135,34 @@ def test_synthetic_scenes_are_seeded():
     assert len(synth.lattice_scene()) == 14 ** 3
     # SplitMix64 known value: the first output for seed 0 (gen.rs:28-34).
     assert int(synth.splitmix_u64(0, 1)[0]) == 0xE220A8397B1DCDAF
+
+
+def test_scene_precision_validation_without_a_gpu(cuda_lib):
+    h = ctypes.c_void_p()
+    d = N.SceneDesc()
+    d.n = 1
+    d.precision = 7
+    assert cuda_lib.splat_cuda_create(ctypes.byref(d), 0, ctypes.byref(h)) == N.SPLAT_ERR_UNSUPPORTED
+    d.precision = N.SPLAT_PRECISION_FP16
+    assert cuda_lib.splat_cuda_create(ctypes.byref(d), 0, ctypes.byref(h)) == N.SPLAT_ERR_INVALID_ARG
+    assert b"FP16" in cuda_lib.splat_cuda_create_error()
+
+
+def test_half_scene_round_trip():
+    from splat_b200 import HalfScene  # noqa: F401
+    from tests import scenes
+
+    s = scenes.clusters(2_000, seed=3, sh_degree=2)
+    half = s.to_fp16()
+    assert half.sh.shape == (2_000, 9, 3) and half.sh.dtype == np.uint16
+    # 12 B position + 2 * (3 + 4 + 1 + 27) B of halves per degree-2 splat
+    assert half.positions.nbytes + half.scales.nbytes + half.rotations.nbytes + half.opacities.nbytes + \
+        half.sh.nbytes == 2_000 * (12 + 2 * (3 + 4 + 1 + 27))
+    d = half.decoded()
+    for k, tol in [("scales", 2 ** -11), ("opacities", 2 ** -11), ("colors", 2 ** -11), ("sh_rest", 2 ** -11)]:
+        a = np.asarray(getattr(s, k), np.float32).reshape(d[k].shape)
+        assert np.all(np.abs(d[k] - a) <= tol * np.maximum(np.abs(a), 2 ** -14)), k
+    assert np.array_equal(d["positions"], s.positions)
+    ds = half.decoded_scene()
+    scale = np.max(np.abs(s.cov3d[:, [0, 3, 5]]), axis=1, keepdims=True)  # largest variance per splat
+    assert np.all(np.abs(ds.cov3d - s.cov3d) <= 5e-3 * scale)
