@@ -183,6 +183,12 @@ void* splat_cuda_get_stream(splat_cuda_handle* h);
                                       (FP16 scenes; 0 otherwise) */
 #define SPLAT_OPT_KERNEL_LAUNCHES 6u /* kernels this handle has launched
                                         (set to reset the count) */
+#define SPLAT_OPT_BLEND_CONFIG 7u  /* tile shape and blend threads, packed as
+                                      tile_w | tile_h << 8 | threads << 16;
+                                      shapes 8x8, 16x16 (default), 32x16 and
+                                      128, 256 (default) or 512 threads. The
+                                      image does not depend on it; the keys of
+                                      splat_cuda_debug_dump use its tiles. */
 int splat_cuda_set_option(splat_cuda_handle* h, uint32_t option, uint64_t value);
 int splat_cuda_get_option(splat_cuda_handle* h, uint32_t option, uint64_t* value);
 
@@ -223,6 +229,78 @@ int splat_cuda_sort_tile_noalloc(uint64_t* words, uint32_t n, void* stream);
 
 /* Frees the handle and its device memory. NULL is ignored. */
 int splat_cuda_destroy(splat_cuda_handle* h);
+
+/*
+ * Batched rendering: many views of uneven resolution over several scenes,
+ * each stage of the pipeline one launch over all views, the whole batch
+ * recorded once as a CUDA graph and replayed by splat_cuda_batch_run. No
+ * counterpart in the reference, whose Renderer draws one view per call
+ * (src/render/mod.rs:89-96); every view's image equals what
+ * splat_cuda_render draws for it alone.
+ *
+ * The scenes are handles from splat_cuda_create on one device; they must
+ * outlive the batch and are only read. A view's frame goes to DEVICE memory
+ * dev_out (floor(width/f) * floor(height/f) * 3 bytes). The batch owns its
+ * per-view buffers, its stream and its graph; one thread at a time.
+ */
+typedef struct splat_cuda_batch splat_cuda_batch;
+
+typedef struct splat_batch_view {
+  uint32_t scene;       /* index into the scenes given at creation */
+  uint32_t width;       /* 1..16384 */
+  uint32_t height;      /* 1..16384 */
+  uint32_t downsample;  /* 0 or 1: none; else a factor dividing the tile shape */
+  splat_view_desc view;
+  float bg[3];
+  uint32_t reserved;    /* 0 */
+  uint8_t* dev_out;     /* device frame of this view */
+} splat_batch_view;
+
+/* Tile shape and threads per CTA of the blend: (8,8), (16,16) or (32,16)
+ * tiles with 128, 256 or 512 threads. */
+typedef struct splat_blend_config {
+  uint32_t tile_w, tile_h, threads;
+} splat_blend_config;
+
+typedef struct splat_tune_result {
+  splat_blend_config config;
+  uint32_t reserved;
+  double ms;            /* mean device time of one batch (graph launch) */
+} splat_tune_result;
+
+/* Plans the batch with the default configuration (16x16 tiles, 256
+ * threads), runs it once to size the pair buffers and records the graph. */
+int splat_cuda_batch_create(splat_cuda_handle* const* scenes, uint32_t n_scenes, const splat_batch_view* views,
+                            uint32_t n_views, splat_cuda_batch** out);
+/* Text describing why the last splat_cuda_batch_create of this thread failed. */
+const char* splat_cuda_batch_create_error(void);
+/* Re-plans and re-records the batch for another blend configuration. */
+int splat_cuda_batch_set_config(splat_cuda_batch* b, const splat_blend_config* config);
+int splat_cuda_batch_get_config(const splat_cuda_batch* b, splat_blend_config* config);
+/* The tuner: times `reps` graph launches of every supported configuration
+ * (after one warm-up launch each), keeps the fastest and re-records the
+ * batch with it. Writes up to `capacity` results (all configurations tried,
+ * in the order tried) and their number to *n_results. */
+int splat_cuda_batch_autotune(splat_cuda_batch* b, uint32_t reps, splat_tune_result* results, uint32_t capacity,
+                              uint32_t* n_results);
+/* Launches the recorded graph on the batch's stream; does not wait. */
+int splat_cuda_batch_run(splat_cuda_batch* b);
+/* Waits for the launched batches; per_view (n_views entries, may be NULL)
+ * gets each view's visible splats and pairs, total_ms (may be NULL) the
+ * device time of the last batch. *regrown = 1 when a batch overflowed the
+ * pair buffers: they have been grown and the graph re-recorded; run again. */
+int splat_cuda_batch_finish(splat_cuda_batch* b, splat_render_stats* per_view, double* total_ms, int* regrown);
+/* Options: SPLAT_OPT_EXACT_BLEND and SPLAT_OPT_KERNEL_LAUNCHES as for a
+ * renderer (setting EXACT_BLEND re-records the graph). */
+int splat_cuda_batch_set_option(splat_cuda_batch* b, uint32_t option, uint64_t value);
+int splat_cuda_batch_get_option(const splat_cuda_batch* b, uint32_t option, uint64_t* value);
+/* Uses `stream` (NULL: the batch's own) for later launches of the graph. */
+int splat_cuda_batch_set_stream(splat_cuda_batch* b, void* stream);
+void* splat_cuda_batch_get_stream(const splat_cuda_batch* b);
+/* Text describing the last failure on this batch ("" if none). */
+const char* splat_cuda_batch_last_error(const splat_cuda_batch* b);
+/* Frees the batch (not its scenes). NULL is ignored. */
+int splat_cuda_batch_destroy(splat_cuda_batch* b);
 
 /* Text describing the last failure on this handle ("" if none). */
 const char* splat_cuda_last_error(const splat_cuda_handle* h);

@@ -64,8 +64,8 @@ def lib():
         L.oracle_cpu_threads.argtypes = [ctypes.c_void_p]
         L.oracle_cpu_threads.restype = ctypes.c_uint32
         L.oracle_cpu_destroy.argtypes = [ctypes.c_void_p]
-        L.oracle_bin_sort.argtypes = [ctypes.c_uint64] + [_f32p] * 5 + [_u8p, ctypes.c_uint32, ctypes.c_uint32,
-                                                                         _u64p, _u32p, ctypes.c_uint64, _u32p]
+        L.oracle_bin_sort.argtypes = [ctypes.c_uint64] + [_f32p] * 5 + [_u8p] + [ctypes.c_uint32] * 4 + [
+            _u64p, _u32p, ctypes.c_uint64, _u32p]
         L.oracle_bin_sort.restype = ctypes.c_int64
         _lib = L
     return _lib
@@ -259,20 +259,21 @@ class CpuTiled:
             pass
 
 
-def bin_sort(x, y, ext_x, ext_y, depth, visible, w, h, cap=None):
+def bin_sort(x, y, ext_x, ext_y, depth, visible, w, h, cap=None, tile=(16, 16)):
     """CPU recomputation of sorted (tile<<32 | depth bits) keys, splat values and
-    per-tile [begin, end) ranges from projected values."""
+    per-tile [begin, end) ranges from projected values (tile_w x tile_h tiles)."""
     n = len(x)
     arrs = [_f32(a) for a in (x, y, ext_x, ext_y, depth)]
     vis = np.ascontiguousarray(visible, dtype=np.uint8)
-    tiles = ((w + 15) // 16) * ((h + 15) // 16)
+    tw, th = tile
+    tiles = ((w + tw - 1) // tw) * ((h + th - 1) // th)
     if cap is None:
         cap = max(16, int(np.sum(vis)) * 64)
     while True:
         keys = np.zeros(cap, np.uint64)
         vals = np.zeros(cap, np.uint32)
         ranges = np.zeros(2 * tiles, np.uint32)
-        p = lib().oracle_bin_sort(n, *[_p(a, _f32p) for a in arrs], _p(vis, _u8p), w, h, _p(keys, _u64p),
+        p = lib().oracle_bin_sort(n, *[_p(a, _f32p) for a in arrs], _p(vis, _u8p), w, h, tw, th, _p(keys, _u64p),
                                   _p(vals, _u32p), cap, _p(ranges, _u32p))
         if p >= 0:
             return keys[:p], vals[:p], ranges.reshape(tiles, 2)

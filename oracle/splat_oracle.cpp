@@ -1108,17 +1108,18 @@ void oracle_cpu_destroy(void* handle) { delete static_cast<CpuTiled*>(handle); }
 // pair per tile of each visible splat's pixel_bbox, row-major, in splat-index
 // order (src/render/cpu.rs:251-277), then sort stably by key. ranges holds
 // [begin, end) per tile. Returns the pair count, or -1 if it exceeds cap.
+// tile_w x tile_h tiles (the reference's are 16 x 16).
 int64_t oracle_bin_sort(uint64_t n, const float* x, const float* y, const float* ext_x, const float* ext_y,
-                        const float* depth, const uint8_t* visible, uint32_t w, uint32_t h, uint64_t* keys,
-                        uint32_t* values, uint64_t cap, uint32_t* ranges) {
-  uint32_t tiles_x = (w + TILE - 1) / TILE, tiles_y = (h + TILE - 1) / TILE;
+                        const float* depth, const uint8_t* visible, uint32_t w, uint32_t h, uint32_t tile_w,
+                        uint32_t tile_h, uint64_t* keys, uint32_t* values, uint64_t cap, uint32_t* ranges) {
+  uint32_t tiles_x = (w + tile_w - 1) / tile_w, tiles_y = (h + tile_h - 1) / tile_h;
   std::vector<std::pair<uint64_t, uint32_t>> pairs;
   for (size_t i = 0; i < n; i++) {
     if (!visible[i]) continue;
     BBox bb = pixel_bbox(x[i], y[i], ext_x[i], ext_y[i], w, h);
     if (bb.x0 >= bb.x1 || bb.y0 >= bb.y1) continue;
-    uint32_t tx0 = bb.x0 / TILE, ty0 = bb.y0 / TILE;
-    uint32_t tx1 = (bb.x1 + TILE - 1) / TILE, ty1 = (bb.y1 + TILE - 1) / TILE;
+    uint32_t tx0 = bb.x0 / tile_w, ty0 = bb.y0 / tile_h;
+    uint32_t tx1 = (bb.x1 + tile_w - 1) / tile_w, ty1 = (bb.y1 + tile_h - 1) / tile_h;
     for (uint32_t ty = ty0; ty < ty1; ty++)
       for (uint32_t tx = tx0; tx < tx1; tx++)
         pairs.push_back({((uint64_t)(ty * tiles_x + tx) << 32) | f2u(depth[i]), (uint32_t)i});

@@ -29,6 +29,7 @@ SPLAT_OPT_STAGE_EVENTS = 3
 SPLAT_OPT_DEBUG_CAPTURE = 4
 SPLAT_OPT_FP64_CONICS = 5
 SPLAT_OPT_KERNEL_LAUNCHES = 6
+SPLAT_OPT_BLEND_CONFIG = 7
 
 _STATUS_NAMES = {0: "OK", 1: "INVALID_ARG", 2: "OOM", 3: "CAPACITY", 4: "DEVICE", 5: "TIMEOUT", 6: "UNSUPPORTED"}
 
@@ -38,6 +39,10 @@ EXPORTS = [
     "splat_cuda_render", "splat_cuda_render_device", "splat_cuda_finish", "splat_cuda_set_stream",
     "splat_cuda_get_stream", "splat_cuda_set_option", "splat_cuda_get_option", "splat_cuda_debug_dump",
     "splat_cuda_destroy", "splat_cuda_last_error", "splat_cuda_sort_tile_noalloc",
+    "splat_cuda_batch_create", "splat_cuda_batch_create_error", "splat_cuda_batch_set_config",
+    "splat_cuda_batch_get_config", "splat_cuda_batch_autotune", "splat_cuda_batch_run", "splat_cuda_batch_finish",
+    "splat_cuda_batch_set_option", "splat_cuda_batch_get_option", "splat_cuda_batch_set_stream",
+    "splat_cuda_batch_get_stream", "splat_cuda_batch_last_error", "splat_cuda_batch_destroy",
 ]
 
 
@@ -59,6 +64,20 @@ class SceneDesc(ctypes.Structure):
 class ViewDesc(ctypes.Structure):
     _fields_ = [("eye", ctypes.c_float * 3), ("right", ctypes.c_float * 3), ("down", ctypes.c_float * 3),
                 ("forward", ctypes.c_float * 3), ("fov_y", ctypes.c_float), ("near_plane", ctypes.c_float)]
+
+
+class BatchViewC(ctypes.Structure):
+    _fields_ = [("scene", ctypes.c_uint32), ("width", ctypes.c_uint32), ("height", ctypes.c_uint32),
+                ("downsample", ctypes.c_uint32), ("view", ViewDesc), ("bg", ctypes.c_float * 3),
+                ("reserved", ctypes.c_uint32), ("dev_out", ctypes.c_void_p)]
+
+
+class BlendConfigC(ctypes.Structure):
+    _fields_ = [("tile_w", ctypes.c_uint32), ("tile_h", ctypes.c_uint32), ("threads", ctypes.c_uint32)]
+
+
+class TuneResultC(ctypes.Structure):
+    _fields_ = [("config", BlendConfigC), ("reserved", ctypes.c_uint32), ("ms", ctypes.c_double)]
 
 
 class RenderStatsC(ctypes.Structure):
@@ -97,11 +116,42 @@ def lib():
         L.splat_cuda_sort_tile_noalloc.argtypes = [vp, u32, vp]
         L.splat_cuda_last_error.argtypes = [vp]
         L.splat_cuda_last_error.restype = ctypes.c_char_p
+        L.splat_cuda_batch_create.argtypes = [ctypes.POINTER(vp), u32, ctypes.POINTER(BatchViewC), u32,
+                                              ctypes.POINTER(vp)]
+        L.splat_cuda_batch_create_error.restype = ctypes.c_char_p
+        L.splat_cuda_batch_set_config.argtypes = [vp, ctypes.POINTER(BlendConfigC)]
+        L.splat_cuda_batch_get_config.argtypes = [vp, ctypes.POINTER(BlendConfigC)]
+        L.splat_cuda_batch_autotune.argtypes = [vp, u32, ctypes.POINTER(TuneResultC), u32, ctypes.POINTER(u32)]
+        L.splat_cuda_batch_run.argtypes = [vp]
+        L.splat_cuda_batch_finish.argtypes = [vp, ctypes.POINTER(RenderStatsC), ctypes.POINTER(ctypes.c_double),
+                                              ctypes.POINTER(ctypes.c_int)]
+        L.splat_cuda_batch_set_option.argtypes = [vp, u32, u64]
+        L.splat_cuda_batch_get_option.argtypes = [vp, u32, ctypes.POINTER(u64)]
+        L.splat_cuda_batch_set_stream.argtypes = [vp, vp]
+        L.splat_cuda_batch_get_stream.argtypes = [vp]
+        L.splat_cuda_batch_get_stream.restype = vp
+        L.splat_cuda_batch_last_error.argtypes = [vp]
+        L.splat_cuda_batch_last_error.restype = ctypes.c_char_p
+        L.splat_cuda_batch_destroy.argtypes = [vp]
         _lib = L
     return _lib
 
 
-def check(rc: int, handle=None, what: str = ""):
+def check(rc: int, handle=None, what: str = "", batch=None):
     if rc != SPLAT_OK:
-        msg = lib().splat_cuda_last_error(handle).decode() if handle else ""
+        if handle:
+            msg = lib().splat_cuda_last_error(handle).decode()
+        elif batch:
+            msg = lib().splat_cuda_batch_last_error(batch).decode()
+        else:
+            msg = ""
         raise SplatError(rc, f"{what}: {msg}" if what else msg)
+
+
+def pack_blend_config(tile_w: int, tile_h: int, threads: int) -> int:
+    """SPLAT_OPT_BLEND_CONFIG value."""
+    return int(tile_w) | (int(tile_h) << 8) | (int(threads) << 16)
+
+
+BLEND_CONFIGS = [(16, 16, 256), (16, 16, 128), (16, 16, 512), (8, 8, 128), (8, 8, 256), (8, 8, 512),
+                 (32, 16, 128), (32, 16, 256), (32, 16, 512)]

@@ -29,8 +29,9 @@ SOURCES = {
     "binning.cu": [],
     "blend.cu": [],
     "noalloc.cu": [],
+    "batch.cu": [],
 }
-HEADERS = [os.path.join(CSRC, "common.cuh"), os.path.join(CSRC, "tilesort.cuh"),
+HEADERS = [os.path.join(CSRC, "common.cuh"), os.path.join(CSRC, "tilesort.cuh"), os.path.join(CSRC, "handle.h"),
            os.path.join(ROOT, "include", "splat_cuda.h")]
 
 

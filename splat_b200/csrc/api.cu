@@ -18,65 +18,11 @@
 
 #include "../../include/splat_cuda.h"
 #include "common.cuh"
+#include "handle.h"
 
 #define SPLAT_API extern "C" __attribute__((visibility("default")))
 
 using namespace splat;
-
-struct splat_cuda_handle {
-  int device = 0;
-  int num_sms = 148;
-  cudaStream_t own_stream = nullptr;
-  cudaStream_t stream = nullptr;
-  uint64_t n = 0;
-  uint32_t sh_degree = 0;
-  uint32_t precision = SPLAT_PRECISION_FP32;
-  // scene (device)
-  float4* pos_op = nullptr;
-  float4* cov_a = nullptr;
-  float4* cov_b = nullptr;
-  float* color = nullptr;
-  float* sh = nullptr;
-  float4* pos_k = nullptr;   // FP16 storage: x, y, z, k
-  uint4* geom16 = nullptr;   // FP16 storage: scale, rotation, opacity halves
-  uint16_t* sh16 = nullptr;  // FP16 storage: base colour + SH planes
-  // per-splat frame buffers
-  Record* rec = nullptr;
-  BinInfo* bin = nullptr;
-  // pair buffers: per-tile buckets and the long-tile sort's scratch
-  uint64_t cap = 0;
-  uint64_t* pairs[2] = {nullptr, nullptr};
-  // per-size buffers
-  uint2* ranges = nullptr;
-  uint32_t* counts = nullptr;     // bin_rows x tiles
-  uint32_t* totals = nullptr;     // tiles
-  uint32_t* mid_list = nullptr;   // tiles
-  uint32_t* long_list = nullptr;  // tiles
-  uint64_t ranges_cap = 0;        // tiles
-  size_t max_smem = 48 * 1024;
-  uint8_t* out_dev = nullptr;
-  size_t out_cap = 0;
-  uint8_t* full_dev = nullptr;
-  size_t full_cap = 0;
-  // frame state
-  DevState* st = nullptr;
-  DevState* st_host = nullptr;  // pinned
-  uint8_t* stage = nullptr;     // pinned staging for pageable outputs
-  size_t stage_cap = 0;
-  // debug capture
-  float* dbg_proj = nullptr;
-  float* dbg_color = nullptr;
-  bool debug_capture = false;
-  // options
-  bool exact = false;
-  bool stage_events = true;
-  uint32_t launches = 0;  // kernels this handle has launched (wraps at 2^32)
-  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
-  // last frame
-  FrameParams last_fp{};
-  bool have_frame = false;
-  std::string err;
-};
 
 namespace {
 
@@ -142,20 +88,32 @@ int ensure_pairs(splat_cuda_handle* h, uint64_t cap) {
   return SPLAT_OK;
 }
 
-int ensure_size(splat_cuda_handle* h, uint64_t tiles, size_t out_bytes, size_t full_bytes) {
+int ensure_size(splat_cuda_handle* h, uint64_t tiles, uint32_t rows, size_t out_bytes, size_t full_bytes) {
   if (tiles > h->ranges_cap) {
     dfree(h->ranges);
-    dfree(h->counts);
     dfree(h->totals);
     dfree(h->mid_list);
     dfree(h->long_list);
     h->ranges_cap = 0;
     CK(cudaMalloc(&h->ranges, tiles * sizeof(uint2)), "cudaMalloc ranges");
-    CK(cudaMalloc(&h->counts, (size_t)bin_rows(h->num_sms) * tiles * sizeof(uint32_t)), "cudaMalloc counts");
     CK(cudaMalloc(&h->totals, tiles * sizeof(uint32_t)), "cudaMalloc totals");
     CK(cudaMalloc(&h->mid_list, tiles * sizeof(uint32_t)), "cudaMalloc mid tiles");
     CK(cudaMalloc(&h->long_list, tiles * sizeof(uint32_t)), "cudaMalloc long tiles");
     h->ranges_cap = tiles;
+  }
+  const size_t words = (size_t)rows * tiles;
+  if (words > h->counts_cap) {
+    dfree(h->counts);
+    h->counts_cap = 0;
+    CK(cudaMalloc(&h->counts, words * sizeof(uint32_t)), "cudaMalloc counts");
+    h->counts_cap = words;
+  }
+  const uint32_t chunks = (uint32_t)((tiles + kScanChunk - 1) / kScanChunk);
+  if (chunks > h->chunks_cap || !h->st) {
+    dfree(h->st);
+    h->chunks_cap = 0;
+    CK(cudaMalloc(&h->st, frame_counters_bytes(1, std::max(chunks, 1u))), "cudaMalloc frame counters");
+    h->chunks_cap = std::max(chunks, 1u);
   }
   if (out_bytes > h->out_cap) {
     dfree(h->out_dev);
@@ -169,6 +127,19 @@ int ensure_size(splat_cuda_handle* h, uint64_t tiles, size_t out_bytes, size_t f
   }
   return SPLAT_OK;
 }
+
+bool is_pinned_host(const void* p) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+}  // namespace
+
+namespace splat {
 
 // ProjectCtx::new (src/render/mod.rs:169-196) with View::rotation/focal
 // (src/camera.rs:172-181), in f32 exactly as the reference computes it.
@@ -196,48 +167,78 @@ FrameParams make_params(const splat_view_desc& v, uint32_t w, uint32_t hgt, cons
   p.lim_y = lim(fh * 0.5f);
   p.w = w;
   p.h = hgt;
-  p.tiles_x = (w + kTile - 1) / kTile;
-  p.tiles_y = (hgt + kTile - 1) / kTile;
   p.downsample = f;
   p.out_w = w / f;
   p.out_h = hgt / f;
   return p;
 }
 
-bool is_pinned_host(const void* p) {
-  cudaPointerAttributes a{};
-  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
-    cudaGetLastError();
-    return false;
-  }
-  return a.type == cudaMemoryTypeHost;
+SceneDev scene_dev(const splat_cuda_handle* h) {
+  return SceneDev{h->pos_op, h->cov_a, h->cov_b, h->color, h->sh, h->pos_k, h->geom16, h->sh16, h->n, h->sh_degree,
+                  h->precision == SPLAT_PRECISION_FP16 ? 1u : 0u};
 }
 
+// Tile shape of a frame: sets tile_w/h, their logs and the tile grid.
+void set_tile_shape(FrameParams& p, uint32_t tile_w, uint32_t tile_h) {
+  p.tile_w = tile_w;
+  p.tile_h = tile_h;
+  p.tile_sx = (uint32_t)__builtin_ctz(tile_w);
+  p.tile_sy = (uint32_t)__builtin_ctz(tile_h);
+  p.tiles_x = (p.w + tile_w - 1) / tile_w;
+  p.tiles_y = (p.h + tile_h - 1) / tile_h;
+}
+
+}  // namespace splat
+
+namespace {
+
 // Enqueues one frame into dev_out (no host synchronisation).
-int enqueue_frame(splat_cuda_handle* h, const FrameParams& fp, uint8_t* dev_out) {
+int enqueue_frame(splat_cuda_handle* h, const FrameParams& fp_in, uint8_t* dev_out) {
+  FrameParams fp = fp_in;
+  set_tile_shape(fp, h->blend.tile_w, h->blend.tile_h);
   const uint64_t tiles = (uint64_t)fp.tiles_x * fp.tiles_y;
-  const size_t full_bytes = (fp.downsample > 1 && kTile % fp.downsample != 0) ? (size_t)fp.w * fp.h * 3 : 0;
-  int rc = ensure_size(h, tiles, 0, full_bytes);
+  const uint32_t f = fp.downsample;
+  const bool scratch = f > 1 && (fp.tile_w % f != 0 || fp.tile_h % f != 0);
+  const size_t full_bytes = scratch ? (size_t)fp.w * fp.h * 3 : 0;
+  const uint32_t rows = bin_rows(h->n, h->num_sms);
+  int rc = ensure_size(h, tiles, rows, 0, full_bytes);
   if (rc) return rc;
+  const uint32_t chunks = (uint32_t)((tiles + kScanChunk - 1) / kScanChunk);
   cudaStream_t s = h->stream;
-  CK(cudaMemsetAsync(h->st, 0, sizeof(DevState), s), "clear frame state");
+  CK(cudaMemsetAsync(h->st, 0, frame_counters_bytes(1, chunks), s), "clear frame state");
+  const FrameCounters fc = frame_counters_at(h->st, 1);
+  ViewTask t{};
+  t.fp = fp;
+  t.s = scene_dev(h);
+  t.rec = h->rec;
+  t.bin = h->bin;
+  t.counts = h->counts;
+  t.out = dev_out;
+  t.full = scratch ? h->full_dev : nullptr;
+  t.rows = rows;
   if (h->stage_events) CK(cudaEventRecord(h->ev[0], s), "event");
-  if (h->n) {
-    SceneDev sd{h->pos_op, h->cov_a, h->cov_b, h->color, h->sh, h->pos_k, h->geom16, h->sh16, h->n, h->sh_degree,
-                h->precision == SPLAT_PRECISION_FP16 ? 1u : 0u};
-    CK(launch_project(fp, sd, h->rec, h->bin, h->debug_capture ? h->dbg_proj : nullptr,
-                      h->debug_capture ? h->dbg_color : nullptr, h->st, s, &h->launches),
-       "project kernel");
-  }
+  CK(launch_project(t, h->table, h->debug_capture ? h->dbg_proj : nullptr, h->debug_capture ? h->dbg_color : nullptr,
+                    fc, s, &h->launches),
+     "project kernel");
   if (h->stage_events) CK(cudaEventRecord(h->ev[1], s), "event");
-  CK(launch_binning(fp, h->bin, h->n, h->counts, h->totals, h->ranges, h->mid_list, h->long_list, h->pairs[0],
-                    h->pairs[1], h->cap, h->st, h->num_sms, h->max_smem, s, &h->launches),
+  BinLaunch bl{};
+  bl.n_views = 1;
+  bl.bin_ctas = rows;
+  bl.col_ctas = (uint32_t)((tiles + 31) / 32);
+  bl.n_tiles = (uint32_t)tiles;
+  bl.max_tiles = (uint32_t)tiles;
+  bl.counts_all = h->counts;
+  bl.counts_bytes = (size_t)rows * tiles * sizeof(uint32_t);
+  CK(launch_binning(h->table, bl, h->totals, h->ranges, h->mid_list, h->long_list, h->pairs[0], h->pairs[1], h->cap,
+                    fc, h->num_sms, h->max_smem, s, &h->launches),
      "binning kernels");
   if (h->stage_events) CK(cudaEventRecord(h->ev[2], s), "event");
-  CK(launch_blend(fp, h->rec, h->pairs[0], h->ranges, h->exact, dev_out, h->full_dev, s, &h->launches),
+  CK(launch_blend(h->table, 1, (uint32_t)tiles, h->pairs[0], h->ranges, h->exact, h->blend, fc.st, h->num_sms, s,
+                  &h->launches),
      "blend kernel");
+  if (scratch) CK(launch_downsample(fp, h->full_dev, dev_out, s, &h->launches), "downsample kernel");
   if (h->stage_events) CK(cudaEventRecord(h->ev[3], s), "event");
-  CK(cudaMemcpyAsync(h->st_host, h->st, sizeof(DevState), cudaMemcpyDeviceToHost, s), "copy frame state");
+  CK(cudaMemcpyAsync(h->st_host, h->st, frame_counters_bytes(1, 0), cudaMemcpyDeviceToHost, s), "copy frame state");
   h->last_fp = fp;
   return SPLAT_OK;
 }
@@ -345,10 +346,10 @@ SPLAT_API int splat_cuda_create(const splat_scene_desc* d, int device, splat_cud
   h->stream = h->own_stream;
   for (auto& ev : h->ev)
     if ((e = cudaEventCreate(&ev)) != cudaSuccess) return bail(cuda_fail(h, e, "cudaEventCreate"));
-  if ((e = cudaMalloc(&h->st, sizeof(DevState))) != cudaSuccess) return bail(cuda_fail(h, e, "cudaMalloc state"));
-  if ((e = cudaMallocHost(&h->st_host, sizeof(DevState))) != cudaSuccess)
+  if ((e = cudaMalloc(&h->table, sizeof(ViewTask))) != cudaSuccess) return bail(cuda_fail(h, e, "cudaMalloc views"));
+  if ((e = cudaMallocHost(&h->st_host, frame_counters_bytes(1, 0))) != cudaSuccess)
     return bail(cuda_fail(h, e, "cudaMallocHost state"));
-  std::memset(h->st_host, 0, sizeof(DevState));
+  std::memset(h->st_host, 0, frame_counters_bytes(1, 0));
 
   if (n && f16) {
     // FP16 layout, 128 bytes per splat: float4 (pos, k); 8 halves (scale xyz,
@@ -463,7 +464,7 @@ SPLAT_API int splat_cuda_render(splat_cuda_handle* h, const splat_view_desc* vie
   const uint32_t f = downsample ? downsample : 1;
   const FrameParams fp = make_params(*view, width, height, bg, f);
   const size_t bytes = (size_t)fp.out_w * fp.out_h * 3;
-  if ((rc = ensure_size(h, 0, bytes, 0))) return rc;
+  if ((rc = ensure_size(h, 0, 0, bytes, 0))) return rc;
   const bool direct = bytes && is_pinned_host(rgb_out);
   if (!direct && bytes > h->stage_cap) {
     if (h->stage) cudaFreeHost(h->stage);
@@ -518,6 +519,12 @@ SPLAT_API int splat_cuda_set_option(splat_cuda_handle* h, uint32_t option, uint6
     case SPLAT_OPT_KERNEL_LAUNCHES:
       h->launches = (uint32_t)value;
       return SPLAT_OK;
+    case SPLAT_OPT_BLEND_CONFIG: {
+      const BlendConfig c{(uint32_t)(value & 0xFF), (uint32_t)((value >> 8) & 0xFF), (uint32_t)(value >> 16)};
+      if (!blend_config_supported(c)) return fail(h, SPLAT_ERR_UNSUPPORTED, "unsupported tile shape or thread count");
+      h->blend = c;
+      return SPLAT_OK;
+    }
     case SPLAT_OPT_DEBUG_CAPTURE: {
       h->debug_capture = value != 0;
       if (h->debug_capture && h->n && !h->dbg_proj) {
@@ -540,6 +547,9 @@ SPLAT_API int splat_cuda_get_option(splat_cuda_handle* h, uint32_t option, uint6
     case SPLAT_OPT_DEBUG_CAPTURE: *value = h->debug_capture; return SPLAT_OK;
     case SPLAT_OPT_FP64_CONICS: *value = h->have_frame ? h->st_host->fp64_conics : 0; return SPLAT_OK;
     case SPLAT_OPT_KERNEL_LAUNCHES: *value = h->launches; return SPLAT_OK;
+    case SPLAT_OPT_BLEND_CONFIG:
+      *value = h->blend.tile_w | (h->blend.tile_h << 8) | ((uint64_t)h->blend.threads << 16);
+      return SPLAT_OK;
     default: return fail(h, SPLAT_ERR_UNSUPPORTED, "unknown option");
   }
 }
@@ -612,6 +622,7 @@ SPLAT_API int splat_cuda_destroy(splat_cuda_handle* h) {
   dfree(h->out_dev);
   dfree(h->full_dev);
   dfree(h->st);
+  dfree(h->table);
   dfree(h->dbg_proj);
   dfree(h->dbg_color);
   if (h->st_host) cudaFreeHost(h->st_host);

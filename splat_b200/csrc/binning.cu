@@ -9,15 +9,26 @@
 //  k_bin_count    each CTA counts the pairs of its slice of splats per tile
 //                 in shared memory and writes its row of the count matrix;
 //  k_bin_colscan  per tile, an exclusive scan of the counts down the rows;
-//  k_bin_tilescan an exclusive scan of the tile totals: the tile ranges
-//                 ([begin, end); [0, 0) for an empty tile) and the list of
-//                 tiles longer than the blend CTA sorts itself;
+//                 tile totals, and their sums per chunk of kScanChunk tiles;
+//  k_tile_ranges  per chunk, an exclusive scan of the tile totals offset by
+//                 the preceding chunks: the tile ranges ([begin, end); [0, 0)
+//                 for an empty tile) and the lists of tiles too long for a
+//                 warp sort;
 //  k_bin_scatter  each CTA writes its pairs at its row's offsets, positions
 //                 handed out by shared-memory atomics.
+//
+// Every launch covers all views of the view table: the tiles of the views
+// are concatenated (each view's first tile aligned to kTileAlign) into one
+// global tile space, so the ranges, the pair buffer and the sorts are shared
+// by the views; a CTA of the count, column-scan and scatter launches finds
+// its view by binary search over the views' first CTA.
 //
 // A pair is the word depth bits << 32 | splat index. Order inside a bucket is
 // whatever the atomics produced; the per-tile depth sort that follows (in the
 // blend CTA, or k_sort_long for long tiles) restores the reference's order.
+#include <algorithm>
+#include <cstddef>
+
 #include "common.cuh"
 #include "tilesort.cuh"
 
@@ -66,40 +77,67 @@ __device__ __forceinline__ void for_each_pair(const BinInfo* __restrict__ bin, u
   }
 }
 
+// The per-view fields the count and scatter CTAs need.
+struct BinView {
+  const BinInfo* bin;
+  uint32_t* row;  // this CTA's row of the view's count matrix
+  uint64_t s0, s1;
+  uint32_t tiles_x, tiles, tile0;
+};
+
+__device__ __forceinline__ BinView bin_view(const ViewTask* __restrict__ table, uint32_t n_views) {
+  const uint32_t v = find_view(table, n_views, blockIdx.x, offsetof(ViewTask, bin_cta0));
+  const ViewTask* t = table + v;
+  BinView b;
+  b.bin = t->bin;
+  b.tiles_x = t->fp.tiles_x;
+  b.tiles = t->fp.tiles_x * t->fp.tiles_y;
+  b.tile0 = t->tile0;
+  const uint32_t r = blockIdx.x - t->bin_cta0, rows = t->rows;
+  const uint64_t n = t->s.n, per_cta = n ? (n + rows - 1) / rows : 1;
+  b.row = t->counts + (uint64_t)r * b.tiles;
+  b.s0 = min(n, (uint64_t)r * per_cta);
+  b.s1 = min(n, b.s0 + per_cta);
+  return b;
+}
+
 // SMEM: the CTA's row lives in shared memory (tiles * 4 bytes); otherwise the
 // CTA counts straight into its global row (zeroed beforehand).
 template <bool SMEM>
-__global__ void __launch_bounds__(kBinThreads) k_bin_count(const BinInfo* __restrict__ bin, uint64_t n,
-                                                           uint64_t per_cta, uint32_t tiles_x, uint32_t tiles,
-                                                           uint32_t* __restrict__ counts) {
+__global__ void __launch_bounds__(kBinThreads) k_bin_count(const ViewTask* __restrict__ table, uint32_t n_views) {
   extern __shared__ uint32_t s_row[];
-  uint32_t* row = counts + (uint64_t)blockIdx.x * tiles;
+  const BinView b = bin_view(table, n_views);
   if (SMEM) {
-    for (uint32_t t = threadIdx.x; t < tiles; t += kBinThreads) s_row[t] = 0u;
+    for (uint32_t t = threadIdx.x; t < b.tiles; t += kBinThreads) s_row[t] = 0u;
     __syncthreads();
   }
-  const uint64_t s0 = min(n, (uint64_t)blockIdx.x * per_cta), s1 = min(n, s0 + per_cta);
-  for_each_pair(bin, s0, s1, tiles_x, [&](uint32_t t, uint32_t, uint32_t) {
+  for_each_pair(b.bin, b.s0, b.s1, b.tiles_x, [&](uint32_t t, uint32_t, uint32_t) {
     if (SMEM)
       atomicAdd(&s_row[t], 1u);
     else
-      atomicAdd(&row[t], 1u);
+      atomicAdd(&b.row[t], 1u);
   });
   if (SMEM) {
     __syncthreads();
-    for (uint32_t t = threadIdx.x; t < tiles; t += kBinThreads) row[t] = s_row[t];
+    for (uint32_t t = threadIdx.x; t < b.tiles; t += kBinThreads) b.row[t] = s_row[t];
   }
 }
 
 // Per tile: exclusive scan of the counts down the rows; the tile's total.
-// A CTA takes 32 tiles; its 8 warps each scan a contiguous eighth of the rows
-// (a warp reads 32 adjacent tiles of a row: coalesced), then the segment sums
-// are combined and the rows rewritten with exclusive offsets.
-__global__ void __launch_bounds__(256) k_bin_colscan(uint32_t* __restrict__ counts, uint32_t rows, uint32_t tiles,
-                                                     uint32_t* __restrict__ totals) {
+// A CTA takes 32 tiles of one view; its 8 warps each scan a contiguous eighth
+// of the rows (a warp reads 32 adjacent tiles of a row: coalesced), then the
+// segment sums are combined and the rows rewritten with exclusive offsets.
+// The CTA's pair total goes to its scan chunk and to its view.
+__global__ void __launch_bounds__(256) k_bin_colscan(const ViewTask* __restrict__ table, uint32_t n_views,
+                                                     uint32_t* __restrict__ totals, FrameCounters fc) {
   __shared__ uint32_t s_seg[8][32];
+  const uint32_t v = find_view(table, n_views, blockIdx.x, offsetof(ViewTask, col_cta0));
+  const ViewTask* tv = table + v;
+  uint32_t* counts = tv->counts;
+  const uint32_t rows = tv->rows, tiles = tv->fp.tiles_x * tv->fp.tiles_y;
+  const uint32_t first = (blockIdx.x - tv->col_cta0) * 32, tile0 = tv->tile0;
   const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const uint32_t t = blockIdx.x * 32 + lane;
+  const uint32_t t = first + lane;
   const uint32_t per = (rows + 7) / 8;
   const uint32_t r0 = min(rows, warp * per), r1 = min(rows, r0 + per);
   uint32_t sum = 0;
@@ -114,89 +152,114 @@ __global__ void __launch_bounds__(256) k_bin_colscan(uint32_t* __restrict__ coun
   }
   if (t < tiles) {
     for (uint32_t r = r0; r < r1; r++) {
-      const uint32_t v = counts[(uint64_t)r * tiles + t];
+      const uint32_t c = counts[(uint64_t)r * tiles + t];
       counts[(uint64_t)r * tiles + t] = run;
-      run += v;
+      run += c;
     }
-    if (warp == 0) totals[t] = total;
+    if (warp == 0) totals[tile0 + t] = total;
+  }
+  if (warp == 0) {
+    unsigned long long cta = t < tiles ? total : 0u;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) cta += __shfl_xor_sync(0xffffffffu, cta, o);
+    if (lane == 0 && cta) {
+      // tile0 and first are multiples of 32, so the CTA's tiles share a chunk.
+      atomicAdd(&fc.chunk_sum[(tile0 + first) / kScanChunk], cta);
+      atomicAdd(&fc.view_pairs[v], cta);
+    }
   }
 }
 
-// One CTA: exclusive scan of the tile totals -> ranges, total pairs, and the
-// lists of tiles sorted by a whole CTA (mid) or in chunks (long).
-__global__ void __launch_bounds__(1024) k_bin_tilescan(const uint32_t* __restrict__ totals, uint32_t tiles,
-                                                       uint64_t cap, uint2* __restrict__ ranges,
-                                                       uint32_t* __restrict__ mid_list,
-                                                       uint32_t* __restrict__ long_list, DevState* st) {
-  __shared__ unsigned long long s_warp[32];
+// One CTA per chunk of kScanChunk global tiles: exclusive scan of the tile
+// totals offset by the sum of the preceding chunks -> ranges, the lists of
+// tiles sorted by a whole CTA (mid) or in chunks (long), and (last chunk)
+// the total pair count.
+constexpr int kRangeThreads = 512;
+static_assert(kScanChunk == kRangeThreads * 4, "four tiles per thread");
+
+__global__ void __launch_bounds__(kRangeThreads) k_tile_ranges(const uint32_t* __restrict__ totals, uint32_t n_tiles,
+                                                               uint64_t cap, uint2* __restrict__ ranges,
+                                                               uint32_t* __restrict__ mid_list,
+                                                               uint32_t* __restrict__ long_list, FrameCounters fc) {
+  __shared__ unsigned long long s_warp[kRangeThreads / 32];
+  __shared__ unsigned long long s_base;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  unsigned long long running = 0;
-  for (uint32_t b0 = 0; b0 < tiles; b0 += 1024 * 4) {
-    uint32_t c[4];
-    unsigned long long sum = 0;
+  const uint32_t chunk = blockIdx.x;
+  // Sum of the preceding chunks.
+  unsigned long long pre = 0;
+  for (uint32_t c = tid; c < chunk; c += kRangeThreads) pre += fc.chunk_sum[c];
 #pragma unroll
-    for (int k = 0; k < 4; k++) {
-      const uint32_t t = b0 + tid * 4 + k;
-      c[k] = t < tiles ? totals[t] : 0u;
-      sum += c[k];
-    }
-    unsigned long long x = sum;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
-      if (lane >= o) x += y;
-    }
-    if (lane == 31) s_warp[warp] = x;
-    __syncthreads();
-    unsigned long long base = running, chunk = 0;
-    for (int w = 0; w < 32; w++) {
-      if (w < warp) base += s_warp[w];
-      chunk += s_warp[w];
-    }
-    unsigned long long start = base + x - sum;
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
-      const uint32_t t = b0 + tid * 4 + k;
-      if (t < tiles) {
-        // Ranges are clamped to the pair capacity: past it the frame is
-        // incomplete and rendered again with larger buffers, and nothing
-        // reads beyond the buffers meanwhile.
-        const uint32_t s = (uint32_t)min(start, (unsigned long long)cap);
-        const uint32_t e = (uint32_t)min(start + c[k], (unsigned long long)cap);
-        ranges[t] = e > s ? make_uint2(s, e) : make_uint2(0u, 0u);
-        const uint32_t len = e > s ? e - s : 0u;
-        if (len > kMidSortCap)
-          long_list[atomicAdd(&st->long_tiles, 1u)] = t;
-        else if (len > kWarpSortCap)
-          mid_list[atomicAdd(&st->mid_tiles, 1u)] = t;
-      }
-      start += c[k];
-    }
-    running += chunk;
-    __syncthreads();
+  for (int o = 16; o > 0; o >>= 1) pre += __shfl_xor_sync(0xffffffffu, pre, o);
+  if (lane == 0) s_warp[warp] = pre;
+  __syncthreads();
+  if (tid == 0) {
+    unsigned long long b = 0;
+    for (int w = 0; w < kRangeThreads / 32; w++) b += s_warp[w];
+    s_base = b;
   }
-  if (tid == 0) st->total_pairs = running;
+  __syncthreads();
+  const unsigned long long base = s_base;
+  uint32_t c[4];
+  unsigned long long sum = 0;
+  const uint32_t t0 = chunk * kScanChunk + tid * 4;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    c[k] = t0 + k < n_tiles ? totals[t0 + k] : 0u;
+    sum += c[k];
+  }
+  unsigned long long x = sum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  __syncthreads();  // s_warp is reused
+  if (lane == 31) s_warp[warp] = x;
+  __syncthreads();
+  unsigned long long before = 0, chunk_total = 0;
+  for (int w = 0; w < kRangeThreads / 32; w++) {
+    if (w < warp) before += s_warp[w];
+    chunk_total += s_warp[w];
+  }
+  unsigned long long start = base + before + x - sum;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const uint32_t t = t0 + k;
+    if (t < n_tiles) {
+      // Ranges are clamped to the pair capacity: past it the frame is
+      // incomplete and rendered again with larger buffers, and nothing
+      // reads beyond the buffers meanwhile.
+      const uint32_t s = (uint32_t)min(start, (unsigned long long)cap);
+      const uint32_t e = (uint32_t)min(start + c[k], (unsigned long long)cap);
+      ranges[t] = e > s ? make_uint2(s, e) : make_uint2(0u, 0u);
+      const uint32_t len = e > s ? e - s : 0u;
+      if (len > kMidSortCap)
+        long_list[atomicAdd(&fc.st->long_tiles, 1u)] = t;
+      else if (len > kWarpSortCap)
+        mid_list[atomicAdd(&fc.st->mid_tiles, 1u)] = t;
+    }
+    start += c[k];
+  }
+  if (chunk == gridDim.x - 1 && tid == 0) fc.st->total_pairs = base + chunk_total;
 }
 
 template <bool SMEM>
-__global__ void __launch_bounds__(kBinThreads) k_bin_scatter(const BinInfo* __restrict__ bin, uint64_t n,
-                                                             uint64_t per_cta, uint32_t tiles_x, uint32_t tiles,
-                                                             uint32_t* __restrict__ counts,
+__global__ void __launch_bounds__(kBinThreads) k_bin_scatter(const ViewTask* __restrict__ table, uint32_t n_views,
                                                              const uint2* __restrict__ ranges,
                                                              uint64_t* __restrict__ pairs, uint64_t cap) {
   extern __shared__ uint32_t s_row[];
-  uint32_t* row = counts + (uint64_t)blockIdx.x * tiles;
+  const BinView b = bin_view(table, n_views);
+  const uint2* vr = ranges + b.tile0;
   if (SMEM) {
-    for (uint32_t t = threadIdx.x; t < tiles; t += kBinThreads) s_row[t] = ranges[t].x + row[t];
+    for (uint32_t t = threadIdx.x; t < b.tiles; t += kBinThreads) s_row[t] = vr[t].x + b.row[t];
     __syncthreads();
   }
-  const uint64_t s0 = min(n, (uint64_t)blockIdx.x * per_cta), s1 = min(n, s0 + per_cta);
-  for_each_pair(bin, s0, s1, tiles_x, [&](uint32_t t, uint32_t i, uint32_t depth_bits) {
+  for_each_pair(b.bin, b.s0, b.s1, b.tiles_x, [&](uint32_t t, uint32_t i, uint32_t depth_bits) {
     uint64_t pos;
     if (SMEM)
       pos = atomicAdd(&s_row[t], 1u);
     else
-      pos = (uint64_t)ranges[t].x + atomicAdd(&row[t], 1u);
+      pos = (uint64_t)vr[t].x + atomicAdd(&b.row[t], 1u);
     if (pos < cap) pairs[pos] = ((uint64_t)depth_bits << 32) | i;
   });
 }
@@ -346,51 +409,49 @@ __global__ void __launch_bounds__(kTileThreads) k_sort_long(const uint2* __restr
 
 }  // namespace
 
-uint32_t bin_rows(int num_sms) { return 2u * (uint32_t)num_sms; }
+uint32_t bin_rows(uint64_t n, int num_sms) {
+  // About 4096 splats per CTA, at most two CTAs per SM.
+  const uint64_t r = (n + 4095) / 4096;
+  return (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(r, 2ull * (uint64_t)num_sms));
+}
 
-cudaError_t launch_binning(const FrameParams& fp, const BinInfo* bin, uint64_t n, uint32_t* counts, uint32_t* totals,
-                           uint2* ranges, uint32_t* mid_list, uint32_t* long_list, uint64_t* pairs,
-                           uint64_t* pairs_alt, uint64_t cap, DevState* st, int num_sms, size_t max_smem,
-                           cudaStream_t stream, uint32_t* launches) {
-  const uint32_t tiles = fp.tiles_x * fp.tiles_y;
-  const uint32_t rows = bin_rows(num_sms);
-  const uint64_t per_cta = n ? (n + rows - 1) / rows : 1;
-  const size_t smem = (size_t)tiles * sizeof(uint32_t);
+cudaError_t launch_binning(const ViewTask* table, const BinLaunch& bl, uint32_t* totals, uint2* ranges,
+                           uint32_t* mid_list, uint32_t* long_list, uint64_t* pairs, uint64_t* pairs_alt,
+                           uint64_t cap, const FrameCounters& fc, int num_sms, size_t max_smem, cudaStream_t stream,
+                           uint32_t* launches) {
+  if (bl.n_tiles == 0) return cudaSuccess;
+  const size_t smem = (size_t)bl.max_tiles * sizeof(uint32_t);
   const bool use_smem = smem <= max_smem;
   cudaError_t e = cudaSuccess;
-  if (n) {
-    if (use_smem) {
-      if ((e = cudaFuncSetAttribute(k_bin_count<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
-        return e;
-      k_bin_count<true><<<rows, kBinThreads, smem, stream>>>(bin, n, per_cta, fp.tiles_x, tiles, counts);
-    } else {
-      if ((e = cudaMemsetAsync(counts, 0, (size_t)rows * tiles * sizeof(uint32_t), stream))) return e;
-      k_bin_count<false><<<rows, kBinThreads, 0, stream>>>(bin, n, per_cta, fp.tiles_x, tiles, counts);
-    }
-    k_bin_colscan<<<(tiles + 31) / 32, 256, 0, stream>>>(counts, rows, tiles, totals);
-    *launches += 2;
+  // Shared-memory limits are raised to the device's opt-in maximum outside
+  // stream capture (the first frame or batch always runs uncaptured).
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if ((e = cudaStreamIsCapturing(stream, &cs))) return e;
+  if (cs == cudaStreamCaptureStatusNone) {
+    const int big = (int)max_smem;
+    if ((e = cudaFuncSetAttribute(k_bin_count<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, big))) return e;
+    if ((e = cudaFuncSetAttribute(k_bin_scatter<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, big))) return e;
+    if ((e = cudaFuncSetAttribute(k_sort_mid, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MidSmem))))
+      return e;
+  }
+  if (use_smem) {
+    k_bin_count<true><<<bl.bin_ctas, kBinThreads, smem, stream>>>(table, bl.n_views);
   } else {
-    if ((e = cudaMemsetAsync(totals, 0, (size_t)tiles * sizeof(uint32_t), stream))) return e;
+    if ((e = cudaMemsetAsync(bl.counts_all, 0, bl.counts_bytes, stream))) return e;
+    k_bin_count<false><<<bl.bin_ctas, kBinThreads, 0, stream>>>(table, bl.n_views);
   }
-  k_bin_tilescan<<<1, 1024, 0, stream>>>(totals, tiles, cap, ranges, mid_list, long_list, st);
-  *launches += 1;
-  if (n) {
-    if (use_smem) {
-      if ((e = cudaFuncSetAttribute(k_bin_scatter<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
-        return e;
-      k_bin_scatter<true><<<rows, kBinThreads, smem, stream>>>(bin, n, per_cta, fp.tiles_x, tiles, counts, ranges,
-                                                               pairs, cap);
-    } else {
-      k_bin_scatter<false><<<rows, kBinThreads, 0, stream>>>(bin, n, per_cta, fp.tiles_x, tiles, counts, ranges,
-                                                             pairs, cap);
-    }
-    k_sort_small<<<(tiles + 7) / 8, 256, 0, stream>>>(ranges, tiles, pairs);
-    const int mid_smem = (int)sizeof(MidSmem);
-    if ((e = cudaFuncSetAttribute(k_sort_mid, cudaFuncAttributeMaxDynamicSharedMemorySize, mid_smem))) return e;
-    k_sort_mid<<<num_sms * 3, kTileThreads, mid_smem, stream>>>(ranges, mid_list, pairs, st);
-    k_sort_long<<<num_sms, kTileThreads, 0, stream>>>(ranges, long_list, pairs, pairs_alt, cap, st);
-    *launches += 4;  // scatter, small, mid, long
+  k_bin_colscan<<<bl.col_ctas, 256, 0, stream>>>(table, bl.n_views, totals, fc);
+  const uint32_t chunks = (bl.n_tiles + kScanChunk - 1) / kScanChunk;
+  k_tile_ranges<<<chunks, kRangeThreads, 0, stream>>>(totals, bl.n_tiles, cap, ranges, mid_list, long_list, fc);
+  if (use_smem) {
+    k_bin_scatter<true><<<bl.bin_ctas, kBinThreads, smem, stream>>>(table, bl.n_views, ranges, pairs, cap);
+  } else {
+    k_bin_scatter<false><<<bl.bin_ctas, kBinThreads, 0, stream>>>(table, bl.n_views, ranges, pairs, cap);
   }
+  k_sort_small<<<(bl.n_tiles + 7) / 8, 256, 0, stream>>>(ranges, bl.n_tiles, pairs);
+  k_sort_mid<<<num_sms * 3, kTileThreads, sizeof(MidSmem), stream>>>(ranges, mid_list, pairs, fc.st);
+  k_sort_long<<<num_sms, kTileThreads, 0, stream>>>(ranges, long_list, pairs, pairs_alt, cap, fc.st);
+  *launches += 7;
   return cudaGetLastError();
 }
 

@@ -1,17 +1,25 @@
 // Kernel (d): per-tile front-to-back blend with the terminal box-filter
 // downsample fused in.
 //
-// One CTA per 16x16 tile, one pixel per thread, over the tile's pairs in
-// depth order (sorted per tile by the binning stage); each warp covers an 8x4 block
-// of the tile so a splat whose pixel bbox misses the block is skipped by the
-// whole warp. The tile's depth-sorted splat list is walked in batches of 256:
-// the CTA gathers the batch's 48-byte records into shared memory (one per
-// thread, coalesced index loads, the next batch's gather in flight while the
-// current one blends), storing each splat's bbox as a row/column bit mask so
-// the per-pixel bbox test is one AND and one compare; then every pixel blends
-// the batch front to back. A pixel stops once its transmittance drops below T_MIN; the CTA stops
-// when a block vote finds no live pixel (the reference stops a tile when all
-// its row masks are empty, src/render/cpu.rs:693-702).
+// A persistent kernel over the tiles of every view of the view table: each
+// CTA of NT threads runs NT / G tile groups of G = min(NT, TW*TH) threads,
+// and each group takes the next tile from a global counter until none is
+// left (views of uneven resolution share one launch). A thread blends
+// PPT = TW*TH / G pixels of its tile (one column, PPT consecutive rows); each
+// warp covers an 8 x 4*PPT block of the tile, so a splat whose pixel bbox
+// misses the block is skipped by the whole warp. The tile's depth-sorted
+// splat list is walked in batches of G: the group gathers the batch's
+// 48-byte records into shared memory (one per thread, the next batch's
+// gather in flight while the current one blends), storing each splat's bbox
+// as column and row bit masks; each warp lists the entries that touch its
+// block (ballot compaction) and every pixel blends the batch front to back.
+// A pixel stops once its transmittance drops below T_MIN; the group stops
+// when a vote finds no live pixel (the reference stops a tile when all its
+// row masks are empty, src/render/cpu.rs:693-702).
+//
+// Tile shapes 8x8, 16x16 (the reference's) and 32x16 with 128, 256 or 512
+// threads are instantiated; the image does not depend on the choice (each
+// pixel sees the same splats in the same order).
 //
 // Per pixel and splat the arithmetic is that of raster_tile
 // (src/render/cpu.rs:638-703): power = (-a/2 dx^2 + -c/2 dy^2) + (-b dy) dx
@@ -19,13 +27,17 @@
 // masked by power <= 0 and alpha >= 1/255, C += colour * alpha * T,
 // T *= 1 - alpha. EXACT = true evaluates it with the reference's x86 f32
 // semantics (unfused multiply-adds, the polynomial exp_neg of
-// src/render/simd.rs:315-331), which reproduces the cpu backend's image bit
+// src/render/simd.rs:315-331, and dx associated as the reference's 4-wide
+// lanes of a 16-pixel tile do), which reproduces the cpu backend's image bit
 // for bit; EXACT = false uses FMA and the hardware exp2 (the default).
 // The result is quantised with to_u8 (src/render/mod.rs:282-285) and, for a
-// downsample factor f dividing 16, averaged over f x f blocks in shared
-// memory with term::downsample's truncating integer division
+// downsample factor f dividing the tile shape, averaged over f x f blocks in
+// shared memory with term::downsample's truncating integer division
 // (src/term.rs:74-99); other factors go through a full-resolution scratch
 // frame and k_downsample.
+#include <atomic>
+#include <cstddef>
+
 #include "common.cuh"
 
 namespace splat {
@@ -66,11 +78,10 @@ __device__ __forceinline__ uint32_t to_u8(float v) {
   return (uint32_t)q;
 }
 
-// One splat's contribution test at this pixel: returns alpha, or 0 when the
-// splat does not contribute (outside the bbox, power > 0, alpha < 1/255).
+
 template <bool EXACT>
-__device__ __forceinline__ float splat_alpha(uint32_t m, uint32_t mybits, const float4& a, const float4& b,
-                                             float fx05, float gbase, float lanef, float rowc, float lxf, float lyf) {
+__device__ __forceinline__ float splat_alpha(bool inbox, const float4& a, const float4& b, float fx05, float gbase,
+                                             float lanef, float rowc, float lxf, float lyf) {
   float pw, alpha;
   if (EXACT) {
     const float cx0 = __fsub_rn(fx05, a.x);
@@ -92,7 +103,7 @@ __device__ __forceinline__ float splat_alpha(uint32_t m, uint32_t mybits, const 
   // extent rounded outwards and pixels are sampled at their centres), so the
   // alpha test alone excludes it in the default path; the exact path also
   // tests the bbox, as the reference does.
-  const bool on = (pw <= 0.0f) && (alpha >= kAlphaMin) && (!EXACT || (m & mybits) == mybits);
+  const bool on = (pw <= 0.0f) && (alpha >= kAlphaMin) && (!EXACT || inbox);
   return on ? alpha : 0.0f;
 }
 
@@ -114,175 +125,281 @@ __device__ __forceinline__ void accumulate(float alpha, const float4& b, float b
   }
 }
 
-template <bool EXACT>
-__global__ void __launch_bounds__(256) k_blend(FrameParams fp, const Record* __restrict__ rec,
-                                               const uint64_t* __restrict__ pairs, const uint2* __restrict__ ranges,
-                                               uint8_t* __restrict__ out, uint8_t* __restrict__ full) {
-  // Per batch entry: the splat's pixel bbox clipped to this tile as a bit
-  // mask (columns in bits 0-15, rows in bits 16-31), its geometry and colour.
-  // The default path stores the centre relative to the tile's first pixel
-  // centre and the conic pre-scaled by log2(e) for exp2. Each warp then lists
-  // the entries whose bbox meets its 8x4 block and walks only those, two at a
-  // time (the second splat's alpha is computed while the first one's is being
-  // accumulated).
-  __shared__ float4 s_a[256];  // x, y, -a/2, -b
-  __shared__ float4 s_b[256];  // -c/2, opacity, red, green
-  __shared__ uint32_t s_mask[256];
-  __shared__ float s_c[256];  // blue
-  __shared__ uint8_t s_list[8][256];
-  __shared__ uint32_t s_px[256];
+// Bits [lo, hi) of a 32-bit mask (0 <= lo <= hi <= 32).
+__device__ __forceinline__ uint32_t bit_range(int lo, int hi) {
+  return (uint32_t)(((1ull << hi) - 1ull) & ~((1ull << lo) - 1ull));
+}
 
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const uint32_t tile = blockIdx.x;
-  const uint32_t tx = tile % fp.tiles_x, ty = tile / fp.tiles_x;
-  const uint32_t ox = tx * kTile, oy = ty * kTile;
-  const uint32_t wx = (warp & 1) * 8, wy = (warp >> 1) * 4;
-  const uint32_t lx = wx + (lane & 7), ly = wy + (lane >> 3);
-  const uint32_t px = ox + lx, py = oy + ly;
-  const bool inside = px < fp.w && py < fp.h;
-  const uint32_t mybits = (1u << lx) | (1u << (16 + ly));
-  const uint32_t wxbits = 0xFFu << wx, wybits = 0xFu << (16 + wy);
-  const uint2 range = ranges[tile];
-  const uint32_t begin = range.x, n = range.y > range.x ? range.y - range.x : 0u;
-  auto splat_at = [&](uint32_t p) -> uint32_t { return (uint32_t)pairs[begin + p]; };
+// Barrier over the `count` threads of named barrier `id` (0 = the whole CTA).
+__device__ __forceinline__ void group_sync(uint32_t id, uint32_t count) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
 
-  // EXACT: dx = lane + ((g*4) + ((ox + 0.5) - x)), dy = ((oy + ly) + 0.5) - y
-  // in the reference's association (src/render/cpu.rs:658-671).
-  const float fx05 = __fadd_rn((float)ox, 0.5f);
-  const float gbase = (float)(lx & ~3u), lanef = (float)(lx & 3u);
-  const float rowc = __fadd_rn(__fadd_rn((float)oy, (float)ly), 0.5f);
-  const float lxf = (float)lx, lyf = (float)ly;
-  const float ox05 = (float)ox + 0.5f, oy05 = (float)oy + 0.5f;
+// Barrier with a population count of `pred` over the same threads.
+__device__ __forceinline__ uint32_t group_count(uint32_t id, uint32_t count, bool pred) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.u32 p, %1, 0;\n\tbar.red.popc.u32 %0, %2, %3, p;\n\t}"
+      : "=r"(r)
+      : "r"((uint32_t)pred), "r"(id), "r"(count)
+      : "memory");
+  return r;
+}
 
-  float T = 1.0f, cr = 0.0f, cg = 0.0f, cb = 0.0f;
-  bool done = !inside;
+template <int TW, int TH, int NT>
+struct BlendShape {
+  static constexpr int P = TW * TH;         // pixels per tile
+  static constexpr int G = NT < P ? NT : P;  // threads per tile group
+  static constexpr int NG = NT / G;          // tile groups per CTA
+  static constexpr int PPT = P / G;          // pixels per thread
+  static constexpr int GW = G / 32;          // warps per group
+  static constexpr int BH = 4 * PPT;         // warp block height (width 8)
+  static constexpr int WCOLS = TW / 8;       // warp blocks per tile row
+  static_assert(TW % 8 == 0 && TH % BH == 0 && WCOLS * (TH / BH) == GW, "tile shape and threads");
+  static_assert(TW <= 32 && TH <= 16, "bbox masks hold 32 columns and 16 rows");
+  static_assert(NG <= 8, "named barriers 1..8");
+};
 
-  // The next batch's record is gathered into registers while the current
-  // batch is blended.
-  Record nr;
-  bool has = false;
-  if ((uint32_t)tid < n) {
-    nr = rec[splat_at(tid)];
-    has = true;
-  }
-  for (uint32_t start = 0; start < n; start += 256) {
-    if (has) {
-      const uint32_t bx = __float_as_uint(nr.r2.y), by = __float_as_uint(nr.r2.z);
-      const int x0 = min(max((int)(bx & 0xFFFFu) - (int)ox, 0), 16), x1 = min(max((int)(bx >> 16) - (int)ox, 0), 16);
-      const int y0 = min(max((int)(by & 0xFFFFu) - (int)oy, 0), 16), y1 = min(max((int)(by >> 16) - (int)oy, 0), 16);
-      const uint32_t xb = ((1u << x1) - 1u) & ~((1u << x0) - 1u);
-      const uint32_t yb = ((1u << y1) - 1u) & ~((1u << y0) - 1u);
-      s_mask[tid] = xb | (yb << 16);
-      float4 a = nr.r0, b = nr.r1;
-      if (!EXACT) {
-        a.x -= ox05;
-        a.y -= oy05;
-        a.z *= kLog2e;
-        a.w *= kLog2e;
-        b.x *= kLog2e;
-      }
-      s_a[tid] = a;
-      s_b[tid] = b;
-      s_c[tid] = nr.r2.x;
+// Shared memory of one tile group: a batch of G staged splats (centre,
+// conic, opacity, colour, bbox masks), the warps' lists of batch entries,
+// the tile's quantised pixels for the fused downsample, the group's tile.
+template <int TW, int TH, int NT>
+struct __align__(16) GroupSmem {
+  using S = BlendShape<TW, TH, NT>;
+  float4 a[S::G];  // x, y, -a/2, -b
+  float4 b[S::G];  // -c/2, opacity, red, green
+  float c[S::G];   // blue
+  uint32_t mx[S::G];
+  uint32_t my[S::G];
+  uint16_t list[S::GW][S::G];
+  uint32_t px[S::P];
+  uint32_t work;
+};
+
+template <bool EXACT, int TW, int TH, int NT>
+__global__ void __launch_bounds__(NT) k_blend(const ViewTask* __restrict__ table, uint32_t n_views, uint32_t n_tiles,
+                                              const uint64_t* __restrict__ pairs, const uint2* __restrict__ ranges,
+                                              DevState* st) {
+  using S = BlendShape<TW, TH, NT>;
+  using Smem = GroupSmem<TW, TH, NT>;
+  constexpr int G = S::G, PPT = S::PPT;
+  extern __shared__ __align__(16) unsigned char s_raw[];
+  const int tid = threadIdx.x, lane = tid & 31;
+  const int g = tid / G, gt = tid % G, gw = gt >> 5;
+  Smem& sm = reinterpret_cast<Smem*>(s_raw)[g];
+  const uint32_t bar = S::NG == 1 ? 0u : 1u + (uint32_t)g;
+  auto sync = [&]() {
+    if (S::NG == 1)
+      __syncthreads();
+    else
+      group_sync(bar, G);
+  };
+  auto count = [&](bool p) -> uint32_t {
+    if (S::NG == 1) return (uint32_t)__syncthreads_count(p);
+    return group_count(bar, G, p);
+  };
+
+  const uint32_t wbx = gw % S::WCOLS, wby = gw / S::WCOLS;
+  const uint32_t lx = wbx * 8 + (lane & 7);
+  const uint32_t ly0 = wby * S::BH + (lane >> 3) * PPT;
+  const uint32_t wxbits = 0xFFu << (wbx * 8);
+  const uint32_t wybits = ((1u << S::BH) - 1u) << (wby * S::BH);
+
+  for (;;) {
+    if (gt == 0) sm.work = atomicAdd(&st->blend_next, 1u);
+    sync();
+    const uint32_t tile = sm.work;
+    if (tile >= n_tiles) break;
+    const uint32_t v = find_view(table, n_views, tile, offsetof(ViewTask, tile0));
+    const ViewTask* tv = table + v;
+    const uint32_t local = tile - tv->tile0;
+    const uint32_t tiles_x = tv->fp.tiles_x;
+    if (local >= tiles_x * tv->fp.tiles_y) {  // alignment padding between views
+      sync();
+      continue;
     }
-    __syncthreads();
-    const uint32_t nxt = start + 256 + tid;
-    has = nxt < n;
-    if (has) nr = rec[splat_at(nxt)];
-    const uint32_t cnt = min(256u, n - start);
-    // This warp's list of batch entries whose bbox meets its block.
-    uint32_t len = 0;
-    if (__any_sync(0xffffffffu, !done)) {
-      for (uint32_t c0 = 0; c0 < cnt; c0 += 32) {
-        const uint32_t e = c0 + lane;
-        const uint32_t m = e < cnt ? s_mask[e] : 0u;
-        const bool hit = (m & wxbits) && (m & wybits);
-        const uint32_t bal = __ballot_sync(0xffffffffu, hit);
-        if (hit) s_list[warp][len + __popc(bal & ((1u << lane) - 1u))] = (uint8_t)e;
-        len += __popc(bal);
-      }
-      __syncwarp();
+    const uint32_t W = tv->fp.w, H = tv->fp.h;
+    const Record* __restrict__ rec = tv->rec;
+    const uint32_t ox = (local % tiles_x) * TW, oy = (local / tiles_x) * TH;
+    const uint32_t px = ox + lx;
+
+    // EXACT: dx = lane + ((g*4) + ((ox16 + 0.5) - x)), dy = (py + 0.5) - y
+    // in the reference's association, ox16 the pixel's 16-pixel tile origin
+    // (src/render/cpu.rs:658-671).
+    const float fx05 = __fadd_rn((float)(px & ~15u), 0.5f);
+    const float gbase = (float)(px & 12u), lanef = (float)(px & 3u);
+    const float lxf = (float)lx;
+    const float ox05 = (float)ox + 0.5f, oy05 = (float)oy + 0.5f;
+
+    float T[PPT], cr[PPT], cg[PPT], cb[PPT];
+    bool done[PPT];
+    bool all_done = true;
+#pragma unroll
+    for (int k = 0; k < PPT; k++) {
+      T[k] = 1.0f;
+      cr[k] = cg[k] = cb[k] = 0.0f;
+      done[k] = !(px < W && oy + ly0 + k < H);
+      all_done = all_done && done[k];
     }
-    if (!done) {
-      uint32_t k = 0;
-      for (; k + 1 < len; k += 2) {
-        const uint32_t j0 = s_list[warp][k], j1 = s_list[warp][k + 1];
-        const float4 a0 = s_a[j0], b0 = s_b[j0];
-        const float4 a1 = s_a[j1], b1 = s_b[j1];
-        const float al0 = splat_alpha<EXACT>(s_mask[j0], mybits, a0, b0, fx05, gbase, lanef, rowc, lxf, lyf);
-        const float al1 = splat_alpha<EXACT>(s_mask[j1], mybits, a1, b1, fx05, gbase, lanef, rowc, lxf, lyf);
-        if (al0 > 0.0f) {
-          accumulate<EXACT>(al0, b0, s_c[j0], T, cr, cg, cb);
-          if (T < kTMin) {
-            done = true;
-            break;
+
+    const uint2 range = ranges[tile];
+    const uint32_t begin = range.x, n = range.y > range.x ? range.y - range.x : 0u;
+    Record nr;
+    bool has = false;
+    if ((uint32_t)gt < n) {
+      nr = rec[(uint32_t)pairs[begin + gt]];
+      has = true;
+    }
+    for (uint32_t start = 0; start < n; start += G) {
+      if (has) {
+        const uint32_t bx = __float_as_uint(nr.r2.y), by = __float_as_uint(nr.r2.z);
+        const int x0 = min(max((int)(bx & 0xFFFFu) - (int)ox, 0), TW), x1 = min(max((int)(bx >> 16) - (int)ox, 0), TW);
+        const int y0 = min(max((int)(by & 0xFFFFu) - (int)oy, 0), TH), y1 = min(max((int)(by >> 16) - (int)oy, 0), TH);
+        sm.mx[gt] = x1 > x0 ? bit_range(x0, x1) : 0u;
+        sm.my[gt] = y1 > y0 ? bit_range(y0, y1) : 0u;
+        float4 a = nr.r0, b = nr.r1;
+        if (!EXACT) {
+          a.x -= ox05;
+          a.y -= oy05;
+          a.z *= kLog2e;
+          a.w *= kLog2e;
+          b.x *= kLog2e;
+        }
+        sm.a[gt] = a;
+        sm.b[gt] = b;
+        sm.c[gt] = nr.r2.x;
+      }
+      sync();
+      const uint32_t nxt = start + G + gt;
+      has = nxt < n;
+      if (has) nr = rec[(uint32_t)pairs[begin + nxt]];
+      const uint32_t cnt = min((uint32_t)G, n - start);
+      // This warp's list of batch entries whose bbox meets its block.
+      uint32_t len = 0;
+      if (__any_sync(0xffffffffu, !all_done)) {
+        for (uint32_t c0 = 0; c0 < cnt; c0 += 32) {
+          const uint32_t e = c0 + lane;
+          const bool hit = e < cnt && (sm.mx[e] & wxbits) && (sm.my[e] & wybits);
+          const uint32_t bal = __ballot_sync(0xffffffffu, hit);
+          if (hit) sm.list[gw][len + __popc(bal & ((1u << lane) - 1u))] = (uint16_t)e;
+          len += __popc(bal);
+        }
+        __syncwarp();
+      }
+      if (!all_done) {
+        if constexpr (PPT == 1) {
+          // Two splats per iteration: the second one's alpha is computed
+          // while the first one is accumulated.
+          const float rowc = (float)(oy + ly0) + 0.5f, lyf = (float)ly0;
+          const uint32_t ybit = 1u << ly0, xbit = 1u << lx;
+          uint32_t k = 0;
+          for (; k + 1 < len; k += 2) {
+            const uint32_t j0 = sm.list[gw][k], j1 = sm.list[gw][k + 1];
+            const float4 a0 = sm.a[j0], b0 = sm.b[j0];
+            const float4 a1 = sm.a[j1], b1 = sm.b[j1];
+            const bool in0 = !EXACT || ((sm.mx[j0] & xbit) && (sm.my[j0] & ybit));
+            const bool in1 = !EXACT || ((sm.mx[j1] & xbit) && (sm.my[j1] & ybit));
+            const float al0 = splat_alpha<EXACT>(in0, a0, b0, fx05, gbase, lanef, rowc, lxf, lyf);
+            const float al1 = splat_alpha<EXACT>(in1, a1, b1, fx05, gbase, lanef, rowc, lxf, lyf);
+            if (al0 > 0.0f) {
+              accumulate<EXACT>(al0, b0, sm.c[j0], T[0], cr[0], cg[0], cb[0]);
+              if (T[0] < kTMin) {
+                done[0] = true;
+                break;
+              }
+            }
+            if (al1 > 0.0f) {
+              accumulate<EXACT>(al1, b1, sm.c[j1], T[0], cr[0], cg[0], cb[0]);
+              if (T[0] < kTMin) {
+                done[0] = true;
+                break;
+              }
+            }
+          }
+          if (!done[0] && k < len) {
+            const uint32_t j0 = sm.list[gw][k];
+            const float4 a0 = sm.a[j0], b0 = sm.b[j0];
+            const bool in0 = !EXACT || ((sm.mx[j0] & xbit) && (sm.my[j0] & ybit));
+            const float al0 = splat_alpha<EXACT>(in0, a0, b0, fx05, gbase, lanef, rowc, lxf, lyf);
+            if (al0 > 0.0f) {
+              accumulate<EXACT>(al0, b0, sm.c[j0], T[0], cr[0], cg[0], cb[0]);
+              if (T[0] < kTMin) done[0] = true;
+            }
+          }
+          all_done = done[0];
+        } else {
+          const uint32_t xbit = 1u << lx;
+          for (uint32_t k = 0; k < len && !all_done; k++) {
+            const uint32_t j = sm.list[gw][k];
+            const float4 a = sm.a[j], b = sm.b[j];
+            const uint32_t mx = sm.mx[j], my = sm.my[j];
+            const float blue = sm.c[j];
+            all_done = true;
+#pragma unroll
+            for (int q = 0; q < PPT; q++) {
+              if (!done[q]) {
+                const uint32_t ly = ly0 + q;
+                const bool in = !EXACT || ((mx & xbit) && ((my >> ly) & 1u));
+                const float al = splat_alpha<EXACT>(in, a, b, fx05, gbase, lanef, (float)(oy + ly) + 0.5f, lxf,
+                                                    (float)ly);
+                if (al > 0.0f) {
+                  accumulate<EXACT>(al, b, blue, T[q], cr[q], cg[q], cb[q]);
+                  if (T[q] < kTMin) done[q] = true;
+                }
+              }
+              all_done = all_done && done[q];
+            }
           }
         }
-        if (al1 > 0.0f) {
-          accumulate<EXACT>(al1, b1, s_c[j1], T, cr, cg, cb);
-          if (T < kTMin) {
-            done = true;
-            break;
-          }
-        }
       }
-      if (!done && k < len) {
-        const uint32_t j0 = s_list[warp][k];
-        const float4 a0 = s_a[j0], b0 = s_b[j0];
-        const float al0 = splat_alpha<EXACT>(s_mask[j0], mybits, a0, b0, fx05, gbase, lanef, rowc, lxf, lyf);
-        if (al0 > 0.0f) {
-          accumulate<EXACT>(al0, b0, s_c[j0], T, cr, cg, cb);
-          if (T < kTMin) done = true;
-        }
-      }
+      if (count(!all_done) == 0) break;
     }
-    if (__syncthreads_count(!done) == 0) break;
-  }
 
-  // C + T * bg, quantised (the reference adds unfused: c + (t * bg)).
-  const uint32_t qr = to_u8(__fadd_rn(cr, __fmul_rn(T, fp.bg[0])));
-  const uint32_t qg = to_u8(__fadd_rn(cg, __fmul_rn(T, fp.bg[1])));
-  const uint32_t qb = to_u8(__fadd_rn(cb, __fmul_rn(T, fp.bg[2])));
-  const uint32_t f = fp.downsample;
-  if (f == 1) {
-    if (inside) {
-      uint8_t* o = out + ((size_t)py * fp.w + px) * 3;
-      o[0] = (uint8_t)qr;
-      o[1] = (uint8_t)qg;
-      o[2] = (uint8_t)qb;
+    // C + T * bg, quantised (the reference adds unfused: c + (t * bg)).
+    const uint32_t f = tv->fp.downsample;
+    uint8_t* __restrict__ out = tv->out;
+    const float bg0 = tv->fp.bg[0], bg1 = tv->fp.bg[1], bg2 = tv->fp.bg[2];
+    const bool fused = f > 1 && TW % f == 0 && TH % f == 0;
+#pragma unroll
+    for (int k = 0; k < PPT; k++) {
+      const uint32_t ly = ly0 + k, py = oy + ly;
+      const uint32_t qr = to_u8(__fadd_rn(cr[k], __fmul_rn(T[k], bg0)));
+      const uint32_t qg = to_u8(__fadd_rn(cg[k], __fmul_rn(T[k], bg1)));
+      const uint32_t qb = to_u8(__fadd_rn(cb[k], __fmul_rn(T[k], bg2)));
+      if (fused) {
+        sm.px[ly * TW + lx] = qr | (qg << 8) | (qb << 16);
+      } else if (px < W && py < H) {
+        // f == 1: the frame; other factors: the full-resolution scratch frame.
+        uint8_t* o = (f == 1 ? out : tv->full) + ((size_t)py * W + px) * 3;
+        o[0] = (uint8_t)qr;
+        o[1] = (uint8_t)qg;
+        o[2] = (uint8_t)qb;
+      }
     }
-    return;
-  }
-  if (kTile % f != 0) {  // factor 3 etc.: full-resolution scratch, then k_downsample
-    if (inside) {
-      uint8_t* o = full + ((size_t)py * fp.w + px) * 3;
-      o[0] = (uint8_t)qr;
-      o[1] = (uint8_t)qg;
-      o[2] = (uint8_t)qb;
-    }
-    return;
-  }
-  s_px[ly * kTile + lx] = qr | (qg << 8) | (qb << 16);
-  __syncthreads();
-  const uint32_t per = kTile / f;  // output pixels per tile edge
-  if ((uint32_t)tid < per * per) {
-    const uint32_t bxl = tid % per, byl = tid / per;
-    const uint32_t obx = ox / f + bxl, oby = oy / f + byl;
-    if (obx < fp.out_w && oby < fp.out_h) {
-      uint32_t acc[3] = {0u, 0u, 0u};
-      for (uint32_t sy = 0; sy < f; sy++)
-        for (uint32_t sx = 0; sx < f; sx++) {
-          const uint32_t p = s_px[(byl * f + sy) * kTile + bxl * f + sx];
-          acc[0] += p & 255u;
-          acc[1] += (p >> 8) & 255u;
-          acc[2] += (p >> 16) & 255u;
+    if (fused) {
+      sync();
+      const uint32_t pw_ = TW / f, ph_ = TH / f;  // output pixels of the tile
+      if ((uint32_t)gt < pw_ * ph_) {
+        const uint32_t bxl = gt % pw_, byl = gt / pw_;
+        const uint32_t obx = ox / f + bxl, oby = oy / f + byl;
+        if (obx < tv->fp.out_w && oby < tv->fp.out_h) {
+          uint32_t acc[3] = {0u, 0u, 0u};
+          for (uint32_t sy = 0; sy < f; sy++)
+            for (uint32_t sx = 0; sx < f; sx++) {
+              const uint32_t p = sm.px[(byl * f + sy) * TW + bxl * f + sx];
+              acc[0] += p & 255u;
+              acc[1] += (p >> 8) & 255u;
+              acc[2] += (p >> 16) & 255u;
+            }
+          const uint32_t nn = f * f;
+          uint8_t* o = out + ((size_t)oby * tv->fp.out_w + obx) * 3;
+          o[0] = (uint8_t)(acc[0] / nn);
+          o[1] = (uint8_t)(acc[1] / nn);
+          o[2] = (uint8_t)(acc[2] / nn);
         }
-      const uint32_t nn = f * f;
-      uint8_t* o = out + ((size_t)oby * fp.out_w + obx) * 3;
-      o[0] = (uint8_t)(acc[0] / nn);
-      o[1] = (uint8_t)(acc[1] / nn);
-      o[2] = (uint8_t)(acc[2] / nn);
+      }
     }
+    sync();  // the group's shared memory is reused by its next tile
   }
 }
 
@@ -309,20 +426,73 @@ __global__ void k_downsample(FrameParams fp, const uint8_t* __restrict__ full, u
 
 }  // namespace
 
-cudaError_t launch_blend(const FrameParams& fp, const Record* rec, const uint64_t* pairs, const uint2* ranges,
-                         bool exact, uint8_t* out, uint8_t* full_scratch, cudaStream_t stream, uint32_t* launches) {
-  const unsigned tiles = fp.tiles_x * fp.tiles_y;
-  if (tiles == 0) return cudaSuccess;
-  if (exact)
-    k_blend<true><<<tiles, 256, 0, stream>>>(fp, rec, pairs, ranges, out, full_scratch);
-  else
-    k_blend<false><<<tiles, 256, 0, stream>>>(fp, rec, pairs, ranges, out, full_scratch);
-  *launches += 1;
-  if (fp.downsample > 1 && kTile % fp.downsample != 0 && fp.out_w > 0 && fp.out_h > 0) {
-    dim3 grid((fp.out_w + 127) / 128, fp.out_h);
-    k_downsample<<<grid, 128, 0, stream>>>(fp, full_scratch, out);
-    *launches += 1;
+bool blend_config_supported(const BlendConfig& c) {
+  const bool shape = (c.tile_w == 8 && c.tile_h == 8) || (c.tile_w == 16 && c.tile_h == 16) ||
+                     (c.tile_w == 32 && c.tile_h == 16);
+  return shape && (c.threads == 128 || c.threads == 256 || c.threads == 512);
+}
+
+namespace {
+
+template <bool EXACT, int TW, int TH, int NT>
+cudaError_t launch_blend_t(const ViewTask* table, uint32_t n_views, uint32_t n_tiles, const uint64_t* pairs,
+                           const uint2* ranges, DevState* st, int num_sms, cudaStream_t stream) {
+  using S = BlendShape<TW, TH, NT>;
+  const int smem = (int)(S::NG * sizeof(GroupSmem<TW, TH, NT>));
+  // Resident CTAs per SM, looked up once per instantiation.
+  static std::atomic<int> occ{0};
+  int o = occ.load(std::memory_order_relaxed);
+  if (o == 0) {
+    cudaError_t e = cudaFuncSetAttribute(k_blend<EXACT, TW, TH, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_blend<EXACT, TW, TH, NT>, NT, smem);
+    if (e != cudaSuccess) return e;
+    if (o < 1) o = 1;
+    occ.store(o, std::memory_order_relaxed);
   }
+  const uint64_t want = ((uint64_t)n_tiles + S::NG - 1) / S::NG;
+  const uint32_t grid = (uint32_t)std::min<uint64_t>(want, (uint64_t)num_sms * (uint64_t)o);
+  k_blend<EXACT, TW, TH, NT><<<grid, NT, smem, stream>>>(table, n_views, n_tiles, pairs, ranges, st);
+  return cudaGetLastError();
+}
+
+template <bool EXACT>
+cudaError_t launch_blend_e(const ViewTask* table, uint32_t n_views, uint32_t n_tiles, const uint64_t* pairs,
+                           const uint2* ranges, const BlendConfig& c, DevState* st, int num_sms, cudaStream_t s) {
+#define SPLAT_BLEND(TW, TH, NT)                                                                      \
+  if (c.tile_w == TW && c.tile_h == TH && c.threads == NT)                                           \
+    return launch_blend_t<EXACT, TW, TH, NT>(table, n_views, n_tiles, pairs, ranges, st, num_sms, s);
+  SPLAT_BLEND(16, 16, 256)
+  SPLAT_BLEND(16, 16, 128)
+  SPLAT_BLEND(16, 16, 512)
+  SPLAT_BLEND(8, 8, 128)
+  SPLAT_BLEND(8, 8, 256)
+  SPLAT_BLEND(8, 8, 512)
+  SPLAT_BLEND(32, 16, 128)
+  SPLAT_BLEND(32, 16, 256)
+  SPLAT_BLEND(32, 16, 512)
+#undef SPLAT_BLEND
+  return cudaErrorInvalidValue;
+}
+
+}  // namespace
+
+cudaError_t launch_blend(const ViewTask* table, uint32_t n_views, uint32_t n_tiles, const uint64_t* pairs,
+                         const uint2* ranges, bool exact, const BlendConfig& cfg, DevState* st, int num_sms,
+                         cudaStream_t stream, uint32_t* launches) {
+  if (n_tiles == 0) return cudaSuccess;
+  const cudaError_t e = exact ? launch_blend_e<true>(table, n_views, n_tiles, pairs, ranges, cfg, st, num_sms, stream)
+                              : launch_blend_e<false>(table, n_views, n_tiles, pairs, ranges, cfg, st, num_sms, stream);
+  if (e == cudaSuccess) *launches += 1;
+  return e;
+}
+
+cudaError_t launch_downsample(const FrameParams& fp, const uint8_t* full, uint8_t* out, cudaStream_t stream,
+                              uint32_t* launches) {
+  if (fp.out_w == 0 || fp.out_h == 0) return cudaSuccess;
+  dim3 grid((fp.out_w + 127) / 128, fp.out_h);
+  k_downsample<<<grid, 128, 0, stream>>>(fp, full, out);
+  *launches += 1;
   return cudaGetLastError();
 }
 

@@ -14,9 +14,13 @@ constexpr float kTMin = 1e-4f;
 // FP16 storage: a 2D covariance determinant below this is recomputed in FP64.
 constexpr float kFp64DetBelow = 1e-6f;
 constexpr uint32_t kMaxDim = 16384;
-// src/render/cpu.rs:34 (16x16 tiles; row masks there, one CTA per tile here)
+// src/render/cpu.rs:34: the reference's 16x16 tiles (the default tile shape
+// here; 8x8 and 32x16 are the other shapes the tuner may choose).
 constexpr uint32_t kTile = 16;
-constexpr uint32_t kTilePixels = kTile * kTile;
+// Tile starts of consecutive views in a batch are aligned to this many tiles,
+// and the tile scan works on chunks of kScanChunk tiles.
+constexpr uint32_t kTileAlign = 32;
+constexpr uint32_t kScanChunk = 2048;
 
 // Marks a culled splat in BinInfo::rect_lo.
 constexpr uint32_t kCulled = 0xFFFFFFFFu;
@@ -31,6 +35,8 @@ struct FrameParams {
   float focal, cx, cy, width, height, near_plane, lim_x, lim_y;
   float bg[3];
   uint32_t w, h;
+  uint32_t tile_w, tile_h;      // tile shape (powers of two)
+  uint32_t tile_sx, tile_sy;    // log2 of the tile shape
   uint32_t tiles_x, tiles_y;
   uint32_t downsample;      // 1 = none
   uint32_t out_w, out_h;    // floor(w/f), floor(h/f)
@@ -74,29 +80,117 @@ struct __align__(16) BinInfo {
 constexpr uint32_t kWarpSortCap = 512;
 constexpr uint32_t kMidSortCap = 4096;
 
-// Frame state in device memory, cleared at the start of every frame.
+// Frame state in device memory, cleared at the start of every frame (or
+// batch). Followed in the same allocation by the per-view counters and the
+// tile-scan chunk sums, cleared with it (FrameCounters).
 struct DevState {
-  unsigned long long visible;      // splats that survived culling
+  unsigned long long visible;      // splats that survived culling (all views)
   unsigned long long total_pairs;  // (splat, tile) pairs, may exceed the capacity
   unsigned int error;
   unsigned int mid_tiles;          // tiles with (kWarpSortCap, kMidSortCap] pairs
   unsigned int long_tiles;         // tiles with more than kMidSortCap pairs
   unsigned int fp64_conics;        // splats whose 2D conic was recomputed in FP64
+  unsigned int blend_next;         // the persistent blend's next tile
+  unsigned int pad;
 };
 
-// Launchers (each returns the cudaGetLastError of its launches).
-// (a) projection: records, tile rectangles and pair counts, visible count.
-cudaError_t launch_project(const FrameParams& fp, const SceneDev& s, Record* rec, BinInfo* bin, float* dbg_proj,
-                           float* dbg_color, DevState* st, cudaStream_t stream, uint32_t* launches);
-// (b) binning into per-tile buckets (count matrix of bin_rows() x tiles,
-// tile totals, ranges, mid/long tile lists) and (c) the per-tile depth sorts.
-uint32_t bin_rows(int num_sms);
-cudaError_t launch_binning(const FrameParams& fp, const BinInfo* bin, uint64_t n, uint32_t* counts, uint32_t* totals,
-                           uint2* ranges, uint32_t* mid_list, uint32_t* long_list, uint64_t* pairs,
-                           uint64_t* pairs_alt, uint64_t cap, DevState* st, int num_sms, size_t max_smem,
-                           cudaStream_t stream, uint32_t* launches);
-// (d) blend + downsample over the depth-sorted buckets.
-cudaError_t launch_blend(const FrameParams& fp, const Record* rec, const uint64_t* pairs, const uint2* ranges,
-                         bool exact, uint8_t* out, uint8_t* full_scratch, cudaStream_t stream, uint32_t* launches);
+// The cleared counters of a frame or batch of n_views views over n_chunks
+// tile-scan chunks: DevState, then visible splats per view, pairs per view,
+// pair totals per scan chunk (all unsigned long long).
+struct FrameCounters {
+  DevState* st;
+  unsigned long long* view_visible;
+  unsigned long long* view_pairs;
+  unsigned long long* chunk_sum;
+};
+inline size_t frame_counters_bytes(uint32_t n_views, uint32_t n_chunks) {
+  return sizeof(DevState) + sizeof(unsigned long long) * (2 * (size_t)n_views + n_chunks);
+}
+inline FrameCounters frame_counters_at(void* base, uint32_t n_views) {
+  FrameCounters c;
+  c.st = static_cast<DevState*>(base);
+  c.view_visible = reinterpret_cast<unsigned long long*>(c.st + 1);
+  c.view_pairs = c.view_visible + n_views;
+  c.chunk_sum = c.view_pairs + n_views;
+  return c;
+}
+
+// One view of a frame or of a batch, as every kernel of the pipeline reads
+// it from the view table (device memory). Each launch covers all views: a
+// CTA finds its view by binary search over the views' first CTA (or first
+// tile) for that launch.
+struct ViewTask {
+  FrameParams fp;
+  SceneDev s;
+  Record* rec;          // n records of this view
+  BinInfo* bin;         // n tile rectangles of this view
+  uint32_t* counts;     // rows x tiles count matrix
+  uint8_t* out;         // device frame, out_w * out_h * 3 bytes
+  uint8_t* full;        // full-resolution scratch for a downsample factor
+                        // that does not divide the tile shape (or null)
+  uint32_t rows;        // CTAs of the count and scatter launches for this view
+  uint32_t tile0;       // first global tile (a multiple of kTileAlign)
+  uint32_t proj_cta0;   // first CTA of the view in the projection launch
+  uint32_t bin_cta0;    // ... in the count and scatter launches
+  uint32_t col_cta0;    // ... in the column-scan launch
+  uint32_t pad[3];
+};
+
+// The view whose `field` (a first-CTA or first-tile member) is the largest
+// one <= x; views are in increasing order of every such field.
+__device__ __forceinline__ uint32_t find_view(const ViewTask* __restrict__ table, uint32_t n_views, uint32_t x,
+                                              size_t field_offset) {
+  uint32_t lo = 0, hi = n_views;  // answer in [lo, hi)
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    const uint32_t v =
+        __ldg(reinterpret_cast<const uint32_t*>(reinterpret_cast<const char*>(table + mid) + field_offset));
+    if (v <= x)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+// Blend configuration: tile shape and threads per CTA.
+struct BlendConfig {
+  uint32_t tile_w, tile_h, threads;
+};
+bool blend_config_supported(const BlendConfig& c);
+
+// Launchers (each returns the cudaGetLastError of its launches and adds the
+// number of kernels it launched to *launches).
+// (a) projection of one view (`t` by value; CTA 0 also stores it as table[0]),
+// or of every view of the table (batch).
+cudaError_t launch_project(const ViewTask& t, ViewTask* table, float* dbg_proj, float* dbg_color,
+                           const FrameCounters& fc, cudaStream_t stream, uint32_t* launches);
+cudaError_t launch_project_batch(const ViewTask* table, uint32_t n_views, uint32_t total_ctas,
+                                 const FrameCounters& fc, cudaStream_t stream, uint32_t* launches);
+// Count-matrix rows (CTAs of the count and scatter launches) for n splats.
+uint32_t bin_rows(uint64_t n, int num_sms);
+// (b) binning into per-tile buckets and (c) the per-tile depth sorts, over
+// all views of the table: count matrix, tile totals, ranges, mid/long lists.
+struct BinLaunch {
+  uint32_t n_views;
+  uint32_t bin_ctas;      // total CTAs of the count and scatter launches
+  uint32_t col_ctas;      // total CTAs of the column-scan launch
+  uint32_t n_tiles;       // global tiles (views' tile ranges, padded)
+  uint32_t max_tiles;     // largest view's tile count
+  bool counts_zeroed;     // counts must be zeroed when a row does not fit shared memory
+  uint32_t* counts_all;   // all count matrices (for the zeroing)
+  size_t counts_bytes;
+};
+cudaError_t launch_binning(const ViewTask* table, const BinLaunch& bl, uint32_t* totals, uint2* ranges,
+                           uint32_t* mid_list, uint32_t* long_list, uint64_t* pairs, uint64_t* pairs_alt,
+                           uint64_t cap, const FrameCounters& fc, int num_sms, size_t max_smem, cudaStream_t stream,
+                           uint32_t* launches);
+// (d) blend + downsample over the depth-sorted buckets of every view.
+cudaError_t launch_blend(const ViewTask* table, uint32_t n_views, uint32_t n_tiles, const uint64_t* pairs,
+                         const uint2* ranges, bool exact, const BlendConfig& cfg, DevState* st, int num_sms,
+                         cudaStream_t stream, uint32_t* launches);
+// term::downsample of one view's full-resolution scratch frame.
+cudaError_t launch_downsample(const FrameParams& fp, const uint8_t* full, uint8_t* out, cudaStream_t stream,
+                              uint32_t* launches);
 
 }  // namespace splat

@@ -1,0 +1,80 @@
+// The renderer handle behind the C ABI (include/splat_cuda.h) and the host
+// helpers that the single-view entry points (api.cu) and the batch entry
+// points (batch.cu) share.
+#pragma once
+
+#include <string>
+
+#include "../../include/splat_cuda.h"
+#include "common.cuh"
+
+struct splat_cuda_handle {
+  int device = 0;
+  int num_sms = 148;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  uint64_t n = 0;
+  uint32_t sh_degree = 0;
+  uint32_t precision = SPLAT_PRECISION_FP32;
+  // scene (device)
+  float4* pos_op = nullptr;
+  float4* cov_a = nullptr;
+  float4* cov_b = nullptr;
+  float* color = nullptr;
+  float* sh = nullptr;
+  float4* pos_k = nullptr;   // FP16 storage: x, y, z, k
+  uint4* geom16 = nullptr;   // FP16 storage: scale, rotation, opacity halves
+  uint16_t* sh16 = nullptr;  // FP16 storage: base colour + SH planes
+  // per-splat frame buffers
+  splat::Record* rec = nullptr;
+  splat::BinInfo* bin = nullptr;
+  // pair buffers: per-tile buckets and the long-tile sort's scratch
+  uint64_t cap = 0;
+  uint64_t* pairs[2] = {nullptr, nullptr};
+  // per-size buffers
+  uint2* ranges = nullptr;
+  uint32_t* counts = nullptr;     // bin_rows x tiles
+  size_t counts_cap = 0;          // words
+  uint32_t* totals = nullptr;     // tiles
+  uint32_t* mid_list = nullptr;   // tiles
+  uint32_t* long_list = nullptr;  // tiles
+  uint64_t ranges_cap = 0;        // tiles
+  size_t max_smem = 48 * 1024;
+  uint8_t* out_dev = nullptr;
+  size_t out_cap = 0;
+  uint8_t* full_dev = nullptr;
+  size_t full_cap = 0;
+  // frame state
+  splat::DevState* st = nullptr;       // the frame counters (splat::DevState first)
+  splat::DevState* st_host = nullptr;  // pinned copy of splat::DevState + the view's counters
+  uint32_t chunks_cap = 0;      // tile-scan chunks the counters hold
+  splat::ViewTask* table = nullptr;    // the view table (one entry)
+  splat::BlendConfig blend{splat::kTile, splat::kTile, 256};
+  uint8_t* stage = nullptr;     // pinned staging for pageable outputs
+  size_t stage_cap = 0;
+  // debug capture
+  float* dbg_proj = nullptr;
+  float* dbg_color = nullptr;
+  bool debug_capture = false;
+  // options
+  bool exact = false;
+  bool stage_events = true;
+  uint32_t launches = 0;  // kernels this handle has launched (wraps at 2^32)
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  // last frame
+  splat::FrameParams last_fp{};
+  bool have_frame = false;
+  std::string err;
+};
+
+
+namespace splat {
+
+// ProjectCtx::new with View::rotation/focal, in f32 as the reference computes it.
+FrameParams make_params(const splat_view_desc& v, uint32_t w, uint32_t h, const float bg[3], uint32_t f);
+// Sets the tile shape (powers of two), its logs and the tile grid of a frame.
+void set_tile_shape(FrameParams& p, uint32_t tile_w, uint32_t tile_h);
+// The handle's device scene as the kernels read it.
+SceneDev scene_dev(const splat_cuda_handle* h);
+
+}  // namespace splat

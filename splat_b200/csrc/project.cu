@@ -10,6 +10,8 @@
 // count and depth bits for the binning, and counts the visible splats.
 #include <cuda_fp16.h>
 
+#include <cstddef>
+
 #include "common.cuh"
 
 namespace splat {
@@ -140,15 +142,15 @@ __device__ __forceinline__ void conic_terms(const T c[6], T t0x, T t0y, T t0z, T
 // F16: the scene is stored in FP16 (positions FP32); the 3D covariance is
 // formed here in FP32, and a 2D covariance whose FP32 determinant falls below
 // kFp64DetBelow is recomputed in FP64.
+// Projects splat i < s.n of the view: writes its record (when visible), its
+// tile rectangle and the optional debug values; reports visibility and
+// whether its conic took the FP64 path.
 template <int DEG, bool F16>
-__global__ void __launch_bounds__(256) k_project(FrameParams fp, SceneDev s, Record* __restrict__ rec,
-                                                 BinInfo* __restrict__ bin, float* __restrict__ dbg_proj,
-                                                 float* __restrict__ dbg_color, DevState* st) {
-  const int tid = threadIdx.x;
-  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + tid;
-  bool vis = false;
-  bool used_fp64 = false;
-  if (i < s.n) {
+__device__ __forceinline__ void project_splat(const FrameParams& fp, const SceneDev& s, uint64_t i,
+                                              Record* __restrict__ rec, BinInfo* __restrict__ bin,
+                                              float* __restrict__ dbg_proj, float* __restrict__ dbg_color,
+                                              bool& vis, bool& used_fp64) {
+  {
     float px, py, pz, opacity, k;
     uint4 g16 = make_uint4(0, 0, 0, 0);
     if (F16) {
@@ -290,8 +292,8 @@ __global__ void __launch_bounds__(256) k_project(FrameParams fp, SceneDev s, Rec
       rec[i] = r;
       b.depth_bits = __float_as_uint(tz);
       if (bx0 < x1 && by0 < y1) {
-        const uint32_t tx0 = bx0 / kTile, ty0 = by0 / kTile;
-        const uint32_t tx1 = (x1 + kTile - 1) / kTile, ty1 = (y1 + kTile - 1) / kTile;
+        const uint32_t tx0 = bx0 >> fp.tile_sx, ty0 = by0 >> fp.tile_sy;
+        const uint32_t tx1 = (x1 + fp.tile_w - 1) >> fp.tile_sx, ty1 = (y1 + fp.tile_h - 1) >> fp.tile_sy;
         b.rect_lo = tx0 | (ty0 << 16);
         b.rect_hi = tx1 | (ty1 << 16);
         b.count = (tx1 - tx0) * (ty1 - ty0);
@@ -318,35 +320,90 @@ __global__ void __launch_bounds__(256) k_project(FrameParams fp, SceneDev s, Rec
       dbg_color[3 * i + 2] = vis ? col[2] : 0.f;
     }
   }
+}
+
+__device__ __forceinline__ void count_visible(bool vis, bool used_fp64, const FrameCounters& fc, uint32_t view) {
   const int nvis = __syncthreads_count(vis);
-  if (tid == 0 && nvis) atomicAdd(&st->visible, (unsigned long long)nvis);
-  if (F16) {
-    const int n64 = __syncthreads_count(used_fp64);
-    if (tid == 0 && n64) atomicAdd(&st->fp64_conics, (unsigned)n64);
+  const int n64 = __syncthreads_count(used_fp64);
+  if (threadIdx.x == 0) {
+    if (nvis) {
+      atomicAdd(&fc.st->visible, (unsigned long long)nvis);
+      atomicAdd(&fc.view_visible[view], (unsigned long long)nvis);
+    }
+    if (n64) atomicAdd(&fc.st->fp64_conics, (unsigned)n64);
   }
+}
+
+// One view, passed by value; CTA 0 also stores it as the view table's only
+// entry for the launches that follow.
+template <int DEG, bool F16>
+__global__ void __launch_bounds__(256) k_project(ViewTask t, ViewTask* __restrict__ table,
+                                                 float* __restrict__ dbg_proj, float* __restrict__ dbg_color,
+                                                 FrameCounters fc) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) *table = t;
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  bool vis = false, used_fp64 = false;
+  if (i < t.s.n) project_splat<DEG, F16>(t.fp, t.s, i, t.rec, t.bin, dbg_proj, dbg_color, vis, used_fp64);
+  count_visible(vis, used_fp64, fc, 0);
+}
+
+// Every view of the table: CTA c projects 256 splats of the view whose
+// proj_cta0 is the largest one <= c (views of different scenes, SH degrees
+// and storage precisions in one launch).
+__global__ void __launch_bounds__(256) k_project_batch(const ViewTask* __restrict__ table, uint32_t n_views,
+                                                       FrameCounters fc) {
+  __shared__ ViewTask s_t;
+  const uint32_t v = find_view(table, n_views, blockIdx.x, offsetof(ViewTask, proj_cta0));
+  static_assert(sizeof(ViewTask) % 16 == 0, "ViewTask copies as uint4");
+  if (threadIdx.x < sizeof(ViewTask) / 16)
+    reinterpret_cast<uint4*>(&s_t)[threadIdx.x] = __ldg(reinterpret_cast<const uint4*>(table + v) + threadIdx.x);
+  __syncthreads();
+  const uint64_t i = (uint64_t)(blockIdx.x - s_t.proj_cta0) * blockDim.x + threadIdx.x;
+  bool vis = false, used_fp64 = false;
+  if (i < s_t.s.n) {
+    switch (s_t.s.sh_degree * 2 + (s_t.s.fp16 ? 1 : 0)) {
+      case 0: project_splat<0, false>(s_t.fp, s_t.s, i, s_t.rec, s_t.bin, nullptr, nullptr, vis, used_fp64); break;
+      case 1: project_splat<0, true>(s_t.fp, s_t.s, i, s_t.rec, s_t.bin, nullptr, nullptr, vis, used_fp64); break;
+      case 2: project_splat<1, false>(s_t.fp, s_t.s, i, s_t.rec, s_t.bin, nullptr, nullptr, vis, used_fp64); break;
+      case 3: project_splat<1, true>(s_t.fp, s_t.s, i, s_t.rec, s_t.bin, nullptr, nullptr, vis, used_fp64); break;
+      case 4: project_splat<2, false>(s_t.fp, s_t.s, i, s_t.rec, s_t.bin, nullptr, nullptr, vis, used_fp64); break;
+      case 5: project_splat<2, true>(s_t.fp, s_t.s, i, s_t.rec, s_t.bin, nullptr, nullptr, vis, used_fp64); break;
+      case 6: project_splat<3, false>(s_t.fp, s_t.s, i, s_t.rec, s_t.bin, nullptr, nullptr, vis, used_fp64); break;
+      default: project_splat<3, true>(s_t.fp, s_t.s, i, s_t.rec, s_t.bin, nullptr, nullptr, vis, used_fp64); break;
+    }
+  }
+  count_visible(vis, used_fp64, fc, v);
 }
 
 }  // namespace
 
-cudaError_t launch_project(const FrameParams& fp, const SceneDev& s, Record* rec, BinInfo* bin, float* dbg_proj,
-                           float* dbg_color, DevState* st, cudaStream_t stream, uint32_t* launches) {
-  if (s.n == 0) return cudaSuccess;
-  *launches += 1;
-  const unsigned grid = (unsigned)((s.n + 255) / 256);
+cudaError_t launch_project(const ViewTask& t, ViewTask* table, float* dbg_proj, float* dbg_color,
+                           const FrameCounters& fc, cudaStream_t stream, uint32_t* launches) {
+  // An empty scene still stores the view table.
+  const unsigned grid = t.s.n ? (unsigned)((t.s.n + 255) / 256) : 1u;
 #define SPLAT_PROJECT(D)                                                                          \
   do {                                                                                            \
-    if (s.fp16)                                                                                   \
-      k_project<D, true><<<grid, 256, 0, stream>>>(fp, s, rec, bin, dbg_proj, dbg_color, st);     \
+    if (t.s.fp16)                                                                                 \
+      k_project<D, true><<<grid, 256, 0, stream>>>(t, table, dbg_proj, dbg_color, fc);            \
     else                                                                                          \
-      k_project<D, false><<<grid, 256, 0, stream>>>(fp, s, rec, bin, dbg_proj, dbg_color, st);    \
+      k_project<D, false><<<grid, 256, 0, stream>>>(t, table, dbg_proj, dbg_color, fc);           \
   } while (0)
-  switch (s.sh_degree) {
+  switch (t.s.sh_degree) {
     case 0: SPLAT_PROJECT(0); break;
     case 1: SPLAT_PROJECT(1); break;
     case 2: SPLAT_PROJECT(2); break;
     default: SPLAT_PROJECT(3); break;
   }
 #undef SPLAT_PROJECT
+  *launches += 1;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_project_batch(const ViewTask* table, uint32_t n_views, uint32_t total_ctas,
+                                 const FrameCounters& fc, cudaStream_t stream, uint32_t* launches) {
+  if (total_ctas == 0) return cudaSuccess;
+  k_project_batch<<<total_ctas, 256, 0, stream>>>(table, n_views, fc);
+  *launches += 1;
   return cudaGetLastError();
 }
 

@@ -204,6 +204,11 @@ class CudaRenderer(Renderer):
         N.check(N.lib().splat_cuda_get_option(self._h, option, ctypes.byref(v)), self._h, "get_option")
         return int(v.value)
 
+    def set_blend_config(self, tile_w: int, tile_h: int, threads: int):
+        """Tile shape and blend threads: (8, 8), (16, 16) or (32, 16) tiles with
+        128, 256 or 512 threads. The image does not depend on it."""
+        self.set_option(N.SPLAT_OPT_BLEND_CONFIG, N.pack_blend_config(tile_w, tile_h, threads))
+
     def set_exact(self, exact: bool):
         """Blend with the reference cpu backend's exact f32 arithmetic."""
         self.set_option(N.SPLAT_OPT_EXACT_BLEND, int(exact))
@@ -222,7 +227,9 @@ class CudaRenderer(Renderer):
         vis = np.zeros(n, np.uint8)
         col = np.zeros((n, 3), np.float32)
         npairs = ctypes.c_uint64(0)
-        tiles = ((width + TILE - 1) // TILE) * ((height + TILE - 1) // TILE)
+        packed = self.get_option(N.SPLAT_OPT_BLEND_CONFIG)
+        tw, th = packed & 0xFF, (packed >> 8) & 0xFF
+        tiles = ((width + tw - 1) // tw) * ((height + th - 1) // th)
         ranges = np.zeros((tiles, 2), np.uint32)
         N.check(L.splat_cuda_debug_dump(self._h, None, None, None, None, None, 0, None, 0, ctypes.byref(npairs)),
                 self._h, "debug_dump")

@@ -166,3 +166,21 @@ def test_half_scene_round_trip():
     ds = half.decoded_scene()
     scale = np.max(np.abs(s.cov3d[:, [0, 3, 5]]), axis=1, keepdims=True)  # largest variance per splat
     assert np.all(np.abs(ds.cov3d - s.cov3d) <= 5e-3 * scale)
+
+
+def test_batch_abi_layouts_and_validation_without_a_gpu(cuda_lib):
+    # splat_batch_view: 4 u32 + view (14 f32) + 3 f32 + u32 + pointer.
+    assert ctypes.sizeof(N.BatchViewC) == 16 + 56 + 12 + 4 + 8
+    assert ctypes.sizeof(N.BlendConfigC) == 12
+    assert ctypes.sizeof(N.TuneResultC) == 24
+    b = ctypes.c_void_p()
+    assert cuda_lib.splat_cuda_batch_create(None, 0, None, 0, ctypes.byref(b)) == N.SPLAT_ERR_INVALID_ARG
+    assert b"no scenes" in cuda_lib.splat_cuda_batch_create_error()
+    handles = (ctypes.c_void_p * 1)(None)
+    views = (N.BatchViewC * 1)()
+    assert cuda_lib.splat_cuda_batch_create(handles, 1, views, 1, ctypes.byref(b)) == N.SPLAT_ERR_INVALID_ARG
+    assert b"null scene" in cuda_lib.splat_cuda_batch_create_error()
+    assert cuda_lib.splat_cuda_batch_destroy(None) == N.SPLAT_OK
+    assert cuda_lib.splat_cuda_batch_run(None) == N.SPLAT_ERR_INVALID_ARG
+    assert cuda_lib.splat_cuda_batch_last_error(None) == b""
+    assert len(N.BLEND_CONFIGS) == 9 and len(set(N.BLEND_CONFIGS)) == 9
