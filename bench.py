@@ -47,6 +47,10 @@ CONFIGS = {
     "plain": {"metric": "frames/s at 1920x1080, 1.2M SH3 splats", "w": 1920, "h": 1080, "precision": "fp32",
               "s_in": 232,  # f32 position, opacity, colour, cov3d, 45 SH coefficients
               "workload": "1.2M SH-degree-3 gaussians (64 seeded clusters), 1920x1080, 16x16 tiles, 40-view orbit"},
+    "batch": {"metric": "views/s, 96 views of mixed resolution over 3 scenes (50k SH0, 400k SH1, 3M SH3)",
+              "workload": "3 seeded cluster scenes (50k SH0, 400k SH1, 3M SH3, f32), 96 views: resolution uniform "
+                          "from 160x96..3840x2160, yaw U[0, 2pi), pitch U[-0.6, 0.6], FOV U[40, 70] deg, "
+                          "distance 12; one CUDA graph per batch"},
     "fp16": {"metric": "frames/s at 3840x2160, 1.2M SH3 splats, FP16 storage", "w": 3840, "h": 2160,
              "precision": "fp16",
              "s_in": 124,  # f32 position; f16 scale, rotation, opacity, 48 SH coefficients
@@ -58,10 +62,13 @@ CONFIGS = {
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=4000)
+    p.add_argument("--steps", type=int, default=None,
+                   help="timed steps (default: 4000 frames plain, 1000 fp16, 20 batches)")
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--config", default="plain", choices=sorted(CONFIGS))
+    p.add_argument("--batch-views", type=int, default=96)
+    p.add_argument("--batch-scale", type=float, default=1.0, help="batch: scale the three scene sizes")
     p.add_argument("--error-frames", type=int, default=2,
                    help="fp16: frames whose error against the FP64 naive rasterizer is stated")
     p.add_argument("--splats", type=int, default=N_SPLATS)
@@ -69,7 +76,10 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--profile", action="store_true",
                    help="render --warmup then --steps frames and exit (a short command for ncu captures)")
-    return p.parse_args()
+    a = p.parse_args()
+    if a.steps is None:
+        a.steps = {"plain": 4000, "fp16": 1000, "batch": 20}[a.config]
+    return a
 
 
 def dist_env():
@@ -402,9 +412,246 @@ def run_ours(args):
         torch.distributed.destroy_process_group()
 
 
+def batch_workload(args):
+    from splat_b200 import synth
+
+    n = max(args.batch_scale, 1e-6)
+    sizes = tuple(max(int(x * n), 1000) for x in (50_000, 400_000, 3_000_000))
+    scenes = synth.batch_scenes(sizes=sizes)
+    views = synth.batch_views(scenes, n_views=args.batch_views)
+    return scenes, views
+
+
+def run_batch_reference(args):
+    """The oracle's cpu backend over the batch's views, one after another,
+    all host threads, for a bounded time."""
+    rank, world, _ = dist_env()
+    if world > 1 and rank != 0:
+        return
+    cfg = CONFIGS["batch"]
+    scenes, views = batch_workload(args)
+    from oracle import oracle as O
+
+    cpus = [O.CpuTiled(s, threads=0) for s in scenes]
+    t_start = time.perf_counter()
+    times, pixels = [], 0
+    i = 0
+    while i < len(views) * max(args.steps, 1):
+        k, v, w, h = views[i % len(views)]
+        out = np.zeros((h, w, 3), np.uint8)
+        t0 = time.perf_counter()
+        cpus[k].render(v, w, h, (0, 0, 0), out)
+        times.append(time.perf_counter() - t0)
+        pixels += w * h
+        i += 1
+        if time.perf_counter() - t_start > 120.0:
+            break
+    vps = len(times) / sum(times)
+    threads = cpus[0].threads
+    for c in cpus:
+        c.close()
+    line = {
+        "impl": "reference", "metric": cfg["metric"], "value": vps, "unit": "views/s", "n_gpus": 0,
+        "steps": len(times), "warmup": 0, "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": cfg["workload"], "views": len(views)},
+        "cpu_baseline": {"value": vps, "unit": "views/s", "cores": threads, "kind": "port",
+                         "sample": f"{len(times)} views of the batch, one at a time"},
+        "e2e": {"value": vps, "unit": "views/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_batch(args):
+    """The batching workload: every view rendered one at a time through the
+    single-view path (the baseline), then the whole batch as one recorded
+    CUDA graph after the tuner picked its tile shape and block size."""
+    import torch
+
+    rank, world, local = dist_env()
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+    cfg = CONFIGS["batch"]
+    from splat_b200 import _native as Nat
+    from splat_b200.batch import BatchRenderer, BatchView
+    from splat_b200.render import CudaRenderer
+
+    scenes, views_all = batch_workload(args)
+    views = views_all[rank::world] if world > 1 else views_all
+    rends = [CudaRenderer(s, device=dev) for s in scenes]
+    stream = torch.cuda.Stream(device=dev)
+    for r in rends:
+        r.set_stream(stream.cuda_stream)
+    max_bytes = max(w * h * 3 for _, _, w, h in views)
+    out = torch.empty(max_bytes, dtype=torch.uint8, device=dev)
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    if args.profile:
+        # A short command for ncu: the batch with the default configuration,
+        # --warmup + --steps replays.
+        b = BatchRenderer(rends, [BatchView(k, v, w, h) for k, v, w, h in views])
+        for _ in range(args.warmup + args.steps):
+            stats, _ = b.render()
+        if rank == 0:
+            print(json.dumps({"profile_batches": args.steps, "visible": sum(x.visible for x in stats),
+                              "pairs": sum(x.overlaps for x in stats)}), flush=True)
+        b.close()
+        for r in rends:
+            r.close()
+        return
+
+    # Baseline: the single-view path, one view after another on one stream.
+    for k, v, w, h in views:  # capacity growth settles here
+        while True:
+            rends[k].render_device(v, w, h, (0, 0, 0), out.data_ptr(), max_bytes)
+            _, regrown = rends[k].finish()
+            if not regrown:
+                break
+    K1 = max(1, args.steps // 10)
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    s0.record(stream)
+    for _ in range(K1):
+        for k, v, w, h in views:
+            rends[k].render_device(v, w, h, (0, 0, 0), out.data_ptr(), max_bytes)
+    s1.record(stream)
+    barrier()
+    single_vps = len(views) * K1 / (s0.elapsed_time(s1) / 1e3)
+
+    # The batch: tuner, then K replays of the recorded graph.
+    b = BatchRenderer(rends, [BatchView(k, v, w, h) for k, v, w, h in views])
+    tune = b.autotune(reps=3)
+    bstream = torch.cuda.ExternalStream(b.stream(), device=dev)
+    for _ in range(max(args.warmup, 3)):
+        b.render()
+    K = args.steps
+    launches0 = b.get_option(Nat.SPLAT_OPT_KERNEL_LAUNCHES)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    with Clocks(dev) as clk:
+        start.record(bstream)
+        for _ in range(K):
+            b.run()
+        end.record(bstream)
+        stats, batch_ms, regrown = b.finish()
+        barrier()
+    launches = (b.get_option(Nat.SPLAT_OPT_KERNEL_LAUNCHES) - launches0) % (1 << 32)
+    assert not regrown, "pair buffers overflowed inside the timed region"
+    ms = start.elapsed_time(end)
+    t = torch.tensor([ms], device=dev)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    ms_max = float(t.item())
+    views_total = len(views_all) if world > 1 else len(views)
+    value = views_total * K / (ms_max / 1e3)
+    stats, _ = b.render()  # stage times of one batch
+    stage = {"project_ms": stats[0].project_ms, "sort_ms": stats[0].sort_ms, "raster_ms": stats[0].raster_ms}
+
+    # End to end: the batch plus every frame copied to pinned host memory.
+    host = torch.empty(b.frames_dev.numel(), dtype=torch.uint8).pin_memory()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(K):
+        b.run()
+        with torch.cuda.stream(bstream):
+            host.copy_(b.frames_dev, non_blocking=True)
+        b.finish()
+    e2e_s = time.perf_counter() - t0
+    te = torch.tensor([e2e_s], device=dev)
+    if world > 1:
+        torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
+    e2e = views_total * K / float(te.item())
+
+    if rank == 0:
+        peak, peak_kind = measured_peaks()
+        N_in = sum(len(scenes[k].opacities) for k, _, _, _ in views)
+        s_in = {0: 32, 1: 68, 2: 128, 3: 232}
+        B_in = sum(len(scenes[k].opacities) * s_in[scenes[k].sh_degree] for k, _, _, _ in views)
+        V = sum(s.visible for s in stats)
+        P = sum(s.overlaps for s in stats)
+        px = sum(w * h for _, _, w, h in views)
+        tiles = sum(((w + 15) // 16) * ((h + 15) // 16) for _, _, w, h in views)
+        bytes_stage = {
+            "project": B_in + N_in * S_BIN + V * S_REC,
+            "sort": 2 * N_in * S_BIN + P * 8 + 2 * P * 8,
+            "raster": P * (8 + S_REC) + tiles * 8 + px * 3,
+        }
+        times = {"project": stage["project_ms"], "sort": stage["sort_ms"], "raster": stage["raster_ms"]}
+        dom = max(times, key=times.get)
+        achieved = bytes_stage[dom] / (times[dom] / 1e3) / 1e9
+        cpu = None
+        if not args.no_cpu_baseline:
+            from oracle import oracle as O
+
+            cpus = [O.CpuTiled(s, threads=0) for s in scenes]
+            t_end = time.perf_counter() + args.cpu_sample_s
+            n_cpu, t_cpu, i = 0, 0.0, 0
+            while time.perf_counter() < t_end or n_cpu < 2:
+                k, v, w, h = views[i % len(views)]
+                o = np.zeros((h, w, 3), np.uint8)
+                t1 = time.perf_counter()
+                cpus[k].render(v, w, h, (0, 0, 0), o)
+                t_cpu += time.perf_counter() - t1
+                n_cpu += 1
+                i += 1
+            cpu = {"value": n_cpu / t_cpu, "unit": "views/s", "cores": cpus[0].threads, "kind": "port",
+                   "sample": f"the first {n_cpu} views of the batch, one at a time (~{args.cpu_sample_s:.0f} s)"}
+            for c in cpus:
+                c.close()
+        line = {
+            "metric": cfg["metric"], "value": value, "unit": "views/s", "n_gpus": world, "steps": K,
+            "warmup": args.warmup, "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": cfg["workload"], "views": views_total, "splats_projected": N_in,
+                       "pixels": px, "visible": V, "pairs": P, "parallelism": f"view-parallel x{world}",
+                       "blend_config": list(b.config), "l2": "inputs larger than L2 (scenes 0.8 GB > 126 MB)"},
+            "single_view_path_views_per_s": single_vps,
+            "batch_speedup_vs_single_view_path": value / world / single_vps if world == 1 else None,
+            "tuner": [{"tile": [c[0], c[1]], "threads": c[2], "ms": m} for c, m in tune],
+            "stages_ms": stage,
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                         "algorithmic_bytes": bytes_stage[dom]},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e, "unit": "views/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": int(b.frames_dev.numel()),
+                    "note": "the recorded batch replayed (views fixed in the graph), then every view's frame "
+                            "copied to pinned host memory"},
+            "clocks": clk.summary(),
+            "gpu_launches": launches,
+        }
+        print(json.dumps(line), flush=True)
+    # Free what torch used on the batch's and the renderers' streams before
+    # those streams are destroyed.
+    torch.cuda.synchronize()
+    del host, out, bstream
+    b.close()
+    for r in rends:
+        r.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
 def main():
     args = parse()
-    if args.impl == "reference":
+    if args.config == "batch":
+        if args.impl == "reference":
+            run_batch_reference(args)
+        else:
+            run_batch(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

@@ -286,8 +286,9 @@ int splat_cuda_batch_autotune(splat_cuda_batch* b, uint32_t reps, splat_tune_res
 /* Launches the recorded graph on the batch's stream; does not wait. */
 int splat_cuda_batch_run(splat_cuda_batch* b);
 /* Waits for the launched batches; per_view (n_views entries, may be NULL)
- * gets each view's visible splats and pairs, total_ms (may be NULL) the
- * device time of the last batch. *regrown = 1 when a batch overflowed the
+ * gets each view's visible splats and pairs and the device times of the
+ * last batch's stages (projection, binning + sorts, blend: the same for
+ * every view), total_ms (may be NULL) the device time of the last batch. *regrown = 1 when a batch overflowed the
  * pair buffers: they have been grown and the graph re-recorded; run again. */
 int splat_cuda_batch_finish(splat_cuda_batch* b, splat_render_stats* per_view, double* total_ms, int* regrown);
 /* Options: SPLAT_OPT_EXACT_BLEND and SPLAT_OPT_KERNEL_LAUNCHES as for a

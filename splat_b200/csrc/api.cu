@@ -253,9 +253,10 @@ int finish_frame(splat_cuda_handle* h, splat_render_stats* stats, int* regrown) 
     stats->overlaps = st.total_pairs;
     if (h->stage_events) {
       float a = 0, b = 0, c = 0;
-      cudaEventElapsedTime(&a, h->ev[0], h->ev[1]);
-      cudaEventElapsedTime(&b, h->ev[1], h->ev[2]);
-      cudaEventElapsedTime(&c, h->ev[2], h->ev[3]);
+      if (cudaEventElapsedTime(&a, h->ev[0], h->ev[1]) != cudaSuccess ||
+          cudaEventElapsedTime(&b, h->ev[1], h->ev[2]) != cudaSuccess ||
+          cudaEventElapsedTime(&c, h->ev[2], h->ev[3]) != cudaSuccess)
+        cudaGetLastError();  // stage times unavailable; do not leave the error pending
       stats->project_ms = a;
       stats->sort_ms = b;
       stats->raster_ms = c;

@@ -62,7 +62,8 @@ struct splat_cuda_batch {
   // the recorded batch
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
-  cudaEvent_t ev[2] = {nullptr, nullptr};
+  cudaEvent_t ev[2] = {nullptr, nullptr};     // around a graph launch
+  cudaEvent_t stage[4] = {nullptr, nullptr, nullptr, nullptr};  // between stages, inside the graph
   bool ran = false;
   std::string err;
 };
@@ -192,12 +193,35 @@ int plan(splat_cuda_batch* b) {
   return SPLAT_OK;
 }
 
+// Records stage event k on `s`; under stream capture as an external event
+// node, so that the graph's replays record it.
+cudaError_t stage_event(splat_cuda_batch* b, int k, cudaStream_t s) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  const cudaError_t e = cudaStreamIsCapturing(s, &cs);
+  if (e != cudaSuccess) return e;
+  return cs == cudaStreamCaptureStatusActive ? cudaEventRecordWithFlags(b->stage[k], s, cudaEventRecordExternal)
+                                             : cudaEventRecord(b->stage[k], s);
+}
+
+// Elapsed time between two events, 0 when it is not available (the error is
+// cleared so that it does not surface at a later launch check).
+float elapsed_ms(cudaEvent_t a, cudaEvent_t c) {
+  float ms = 0.0f;
+  if (cudaEventElapsedTime(&ms, a, c) != cudaSuccess) {
+    cudaGetLastError();
+    ms = 0.0f;
+  }
+  return ms;
+}
+
 // Enqueues one batch on `s` (plain or under stream capture).
 int enqueue(splat_cuda_batch* b, cudaStream_t s) {
   const uint32_t nv = (uint32_t)b->views.size();
   const FrameCounters fc = frame_counters_at(b->counters, nv);
   BK(cudaMemsetAsync(b->counters, 0, b->counters_bytes, s), "clear counters");
+  BK(stage_event(b, 0, s), "event");
   BK(launch_project_batch(b->table, nv, b->proj_ctas, fc, s, &b->launches), "project kernel");
+  BK(stage_event(b, 1, s), "event");
   BinLaunch bl{};
   bl.n_views = nv;
   bl.bin_ctas = b->bin_ctas;
@@ -209,9 +233,11 @@ int enqueue(splat_cuda_batch* b, cudaStream_t s) {
   BK(launch_binning(b->table, bl, b->totals, b->ranges, b->mid_list, b->long_list, b->pairs[0], b->pairs[1], b->cap,
                     fc, b->num_sms, b->max_smem, s, &b->launches),
      "binning kernels");
+  BK(stage_event(b, 2, s), "event");
   BK(launch_blend(b->table, nv, b->n_tiles, b->pairs[0], b->ranges, b->exact, b->cfg, fc.st, b->num_sms, s,
                   &b->launches),
      "blend kernel");
+  BK(stage_event(b, 3, s), "event");
   BK(cudaMemcpyAsync(b->counters_host, b->counters, b->counters_bytes, cudaMemcpyDeviceToHost, s), "copy counters");
   return SPLAT_OK;
 }
@@ -275,6 +301,8 @@ void destroy(splat_cuda_batch* b) {
   dfree(b->bin);
   for (auto& e : b->ev)
     if (e) cudaEventDestroy(e);
+  for (auto& e : b->stage)
+    if (e) cudaEventDestroy(e);
   if (b->own_stream) cudaStreamDestroy(b->own_stream);
   delete b;
 }
@@ -324,6 +352,8 @@ SPLAT_API int splat_cuda_batch_create(splat_cuda_handle* const* scenes, uint32_t
     return bail(bcuda(b, e, "cudaStreamCreate"));
   b->stream = b->own_stream;
   for (auto& ev : b->ev)
+    if ((e = cudaEventCreate(&ev)) != cudaSuccess) return bail(bcuda(b, e, "cudaEventCreate"));
+  for (auto& ev : b->stage)
     if ((e = cudaEventCreate(&ev)) != cudaSuccess) return bail(bcuda(b, e, "cudaEventCreate"));
   uint64_t splats = 0;
   b->splat_off.resize(n_views);
@@ -386,14 +416,20 @@ SPLAT_API int splat_cuda_batch_finish(splat_cuda_batch* b, splat_render_stats* p
   BK(cudaStreamSynchronize(b->stream), "batch");
   const uint32_t nv = (uint32_t)b->views.size();
   const FrameCounters fc = frame_counters_at(b->counters_host, nv);
-  float ms = 0.0f;
-  if (b->ran) cudaEventElapsedTime(&ms, b->ev[0], b->ev[1]);
+  float ms = 0.0f, st[3] = {0.0f, 0.0f, 0.0f};
+  if (b->ran) {
+    ms = elapsed_ms(b->ev[0], b->ev[1]);
+    for (int k = 0; k < 3; k++) st[k] = elapsed_ms(b->stage[k], b->stage[k + 1]);
+  }
   if (total_ms) *total_ms = ms;
   if (per_view)
     for (uint32_t i = 0; i < nv; i++) {
       per_view[i] = splat_render_stats{};
       per_view[i].visible = fc.view_visible[i];
       per_view[i].overlaps = fc.view_pairs[i];
+      per_view[i].project_ms = st[0];  // stage times of the whole batch
+      per_view[i].sort_ms = st[1];
+      per_view[i].raster_ms = st[2];
       per_view[i].total_ms = ms;
     }
   if (fc.st->total_pairs > b->cap) {

@@ -27,6 +27,7 @@
 // whatever the atomics produced; the per-tile depth sort that follows (in the
 // blend CTA, or k_sort_long for long tiles) restores the reference's order.
 #include <algorithm>
+#include <atomic>
 #include <cstddef>
 
 #include "common.cuh"
@@ -449,8 +450,20 @@ cudaError_t launch_binning(const ViewTask* table, const BinLaunch& bl, uint32_t*
     k_bin_scatter<false><<<bl.bin_ctas, kBinThreads, 0, stream>>>(table, bl.n_views, ranges, pairs, cap);
   }
   k_sort_small<<<(bl.n_tiles + 7) / 8, 256, 0, stream>>>(ranges, bl.n_tiles, pairs);
-  k_sort_mid<<<num_sms * 3, kTileThreads, sizeof(MidSmem), stream>>>(ranges, mid_list, pairs, fc.st);
-  k_sort_long<<<num_sms, kTileThreads, 0, stream>>>(ranges, long_list, pairs, pairs_alt, cap, fc.st);
+  // The mid and long sorts loop over their tile lists: as many CTAs as fit
+  // on the device at once (looked up once).
+  static std::atomic<int> occ_mid{0}, occ_long{0};
+  if (occ_mid.load(std::memory_order_relaxed) == 0 && cs == cudaStreamCaptureStatusNone) {
+    int om = 0, ol = 0;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&om, k_sort_mid, kTileThreads, sizeof(MidSmem)))) return e;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ol, k_sort_long, kTileThreads, 0))) return e;
+    occ_long.store(std::max(ol, 1), std::memory_order_relaxed);
+    occ_mid.store(std::max(om, 1), std::memory_order_relaxed);
+  }
+  const int om = std::max(occ_mid.load(std::memory_order_relaxed), 1);
+  const int ol = std::max(occ_long.load(std::memory_order_relaxed), 1);
+  k_sort_mid<<<num_sms * om, kTileThreads, sizeof(MidSmem), stream>>>(ranges, mid_list, pairs, fc.st);
+  k_sort_long<<<num_sms * ol, kTileThreads, 0, stream>>>(ranges, long_list, pairs, pairs_alt, cap, fc.st);
   *launches += 7;
   return cudaGetLastError();
 }

@@ -138,3 +138,30 @@ def orbit_views(cam: OrbitCamera, frames: int, warmup: int):
         cam.pitch = f32(0.4) * f32(np.sin(f32(i) * f32(0.1)))
         timed.append(cam.view())
     return home, warm, timed
+
+
+BATCH_SIZES = [(160, 96), (320, 192), (640, 360), (1280, 720), (1920, 1080), (3840, 2160)]
+
+
+def batch_scenes(sizes=(50_000, 400_000, 3_000_000), degrees=(0, 1, 3), seed: int = 0x5EED0B00):
+    """The batching workload's scenes: cluster scenes with the 1.2M workload's
+    distributions, separate seeds (seed + index)."""
+    return [cluster_scene(n, seed=seed + i, sh_degree=d) for i, (n, d) in enumerate(zip(sizes, degrees))]
+
+
+def batch_views(scenes, n_views: int = 96, seed: int = 0x5EED0B96, sizes=BATCH_SIZES):
+    """n_views (scene index, view, width, height) over `scenes`: scene uniform,
+    resolution uniform from `sizes`, yaw U[0, 2 pi), pitch U[-0.6, 0.6], FOV
+    U[40, 70] degrees, target 0 at distance 12, up -y."""
+    u = uniform(seed, 5 * n_views).reshape(n_views, 5)
+    out = []
+    cams = [orbit_camera(s) for s in scenes]
+    for i in range(n_views):
+        k = min(int(u[i, 0] * len(scenes)), len(scenes) - 1)
+        w, h = sizes[min(int(u[i, 1] * len(sizes)), len(sizes) - 1)]
+        base = cams[k]
+        cam = OrbitCamera(base.target.copy(), base.distance, f32(u[i, 2] * f32(2.0 * np.pi)),
+                          f32(u[i, 3] * f32(1.2) - f32(0.6)), to_radians(f32(40.0) + f32(30.0) * u[i, 4]), base.up,
+                          base.scene_radius)
+        out.append((k, cam.view(), w, h))
+    return out
