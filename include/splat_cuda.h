@@ -306,6 +306,110 @@ int splat_cuda_batch_destroy(splat_cuda_batch* b);
 /* Text describing the last failure on this handle ("" if none). */
 const char* splat_cuda_last_error(const splat_cuda_handle* h);
 
+/*
+ * Learned colour. No counterpart in the reference, which evaluates degree-3
+ * SH per splat (src/sh.rs:39-64 via src/render/mod.rs:250-257). Each splat's
+ * 48 SH floats are replaced by SPLAT_MLP_LATENT fp16 latents, decoded by one
+ * MLP shared by all splats:
+ *   x = [latent (16) | unit view direction p - eye (3) | 1 | 0 x 12]
+ *   rgb = sigmoid(W3 relu(W2 relu(W1 x) + b2) + b3)
+ * with fp16 weights and fp32 accumulation on the tensor cores; b1 is W1's
+ * column 19. The view direction is the one the SH colour would be evaluated
+ * at (normalize_or_zero(p - eye), src/render/mod.rs:250-252).
+ *
+ * Parameter vector: SPLAT_MLP_PARAMS values (fp32 masters or fp16 bit
+ * patterns), matrices row-major [out][in], at these offsets:
+ */
+#define SPLAT_MLP_LATENT 16u
+#define SPLAT_MLP_W1 0u    /* 64 x 32; inputs 0-15 latent, 16-18 direction,
+                              19 the bias b1, 20-31 zero */
+#define SPLAT_MLP_W2 2048u /* 64 x 64 */
+#define SPLAT_MLP_B2 6144u /* 64 */
+#define SPLAT_MLP_W3 6208u /* 16 x 64; rows 0-2 give RGB, rows 3-15 zero */
+#define SPLAT_MLP_B3 7232u /* 16; entries 3-15 zero */
+#define SPLAT_MLP_PARAMS 7248u
+
+/* A renderer whose colour is the learned MLP's. `geometry` is an FP16 scene
+ * (precision SPLAT_PRECISION_FP16; sh_degree and sh_f16 are ignored):
+ * positions f32, scales/rotations/opacities f16. latents: n *
+ * SPLAT_MLP_LATENT fp16 values, splat-major; mlp_params: SPLAT_MLP_PARAMS
+ * fp16 values. 64 bytes per splat are read per frame (against 240 for the
+ * FP32 SH3 scene). The handle renders with splat_cuda_render and friends. */
+int splat_cuda_create_learned(const splat_scene_desc* geometry, const uint16_t* latents, const uint16_t* mlp_params,
+                              int device, splat_cuda_handle** out);
+
+/*
+ * Training of the latents and the MLP on the exact SH colours of an SH scene
+ * (a handle from splat_cuda_create, FP32 or FP16 storage), on the scene's
+ * device. Targets are the reference's SH colour (src/sh.rs:39-64), clamped to
+ * [0, 1] (a sigmoid cannot exceed 1), at `directions` Fibonacci-sphere
+ * directions per splat (the construction of src/gen.rs:213-219). An epoch
+ * visits every (splat, direction) sample once, in an order shuffled per
+ * epoch; a step takes `batch` samples (the last step of an epoch fewer), runs
+ * forward and backward on the tensor cores and applies Adam to the MLP and
+ * (lazily, rows touched by the step only) to the latents. Loss: mean squared
+ * error over samples and channels. The scene handle must outlive the learner.
+ */
+typedef struct splat_cuda_learner splat_cuda_learner;
+
+typedef struct splat_learn_config {
+  uint32_t directions; /* per splat, e.g. 256 */
+  uint32_t batch;      /* samples per step: a multiple of 128, <= 2^22 */
+  float lr, beta1, beta2, eps; /* Adam, e.g. 1e-3, 0.9, 0.999, 1e-8 */
+  uint64_t seed;       /* initial parameters and the shuffles */
+} splat_learn_config;
+
+typedef struct splat_learn_stats {
+  uint64_t steps;             /* steps since creation or set_params */
+  double epochs;              /* the same in epochs */
+  double mean_loss;           /* mean of the step losses of this call */
+  double last_loss;           /* loss of the last step */
+  double ms;                  /* device time of this call */
+  uint64_t steps_per_epoch;
+  uint64_t samples_per_epoch; /* n * directions */
+} splat_learn_stats;
+
+/* Learner options (read-only, splat_cuda_learner_get_option). */
+#define SPLAT_LEARN_STEPS_PER_EPOCH 100u
+#define SPLAT_LEARN_SHUFFLE_BITS 101u /* the sample shuffle's word width */
+#define SPLAT_LEARN_TRAIN_CTAS 102u   /* CTAs of the training kernel */
+
+/* Initial parameters: He-uniform hidden layers, Xavier-uniform output, zero
+ * biases; latents a fixed random projection of each splat's colour
+ * coefficients. */
+int splat_cuda_learner_create(const splat_cuda_handle* sh_scene, const splat_learn_config* config,
+                              splat_cuda_learner** out);
+const char* splat_cuda_learner_create_error(void);
+/* Runs `steps` training steps (blocks until done). */
+int splat_cuda_learner_train(splat_cuda_learner* l, uint64_t steps, splat_learn_stats* stats);
+/* Replaces the fp32 master parameters (SPLAT_MLP_PARAMS) and/or latents
+ * (n * 16; either may be NULL) and resets Adam and the step count. */
+int splat_cuda_learner_set_params(splat_cuda_learner* l, const float* params, const float* latents);
+/* Copies the current parameters out; any pointer may be NULL. params and
+ * latents are the fp32 masters, the _f16 ones the fp16 values the kernels use
+ * (what splat_cuda_create_learned takes). */
+int splat_cuda_learner_params(splat_cuda_learner* l, float* params, float* latents, uint16_t* params_f16,
+                              uint16_t* latents_f16);
+/* One step that also reports its gradient before Adam applies it: d loss /
+ * d params (SPLAT_MLP_PARAMS) and d loss / d latents (n * 16, zero for rows
+ * the step did not sample); either may be NULL. */
+int splat_cuda_learner_step_debug(splat_cuda_learner* l, float* grad_params, float* grad_latents);
+/* The learner's unit directions (directions * 3 floats). */
+int splat_cuda_learner_directions(const splat_cuda_learner* l, float* dirs);
+/* SPLAT_LEARN_* and SPLAT_OPT_KERNEL_LAUNCHES. */
+int splat_cuda_learner_get_option(const splat_cuda_learner* l, uint32_t option, uint64_t* value);
+const char* splat_cuda_learner_last_error(const splat_cuda_learner* l);
+int splat_cuda_learner_destroy(splat_cuda_learner* l);
+
+/* Forward and backward of the MLP on `count` explicit samples (latents fp16
+ * count * 16, unit directions and targets count * 3), with fp32 parameters
+ * rounded to fp16 as the learner does: the loss, each sample's output and
+ * the gradients of the mean loss. The training kernel's own code path, for
+ * checking it against an independent computation. Allocates temporaries. */
+int splat_cuda_mlp_gradient(int device, const float* params, const uint16_t* latents, const float* dirs,
+                            const float* targets, uint32_t count, float* grad_params, float* grad_latents,
+                            float* outputs, double* loss);
+
 #ifdef __cplusplus
 }
 #endif

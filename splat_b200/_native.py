@@ -43,7 +43,18 @@ EXPORTS = [
     "splat_cuda_batch_get_config", "splat_cuda_batch_autotune", "splat_cuda_batch_run", "splat_cuda_batch_finish",
     "splat_cuda_batch_set_option", "splat_cuda_batch_get_option", "splat_cuda_batch_set_stream",
     "splat_cuda_batch_get_stream", "splat_cuda_batch_last_error", "splat_cuda_batch_destroy",
+    "splat_cuda_create_learned", "splat_cuda_learner_create", "splat_cuda_learner_create_error",
+    "splat_cuda_learner_train", "splat_cuda_learner_set_params", "splat_cuda_learner_params",
+    "splat_cuda_learner_step_debug", "splat_cuda_learner_directions", "splat_cuda_learner_get_option",
+    "splat_cuda_learner_last_error", "splat_cuda_learner_destroy", "splat_cuda_mlp_gradient",
 ]
+
+# Learned colour (include/splat_cuda.h).
+MLP_LATENT = 16
+MLP_W1, MLP_W2, MLP_B2, MLP_W3, MLP_B3, MLP_PARAMS = 0, 2048, 6144, 6208, 7232, 7248
+LEARN_STEPS_PER_EPOCH = 100
+LEARN_SHUFFLE_BITS = 101
+LEARN_TRAIN_CTAS = 102
 
 
 class SplatError(RuntimeError):
@@ -78,6 +89,18 @@ class BlendConfigC(ctypes.Structure):
 
 class TuneResultC(ctypes.Structure):
     _fields_ = [("config", BlendConfigC), ("reserved", ctypes.c_uint32), ("ms", ctypes.c_double)]
+
+
+class LearnConfigC(ctypes.Structure):
+    _fields_ = [("directions", ctypes.c_uint32), ("batch", ctypes.c_uint32), ("lr", ctypes.c_float),
+                ("beta1", ctypes.c_float), ("beta2", ctypes.c_float), ("eps", ctypes.c_float),
+                ("seed", ctypes.c_uint64)]
+
+
+class LearnStatsC(ctypes.Structure):
+    _fields_ = [("steps", ctypes.c_uint64), ("epochs", ctypes.c_double), ("mean_loss", ctypes.c_double),
+                ("last_loss", ctypes.c_double), ("ms", ctypes.c_double), ("steps_per_epoch", ctypes.c_uint64),
+                ("samples_per_epoch", ctypes.c_uint64)]
 
 
 class RenderStatsC(ctypes.Structure):
@@ -133,6 +156,20 @@ def lib():
         L.splat_cuda_batch_last_error.argtypes = [vp]
         L.splat_cuda_batch_last_error.restype = ctypes.c_char_p
         L.splat_cuda_batch_destroy.argtypes = [vp]
+        L.splat_cuda_create_learned.argtypes = [ctypes.POINTER(SceneDesc), vp, vp, ctypes.c_int, ctypes.POINTER(vp)]
+        L.splat_cuda_learner_create.argtypes = [vp, ctypes.POINTER(LearnConfigC), ctypes.POINTER(vp)]
+        L.splat_cuda_learner_create_error.restype = ctypes.c_char_p
+        L.splat_cuda_learner_train.argtypes = [vp, u64, ctypes.POINTER(LearnStatsC)]
+        L.splat_cuda_learner_set_params.argtypes = [vp, vp, vp]
+        L.splat_cuda_learner_params.argtypes = [vp, vp, vp, vp, vp]
+        L.splat_cuda_learner_step_debug.argtypes = [vp, vp, vp]
+        L.splat_cuda_learner_directions.argtypes = [vp, vp]
+        L.splat_cuda_learner_get_option.argtypes = [vp, u32, ctypes.POINTER(u64)]
+        L.splat_cuda_learner_last_error.argtypes = [vp]
+        L.splat_cuda_learner_last_error.restype = ctypes.c_char_p
+        L.splat_cuda_learner_destroy.argtypes = [vp]
+        L.splat_cuda_mlp_gradient.argtypes = [ctypes.c_int, vp, vp, vp, vp, u32, vp, vp, vp,
+                                              ctypes.POINTER(ctypes.c_double)]
         _lib = L
     return _lib
 

@@ -30,8 +30,10 @@ SOURCES = {
     "blend.cu": [],
     "noalloc.cu": [],
     "batch.cu": [],
+    "mlp.cu": [],
 }
 HEADERS = [os.path.join(CSRC, "common.cuh"), os.path.join(CSRC, "tilesort.cuh"), os.path.join(CSRC, "handle.h"),
+           os.path.join(CSRC, "umma.cuh"), os.path.join(CSRC, "mlp.cuh"), os.path.join(CSRC, "sh.cuh"),
            os.path.join(ROOT, "include", "splat_cuda.h")]
 
 

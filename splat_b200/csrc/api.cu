@@ -175,7 +175,7 @@ FrameParams make_params(const splat_view_desc& v, uint32_t w, uint32_t hgt, cons
 
 SceneDev scene_dev(const splat_cuda_handle* h) {
   return SceneDev{h->pos_op, h->cov_a, h->cov_b, h->color, h->sh, h->pos_k, h->geom16, h->sh16, h->n, h->sh_degree,
-                  h->precision == SPLAT_PRECISION_FP16 ? 1u : 0u};
+                  h->precision == SPLAT_PRECISION_FP16 ? 1u : 0u, h->lat16, h->mlp16, h->lat16 ? 1u : 0u, 0u};
 }
 
 // Tile shape of a frame: sets tile_w/h, their logs and the tile grid.
@@ -261,6 +261,10 @@ int finish_frame(splat_cuda_handle* h, splat_render_stats* stats, int* regrown) 
       stats->sort_ms = b;
       stats->raster_ms = c;
     }
+  }
+  if (st.error) {
+    cudaMemsetAsync(h->st, 0, sizeof(DevState), h->stream);
+    return fail(h, SPLAT_ERR_TIMEOUT, "a tensor-core wait in the learned-colour projection gave up");
   }
   if (st.total_pairs > h->cap) {
     const uint64_t want = std::max<uint64_t>(st.total_pairs + st.total_pairs / 4, h->cap + 1);
@@ -599,6 +603,52 @@ SPLAT_API int splat_cuda_debug_dump(splat_cuda_handle* h, float* proj, uint8_t* 
   return SPLAT_OK;
 }
 
+SPLAT_API int splat_cuda_create_learned(const splat_scene_desc* d, const uint16_t* latents, const uint16_t* mlp_params,
+                                        int device, splat_cuda_handle** out) {
+  g_create_error.clear();
+  if (!out) return SPLAT_ERR_INVALID_ARG;
+  *out = nullptr;
+  if (!d || !mlp_params || (d->n && !latents)) {
+    g_create_error = "null geometry, latents or MLP parameters";
+    return SPLAT_ERR_INVALID_ARG;
+  }
+  if (d->precision != SPLAT_PRECISION_FP16) {
+    g_create_error = "learned colour needs FP16 geometry (SPLAT_PRECISION_FP16)";
+    return SPLAT_ERR_UNSUPPORTED;
+  }
+  // The geometry through the FP16 upload, with a zero base colour in place
+  // of the SH (never read: the colour comes from the MLP).
+  splat_scene_desc g = *d;
+  g.sh_degree = 0;
+  std::vector<uint16_t> zero_colour(d->n ? (size_t)d->n * 3 : 1, 0);
+  g.sh_f16 = zero_colour.data();
+  splat_cuda_handle* h = nullptr;
+  int rc = splat_cuda_create(&g, device, &h);
+  if (rc) return rc;
+  auto up = [&](void** dst, const void* src, size_t bytes, const char* what) -> int {
+    cudaError_t er = cudaMalloc(dst, bytes);
+    if (er != cudaSuccess) return cuda_fail(h, er, what);
+    er = cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice);
+    if (er != cudaSuccess) return cuda_fail(h, er, what);
+    return SPLAT_OK;
+  };
+  if ((rc = up((void**)&h->mlp16, mlp_params, SPLAT_MLP_PARAMS * sizeof(uint16_t), "upload MLP parameters")) ||
+      (d->n && (rc = up((void**)&h->lat16, latents, d->n * SPLAT_MLP_LATENT * sizeof(uint16_t), "upload latents")))) {
+    g_create_error = h->err;
+    splat_cuda_destroy(h);
+    return rc;
+  }
+  if (!d->n) {  // an empty scene still marks the handle learned
+    if ((rc = up((void**)&h->lat16, mlp_params, 16, "latents"))) {
+      g_create_error = h->err;
+      splat_cuda_destroy(h);
+      return rc;
+    }
+  }
+  *out = h;
+  return SPLAT_OK;
+}
+
 SPLAT_API int splat_cuda_destroy(splat_cuda_handle* h) {
   if (!h) return SPLAT_OK;
   cudaSetDevice(h->device);
@@ -612,6 +662,8 @@ SPLAT_API int splat_cuda_destroy(splat_cuda_handle* h) {
   dfree(h->pos_k);
   dfree(h->geom16);
   dfree(h->sh16);
+  dfree(h->lat16);
+  dfree(h->mlp16);
   dfree(h->rec);
   dfree(h->bin);
   free_pairs(h);

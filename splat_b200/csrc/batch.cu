@@ -324,6 +324,7 @@ SPLAT_API int splat_cuda_batch_create(splat_cuda_handle* const* scenes, uint32_t
   for (uint32_t i = 0; i < n_scenes; i++) {
     if (!scenes[i]) return reject(SPLAT_ERR_INVALID_ARG, "null scene handle");
     if (scenes[i]->device != scenes[0]->device) return reject(SPLAT_ERR_INVALID_ARG, "scenes on different devices");
+    if (scenes[i]->lat16) return reject(SPLAT_ERR_UNSUPPORTED, "learned-colour scenes render one view per call");
   }
   for (uint32_t i = 0; i < n_views; i++) {
     const splat_batch_view& v = views[i];

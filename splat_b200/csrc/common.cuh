@@ -57,6 +57,12 @@ struct SceneDev {
   uint64_t n;
   uint32_t sh_degree;
   uint32_t fp16;
+  // Learned colour (FP16 storage only): per-splat latents, 16 halves each
+  // (two uint4), and the MLP's fp16 parameters (mlp.cuh layout).
+  const uint4* lat16;
+  const uint16_t* mlp16;
+  uint32_t learned;
+  uint32_t pad;
 };
 
 // A projected splat as the blend reads it: 48 bytes, three float4.
@@ -133,7 +139,7 @@ struct ViewTask {
   uint32_t proj_cta0;   // first CTA of the view in the projection launch
   uint32_t bin_cta0;    // ... in the count and scatter launches
   uint32_t col_cta0;    // ... in the column-scan launch
-  uint32_t pad[3];
+  uint32_t pad[1];
 };
 
 // The view whose `field` (a first-CTA or first-tile member) is the largest

@@ -25,6 +25,8 @@ struct splat_cuda_handle {
   float4* pos_k = nullptr;   // FP16 storage: x, y, z, k
   uint4* geom16 = nullptr;   // FP16 storage: scale, rotation, opacity halves
   uint16_t* sh16 = nullptr;  // FP16 storage: base colour + SH planes
+  uint4* lat16 = nullptr;     // learned colour: 16 fp16 latents per splat
+  uint16_t* mlp16 = nullptr;  // learned colour: the MLP's fp16 parameters
   // per-splat frame buffers
   splat::Record* rec = nullptr;
   splat::BinInfo* bin = nullptr;

@@ -10,19 +10,15 @@
 // count and depth bits for the binning, and counts the visible splats.
 #include <cuda_fp16.h>
 
+#include <algorithm>
 #include <cstddef>
 
 #include "common.cuh"
+#include "mlp.cuh"
+#include "sh.cuh"
 
 namespace splat {
 namespace {
-
-// src/sh.rs:5-22
-constexpr float kShC1 = 0.4886025f;
-constexpr float kShC2_0 = 1.0925485f, kShC2_1 = -1.0925485f, kShC2_2 = 0.31539157f, kShC2_3 = -1.0925485f,
-                kShC2_4 = 0.54627424f;
-constexpr float kShC3_0 = -0.5900436f, kShC3_1 = 2.8906114f, kShC3_2 = -0.4570458f, kShC3_3 = 0.37317633f,
-                kShC3_4 = -0.4570458f, kShC3_5 = 1.4453057f, kShC3_6 = -0.5900436f;
 
 // `x as u32` of a float: saturating, NaN -> 0.
 __device__ __forceinline__ uint32_t sat_u32(float v) {
@@ -33,57 +29,6 @@ __device__ __forceinline__ uint32_t sat_u32(float v) {
 
 // f32::clamp (NaN passes through).
 __device__ __forceinline__ float rclamp(float v, float lo, float hi) { return v < lo ? lo : (v > hi ? hi : v); }
-
-// sh::eval_rest added to c; R(coef, ch) loads rest coefficient `coef`,
-// channel `ch` of the splat.
-template <int DEG, class Load>
-__device__ __forceinline__ void eval_sh(Load&& R, float x, float y, float z, float c[3]) {
-  if constexpr (DEG >= 1) {
-    float r[3];
-#pragma unroll
-    for (int ch = 0; ch < 3; ch++) {
-      float v = kShC1 * (((-y) * R(0, ch) + z * R(1, ch)) - x * R(2, ch));
-      r[ch] = v;
-    }
-    if constexpr (DEG >= 2) {
-      float xx = x * x, yy = y * y, zz = z * z;
-      float xy = x * y, yz = y * z, xz = x * z;
-      float b3 = kShC2_0 * xy, b4 = kShC2_1 * yz, b5 = kShC2_2 * ((2.0f * zz - xx) - yy), b6 = kShC2_3 * xz,
-            b7 = kShC2_4 * (xx - yy);
-#pragma unroll
-      for (int ch = 0; ch < 3; ch++) {
-        float s = b3 * R(3, ch);
-        s = s + b4 * R(4, ch);
-        s = s + b5 * R(5, ch);
-        s = s + b6 * R(6, ch);
-        s = s + b7 * R(7, ch);
-        r[ch] = r[ch] + s;
-      }
-      if constexpr (DEG >= 3) {
-        float b8 = (kShC3_0 * y) * (3.0f * xx - yy);
-        float b9 = (kShC3_1 * xy) * z;
-        float b10 = (kShC3_2 * y) * ((4.0f * zz - xx) - yy);
-        float b11 = (kShC3_3 * z) * ((2.0f * zz - 3.0f * xx) - 3.0f * yy);
-        float b12 = (kShC3_4 * x) * ((4.0f * zz - xx) - yy);
-        float b13 = (kShC3_5 * z) * (xx - yy);
-        float b14 = (kShC3_6 * x) * (xx - 3.0f * yy);
-#pragma unroll
-        for (int ch = 0; ch < 3; ch++) {
-          float u = b8 * R(8, ch);
-          u = u + b9 * R(9, ch);
-          u = u + b10 * R(10, ch);
-          u = u + b11 * R(11, ch);
-          u = u + b12 * R(12, ch);
-          u = u + b13 * R(13, ch);
-          u = u + b14 * R(14, ch);
-          r[ch] = r[ch] + u;
-        }
-      }
-    }
-#pragma unroll
-    for (int ch = 0; ch < 3; ch++) c[ch] = c[ch] + r[ch];
-  }
-}
 
 __device__ __forceinline__ float h2f(uint32_t bits16) { return __half2float(__ushort_as_half((unsigned short)bits16)); }
 
@@ -145,11 +90,14 @@ __device__ __forceinline__ void conic_terms(const T c[6], T t0x, T t0y, T t0z, T
 // Projects splat i < s.n of the view: writes its record (when visible), its
 // tile rectangle and the optional debug values; reports visibility and
 // whether its conic took the FP64 path.
-template <int DEG, bool F16>
+// LEARNED: the colour comes from the learned-colour MLP afterwards; the
+// record's colour is left 0 and `dir` receives normalize_or_zero(p - eye),
+// the direction the SH colour would be evaluated at.
+template <int DEG, bool F16, bool LEARNED = false>
 __device__ __forceinline__ void project_splat(const FrameParams& fp, const SceneDev& s, uint64_t i,
                                               Record* __restrict__ rec, BinInfo* __restrict__ bin,
                                               float* __restrict__ dbg_proj, float* __restrict__ dbg_color,
-                                              bool& vis, bool& used_fp64) {
+                                              bool& vis, bool& used_fp64, float* dir = nullptr) {
   {
     float px, py, pz, opacity, k;
     uint4 g16 = make_uint4(0, 0, 0, 0);
@@ -244,35 +192,45 @@ __device__ __forceinline__ void project_splat(const FrameParams& fp, const Scene
       const float ext_x = k * sqrtf(a);
       const float ext_y = k * sqrtf(cc);
       if (x + ext_x <= 0.0f || x - ext_x >= fp.width || y + ext_y <= 0.0f || y - ext_y >= fp.height) break;
-      if (F16) {
-        col[0] = h2f(__ldg(s.sh16 + i));
-        col[1] = h2f(__ldg(s.sh16 + s.n + i));
-        col[2] = h2f(__ldg(s.sh16 + 2 * s.n + i));
-      } else {
-        col[0] = __ldg(s.color + i);
-        col[1] = __ldg(s.color + s.n + i);
-        col[2] = __ldg(s.color + 2 * s.n + i);
-      }
-      if constexpr (DEG > 0) {
-        // normalize_or_zero(p - eye)
+      if constexpr (LEARNED) {
         const float len = sqrtf((dx * dx + dy * dy) + dz * dz);
         const float rcp = 1.0f / len;
-        float nx = 0.f, ny = 0.f, nz = 0.f;
         if (isfinite(rcp) && rcp > 0.0f) {
-          nx = dx * rcp;
-          ny = dy * rcp;
-          nz = dz * rcp;
+          dir[0] = dx * rcp;
+          dir[1] = dy * rcp;
+          dir[2] = dz * rcp;
         }
-        if (F16)
-          eval_sh<DEG>([&](int coef, int ch) { return h2f(__ldg(s.sh16 + (uint64_t)((coef + 1) * 3 + ch) * s.n + i)); },
-                       nx, ny, nz, col);
-        else
-          eval_sh<DEG>([&](int coef, int ch) { return __ldg(s.sh + (uint64_t)(coef * 3 + ch) * s.n + i); }, nx, ny,
-                       nz, col);
+      } else {
+        if (F16) {
+          col[0] = h2f(__ldg(s.sh16 + i));
+          col[1] = h2f(__ldg(s.sh16 + s.n + i));
+          col[2] = h2f(__ldg(s.sh16 + 2 * s.n + i));
+        } else {
+          col[0] = __ldg(s.color + i);
+          col[1] = __ldg(s.color + s.n + i);
+          col[2] = __ldg(s.color + 2 * s.n + i);
+        }
+        if constexpr (DEG > 0) {
+          // normalize_or_zero(p - eye)
+          const float len = sqrtf((dx * dx + dy * dy) + dz * dz);
+          const float rcp = 1.0f / len;
+          float nx = 0.f, ny = 0.f, nz = 0.f;
+          if (isfinite(rcp) && rcp > 0.0f) {
+            nx = dx * rcp;
+            ny = dy * rcp;
+            nz = dz * rcp;
+          }
+          if (F16)
+            sh::eval_sh<DEG>([&](int coef, int ch) { return h2f(__ldg(s.sh16 + (uint64_t)((coef + 1) * 3 + ch) * s.n + i)); },
+                         nx, ny, nz, col);
+          else
+            sh::eval_sh<DEG>([&](int coef, int ch) { return __ldg(s.sh + (uint64_t)(coef * 3 + ch) * s.n + i); }, nx, ny,
+                         nz, col);
+        }
+        col[0] = fmaxf(col[0], 0.0f);
+        col[1] = fmaxf(col[1], 0.0f);
+        col[2] = fmaxf(col[2], 0.0f);
       }
-      col[0] = fmaxf(col[0], 0.0f);
-      col[1] = fmaxf(col[1], 0.0f);
-      col[2] = fmaxf(col[2], 0.0f);
       if (!(isfinite(x) && isfinite(y) && isfinite(ext_x) && isfinite(ext_y))) break;
       if (!conic_done) {
         c0 = cc * inv_det;
@@ -314,7 +272,7 @@ __device__ __forceinline__ void project_splat(const FrameParams& fp, const Scene
       float* d = dbg_proj + 8 * i;
       d[0] = out_x; d[1] = out_y; d[2] = out_ex; d[3] = out_ey; d[4] = out_depth; d[5] = c0; d[6] = c1; d[7] = c2;
     }
-    if (dbg_color) {
+    if (!LEARNED && dbg_color) {
       dbg_color[3 * i] = vis ? col[0] : 0.f;
       dbg_color[3 * i + 1] = vis ? col[1] : 0.f;
       dbg_color[3 * i + 2] = vis ? col[2] : 0.f;
@@ -375,10 +333,135 @@ __global__ void __launch_bounds__(256) k_project_batch(const ViewTask* __restric
   count_visible(vis, used_fp64, fc, v);
 }
 
+// Learned colour (FP16 storage): the projection of k_project, then the
+// colour MLP of each 128-splat tile on the tensor cores (mlp.cuh), fused:
+// persistent CTAs of 128 threads, thread t = splat t of the tile = TMEM lane
+// t. The MLP's input row is the splat's 16 latents and its view direction;
+// layers 1-3 are three tcgen05.mma groups with their epilogues between. The
+// record is written by the projection and its colour filled in after.
+constexpr uint32_t kLearnedThreads = 128;
+constexpr uint32_t kLearnedTmemCols = 128;  // z1/z2 at 0-63, z3 at 64-79
+// Requested dynamic shared memory: more than a CTA needs, so that at most
+// four CTAs share an SM (4 x 128 TMEM columns = all 512).
+constexpr size_t kLearnedSmem = 48 * 1024;
+
+struct LearnedSmem {
+  mlp::ForwardTiles t;
+  uint64_t mbar;
+  uint32_t tmem;
+};
+static_assert(sizeof(LearnedSmem) <= kLearnedSmem, "learned projection shared memory");
+
+__global__ void __launch_bounds__(kLearnedThreads) k_project_learned(ViewTask t, ViewTask* __restrict__ table,
+                                                                     float* __restrict__ dbg_proj,
+                                                                     float* __restrict__ dbg_color, FrameCounters fc) {
+  extern __shared__ __align__(128) uint8_t smem_raw[];
+  LearnedSmem& S = *reinterpret_cast<LearnedSmem*>(smem_raw);
+  const uint32_t tid = threadIdx.x;
+  if (blockIdx.x == 0 && tid == 0) *table = t;
+  mlp::load_forward_weights(S.t, t.s.mlp16);
+  if (tid == 0) umma::mbar_init(umma::smem_u32(&S.mbar), 1);
+  if (tid < 32) umma::tmem_alloc(&S.tmem, kLearnedTmemCols);
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  const uint32_t tmem = S.tmem, mbar = umma::smem_u32(&S.mbar);
+  const uint32_t act = umma::smem_u32(S.t.act);
+  uint32_t phase = 0;
+  bool timed_out = false, aborted = false;
+  auto wait_mma = [&]() {
+    if (!umma::mbar_wait(mbar, phase)) timed_out = true;
+    phase ^= 1u;
+    umma::fence_after_sync();
+  };
+  auto sync_or_abort = [&]() -> bool {
+    umma::fence_async_smem();
+    umma::fence_before_sync();
+    return __syncthreads_or(timed_out) != 0;
+  };
+  const uint64_t n = t.s.n;
+  const uint64_t tiles = (n + mlp::kRows - 1) / mlp::kRows;
+  for (uint64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    const uint64_t i = tile * mlp::kRows + tid;
+    bool vis = false, used_fp64 = false;
+    float dir[3] = {0.f, 0.f, 0.f};
+    uint4 l0 = make_uint4(0, 0, 0, 0), l1 = l0;
+    if (i < n) {
+      project_splat<0, true, true>(t.fp, t.s, i, t.rec, t.bin, dbg_proj, nullptr, vis, used_fp64, dir);
+      l0 = __ldg(t.s.lat16 + 2 * i);
+      l1 = __ldg(t.s.lat16 + 2 * i + 1);
+    }
+    mlp::store_input(S.t.act, 8, tid, l0, l1, dir[0], dir[1], dir[2]);
+    if (sync_or_abort()) { aborted = true; break; }
+    if (tid == 0) {
+      umma::fence_after_sync();
+      mlp::gemm_k(tmem, act, 8, umma::smem_u32(S.t.w1f), 64, 2, mlp::kIdN64);
+      umma::commit(mbar);
+    }
+    wait_mma();
+    mlp::hidden_epilogue(tmem, 0, nullptr, S.t.act, tid);
+    if (sync_or_abort()) { aborted = true; break; }
+    if (tid == 0) {
+      umma::fence_after_sync();
+      mlp::gemm_k(tmem, act, 0, umma::smem_u32(S.t.w2f), 64, 4, mlp::kIdN64);
+      umma::commit(mbar);
+    }
+    wait_mma();
+    mlp::hidden_epilogue(tmem, 0, S.t.b2, S.t.act, tid);  // h2 over h1 (layer 2 is done)
+    if (sync_or_abort()) { aborted = true; break; }
+    if (tid == 0) {
+      umma::fence_after_sync();
+      mlp::gemm_k(tmem + 64, act, 0, umma::smem_u32(S.t.w3f), 16, 4, mlp::kIdN16);
+      umma::commit(mbar);
+    }
+    wait_mma();
+    float z[16];
+    umma::tmem_ld16(umma::tmem_warp_addr(tmem, 64), z);
+    float rgb[3];
+    for (int c = 0; c < 3; c++) rgb[c] = mlp::sigmoidf(z[c] + S.t.b3[c]);
+    if (vis) {
+      float* r = reinterpret_cast<float*>(t.rec + i);
+      r[6] = rgb[0];  // r1.z, r1.w, r2.x
+      r[7] = rgb[1];
+      r[8] = rgb[2];
+    }
+    if (dbg_color && i < n)
+      for (int c = 0; c < 3; c++) dbg_color[3 * i + c] = vis ? rgb[c] : 0.0f;
+    count_visible(vis, used_fp64, fc, 0);
+    umma::fence_before_sync();
+  }
+  if (!aborted && __syncthreads_or(timed_out)) aborted = true;
+  if (aborted) {
+    if (tid == 0) atomicExch(&fc.st->error, 1u);
+    umma::mbar_wait(mbar, phase, 100000000ull);  // an MMA still in flight, if any
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  if (tid < 32) {
+    umma::fence_after_sync();
+    umma::tmem_free(tmem, kLearnedTmemCols);
+  }
+}
+
 }  // namespace
 
 cudaError_t launch_project(const ViewTask& t, ViewTask* table, float* dbg_proj, float* dbg_color,
                            const FrameCounters& fc, cudaStream_t stream, uint32_t* launches) {
+  if (t.s.learned) {
+    static int sms[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int& ns = sms[dev & 63];
+    if (!ns) {
+      cudaError_t e = cudaDeviceGetAttribute(&ns, cudaDevAttrMultiProcessorCount, dev);
+      if (e != cudaSuccess) return e;
+    }
+    const uint64_t tiles = (t.s.n + mlp::kRows - 1) / mlp::kRows;
+    const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(tiles, 4ull * ns));
+    k_project_learned<<<grid, kLearnedThreads, kLearnedSmem, stream>>>(t, table, dbg_proj, dbg_color, fc);
+    *launches += 1;
+    return cudaGetLastError();
+  }
   // An empty scene still stores the view table.
   const unsigned grid = t.s.n ? (unsigned)((t.s.n + 255) / 256) : 1u;
 #define SPLAT_PROJECT(D)                                                                          \

@@ -1,0 +1,244 @@
+"""Learned colour on the GPU: the tcgen05 training kernel's forward pass and
+gradients against the float64 oracle (oracle/mlp_oracle.py, fp16 rounding
+emulated at the same points), the learner's sample order, gradient and Adam
+step against the oracle, training reducing the loss, the fused projection's
+MLP colours and images against the oracle, and what the trained network
+gains over the method without it (base colour only).
+
+Tolerances: outputs within 2e-3 absolute (fp16 operands, fp32 accumulation);
+each gradient block within 1e-2 relative (Frobenius) of the oracle's; Adam
+updates within 1e-6 relative of a float32 restatement applied to the
+device's own gradient."""
+
+import numpy as np
+import pytest
+
+from oracle import mlp_oracle as M
+
+pytestmark = pytest.mark.gpu
+
+BLOCKS = {"W1": (M.W1, M.W2), "W2": (M.W2, M.B2), "b2": (M.B2, M.W3), "W3": (M.W3, M.B3), "b3": (M.B3, M.PARAMS)}
+
+
+def he_params(rng):
+    w1 = np.zeros((64, 32))
+    w1[:, :19] = rng.uniform(-1, 1, (64, 19)) * np.sqrt(6 / 20)
+    w1[:, 19] = rng.normal(0, 0.05, 64)
+    w2 = rng.uniform(-1, 1, (64, 64)) * np.sqrt(6 / 64)
+    b2 = rng.normal(0, 0.05, 64)
+    w3 = np.zeros((16, 64))
+    w3[:3] = rng.uniform(-1, 1, (3, 64)) * np.sqrt(6 / 67)
+    b3 = np.zeros(16)
+    b3[:3] = rng.normal(0, 0.1, 3)
+    return M.pack(w1, w2, b2, w3, b3).astype(np.float32)
+
+
+def unit(rng, n):
+    d = rng.normal(size=(n, 3))
+    return (d / np.linalg.norm(d, axis=1, keepdims=True)).astype(np.float32)
+
+
+def rel(a, b):
+    return np.linalg.norm(np.asarray(a, np.float64) - b) / max(np.linalg.norm(b), 1e-30)
+
+
+def check_grads(g, want):
+    for name, (lo, hi) in BLOCKS.items():
+        assert rel(g[lo:hi], want[lo:hi]) < 1e-2, (name, rel(g[lo:hi], want[lo:hi]))
+
+
+@pytest.mark.parametrize("count", [1, 128, 129, 1000, 20_000])
+def test_gradient_matches_oracle(cuda_lib, count):
+    from splat_b200.learned import mlp_gradient
+
+    rng = np.random.default_rng(count)
+    p = he_params(rng)
+    lat = rng.normal(0, 0.7, (count, 16)).astype(np.float16)
+    d = unit(rng, count)
+    t = rng.uniform(0, 1, (count, 3)).astype(np.float32)
+    loss, y, g, gl = mlp_gradient(p, lat.view(np.uint16), d, t)
+    wl, wy, wg, wgl = M.backward(p, lat.astype(np.float64), d, t)
+    assert np.abs(y - wy).max() < 2e-3
+    assert abs(loss - wl) <= 1e-3 * wl + 1e-7
+    check_grads(g, wg)
+    assert rel(gl, wgl) < 1e-2
+    # no gradient where no input or output exists
+    assert np.all(g[M.W1:M.W2].reshape(64, 32)[:, 20:] == 0)
+    assert np.all(g[M.W3:M.B3].reshape(16, 64)[3:] == 0) and np.all(g[M.B3 + 3:] == 0)
+
+
+def small_scene(n=300, seed=3, degree=3):
+    from tests.scenes import clusters
+
+    return clusters(n, seed=seed, sh_degree=degree)
+
+
+def make_learner(scene, directions=64, batch=2048, seed=1):
+    from splat_b200.learned import LearnConfig, Learner
+    from splat_b200.render import CudaRenderer
+
+    r = CudaRenderer(scene)
+    return r, Learner(r, LearnConfig(directions=directions, batch=batch, seed=seed))
+
+
+def oracle_step(scene, learner, step, p, lat32, batch, seed):
+    si, di = M.step_samples(step, len(scene), learner.config.directions, batch, seed)
+    dirs = learner.directions()[di]
+    t = M.sh_targets(scene.colors[si], scene.sh_rest[si], scene.sh_degree, dirs)
+    lat = M.f16(lat32[si])
+    _, _, g, glat_s = M.backward(p, lat, dirs, t)
+    glat = np.zeros_like(lat32, dtype=np.float64)
+    np.add.at(glat, si, glat_s)
+    return g, glat, si
+
+
+@pytest.mark.parametrize("degree", [1, 3])
+def test_learner_step_matches_oracle(cuda_lib, degree):
+    scene = small_scene(degree=degree)
+    r, L = make_learner(scene)
+    rng = np.random.default_rng(5)
+    p0 = he_params(rng)
+    lat0 = rng.normal(0, 0.5, (len(scene), 16)).astype(np.float32)
+    L.set_params(p0, lat0)
+    assert np.array_equal(L.directions(), M.fibonacci_dirs(64))
+    g, gl = L.step_debug()
+    wg, wgl, si = oracle_step(scene, L, 0, p0, lat0, 2048, 1)
+    check_grads(g, wg)
+    assert rel(gl, wgl) < 1e-2
+    touched = np.zeros(len(scene), bool)
+    touched[si] = True
+    assert np.all(gl[~touched] == 0)
+    # Adam on the device's own gradient, step 1
+    p1, lat1 = L.params()
+    wp, _, _ = M.adam(p0, np.zeros_like(p0), np.zeros_like(p0), g, 1)
+    np.testing.assert_allclose(p1, wp, rtol=1e-6, atol=1e-9)
+    wl, _, _ = M.adam(lat0[touched], np.zeros((touched.sum(), 16)), np.zeros((touched.sum(), 16)), gl[touched], 1)
+    np.testing.assert_allclose(lat1[touched], wl, rtol=1e-6, atol=1e-9)
+    assert np.array_equal(lat1[~touched], lat0[~touched])
+    p16, lat16 = L.params_f16()
+    assert np.array_equal(p16, p1.astype(np.float16).view(np.uint16))
+    assert np.array_equal(lat16, lat1.astype(np.float16).view(np.uint16))
+    L.close()
+    r.close()
+
+
+def test_last_step_of_epoch_is_partial(cuda_lib):
+    scene = small_scene()
+    r, L = make_learner(scene)
+    spe = L.steps_per_epoch
+    assert spe == (300 * 64 + 2047) // 2048
+    L.train(spe - 1)
+    p, lat = L.params()
+    g, _ = L.step_debug()
+    wg, _, si = oracle_step(scene, L, spe - 1, p, lat, 2048, 1)
+    assert len(si) == 300 * 64 - (spe - 1) * 2048
+    check_grads(g, wg)
+    L.close()
+    r.close()
+
+
+def test_training_reduces_loss(cuda_lib):
+    scene = small_scene(n=2000)
+    r, L = make_learner(scene, directions=64, batch=4096)
+    first = L.train(1).last_loss
+    s = L.train_epochs(20)
+    assert s.steps == 1 + 20 * L.steps_per_epoch
+    assert s.last_loss < 0.5 * first, (first, s.last_loss)
+    L.close()
+    r.close()
+
+
+def view_dirs(scene, view):
+    a = view.to_array()
+    eye = np.asarray(a[0:3], np.float32)
+    d = (scene.positions - eye).astype(np.float32)
+    ln = np.sqrt((d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1]) + d[:, 2] * d[:, 2])
+    return d / ln[:, None]
+
+
+def test_learned_render_matches_oracle(cuda_lib, oracle):
+    from splat_b200 import Frame, synth
+    from splat_b200 import _native as N
+    from splat_b200.learned import learned_renderer
+
+    scene = small_scene(n=5000, seed=8)
+    r, L = make_learner(scene, batch=4096)
+    L.train_epochs(2)
+    p16, lat16 = L.params_f16()
+    half = scene.to_fp16()
+    lr = learned_renderer(half, lat16, p16)
+    lr.set_option(N.SPLAT_OPT_DEBUG_CAPTURE, 1)
+    cam = synth.orbit_camera(scene)
+    view = cam.view()
+    f = Frame()
+    lr.render(view, 640, 360, (0.0, 0.0, 0.0), f)
+    dump = lr.debug_dump(640, 360)
+    vis = dump["visible"]
+    assert vis.sum() > 1000
+    want = M.forward(p16.view(np.float16).astype(np.float64), lat16.view(np.float16).astype(np.float64),
+                     view_dirs(scene, view))["y"]
+    assert np.abs(dump["color"][vis] - want[vis]).max() < 2e-3
+    # the image: the oracle's cpu backend over the decoded geometry, coloured
+    # by the oracle's MLP at each splat's view direction
+    dec = half.decoded_scene()
+    dec.colors = want.astype(np.float32)
+    dec.sh_degree = 0
+    dec.sh_rest = np.zeros((len(dec), 0, 3), np.float32)
+    cpu = oracle.CpuTiled(dec)
+    img, _ = cpu.render(view, 640, 360, (0.0, 0.0, 0.0))
+    assert oracle.psnr(f.pixels, img) >= 50.0
+    assert np.abs(f.pixels.astype(int) - img).max() <= 3
+    cpu.close()
+    lr.close()
+    L.close()
+    r.close()
+
+
+def test_learned_colour_gains_over_base_colour(cuda_lib, oracle):
+    """The ablation: the trained MLP against the method without it (each
+    splat's base colour, i.e. SH degree 0), both against exact SH."""
+    from splat_b200 import Frame, synth
+    from splat_b200.learned import learned_renderer
+    from splat_b200.render import CudaRenderer
+
+    scene = small_scene(n=20_000, seed=9)
+    r, L = make_learner(scene, directions=256, batch=65536)
+    s = L.train_epochs(30)
+    p16, lat16 = L.params_f16()
+    lr = learned_renderer(scene.to_fp16(), lat16, p16)
+    dc = scene.to_fp16()
+    dc.sh = dc.sh[:, :1, :].copy()
+    dc.sh_degree = 0
+    rdc = CudaRenderer(dc)
+    cam = synth.orbit_camera(scene)
+    gains = []
+    for k in range(4):
+        cam.rotate(2 * np.pi / 4 * k, 0.2)
+        v = cam.view()
+        exact, mlp, base = Frame(), Frame(), Frame()
+        r.render(v, 480, 270, (0.0, 0.0, 0.0), exact)
+        lr.render(v, 480, 270, (0.0, 0.0, 0.0), mlp)
+        rdc.render(v, 480, 270, (0.0, 0.0, 0.0), base)
+        gains.append((oracle.psnr(mlp.pixels, exact.pixels), oracle.psnr(base.pixels, exact.pixels)))
+    g = np.array(gains)
+    print(f"loss {s.last_loss:.5f}; PSNR vs exact SH: mlp {g[:, 0].round(2)}, base colour {g[:, 1].round(2)}")
+    assert np.all(g[:, 0] > g[:, 1] + 0.5)
+    for x in (rdc, lr, L, r):
+        x.close()
+
+
+def test_learned_scene_is_refused_by_batches(cuda_lib):
+    import ctypes
+
+    from splat_b200 import _native as N
+    from splat_b200.learned import learned_renderer
+
+    scene = small_scene(n=100)
+    lr = learned_renderer(scene.to_fp16(), np.zeros((100, 16), np.uint16), np.zeros(M.PARAMS, np.uint16))
+    views = (N.BatchViewC * 1)()
+    views[0].scene, views[0].width, views[0].height, views[0].dev_out = 0, 64, 64, 1
+    h = ctypes.c_void_p()
+    scenes = (ctypes.c_void_p * 1)(lr._h.value)
+    rc = cuda_lib.splat_cuda_batch_create(scenes, 1, views, 1, ctypes.byref(h))
+    assert rc == N.SPLAT_ERR_UNSUPPORTED
+    lr.close()
