@@ -8,6 +8,14 @@ Workloads (--config):
   fp16   the same scene with scales, rotations, opacities and SH stored as
          FP16 (positions f32), 3840x2160; the per-frame error against the
          FP64 naive rasterizer is stated for the first frames.
+  learned
+         the plain scene's 48 SH floats per splat replaced by 16 FP16 latents
+         and a shared MLP (FP16 geometry), trained first on the device from
+         exact SH at 256 Fibonacci directions per splat (batch 65536, Adam lr
+         1e-3; the training is timed and reported separately), then rendered
+         over the same 1080p orbit; PSNR against the exact-SH plain path, and
+         the plain path's frames/s from the same run.
+  batch  96 views of mixed resolution over three scenes, one CUDA graph.
 A step is one frame.
 
   value  frames/s with the scene resident in HBM and the frame written to
@@ -51,6 +59,11 @@ CONFIGS = {
               "workload": "3 seeded cluster scenes (50k SH0, 400k SH1, 3M SH3, f32), 96 views: resolution uniform "
                           "from 160x96..3840x2160, yaw U[0, 2pi), pitch U[-0.6, 0.6], FOV U[40, 70] deg, "
                           "distance 12; one CUDA graph per batch"},
+    "learned": {"metric": "frames/s at 1920x1080, 1.2M splats, learned colour (16 FP16 latents + MLP)",
+                "w": 1920, "h": 1080, "precision": "learned",
+                "s_in": 64,  # f32 position + k, f16 scale/rotation/opacity, 16 f16 latents
+                "workload": "1.2M gaussians of the SH3 workload with colour from 16 FP16 latents + a shared "
+                            "19-64-64-3 MLP (FP16 geometry), 1920x1080, 16x16 tiles, 40-view orbit"},
     "fp16": {"metric": "frames/s at 3840x2160, 1.2M SH3 splats, FP16 storage", "w": 3840, "h": 2160,
              "precision": "fp16",
              "s_in": 124,  # f32 position; f16 scale, rotation, opacity, 48 SH coefficients
@@ -74,11 +87,13 @@ def parse():
     p.add_argument("--splats", type=int, default=N_SPLATS)
     p.add_argument("--cpu-sample-s", type=float, default=15.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--learn-epochs", type=float, default=30.0, help="learned: training epochs before rendering")
+    p.add_argument("--psnr-frames", type=int, default=40, help="learned: orbit frames compared with exact SH")
     p.add_argument("--profile", action="store_true",
                    help="render --warmup then --steps frames and exit (a short command for ncu captures)")
     a = p.parse_args()
     if a.steps is None:
-        a.steps = {"plain": 4000, "fp16": 1000, "batch": 20}[a.config]
+        a.steps = {"plain": 4000, "fp16": 1000, "batch": 20, "learned": 4000}[a.config]
     return a
 
 
@@ -147,6 +162,8 @@ def make_workload(n, cfg):
     scene = synth.cluster_scene(n, seed=0x5EED0001, sh_degree=3)
     cam = synth.orbit_camera(scene)
     home, warm, timed = synth.orbit_views(cam, ORBIT, 5)
+    if cfg["precision"] == "learned":
+        return scene, scene, scene, home, warm, timed
     if cfg["precision"] == "fp16":
         half = scene.to_fp16()
         return half, half.decoded_scene(), scene, home, warm, timed
@@ -412,6 +429,195 @@ def run_ours(args):
         torch.distributed.destroy_process_group()
 
 
+def run_learned(args):
+    """Learned colour: train on the device, then time the learned renderer
+    (and the exact-SH plain renderer of the same scene) over the orbit."""
+    import torch
+
+    rank, world, local = dist_env()
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+    cfg = CONFIGS["learned"]
+    W, H = cfg["w"], cfg["h"]
+    from oracle import oracle as O  # PSNR and the CPU baseline only
+    from splat_b200 import _native as Nat
+    from splat_b200.learned import LearnConfig, Learner, learned_renderer
+    from splat_b200.render import CudaRenderer
+
+    scene, _, _, home, warm, timed = make_workload(args.splats, cfg)
+    views = timed[rank::world] if world > 1 else timed
+    exact = CudaRenderer(scene, device=dev)
+
+    # Training (every rank trains its own replica: no exchange).
+    learner = Learner(exact, LearnConfig(directions=256, batch=65536, lr=1e-3, seed=1))
+    learner.train(1)  # warm-up: graph capture, clocks
+    learner.set_params(*learner.params())
+    steps = int(round(args.learn_epochs * learner.steps_per_epoch))
+    with Clocks(dev) as clk_train:
+        ts = learner.train(steps)
+    train_ctas = learner.option(Nat.LEARN_TRAIN_CTAS)
+    p16, lat16 = learner.params_f16()
+    learner.close()
+    samples = ts.epochs * ts.samples_per_epoch
+    flop_per_sample = 3 * 11008  # forward 11,008 FLOP; backward ~2x (activation and weight gradients)
+    train_tflops = samples * flop_per_sample / (ts.ms / 1e3) / 1e12
+
+    half = scene.to_fp16()
+    r = learned_renderer(half, lat16, p16, device=dev)
+    base = scene.to_fp16()
+    base.sh = base.sh[:, :1, :].copy()
+    base.sh_degree = 0
+    rbase = CudaRenderer(base, device=dev)
+    out = torch.empty(W * H * 3, dtype=torch.uint8, device=dev)
+    nbytes = out.numel()
+
+    def settle(rr):
+        for v in [home] + warm[: max(args.warmup, 3)]:
+            while True:
+                rr.render_device(v, W, H, (0, 0, 0), out.data_ptr(), nbytes)
+                if not rr.finish()[1]:
+                    break
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    def timed_frames(rr, K):
+        stream = torch.cuda.ExternalStream(rr.stream())
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        barrier()
+        l0 = rr.get_option(Nat.SPLAT_OPT_KERNEL_LAUNCHES)
+        start.record(stream)
+        for i in range(K):
+            rr.render_device(views[i % len(views)], W, H, (0, 0, 0), out.data_ptr(), nbytes)
+        end.record(stream)
+        _, regrown = rr.finish()
+        barrier()
+        assert not regrown, "pair buffers overflowed inside the timed region"
+        t = torch.tensor([start.elapsed_time(end)], device=dev)
+        if world > 1:
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item()), (rr.get_option(Nat.SPLAT_OPT_KERNEL_LAUNCHES) - l0) % (1 << 32)
+
+    settle(r)
+    settle(exact)
+    K = args.steps
+    with Clocks(dev) as clk:
+        ms_max, launches = timed_frames(r, K)
+    value = K * world / (ms_max / 1e3)
+    ms_plain, _ = timed_frames(exact, K)
+    plain_fps = K * world / (ms_plain / 1e3)
+
+    sums = {"project_ms": 0.0, "sort_ms": 0.0, "raster_ms": 0.0}
+    vis = ovl = 0
+    for v in views:
+        r.render_device(v, W, H, (0, 0, 0), out.data_ptr(), nbytes)
+        s, _ = r.finish()
+        for k in sums:
+            sums[k] += getattr(s, k)
+        vis += s.visible
+        ovl += s.overlaps
+    nv = len(views)
+    stage = {k: v / nv for k, v in sums.items()}
+    V, P = vis / nv, ovl / nv
+
+    # End to end through the public C ABI into pinned host memory.
+    host = torch.empty(W * H * 3, dtype=torch.uint8).pin_memory()
+    for v in warm[:3]:
+        r.render_into(v, W, H, (0, 0, 0), host.data_ptr(), host.numel())
+    barrier()
+    t0 = time.perf_counter()
+    for i in range(K):
+        r.render_into(views[i % len(views)], W, H, (0, 0, 0), host.data_ptr(), host.numel())
+    te = torch.tensor([time.perf_counter() - t0], device=dev)
+    if world > 1:
+        torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
+    e2e = K * world / float(te.item())
+
+    line = None
+    if rank == 0:
+        # Quality over the orbit: learned and base-colour-only against exact SH.
+        from splat_b200 import Frame
+
+        ps_l, ps_b, mx_l = [], [], []
+        fe, fl, fb = Frame(), Frame(), Frame()
+        for v in timed[: args.psnr_frames]:
+            exact.render(v, W, H, (0, 0, 0), fe)
+            r.render(v, W, H, (0, 0, 0), fl)
+            rbase.render(v, W, H, (0, 0, 0), fb)
+            ps_l.append(O.psnr(fl.pixels, fe.pixels))
+            ps_b.append(O.psnr(fb.pixels, fe.pixels))
+            mx_l.append(int(np.abs(fl.pixels.astype(int) - fe.pixels.astype(int)).max()))
+        peak, peak_kind = measured_peaks()
+        try:
+            tpeak = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["bf16_tflops_sustained"])
+            tpeak_kind = "measured (sustained dense bf16 GEMM; fp16 runs at the same rate)"
+        except Exception:
+            tpeak, tpeak_kind = 1400.0, "fallback"
+        N = args.splats
+        tiles = ((W + 15) // 16) * ((H + 15) // 16)
+        bytes_stage = {
+            "project": N * cfg["s_in"] + N * S_BIN + V * S_REC,
+            "sort": 2 * N * S_BIN + P * 8 + 2 * P * 8,
+            "raster": P * (8 + S_REC) + tiles * 8 + W * H * 3,
+        }
+        times = {"project": stage["project_ms"], "sort": stage["sort_ms"], "raster": stage["raster_ms"]}
+        dom = max(times, key=times.get)
+        achieved = bytes_stage[dom] / (times[dom] / 1e3) / 1e9
+        cpu = None
+        if not args.no_cpu_baseline:
+            fps, cores, frames = cpu_baseline(scene, timed, W, H, args.cpu_sample_s)
+            cpu = {"value": fps, "unit": "frames/s", "cores": cores, "kind": "port",
+                   "sample": f"{frames} full {W}x{H} frames of the orbit with exact SH (~{args.cpu_sample_s:.0f} s)"}
+        line = {
+            "metric": cfg["metric"], "value": value, "unit": "frames/s", "n_gpus": world, "steps": K,
+            "warmup": args.warmup, "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 (fp16 MLP operands, fp32 accumulate)", "data": "synthetic",
+            "config": {"workload": cfg["workload"], "splats": N, "width": W, "height": H, "tile": 16,
+                       "storage": "fp16 geometry + 16 fp16 latents", "visible": V, "pairs": P,
+                       "parallelism": f"view-parallel x{world}",
+                       "l2": f"inputs larger than L2 (scene {N * cfg['s_in'] / 1e6:.0f} MB + records)"},
+            "plain_exact_sh_frames_per_s": plain_fps,
+            "vs_plain": value / plain_fps,
+            "psnr_vs_exact_sh": {"mean_db": float(np.mean(ps_l)), "min_db": float(np.min(ps_l)),
+                                 "max_abs": int(max(mx_l)), "frames": len(ps_l)},
+            "psnr_base_colour_vs_exact_sh": {"mean_db": float(np.mean(ps_b)), "min_db": float(np.min(ps_b))},
+            "training": {"epochs": ts.epochs, "steps": ts.steps, "samples": int(samples), "ms": ts.ms,
+                         "samples_per_s": samples / (ts.ms / 1e3), "final_loss": ts.last_loss,
+                         "mean_loss_last_call": ts.mean_loss, "train_ctas": train_ctas,
+                         "roofline": {"bound": "tensor", "achieved": train_tflops, "peak": tpeak,
+                                      "unit": "TFLOP/s", "frac": train_tflops / tpeak, "peak_kind": tpeak_kind,
+                                      "algorithmic_flop_per_sample": flop_per_sample},
+                         "clocks": clk_train.summary()},
+            "gsplat_tiles_per_s": P * value / world / 1e9,
+            "stages_ms": stage,
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                         "algorithmic_bytes": bytes_stage[dom]},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e, "unit": "frames/s", "h2d_bytes_per_step": 56,
+                    "d2h_bytes_per_step": W * H * 3 + 32,
+                    "note": "input per step: the 56-byte view (the trained scene stays resident); output: the u8 "
+                            "frame into pinned host memory plus the 32-byte frame state"},
+            "clocks": clk.summary(),
+            "gpu_launches": launches,
+        }
+        print(json.dumps(line), flush=True)
+    for x in (r, rbase, exact):
+        x.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
 def batch_workload(args):
     from splat_b200 import synth
 
@@ -653,6 +859,8 @@ def main():
             run_batch(args)
     elif args.impl == "reference":
         run_reference(args)
+    elif args.config == "learned":
+        run_learned(args)
     else:
         run_ours(args)
 

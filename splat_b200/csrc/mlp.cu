@@ -9,13 +9,13 @@
 // splat: sample s of an epoch is (splat, direction) = divmod(perm(s), n_dirs)
 // for a bijective shuffle `perm` of [0, n * n_dirs) keyed by the epoch.
 //
-// One step over `batch` samples is three launches:
+// One step over `batch` samples is two launches:
 //   k_train<SRC>     forward + backward, 128 samples per tile, persistent CTAs;
 //                    weight gradients accumulate in TMEM over a CTA's tiles and
 //                    are added to one fp32 vector; latent gradients are added
 //                    to per-splat rows and the touched rows listed
-//   k_adam_params    Adam on the fp32 master parameters, fp16 operand copy
-//   k_adam_latents   lazy Adam on the touched latent rows only
+//   k_adam           Adam on the fp32 master parameters (fp16 operand copy
+//                    refreshed) and lazy Adam on the touched latent rows only
 // Loss: mean over active samples and channels of (rgb - target)^2.
 #include <cuda_fp16.h>
 
@@ -75,9 +75,7 @@ struct StepState {
   unsigned long long loss_steps;
   float last_loss;
   unsigned int touched;       // latent rows touched by the running step
-  unsigned int lat_count;     // ... handed to k_adam_latents
-  unsigned int lat_t;         // Adam step of k_adam_latents
-  float lat_inv;              // gradient scale of k_adam_latents
+  unsigned int adam_done;     // CTAs of k_adam finished with the step
   unsigned int error;         // a bounded wait gave up
 };
 
@@ -85,7 +83,7 @@ enum class Src { kExplicit, kScene };
 
 struct TrainArgs {
   const uint16_t* p16;  // fp16 operand copy of the parameters
-  float* grad;          // kParams fp32 gradient sums (zeroed by k_adam_params)
+  float* grad;          // kParams fp32 gradient sums (zeroed by k_adam)
   StepState* st;
   // explicit samples (gradient checks)
   const uint4* ex_lat;  // count x 16 halves
@@ -99,6 +97,9 @@ struct TrainArgs {
   const float* color;   // FP32 scene: 3 planes of n
   const float* sh;      // FP32 scene: rest*3 planes of n
   const uint16_t* sh16; // FP16 scene: (rest+1)*3 planes of n halves
+  const float4* shs;    // the same coefficients splat-major: base colour, then
+                        // the rest (RGB innermost), padded to sh_row4 float4
+  uint32_t sh_row4;
   uint64_t n;
   const float4* dirs;
   uint32_t n_dirs;
@@ -118,20 +119,41 @@ __device__ __forceinline__ uint64_t epoch_key(uint64_t seed, uint64_t epoch) {
   return seed * 0x9E3779B97F4A7C15ull + epoch * 0xD1B54A32D192ED03ull + 1;
 }
 
-// Exact SH colour of splat `s` at unit direction d, clamped to [0, 1].
+// Float4s per splat-major coefficient row of SH degree DEG.
 template <int DEG>
-__device__ __forceinline__ void sh_target(const TrainArgs& a, uint64_t s, float dx, float dy, float dz, float c[3]) {
-  if (a.sh16) {
-    const uint64_t n = a.n;
-    for (int ch = 0; ch < 3; ch++) c[ch] = __half2float(__ushort_as_half(__ldg(a.sh16 + ch * n + s)));
-    sh::eval_sh<DEG>([&](int coef, int ch) { return __half2float(__ushort_as_half(__ldg(a.sh16 + ((uint64_t)(coef + 1) * 3 + ch) * n + s))); },
-                     dx, dy, dz, c);
-  } else {
-    const uint64_t n = a.n;
-    for (int ch = 0; ch < 3; ch++) c[ch] = __ldg(a.color + ch * n + s);
-    sh::eval_sh<DEG>([&](int coef, int ch) { return __ldg(a.sh + ((uint64_t)coef * 3 + ch) * n + s); }, dx, dy, dz, c);
-  }
+__host__ __device__ constexpr uint32_t sh_row4() {
+  return ((DEG + 1) * (DEG + 1) * 3 + 3) / 4;
+}
+
+// Exact SH colour of a splat whose coefficient row is `row` (base colour,
+// then the rest coefficients, RGB innermost) at unit direction d, clamped
+// to [0, 1].
+template <int DEG>
+__device__ __forceinline__ void sh_target(const float* row, float dx, float dy, float dz, float c[3]) {
+  c[0] = row[0];
+  c[1] = row[1];
+  c[2] = row[2];
+  sh::eval_sh<DEG>([&](int coef, int ch) { return row[3 + 3 * coef + ch]; }, dx, dy, dz, c);
   for (int ch = 0; ch < 3; ch++) c[ch] = fminf(fmaxf(c[ch], 0.0f), 1.0f);
+}
+
+// The splat-major coefficient rows from the scene's planes.
+__global__ void k_pack_sh(const float* __restrict__ color, const float* __restrict__ sh,
+                          const uint16_t* __restrict__ sh16, uint64_t n, uint32_t coefs, uint32_t row4,
+                          float* __restrict__ out) {
+  for (uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n * row4 * 4;
+       q += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t s = q / (row4 * 4);
+    const uint32_t c = (uint32_t)(q % (row4 * 4));
+    float v = 0.0f;
+    if (c < coefs) {
+      if (sh16)
+        v = __half2float(__ushort_as_half(sh16[(uint64_t)c * n + s]));
+      else
+        v = c < 3 ? color[(uint64_t)c * n + s] : sh[(uint64_t)(c - 3) * n + s];
+    }
+    out[q] = v;
+  }
 }
 
 __device__ __forceinline__ float warp_sum(float v) {
@@ -219,6 +241,8 @@ __global__ void __launch_bounds__(kTrainThreads) k_train(TrainArgs a) {
     uint64_t splat = 0;
     uint4 l0 = make_uint4(0, 0, 0, 0), l1 = l0;
     float d[3] = {0.f, 0.f, 0.f}, tgt[3] = {0.f, 0.f, 0.f};
+    constexpr uint32_t R4 = sh_row4<DEG>();
+    float4 row4[R4];  // the splat's coefficients: loads in flight during the forward pass
     if (SRC == Src::kExplicit) {
       active = j < a.ex_count;
       if (active) {
@@ -240,7 +264,9 @@ __global__ void __launch_bounds__(kTrainThreads) k_train(TrainArgs a) {
         d[2] = dv.z;
         l0 = __ldg(a.lat16 + 2 * splat);
         l1 = __ldg(a.lat16 + 2 * splat + 1);
-        sh_target<DEG>(a, splat, d[0], d[1], d[2], tgt);
+        const float4* src = a.shs + splat * R4;
+#pragma unroll
+        for (uint32_t q = 0; q < R4; q++) row4[q] = __ldg(src + q);
       }
     }
     mlp::store_input(S.R, 8, tid, l0, l1, d[0], d[1], d[2]);
@@ -269,6 +295,7 @@ __global__ void __launch_bounds__(kTrainThreads) k_train(TrainArgs a) {
       umma::commit(mbar);
     }
     wait_mma();
+    if (SRC == Src::kScene && active) sh_target<DEG>(reinterpret_cast<const float*>(row4), d[0], d[1], d[2], tgt);
     {
       float z[16];
       umma::tmem_ld16(umma::tmem_warp_addr(tmem, kTZ), z);
@@ -399,61 +426,94 @@ __device__ __forceinline__ float adam_update(float& m, float& v, float g, float 
   return lr * mh / (sqrtf(vh) + eps);
 }
 
-// Adam on the fp32 masters; refreshes the fp16 operand copy and hands the
-// step's loss and touched latent rows over.
-__global__ void k_adam_params(float* __restrict__ p32, float* __restrict__ pm, float* __restrict__ pv,
-                              uint16_t* __restrict__ p16, float* __restrict__ grad, StepState* st, AdamArgs a) {
+constexpr uint32_t kAdamThreads = 256;
+constexpr uint32_t kAdamParamCtas = (mlp::kParams + kAdamThreads - 1) / kAdamThreads;
+
+// One launch after each training step. CTAs [0, kAdamParamCtas) apply Adam
+// to the fp32 master parameters and refresh their fp16 copy; the others
+// apply lazy Adam to the latent rows the step touched, one thread per row
+// (16 elements as float4s). The last CTA to finish closes the step: records
+// its loss, clears the touched list and advances the step counter.
+__global__ void __launch_bounds__(kAdamThreads) k_adam(float* __restrict__ p32, float* __restrict__ pm,
+                                                       float* __restrict__ pv, uint16_t* __restrict__ p16,
+                                                       float* __restrict__ grad, float* __restrict__ lat32,
+                                                       float* __restrict__ lm, float* __restrict__ lv,
+                                                       uint16_t* __restrict__ lat16, float* __restrict__ lat_grad,
+                                                       const uint32_t* __restrict__ touched, StepState* st,
+                                                       AdamArgs a) {
   const uint64_t step = *reinterpret_cast<volatile unsigned long long*>(&st->step);
   const uint64_t k = step % a.steps_per_epoch;
   const uint64_t active = min((uint64_t)a.batch, a.samples - k * a.batch);
   const float inv = 1.0f / (kLossScale * (float)active);
   const float t = (float)(step + 1);
   const float c1 = 1.0f - powf(a.b1, t), c2 = 1.0f - powf(a.b2, t);
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < mlp::kParams) {
-    const float g = grad[i] * inv;
-    grad[i] = 0.0f;
-    float m = pm[i], v = pv[i];
-    const float p = p32[i] - adam_update(m, v, g, a.lr, a.b1, a.b2, a.eps, c1, c2);
-    pm[i] = m;
-    pv[i] = v;
-    p32[i] = p;
-    p16[i] = __half_as_ushort(__float2half_rn(p));
+  if (blockIdx.x < kAdamParamCtas) {
+    const uint32_t i = blockIdx.x * kAdamThreads + threadIdx.x;
+    if (i < mlp::kParams) {
+      const float g = grad[i] * inv;
+      grad[i] = 0.0f;
+      float m = pm[i], v = pv[i];
+      const float p = p32[i] - adam_update(m, v, g, a.lr, a.b1, a.b2, a.eps, c1, c2);
+      pm[i] = m;
+      pv[i] = v;
+      p32[i] = p;
+      p16[i] = __half_as_ushort(__float2half_rn(p));
+    }
+  } else {
+    const uint32_t count = *reinterpret_cast<volatile unsigned int*>(&st->touched);
+    for (uint32_t q = (blockIdx.x - kAdamParamCtas) * kAdamThreads + threadIdx.x; q < count;
+         q += (gridDim.x - kAdamParamCtas) * kAdamThreads) {
+      const uint64_t row = (uint64_t)__ldg(touched + q) * 16;
+      float4* g4 = reinterpret_cast<float4*>(lat_grad + row);
+      float4* m4 = reinterpret_cast<float4*>(lm + row);
+      float4* v4 = reinterpret_cast<float4*>(lv + row);
+      float4* p4 = reinterpret_cast<float4*>(lat32 + row);
+      float4 g[4], m[4], v[4], p[4];
+#pragma unroll
+      for (int c = 0; c < 4; c++) {
+        g[c] = g4[c];
+        m[c] = m4[c];
+        v[c] = v4[c];
+        p[c] = p4[c];
+      }
+      uint32_t h[8];
+#pragma unroll
+      for (int c = 0; c < 4; c++) {
+        float* gg = &g[c].x;
+        float* mm = &m[c].x;
+        float* vv = &v[c].x;
+        float* pp = &p[c].x;
+#pragma unroll
+        for (int e = 0; e < 4; e++) pp[e] -= adam_update(mm[e], vv[e], gg[e] * inv, a.lr, a.b1, a.b2, a.eps, c1, c2);
+        h[2 * c] = mlp::pack_half2(p[c].x, p[c].y);
+        h[2 * c + 1] = mlp::pack_half2(p[c].z, p[c].w);
+        g4[c] = make_float4(0.f, 0.f, 0.f, 0.f);
+        m4[c] = m[c];
+        v4[c] = v[c];
+        p4[c] = p[c];
+      }
+      uint4* o = reinterpret_cast<uint4*>(lat16 + row);
+      o[0] = make_uint4(h[0], h[1], h[2], h[3]);
+      o[1] = make_uint4(h[4], h[5], h[6], h[7]);
+    }
   }
-  if (i == 0) {
-    const double ls = st->loss_step / (3.0 * (double)active);
-    st->loss_step = 0.0;
-    st->loss_sum += ls;
-    st->loss_steps += 1;
-    st->last_loss = (float)ls;
-    st->lat_count = st->touched;
-    st->touched = 0;
-    st->lat_t = (uint32_t)(step + 1);
-    st->lat_inv = inv;
+  // The last CTA closes the step.
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(&st->adam_done, 1u) == gridDim.x - 1) {
+      __threadfence();
+      const double ls = *reinterpret_cast<volatile double*>(&st->loss_step) / (3.0 * (double)active);
+      st->loss_step = 0.0;
+      st->loss_sum += ls;
+      st->loss_steps += 1;
+      st->last_loss = (float)ls;
+      st->touched = 0;
+      st->adam_done = 0;
+      __threadfence();
+      st->step = step + 1;
+    }
   }
-}
-
-// Lazy Adam on the latent rows the step touched; advances the step counter.
-__global__ void k_adam_latents(float* __restrict__ lat32, float* __restrict__ lm, float* __restrict__ lv,
-                               uint16_t* __restrict__ lat16, float* __restrict__ lat_grad,
-                               const uint32_t* __restrict__ touched, StepState* st, AdamArgs a) {
-  const uint32_t count = st->lat_count;
-  const float t = (float)st->lat_t;
-  const float inv = st->lat_inv;
-  const float c1 = 1.0f - powf(a.b1, t), c2 = 1.0f - powf(a.b2, t);
-  for (uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; q < (uint64_t)count * 16;
-       q += (uint64_t)gridDim.x * blockDim.x) {
-    const uint64_t e = (uint64_t)touched[q >> 4] * 16 + (q & 15);
-    const float g = lat_grad[e] * inv;
-    lat_grad[e] = 0.0f;
-    float m = lm[e], v = lv[e];
-    const float p = lat32[e] - adam_update(m, v, g, a.lr, a.b1, a.b2, a.eps, c1, c2);
-    lm[e] = m;
-    lv[e] = v;
-    lat32[e] = p;
-    lat16[e] = __half_as_ushort(__float2half_rn(p));
-  }
-  if (blockIdx.x == 0 && threadIdx.x == 0) st->step += 1;
 }
 
 __global__ void k_to_half(const float* __restrict__ src, uint16_t* __restrict__ dst, uint64_t count) {
@@ -552,6 +612,7 @@ struct splat_cuda_learner {
   uint16_t* lat16 = nullptr;
   uint32_t *stamp = nullptr, *touched = nullptr;
   float4* dirs = nullptr;
+  float* shs = nullptr;
   StepState* st = nullptr;
   cudaGraphExec_t graph = nullptr;  // kGraphSteps steps
   uint32_t launches = 0;
@@ -576,14 +637,18 @@ int lcuda(splat_cuda_learner* L, cudaError_t e, const char* what) {
     if (e_ != cudaSuccess) return lcuda(L, e_, what); \
   } while (0)
 
-// One step: train, Adam on the parameters, Adam on the touched latents.
+void enqueue_adam(splat_cuda_learner* L, cudaStream_t s) {
+  const uint32_t lat_ctas = std::max(1u, std::min((L->batch + kAdamThreads - 1) / kAdamThreads, 4u * L->num_sms));
+  k_adam<<<kAdamParamCtas + lat_ctas, kAdamThreads, 0, s>>>(L->p32, L->pm, L->pv, L->p16, L->grad, L->lat32, L->lm,
+                                                             L->lv, L->lat16, L->lgrad, L->touched, L->st, L->adam);
+}
+
+// One step: train, then Adam on the parameters and the touched latents.
 cudaError_t enqueue_step(splat_cuda_learner* L, cudaStream_t s) {
   cudaError_t e = launch_train<Src::kScene>(L->args, L->grid, L->sh_degree, s);
   if (e != cudaSuccess) return e;
-  k_adam_params<<<(mlp::kParams + 255) / 256, 256, 0, s>>>(L->p32, L->pm, L->pv, L->p16, L->grad, L->st, L->adam);
-  k_adam_latents<<<std::max(1u, std::min(L->batch * 16u / 256u, 2048u)), 256, 0, s>>>(
-      L->lat32, L->lm, L->lv, L->lat16, L->lgrad, L->touched, L->st, L->adam);
-  L->launches += 3;
+  enqueue_adam(L, s);
+  L->launches += 2;
   return cudaGetLastError();
 }
 
@@ -661,6 +726,9 @@ SPLAT_API int splat_cuda_learner_create(const splat_cuda_handle* h, const splat_
       (rc = dalloc((void**)&L->lat16, nl * 2, "latents")) || (rc = dalloc((void**)&L->stamp, L->n * 4, "latents")) ||
       (rc = dalloc((void**)&L->touched, (size_t)L->batch * 4, "latents")) ||
       (rc = dalloc((void**)&L->dirs, (size_t)L->n_dirs * sizeof(float4), "directions")) ||
+      (rc = dalloc((void**)&L->shs,
+                   (size_t)L->n * (((L->sh_degree + 1) * (L->sh_degree + 1) * 3 + 3) / 4) * sizeof(float4),
+                   "coefficient rows")) ||
       (rc = dalloc((void**)&L->st, sizeof(StepState), "state")))
     return bail(rc);
 
@@ -688,6 +756,14 @@ SPLAT_API int splat_cuda_learner_create(const splat_cuda_handle* h, const splat_
     a.sh = h->sh;
   }
   a.n = L->n;
+  a.shs = reinterpret_cast<const float4*>(L->shs);
+  a.sh_row4 = ((L->sh_degree + 1) * (L->sh_degree + 1) * 3 + 3) / 4;
+  {
+    const uint32_t coefs = (L->sh_degree + 1) * (L->sh_degree + 1) * 3;
+    k_pack_sh<<<(uint32_t)std::min<uint64_t>((L->n * a.sh_row4 * 4 + 255) / 256, 8192), 256, 0, L->stream>>>(
+        a.color, a.sh, a.sh16, L->n, coefs, a.sh_row4, L->shs);
+    if ((e = cudaGetLastError()) != cudaSuccess) return bail(lcuda(L, e, "coefficient rows"));
+  }
   a.dirs = L->dirs;
   a.n_dirs = L->n_dirs;
   a.lat16 = reinterpret_cast<const uint4*>(L->lat16);
@@ -777,7 +853,7 @@ SPLAT_API int splat_cuda_learner_train(splat_cuda_learner* L, uint64_t steps, sp
       L->graph = nullptr;
       return lcuda(L, e, "instantiate training graph");
     }
-    L->launches -= 3 * kGraphSteps;  // counted again at each replay
+    L->launches -= 2 * kGraphSteps;  // counted again at each replay
   }
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   LCK(cudaEventCreate(&e0), "event");
@@ -786,7 +862,7 @@ SPLAT_API int splat_cuda_learner_train(splat_cuda_learner* L, uint64_t steps, sp
   uint64_t left = steps;
   while (L->graph && left >= kGraphSteps) {
     LCK(cudaGraphLaunch(L->graph, L->stream), "training graph");
-    L->launches += 3 * kGraphSteps;
+    L->launches += 2 * kGraphSteps;
     left -= kGraphSteps;
   }
   for (; left; left--) LCK(enqueue_step(L, L->stream), "training step");
@@ -829,12 +905,9 @@ SPLAT_API int splat_cuda_learner_step_debug(splat_cuda_learner* L, float* grad_p
     LCK(cudaMemcpy(grad_latents, L->lgrad, L->n * 64, cudaMemcpyDeviceToHost), "read gradient");
     for (uint64_t i = 0; i < L->n * 16; i++) grad_latents[i] = (float)(grad_latents[i] * inv);
   }
-  k_adam_params<<<(mlp::kParams + 255) / 256, 256, 0, L->stream>>>(L->p32, L->pm, L->pv, L->p16, L->grad, L->st,
-                                                                     L->adam);
-  k_adam_latents<<<std::max(1u, std::min(L->batch * 16u / 256u, 2048u)), 256, 0, L->stream>>>(
-      L->lat32, L->lm, L->lv, L->lat16, L->lgrad, L->touched, L->st, L->adam);
-  L->launches += 2;
-  LCK(cudaGetLastError(), "Adam kernels");
+  enqueue_adam(L, L->stream);
+  L->launches += 1;
+  LCK(cudaGetLastError(), "Adam kernel");
   return sync_state(L, &st);
 }
 
@@ -884,7 +957,7 @@ SPLAT_API int splat_cuda_learner_destroy(splat_cuda_learner* L) {
   if (L->graph) cudaGraphExecDestroy(L->graph);
   for (void* p : {(void*)L->p32, (void*)L->pm, (void*)L->pv, (void*)L->grad, (void*)L->p16, (void*)L->lat32,
                   (void*)L->lm, (void*)L->lv, (void*)L->lgrad, (void*)L->lat16, (void*)L->stamp, (void*)L->touched,
-                  (void*)L->dirs, (void*)L->st})
+                  (void*)L->dirs, (void*)L->shs, (void*)L->st})
     if (p) cudaFree(p);
   if (L->stream) cudaStreamDestroy(L->stream);
   delete L;

@@ -43,16 +43,16 @@ constexpr uint32_t kIdN16 = umma::idesc_f16(128, 16, false, false);
 constexpr uint32_t kIdWgN96 = umma::idesc_f16(128, 96, true, true);
 constexpr uint32_t kIdWgN16 = umma::idesc_f16(128, 16, true, true);
 
-// Forward operand tiles of one CTA (feature-chunked, 128 rows).
-//   act: chunks 0-7 = h1, then h2 (in place); chunks 8-11 = x
+// Inference tiles of one CTA (feature-chunked, 128 rows).
+//   act: chunks 0-3 = x; then chunks 0-7 = h1 once layer 1 is done; then h2
 //   w1f: W1 as B (n = out 64, k = in 32); w2f: W2 (64 x 64); w3f: W3 (16 x 64)
 struct ForwardTiles {
-  alignas(128) uint16_t act[kRows * 96];
+  alignas(128) uint16_t act[kRows * kHidden];
   alignas(128) uint16_t w1f[kHidden * kIn];
   alignas(128) uint16_t w2f[kHidden * kHidden];
   alignas(128) uint16_t w3f[kOut * kHidden];
-  float b2[kHidden];
-  float b3[kOut];
+  alignas(16) float b2[kHidden];
+  float b3[4];
 };
 
 __device__ __forceinline__ uint32_t pack_half2(float a, float b) {
@@ -89,14 +89,6 @@ __device__ __forceinline__ void load_cols(uint16_t* tile, const uint16_t* __rest
   }
 }
 
-__device__ __forceinline__ void load_forward_weights(ForwardTiles& S, const uint16_t* __restrict__ p) {
-  load_rows(S.w1f, p + kW1, kHidden, kIn);
-  load_rows(S.w2f, p + kW2, kHidden, kHidden);
-  load_rows(S.w3f, p + kW3, kOut, kHidden);
-  for (uint32_t i = threadIdx.x; i < kHidden; i += blockDim.x) S.b2[i] = __half2float(__ushort_as_half(p[kB2 + i]));
-  for (uint32_t i = threadIdx.x; i < kOut; i += blockDim.x) S.b3[i] = __half2float(__ushort_as_half(p[kB3 + i]));
-}
-
 // Stores 8 consecutive features (chunk `chunk`) of row r.
 __device__ __forceinline__ void store_chunk(uint16_t* tile, uint32_t r, uint32_t chunk, const float (&v)[8]) {
   uint4 u;
@@ -108,6 +100,42 @@ __device__ __forceinline__ void store_chunk(uint16_t* tile, uint32_t r, uint32_t
 }
 __device__ __forceinline__ void store_chunk_raw(uint16_t* tile, uint32_t r, uint32_t chunk, uint4 u) {
   *reinterpret_cast<uint4*>(reinterpret_cast<uint8_t*>(tile) + chunk * kRows * 16u + r * 16u) = u;
+}
+
+__device__ __forceinline__ void load_forward_weights(ForwardTiles& S, const uint16_t* __restrict__ p) {
+  load_rows(S.w1f, p + kW1, kHidden, kIn);
+  load_rows(S.w2f, p + kW2, kHidden, kHidden);
+  load_rows(S.w3f, p + kW3, kOut, kHidden);
+  for (uint32_t i = threadIdx.x; i < kHidden; i += blockDim.x) S.b2[i] = __half2float(__ushort_as_half(p[kB2 + i]));
+  for (uint32_t i = threadIdx.x; i < 4; i += blockDim.x)
+    S.b3[i] = i < 3 ? __half2float(__ushort_as_half(p[kB3 + i])) : 0.0f;
+}
+
+// Inference epilogue of layer 1 or 2 for this thread's row: h = fp16(relu(z
+// (+ bias))) from TMEM columns [col, col + 64) into chunks 0-7 of `act`,
+// converted and clamped two values at a time (relu after the rounding gives
+// the same values: rounding is monotonic and keeps 0).
+__device__ __forceinline__ void relu_epilogue(uint32_t tmem_base, uint32_t col, const float* bias, uint16_t* act,
+                                              uint32_t r) {
+  const __half2 zero = __float2half2_rn(0.0f);
+#pragma unroll
+  for (uint32_t q = 0; q < 2; q++) {
+    float v[32];
+    umma::tmem_ld32(umma::tmem_warp_addr(tmem_base, col + 32 * q), v);
+    uint32_t h[16];
+#pragma unroll
+    for (int j = 0; j < 16; j++) {
+      float a = v[2 * j], b = v[2 * j + 1];
+      if (bias) {
+        a += bias[32 * q + 2 * j];
+        b += bias[32 * q + 2 * j + 1];
+      }
+      const __half2 x = __hmax2(__floats2half2_rn(a, b), zero);
+      h[j] = *reinterpret_cast<const uint32_t*>(&x);
+    }
+#pragma unroll
+    for (int c = 0; c < 4; c++) store_chunk_raw(act, r, 4 * q + c, make_uint4(h[4 * c], h[4 * c + 1], h[4 * c + 2], h[4 * c + 3]));
+  }
 }
 
 // Writes the input row r: 16 latent halves (two uint4), direction, 1, zeros.

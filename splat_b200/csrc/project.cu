@@ -334,25 +334,25 @@ __global__ void __launch_bounds__(256) k_project_batch(const ViewTask* __restric
 }
 
 // Learned colour (FP16 storage): the projection of k_project, then the
-// colour MLP of each 128-splat tile on the tensor cores (mlp.cuh), fused:
-// persistent CTAs of 128 threads, thread t = splat t of the tile = TMEM lane
-// t. The MLP's input row is the splat's 16 latents and its view direction;
-// layers 1-3 are three tcgen05.mma groups with their epilogues between. The
-// record is written by the projection and its colour filled in after.
+// colour MLP of each 128-splat tile (mlp.cuh), fused: persistent CTAs of 128
+// threads, thread t = splat t of the tile = TMEM lane t. The MLP's input row
+// is the splat's 16 latents and its view direction; the three layers are
+// tcgen05.mma groups with their epilogues between. The record is written by
+// the projection and its colour filled in after.
 constexpr uint32_t kLearnedThreads = 128;
-constexpr uint32_t kLearnedTmemCols = 128;  // z1/z2 at 0-63, z3 at 64-79
-// Requested dynamic shared memory: more than a CTA needs, so that at most
-// four CTAs share an SM (4 x 128 TMEM columns = all 512).
-constexpr size_t kLearnedSmem = 48 * 1024;
+constexpr uint32_t kLearnedTmemCols = 64;  // z1, then z2, then z3 (16)
 
 struct LearnedSmem {
   mlp::ForwardTiles t;
   uint64_t mbar;
   uint32_t tmem;
 };
-static_assert(sizeof(LearnedSmem) <= kLearnedSmem, "learned projection shared memory");
+// At most 7 CTAs fit an SM by shared memory (228 KB, 1 KB reserved per CTA),
+// so the CTAs of an SM never ask for more than 7 x 64 of its 512 TMEM columns.
+constexpr size_t kLearnedSmem = sizeof(LearnedSmem);
+static_assert((228 * 1024) / (kLearnedSmem + 1024) * kLearnedTmemCols <= 512, "TMEM oversubscribed");
 
-__global__ void __launch_bounds__(kLearnedThreads) k_project_learned(ViewTask t, ViewTask* __restrict__ table,
+__global__ void __launch_bounds__(kLearnedThreads, 7) k_project_learned(ViewTask t, ViewTask* __restrict__ table,
                                                                      float* __restrict__ dbg_proj,
                                                                      float* __restrict__ dbg_color, FrameCounters fc) {
   extern __shared__ __align__(128) uint8_t smem_raw[];
@@ -387,19 +387,19 @@ __global__ void __launch_bounds__(kLearnedThreads) k_project_learned(ViewTask t,
     float dir[3] = {0.f, 0.f, 0.f};
     uint4 l0 = make_uint4(0, 0, 0, 0), l1 = l0;
     if (i < n) {
-      project_splat<0, true, true>(t.fp, t.s, i, t.rec, t.bin, dbg_proj, nullptr, vis, used_fp64, dir);
-      l0 = __ldg(t.s.lat16 + 2 * i);
+      l0 = __ldg(t.s.lat16 + 2 * i);  // in flight during the projection
       l1 = __ldg(t.s.lat16 + 2 * i + 1);
+      project_splat<0, true, true>(t.fp, t.s, i, t.rec, t.bin, dbg_proj, nullptr, vis, used_fp64, dir);
     }
-    mlp::store_input(S.t.act, 8, tid, l0, l1, dir[0], dir[1], dir[2]);
+    mlp::store_input(S.t.act, 0, tid, l0, l1, dir[0], dir[1], dir[2]);
     if (sync_or_abort()) { aborted = true; break; }
     if (tid == 0) {
       umma::fence_after_sync();
-      mlp::gemm_k(tmem, act, 8, umma::smem_u32(S.t.w1f), 64, 2, mlp::kIdN64);
+      mlp::gemm_k(tmem, act, 0, umma::smem_u32(S.t.w1f), 64, 2, mlp::kIdN64);
       umma::commit(mbar);
     }
     wait_mma();
-    mlp::hidden_epilogue(tmem, 0, nullptr, S.t.act, tid);
+    mlp::relu_epilogue(tmem, 0, nullptr, S.t.act, tid);  // h1 over x (layer 1 is done)
     if (sync_or_abort()) { aborted = true; break; }
     if (tid == 0) {
       umma::fence_after_sync();
@@ -407,16 +407,16 @@ __global__ void __launch_bounds__(kLearnedThreads) k_project_learned(ViewTask t,
       umma::commit(mbar);
     }
     wait_mma();
-    mlp::hidden_epilogue(tmem, 0, S.t.b2, S.t.act, tid);  // h2 over h1 (layer 2 is done)
+    mlp::relu_epilogue(tmem, 0, S.t.b2, S.t.act, tid);  // h2 over h1 (layer 2 is done)
     if (sync_or_abort()) { aborted = true; break; }
     if (tid == 0) {
       umma::fence_after_sync();
-      mlp::gemm_k(tmem + 64, act, 0, umma::smem_u32(S.t.w3f), 16, 4, mlp::kIdN16);
+      mlp::gemm_k(tmem, act, 0, umma::smem_u32(S.t.w3f), 16, 4, mlp::kIdN16);
       umma::commit(mbar);
     }
     wait_mma();
     float z[16];
-    umma::tmem_ld16(umma::tmem_warp_addr(tmem, 64), z);
+    umma::tmem_ld16(umma::tmem_warp_addr(tmem, 0), z);
     float rgb[3];
     for (int c = 0; c < 3; c++) rgb[c] = mlp::sigmoidf(z[c] + S.t.b3[c]);
     if (vis) {
@@ -457,7 +457,7 @@ cudaError_t launch_project(const ViewTask& t, ViewTask* table, float* dbg_proj, 
       if (e != cudaSuccess) return e;
     }
     const uint64_t tiles = (t.s.n + mlp::kRows - 1) / mlp::kRows;
-    const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(tiles, 4ull * ns));
+    const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(tiles, 7ull * ns));
     k_project_learned<<<grid, kLearnedThreads, kLearnedSmem, stream>>>(t, table, dbg_proj, dbg_color, fc);
     *launches += 1;
     return cudaGetLastError();
