@@ -460,7 +460,7 @@ def run_learned(args):
     learner = Learner(exact, LearnConfig(directions=256, batch=65536, lr=1e-3, seed=1))
     learner.train(1)  # warm-up: graph capture, clocks
     learner.set_params(*learner.params())
-    steps = int(round(args.learn_epochs * learner.steps_per_epoch))
+    steps = max(1, int(round(args.learn_epochs * learner.steps_per_epoch)))
     with Clocks(dev) as clk_train:
         ts = learner.train(steps)
     train_ctas = learner.option(Nat.LEARN_TRAIN_CTAS)
@@ -508,6 +508,16 @@ def run_learned(args):
             torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         return float(t.item()), (rr.get_option(Nat.SPLAT_OPT_KERNEL_LAUNCHES) - l0) % (1 << 32)
 
+    if args.profile:  # a short command for ncu: the training above, then --steps learned frames
+        for i in range(args.steps):
+            r.render_device(views[i % len(views)], W, H, (0, 0, 0), out.data_ptr(), nbytes)
+            s, _ = r.finish()
+        if rank == 0:
+            print(json.dumps({"profile_train_steps": ts.steps, "profile_frames": args.steps, "visible": s.visible,
+                              "pairs": s.overlaps}), flush=True)
+        for x in (r, rbase, exact):
+            x.close()
+        return
     settle(r)
     settle(exact)
     K = args.steps
