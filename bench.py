@@ -553,6 +553,29 @@ def run_learned(args):
         torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
     e2e = K * world / float(te.item())
 
+    # The batched form: the rank's orbit views as one recorded batch (one
+    # graph replay draws them all), learned colour and FP16 geometry.
+    from splat_b200.batch import BatchRenderer, BatchView
+
+    bat = BatchRenderer([r], [BatchView(0, v, W, H) for v in views])
+    bat.render()
+    bstream = torch.cuda.ExternalStream(bat.stream())
+    reps = max(1, K // max(len(views), 1))
+    bs, be = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    bs.record(bstream)
+    for _ in range(reps):
+        bat.run()
+    be.record(bstream)
+    _, _, regrown = bat.finish()
+    barrier()
+    assert not regrown
+    tb = torch.tensor([bs.elapsed_time(be)], device=dev)
+    if world > 1:
+        torch.distributed.all_reduce(tb, op=torch.distributed.ReduceOp.MAX)
+    batched_fps = reps * len(views) * world / (float(tb.item()) / 1e3)
+    bat.close()
+
     line = None
     if rank == 0:
         # Quality over the orbit: learned and base-colour-only against exact SH.
@@ -598,6 +621,8 @@ def run_learned(args):
                        "l2": f"inputs larger than L2 (scene {N * cfg['s_in'] / 1e6:.0f} MB + records)"},
             "plain_exact_sh_frames_per_s": plain_fps,
             "vs_plain": value / plain_fps,
+            "batched_learned_frames_per_s": batched_fps,
+            "batched_vs_plain": batched_fps / plain_fps,
             "psnr_vs_exact_sh": {"mean_db": float(np.mean(ps_l)), "min_db": float(np.min(ps_l)),
                                  "max_abs": int(max(mx_l)), "frames": len(ps_l)},
             "psnr_base_colour_vs_exact_sh": {"mean_db": float(np.mean(ps_b)), "min_db": float(np.min(ps_b))},

@@ -334,7 +334,8 @@ const char* splat_cuda_last_error(const splat_cuda_handle* h);
  * positions f32, scales/rotations/opacities f16. latents: n *
  * SPLAT_MLP_LATENT fp16 values, splat-major; mlp_params: SPLAT_MLP_PARAMS
  * fp16 values. 64 bytes per splat are read per frame (against 240 for the
- * FP32 SH3 scene). The handle renders with splat_cuda_render and friends. */
+ * FP32 SH3 scene). The handle renders with splat_cuda_render and friends,
+ * and in batches (splat_cuda_batch_create) beside SH scenes. */
 int splat_cuda_create_learned(const splat_scene_desc* geometry, const uint16_t* latents, const uint16_t* mlp_params,
                               int device, splat_cuda_handle** out);
 

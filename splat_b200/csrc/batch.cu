@@ -47,6 +47,9 @@ struct splat_cuda_batch {
   // plan (depends on the tile configuration)
   std::vector<ViewTask> tasks;
   ViewTask* table = nullptr;
+  std::vector<ViewTask> ltasks;  // the learned-colour views (their own projection launch)
+  ViewTask* ltable = nullptr;
+  uint64_t learned_tiles = 0;
   uint32_t n_tiles = 0, n_chunks = 0, proj_ctas = 0, bin_ctas = 0, col_ctas = 0, max_tiles = 0;
   uint32_t* counts = nullptr;
   size_t counts_words = 0;
@@ -103,6 +106,7 @@ void drop_graph(splat_cuda_batch* b) {
 void free_plan(splat_cuda_batch* b) {
   drop_graph(b);
   dfree(b->table);
+  dfree(b->ltable);
   dfree(b->counts);
   dfree(b->totals);
   dfree(b->ranges);
@@ -134,6 +138,8 @@ int plan(splat_cuda_batch* b) {
   free_plan(b);
   const uint32_t nv = (uint32_t)b->views.size();
   b->tasks.assign(nv, ViewTask{});
+  b->ltasks.clear();
+  b->learned_tiles = 0;
   uint64_t tile = 0, proj = 0, bins = 0, cols = 0, words = 0;
   uint32_t max_tiles = 0;
   for (uint32_t i = 0; i < nv; i++) {
@@ -155,13 +161,21 @@ int plan(splat_cuda_batch* b) {
     t.bin_cta0 = (uint32_t)bins;
     t.col_cta0 = (uint32_t)cols;
     tile += tiles;
-    proj += (h->n + 255) / 256;
+    if (h->lat16) {  // projected by the learned-colour launch, in tiles of 128 splats
+      t.pad[0] = i;
+      b->ltasks.push_back(t);
+      b->ltasks.back().proj_cta0 = (uint32_t)b->learned_tiles;
+      b->learned_tiles += (h->n + 127) / 128;
+    } else {
+      proj += (h->n + 255) / 256;
+    }
     bins += t.rows;
     cols += (tiles + 31) / 32;
     words += (uint64_t)t.rows * tiles;
     max_tiles = std::max(max_tiles, tiles);
   }
-  if (tile >= (1ull << 31) || proj >= (1ull << 31) || bins >= (1ull << 31) || cols >= (1ull << 31))
+  if (tile >= (1ull << 31) || proj >= (1ull << 31) || bins >= (1ull << 31) || cols >= (1ull << 31) ||
+      b->learned_tiles >= (1ull << 31))
     return bfail(b, SPLAT_ERR_CAPACITY, "batch too large for one launch per stage");
   b->n_tiles = (uint32_t)tile;
   b->n_chunks = (uint32_t)((tile + kScanChunk - 1) / kScanChunk);
@@ -178,6 +192,12 @@ int plan(splat_cuda_batch* b) {
   }
   BK(cudaMalloc(&b->table, nv * sizeof(ViewTask)), "cudaMalloc views");
   BK(cudaMemcpy(b->table, b->tasks.data(), nv * sizeof(ViewTask), cudaMemcpyHostToDevice), "upload views");
+  if (!b->ltasks.empty()) {
+    for (auto& lt : b->ltasks) lt.counts = b->tasks[lt.pad[0]].counts;
+    BK(cudaMalloc(&b->ltable, b->ltasks.size() * sizeof(ViewTask)), "cudaMalloc learned views");
+    BK(cudaMemcpy(b->ltable, b->ltasks.data(), b->ltasks.size() * sizeof(ViewTask), cudaMemcpyHostToDevice),
+       "upload learned views");
+  }
   const size_t nt = std::max<uint32_t>(b->n_tiles, 1);
   BK(cudaMalloc(&b->totals, nt * sizeof(uint32_t)), "cudaMalloc totals");
   BK(cudaMalloc(&b->ranges, nt * sizeof(uint2)), "cudaMalloc ranges");
@@ -221,6 +241,8 @@ int enqueue(splat_cuda_batch* b, cudaStream_t s) {
   BK(cudaMemsetAsync(b->counters, 0, b->counters_bytes, s), "clear counters");
   BK(stage_event(b, 0, s), "event");
   BK(launch_project_batch(b->table, nv, b->proj_ctas, fc, s, &b->launches), "project kernel");
+  BK(launch_project_learned_batch(b->ltable, (uint32_t)b->ltasks.size(), b->learned_tiles, fc, s, &b->launches),
+     "learned-colour project kernel");
   BK(stage_event(b, 1, s), "event");
   BinLaunch bl{};
   bl.n_views = nv;
@@ -262,7 +284,10 @@ int record(splat_cuda_batch* b) {
 }
 
 // Kernels per batch (the launch count one graph replay adds).
-uint32_t kernels_per_batch(const splat_cuda_batch* b) { return b->n_tiles ? 9u : 0u; }
+uint32_t kernels_per_batch(const splat_cuda_batch* b) {
+  if (!b->n_tiles) return 0u;
+  return 8u + (b->proj_ctas ? 1u : 0u) + (b->learned_tiles ? 1u : 0u);
+}
 
 const DevState& host_state(const splat_cuda_batch* b) { return *static_cast<const DevState*>(b->counters_host); }
 
@@ -324,7 +349,6 @@ SPLAT_API int splat_cuda_batch_create(splat_cuda_handle* const* scenes, uint32_t
   for (uint32_t i = 0; i < n_scenes; i++) {
     if (!scenes[i]) return reject(SPLAT_ERR_INVALID_ARG, "null scene handle");
     if (scenes[i]->device != scenes[0]->device) return reject(SPLAT_ERR_INVALID_ARG, "scenes on different devices");
-    if (scenes[i]->lat16) return reject(SPLAT_ERR_UNSUPPORTED, "learned-colour scenes render one view per call");
   }
   for (uint32_t i = 0; i < n_views; i++) {
     const splat_batch_view& v = views[i];

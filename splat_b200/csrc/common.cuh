@@ -139,7 +139,7 @@ struct ViewTask {
   uint32_t proj_cta0;   // first CTA of the view in the projection launch
   uint32_t bin_cta0;    // ... in the count and scatter launches
   uint32_t col_cta0;    // ... in the column-scan launch
-  uint32_t pad[1];
+  uint32_t pad[1];      // learned-colour batch table: the view's batch index
 };
 
 // The view whose `field` (a first-CTA or first-tile member) is the largest
@@ -173,6 +173,11 @@ cudaError_t launch_project(const ViewTask& t, ViewTask* table, float* dbg_proj, 
                            const FrameCounters& fc, cudaStream_t stream, uint32_t* launches);
 cudaError_t launch_project_batch(const ViewTask* table, uint32_t n_views, uint32_t total_ctas,
                                  const FrameCounters& fc, cudaStream_t stream, uint32_t* launches);
+// The learned-colour views of a batch: `table` holds n_views copies of them
+// with proj_cta0 = first tile of 128 splats in this launch and pad[0] = the
+// view's index in the batch.
+cudaError_t launch_project_learned_batch(ViewTask* table, uint32_t n_views, uint64_t total_tiles,
+                                         const FrameCounters& fc, cudaStream_t stream, uint32_t* launches);
 // Count-matrix rows (CTAs of the count and scatter launches) for n splats.
 uint32_t bin_rows(uint64_t n, int num_sms);
 // (b) binning into per-tile buckets and (c) the per-tile depth sorts, over

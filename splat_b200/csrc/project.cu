@@ -344,6 +344,7 @@ constexpr uint32_t kLearnedTmemCols = 64;  // z1, then z2, then z3 (16)
 
 struct LearnedSmem {
   mlp::ForwardTiles t;
+  ViewTask vt;  // the current tile's view
   uint64_t mbar;
   uint32_t tmem;
 };
@@ -352,14 +353,18 @@ struct LearnedSmem {
 constexpr size_t kLearnedSmem = sizeof(LearnedSmem);
 static_assert((228 * 1024) / (kLearnedSmem + 1024) * kLearnedTmemCols <= 512, "TMEM oversubscribed");
 
-__global__ void __launch_bounds__(kLearnedThreads, 7) k_project_learned(ViewTask t, ViewTask* __restrict__ table,
-                                                                     float* __restrict__ dbg_proj,
-                                                                     float* __restrict__ dbg_color, FrameCounters fc) {
+// BATCH = false: one view, `t0`; CTA 0 also stores it as the view table's
+// only entry. BATCH = true: the learned views of a batch, `table` holding
+// n_views of them with proj_cta0 = the view's first tile in this launch's
+// tile space (total_tiles tiles) and pad[0] = its index in the batch.
+template <bool BATCH>
+__global__ void __launch_bounds__(kLearnedThreads, 7)
+    k_project_learned(ViewTask t0, ViewTask* __restrict__ table, uint32_t n_views, uint64_t total_tiles,
+                      float* __restrict__ dbg_proj, float* __restrict__ dbg_color, FrameCounters fc) {
   extern __shared__ __align__(128) uint8_t smem_raw[];
   LearnedSmem& S = *reinterpret_cast<LearnedSmem*>(smem_raw);
   const uint32_t tid = threadIdx.x;
-  if (blockIdx.x == 0 && tid == 0) *table = t;
-  mlp::load_forward_weights(S.t, t.s.mlp16);
+  if (!BATCH && blockIdx.x == 0 && tid == 0) *table = t0;
   if (tid == 0) umma::mbar_init(umma::smem_u32(&S.mbar), 1);
   if (tid < 32) umma::tmem_alloc(&S.tmem, kLearnedTmemCols);
   umma::fence_before_sync();
@@ -379,10 +384,27 @@ __global__ void __launch_bounds__(kLearnedThreads, 7) k_project_learned(ViewTask
     umma::fence_before_sync();
     return __syncthreads_or(timed_out) != 0;
   };
-  const uint64_t n = t.s.n;
-  const uint64_t tiles = (n + mlp::kRows - 1) / mlp::kRows;
+  const uint64_t tiles = BATCH ? total_tiles : (t0.s.n + mlp::kRows - 1) / mlp::kRows;
+  uint32_t cur = 0xFFFFFFFFu;              // view staged in S.vt
+  const uint16_t* weights = nullptr;       // parameters staged in S.t
   for (uint64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
-    const uint64_t i = tile * mlp::kRows + tid;
+    const uint32_t v = BATCH ? find_view(table, n_views, (uint32_t)tile, offsetof(ViewTask, proj_cta0)) : 0u;
+    if (v != cur) {  // uniform over the CTA
+      static_assert(sizeof(ViewTask) % 16 == 0, "ViewTask copies as uint4");
+      __syncthreads();
+      if (tid < sizeof(ViewTask) / 16)
+        reinterpret_cast<uint4*>(&S.vt)[tid] =
+            BATCH ? __ldg(reinterpret_cast<const uint4*>(table + v) + tid) : reinterpret_cast<const uint4*>(&t0)[tid];
+      __syncthreads();
+      cur = v;
+      if (S.vt.s.mlp16 != weights) {
+        weights = S.vt.s.mlp16;
+        mlp::load_forward_weights(S.t, weights);  // the previous tile's MMAs are complete
+      }
+    }
+    const ViewTask& t = S.vt;
+    const uint64_t n = t.s.n;
+    const uint64_t i = (tile - (BATCH ? t.proj_cta0 : 0u)) * mlp::kRows + tid;
     bool vis = false, used_fp64 = false;
     float dir[3] = {0.f, 0.f, 0.f};
     uint4 l0 = make_uint4(0, 0, 0, 0), l1 = l0;
@@ -425,9 +447,9 @@ __global__ void __launch_bounds__(kLearnedThreads, 7) k_project_learned(ViewTask
       r[7] = rgb[1];
       r[8] = rgb[2];
     }
-    if (dbg_color && i < n)
+    if (!BATCH && dbg_color && i < n)
       for (int c = 0; c < 3; c++) dbg_color[3 * i + c] = vis ? rgb[c] : 0.0f;
-    count_visible(vis, used_fp64, fc, 0);
+    count_visible(vis, used_fp64, fc, BATCH ? t.pad[0] : 0u);
     umma::fence_before_sync();
   }
   if (!aborted && __syncthreads_or(timed_out)) aborted = true;
@@ -443,22 +465,24 @@ __global__ void __launch_bounds__(kLearnedThreads, 7) k_project_learned(ViewTask
   }
 }
 
+int learned_ctas_per_sm_times_sms() {
+  static int sms[64] = {0};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  int& ns = sms[dev & 63];
+  if (!ns && cudaDeviceGetAttribute(&ns, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) ns = 148;
+  return 7 * ns;
+}
+
 }  // namespace
 
 cudaError_t launch_project(const ViewTask& t, ViewTask* table, float* dbg_proj, float* dbg_color,
                            const FrameCounters& fc, cudaStream_t stream, uint32_t* launches) {
   if (t.s.learned) {
-    static int sms[64] = {0};
-    int dev = 0;
-    cudaGetDevice(&dev);
-    int& ns = sms[dev & 63];
-    if (!ns) {
-      cudaError_t e = cudaDeviceGetAttribute(&ns, cudaDevAttrMultiProcessorCount, dev);
-      if (e != cudaSuccess) return e;
-    }
     const uint64_t tiles = (t.s.n + mlp::kRows - 1) / mlp::kRows;
-    const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(tiles, 7ull * ns));
-    k_project_learned<<<grid, kLearnedThreads, kLearnedSmem, stream>>>(t, table, dbg_proj, dbg_color, fc);
+    const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(tiles, learned_ctas_per_sm_times_sms()));
+    k_project_learned<false>
+        <<<grid, kLearnedThreads, kLearnedSmem, stream>>>(t, table, 1u, 0ull, dbg_proj, dbg_color, fc);
     *launches += 1;
     return cudaGetLastError();
   }
@@ -478,6 +502,17 @@ cudaError_t launch_project(const ViewTask& t, ViewTask* table, float* dbg_proj, 
     default: SPLAT_PROJECT(3); break;
   }
 #undef SPLAT_PROJECT
+  *launches += 1;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_project_learned_batch(ViewTask* table, uint32_t n_views, uint64_t total_tiles,
+                                         const FrameCounters& fc, cudaStream_t stream, uint32_t* launches) {
+  if (n_views == 0 || total_tiles == 0) return cudaSuccess;
+  const unsigned grid =
+      (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(total_tiles, learned_ctas_per_sm_times_sms()));
+  k_project_learned<true><<<grid, kLearnedThreads, kLearnedSmem, stream>>>(ViewTask{}, table, n_views, total_tiles,
+                                                                            nullptr, nullptr, fc);
   *launches += 1;
   return cudaGetLastError();
 }

@@ -227,18 +227,55 @@ def test_learned_colour_gains_over_base_colour(cuda_lib, oracle):
         x.close()
 
 
-def test_learned_scene_is_refused_by_batches(cuda_lib):
-    import ctypes
-
+def test_learned_views_in_batches(cuda_lib):
+    """Learned-colour scenes in a batch beside SH scenes (FP32 and FP16): each
+    view's image equals the single-view path's, with the same counts, over
+    replays and blend configurations."""
+    from splat_b200 import Frame, OrbitCamera, UpAxis
     from splat_b200 import _native as N
+    from splat_b200.batch import BatchRenderer, BatchView
     from splat_b200.learned import learned_renderer
+    from splat_b200.render import CudaRenderer
 
-    scene = small_scene(n=100)
-    lr = learned_renderer(scene.to_fp16(), np.zeros((100, 16), np.uint16), np.zeros(M.PARAMS, np.uint16))
-    views = (N.BatchViewC * 1)()
-    views[0].scene, views[0].width, views[0].height, views[0].dev_out = 0, 64, 64, 1
-    h = ctypes.c_void_p()
-    scenes = (ctypes.c_void_p * 1)(lr._h.value)
-    rc = cuda_lib.splat_cuda_batch_create(scenes, 1, views, 1, ctypes.byref(h))
-    assert rc == N.SPLAT_ERR_UNSUPPORTED
-    lr.close()
+    rng = np.random.default_rng(4)
+    sa = small_scene(n=6000, seed=21)
+    sb = small_scene(n=3000, seed=22, degree=1)
+    la = learned_renderer(sa.to_fp16(), rng.normal(0, 0.6, (6000, 16)).astype(np.float16).view(np.uint16),
+                          he_params(rng).astype(np.float16).view(np.uint16))
+    lb = learned_renderer(sb.to_fp16(), rng.normal(0, 0.6, (3000, 16)).astype(np.float16).view(np.uint16),
+                          he_params(rng).astype(np.float16).view(np.uint16))
+    sh = CudaRenderer(small_scene(n=5000, seed=23))
+    half = CudaRenderer(small_scene(n=4000, seed=24, degree=2).to_fp16())
+    rends = [la, sh, lb, half]
+    views = []
+    for i in range(9):
+        sc = i % 4
+        cam = OrbitCamera.new(np.zeros(3, np.float32), np.float32(6.0), UpAxis.NEG_Y)
+        cam.rotate(0.7 * i, 0.1 * (i % 3))
+        cam.zoom(1.0 + 0.2 * (i % 2))
+        w, h = [(160, 96), (333, 190), (64, 48), (320, 192)][i % 4]
+        views.append(BatchView(sc, cam.view(), w, h, (0.1, 0.0, 0.2)))
+    want, want_st = [], []
+    for v in views:
+        f = Frame()
+        want_st.append(rends[v.scene].render(v.view, v.width, v.height, v.background, f))
+        want.append(f.pixels.copy())
+    b = BatchRenderer(rends, views)
+    for rep in range(2):
+        stats, _ = b.render()
+        got = b.frames()
+        for i in range(len(views)):
+            assert np.array_equal(got[i], want[i]), f"view {i}: {np.sum(got[i] != want[i])} channels differ"
+            assert stats[i].visible == want_st[i].visible and stats[i].overlaps == want_st[i].overlaps, i
+        b.frames_dev.zero_()
+    n0 = b.get_option(N.SPLAT_OPT_KERNEL_LAUNCHES)
+    b.render()
+    assert b.get_option(N.SPLAT_OPT_KERNEL_LAUNCHES) - n0 == 10  # 9 + the learned-colour projection
+    b.set_config(8, 8, 256)
+    b.render()
+    got = b.frames()
+    for i in range(len(views)):
+        assert np.array_equal(got[i], want[i]), f"8x8 view {i}"
+    b.close()
+    for r in rends:
+        r.close()
