@@ -44,6 +44,8 @@ namespace splat {
 namespace {
 
 constexpr float kLog2e = 1.44269504088896340736f;
+constexpr float kLog2AlphaMin = -7.99435343685886f;  // log2(1/255)
+constexpr float kLog2AlphaMax = -0.0144995696951f;   // log2(0.99)
 
 // src/render/simd.rs:315-331 with the portable F4's unfused mul_add.
 __device__ __forceinline__ float exp_neg_exact(float xin) {
@@ -79,10 +81,23 @@ __device__ __forceinline__ uint32_t to_u8(float v) {
 }
 
 
+// Default path staging: the splat's centre in tile pixel coordinates (xs,
+// ys; exact differences, the same whatever the tile shape), its conic times
+// log2 e (A, B, C: power = A dx^2 + B dx dy + C dy^2 in log2 units), lop =
+// log2 opacity and cap = min(lop, log2 0.99). Then pw' = power + lop and
+// alpha = 2^min(pw', cap) is min(opacity exp(power), 0.99) with power <= 0
+// enforced, and the alpha test is pw' >= log2(1/255).
+// a = (xs, ys, A, B), b = (C, lop, cap, red), c = (green, blue).
+__device__ __forceinline__ void stage_splat(const Record& r, float ox05, float oy05, float4& a, float4& b, float2& c) {
+  const float lop = __log2f(r.r1.y);
+  a = make_float4(r.r0.x - ox05, r.r0.y - oy05, r.r0.z * kLog2e, r.r0.w * kLog2e);
+  b = make_float4(r.r1.x * kLog2e, lop, fminf(lop, kLog2AlphaMax), r.r1.z);
+  c = make_float2(r.r1.w, r.r2.x);
+}
+
 template <bool EXACT>
 __device__ __forceinline__ float splat_alpha(bool inbox, const float4& a, const float4& b, float fx05, float gbase,
                                              float lanef, float rowc, float lxf, float lyf) {
-  float pw, alpha;
   if (EXACT) {
     const float cx0 = __fsub_rn(fx05, a.x);
     const float dx = __fadd_rn(lanef, __fadd_rn(gbase, cx0));
@@ -90,38 +105,54 @@ __device__ __forceinline__ float splat_alpha(bool inbox, const float4& a, const 
     const float dy = __fsub_rn(rowc, a.y);
     const float qy = __fmul_rn(__fmul_rn(b.x, dy), dy);
     const float bdy = __fmul_rn(a.w, dy);
-    pw = __fadd_rn(__fadd_rn(qx, qy), __fmul_rn(bdy, dx));
-    alpha = fminf(__fmul_rn(exp_neg_exact(pw), b.y), kAlphaMax);
+    const float pw = __fadd_rn(__fadd_rn(qx, qy), __fmul_rn(bdy, dx));
+    const float alpha = fminf(__fmul_rn(exp_neg_exact(pw), b.y), kAlphaMax);
+    const bool on = (pw <= 0.0f) && (alpha >= kAlphaMin) && inbox;
+    return on ? alpha : 0.0f;
   } else {
+    // A pixel outside the splat's bbox is at least half a pixel beyond the
+    // ellipse on which opacity * exp(power) = 1/255 (the bbox is the k-sigma
+    // extent rounded outwards and pixels are sampled at their centres), so
+    // the alpha test alone excludes it here; the exact path also tests the
+    // bbox, as the reference does.
     const float dx = lxf - a.x;
     const float dy = lyf - a.y;
-    pw = fmaf(dx, fmaf(a.z, dx, a.w * dy), (b.x * dy) * dy);
-    alpha = fminf(ex2_approx(pw) * b.y, kAlphaMax);
+    const float pw = fminf(fmaf(dx, fmaf(a.z, dx, a.w * dy), fmaf(b.x * dy, dy, b.y)), b.z);
+    return pw >= kLog2AlphaMin ? ex2_approx(pw) : 0.0f;
   }
-  // A pixel outside the splat's bbox is at least half a pixel beyond the
-  // ellipse on which opacity * exp(power) = 1/255 (the bbox is the k-sigma
-  // extent rounded outwards and pixels are sampled at their centres), so the
-  // alpha test alone excludes it in the default path; the exact path also
-  // tests the bbox, as the reference does.
-  const bool on = (pw <= 0.0f) && (alpha >= kAlphaMin) && (!EXACT || inbox);
-  return on ? alpha : 0.0f;
 }
 
+// C += colour * alpha * T, T *= 1 - alpha.
 template <bool EXACT>
-__device__ __forceinline__ void accumulate(float alpha, const float4& b, float blue, float& T, float& cr, float& cg,
-                                           float& cb) {
+__device__ __forceinline__ void accumulate(float alpha, float red, float green, float blue, float& T, float& cr,
+                                           float& cg, float& cb) {
   if (EXACT) {
     const float w = __fmul_rn(alpha, T);
-    cr = __fadd_rn(cr, __fmul_rn(b.z, w));
-    cg = __fadd_rn(cg, __fmul_rn(b.w, w));
+    cr = __fadd_rn(cr, __fmul_rn(red, w));
+    cg = __fadd_rn(cg, __fmul_rn(green, w));
     cb = __fadd_rn(cb, __fmul_rn(blue, w));
     T = __fmul_rn(T, __fsub_rn(1.0f, alpha));
   } else {
     const float w = alpha * T;
-    cr = fmaf(b.z, w, cr);
-    cg = fmaf(b.w, w, cg);
+    cr = fmaf(red, w, cr);
+    cg = fmaf(green, w, cg);
     cb = fmaf(blue, w, cb);
     T = T - w;
+  }
+}
+// The staged colour: exact path (red, green) in b.zw and blue in c.x; default
+// path red in b.w, (green, blue) in c (stage_splat).
+template <bool EXACT>
+__device__ __forceinline__ void staged_colour(const float4& b, const float2& c, float& red, float& green,
+                                              float& blue) {
+  if (EXACT) {
+    red = b.z;
+    green = b.w;
+    blue = c.x;
+  } else {
+    red = b.w;
+    green = c.x;
+    blue = c.y;
   }
 }
 
@@ -168,7 +199,7 @@ struct __align__(16) GroupSmem {
   using S = BlendShape<TW, TH, NT>;
   float4 a[S::G];  // x, y, -a/2, -b
   float4 b[S::G];  // -c/2, opacity, red, green
-  float c[S::G];   // blue
+  float2 c[S::G];  // see staged_colour
   uint32_t mx[S::G];
   uint32_t my[S::G];
   uint16_t list[S::GW][S::G];
@@ -228,7 +259,6 @@ __global__ void __launch_bounds__(NT) k_blend(const ViewTask* __restrict__ table
     // (src/render/cpu.rs:658-671).
     const float fx05 = __fadd_rn((float)(px & ~15u), 0.5f);
     const float gbase = (float)(px & 12u), lanef = (float)(px & 3u);
-    const float lxf = (float)lx;
     const float ox05 = (float)ox + 0.5f, oy05 = (float)oy + 0.5f;
 
     float T[PPT], cr[PPT], cg[PPT], cb[PPT];
@@ -257,17 +287,18 @@ __global__ void __launch_bounds__(NT) k_blend(const ViewTask* __restrict__ table
         const int y0 = min(max((int)(by & 0xFFFFu) - (int)oy, 0), TH), y1 = min(max((int)(by >> 16) - (int)oy, 0), TH);
         sm.mx[gt] = x1 > x0 ? bit_range(x0, x1) : 0u;
         sm.my[gt] = y1 > y0 ? bit_range(y0, y1) : 0u;
-        float4 a = nr.r0, b = nr.r1;
-        if (!EXACT) {
-          a.x -= ox05;
-          a.y -= oy05;
-          a.z *= kLog2e;
-          a.w *= kLog2e;
-          b.x *= kLog2e;
+        if (EXACT) {
+          sm.a[gt] = nr.r0;
+          sm.b[gt] = nr.r1;
+          sm.c[gt] = make_float2(nr.r2.x, 0.0f);
+        } else {
+          float4 a, b;
+          float2 c;
+          stage_splat(nr, ox05, oy05, a, b, c);
+          sm.a[gt] = a;
+          sm.b[gt] = b;
+          sm.c[gt] = c;
         }
-        sm.a[gt] = a;
-        sm.b[gt] = b;
-        sm.c[gt] = nr.r2.x;
       }
       sync();
       const uint32_t nxt = start + G + gt;
@@ -290,7 +321,7 @@ __global__ void __launch_bounds__(NT) k_blend(const ViewTask* __restrict__ table
         if constexpr (PPT == 1) {
           // Two splats per iteration: the second one's alpha is computed
           // while the first one is accumulated.
-          const float rowc = (float)(oy + ly0) + 0.5f, lyf = (float)ly0;
+          const float rowc = (float)(oy + ly0) + 0.5f, lxf = (float)lx, lyf = (float)ly0;
           const uint32_t ybit = 1u << ly0, xbit = 1u << lx;
           uint32_t k = 0;
           for (; k + 1 < len; k += 2) {
@@ -302,14 +333,18 @@ __global__ void __launch_bounds__(NT) k_blend(const ViewTask* __restrict__ table
             const float al0 = splat_alpha<EXACT>(in0, a0, b0, fx05, gbase, lanef, rowc, lxf, lyf);
             const float al1 = splat_alpha<EXACT>(in1, a1, b1, fx05, gbase, lanef, rowc, lxf, lyf);
             if (al0 > 0.0f) {
-              accumulate<EXACT>(al0, b0, sm.c[j0], T[0], cr[0], cg[0], cb[0]);
+              float r_, g_, b_;
+              staged_colour<EXACT>(b0, sm.c[j0], r_, g_, b_);
+              accumulate<EXACT>(al0, r_, g_, b_, T[0], cr[0], cg[0], cb[0]);
               if (T[0] < kTMin) {
                 done[0] = true;
                 break;
               }
             }
             if (al1 > 0.0f) {
-              accumulate<EXACT>(al1, b1, sm.c[j1], T[0], cr[0], cg[0], cb[0]);
+              float r_, g_, b_;
+              staged_colour<EXACT>(b1, sm.c[j1], r_, g_, b_);
+              accumulate<EXACT>(al1, r_, g_, b_, T[0], cr[0], cg[0], cb[0]);
               if (T[0] < kTMin) {
                 done[0] = true;
                 break;
@@ -322,7 +357,9 @@ __global__ void __launch_bounds__(NT) k_blend(const ViewTask* __restrict__ table
             const bool in0 = !EXACT || ((sm.mx[j0] & xbit) && (sm.my[j0] & ybit));
             const float al0 = splat_alpha<EXACT>(in0, a0, b0, fx05, gbase, lanef, rowc, lxf, lyf);
             if (al0 > 0.0f) {
-              accumulate<EXACT>(al0, b0, sm.c[j0], T[0], cr[0], cg[0], cb[0]);
+              float r_, g_, b_;
+              staged_colour<EXACT>(b0, sm.c[j0], r_, g_, b_);
+              accumulate<EXACT>(al0, r_, g_, b_, T[0], cr[0], cg[0], cb[0]);
               if (T[0] < kTMin) done[0] = true;
             }
           }
@@ -333,17 +370,18 @@ __global__ void __launch_bounds__(NT) k_blend(const ViewTask* __restrict__ table
             const uint32_t j = sm.list[gw][k];
             const float4 a = sm.a[j], b = sm.b[j];
             const uint32_t mx = sm.mx[j], my = sm.my[j];
-            const float blue = sm.c[j];
+            float red, green, blue;
+            staged_colour<EXACT>(b, sm.c[j], red, green, blue);
             all_done = true;
 #pragma unroll
             for (int q = 0; q < PPT; q++) {
               if (!done[q]) {
                 const uint32_t ly = ly0 + q;
                 const bool in = !EXACT || ((mx & xbit) && ((my >> ly) & 1u));
-                const float al = splat_alpha<EXACT>(in, a, b, fx05, gbase, lanef, (float)(oy + ly) + 0.5f, lxf,
-                                                    (float)ly);
+                const float al = splat_alpha<EXACT>(in, a, b, fx05, gbase, lanef, (float)(oy + ly) + 0.5f,
+                                                    (float)lx, (float)ly);
                 if (al > 0.0f) {
-                  accumulate<EXACT>(al, b, blue, T[q], cr[q], cg[q], cb[q]);
+                  accumulate<EXACT>(al, red, green, blue, T[q], cr[q], cg[q], cb[q]);
                   if (T[q] < kTMin) done[q] = true;
                 }
               }
