@@ -186,7 +186,7 @@ void* splat_cuda_get_stream(splat_cuda_handle* h);
 #define SPLAT_OPT_BLEND_CONFIG 7u  /* tile shape and blend threads, packed as
                                       tile_w | tile_h << 8 | threads << 16;
                                       shapes 8x8, 16x16 (default), 32x16 and
-                                      128, 256 (default) or 512 threads. The
+                                      128, 256 or 512 (default) threads. The
                                       image does not depend on it; the keys of
                                       splat_cuda_debug_dump use its tiles. */
 int splat_cuda_set_option(splat_cuda_handle* h, uint32_t option, uint64_t value);
@@ -268,7 +268,7 @@ typedef struct splat_tune_result {
   double ms;            /* mean device time of one batch (graph launch) */
 } splat_tune_result;
 
-/* Plans the batch with the default configuration (16x16 tiles, 256
+/* Plans the batch with the default configuration (16x16 tiles, 512
  * threads), runs it once to size the pair buffers and records the graph. */
 int splat_cuda_batch_create(splat_cuda_handle* const* scenes, uint32_t n_scenes, const splat_batch_view* views,
                             uint32_t n_views, splat_cuda_batch** out);

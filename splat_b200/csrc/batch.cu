@@ -35,7 +35,7 @@ struct splat_cuda_batch {
   size_t max_smem = 48 * 1024;
   std::vector<splat_cuda_handle*> scenes;
   std::vector<splat_batch_view> views;
-  BlendConfig cfg{kTile, kTile, 256};
+  BlendConfig cfg{kTile, kTile, 512};
   bool exact = false;
   uint32_t launches = 0;
   cudaStream_t own_stream = nullptr;

@@ -95,6 +95,15 @@ __device__ __forceinline__ void stage_splat(const Record& r, float ox05, float o
   c = make_float2(r.r1.w, r.r2.x);
 }
 
+// Default path alpha from the staged splat (stage_splat) at a pixel offset
+// (dx, dy), adx = A dx: pw' = dx (B dy + A dx) + (C dy dy + lop), clamped;
+// 0 when below the alpha threshold. Every blend shape evaluates this same
+// expression, so images do not depend on the shape.
+__device__ __forceinline__ float fast_alpha(const float4& a, const float4& b, float dx, float adx, float dy) {
+  const float pw = fminf(fmaf(dx, fmaf(a.w, dy, adx), fmaf(b.x * dy, dy, b.y)), b.z);
+  return pw >= kLog2AlphaMin ? ex2_approx(pw) : 0.0f;
+}
+
 template <bool EXACT>
 __device__ __forceinline__ float splat_alpha(bool inbox, const float4& a, const float4& b, float fx05, float gbase,
                                              float lanef, float rowc, float lxf, float lyf) {
@@ -117,8 +126,7 @@ __device__ __forceinline__ float splat_alpha(bool inbox, const float4& a, const 
     // bbox, as the reference does.
     const float dx = lxf - a.x;
     const float dy = lyf - a.y;
-    const float pw = fminf(fmaf(dx, fmaf(a.z, dx, a.w * dy), fmaf(b.x * dy, dy, b.y)), b.z);
-    return pw >= kLog2AlphaMin ? ex2_approx(pw) : 0.0f;
+    return fast_alpha(a, b, dx, a.z * dx, dy);
   }
 }
 

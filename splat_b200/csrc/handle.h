@@ -51,7 +51,7 @@ struct splat_cuda_handle {
   splat::DevState* st_host = nullptr;  // pinned copy of splat::DevState + the view's counters
   uint32_t chunks_cap = 0;      // tile-scan chunks the counters hold
   splat::ViewTask* table = nullptr;    // the view table (one entry)
-  splat::BlendConfig blend{splat::kTile, splat::kTile, 256};
+  splat::BlendConfig blend{splat::kTile, splat::kTile, 512};  // two 16x16 tile groups per CTA
   uint8_t* stage = nullptr;     // pinned staging for pageable outputs
   size_t stage_cap = 0;
   // debug capture
