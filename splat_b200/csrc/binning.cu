@@ -279,10 +279,13 @@ __global__ void __launch_bounds__(256, 3) k_sort_small(const uint2* __restrict__
   warp_sort_tile(pairs + r.x, n, s_scratch[warp], s_counts[warp]);
 }
 
-// Tiles of (kWarpSortCap, kMidSortCap] pairs: one CTA per tile, in shared memory.
+// Tiles of (kWarpSortCap, kMidSortCap] pairs: one CTA per tile, in shared
+// memory (smem_count_sort).
 struct MidSmem {
   uint64_t words[kMidSortCap];
-  uint32_t key[2][kMidSortCap];
+  uint32_t hist[kCountBuckets];
+  uint16_t slot[kMidSortCap];
+  uint16_t qv[kMidSortCap];
   TileSortSmem t;
 };
 
@@ -291,14 +294,37 @@ __global__ void __launch_bounds__(kTileThreads) k_sort_mid(const uint2* __restri
                                                            uint64_t* __restrict__ pairs, const DevState* st) {
   extern __shared__ __align__(16) unsigned char s_raw[];
   MidSmem& sm = *reinterpret_cast<MidSmem*>(s_raw);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const uint32_t nmid = *(const volatile uint32_t*)&st->mid_tiles;
   for (uint32_t li = blockIdx.x; li < nmid; li += gridDim.x) {
     const uint2 r = ranges[mid_list[li]];
     const uint32_t n = r.y - r.x;
-    for (uint32_t e = threadIdx.x; e < n; e += kTileThreads) sm.words[e] = pairs[r.x + e];
+    uint32_t mn = 0xFFFFFFFFu, mx = 0u;
+    for (uint32_t e = tid; e < n; e += kTileThreads) {
+      const uint64_t w = pairs[r.x + e];
+      sm.words[e] = w;
+      mn = min(mn, (uint32_t)(w >> 32));
+      mx = max(mx, (uint32_t)(w >> 32));
+    }
+    for (uint32_t b = tid; b < kCountBuckets; b += kTileThreads) sm.hist[b] = 0u;
+    // block min / max of the depth bits (positive floats order like their bits)
+#pragma unroll
+    for (int s2 = 16; s2 > 0; s2 >>= 1) {
+      mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, s2));
+      mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, s2));
+    }
+    if (lane == 0) {
+      sm.t.red[0][warp] = mn;
+      sm.t.red[1][warp] = mx;
+    }
     __syncthreads();
-    const int fin = smem_sort<kMidSortCap>(sm.key, sm.words, n, sm.t);
-    for (uint32_t e = threadIdx.x; e < n; e += kTileThreads) pairs[r.x + e] = sm.words[sm.key[fin][e] & 0xFFFFu];
+#pragma unroll
+    for (int w = 0; w < kTileWarps; w++) {
+      mn = min(mn, sm.t.red[0][w]);
+      mx = max(mx, sm.t.red[1][w]);
+    }
+    smem_count_sort(sm.words, n, mn, mx, sm.hist, sm.slot, sm.qv, sm.t);
+    for (uint32_t e = tid; e < n; e += kTileThreads) pairs[r.x + e] = sm.words[sm.slot[e]];
     __syncthreads();
   }
 }

@@ -242,6 +242,75 @@ __device__ int smem_sort(uint32_t (*key)[kCap], const uint64_t* words, uint32_t 
   return cur;
 }
 
+// CTA sort of one tile's n <= kCap words (already in shared memory, their
+// depth-bit range [mn, mx] known): one counting pass on the depth quantised
+// to 12 bits over that range, q = min(4095, (d - dmin) * 4095 / (dmax -
+// dmin)) (monotone, as DepthQuant), positions handed out by shared-memory
+// atomics, then every run of equal q ordered by the full word. The order the
+// atomics produce within a run does not matter, so the result is exactly the
+// (depth, scene index) order. slot[i] receives the index into words[] of the
+// i-th word of the order; hist holds 4096 counters, qv n quantised depths.
+constexpr int kCountBits = 12;
+constexpr uint32_t kCountBuckets = 1u << kCountBits;
+
+__device__ __forceinline__ void smem_count_sort(const uint64_t* words, uint32_t n, uint32_t mn, uint32_t mx,
+                                                uint32_t* hist, uint16_t* slot, uint16_t* qv, TileSortSmem& sm) {
+  static_assert(kCountBuckets == 16 * kTileThreads, "16 counters per thread");
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const float dmin = __uint_as_float(mn), range = __uint_as_float(mx) - dmin;
+  const float scale = range > 0.0f ? (float)(kCountBuckets - 1) / range : 0.0f;
+  // hist was zeroed by the caller before its last barrier.
+  for (uint32_t e = tid; e < n; e += kTileThreads) {
+    const float q = (__uint_as_float((uint32_t)(words[e] >> 32)) - dmin) * scale;
+    const uint32_t qi = q >= (float)(kCountBuckets - 1) ? kCountBuckets - 1 : (uint32_t)q;
+    qv[e] = (uint16_t)qi;
+    atomicAdd(&hist[qi], 1u);
+  }
+  __syncthreads();
+  // Exclusive scan of the counters, 16 per thread.
+  uint32_t c[16], sum = 0;
+  uint4* h4 = reinterpret_cast<uint4*>(hist + 16 * tid);
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const uint4 v = h4[k];
+    c[4 * k] = v.x;
+    c[4 * k + 1] = v.y;
+    c[4 * k + 2] = v.z;
+    c[4 * k + 3] = v.w;
+  }
+#pragma unroll
+  for (int k = 0; k < 16; k++) sum += c[k];
+  uint32_t x = sum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) sm.wsum[warp] = x;
+  __syncthreads();
+  uint32_t run = x - sum;
+  for (int w = 0; w < warp; w++) run += sm.wsum[w];
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    uint4 v;
+    v.x = run;
+    run += c[4 * k];
+    v.y = run;
+    run += c[4 * k + 1];
+    v.z = run;
+    run += c[4 * k + 2];
+    v.w = run;
+    run += c[4 * k + 3];
+    h4[k] = v;
+  }
+  __syncthreads();
+  for (uint32_t e = tid; e < n; e += kTileThreads) slot[atomicAdd(&hist[qv[e]], 1u)] = (uint16_t)e;
+  __syncthreads();
+  sort_runs(
+      slot, n, tid, kTileThreads, [&](uint16_t i) { return (uint32_t)qv[i]; }, [&](uint16_t i) { return words[i]; });
+  __syncthreads();
+}
+
 // Warp sort of one tile's n <= kWarpSortCap words in place in global memory.
 // The words live in registers, warp-striped (element j*32 + lane); each of
 // the two passes on the quantised depth ranks them stably with ballots,
