@@ -170,6 +170,36 @@ def make_workload(n, cfg):
     return scene, scene, scene, home, warm, timed
 
 
+def scene_load(scene, dev):
+    """The workload scene as a 3DGS PLY and as .splat records, loaded by the
+    device decoders (header parse, one host-to-device copy, decode + finalize
+    kernel, handle set-up; wall clock) beside the host path (the reader
+    restated in numpy, Scene::finalize, splat_cuda_create's upload)."""
+    import torch
+
+    from oracle import scene_io as IO
+    from splat_b200.render import CudaRenderer, from_ply_bytes, from_splat_bytes
+
+    out = {}
+    for kind, data, loader, parse in (("ply", IO.write_ply(scene), from_ply_bytes, IO.parse_ply),
+                                      ("splat", IO.write_splat(scene), from_splat_bytes, IO.parse_splat)):
+        loader(data, device=dev).close()  # warm-up
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = loader(data, device=dev)
+        t_dev = time.perf_counter() - t0
+        r.close()
+        t0 = time.perf_counter()
+        r = CudaRenderer(parse(data).finalize(), device=dev)
+        t_host = time.perf_counter() - t0
+        r.close()
+        out[kind] = {"bytes": len(data), "device_decode_ms": 1e3 * t_dev, "device_gb_per_s": len(data) / t_dev / 1e9,
+                     "host_parse_finalize_upload_ms": 1e3 * t_host}
+    out["note"] = ("create_from_ply / create_from_splat (wall clock: header parse, copy, decode kernel, buffers) "
+                   "against the reader restated in numpy + finalize + splat_cuda_create, same process")
+    return out
+
+
 def measured_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -393,6 +423,7 @@ def run_ours(args):
                 traffic = json.load(open(prof)).get(args.config, {}).get(dom)
             except Exception:
                 traffic = None
+        load = scene_load(source, dev) if cfg["precision"] == "fp32" else None
         cpu = None
         if not args.no_cpu_baseline:
             fps, cores, frames = cpu_baseline(f32_scene, timed, W, H, args.cpu_sample_s)
@@ -423,6 +454,8 @@ def run_ours(args):
         }
         if errors is not None:
             line["error_vs_fp64_naive"] = errors
+        if load is not None:
+            line["scene_load"] = load
         print(json.dumps(line), flush=True)
     r.close()
     if world > 1:

@@ -130,8 +130,30 @@ const char* splat_cuda_backend_name(void);
  * splat_cuda_create_error). */
 int splat_cuda_create(const splat_scene_desc* scene, int device, splat_cuda_handle** out);
 
-/* Text of the last splat_cuda_create failure on this thread. */
+/* Text of the last splat_cuda_create failure on this thread (also of
+ * splat_cuda_create_from_splat / _from_ply / splat_cuda_create_learned). */
 const char* splat_cuda_create_error(void);
+
+/* A renderer for a scene file's bytes (in host memory), decoded on the
+ * device: the reader and Scene::finalize run in one GPU thread per splat
+ * and write the renderer's device layout directly (precision
+ * SPLAT_PRECISION_FP32 or _FP16). The image equals that of splat_cuda_create
+ * on the host-parsed, finalized scene.
+ *   _from_splat: the 32-byte .splat records; replaces splat_format::parse
+ *                (src/splat_format.rs:18-44) + Scene::finalize
+ *                (src/scene.rs:62-94). Sizes not a multiple of 32 are
+ *                rejected with the reference's message.
+ *   _from_ply:   a 3DGS PLY (ascii, binary_little_endian or
+ *                binary_big_endian; x y z, f_dc_* or red green blue,
+ *                f_rest_*, opacity, scale_*, rot_*, each optional but x y z,
+ *                any scalar type); replaces ply::parse (src/ply.rs:218-379) +
+ *                Scene::finalize. The header is parsed on the host (ASCII
+ *                bodies are converted to f64 rows there), the records decoded
+ *                on the device. Errors follow the reference's messages. */
+int splat_cuda_create_from_splat(const void* data, size_t bytes, uint32_t precision, int device,
+                                 splat_cuda_handle** out);
+int splat_cuda_create_from_ply(const void* data, size_t bytes, uint32_t precision, int device,
+                               splat_cuda_handle** out);
 
 /* Renders `view` at width x height over background bg (linear RGB) and writes
  * the u8 RGB frame, row-major, to host memory rgb_out (Frame::pixels,
@@ -189,6 +211,7 @@ void* splat_cuda_get_stream(splat_cuda_handle* h);
                                       128, 256 or 512 (default) threads. The
                                       image does not depend on it; the keys of
                                       splat_cuda_debug_dump use its tiles. */
+#define SPLAT_OPT_SCENE_SPLATS 8u    /* read-only: gaussians in the scene */
 int splat_cuda_set_option(splat_cuda_handle* h, uint32_t option, uint64_t value);
 int splat_cuda_get_option(splat_cuda_handle* h, uint32_t option, uint64_t* value);
 

@@ -30,6 +30,7 @@ SPLAT_OPT_DEBUG_CAPTURE = 4
 SPLAT_OPT_FP64_CONICS = 5
 SPLAT_OPT_KERNEL_LAUNCHES = 6
 SPLAT_OPT_BLEND_CONFIG = 7
+SPLAT_OPT_SCENE_SPLATS = 8
 
 _STATUS_NAMES = {0: "OK", 1: "INVALID_ARG", 2: "OOM", 3: "CAPACITY", 4: "DEVICE", 5: "TIMEOUT", 6: "UNSUPPORTED"}
 
@@ -47,6 +48,7 @@ EXPORTS = [
     "splat_cuda_learner_train", "splat_cuda_learner_set_params", "splat_cuda_learner_params",
     "splat_cuda_learner_step_debug", "splat_cuda_learner_directions", "splat_cuda_learner_get_option",
     "splat_cuda_learner_last_error", "splat_cuda_learner_destroy", "splat_cuda_mlp_gradient",
+    "splat_cuda_create_from_splat", "splat_cuda_create_from_ply",
 ]
 
 # Learned colour (include/splat_cuda.h).
@@ -156,6 +158,8 @@ def lib():
         L.splat_cuda_batch_last_error.argtypes = [vp]
         L.splat_cuda_batch_last_error.restype = ctypes.c_char_p
         L.splat_cuda_batch_destroy.argtypes = [vp]
+        L.splat_cuda_create_from_splat.argtypes = [vp, ctypes.c_size_t, u32, ctypes.c_int, ctypes.POINTER(vp)]
+        L.splat_cuda_create_from_ply.argtypes = [vp, ctypes.c_size_t, u32, ctypes.c_int, ctypes.POINTER(vp)]
         L.splat_cuda_create_learned.argtypes = [ctypes.POINTER(SceneDesc), vp, vp, ctypes.c_int, ctypes.POINTER(vp)]
         L.splat_cuda_learner_create.argtypes = [vp, ctypes.POINTER(LearnConfigC), ctypes.POINTER(vp)]
         L.splat_cuda_learner_create_error.restype = ctypes.c_char_p

@@ -31,9 +31,11 @@ SOURCES = {
     "noalloc.cu": [],
     "batch.cu": [],
     "mlp.cu": [],
+    "decode.cu": ["--fmad=false"],
 }
 HEADERS = [os.path.join(CSRC, "common.cuh"), os.path.join(CSRC, "tilesort.cuh"), os.path.join(CSRC, "handle.h"),
            os.path.join(CSRC, "umma.cuh"), os.path.join(CSRC, "mlp.cuh"), os.path.join(CSRC, "sh.cuh"),
+           os.path.join(CSRC, "geom.cuh"),
            os.path.join(ROOT, "include", "splat_cuda.h")]
 
 

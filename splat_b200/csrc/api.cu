@@ -298,7 +298,12 @@ SPLAT_API const char* splat_cuda_backend_name(void) { return "cuda"; }
 
 SPLAT_API const char* splat_cuda_create_error(void) { return g_create_error.c_str(); }
 
-SPLAT_API int splat_cuda_create(const splat_scene_desc* d, int device, splat_cuda_handle** out) {
+namespace {
+
+// splat_cuda_create; with upload = false the scene's device arrays are
+// allocated but not filled (the caller fills them on the device) and the
+// desc's array pointers are not read.
+int create_impl(const splat_scene_desc* d, int device, splat_cuda_handle** out, bool upload) {
   g_create_error.clear();
   if (!out) return SPLAT_ERR_INVALID_ARG;
   *out = nullptr;
@@ -320,11 +325,12 @@ SPLAT_API int splat_cuda_create(const splat_scene_desc* d, int device, splat_cud
   }
   const uint64_t n = d->n;
   const bool f16 = d->precision == SPLAT_PRECISION_FP16;
-  if (n && !f16 && (!d->positions || !d->opacities || !d->colors || !d->cov3d || (d->sh_degree && !d->sh_rest))) {
+  if (upload && n && !f16 &&
+      (!d->positions || !d->opacities || !d->colors || !d->cov3d || (d->sh_degree && !d->sh_rest))) {
     g_create_error = "null scene array";
     return SPLAT_ERR_INVALID_ARG;
   }
-  if (n && f16 && (!d->positions || !d->scales_f16 || !d->rotations_f16 || !d->opacities_f16 || !d->sh_f16)) {
+  if (upload && n && f16 && (!d->positions || !d->scales_f16 || !d->rotations_f16 || !d->opacities_f16 || !d->sh_f16)) {
     g_create_error = "null FP16 scene array";
     return SPLAT_ERR_INVALID_ARG;
   }
@@ -361,9 +367,9 @@ SPLAT_API int splat_cuda_create(const splat_scene_desc* d, int device, splat_cud
     // rotation xyzw, opacity) as one uint4; base colour and SH as planes of n
     // halves. k is computed from the decoded opacity as in the FP32 layout.
     const uint32_t planes = d->sh_degree ? (d->sh_degree + 1) * (d->sh_degree + 1) * 3 : 3;
-    std::vector<float4> pk(n);
-    std::vector<uint4> g(n);
-    for (uint64_t i = 0; i < n; i++) {
+    std::vector<float4> pk(upload ? n : 0);
+    std::vector<uint4> g(upload ? n : 0);
+    for (uint64_t i = 0; upload && i < n; i++) {
       const float* p = d->positions + 3 * i;
       const uint16_t* sc = d->scales_f16 + 3 * i;
       const uint16_t* q = d->rotations_f16 + 4 * i;
@@ -374,12 +380,13 @@ SPLAT_API int splat_cuda_create(const splat_scene_desc* d, int device, splat_cud
       g[i] = make_uint4(sc[0] | ((uint32_t)sc[1] << 16), sc[2] | ((uint32_t)q[0] << 16), q[1] | ((uint32_t)q[2] << 16),
                         q[3] | ((uint32_t)ob << 16));
     }
-    std::vector<uint16_t> sh((size_t)planes * n);
-    for (uint64_t i = 0; i < n; i++)
+    std::vector<uint16_t> sh(upload ? (size_t)planes * n : 0);
+    for (uint64_t i = 0; upload && i < n; i++)
       for (uint32_t k = 0; k < planes; k++) sh[(size_t)k * n + i] = d->sh_f16[i * planes + k];
     auto up = [&](void** dst, const void* src, size_t bytes, const char* what) -> int {
       cudaError_t er = cudaMalloc(dst, bytes);
       if (er != cudaSuccess) return cuda_fail(h, er, what);
+      if (!upload) return SPLAT_OK;
       er = cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice);
       if (er != cudaSuccess) return cuda_fail(h, er, what);
       return SPLAT_OK;
@@ -387,7 +394,8 @@ SPLAT_API int splat_cuda_create(const splat_scene_desc* d, int device, splat_cud
     int rc;
     if ((rc = up((void**)&h->pos_k, pk.data(), n * sizeof(float4), "upload positions"))) return bail(rc);
     if ((rc = up((void**)&h->geom16, g.data(), n * sizeof(uint4), "upload FP16 geometry"))) return bail(rc);
-    if ((rc = up((void**)&h->sh16, sh.data(), sh.size() * sizeof(uint16_t), "upload FP16 SH"))) return bail(rc);
+    if ((rc = up((void**)&h->sh16, sh.data(), (size_t)planes * n * sizeof(uint16_t), "upload FP16 SH")))
+      return bail(rc);
     if ((e = cudaMalloc(&h->rec, n * sizeof(Record))) != cudaSuccess) return bail(cuda_fail(h, e, "cudaMalloc records"));
     if ((e = cudaMalloc(&h->bin, n * sizeof(BinInfo))) != cudaSuccess) return bail(cuda_fail(h, e, "cudaMalloc bins"));
   } else if (n) {
@@ -396,8 +404,8 @@ SPLAT_API int splat_cuda_create(const splat_scene_desc* d, int device, splat_cud
     // radius the reference's cpu backend also precomputes, cpu.rs:384-388),
     // colour and SH as planes of n floats for coalesced loads.
     const uint32_t rest = d->sh_degree ? (d->sh_degree + 1) * (d->sh_degree + 1) - 1 : 0;
-    std::vector<float4> a(n), b(n), c(n);
-    for (uint64_t i = 0; i < n; i++) {
+    std::vector<float4> a(upload ? n : 0), b(upload ? n : 0), c(upload ? n : 0);
+    for (uint64_t i = 0; upload && i < n; i++) {
       const float* p = d->positions + 3 * i;
       const float o = d->opacities[i];
       a[i] = make_float4(p[0], p[1], p[2], o);
@@ -406,12 +414,13 @@ SPLAT_API int splat_cuda_create(const splat_scene_desc* d, int device, splat_cud
       const float k = o < kAlphaMin ? 0.0f : std::sqrt(2.0f * std::log(o / kAlphaMin));
       c[i] = make_float4(cv[4], cv[5], k, 0.0f);
     }
-    std::vector<float> col(3 * n);
-    for (uint64_t i = 0; i < n; i++)
+    std::vector<float> col(upload ? 3 * n : 0);
+    for (uint64_t i = 0; upload && i < n; i++)
       for (int ch = 0; ch < 3; ch++) col[ch * n + i] = d->colors[3 * i + ch];
     auto up = [&](void** dst, const void* src, size_t bytes, const char* what) -> int {
       cudaError_t er = cudaMalloc(dst, bytes);
       if (er != cudaSuccess) return cuda_fail(h, er, what);
+      if (!upload) return SPLAT_OK;
       er = cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice);
       if (er != cudaSuccess) return cuda_fail(h, er, what);
       return SPLAT_OK;
@@ -422,10 +431,10 @@ SPLAT_API int splat_cuda_create(const splat_scene_desc* d, int device, splat_cud
     if ((rc = up((void**)&h->cov_b, c.data(), n * sizeof(float4), "upload covariance"))) return bail(rc);
     if ((rc = up((void**)&h->color, col.data(), 3 * n * sizeof(float), "upload colours"))) return bail(rc);
     if (rest) {
-      std::vector<float> sh((size_t)rest * 3 * n);
-      for (uint64_t i = 0; i < n; i++)
+      std::vector<float> sh(upload ? (size_t)rest * 3 * n : 0);
+      for (uint64_t i = 0; upload && i < n; i++)
         for (uint32_t k = 0; k < rest * 3; k++) sh[(size_t)k * n + i] = d->sh_rest[i * rest * 3 + k];
-      if ((rc = up((void**)&h->sh, sh.data(), sh.size() * sizeof(float), "upload SH"))) return bail(rc);
+      if ((rc = up((void**)&h->sh, sh.data(), (size_t)rest * 3 * n * sizeof(float), "upload SH"))) return bail(rc);
     }
     if ((e = cudaMalloc(&h->rec, n * sizeof(Record))) != cudaSuccess) return bail(cuda_fail(h, e, "cudaMalloc records"));
     if ((e = cudaMalloc(&h->bin, n * sizeof(BinInfo))) != cudaSuccess) return bail(cuda_fail(h, e, "cudaMalloc bins"));
@@ -436,6 +445,21 @@ SPLAT_API int splat_cuda_create(const splat_scene_desc* d, int device, splat_cud
   *out = h;
   return SPLAT_OK;
 }
+
+}  // namespace
+
+SPLAT_API int splat_cuda_create(const splat_scene_desc* d, int device, splat_cuda_handle** out) {
+  return create_impl(d, device, out, true);
+}
+
+namespace splat {
+int create_unfilled(const splat_scene_desc* d, int device, splat_cuda_handle** out, std::string* err) {
+  const int rc = create_impl(d, device, out, false);
+  if (rc && err) *err = g_create_error;
+  return rc;
+}
+void set_create_error(const std::string& msg) { g_create_error = msg; }
+}  // namespace splat
 
 SPLAT_API int splat_cuda_render_device(splat_cuda_handle* h, const splat_view_desc* view, uint32_t width,
                                        uint32_t height, const float bg[3], uint32_t downsample, uint8_t* dev_out,
@@ -554,6 +578,9 @@ SPLAT_API int splat_cuda_get_option(splat_cuda_handle* h, uint32_t option, uint6
     case SPLAT_OPT_KERNEL_LAUNCHES: *value = h->launches; return SPLAT_OK;
     case SPLAT_OPT_BLEND_CONFIG:
       *value = h->blend.tile_w | (h->blend.tile_h << 8) | ((uint64_t)h->blend.threads << 16);
+      return SPLAT_OK;
+    case SPLAT_OPT_SCENE_SPLATS:
+      *value = h->n;
       return SPLAT_OK;
     default: return fail(h, SPLAT_ERR_UNSUPPORTED, "unknown option");
   }

@@ -78,5 +78,11 @@ FrameParams make_params(const splat_view_desc& v, uint32_t w, uint32_t h, const 
 void set_tile_shape(FrameParams& p, uint32_t tile_w, uint32_t tile_h);
 // The handle's device scene as the kernels read it.
 SceneDev scene_dev(const splat_cuda_handle* h);
+// A handle for the scene shape of `d` (n, sh_degree, precision) whose scene
+// arrays are allocated on the device but not filled; d's pointers are not
+// read. On failure *err gets the reason.
+int create_unfilled(const splat_scene_desc* d, int device, splat_cuda_handle** out, std::string* err);
+// Sets the text splat_cuda_create_error reports on this thread.
+void set_create_error(const std::string& msg);
 
 }  // namespace splat

@@ -254,6 +254,54 @@ class CudaRenderer(Renderer):
             pass
 
 
+def _from_handle(h, n: int, precision: int, device: int) -> CudaRenderer:
+    r = CudaRenderer.__new__(CudaRenderer)
+    r._keep = None
+    r._h = h
+    r.n = n
+    r.device = device
+    r.precision = precision
+    return r
+
+
+def _load_bytes(fn, data: bytes, precision: int, device: int) -> CudaRenderer:
+    L = N.lib()
+    buf = np.frombuffer(data, np.uint8) if len(data) else np.zeros(1, np.uint8)
+    h = ctypes.c_void_p()
+    rc = getattr(L, fn)(buf.ctypes.data, len(data), precision, device, ctypes.byref(h))
+    if rc != N.SPLAT_OK:
+        raise N.SplatError(rc, L.splat_cuda_create_error().decode())
+    r = _from_handle(h, 0, precision, device)
+    r.n = r.get_option(N.SPLAT_OPT_SCENE_SPLATS)
+    return r
+
+
+def from_splat_bytes(data: bytes, precision: int = N.SPLAT_PRECISION_FP32, device: int = 0) -> CudaRenderer:
+    """A renderer for the bytes of a ``.splat`` file, decoded and finalized on
+    the device (``splat_format::parse`` + ``Scene::finalize``)."""
+    return _load_bytes("splat_cuda_create_from_splat", data, precision, device)
+
+
+def from_ply_bytes(data: bytes, precision: int = N.SPLAT_PRECISION_FP32, device: int = 0) -> CudaRenderer:
+    """A renderer for the bytes of a 3DGS PLY file, decoded and finalized on
+    the device (``ply::parse`` + ``Scene::finalize``)."""
+    return _load_bytes("splat_cuda_create_from_ply", data, precision, device)
+
+
+def load(path: str, precision: int = N.SPLAT_PRECISION_FP32, device: int = 0) -> CudaRenderer:
+    """``Scene::load`` (``src/scene.rs:96-110``) straight to a device scene:
+    the format is chosen by extension (``.ply`` or ``.splat``)."""
+    with open(path, "rb") as fh:
+        data = fh.read()
+    base = path.replace("\\", "/").rsplit("/", 1)[-1]
+    ext = base.rsplit(".", 1)[-1].lower() if "." in base else ""
+    if ext == "splat":
+        return from_splat_bytes(data, precision, device)
+    if ext == "ply" or data.startswith(b"ply"):
+        return from_ply_bytes(data, precision, device)
+    raise ValueError(f"unknown file type (expected .ply or .splat): {path}")
+
+
 def create(backend: Backend, scene: Scene, device: int = 0) -> Renderer:
     """``render::create`` (``mod.rs:115-121``)."""
     if backend == Backend.CUDA:
