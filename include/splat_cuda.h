@@ -179,6 +179,22 @@ int splat_cuda_render(splat_cuda_handle* h, const splat_view_desc* view, uint32_
 int splat_cuda_render_device(splat_cuda_handle* h, const splat_view_desc* view, uint32_t width, uint32_t height,
                              const float bg[3], uint32_t downsample, uint8_t* dev_out, size_t out_bytes);
 
+/* Terminal cells (the half-block widget HalfBlockImage, src/term.rs:109-130,
+ * with ColorMode::color, src/term.rs:39-72): the frame is rendered and
+ * downsampled as by splat_cuda_render, then each cell (x, y) of the
+ * floor(w/f) x floor(floor(h/f) / 2) grid gets the pixel pair (x, 2y) over
+ * (x, 2y + 1): foreground the top pixel, background the bottom one, as
+ *   SPLAT_CELLS_TRUECOLOR  6 bytes: fg r, g, b, bg r, g, b
+ *   SPLAT_CELLS_ANSI256    2 bytes: fg, bg xterm-256 indices (rgb_to_ansi256)
+ * row-major in host memory cells_out (out_bytes at least cols * rows * 6 or
+ * * 2); *cols and *rows receive the grid size (either may be NULL). A frame
+ * of odd height drops its last row, as the widget does. */
+#define SPLAT_CELLS_TRUECOLOR 0u
+#define SPLAT_CELLS_ANSI256 1u
+int splat_cuda_render_cells(splat_cuda_handle* h, const splat_view_desc* view, uint32_t width, uint32_t height,
+                            const float bg[3], uint32_t downsample, uint32_t mode, uint8_t* cells_out,
+                            size_t out_bytes, uint32_t* cols, uint32_t* rows, splat_render_stats* stats);
+
 /* Waits for the frames enqueued by splat_cuda_render_device, fills the stats
  * of the last one and reports whether it overflowed the pair buffers
  * (*regrown = 1: the buffers have been grown; enqueue the frame again). */

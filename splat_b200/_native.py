@@ -32,6 +32,9 @@ SPLAT_OPT_KERNEL_LAUNCHES = 6
 SPLAT_OPT_BLEND_CONFIG = 7
 SPLAT_OPT_SCENE_SPLATS = 8
 
+SPLAT_CELLS_TRUECOLOR = 0
+SPLAT_CELLS_ANSI256 = 1
+
 _STATUS_NAMES = {0: "OK", 1: "INVALID_ARG", 2: "OOM", 3: "CAPACITY", 4: "DEVICE", 5: "TIMEOUT", 6: "UNSUPPORTED"}
 
 # Every symbol include/splat_cuda.h declares.
@@ -48,7 +51,7 @@ EXPORTS = [
     "splat_cuda_learner_train", "splat_cuda_learner_set_params", "splat_cuda_learner_params",
     "splat_cuda_learner_step_debug", "splat_cuda_learner_directions", "splat_cuda_learner_get_option",
     "splat_cuda_learner_last_error", "splat_cuda_learner_destroy", "splat_cuda_mlp_gradient",
-    "splat_cuda_create_from_splat", "splat_cuda_create_from_ply",
+    "splat_cuda_create_from_splat", "splat_cuda_create_from_ply", "splat_cuda_render_cells",
 ]
 
 # Learned colour (include/splat_cuda.h).
@@ -158,6 +161,9 @@ def lib():
         L.splat_cuda_batch_last_error.argtypes = [vp]
         L.splat_cuda_batch_last_error.restype = ctypes.c_char_p
         L.splat_cuda_batch_destroy.argtypes = [vp]
+        L.splat_cuda_render_cells.argtypes = [vp, ctypes.POINTER(ViewDesc), u32, u32, f32p, u32, u32, vp,
+                                              ctypes.c_size_t, ctypes.POINTER(u32), ctypes.POINTER(u32),
+                                              ctypes.POINTER(RenderStatsC)]
         L.splat_cuda_create_from_splat.argtypes = [vp, ctypes.c_size_t, u32, ctypes.c_int, ctypes.POINTER(vp)]
         L.splat_cuda_create_from_ply.argtypes = [vp, ctypes.c_size_t, u32, ctypes.c_int, ctypes.POINTER(vp)]
         L.splat_cuda_create_learned.argtypes = [ctypes.POINTER(SceneDesc), vp, vp, ctypes.c_int, ctypes.POINTER(vp)]

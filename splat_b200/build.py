@@ -32,6 +32,7 @@ SOURCES = {
     "batch.cu": [],
     "mlp.cu": [],
     "decode.cu": ["--fmad=false"],
+    "term.cu": [],
 }
 HEADERS = [os.path.join(CSRC, "common.cuh"), os.path.join(CSRC, "tilesort.cuh"), os.path.join(CSRC, "handle.h"),
            os.path.join(CSRC, "umma.cuh"), os.path.join(CSRC, "mlp.cuh"), os.path.join(CSRC, "sh.cuh"),

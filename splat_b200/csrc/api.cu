@@ -519,6 +519,61 @@ SPLAT_API int splat_cuda_render(splat_cuda_handle* h, const splat_view_desc* vie
   return fail(h, SPLAT_ERR_CAPACITY, "pair buffers kept overflowing");
 }
 
+SPLAT_API int splat_cuda_render_cells(splat_cuda_handle* h, const splat_view_desc* view, uint32_t width,
+                                      uint32_t height, const float bg[3], uint32_t downsample, uint32_t mode,
+                                      uint8_t* cells_out, size_t out_bytes, uint32_t* cols, uint32_t* rows,
+                                      splat_render_stats* stats) {
+  const auto t0 = std::chrono::steady_clock::now();
+  if (stats) std::memset(stats, 0, sizeof(*stats));
+  if (!h) return SPLAT_ERR_INVALID_ARG;
+  if (mode != SPLAT_CELLS_TRUECOLOR && mode != SPLAT_CELLS_ANSI256)
+    return fail(h, SPLAT_ERR_INVALID_ARG, "unknown cell colour mode");
+  const uint32_t f = downsample ? downsample : 1;
+  const uint32_t nc = width / f, nr = (height / f) / 2;
+  const size_t need = (size_t)nc * nr * (mode == SPLAT_CELLS_TRUECOLOR ? 6 : 2);
+  if (cols) *cols = nc;
+  if (rows) *rows = nr;
+  int rc = check_frame_args(h, view, width, height, bg, downsample, (size_t)-1, h);
+  if (rc) return rc;
+  if (need && (!cells_out || out_bytes < need))
+    return fail(h, SPLAT_ERR_INVALID_ARG, "cell buffer smaller than cols * rows * bytes per cell");
+  if (width == 0 || height == 0) return SPLAT_OK;
+  CK(cudaSetDevice(h->device), "cudaSetDevice");
+  const FrameParams fp = make_params(*view, width, height, bg, f);
+  if ((rc = ensure_size(h, 0, 0, (size_t)fp.out_w * fp.out_h * 3, 0))) return rc;
+  if (need > h->cells_cap) {
+    if (h->cells_dev) cudaFree(h->cells_dev);
+    h->cells_dev = nullptr;
+    h->cells_cap = 0;
+    CK(cudaMalloc(&h->cells_dev, need), "cudaMalloc cells");
+    h->cells_cap = need;
+  }
+  const bool direct = need && is_pinned_host(cells_out);
+  if (!direct && need > h->stage_cap) {
+    if (h->stage) cudaFreeHost(h->stage);
+    h->stage = nullptr;
+    h->stage_cap = 0;
+    CK(cudaMallocHost(&h->stage, need), "cudaMallocHost staging");
+    h->stage_cap = need;
+  }
+  for (int attempt = 0; attempt < 8; attempt++) {
+    if ((rc = enqueue_frame(h, fp, h->out_dev))) return rc;
+    CK(launch_cells(h->out_dev, fp.out_w, nc, nr, mode, h->cells_dev, h->stream, &h->launches), "cells kernel");
+    if (need)
+      CK(cudaMemcpyAsync(direct ? cells_out : h->stage, h->cells_dev, need, cudaMemcpyDeviceToHost, h->stream),
+         "copy cells");
+    int regrown = 0;
+    if ((rc = finish_frame(h, stats, &regrown))) return rc;
+    if (!regrown) {
+      if (!direct && need) std::memcpy(cells_out, h->stage, need);
+      if (stats)
+        stats->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+      return SPLAT_OK;
+    }
+  }
+  return fail(h, SPLAT_ERR_CAPACITY, "pair buffers kept overflowing");
+}
+
 SPLAT_API int splat_cuda_set_stream(splat_cuda_handle* h, void* stream) {
   if (!h) return SPLAT_ERR_INVALID_ARG;
   h->stream = stream ? (cudaStream_t)stream : h->own_stream;
@@ -691,6 +746,7 @@ SPLAT_API int splat_cuda_destroy(splat_cuda_handle* h) {
   dfree(h->sh16);
   dfree(h->lat16);
   dfree(h->mlp16);
+  dfree(h->cells_dev);
   dfree(h->rec);
   dfree(h->bin);
   free_pairs(h);

@@ -4,6 +4,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "../../include/splat_cuda.h"
+
 namespace splat {
 
 // src/render/mod.rs:23-33
@@ -199,6 +201,9 @@ cudaError_t launch_binning(const ViewTask* table, const BinLaunch& bl, uint32_t*
 // (d) blend + downsample over the depth-sorted buckets of every view.
 cudaError_t launch_blend(const ViewTask* table, uint32_t n_views, uint32_t n_tiles, const uint64_t* pairs,
                          const uint2* ranges, bool exact, const BlendConfig& cfg, DevState* st, int num_sms,
+                         cudaStream_t stream, uint32_t* launches);
+// Half-block terminal cells (SPLAT_CELLS_*) of a frame of width w.
+cudaError_t launch_cells(const uint8_t* frame, uint32_t w, uint32_t cols, uint32_t rows, uint32_t mode, uint8_t* cells,
                          cudaStream_t stream, uint32_t* launches);
 // term::downsample of one view's full-resolution scratch frame.
 cudaError_t launch_downsample(const FrameParams& fp, const uint8_t* full, uint8_t* out, cudaStream_t stream,

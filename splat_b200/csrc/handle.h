@@ -46,6 +46,8 @@ struct splat_cuda_handle {
   size_t out_cap = 0;
   uint8_t* full_dev = nullptr;
   size_t full_cap = 0;
+  uint8_t* cells_dev = nullptr;  // terminal cells of the last splat_cuda_render_cells
+  size_t cells_cap = 0;
   // frame state
   splat::DevState* st = nullptr;       // the frame counters (splat::DevState first)
   splat::DevState* st_host = nullptr;  // pinned copy of splat::DevState + the view's counters

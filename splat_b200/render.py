@@ -160,6 +160,27 @@ class CudaRenderer(Renderer):
         N.check(rc, self._h, "render")
         return RenderStats.from_c(st)
 
+    def render_cells(self, view: View, width: int, height: int, background=(0.0, 0.0, 0.0), downsample: int = 1,
+                     mode: int = N.SPLAT_CELLS_TRUECOLOR, stats: bool = False):
+        """The terminal widget's cells (``HalfBlockImage``, ``term.rs:109-130``)
+        of the downsampled frame, computed on the device: a (rows, cols, 6)
+        array of fg RGB + bg RGB (truecolor) or (rows, cols, 2) of xterm-256
+        indices (ansi256)."""
+        f = max(int(downsample), 1)
+        _pixel_count(width, height)
+        cols, rows = width // f, (height // f) // 2
+        per = 6 if mode == N.SPLAT_CELLS_TRUECOLOR else 2
+        out = np.zeros((rows, cols, per), np.uint8)
+        c, r = ctypes.c_uint32(0), ctypes.c_uint32(0)
+        st = N.RenderStatsC()
+        bg = _f32(background)
+        rc = N.lib().splat_cuda_render_cells(self._h, ctypes.byref(_view_desc(view)), width, height,
+                                             bg.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), f, mode,
+                                             out.ctypes.data if out.size else None, out.nbytes, ctypes.byref(c),
+                                             ctypes.byref(r), ctypes.byref(st))
+        N.check(rc, self._h, "render_cells")
+        return (out, RenderStats.from_c(st)) if stats else out
+
     # --- device-side entry points --------------------------------------------
     def render_into(self, view: View, width: int, height: int, background, out_ptr: int, out_bytes: int,
                     downsample: int = 1) -> RenderStats:

@@ -354,3 +354,24 @@ def test_device_path_matches_host_path():
     r.render_into(v, 320, 180, (0.1, 0.1, 0.1), pinned.data_ptr(), pinned.numel())
     assert np.array_equal(pinned.numpy().reshape(180, 320, 3), host)
     r.close()
+
+
+@pytest.mark.parametrize("mode", ["truecolor", "ansi256"])
+@pytest.mark.parametrize("size,f", [((320, 192), 2), ((333, 191), 3), ((161, 95), 1)])
+def test_terminal_cells_match_widget(oracle, mode, size, f):
+    """splat_cuda_render_cells: the HalfBlockImage cells (src/term.rs:109-130)
+    of the term::downsample'd frame, truecolor and xterm-256."""
+    from oracle import term_oracle as T
+    from splat_b200 import _native as N
+
+    s = scenes.clusters(20_000, seed=11, sh_degree=2)
+    r = CudaRenderer(s)
+    v = orbit_views(s, 2)[1]
+    w, h = size
+    frame = Frame()
+    r.render(v, w, h, (0.05, 0.1, 0.2), frame, downsample=f)
+    m = N.SPLAT_CELLS_TRUECOLOR if mode == "truecolor" else N.SPLAT_CELLS_ANSI256
+    got = r.render_cells(v, w, h, (0.05, 0.1, 0.2), downsample=f, mode=m)
+    want = T.cells(frame.pixels, mode)
+    assert got.shape == want.shape and np.array_equal(got, want)
+    r.close()
