@@ -283,10 +283,9 @@ __global__ void __launch_bounds__(256, 3) k_sort_small(const uint2* __restrict__
 // memory (smem_count_sort).
 struct MidSmem {
   uint64_t words[kMidSortCap];
-  uint32_t hist[kCountBuckets];
+  uint32_t hist[kCountBuckets / 2];
   uint16_t slot[kMidSortCap];
-  uint16_t qv[kMidSortCap];
-  TileSortSmem t;
+  CountSortSmem t;
 };
 
 __global__ void __launch_bounds__(kTileThreads) k_sort_mid(const uint2* __restrict__ ranges,
@@ -306,7 +305,7 @@ __global__ void __launch_bounds__(kTileThreads) k_sort_mid(const uint2* __restri
       mn = min(mn, (uint32_t)(w >> 32));
       mx = max(mx, (uint32_t)(w >> 32));
     }
-    for (uint32_t b = tid; b < kCountBuckets; b += kTileThreads) sm.hist[b] = 0u;
+    for (uint32_t b = tid; b < kCountBuckets / 2; b += kTileThreads) sm.hist[b] = 0u;
     // block min / max of the depth bits (positive floats order like their bits)
 #pragma unroll
     for (int s2 = 16; s2 > 0; s2 >>= 1) {
@@ -323,7 +322,7 @@ __global__ void __launch_bounds__(kTileThreads) k_sort_mid(const uint2* __restri
       mn = min(mn, sm.t.red[0][w]);
       mx = max(mx, sm.t.red[1][w]);
     }
-    smem_count_sort(sm.words, n, mn, mx, sm.hist, sm.slot, sm.qv, sm.t);
+    smem_count_sort(sm.words, n, mn, mx, sm.hist, sm.slot, sm.t);
     for (uint32_t e = tid; e < n; e += kTileThreads) pairs[r.x + e] = sm.words[sm.slot[e]];
     __syncthreads();
   }

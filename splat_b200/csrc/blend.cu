@@ -216,7 +216,7 @@ struct __align__(16) GroupSmem {
 };
 
 template <bool EXACT, int TW, int TH, int NT>
-__global__ void __launch_bounds__(NT) k_blend(const ViewTask* __restrict__ table, uint32_t n_views, uint32_t n_tiles,
+__global__ void __launch_bounds__(NT, NT == 512 ? 2 : (NT == 256 ? 5 : 8)) k_blend(const ViewTask* __restrict__ table, uint32_t n_views, uint32_t n_tiles,
                                               const uint64_t* __restrict__ pairs, const uint2* __restrict__ ranges,
                                               DevState* st) {
   using S = BlendShape<TW, TH, NT>;

@@ -1,6 +1,8 @@
 // Per-tile depth sort: the reference's per-tile radix::sort_hi32 followed by
 // fix_ties (src/render/cpu.rs:208-210, radix.rs:13-57, cpu.rs:396-414), by
-// one warp (short tiles) or one CTA of kTileThreads threads.
+// one warp (short tiles: the LSD scheme below), one CTA of kTileThreads
+// threads (mid tiles: one counting pass, smem_count_sort) or one CTA over
+// chunks in global memory (long tiles, binning.cu: the LSD scheme).
 //
 // A tile's pairs arrive in arbitrary order (they are bucketed with shared-
 // memory atomics). Each pair is the word depth bits << 32 | splat index. A
@@ -168,115 +170,53 @@ __device__ __forceinline__ void clear_counts(TileSortSmem& sm) {
   for (int w = 0; w < kTileWarps; w++) sm.wh[w][threadIdx.x] = 0u;
 }
 
-// CTA sort of one tile's n <= kCap words in shared memory: key[0][e] =
-// quantised depth << 16 | e (e the word's slot in words[]); two passes on the
-// quantised depth (digits at bits 16 and 24), then runs of equal quantised
-// depth ordered by word. Returns the key buffer holding the order; its low 16
-// bits index words[].
-template <int kCap>
-__device__ int smem_sort(uint32_t (*key)[kCap], const uint64_t* words, uint32_t n, TileSortSmem& sm) {
-  static_assert(kCap <= 65536, "slots are 16-bit");
-  constexpr int kChunks = kCap / (32 * kTileWarps);
-  uint32_t a = 0xFFFFFFFFu, o = 0u, mn = 0xFFFFFFFFu, mx = 0u;
-  for (uint32_t e = threadIdx.x; e < n; e += kTileThreads) {
-    const uint32_t b = (uint32_t)(words[e] >> 32);
-    mn = min(mn, b);
-    mx = max(mx, b);
-  }
-  // block min / max of the depth bits (positive floats order like their bits)
-  {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-    for (int s2 = 16; s2 > 0; s2 >>= 1) {
-      mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, s2));
-      mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, s2));
-    }
-    if (lane == 0) {
-      sm.red[0][warp] = mn;
-      sm.red[1][warp] = mx;
-    }
-    __syncthreads();
-    mn = 0xFFFFFFFFu;
-    mx = 0u;
-#pragma unroll
-    for (int w = 0; w < kTileWarps; w++) {
-      mn = min(mn, sm.red[0][w]);
-      mx = max(mx, sm.red[1][w]);
-    }
-    __syncthreads();
-  }
-  const DepthQuant quant = make_quant(mn, mx);
-  for (uint32_t e = threadIdx.x; e < n; e += kTileThreads) {
-    const uint32_t k2 = (quant(words[e]) << 16) | e;
-    key[0][e] = k2;
-    a &= k2;
-    o |= k2;
-  }
-  uint32_t and_all, or_all;
-  block_and_or(a, o, sm, and_all, or_all);
-  const uint32_t vary = and_all ^ or_all;
-  const int warp = threadIdx.x >> 5;
-  const uint32_t seg = (n + kTileWarps - 1) / kTileWarps;
-  const uint32_t seg0 = min(n, (uint32_t)warp * seg), seg1 = min(n, seg0 + seg);
-  int cur = 0;
-  for (int d = 2; d < 4; d++) {
-    const int shift = 8 * d;
-    if (((vary >> shift) & 255u) == 0u) continue;
-    clear_counts(sm);
-    __syncthreads();
-    uint32_t k[kChunks], dr[kChunks];
-    warp_rank<kChunks>(key[cur], seg0, seg1, shift, sm, k, dr);
-    __syncthreads();
-    digit_offsets(sm);
-#pragma unroll
-    for (int c = 0; c < kChunks; c++)
-      if (dr[c] != 0xFFFFFFFFu) key[cur ^ 1][sm.dstart[dr[c] & 255u] + sm.wh[warp][dr[c] & 255u] + (dr[c] >> 8)] = k[c];
-    __syncthreads();
-    cur ^= 1;
-  }
-  // Runs of equal quantised depth, ordered by the full word: sort the slots.
-  sort_runs(
-      key[cur], n, threadIdx.x, kTileThreads, [](uint32_t k2) { return k2 >> 16; },
-      [&](uint32_t k2) { return words[k2 & 0xFFFFu]; });
-  __syncthreads();
-  return cur;
-}
-
-// CTA sort of one tile's n <= kCap words (already in shared memory, their
-// depth-bit range [mn, mx] known): one counting pass on the depth quantised
-// to 12 bits over that range, q = min(4095, (d - dmin) * 4095 / (dmax -
-// dmin)) (monotone, as DepthQuant), positions handed out by shared-memory
-// atomics, then every run of equal q ordered by the full word. The order the
-// atomics produce within a run does not matter, so the result is exactly the
-// (depth, scene index) order. slot[i] receives the index into words[] of the
-// i-th word of the order; hist holds 4096 counters, qv n quantised depths.
+// CTA sort of one tile's n <= kMidSortCap words (already in shared memory,
+// their depth-bit range [mn, mx] known): one counting pass on the depth
+// quantised to 12 bits over that range, q = min(4095, (d - dmin) * 4095 /
+// (dmax - dmin)) (monotone, as DepthQuant), positions handed out by
+// shared-memory atomics, then every run of equal q ordered by the full word.
+// The order the atomics produce within a run does not matter, so the result
+// is exactly the (depth, scene index) order. slot[i] receives the index into
+// words[] of the i-th word of the order. The 4096 counters are 16-bit, two
+// per word of hist (counts and offsets never exceed n <= 4096).
 constexpr int kCountBits = 12;
 constexpr uint32_t kCountBuckets = 1u << kCountBits;
 
+struct CountSortSmem {
+  uint32_t red[2][kTileWarps];
+  uint32_t wsum[kTileWarps];
+};
+
 __device__ __forceinline__ void smem_count_sort(const uint64_t* words, uint32_t n, uint32_t mn, uint32_t mx,
-                                                uint32_t* hist, uint16_t* slot, uint16_t* qv, TileSortSmem& sm) {
+                                                uint32_t* hist /* kCountBuckets / 2 words */, uint16_t* slot,
+                                                CountSortSmem& sm) {
   static_assert(kCountBuckets == 16 * kTileThreads, "16 counters per thread");
+  static_assert(kMidSortCap < 65536, "16-bit counters");
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const float dmin = __uint_as_float(mn), range = __uint_as_float(mx) - dmin;
   const float scale = range > 0.0f ? (float)(kCountBuckets - 1) / range : 0.0f;
+  auto quant = [&](uint64_t w) -> uint32_t {
+    const float q = (__uint_as_float((uint32_t)(w >> 32)) - dmin) * scale;
+    return q >= (float)(kCountBuckets - 1) ? kCountBuckets - 1 : (uint32_t)q;
+  };
   // hist was zeroed by the caller before its last barrier.
   for (uint32_t e = tid; e < n; e += kTileThreads) {
-    const float q = (__uint_as_float((uint32_t)(words[e] >> 32)) - dmin) * scale;
-    const uint32_t qi = q >= (float)(kCountBuckets - 1) ? kCountBuckets - 1 : (uint32_t)q;
-    qv[e] = (uint16_t)qi;
-    atomicAdd(&hist[qi], 1u);
+    const uint32_t q = quant(words[e]);
+    atomicAdd(&hist[q >> 1], 1u << (16 * (q & 1u)));
   }
   __syncthreads();
-  // Exclusive scan of the counters, 16 per thread.
+  // Exclusive scan of the counters, 16 per thread (8 words).
   uint32_t c[16], sum = 0;
-  uint4* h4 = reinterpret_cast<uint4*>(hist + 16 * tid);
+  uint4* h4 = reinterpret_cast<uint4*>(hist + 8 * tid);
 #pragma unroll
-  for (int k = 0; k < 4; k++) {
+  for (int k = 0; k < 2; k++) {
     const uint4 v = h4[k];
-    c[4 * k] = v.x;
-    c[4 * k + 1] = v.y;
-    c[4 * k + 2] = v.z;
-    c[4 * k + 3] = v.w;
+    const uint32_t w4[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      c[8 * k + 2 * j] = w4[j] & 0xFFFFu;
+      c[8 * k + 2 * j + 1] = w4[j] >> 16;
+    }
   }
 #pragma unroll
   for (int k = 0; k < 16; k++) sum += c[k];
@@ -290,24 +230,24 @@ __device__ __forceinline__ void smem_count_sort(const uint64_t* words, uint32_t 
   __syncthreads();
   uint32_t run = x - sum;
   for (int w = 0; w < warp; w++) run += sm.wsum[w];
+  uint32_t pk[8];
 #pragma unroll
-  for (int k = 0; k < 4; k++) {
-    uint4 v;
-    v.x = run;
-    run += c[4 * k];
-    v.y = run;
-    run += c[4 * k + 1];
-    v.z = run;
-    run += c[4 * k + 2];
-    v.w = run;
-    run += c[4 * k + 3];
-    h4[k] = v;
+  for (int j = 0; j < 8; j++) {
+    const uint32_t lo = run;
+    run += c[2 * j];
+    pk[j] = lo | (run << 16);
+    run += c[2 * j + 1];
+  }
+  h4[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+  h4[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+  __syncthreads();
+  for (uint32_t e = tid; e < n; e += kTileThreads) {
+    const uint32_t q = quant(words[e]), sh = 16 * (q & 1u);
+    slot[(atomicAdd(&hist[q >> 1], 1u << sh) >> sh) & 0xFFFFu] = (uint16_t)e;
   }
   __syncthreads();
-  for (uint32_t e = tid; e < n; e += kTileThreads) slot[atomicAdd(&hist[qv[e]], 1u)] = (uint16_t)e;
-  __syncthreads();
   sort_runs(
-      slot, n, tid, kTileThreads, [&](uint16_t i) { return (uint32_t)qv[i]; }, [&](uint16_t i) { return words[i]; });
+      slot, n, tid, kTileThreads, [&](uint16_t i) { return quant(words[i]); }, [&](uint16_t i) { return words[i]; });
   __syncthreads();
 }
 
