@@ -97,8 +97,7 @@ def parse():
     return a
 
 
-def dist_env():
-    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+from splat_b200.multi import dist_env, max_over_ranks, shard  # noqa: E402
 
 
 class Clocks:
@@ -309,9 +308,7 @@ def run_ours(args):
     from splat_b200.render import CudaRenderer
 
     stored, f32_scene, source, home, warm, timed = make_workload(args.splats, cfg)
-    views = timed[rank::world] if world > 1 else timed
-    if not views:
-        views = timed
+    views = shard(timed, rank, world)
     r = CudaRenderer(stored, device=dev)
     stream = torch.cuda.ExternalStream(r.stream())
     out = torch.empty(W * H * 3, dtype=torch.uint8, device=dev)
@@ -354,10 +351,8 @@ def run_ours(args):
     launches = (r.get_option(Nat.SPLAT_OPT_KERNEL_LAUNCHES) - launches0) % (1 << 32)
     assert not regrown, "pair buffers overflowed inside the timed region"
     ms = start.elapsed_time(end)
-    t = torch.tensor([ms], device=dev)
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    ms_max = float(t.item())
+    t_max = max_over_ranks(ms, dev)
+    ms_max = t_max
     frames_total = K * world
     value = frames_total / (ms_max / 1e3)
 
@@ -386,10 +381,8 @@ def run_ours(args):
     for i in range(K):
         r.render_into(views[i % len(views)], W, H, (0, 0, 0), host.data_ptr(), host.numel())
     e2e_s = time.perf_counter() - t0
-    te = torch.tensor([e2e_s], device=dev)
-    if world > 1:
-        torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
-    e2e = frames_total / float(te.item())
+    te_max = max_over_ranks(e2e_s, dev)
+    e2e = frames_total / te_max
 
     errors = None
     if rank == 0 and cfg["precision"] == "fp16" and args.error_frames > 0:
@@ -486,7 +479,7 @@ def run_learned(args):
     from splat_b200.render import CudaRenderer
 
     scene, _, _, home, warm, timed = make_workload(args.splats, cfg)
-    views = timed[rank::world] if world > 1 else timed
+    views = shard(timed, rank, world)
     exact = CudaRenderer(scene, device=dev)
 
     # Training (every rank trains its own replica: no exchange).
@@ -536,10 +529,8 @@ def run_learned(args):
         _, regrown = rr.finish()
         barrier()
         assert not regrown, "pair buffers overflowed inside the timed region"
-        t = torch.tensor([start.elapsed_time(end)], device=dev)
-        if world > 1:
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return float(t.item()), (rr.get_option(Nat.SPLAT_OPT_KERNEL_LAUNCHES) - l0) % (1 << 32)
+        t_max = max_over_ranks(start.elapsed_time(end), dev)
+        return t_max, (rr.get_option(Nat.SPLAT_OPT_KERNEL_LAUNCHES) - l0) % (1 << 32)
 
     if args.profile:  # a short command for ncu: the training above, then --steps learned frames
         for i in range(args.steps):
@@ -581,10 +572,8 @@ def run_learned(args):
     t0 = time.perf_counter()
     for i in range(K):
         r.render_into(views[i % len(views)], W, H, (0, 0, 0), host.data_ptr(), host.numel())
-    te = torch.tensor([time.perf_counter() - t0], device=dev)
-    if world > 1:
-        torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
-    e2e = K * world / float(te.item())
+    te_max = max_over_ranks(time.perf_counter() - t0, dev)
+    e2e = K * world / te_max
 
     # The batched form: the rank's orbit views as one recorded batch (one
     # graph replay draws them all), learned colour and FP16 geometry.
@@ -603,10 +592,8 @@ def run_learned(args):
     _, _, regrown = bat.finish()
     barrier()
     assert not regrown
-    tb = torch.tensor([bs.elapsed_time(be)], device=dev)
-    if world > 1:
-        torch.distributed.all_reduce(tb, op=torch.distributed.ReduceOp.MAX)
-    batched_fps = reps * len(views) * world / (float(tb.item()) / 1e3)
+    tb_max = max_over_ranks(bs.elapsed_time(be), dev)
+    batched_fps = reps * len(views) * world / (tb_max / 1e3)
     bat.close()
 
     line = None
@@ -759,7 +746,7 @@ def run_batch(args):
     from splat_b200.render import CudaRenderer
 
     scenes, views_all = batch_workload(args)
-    views = views_all[rank::world] if world > 1 else views_all
+    views = shard(views_all, rank, world)
     rends = [CudaRenderer(s, device=dev) for s in scenes]
     stream = torch.cuda.Stream(device=dev)
     for r in rends:
@@ -824,10 +811,8 @@ def run_batch(args):
     launches = (b.get_option(Nat.SPLAT_OPT_KERNEL_LAUNCHES) - launches0) % (1 << 32)
     assert not regrown, "pair buffers overflowed inside the timed region"
     ms = start.elapsed_time(end)
-    t = torch.tensor([ms], device=dev)
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    ms_max = float(t.item())
+    t_max = max_over_ranks(ms, dev)
+    ms_max = t_max
     views_total = len(views_all) if world > 1 else len(views)
     value = views_total * K / (ms_max / 1e3)
     stats, _ = b.render()  # stage times of one batch
@@ -843,10 +828,8 @@ def run_batch(args):
             host.copy_(b.frames_dev, non_blocking=True)
         b.finish()
     e2e_s = time.perf_counter() - t0
-    te = torch.tensor([e2e_s], device=dev)
-    if world > 1:
-        torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
-    e2e = views_total * K / float(te.item())
+    te_max = max_over_ranks(e2e_s, dev)
+    e2e = views_total * K / te_max
 
     if rank == 0:
         peak, peak_kind = measured_peaks()
