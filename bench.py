@@ -229,6 +229,23 @@ def cpu_baseline(scene, views, w, h, sample_s, threads=0):
     return len(times) / sum(times), threads_used, len(times)
 
 
+def cpu_naive_baseline(scene, views, w, h, sample_s):
+    """The reference's `cpu-naive` backend (oracle restatement of
+    src/render/naive.rs: global depth sort, every splat over its bbox, one
+    thread) over a bounded sample of the orbit."""
+    from oracle import oracle as O
+
+    times = []
+    t_end = time.perf_counter() + sample_s
+    i = 0
+    while time.perf_counter() < t_end or i < 1:
+        t0 = time.perf_counter()
+        O.render_naive(scene, views[i % len(views)], w, h)
+        times.append(time.perf_counter() - t0)
+        i += 1
+    return len(times) / sum(times), len(times)
+
+
 def run_reference(args):
     rank, world, _ = dist_env()
     if world > 1 and rank != 0:
@@ -422,6 +439,10 @@ def run_ours(args):
             fps, cores, frames = cpu_baseline(f32_scene, timed, W, H, args.cpu_sample_s)
             cpu = {"value": fps, "unit": "frames/s", "cores": cores, "kind": "port",
                    "sample": f"{frames} full {W}x{H} frames of the orbit (~{args.cpu_sample_s:.0f} s)"}
+            nfps, nframes = cpu_naive_baseline(f32_scene, timed, W, H, min(args.cpu_sample_s, 10.0))
+            cpu_naive = {"value": nfps, "unit": "frames/s", "cores": 1, "kind": "port",
+                         "sample": f"{nframes} full {W}x{H} frames of the orbit",
+                         "backend": "cpu-naive (src/render/naive.rs), one thread"}
         line = {
             "metric": cfg["metric"], "value": value, "unit": "frames/s", "n_gpus": world, "steps": K,
             "warmup": args.warmup, "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak",
@@ -449,6 +470,8 @@ def run_ours(args):
             line["error_vs_fp64_naive"] = errors
         if load is not None:
             line["scene_load"] = load
+        if cpu is not None:
+            line["cpu_naive_baseline"] = cpu_naive
         print(json.dumps(line), flush=True)
     r.close()
     if world > 1:

@@ -184,3 +184,10 @@ def test_batch_abi_layouts_and_validation_without_a_gpu(cuda_lib):
     assert cuda_lib.splat_cuda_batch_run(None) == N.SPLAT_ERR_INVALID_ARG
     assert cuda_lib.splat_cuda_batch_last_error(None) == b""
     assert len(N.BLEND_CONFIGS) == 9 and len(set(N.BLEND_CONFIGS)) == 9
+
+
+def test_c_driver_builds_against_the_header(cuda_lib, tmp_path):
+    """include/splat_cuda.h is valid C99 and the library links from C."""
+    from tests import c_driver
+
+    assert os.path.exists(c_driver.build(str(tmp_path)))

@@ -375,3 +375,38 @@ def test_terminal_cells_match_widget(oracle, mode, size, f):
     want = T.cells(frame.pixels, mode)
     assert got.shape == want.shape and np.array_equal(got, want)
     r.close()
+
+
+def test_c_driver_matches_python_path(tmp_path):
+    """The C host renders the same frame and cells as the ctypes path."""
+    import subprocess
+
+    from splat_b200 import View
+    from splat_b200.scene import Scene
+    from tests import c_driver
+
+    exe = c_driver.build(str(tmp_path))
+    fr, ce = str(tmp_path / "frame.rgb"), str(tmp_path / "cells.bin")
+    out = subprocess.run([exe, fr, ce], capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0, out.stderr
+    side = 8
+    s = Scene()
+    idx = np.arange(side ** 3)
+    x, y, z = idx % side, (idx // side) % side, idx // (side * side)
+    lin = lambda a: (np.float32(-1.0) + np.float32(2.0) * a.astype(np.float32) / np.float32(side - 1))  # noqa: E731
+    s.positions = np.stack([lin(x), lin(y), lin(z)], 1).astype(np.float32)
+    s.scales = np.full((side ** 3, 3), 0.05, np.float32)
+    s.rotations = np.tile(np.array([0, 0, 0, 1], np.float32), (side ** 3, 1))
+    s.opacities = np.full(side ** 3, 0.9, np.float32)
+    s.colors = (np.stack([x, y, z], 1).astype(np.float32) / np.float32(side - 1)).astype(np.float32)
+    s.finalize()
+    r = CudaRenderer(s)
+    v = View.from_array(np.array([0, 0, -4, 1, 0, 0, 0, 1, 0, 0, 0, 1, np.float32(50.0) * np.float32(3.14159265)
+                                  / np.float32(180.0), 0.05], np.float32))
+    f = Frame()
+    r.render(v, 160, 96, (0.1, 0.1, 0.1), f)
+    got = np.fromfile(fr, np.uint8).reshape(96, 160, 3)
+    assert np.array_equal(got, f.pixels)
+    cells = r.render_cells(v, 160, 96, (0.1, 0.1, 0.1), mode=N.SPLAT_CELLS_ANSI256)
+    assert np.array_equal(np.fromfile(ce, np.uint8).reshape(cells.shape), cells)
+    r.close()
