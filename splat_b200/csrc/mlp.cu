@@ -13,9 +13,10 @@
 //   k_train<SRC>     forward + backward, 128 samples per tile, persistent CTAs;
 //                    weight gradients accumulate in TMEM over a CTA's tiles and
 //                    are added to one fp32 vector; latent gradients are added
-//                    to per-splat rows and the touched rows listed
+//                    to per-splat rows
 //   k_adam           Adam on the fp32 master parameters (fp16 operand copy
-//                    refreshed) and lazy Adam on the touched latent rows only
+//                    refreshed) and lazy Adam on the latent rows the step
+//                    sampled (found again from the epoch's shuffle)
 // Loss: mean over active samples and channels of (rgb - target)^2.
 #include <cuda_fp16.h>
 
@@ -56,10 +57,9 @@ struct TrainSmem {
   alignas(128) uint16_t D3[mlp::kRows * 16];  // chunks 0-1 dz3
   alignas(128) uint16_t w1f[64 * 32];         // B: n = out, k = in
   alignas(128) uint16_t w2f[64 * 64];
-  alignas(128) uint16_t w3f[16 * 64];
-  alignas(128) uint16_t w3b[64 * 16];         // B: n = in, k = out (W3^T)
-  alignas(128) uint16_t w2b[64 * 64];         // W2^T
+  alignas(128) uint16_t w2b[64 * 64];         // B: n = in, k = out (W2^T)
   alignas(128) uint16_t w1b[16 * 64];         // W1^T, latent inputs only
+  float w3[3][64];  // layer 3 on the CUDA cores: the fp16 values of W3's rows 0-2
   float b2[64];
   float b3[16];
   float db3[16];
@@ -74,7 +74,6 @@ struct StepState {
   double loss_sum;          // sum of per-step mean losses since the last reset
   unsigned long long loss_steps;
   float last_loss;
-  unsigned int touched;       // latent rows touched by the running step
   unsigned int adam_done;     // CTAs of k_adam finished with the step
   unsigned int error;         // a bounded wait gave up
 };
@@ -105,8 +104,6 @@ struct TrainArgs {
   uint32_t n_dirs;
   const uint4* lat16;   // n x 16 halves
   float* lat_grad;      // n x 16
-  uint32_t* stamp;      // n: step + 1 of the last step that listed the row
-  uint32_t* touched;    // rows listed this step
   uint64_t samples;     // n * n_dirs
   uint64_t seed;
   uint32_t bits;
@@ -181,6 +178,27 @@ __device__ __forceinline__ void masked_epilogue(uint32_t tmem, uint32_t col, uin
   }
 }
 
+// dst (out_rows x k_count, feature-chunked) = the transpose of the first
+// out_rows columns of src (src_rows x >= out_rows, feature-chunked), both
+// in shared memory: dst row n, column k = src row k, column n.
+__device__ __forceinline__ void transpose_tile(uint16_t* dst, const uint16_t* src, uint32_t src_rows,
+                                               uint32_t out_rows, uint32_t k_count) {
+  const uint8_t* sb = reinterpret_cast<const uint8_t*>(src);
+  for (uint32_t q = threadIdx.x; q < out_rows * k_count / 8; q += blockDim.x) {
+    const uint32_t n = q % out_rows, k = (q / out_rows) * 8;
+    uint16_t v[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++)
+      v[j] = *reinterpret_cast<const uint16_t*>(sb + umma::chunked_offset(k + j, n, src_rows));
+    uint4 u;
+    u.x = v[0] | ((uint32_t)v[1] << 16);
+    u.y = v[2] | ((uint32_t)v[3] << 16);
+    u.z = v[4] | ((uint32_t)v[5] << 16);
+    u.w = v[6] | ((uint32_t)v[7] << 16);
+    *reinterpret_cast<uint4*>(reinterpret_cast<uint8_t*>(dst) + umma::chunked_offset(n, k, out_rows)) = u;
+  }
+}
+
 template <Src SRC, int DEG>
 __global__ void __launch_bounds__(kTrainThreads) k_train(TrainArgs a) {
   extern __shared__ __align__(128) uint8_t smem_raw[];
@@ -190,10 +208,12 @@ __global__ void __launch_bounds__(kTrainThreads) k_train(TrainArgs a) {
   // Parameters into the operand tiles (forward and transposed copies).
   mlp::load_rows(S.w1f, a.p16 + mlp::kW1, 64, 32);
   mlp::load_rows(S.w2f, a.p16 + mlp::kW2, 64, 64);
-  mlp::load_rows(S.w3f, a.p16 + mlp::kW3, 16, 64);
-  mlp::load_cols(S.w3b, a.p16 + mlp::kW3, 16, 64, 64);
-  mlp::load_cols(S.w2b, a.p16 + mlp::kW2, 64, 64, 64);
-  mlp::load_cols(S.w1b, a.p16 + mlp::kW1, 64, 32, 16);
+  for (uint32_t i = tid; i < 3 * 64; i += kTrainThreads)
+    S.w3[i / 64][i % 64] = __half2float(__ushort_as_half(a.p16[mlp::kW3 + i]));
+  __syncthreads();
+  // The transposed operands of the backward pass, from the forward tiles.
+  transpose_tile(S.w2b, S.w2f, 64, 64, 64);
+  transpose_tile(S.w1b, S.w1f, 64, 16, 64);
   if (tid < 64) S.b2[tid] = __half2float(__ushort_as_half(a.p16[mlp::kB2 + tid]));
   if (tid < 16) {
     S.b3[tid] = __half2float(__ushort_as_half(a.p16[mlp::kB3 + tid]));
@@ -210,13 +230,11 @@ __global__ void __launch_bounds__(kTrainThreads) k_train(TrainArgs a) {
 
   // Step bookkeeping (scene samples).
   uint64_t step = 0, base = 0, key = 0;
-  uint32_t tag = 0;
   if (SRC == Src::kScene) {
     step = *reinterpret_cast<volatile unsigned long long*>(&a.st->step);
     const uint64_t k = step % a.steps_per_epoch;
     base = k * a.batch;
     key = epoch_key(a.seed, step / a.steps_per_epoch);
-    tag = (uint32_t)(step + 1);
   }
 
   uint32_t phase = 0;
@@ -287,22 +305,39 @@ __global__ void __launch_bounds__(kTrainThreads) k_train(TrainArgs a) {
       umma::commit(mbar);
     }
     wait_mma();
-    const uint64_t mask2 = mlp::hidden_epilogue(tmem, kTS, S.b2, S.Q, tid);
-    if (sync_or_abort()) { aborted = true; break; }
-    if (tid == 0) {
-      umma::fence_after_sync();
-      mlp::gemm_k(tmem + kTZ, sQ, 0, umma::smem_u32(S.w3f), 16, 4, mlp::kIdN16);
-      umma::commit(mbar);
-    }
-    wait_mma();
+    // Layer 2's epilogue with layer 3 and its backward on the CUDA cores:
+    // h2 = fp16(relu(z2 + b2)) to Q chunks 0-7, z3 = W3 h2 + b3, rgb, loss,
+    // dz3 (fp16) to D3, dh2 = W3^T dz3, dz2 = dh2 masked by h2 > 0 to Q 8-15.
     if (SRC == Src::kScene && active) sh_target<DEG>(reinterpret_cast<const float*>(row4), d[0], d[1], d[2], tgt);
     {
-      float z[16];
-      umma::tmem_ld16(umma::tmem_warp_addr(tmem, kTZ), z);
+      uint64_t mask2 = 0;
+      float z3[3] = {S.b3[0], S.b3[1], S.b3[2]};
+#pragma unroll
+      for (uint32_t q = 0; q < 4; q++) {
+        float v[16];
+        umma::tmem_ld16(umma::tmem_warp_addr(tmem, kTS + 16 * q), v);
+#pragma unroll
+        for (int k = 0; k < 16; k++) {
+          const uint32_t c = 16 * q + k;
+          v[k] = __half2float(__float2half_rn(fmaxf(v[k] + S.b2[c], 0.0f)));
+          if (v[k] > 0.0f) mask2 |= 1ull << c;
+          z3[0] = fmaf(S.w3[0][c], v[k], z3[0]);
+          z3[1] = fmaf(S.w3[1][c], v[k], z3[1]);
+          z3[2] = fmaf(S.w3[2][c], v[k], z3[2]);
+        }
+        float lo[8], hi[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+          lo[k] = v[k];
+          hi[k] = v[8 + k];
+        }
+        mlp::store_chunk(S.Q, tid, 2 * q, lo);
+        mlp::store_chunk(S.Q, tid, 2 * q + 1, hi);
+      }
       float dz[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
       float y[3];
       for (int c = 0; c < 3; c++) {
-        y[c] = mlp::sigmoidf(z[c] + S.b3[c]);
+        y[c] = mlp::sigmoidf(z3[c]);
         if (active) {
           const float e = y[c] - tgt[c];
           loss += e * e;
@@ -311,26 +346,27 @@ __global__ void __launch_bounds__(kTrainThreads) k_train(TrainArgs a) {
       }
       if (SRC == Src::kExplicit && active)
         for (int c = 0; c < 3; c++) a.ex_out[3 * j + c] = y[c];
-      // The bias gradient sums the fp16-rounded dz3 the GEMMs use.
+      // The GEMMs and the bias gradient use the fp16-rounded dz3.
       for (int c = 0; c < 3; c++) {
         dz[c] = __half2float(__float2half_rn(dz[c]));
-        const float s = warp_sum(dz[c]);
-        if ((tid & 31) == 0) atomicAdd(&S.db3[c], s);
+        const float s3 = warp_sum(dz[c]);
+        if ((tid & 31) == 0) atomicAdd(&S.db3[c], s3);
       }
       mlp::store_chunk(S.D3, tid, 0, dz);
       const float zero[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
       mlp::store_chunk(S.D3, tid, 1, zero);
+#pragma unroll
+      for (uint32_t q = 0; q < 8; q++) {
+        float g8[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+          const uint32_t c = 8 * q + k;
+          const float dh = fmaf(dz[2], S.w3[2][c], fmaf(dz[1], S.w3[1][c], dz[0] * S.w3[0][c]));
+          g8[k] = ((mask2 >> c) & 1ull) ? dh : 0.0f;
+        }
+        mlp::store_chunk(S.Q, tid, 8 + q, g8);
+      }
     }
-    if (sync_or_abort()) { aborted = true; break; }
-
-    // ---- backward --------------------------------------------------------------
-    if (tid == 0) {  // dh2 = dz3 W3
-      umma::fence_after_sync();
-      mlp::gemm_k(tmem + kTS, sD3, 0, umma::smem_u32(S.w3b), 64, 1, mlp::kIdN64);
-      umma::commit(mbar);
-    }
-    wait_mma();
-    masked_epilogue(tmem, kTS, mask2, S.Q, 8, tid);  // dz2
     if (sync_or_abort()) { aborted = true; break; }
     if (tid == 0) {
       umma::fence_after_sync();
@@ -362,7 +398,6 @@ __global__ void __launch_bounds__(kTrainThreads) k_train(TrainArgs a) {
         } else {
           float4* o = reinterpret_cast<float4*>(a.lat_grad + 16 * splat);
           for (int q = 0; q < 4; q++) atomicAdd(o + q, make_float4(g[4 * q], g[4 * q + 1], g[4 * q + 2], g[4 * q + 3]));
-          if (atomicExch(a.stamp + splat, tag) != tag) a.touched[atomicAdd(&a.st->touched, 1u)] = (uint32_t)splat;
         }
       }
     }
@@ -416,6 +451,9 @@ struct AdamArgs {
   float lr, b1, b2, eps;
   uint32_t batch, steps_per_epoch;
   uint64_t samples;
+  // the step's sample order (for the latent rows it touched)
+  uint64_t seed;
+  uint32_t bits, n_dirs;
 };
 
 __device__ __forceinline__ float adam_update(float& m, float& v, float g, float lr, float b1, float b2, float eps,
@@ -431,16 +469,18 @@ constexpr uint32_t kAdamParamCtas = (mlp::kParams + kAdamThreads - 1) / kAdamThr
 
 // One launch after each training step. CTAs [0, kAdamParamCtas) apply Adam
 // to the fp32 master parameters and refresh their fp16 copy; the others
-// apply lazy Adam to the latent rows the step touched, one thread per row
-// (16 elements as float4s). The last CTA to finish closes the step: records
-// its loss, clears the touched list and advances the step counter.
+// apply lazy Adam to the latent rows the step touched: one thread per
+// sample of the step recomputes its splat from the epoch's shuffle, and the
+// first thread to stamp the row with the step (step + 1) updates it (16
+// elements as float4s), so a row sampled twice is updated once with its
+// summed gradient. The last CTA to finish closes the step: records its loss
+// and advances the step counter.
 __global__ void __launch_bounds__(kAdamThreads) k_adam(float* __restrict__ p32, float* __restrict__ pm,
                                                        float* __restrict__ pv, uint16_t* __restrict__ p16,
                                                        float* __restrict__ grad, float* __restrict__ lat32,
                                                        float* __restrict__ lm, float* __restrict__ lv,
                                                        uint16_t* __restrict__ lat16, float* __restrict__ lat_grad,
-                                                       const uint32_t* __restrict__ touched, StepState* st,
-                                                       AdamArgs a) {
+                                                       uint32_t* __restrict__ stamp, StepState* st, AdamArgs a) {
   const uint64_t step = *reinterpret_cast<volatile unsigned long long*>(&st->step);
   const uint64_t k = step % a.steps_per_epoch;
   const uint64_t active = min((uint64_t)a.batch, a.samples - k * a.batch);
@@ -460,10 +500,13 @@ __global__ void __launch_bounds__(kAdamThreads) k_adam(float* __restrict__ p32, 
       p16[i] = __half_as_ushort(__float2half_rn(p));
     }
   } else {
-    const uint32_t count = *reinterpret_cast<volatile unsigned int*>(&st->touched);
-    for (uint32_t q = (blockIdx.x - kAdamParamCtas) * kAdamThreads + threadIdx.x; q < count;
+    const uint64_t key = epoch_key(a.seed, step / a.steps_per_epoch);
+    const uint32_t tag = (uint32_t)(step + 1);
+    for (uint32_t q = (blockIdx.x - kAdamParamCtas) * kAdamThreads + threadIdx.x; q < active;
          q += (gridDim.x - kAdamParamCtas) * kAdamThreads) {
-      const uint64_t row = (uint64_t)__ldg(touched + q) * 16;
+      const uint64_t splat = mlp::shuffle_index(k * a.batch + q, a.samples, key, a.bits) / a.n_dirs;
+      if (atomicExch(stamp + splat, tag) == tag) continue;  // another sample of the row updates it
+      const uint64_t row = splat * 16;
       float4* g4 = reinterpret_cast<float4*>(lat_grad + row);
       float4* m4 = reinterpret_cast<float4*>(lm + row);
       float4* v4 = reinterpret_cast<float4*>(lv + row);
@@ -508,7 +551,6 @@ __global__ void __launch_bounds__(kAdamThreads) k_adam(float* __restrict__ p32, 
       st->loss_sum += ls;
       st->loss_steps += 1;
       st->last_loss = (float)ls;
-      st->touched = 0;
       st->adam_done = 0;
       __threadfence();
       st->step = step + 1;
@@ -610,7 +652,7 @@ struct splat_cuda_learner {
   uint16_t* p16 = nullptr;
   float *lat32 = nullptr, *lm = nullptr, *lv = nullptr, *lgrad = nullptr;
   uint16_t* lat16 = nullptr;
-  uint32_t *stamp = nullptr, *touched = nullptr;
+  uint32_t* stamp = nullptr;
   float4* dirs = nullptr;
   float* shs = nullptr;
   StepState* st = nullptr;
@@ -640,7 +682,7 @@ int lcuda(splat_cuda_learner* L, cudaError_t e, const char* what) {
 void enqueue_adam(splat_cuda_learner* L, cudaStream_t s) {
   const uint32_t lat_ctas = std::max(1u, std::min((L->batch + kAdamThreads - 1) / kAdamThreads, 4u * L->num_sms));
   k_adam<<<kAdamParamCtas + lat_ctas, kAdamThreads, 0, s>>>(L->p32, L->pm, L->pv, L->p16, L->grad, L->lat32, L->lm,
-                                                             L->lv, L->lat16, L->lgrad, L->touched, L->st, L->adam);
+                                                             L->lv, L->lat16, L->lgrad, L->stamp, L->st, L->adam);
 }
 
 // One step: train, then Adam on the parameters and the touched latents.
@@ -696,7 +738,8 @@ SPLAT_API int splat_cuda_learner_create(const splat_cuda_handle* h, const splat_
   L->bits = 1;
   while ((1ull << L->bits) < L->samples) L->bits++;
   L->seed = cfg->seed;
-  L->adam = AdamArgs{cfg->lr, cfg->beta1, cfg->beta2, cfg->eps, L->batch, L->steps_per_epoch, L->samples};
+  L->adam = AdamArgs{cfg->lr, cfg->beta1, cfg->beta2, cfg->eps, L->batch, L->steps_per_epoch, L->samples,
+                     L->seed, L->bits, L->n_dirs};
   cudaError_t e = cudaSetDevice(L->device);
   if (e != cudaSuccess) return bail(lcuda(L, e, "cudaSetDevice"));
   if ((e = cudaDeviceGetAttribute(&L->num_sms, cudaDevAttrMultiProcessorCount, L->device)) != cudaSuccess)
@@ -724,7 +767,6 @@ SPLAT_API int splat_cuda_learner_create(const splat_cuda_handle* h, const splat_
       (rc = dalloc((void**)&L->lat32, nl * 4, "latents")) || (rc = dalloc((void**)&L->lm, nl * 4, "latents")) ||
       (rc = dalloc((void**)&L->lv, nl * 4, "latents")) || (rc = dalloc((void**)&L->lgrad, nl * 4, "latents")) ||
       (rc = dalloc((void**)&L->lat16, nl * 2, "latents")) || (rc = dalloc((void**)&L->stamp, L->n * 4, "latents")) ||
-      (rc = dalloc((void**)&L->touched, (size_t)L->batch * 4, "latents")) ||
       (rc = dalloc((void**)&L->dirs, (size_t)L->n_dirs * sizeof(float4), "directions")) ||
       (rc = dalloc((void**)&L->shs,
                    (size_t)L->n * (((L->sh_degree + 1) * (L->sh_degree + 1) * 3 + 3) / 4) * sizeof(float4),
@@ -768,8 +810,6 @@ SPLAT_API int splat_cuda_learner_create(const splat_cuda_handle* h, const splat_
   a.n_dirs = L->n_dirs;
   a.lat16 = reinterpret_cast<const uint4*>(L->lat16);
   a.lat_grad = L->lgrad;
-  a.stamp = L->stamp;
-  a.touched = L->touched;
   a.samples = L->samples;
   a.seed = L->seed;
   a.bits = L->bits;
@@ -956,7 +996,7 @@ SPLAT_API int splat_cuda_learner_destroy(splat_cuda_learner* L) {
   if (L->stream) cudaStreamSynchronize(L->stream);
   if (L->graph) cudaGraphExecDestroy(L->graph);
   for (void* p : {(void*)L->p32, (void*)L->pm, (void*)L->pv, (void*)L->grad, (void*)L->p16, (void*)L->lat32,
-                  (void*)L->lm, (void*)L->lv, (void*)L->lgrad, (void*)L->lat16, (void*)L->stamp, (void*)L->touched,
+                  (void*)L->lm, (void*)L->lv, (void*)L->lgrad, (void*)L->lat16, (void*)L->stamp,
                   (void*)L->dirs, (void*)L->shs, (void*)L->st})
     if (p) cudaFree(p);
   if (L->stream) cudaStreamDestroy(L->stream);
