@@ -92,13 +92,11 @@ int ensure_size(splat_cuda_handle* h, uint64_t tiles, uint32_t rows, size_t out_
   if (tiles > h->ranges_cap) {
     dfree(h->ranges);
     dfree(h->totals);
-    dfree(h->mid_list);
-    dfree(h->long_list);
+    dfree(h->order);
     h->ranges_cap = 0;
     CK(cudaMalloc(&h->ranges, tiles * sizeof(uint2)), "cudaMalloc ranges");
     CK(cudaMalloc(&h->totals, tiles * sizeof(uint32_t)), "cudaMalloc totals");
-    CK(cudaMalloc(&h->mid_list, tiles * sizeof(uint32_t)), "cudaMalloc mid tiles");
-    CK(cudaMalloc(&h->long_list, tiles * sizeof(uint32_t)), "cudaMalloc long tiles");
+    CK(cudaMalloc(&h->order, kTileClasses * tiles * sizeof(uint32_t)), "cudaMalloc tile classes");
     h->ranges_cap = tiles;
   }
   const size_t words = (size_t)rows * tiles;
@@ -229,12 +227,12 @@ int enqueue_frame(splat_cuda_handle* h, const FrameParams& fp_in, uint8_t* dev_o
   bl.max_tiles = (uint32_t)tiles;
   bl.counts_all = h->counts;
   bl.counts_bytes = (size_t)rows * tiles * sizeof(uint32_t);
-  CK(launch_binning(h->table, bl, h->totals, h->ranges, h->mid_list, h->long_list, h->pairs[0], h->pairs[1], h->cap,
+  CK(launch_binning(h->table, bl, h->totals, h->ranges, h->order, h->pairs[0], h->pairs[1], h->cap,
                     fc, h->num_sms, h->max_smem, s, &h->launches),
      "binning kernels");
   if (h->stage_events) CK(cudaEventRecord(h->ev[2], s), "event");
-  CK(launch_blend(h->table, 1, (uint32_t)tiles, h->pairs[0], h->ranges, h->exact, h->blend, fc.st, h->num_sms, s,
-                  &h->launches),
+  CK(launch_blend(h->table, 1, (uint32_t)tiles, h->pairs[0], h->ranges, h->order, h->exact, h->blend, fc.st,
+                  h->num_sms, s, &h->launches),
      "blend kernel");
   if (scratch) CK(launch_downsample(fp, h->full_dev, dev_out, s, &h->launches), "downsample kernel");
   if (h->stage_events) CK(cudaEventRecord(h->ev[3], s), "event");
@@ -753,8 +751,7 @@ SPLAT_API int splat_cuda_destroy(splat_cuda_handle* h) {
   dfree(h->ranges);
   dfree(h->counts);
   dfree(h->totals);
-  dfree(h->mid_list);
-  dfree(h->long_list);
+  dfree(h->order);
   dfree(h->out_dev);
   dfree(h->full_dev);
   dfree(h->st);

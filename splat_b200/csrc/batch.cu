@@ -55,8 +55,7 @@ struct splat_cuda_batch {
   size_t counts_words = 0;
   uint32_t* totals = nullptr;
   uint2* ranges = nullptr;
-  uint32_t* mid_list = nullptr;
-  uint32_t* long_list = nullptr;
+  uint32_t* order = nullptr;  // kTileClasses lists of n_tiles tiles
   void* counters = nullptr;        // FrameCounters block (device)
   void* counters_host = nullptr;   // pinned copy
   size_t counters_bytes = 0;
@@ -110,8 +109,7 @@ void free_plan(splat_cuda_batch* b) {
   dfree(b->counts);
   dfree(b->totals);
   dfree(b->ranges);
-  dfree(b->mid_list);
-  dfree(b->long_list);
+  dfree(b->order);
   dfree(b->counters);
   if (b->counters_host) cudaFreeHost(b->counters_host);
   b->counters_host = nullptr;
@@ -201,8 +199,7 @@ int plan(splat_cuda_batch* b) {
   const size_t nt = std::max<uint32_t>(b->n_tiles, 1);
   BK(cudaMalloc(&b->totals, nt * sizeof(uint32_t)), "cudaMalloc totals");
   BK(cudaMalloc(&b->ranges, nt * sizeof(uint2)), "cudaMalloc ranges");
-  BK(cudaMalloc(&b->mid_list, nt * sizeof(uint32_t)), "cudaMalloc mid tiles");
-  BK(cudaMalloc(&b->long_list, nt * sizeof(uint32_t)), "cudaMalloc long tiles");
+  BK(cudaMalloc(&b->order, kTileClasses * nt * sizeof(uint32_t)), "cudaMalloc tile classes");
   // Padding tiles between views are never written by the column scan: their
   // totals stay zero (empty ranges).
   BK(cudaMemset(b->totals, 0, nt * sizeof(uint32_t)), "clear totals");
@@ -252,12 +249,12 @@ int enqueue(splat_cuda_batch* b, cudaStream_t s) {
   bl.max_tiles = b->max_tiles;
   bl.counts_all = b->counts;
   bl.counts_bytes = b->counts_words * sizeof(uint32_t);
-  BK(launch_binning(b->table, bl, b->totals, b->ranges, b->mid_list, b->long_list, b->pairs[0], b->pairs[1], b->cap,
+  BK(launch_binning(b->table, bl, b->totals, b->ranges, b->order, b->pairs[0], b->pairs[1], b->cap,
                     fc, b->num_sms, b->max_smem, s, &b->launches),
      "binning kernels");
   BK(stage_event(b, 2, s), "event");
-  BK(launch_blend(b->table, nv, b->n_tiles, b->pairs[0], b->ranges, b->exact, b->cfg, fc.st, b->num_sms, s,
-                  &b->launches),
+  BK(launch_blend(b->table, nv, b->n_tiles, b->pairs[0], b->ranges, b->order, b->exact, b->cfg, fc.st,
+                  b->num_sms, s, &b->launches),
      "blend kernel");
   BK(stage_event(b, 3, s), "event");
   BK(cudaMemcpyAsync(b->counters_host, b->counters, b->counters_bytes, cudaMemcpyDeviceToHost, s), "copy counters");

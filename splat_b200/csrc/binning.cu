@@ -12,8 +12,8 @@
 //                 tile totals, and their sums per chunk of kScanChunk tiles;
 //  k_tile_ranges  per chunk, an exclusive scan of the tile totals offset by
 //                 the preceding chunks: the tile ranges ([begin, end); [0, 0)
-//                 for an empty tile) and the lists of tiles too long for a
-//                 warp sort;
+//                 for an empty tile) and the tiles' class lists (tile_class:
+//                 the long sort's, the mid sort's and the blend's order);
 //  k_bin_scatter  each CTA writes its pairs at its row's offsets, positions
 //                 handed out by shared-memory atomics.
 //
@@ -45,11 +45,16 @@ template <class F>
 __device__ __forceinline__ void for_each_pair(const BinInfo* __restrict__ bin, uint64_t s0, uint64_t s1,
                                               uint32_t tiles_x, F&& f) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  constexpr int kWarpsPerCta = kBinThreads / 32;
-  for (uint64_t wb = s0 + (uint64_t)warp * 32; wb < s1; wb += (uint64_t)kWarpsPerCta * 32) {
+  constexpr uint64_t kStride = (uint64_t)kBinThreads;
+  // The lane's splat of the warp's next group of 32 is loaded while the
+  // current group's pairs are expanded.
+  const BinInfo culled{kCulled, 0u, 0u, 0u};
+  uint64_t wb = s0 + (uint64_t)warp * 32;
+  BinInfo nb = wb + lane < s1 ? bin[wb + lane] : culled;
+  for (; wb < s1; wb += kStride) {
     const uint64_t i = wb + lane;
-    BinInfo b{kCulled, 0u, 0u, 0u};
-    if (i < s1) b = bin[i];
+    const BinInfo b = nb;
+    nb = i + kStride < s1 ? bin[i + kStride] : culled;
     const uint32_t cnt = b.rect_lo != kCulled ? b.count : 0u;
     if (cnt <= 32) {
       const uint32_t tx0 = b.rect_lo & 0xFFFFu, ty0 = b.rect_lo >> 16, tx1 = b.rect_hi & 0xFFFFu;
@@ -180,8 +185,7 @@ static_assert(kScanChunk == kRangeThreads * 4, "four tiles per thread");
 
 __global__ void __launch_bounds__(kRangeThreads) k_tile_ranges(const uint32_t* __restrict__ totals, uint32_t n_tiles,
                                                                uint64_t cap, uint2* __restrict__ ranges,
-                                                               uint32_t* __restrict__ mid_list,
-                                                               uint32_t* __restrict__ long_list, FrameCounters fc) {
+                                                               uint32_t* __restrict__ order, FrameCounters fc) {
   __shared__ unsigned long long s_warp[kRangeThreads / 32];
   __shared__ unsigned long long s_base;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -226,6 +230,7 @@ __global__ void __launch_bounds__(kRangeThreads) k_tile_ranges(const uint32_t* _
 #pragma unroll
   for (int k = 0; k < 4; k++) {
     const uint32_t t = t0 + k;
+    uint32_t cls = kTileClasses;
     if (t < n_tiles) {
       // Ranges are clamped to the pair capacity: past it the frame is
       // incomplete and rendered again with larger buffers, and nothing
@@ -233,12 +238,15 @@ __global__ void __launch_bounds__(kRangeThreads) k_tile_ranges(const uint32_t* _
       const uint32_t s = (uint32_t)min(start, (unsigned long long)cap);
       const uint32_t e = (uint32_t)min(start + c[k], (unsigned long long)cap);
       ranges[t] = e > s ? make_uint2(s, e) : make_uint2(0u, 0u);
-      const uint32_t len = e > s ? e - s : 0u;
-      if (len > kMidSortCap)
-        long_list[atomicAdd(&fc.st->long_tiles, 1u)] = t;
-      else if (len > kWarpSortCap)
-        mid_list[atomicAdd(&fc.st->mid_tiles, 1u)] = t;
+      cls = tile_class(e > s ? e - s : 0u);
     }
+    // The tile joins its class's list: one atomic per class in the warp.
+    const uint32_t same = __match_any_sync(0xffffffffu, cls);
+    const int leader = __ffs(same) - 1;
+    uint32_t at = 0;
+    if (lane == leader && cls < kTileClasses) at = atomicAdd(&fc.st->cls[cls], (uint32_t)__popc(same));
+    at = __shfl_sync(0xffffffffu, at, leader) + __popc(same & ((1u << lane) - 1u));
+    if (cls < kTileClasses) order[(size_t)cls * n_tiles + at] = t;
     start += c[k];
   }
   if (chunk == gridDim.x - 1 && tid == 0) fc.st->total_pairs = base + chunk_total;
@@ -288,15 +296,28 @@ struct MidSmem {
   CountSortSmem t;
 };
 
+// Tiles of classes 1-3, heaviest class first, taken one at a time from a
+// shared counter (the tiles differ in length up to 8x).
 __global__ void __launch_bounds__(kTileThreads) k_sort_mid(const uint2* __restrict__ ranges,
-                                                           const uint32_t* __restrict__ mid_list,
-                                                           uint64_t* __restrict__ pairs, const DevState* st) {
+                                                           const uint32_t* __restrict__ order, uint32_t n_tiles,
+                                                           uint64_t* __restrict__ pairs, DevState* st) {
   extern __shared__ __align__(16) unsigned char s_raw[];
   MidSmem& sm = *reinterpret_cast<MidSmem*>(s_raw);
+  __shared__ uint32_t s_tile;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const uint32_t nmid = *(const volatile uint32_t*)&st->mid_tiles;
-  for (uint32_t li = blockIdx.x; li < nmid; li += gridDim.x) {
-    const uint2 r = ranges[mid_list[li]];
+  const uint32_t n1 = st->cls[1], n2 = st->cls[2], n3 = st->cls[3];
+  for (;;) {
+    if (tid == 0) {
+      const uint32_t li = atomicAdd(&st->mid_next, 1u);
+      s_tile = li < n1             ? order[(size_t)n_tiles + li]
+               : li < n1 + n2      ? order[2 * (size_t)n_tiles + (li - n1)]
+               : li < n1 + n2 + n3 ? order[3 * (size_t)n_tiles + (li - n1 - n2)]
+                                   : 0xFFFFFFFFu;
+    }
+    __syncthreads();
+    const uint32_t tile = s_tile;
+    if (tile == 0xFFFFFFFFu) break;
+    const uint2 r = ranges[tile];
     const uint32_t n = r.y - r.x;
     uint32_t mn = 0xFFFFFFFFu, mx = 0u;
     for (uint32_t e = tid; e < n; e += kTileThreads) {
@@ -343,11 +364,11 @@ struct LongSmem {
 __global__ void __launch_bounds__(kTileThreads) k_sort_long(const uint2* __restrict__ ranges,
                                                             const uint32_t* __restrict__ long_list,
                                                             uint64_t* __restrict__ w0, uint64_t* __restrict__ w1,
-                                                            uint64_t cap, const DevState* st) {
+                                                            uint64_t cap, const DevState* st) {  // class 0
   __shared__ LongSmem sm;
   constexpr int kChunks = kLongChunk / (32 * kTileWarps);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const uint32_t nlong = *(const volatile uint32_t*)&st->long_tiles;
+  const uint32_t nlong = st->cls[0];
   for (uint32_t li = blockIdx.x; li < nlong; li += gridDim.x) {
     const uint2 r = ranges[long_list[li]];  // within the capacity (k_bin_tilescan)
     const uint32_t b = r.x, n = r.y - r.x;
@@ -442,7 +463,7 @@ uint32_t bin_rows(uint64_t n, int num_sms) {
 }
 
 cudaError_t launch_binning(const ViewTask* table, const BinLaunch& bl, uint32_t* totals, uint2* ranges,
-                           uint32_t* mid_list, uint32_t* long_list, uint64_t* pairs, uint64_t* pairs_alt,
+                           uint32_t* order, uint64_t* pairs, uint64_t* pairs_alt,
                            uint64_t cap, const FrameCounters& fc, int num_sms, size_t max_smem, cudaStream_t stream,
                            uint32_t* launches) {
   if (bl.n_tiles == 0) return cudaSuccess;
@@ -468,7 +489,7 @@ cudaError_t launch_binning(const ViewTask* table, const BinLaunch& bl, uint32_t*
   }
   k_bin_colscan<<<bl.col_ctas, 256, 0, stream>>>(table, bl.n_views, totals, fc);
   const uint32_t chunks = (bl.n_tiles + kScanChunk - 1) / kScanChunk;
-  k_tile_ranges<<<chunks, kRangeThreads, 0, stream>>>(totals, bl.n_tiles, cap, ranges, mid_list, long_list, fc);
+  k_tile_ranges<<<chunks, kRangeThreads, 0, stream>>>(totals, bl.n_tiles, cap, ranges, order, fc);
   if (use_smem) {
     k_bin_scatter<true><<<bl.bin_ctas, kBinThreads, smem, stream>>>(table, bl.n_views, ranges, pairs, cap);
   } else {
@@ -487,8 +508,8 @@ cudaError_t launch_binning(const ViewTask* table, const BinLaunch& bl, uint32_t*
   }
   const int om = std::max(occ_mid.load(std::memory_order_relaxed), 1);
   const int ol = std::max(occ_long.load(std::memory_order_relaxed), 1);
-  k_sort_mid<<<num_sms * om, kTileThreads, sizeof(MidSmem), stream>>>(ranges, mid_list, pairs, fc.st);
-  k_sort_long<<<num_sms * ol, kTileThreads, 0, stream>>>(ranges, long_list, pairs, pairs_alt, cap, fc.st);
+  k_sort_mid<<<num_sms * om, kTileThreads, sizeof(MidSmem), stream>>>(ranges, order, bl.n_tiles, pairs, fc.st);
+  k_sort_long<<<num_sms * ol, kTileThreads, 0, stream>>>(ranges, order, pairs, pairs_alt, cap, fc.st);
   *launches += 7;
   return cudaGetLastError();
 }

@@ -199,17 +199,23 @@ struct BlendShape {
   static_assert(NG <= 8, "named barriers 1..8");
 };
 
-// Shared memory of one tile group: a batch of G staged splats (centre,
-// conic, opacity, colour, bbox masks), the warps' lists of batch entries,
-// the tile's quantised pixels for the fused downsample, the group's tile.
+// A batch of G staged splats: centre, conic, opacity, colour, bbox masks.
+template <int G>
+struct __align__(16) StagedBatch {
+  float4 a[G];  // see stage_splat (exact path: the record's r0)
+  float4 b[G];  // see stage_splat (exact path: the record's r1)
+  float2 c[G];  // see staged_colour
+  uint32_t mx[G];
+  uint32_t my[G];
+};
+
+// Shared memory of one tile group: two staged batches (the group blends one
+// while it stages the next), the warps' lists of batch entries, the tile's
+// quantised pixels for the fused downsample, the group's tile.
 template <int TW, int TH, int NT>
 struct __align__(16) GroupSmem {
   using S = BlendShape<TW, TH, NT>;
-  float4 a[S::G];  // x, y, -a/2, -b
-  float4 b[S::G];  // -c/2, opacity, red, green
-  float2 c[S::G];  // see staged_colour
-  uint32_t mx[S::G];
-  uint32_t my[S::G];
+  StagedBatch<S::G> bt[2];
   uint16_t list[S::GW][S::G];
   uint32_t px[S::P];
   uint32_t work;
@@ -218,7 +224,7 @@ struct __align__(16) GroupSmem {
 template <bool EXACT, int TW, int TH, int NT>
 __global__ void __launch_bounds__(NT, NT == 512 ? 2 : (NT == 256 ? 5 : 8)) k_blend(const ViewTask* __restrict__ table, uint32_t n_views, uint32_t n_tiles,
                                               const uint64_t* __restrict__ pairs, const uint2* __restrict__ ranges,
-                                              DevState* st) {
+                                              const uint32_t* __restrict__ order, DevState* st) {
   using S = BlendShape<TW, TH, NT>;
   using Smem = GroupSmem<TW, TH, NT>;
   constexpr int G = S::G, PPT = S::PPT;
@@ -244,8 +250,24 @@ __global__ void __launch_bounds__(NT, NT == 512 ? 2 : (NT == 256 ? 5 : 8)) k_ble
   const uint32_t wxbits = 0xFFu << (wbx * 8);
   const uint32_t wybits = ((1u << S::BH) - 1u) << (wby * S::BH);
 
+  // Tiles are taken heaviest class first (tile_class), each class's list in
+  // the order k_tile_ranges appended it.
+  __shared__ uint32_t s_cls[kTileClasses];
+  if (tid < kTileClasses) s_cls[tid] = st->cls[tid];
+  __syncthreads();
   for (;;) {
-    if (gt == 0) sm.work = atomicAdd(&st->blend_next, 1u);
+    if (gt == 0) {
+      uint32_t w = atomicAdd(&st->blend_next, 1u), tl = 0xFFFFFFFFu;
+#pragma unroll
+      for (int k = 0; k < kTileClasses; k++) {
+        if (w < s_cls[k]) {
+          tl = order[(size_t)k * n_tiles + w];
+          break;
+        }
+        w -= s_cls[k];
+      }
+      sm.work = tl;
+    }
     sync();
     const uint32_t tile = sm.work;
     if (tile >= n_tiles) break;
@@ -282,43 +304,49 @@ __global__ void __launch_bounds__(NT, NT == 512 ? 2 : (NT == 256 ? 5 : 8)) k_ble
 
     const uint2 range = ranges[tile];
     const uint32_t begin = range.x, n = range.y > range.x ? range.y - range.x : 0u;
-    Record nr;
+    // Batch k is staged into buffer k & 1 by the group while it blends batch
+    // k - 1 from the other buffer; the barrier that ends batch k - 1 (the
+    // early-exit vote) publishes it. The records of batch k + 1 are in
+    // flight during the blend of batch k.
+    Record nr{};
     bool has = false;
-    if ((uint32_t)gt < n) {
-      nr = rec[(uint32_t)pairs[begin + gt]];
-      has = true;
-    }
-    for (uint32_t start = 0; start < n; start += G) {
-      if (has) {
-        const uint32_t bx = __float_as_uint(nr.r2.y), by = __float_as_uint(nr.r2.z);
-        const int x0 = min(max((int)(bx & 0xFFFFu) - (int)ox, 0), TW), x1 = min(max((int)(bx >> 16) - (int)ox, 0), TW);
-        const int y0 = min(max((int)(by & 0xFFFFu) - (int)oy, 0), TH), y1 = min(max((int)(by >> 16) - (int)oy, 0), TH);
-        sm.mx[gt] = x1 > x0 ? bit_range(x0, x1) : 0u;
-        sm.my[gt] = y1 > y0 ? bit_range(y0, y1) : 0u;
-        if (EXACT) {
-          sm.a[gt] = nr.r0;
-          sm.b[gt] = nr.r1;
-          sm.c[gt] = make_float2(nr.r2.x, 0.0f);
-        } else {
-          float4 a, b;
-          float2 c;
-          stage_splat(nr, ox05, oy05, a, b, c);
-          sm.a[gt] = a;
-          sm.b[gt] = b;
-          sm.c[gt] = c;
-        }
+    auto stage = [&](StagedBatch<G>& d) {
+      const uint32_t bx = __float_as_uint(nr.r2.y), by = __float_as_uint(nr.r2.z);
+      const int x0 = min(max((int)(bx & 0xFFFFu) - (int)ox, 0), TW), x1 = min(max((int)(bx >> 16) - (int)ox, 0), TW);
+      const int y0 = min(max((int)(by & 0xFFFFu) - (int)oy, 0), TH), y1 = min(max((int)(by >> 16) - (int)oy, 0), TH);
+      d.mx[gt] = x1 > x0 ? bit_range(x0, x1) : 0u;
+      d.my[gt] = y1 > y0 ? bit_range(y0, y1) : 0u;
+      if (EXACT) {
+        d.a[gt] = nr.r0;
+        d.b[gt] = nr.r1;
+        d.c[gt] = make_float2(nr.r2.x, 0.0f);
+      } else {
+        float4 a, b;
+        float2 c;
+        stage_splat(nr, ox05, oy05, a, b, c);
+        d.a[gt] = a;
+        d.b[gt] = b;
+        d.c[gt] = c;
       }
+    };
+    if (n > 0) {
+      if ((uint32_t)gt < n) {
+        nr = rec[(uint32_t)pairs[begin + gt]];
+        stage(sm.bt[0]);
+      }
+      has = (uint32_t)gt + G < n;
+      if (has) nr = rec[(uint32_t)pairs[begin + G + gt]];
       sync();
-      const uint32_t nxt = start + G + gt;
-      has = nxt < n;
-      if (has) nr = rec[(uint32_t)pairs[begin + nxt]];
+    }
+    for (uint32_t start = 0, buf = 0; start < n; start += G, buf ^= 1u) {
+      const StagedBatch<G>& bt = sm.bt[buf];
       const uint32_t cnt = min((uint32_t)G, n - start);
       // This warp's list of batch entries whose bbox meets its block.
       uint32_t len = 0;
       if (__any_sync(0xffffffffu, !all_done)) {
         for (uint32_t c0 = 0; c0 < cnt; c0 += 32) {
           const uint32_t e = c0 + lane;
-          const bool hit = e < cnt && (sm.mx[e] & wxbits) && (sm.my[e] & wybits);
+          const bool hit = e < cnt && (bt.mx[e] & wxbits) && (bt.my[e] & wybits);
           const uint32_t bal = __ballot_sync(0xffffffffu, hit);
           if (hit) sm.list[gw][len + __popc(bal & ((1u << lane) - 1u))] = (uint16_t)e;
           len += __popc(bal);
@@ -327,59 +355,53 @@ __global__ void __launch_bounds__(NT, NT == 512 ? 2 : (NT == 256 ? 5 : 8)) k_ble
       }
       if (!all_done) {
         if constexpr (PPT == 1) {
-          // Two splats per iteration: the second one's alpha is computed
-          // while the first one is accumulated.
+          // Two splats per iteration, without branches on alpha: a splat
+          // below the alpha test contributes alpha = 0, which leaves C and T
+          // unchanged bit for bit; the second splat is dropped (alpha = 0)
+          // when the first one saturated the pixel.
           const float rowc = (float)(oy + ly0) + 0.5f, lxf = (float)lx, lyf = (float)ly0;
           const uint32_t ybit = 1u << ly0, xbit = 1u << lx;
+          const uint16_t* lst = sm.list[gw];
           uint32_t k = 0;
           for (; k + 1 < len; k += 2) {
-            const uint32_t j0 = sm.list[gw][k], j1 = sm.list[gw][k + 1];
-            const float4 a0 = sm.a[j0], b0 = sm.b[j0];
-            const float4 a1 = sm.a[j1], b1 = sm.b[j1];
-            const bool in0 = !EXACT || ((sm.mx[j0] & xbit) && (sm.my[j0] & ybit));
-            const bool in1 = !EXACT || ((sm.mx[j1] & xbit) && (sm.my[j1] & ybit));
+            const uint32_t jj = *reinterpret_cast<const uint32_t*>(lst + k);  // k even: 4-byte aligned
+            const uint32_t j0 = jj & 0xFFFFu, j1 = jj >> 16;
+            const float4 a0 = bt.a[j0], b0 = bt.b[j0];
+            const float4 a1 = bt.a[j1], b1 = bt.b[j1];
+            const bool in0 = !EXACT || ((bt.mx[j0] & xbit) && (bt.my[j0] & ybit));
+            const bool in1 = !EXACT || ((bt.mx[j1] & xbit) && (bt.my[j1] & ybit));
             const float al0 = splat_alpha<EXACT>(in0, a0, b0, fx05, gbase, lanef, rowc, lxf, lyf);
             const float al1 = splat_alpha<EXACT>(in1, a1, b1, fx05, gbase, lanef, rowc, lxf, lyf);
-            if (al0 > 0.0f) {
-              float r_, g_, b_;
-              staged_colour<EXACT>(b0, sm.c[j0], r_, g_, b_);
-              accumulate<EXACT>(al0, r_, g_, b_, T[0], cr[0], cg[0], cb[0]);
-              if (T[0] < kTMin) {
-                done[0] = true;
-                break;
-              }
-            }
-            if (al1 > 0.0f) {
-              float r_, g_, b_;
-              staged_colour<EXACT>(b1, sm.c[j1], r_, g_, b_);
-              accumulate<EXACT>(al1, r_, g_, b_, T[0], cr[0], cg[0], cb[0]);
-              if (T[0] < kTMin) {
-                done[0] = true;
-                break;
-              }
+            float r_, g_, b_;
+            staged_colour<EXACT>(b0, bt.c[j0], r_, g_, b_);
+            accumulate<EXACT>(al0, r_, g_, b_, T[0], cr[0], cg[0], cb[0]);
+            const bool sat0 = T[0] < kTMin;
+            staged_colour<EXACT>(b1, bt.c[j1], r_, g_, b_);
+            accumulate<EXACT>(sat0 ? 0.0f : al1, r_, g_, b_, T[0], cr[0], cg[0], cb[0]);
+            if (sat0 || T[0] < kTMin) {
+              done[0] = true;
+              break;
             }
           }
           if (!done[0] && k < len) {
-            const uint32_t j0 = sm.list[gw][k];
-            const float4 a0 = sm.a[j0], b0 = sm.b[j0];
-            const bool in0 = !EXACT || ((sm.mx[j0] & xbit) && (sm.my[j0] & ybit));
+            const uint32_t j0 = lst[k];
+            const float4 a0 = bt.a[j0], b0 = bt.b[j0];
+            const bool in0 = !EXACT || ((bt.mx[j0] & xbit) && (bt.my[j0] & ybit));
             const float al0 = splat_alpha<EXACT>(in0, a0, b0, fx05, gbase, lanef, rowc, lxf, lyf);
-            if (al0 > 0.0f) {
-              float r_, g_, b_;
-              staged_colour<EXACT>(b0, sm.c[j0], r_, g_, b_);
-              accumulate<EXACT>(al0, r_, g_, b_, T[0], cr[0], cg[0], cb[0]);
-              if (T[0] < kTMin) done[0] = true;
-            }
+            float r_, g_, b_;
+            staged_colour<EXACT>(b0, bt.c[j0], r_, g_, b_);
+            accumulate<EXACT>(al0, r_, g_, b_, T[0], cr[0], cg[0], cb[0]);
+            if (T[0] < kTMin) done[0] = true;
           }
           all_done = done[0];
         } else {
           const uint32_t xbit = 1u << lx;
           for (uint32_t k = 0; k < len && !all_done; k++) {
             const uint32_t j = sm.list[gw][k];
-            const float4 a = sm.a[j], b = sm.b[j];
-            const uint32_t mx = sm.mx[j], my = sm.my[j];
+            const float4 a = bt.a[j], b = bt.b[j];
+            const uint32_t mx = bt.mx[j], my = bt.my[j];
             float red, green, blue;
-            staged_colour<EXACT>(b, sm.c[j], red, green, blue);
+            staged_colour<EXACT>(b, bt.c[j], red, green, blue);
             all_done = true;
 #pragma unroll
             for (int q = 0; q < PPT; q++) {
@@ -398,6 +420,10 @@ __global__ void __launch_bounds__(NT, NT == 512 ? 2 : (NT == 256 ? 5 : 8)) k_ble
           }
         }
       }
+      const uint32_t nxt = start + 2 * G + gt;
+      if (has) stage(sm.bt[buf ^ 1u]);  // batch start + G
+      has = nxt < n;
+      if (has) nr = rec[(uint32_t)pairs[begin + nxt]];
       if (count(!all_done) == 0) break;
     }
 
@@ -482,7 +508,8 @@ namespace {
 
 template <bool EXACT, int TW, int TH, int NT>
 cudaError_t launch_blend_t(const ViewTask* table, uint32_t n_views, uint32_t n_tiles, const uint64_t* pairs,
-                           const uint2* ranges, DevState* st, int num_sms, cudaStream_t stream) {
+                           const uint2* ranges, const uint32_t* order, DevState* st, int num_sms,
+                           cudaStream_t stream) {
   using S = BlendShape<TW, TH, NT>;
   const int smem = (int)(S::NG * sizeof(GroupSmem<TW, TH, NT>));
   // Resident CTAs per SM, looked up once per instantiation.
@@ -498,16 +525,17 @@ cudaError_t launch_blend_t(const ViewTask* table, uint32_t n_views, uint32_t n_t
   }
   const uint64_t want = ((uint64_t)n_tiles + S::NG - 1) / S::NG;
   const uint32_t grid = (uint32_t)std::min<uint64_t>(want, (uint64_t)num_sms * (uint64_t)o);
-  k_blend<EXACT, TW, TH, NT><<<grid, NT, smem, stream>>>(table, n_views, n_tiles, pairs, ranges, st);
+  k_blend<EXACT, TW, TH, NT><<<grid, NT, smem, stream>>>(table, n_views, n_tiles, pairs, ranges, order, st);
   return cudaGetLastError();
 }
 
 template <bool EXACT>
 cudaError_t launch_blend_e(const ViewTask* table, uint32_t n_views, uint32_t n_tiles, const uint64_t* pairs,
-                           const uint2* ranges, const BlendConfig& c, DevState* st, int num_sms, cudaStream_t s) {
+                           const uint2* ranges, const uint32_t* order, const BlendConfig& c, DevState* st,
+                           int num_sms, cudaStream_t s) {
 #define SPLAT_BLEND(TW, TH, NT)                                                                      \
   if (c.tile_w == TW && c.tile_h == TH && c.threads == NT)                                           \
-    return launch_blend_t<EXACT, TW, TH, NT>(table, n_views, n_tiles, pairs, ranges, st, num_sms, s);
+    return launch_blend_t<EXACT, TW, TH, NT>(table, n_views, n_tiles, pairs, ranges, order, st, num_sms, s);
   SPLAT_BLEND(16, 16, 256)
   SPLAT_BLEND(16, 16, 128)
   SPLAT_BLEND(16, 16, 512)
@@ -524,11 +552,12 @@ cudaError_t launch_blend_e(const ViewTask* table, uint32_t n_views, uint32_t n_t
 }  // namespace
 
 cudaError_t launch_blend(const ViewTask* table, uint32_t n_views, uint32_t n_tiles, const uint64_t* pairs,
-                         const uint2* ranges, bool exact, const BlendConfig& cfg, DevState* st, int num_sms,
+                         const uint2* ranges, const uint32_t* order, bool exact, const BlendConfig& cfg, DevState* st, int num_sms,
                          cudaStream_t stream, uint32_t* launches) {
   if (n_tiles == 0) return cudaSuccess;
-  const cudaError_t e = exact ? launch_blend_e<true>(table, n_views, n_tiles, pairs, ranges, cfg, st, num_sms, stream)
-                              : launch_blend_e<false>(table, n_views, n_tiles, pairs, ranges, cfg, st, num_sms, stream);
+  const cudaError_t e =
+      exact ? launch_blend_e<true>(table, n_views, n_tiles, pairs, ranges, order, cfg, st, num_sms, stream)
+            : launch_blend_e<false>(table, n_views, n_tiles, pairs, ranges, order, cfg, st, num_sms, stream);
   if (e == cudaSuccess) *launches += 1;
   return e;
 }

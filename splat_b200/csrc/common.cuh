@@ -88,6 +88,22 @@ struct __align__(16) BinInfo {
 constexpr uint32_t kWarpSortCap = 512;
 constexpr uint32_t kMidSortCap = 4096;
 
+// Tiles by pair count, heaviest class first: > 4096 (the long sort), 2049 -
+// 4096, 1025 - 2048, 513 - 1024 (the mid sort), 257 - 512, 1 - 256, empty.
+// k_tile_ranges appends every tile to its class's list (kTileClasses lists
+// of n_tiles entries each); the blend and the mid sort take their tiles in
+// class order, so no long tile starts last.
+constexpr int kTileClasses = 7;
+__host__ __device__ constexpr uint32_t tile_class(uint32_t len) {
+  return len > kMidSortCap ? 0u
+         : len > 2048u     ? 1u
+         : len > 1024u     ? 2u
+         : len > kWarpSortCap ? 3u
+         : len > 256u      ? 4u
+         : len > 0u        ? 5u
+                           : 6u;
+}
+
 // Frame state in device memory, cleared at the start of every frame (or
 // batch). Followed in the same allocation by the per-view counters and the
 // tile-scan chunk sums, cleared with it (FrameCounters).
@@ -95,10 +111,10 @@ struct DevState {
   unsigned long long visible;      // splats that survived culling (all views)
   unsigned long long total_pairs;  // (splat, tile) pairs, may exceed the capacity
   unsigned int error;
-  unsigned int mid_tiles;          // tiles with (kWarpSortCap, kMidSortCap] pairs
-  unsigned int long_tiles;         // tiles with more than kMidSortCap pairs
   unsigned int fp64_conics;        // splats whose 2D conic was recomputed in FP64
-  unsigned int blend_next;         // the persistent blend's next tile
+  unsigned int blend_next;         // the persistent blend's next work item
+  unsigned int mid_next;           // the mid sort's next work item
+  unsigned int cls[kTileClasses];  // tiles per class (tile_class)
   unsigned int pad;
 };
 
@@ -195,12 +211,12 @@ struct BinLaunch {
   size_t counts_bytes;
 };
 cudaError_t launch_binning(const ViewTask* table, const BinLaunch& bl, uint32_t* totals, uint2* ranges,
-                           uint32_t* mid_list, uint32_t* long_list, uint64_t* pairs, uint64_t* pairs_alt,
+                           uint32_t* order, uint64_t* pairs, uint64_t* pairs_alt,
                            uint64_t cap, const FrameCounters& fc, int num_sms, size_t max_smem, cudaStream_t stream,
                            uint32_t* launches);
 // (d) blend + downsample over the depth-sorted buckets of every view.
 cudaError_t launch_blend(const ViewTask* table, uint32_t n_views, uint32_t n_tiles, const uint64_t* pairs,
-                         const uint2* ranges, bool exact, const BlendConfig& cfg, DevState* st, int num_sms,
+                         const uint2* ranges, const uint32_t* order, bool exact, const BlendConfig& cfg, DevState* st, int num_sms,
                          cudaStream_t stream, uint32_t* launches);
 // Half-block terminal cells (SPLAT_CELLS_*) of a frame of width w.
 cudaError_t launch_cells(const uint8_t* frame, uint32_t w, uint32_t cols, uint32_t rows, uint32_t mode, uint8_t* cells,

@@ -38,8 +38,7 @@ struct splat_cuda_handle {
   uint32_t* counts = nullptr;     // bin_rows x tiles
   size_t counts_cap = 0;          // words
   uint32_t* totals = nullptr;     // tiles
-  uint32_t* mid_list = nullptr;   // tiles
-  uint32_t* long_list = nullptr;  // tiles
+  uint32_t* order = nullptr;      // kTileClasses x tiles (tile_class lists)
   uint64_t ranges_cap = 0;        // tiles
   size_t max_smem = 48 * 1024;
   uint8_t* out_dev = nullptr;

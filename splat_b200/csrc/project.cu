@@ -302,6 +302,10 @@ __global__ void __launch_bounds__(256) k_project_batch(const ViewTask* __restric
 // is the splat's 16 latents and its view direction; the three layers are
 // tcgen05.mma groups with their epilogues between. The record is written by
 // the projection and its colour filled in after.
+__device__ __forceinline__ void l2_prefetch(const void* p) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
 constexpr uint32_t kLearnedThreads = 128;
 constexpr uint32_t kLearnedTmemCols = 64;  // z1, then z2, then z3 (16)
 
@@ -371,6 +375,14 @@ __global__ void __launch_bounds__(kLearnedThreads, 7)
     bool vis = false, used_fp64 = false;
     float dir[3] = {0.f, 0.f, 0.f};
     uint4 l0 = make_uint4(0, 0, 0, 0), l1 = l0;
+    // The CTA's next tile of the same view is brought into L2 while this
+    // one is projected and run through the MLP.
+    const uint64_t i_next = i + (uint64_t)gridDim.x * mlp::kRows;
+    if (i_next < n) {
+      l2_prefetch(t.s.pos_k + i_next);
+      l2_prefetch(t.s.geom16 + i_next);
+      l2_prefetch(t.s.lat16 + 2 * i_next);
+    }
     if (i < n) {
       l0 = __ldg(t.s.lat16 + 2 * i);  // in flight during the projection
       l1 = __ldg(t.s.lat16 + 2 * i + 1);
