@@ -426,13 +426,14 @@ def run_ours(args):
         times = {"project": stage["project_ms"], "sort": stage["sort_ms"], "raster": stage["raster_ms"]}
         dom = max(times, key=times.get)
         achieved = bytes_stage[dom] / (times[dom] / 1e3) / 1e9
-        traffic = None
+        traffic = traffic_src = None
         prof = os.path.join(ROOT, "profiles", "traffic.json")
         if os.path.exists(prof):
             try:
-                traffic = json.load(open(prof)).get(args.config, {}).get(dom)
+                entry = json.load(open(prof)).get(args.config, {})
+                traffic, traffic_src = entry.get(dom), entry.get("source")
             except Exception:
-                traffic = None
+                traffic = traffic_src = None
         load = scene_load(source, dev) if cfg["precision"] == "fp32" else None
         cpu = None
         if not args.no_cpu_baseline:
@@ -454,15 +455,16 @@ def run_ours(args):
             "gsplat_tiles_per_s": P * value / world / 1e9,
             "stages_ms": stage,
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "algorithmic_bytes": bytes_stage[dom]},
+                         "frac": achieved / peak, "traffic": traffic, "traffic_source": traffic_src,
+                         "peak_kind": peak_kind, "algorithmic_bytes": bytes_stage[dom]},
             "frame_hbm": {"bytes": sum(bytes_stage.values()),
                           "achieved_gbs": sum(bytes_stage.values()) * value / world / 1e9},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e, "unit": "frames/s", "h2d_bytes_per_step": 56,
                     "d2h_bytes_per_step": W * H * 3 + 32,
                     "note": "input per step: the 56-byte view, passed as kernel parameters (the scene stays "
-                            "resident); output: the u8 frame into pinned host memory plus the 32-byte frame state"},
+                            "resident); output: the u8 frame, written by the blend straight into the caller's "
+                            "pinned host buffer through its device mapping, plus the 32-byte frame state"},
             "clocks": clk.summary(),
             "gpu_launches": launches,
         }

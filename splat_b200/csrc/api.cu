@@ -135,6 +135,18 @@ bool is_pinned_host(const void* p) {
   return a.type == cudaMemoryTypeHost;
 }
 
+// The device's address of page-locked host memory it can write directly
+// (mapped pinned memory: every cudaHostAlloc / cudaMallocHost buffer under
+// unified addressing), or null.
+uint8_t* mapped_host(void* p) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return a.type == cudaMemoryTypeHost ? static_cast<uint8_t*>(a.devicePointer) : nullptr;
+}
+
 }  // namespace
 
 namespace splat {
@@ -190,8 +202,9 @@ void set_tile_shape(FrameParams& p, uint32_t tile_w, uint32_t tile_h) {
 
 namespace {
 
-// Enqueues one frame into dev_out (no host synchronisation).
-int enqueue_frame(splat_cuda_handle* h, const FrameParams& fp_in, uint8_t* dev_out) {
+// Enqueues one frame into dev_out (no host synchronisation); host_mapped:
+// dev_out is the device address of mapped pinned host memory.
+int enqueue_frame(splat_cuda_handle* h, const FrameParams& fp_in, uint8_t* dev_out, bool host_mapped = false) {
   FrameParams fp = fp_in;
   set_tile_shape(fp, h->blend.tile_w, h->blend.tile_h);
   const uint64_t tiles = (uint64_t)fp.tiles_x * fp.tiles_y;
@@ -232,7 +245,7 @@ int enqueue_frame(splat_cuda_handle* h, const FrameParams& fp_in, uint8_t* dev_o
      "binning kernels");
   if (h->stage_events) CK(cudaEventRecord(h->ev[2], s), "event");
   CK(launch_blend(h->table, 1, (uint32_t)tiles, h->pairs[0], h->ranges, h->order, h->exact, h->blend, fc.st,
-                  h->num_sms, s, &h->launches),
+                  h->num_sms, s, &h->launches, host_mapped),
      "blend kernel");
   if (scratch) CK(launch_downsample(fp, h->full_dev, dev_out, s, &h->launches), "downsample kernel");
   if (h->stage_events) CK(cudaEventRecord(h->ev[3], s), "event");
@@ -492,7 +505,12 @@ SPLAT_API int splat_cuda_render(splat_cuda_handle* h, const splat_view_desc* vie
   const FrameParams fp = make_params(*view, width, height, bg, f);
   const size_t bytes = (size_t)fp.out_w * fp.out_h * 3;
   if ((rc = ensure_size(h, 0, 0, bytes, 0))) return rc;
-  const bool direct = bytes && is_pinned_host(rgb_out);
+  // Pinned output the device can address: the blend (or the downsample)
+  // writes the frame straight into it, overlapped with the frame's own
+  // compute, instead of a copy after the frame. Other pinned memory gets one
+  // copy; pageable memory goes through the handle's pinned staging buffer.
+  uint8_t* const mapped = bytes ? mapped_host(rgb_out) : nullptr;
+  const bool direct = bytes && (mapped || is_pinned_host(rgb_out));
   if (!direct && bytes > h->stage_cap) {
     if (h->stage) cudaFreeHost(h->stage);
     h->stage = nullptr;
@@ -501,8 +519,8 @@ SPLAT_API int splat_cuda_render(splat_cuda_handle* h, const splat_view_desc* vie
     h->stage_cap = bytes;
   }
   for (int attempt = 0; attempt < 8; attempt++) {
-    if ((rc = enqueue_frame(h, fp, h->out_dev))) return rc;
-    if (bytes)
+    if ((rc = enqueue_frame(h, fp, mapped ? mapped : h->out_dev, mapped != nullptr))) return rc;
+    if (bytes && !mapped)
       CK(cudaMemcpyAsync(direct ? rgb_out : h->stage, h->out_dev, bytes, cudaMemcpyDeviceToHost, h->stream),
          "copy frame");
     int regrown = 0;

@@ -221,7 +221,7 @@ struct __align__(16) GroupSmem {
   uint32_t work;
 };
 
-template <bool EXACT, int TW, int TH, int NT>
+template <bool EXACT, int TW, int TH, int NT, bool ROWS>
 __global__ void __launch_bounds__(NT, NT == 512 ? 2 : (NT == 256 ? 5 : 8)) k_blend(const ViewTask* __restrict__ table, uint32_t n_views, uint32_t n_tiles,
                                               const uint64_t* __restrict__ pairs, const uint2* __restrict__ ranges,
                                               const uint32_t* __restrict__ order, DevState* st) {
@@ -432,13 +432,21 @@ __global__ void __launch_bounds__(NT, NT == 512 ? 2 : (NT == 256 ? 5 : 8)) k_ble
     uint8_t* __restrict__ out = tv->out;
     const float bg0 = tv->fp.bg[0], bg1 = tv->fp.bg[1], bg2 = tv->fp.bg[2];
     const bool fused = f > 1 && TW % f == 0 && TH % f == 0;
+    // ROWS (frames in mapped pinned host memory; f == 1, the tile inside the
+    // frame, rows 4-byte aligned): the tile leaves as whole 4-byte words of
+    // its rows, consecutive threads writing consecutive words, so the bus
+    // carries contiguous row segments rather than single bytes. Device
+    // frames keep the per-pixel byte stores (a separate instantiation: the
+    // word path costs the device-frame kernel about 4 %).
+    constexpr uint32_t kRowWords = (TW * 3) / 4;  // TW is a multiple of 8
+    const bool rows = ROWS && f == 1 && W % 4u == 0 && ox + TW <= W && (reinterpret_cast<uintptr_t>(out) & 3u) == 0;
 #pragma unroll
     for (int k = 0; k < PPT; k++) {
       const uint32_t ly = ly0 + k, py = oy + ly;
       const uint32_t qr = to_u8(__fadd_rn(cr[k], __fmul_rn(T[k], bg0)));
       const uint32_t qg = to_u8(__fadd_rn(cg[k], __fmul_rn(T[k], bg1)));
       const uint32_t qb = to_u8(__fadd_rn(cb[k], __fmul_rn(T[k], bg2)));
-      if (fused) {
+      if (fused || rows) {
         sm.px[ly * TW + lx] = qr | (qg << 8) | (qb << 16);
       } else if (px < W && py < H) {
         // f == 1: the frame; other factors: the full-resolution scratch frame.
@@ -446,6 +454,21 @@ __global__ void __launch_bounds__(NT, NT == 512 ? 2 : (NT == 256 ? 5 : 8)) k_ble
         o[0] = (uint8_t)qr;
         o[1] = (uint8_t)qg;
         o[2] = (uint8_t)qb;
+      }
+    }
+    if (ROWS && rows) {
+      sync();
+      for (uint32_t e = gt; e < TH * kRowWords; e += G) {
+        const uint32_t ly = e / kRowWords, b0 = 4u * (e % kRowWords), py = oy + ly;  // b0: byte of the row
+        if (py < H) {
+          uint32_t v = 0u;
+#pragma unroll
+          for (uint32_t r = 0; r < 4; r++) {
+            const uint32_t bb = b0 + r;
+            v |= ((sm.px[ly * TW + bb / 3u] >> (8u * (bb % 3u))) & 255u) << (8u * r);
+          }
+          *reinterpret_cast<uint32_t*>(out + ((size_t)py * W + ox) * 3 + b0) = v;
+        }
       }
     }
     if (fused) {
@@ -506,36 +529,45 @@ bool blend_config_supported(const BlendConfig& c) {
 
 namespace {
 
-template <bool EXACT, int TW, int TH, int NT>
+template <bool EXACT, int TW, int TH, int NT, bool ROWS>
 cudaError_t launch_blend_t(const ViewTask* table, uint32_t n_views, uint32_t n_tiles, const uint64_t* pairs,
                            const uint2* ranges, const uint32_t* order, DevState* st, int num_sms,
                            cudaStream_t stream) {
   using S = BlendShape<TW, TH, NT>;
+  const auto kernel = k_blend<EXACT, TW, TH, NT, ROWS>;
   const int smem = (int)(S::NG * sizeof(GroupSmem<TW, TH, NT>));
   // Resident CTAs per SM, looked up once per instantiation.
   static std::atomic<int> occ{0};
   int o = occ.load(std::memory_order_relaxed);
   if (o == 0) {
-    cudaError_t e = cudaFuncSetAttribute(k_blend<EXACT, TW, TH, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_blend<EXACT, TW, TH, NT>, NT, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kernel, NT, smem);
     if (e != cudaSuccess) return e;
     if (o < 1) o = 1;
     occ.store(o, std::memory_order_relaxed);
   }
   const uint64_t want = ((uint64_t)n_tiles + S::NG - 1) / S::NG;
   const uint32_t grid = (uint32_t)std::min<uint64_t>(want, (uint64_t)num_sms * (uint64_t)o);
-  k_blend<EXACT, TW, TH, NT><<<grid, NT, smem, stream>>>(table, n_views, n_tiles, pairs, ranges, order, st);
+  kernel<<<grid, NT, smem, stream>>>(table, n_views, n_tiles, pairs, ranges, order, st);
   return cudaGetLastError();
 }
 
 template <bool EXACT>
 cudaError_t launch_blend_e(const ViewTask* table, uint32_t n_views, uint32_t n_tiles, const uint64_t* pairs,
                            const uint2* ranges, const uint32_t* order, const BlendConfig& c, DevState* st,
-                           int num_sms, cudaStream_t s) {
-#define SPLAT_BLEND(TW, TH, NT)                                                                      \
-  if (c.tile_w == TW && c.tile_h == TH && c.threads == NT)                                           \
-    return launch_blend_t<EXACT, TW, TH, NT>(table, n_views, n_tiles, pairs, ranges, order, st, num_sms, s);
+                           int num_sms, cudaStream_t s, bool rows) {
+  // The row-word variant for mapped host frames exists for the default
+  // blend (16x16 tiles, 512 threads); other shapes write such frames byte by
+  // byte, which is as correct.
+#define SPLAT_BLEND(TW, TH, NT)                                                                        \
+  if (c.tile_w == TW && c.tile_h == TH && c.threads == NT) {                                           \
+    if constexpr (!EXACT && TW == 16 && TH == 16 && NT == 512)                                         \
+      if (rows) return launch_blend_t<EXACT, TW, TH, NT, true>(table, n_views, n_tiles, pairs, ranges, \
+                                                               order, st, num_sms, s);                 \
+    return launch_blend_t<EXACT, TW, TH, NT, false>(table, n_views, n_tiles, pairs, ranges, order, st, \
+                                                    num_sms, s);                                       \
+  }
   SPLAT_BLEND(16, 16, 256)
   SPLAT_BLEND(16, 16, 128)
   SPLAT_BLEND(16, 16, 512)
@@ -552,12 +584,12 @@ cudaError_t launch_blend_e(const ViewTask* table, uint32_t n_views, uint32_t n_t
 }  // namespace
 
 cudaError_t launch_blend(const ViewTask* table, uint32_t n_views, uint32_t n_tiles, const uint64_t* pairs,
-                         const uint2* ranges, const uint32_t* order, bool exact, const BlendConfig& cfg, DevState* st, int num_sms,
-                         cudaStream_t stream, uint32_t* launches) {
+                         const uint2* ranges, const uint32_t* order, bool exact, const BlendConfig& cfg, DevState* st,
+                         int num_sms, cudaStream_t stream, uint32_t* launches, bool host_rows) {
   if (n_tiles == 0) return cudaSuccess;
   const cudaError_t e =
-      exact ? launch_blend_e<true>(table, n_views, n_tiles, pairs, ranges, order, cfg, st, num_sms, stream)
-            : launch_blend_e<false>(table, n_views, n_tiles, pairs, ranges, order, cfg, st, num_sms, stream);
+      exact ? launch_blend_e<true>(table, n_views, n_tiles, pairs, ranges, order, cfg, st, num_sms, stream, host_rows)
+            : launch_blend_e<false>(table, n_views, n_tiles, pairs, ranges, order, cfg, st, num_sms, stream, host_rows);
   if (e == cudaSuccess) *launches += 1;
   return e;
 }

@@ -215,9 +215,10 @@ cudaError_t launch_binning(const ViewTask* table, const BinLaunch& bl, uint32_t*
                            uint64_t cap, const FrameCounters& fc, int num_sms, size_t max_smem, cudaStream_t stream,
                            uint32_t* launches);
 // (d) blend + downsample over the depth-sorted buckets of every view.
+// host_rows: the views' frames are mapped pinned host memory (see k_blend).
 cudaError_t launch_blend(const ViewTask* table, uint32_t n_views, uint32_t n_tiles, const uint64_t* pairs,
-                         const uint2* ranges, const uint32_t* order, bool exact, const BlendConfig& cfg, DevState* st, int num_sms,
-                         cudaStream_t stream, uint32_t* launches);
+                         const uint2* ranges, const uint32_t* order, bool exact, const BlendConfig& cfg, DevState* st,
+                         int num_sms, cudaStream_t stream, uint32_t* launches, bool host_rows = false);
 // Half-block terminal cells (SPLAT_CELLS_*) of a frame of width w.
 cudaError_t launch_cells(const uint8_t* frame, uint32_t w, uint32_t cols, uint32_t rows, uint32_t mode, uint8_t* cells,
                          cudaStream_t stream, uint32_t* launches);

@@ -356,6 +356,37 @@ def test_device_path_matches_host_path():
     r.close()
 
 
+@pytest.mark.parametrize("size,f,cfg", [((1920, 1080), 1, (16, 16, 512)), ((1920, 1080), 1, (32, 16, 256)),
+                                        ((1920, 1080), 1, (8, 8, 256)), ((333, 191), 1, (16, 16, 512)),
+                                        ((320, 192), 2, (16, 16, 512)), ((333, 191), 3, (16, 16, 512))])
+def test_frame_written_into_mapped_pinned_memory(size, f, cfg):
+    """Pinned host output is written by the kernels through its device
+    mapping (4-byte words of tile rows where the rows are aligned, bytes
+    elsewhere): the frame equals the one copied out of device memory and the
+    one staged for pageable memory, at aligned and ragged widths and with the
+    fused and unfused downsample."""
+    import torch
+
+    s = scene("clusters3")
+    w, h = size
+    ow, oh = w // f, h // f
+    r = CudaRenderer(s)
+    r.set_blend_config(*cfg)
+    for v in orbit_views(s, 3)[1:]:
+        host, _ = cuda_frame(r, v, w, h, (0.1, 0.2, 0.3), downsample=f)
+        dev = torch.zeros(ow * oh * 3, dtype=torch.uint8, device="cuda")
+        torch.cuda.synchronize()
+        r.render_device(v, w, h, (0.1, 0.2, 0.3), dev.data_ptr(), dev.numel(), downsample=f)
+        _, regrown = r.finish()
+        assert not regrown
+        pinned = torch.full((ow * oh * 3,), 7, dtype=torch.uint8).pin_memory()
+        for _ in range(2):
+            r.render_into(v, w, h, (0.1, 0.2, 0.3), pinned.data_ptr(), pinned.numel(), downsample=f)
+            assert np.array_equal(pinned.numpy().reshape(oh, ow, 3), host)
+        assert np.array_equal(dev.cpu().numpy().reshape(oh, ow, 3), host)
+    r.close()
+
+
 @pytest.mark.parametrize("mode", ["truecolor", "ansi256"])
 @pytest.mark.parametrize("size,f", [((320, 192), 2), ((333, 191), 3), ((161, 95), 1)])
 def test_terminal_cells_match_widget(oracle, mode, size, f):
