@@ -687,7 +687,8 @@ def run_learned(args):
             "e2e": {"value": e2e, "unit": "frames/s", "h2d_bytes_per_step": 56,
                     "d2h_bytes_per_step": W * H * 3 + 32,
                     "note": "input per step: the 56-byte view (the trained scene stays resident); output: the u8 "
-                            "frame into pinned host memory plus the 32-byte frame state"},
+                            "frame, written by the blend straight into the caller's pinned host buffer through its "
+                            "device mapping, plus the 32-byte frame state"},
             "clocks": clk.summary(),
             "gpu_launches": launches,
         }
