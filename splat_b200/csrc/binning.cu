@@ -273,18 +273,21 @@ __global__ void __launch_bounds__(kBinThreads) k_bin_scatter(const ViewTask* __r
   });
 }
 
-// Tiles of at most kWarpSortCap pairs: one warp per tile.
-__global__ void __launch_bounds__(256, 3) k_sort_small(const uint2* __restrict__ ranges, uint32_t tiles,
-                                                    uint64_t* __restrict__ pairs) {
+// Tiles of at most kWarpSortCap pairs (classes 4 and 5, the heavier class
+// first): one warp per tile, persistent warps striding over the two lists.
+__global__ void __launch_bounds__(256, 3) k_sort_small(const uint2* __restrict__ ranges,
+                                                    const uint32_t* __restrict__ order, uint32_t n_tiles,
+                                                    uint64_t* __restrict__ pairs, const DevState* st) {
   __shared__ uint64_t s_scratch[8][kWarpSortCap];
   __shared__ uint32_t s_counts[8][256];
   const uint32_t warp = threadIdx.x >> 5;
-  const uint32_t tile = blockIdx.x * 8 + warp;
-  if (tile >= tiles) return;
-  const uint2 r = ranges[tile];
-  const uint32_t n = r.y - r.x;
-  if (n < 2 || n > kWarpSortCap) return;
-  warp_sort_tile(pairs + r.x, n, s_scratch[warp], s_counts[warp]);
+  const uint32_t n4 = st->cls[4], n5 = st->cls[5];
+  for (uint32_t li = blockIdx.x * 8 + warp; li < n4 + n5; li += gridDim.x * 8) {
+    const uint32_t tile = li < n4 ? order[4 * (size_t)n_tiles + li] : order[5 * (size_t)n_tiles + (li - n4)];
+    const uint2 r = ranges[tile];
+    const uint32_t n = r.y - r.x;
+    if (n >= 2) warp_sort_tile(pairs + r.x, n, s_scratch[warp], s_counts[warp]);
+  }
 }
 
 // Tiles of (kWarpSortCap, kMidSortCap] pairs: one CTA per tile, in shared
@@ -495,19 +498,22 @@ cudaError_t launch_binning(const ViewTask* table, const BinLaunch& bl, uint32_t*
   } else {
     k_bin_scatter<false><<<bl.bin_ctas, kBinThreads, 0, stream>>>(table, bl.n_views, ranges, pairs, cap);
   }
-  k_sort_small<<<(bl.n_tiles + 7) / 8, 256, 0, stream>>>(ranges, bl.n_tiles, pairs);
-  // The mid and long sorts loop over their tile lists: as many CTAs as fit
-  // on the device at once (looked up once).
-  static std::atomic<int> occ_mid{0}, occ_long{0};
+  // The sorts loop over their tile lists: as many CTAs as fit on the device
+  // at once (looked up once).
+  static std::atomic<int> occ_small{0}, occ_mid{0}, occ_long{0};
   if (occ_mid.load(std::memory_order_relaxed) == 0 && cs == cudaStreamCaptureStatusNone) {
-    int om = 0, ol = 0;
+    int os = 0, om = 0, ol = 0;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&os, k_sort_small, 256, 0))) return e;
     if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&om, k_sort_mid, kTileThreads, sizeof(MidSmem)))) return e;
     if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ol, k_sort_long, kTileThreads, 0))) return e;
+    occ_small.store(std::max(os, 1), std::memory_order_relaxed);
     occ_long.store(std::max(ol, 1), std::memory_order_relaxed);
     occ_mid.store(std::max(om, 1), std::memory_order_relaxed);
   }
+  const int os = std::max(occ_small.load(std::memory_order_relaxed), 1);
   const int om = std::max(occ_mid.load(std::memory_order_relaxed), 1);
   const int ol = std::max(occ_long.load(std::memory_order_relaxed), 1);
+  k_sort_small<<<num_sms * os, 256, 0, stream>>>(ranges, order, bl.n_tiles, pairs, fc.st);
   k_sort_mid<<<num_sms * om, kTileThreads, sizeof(MidSmem), stream>>>(ranges, order, bl.n_tiles, pairs, fc.st);
   k_sort_long<<<num_sms * ol, kTileThreads, 0, stream>>>(ranges, order, pairs, pairs_alt, cap, fc.st);
   *launches += 7;
