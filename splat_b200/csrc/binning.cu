@@ -146,9 +146,12 @@ __global__ void __launch_bounds__(256) k_bin_colscan(const ViewTask* __restrict_
   const uint32_t t = first + lane;
   const uint32_t per = (rows + 7) / 8;
   const uint32_t r0 = min(rows, warp * per), r1 = min(rows, r0 + per);
+  // Rows are independent loads: unrolled so that several are in flight.
   uint32_t sum = 0;
-  if (t < tiles)
+  if (t < tiles) {
+#pragma unroll 8
     for (uint32_t r = r0; r < r1; r++) sum += counts[(uint64_t)r * tiles + t];
+  }
   s_seg[warp][lane] = sum;
   __syncthreads();
   uint32_t run = 0, total = 0;
@@ -157,6 +160,7 @@ __global__ void __launch_bounds__(256) k_bin_colscan(const ViewTask* __restrict_
     total += s_seg[w][lane];
   }
   if (t < tiles) {
+#pragma unroll 8
     for (uint32_t r = r0; r < r1; r++) {
       const uint32_t c = counts[(uint64_t)r * tiles + t];
       counts[(uint64_t)r * tiles + t] = run;
@@ -260,6 +264,7 @@ __global__ void __launch_bounds__(kBinThreads) k_bin_scatter(const ViewTask* __r
   const BinView b = bin_view(table, n_views);
   const uint2* vr = ranges + b.tile0;
   if (SMEM) {
+#pragma unroll 4
     for (uint32_t t = threadIdx.x; t < b.tiles; t += kBinThreads) s_row[t] = vr[t].x + b.row[t];
     __syncthreads();
   }

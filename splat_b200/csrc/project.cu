@@ -47,6 +47,10 @@ __device__ __forceinline__ void conic_terms(const T c[6], T t0x, T t0y, T t0z, T
   cc = ((t1x * s1x + t1y * s1y) + t1z * s1z) + T(kDilation);
 }
 
+__device__ __forceinline__ void l2_prefetch(const void* p) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
 // F16: the scene is stored in FP16 (positions FP32); the 3D covariance is
 // formed here in FP32, and a 2D covariance whose FP32 determinant falls below
 // kFp64DetBelow is recomputed in FP64.
@@ -61,6 +65,22 @@ __device__ __forceinline__ void project_splat(const FrameParams& fp, const Scene
                                               Record* __restrict__ rec, BinInfo* __restrict__ bin,
                                               float* __restrict__ dbg_proj, float* __restrict__ dbg_color,
                                               bool& vis, bool& used_fp64, float* dir = nullptr) {
+  if constexpr (!LEARNED && DEG > 0) {
+    // The warp's 32 entries of every SH plane are brought into L2 now; the
+    // loads that read them come after the geometry and the culling tests.
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t base = i - lane, last = min(base + 31, s.n - 1);
+    constexpr uint32_t kPlanes = F16 ? (DEG + 1) * (DEG + 1) * 3 : ((DEG + 1) * (DEG + 1) - 1) * 3;
+    for (uint32_t p = lane; p < kPlanes; p += 32) {
+      if (F16) {
+        l2_prefetch(s.sh16 + (uint64_t)p * s.n + base);
+        l2_prefetch(s.sh16 + (uint64_t)p * s.n + last);
+      } else {
+        l2_prefetch(s.sh + (uint64_t)p * s.n + base);
+        l2_prefetch(s.sh + (uint64_t)p * s.n + last);
+      }
+    }
+  }
   {
     float px, py, pz, opacity, k;
     uint4 g16 = make_uint4(0, 0, 0, 0);
@@ -302,10 +322,6 @@ __global__ void __launch_bounds__(256) k_project_batch(const ViewTask* __restric
 // is the splat's 16 latents and its view direction; the three layers are
 // tcgen05.mma groups with their epilogues between. The record is written by
 // the projection and its colour filled in after.
-__device__ __forceinline__ void l2_prefetch(const void* p) {
-  asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
-}
-
 constexpr uint32_t kLearnedThreads = 128;
 constexpr uint32_t kLearnedTmemCols = 64;  // z1, then z2, then z3 (16)
 
