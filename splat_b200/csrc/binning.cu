@@ -378,7 +378,7 @@ __global__ void __launch_bounds__(kTileThreads) k_sort_long(const uint2* __restr
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const uint32_t nlong = st->cls[0];
   for (uint32_t li = blockIdx.x; li < nlong; li += gridDim.x) {
-    const uint2 r = ranges[long_list[li]];  // within the capacity (k_bin_tilescan)
+    const uint2 r = ranges[long_list[li]];  // within the capacity (k_tile_ranges)
     const uint32_t b = r.x, n = r.y - r.x;
     uint32_t a = 0xFFFFFFFFu, o = 0u;
     for (uint32_t e = tid; e < n; e += kTileThreads) {
