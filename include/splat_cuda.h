@@ -171,6 +171,18 @@ int splat_cuda_render(splat_cuda_handle* h, const splat_view_desc* view, uint32_
                       const float bg[3], uint32_t downsample, uint8_t* rgb_out, size_t out_bytes,
                       splat_render_stats* stats);
 
+/* Rows [row0, row0 + rows) of the width x height frame splat_cuda_render
+ * would produce, bit for bit, into rgb_out (rows * width * 3 bytes, row0
+ * first): the projection covers the whole frame, the tile binning, sorts and
+ * blend only the tile rows that meet the window. One frame split into row
+ * windows over several devices (each with the scene) is the frame's
+ * tile-ownership split without a record exchange. No downsample. The
+ * reference has no counterpart: its backends render whole frames
+ * (Renderer::render, src/render/mod.rs:89-96). */
+int splat_cuda_render_rows(splat_cuda_handle* h, const splat_view_desc* view, uint32_t width, uint32_t height,
+                           const float bg[3], uint32_t row0, uint32_t rows, uint8_t* rgb_out, size_t out_bytes,
+                           splat_render_stats* stats);
+
 /* As splat_cuda_render, but the frame goes to DEVICE memory dev_out (on the
  * handle's device) and the call only enqueues work on the handle's stream: it
  * does not wait for the GPU. Call splat_cuda_finish before using the stats;

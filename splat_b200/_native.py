@@ -40,7 +40,8 @@ _STATUS_NAMES = {0: "OK", 1: "INVALID_ARG", 2: "OOM", 3: "CAPACITY", 4: "DEVICE"
 # Every symbol include/splat_cuda.h declares.
 EXPORTS = [
     "splat_cuda_abi_version", "splat_cuda_backend_name", "splat_cuda_create", "splat_cuda_create_error",
-    "splat_cuda_render", "splat_cuda_render_device", "splat_cuda_finish", "splat_cuda_set_stream",
+    "splat_cuda_render", "splat_cuda_render_rows", "splat_cuda_render_device", "splat_cuda_finish",
+    "splat_cuda_set_stream",
     "splat_cuda_get_stream", "splat_cuda_set_option", "splat_cuda_get_option", "splat_cuda_debug_dump",
     "splat_cuda_destroy", "splat_cuda_last_error", "splat_cuda_sort_tile_noalloc",
     "splat_cuda_batch_create", "splat_cuda_batch_create_error", "splat_cuda_batch_set_config",
@@ -131,6 +132,8 @@ def lib():
         L.splat_cuda_create_error.restype = ctypes.c_char_p
         L.splat_cuda_render.argtypes = [vp, ctypes.POINTER(ViewDesc), u32, u32, f32p, u32, vp, ctypes.c_size_t,
                                         ctypes.POINTER(RenderStatsC)]
+        L.splat_cuda_render_rows.argtypes = [vp, ctypes.POINTER(ViewDesc), u32, u32, f32p, u32, u32, vp,
+                                             ctypes.c_size_t, ctypes.POINTER(RenderStatsC)]
         L.splat_cuda_render_device.argtypes = [vp, ctypes.POINTER(ViewDesc), u32, u32, f32p, u32, vp,
                                                ctypes.c_size_t]
         L.splat_cuda_finish.argtypes = [vp, ctypes.POINTER(RenderStatsC), ctypes.POINTER(ctypes.c_int)]

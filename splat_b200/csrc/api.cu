@@ -180,6 +180,8 @@ FrameParams make_params(const splat_view_desc& v, uint32_t w, uint32_t hgt, cons
   p.downsample = f;
   p.out_w = w / f;
   p.out_h = hgt / f;
+  p.win_y0 = 0;
+  p.win_rows = hgt;
   return p;
 }
 
@@ -195,7 +197,8 @@ void set_tile_shape(FrameParams& p, uint32_t tile_w, uint32_t tile_h) {
   p.tile_sx = (uint32_t)__builtin_ctz(tile_w);
   p.tile_sy = (uint32_t)__builtin_ctz(tile_h);
   p.tiles_x = (p.w + tile_w - 1) / tile_w;
-  p.tiles_y = (p.h + tile_h - 1) / tile_h;
+  p.win_ty0 = p.win_y0 / tile_h;
+  p.tiles_y = (p.win_y0 + p.win_rows + tile_h - 1) / tile_h - p.win_ty0;
 }
 
 }  // namespace splat
@@ -287,13 +290,19 @@ int finish_frame(splat_cuda_handle* h, splat_render_stats* stats, int* regrown) 
   return SPLAT_OK;
 }
 
-int check_frame_args(splat_cuda_handle* h, const splat_view_desc* view, uint32_t w, uint32_t hgt, const float* bg,
-                     uint32_t f, size_t out_bytes, const void* out) {
+int check_view_args(splat_cuda_handle* h, const splat_view_desc* view, uint32_t w, uint32_t hgt, const float* bg) {
   if (!h) return SPLAT_ERR_INVALID_ARG;
   if (!view || !bg) return fail(h, SPLAT_ERR_INVALID_ARG, "null view or background");
   if (w > SPLAT_MAX_DIM || hgt > SPLAT_MAX_DIM)
     return fail(h, SPLAT_ERR_INVALID_ARG,
                 "frame " + std::to_string(w) + "x" + std::to_string(hgt) + " exceeds the 16384 pixel limit");
+  return SPLAT_OK;
+}
+
+int check_frame_args(splat_cuda_handle* h, const splat_view_desc* view, uint32_t w, uint32_t hgt, const float* bg,
+                     uint32_t f, size_t out_bytes, const void* out) {
+  const int rc = check_view_args(h, view, w, hgt, bg);
+  if (rc) return rc;
   if (f == 0) f = 1;
   const size_t need = (size_t)(w / f) * (hgt / f) * 3;
   if (need && (!out || out_bytes < need))
@@ -492,17 +501,13 @@ SPLAT_API int splat_cuda_finish(splat_cuda_handle* h, splat_render_stats* stats,
   return finish_frame(h, stats, regrown);
 }
 
-SPLAT_API int splat_cuda_render(splat_cuda_handle* h, const splat_view_desc* view, uint32_t width, uint32_t height,
-                                const float bg[3], uint32_t downsample, uint8_t* rgb_out, size_t out_bytes,
-                                splat_render_stats* stats) {
-  const auto t0 = std::chrono::steady_clock::now();
-  if (stats) std::memset(stats, 0, sizeof(*stats));
-  int rc = check_frame_args(h, view, width, height, bg, downsample, out_bytes, rgb_out);
-  if (rc) return rc;
-  if (width == 0 || height == 0) return SPLAT_OK;
-  CK(cudaSetDevice(h->device), "cudaSetDevice");
-  const uint32_t f = downsample ? downsample : 1;
-  const FrameParams fp = make_params(*view, width, height, bg, f);
+namespace {
+
+// A frame (or a window of rows) into caller-owned host memory: bytes =
+// out_w * out_h * 3 of fp.
+int render_to_host(splat_cuda_handle* h, const FrameParams& fp, uint8_t* rgb_out, splat_render_stats* stats,
+                   std::chrono::steady_clock::time_point t0) {
+  int rc = SPLAT_OK;
   const size_t bytes = (size_t)fp.out_w * fp.out_h * 3;
   if ((rc = ensure_size(h, 0, 0, bytes, 0))) return rc;
   // Pinned output the device can address: the blend (or the downsample)
@@ -533,6 +538,42 @@ SPLAT_API int splat_cuda_render(splat_cuda_handle* h, const splat_view_desc* vie
     }
   }
   return fail(h, SPLAT_ERR_CAPACITY, "pair buffers kept overflowing");
+}
+
+}  // namespace
+
+SPLAT_API int splat_cuda_render(splat_cuda_handle* h, const splat_view_desc* view, uint32_t width, uint32_t height,
+                                const float bg[3], uint32_t downsample, uint8_t* rgb_out, size_t out_bytes,
+                                splat_render_stats* stats) {
+  const auto t0 = std::chrono::steady_clock::now();
+  if (stats) std::memset(stats, 0, sizeof(*stats));
+  int rc = check_frame_args(h, view, width, height, bg, downsample, out_bytes, rgb_out);
+  if (rc) return rc;
+  if (width == 0 || height == 0) return SPLAT_OK;
+  CK(cudaSetDevice(h->device), "cudaSetDevice");
+  const uint32_t f = downsample ? downsample : 1;
+  return render_to_host(h, make_params(*view, width, height, bg, f), rgb_out, stats, t0);
+}
+
+SPLAT_API int splat_cuda_render_rows(splat_cuda_handle* h, const splat_view_desc* view, uint32_t width,
+                                     uint32_t height, const float bg[3], uint32_t row0, uint32_t rows,
+                                     uint8_t* rgb_out, size_t out_bytes, splat_render_stats* stats) {
+  const auto t0 = std::chrono::steady_clock::now();
+  if (stats) std::memset(stats, 0, sizeof(*stats));
+  int rc = check_view_args(h, view, width, height, bg);
+  if (rc) return rc;
+  if ((uint64_t)row0 + rows > height)
+    return fail(h, SPLAT_ERR_INVALID_ARG, "rows [row0, row0 + rows) exceed the frame height");
+  const size_t need = (size_t)width * rows * 3;
+  if (need && (!rgb_out || out_bytes < need))
+    return fail(h, SPLAT_ERR_INVALID_ARG, "output buffer smaller than width*rows*3 bytes");
+  if (need == 0) return SPLAT_OK;
+  CK(cudaSetDevice(h->device), "cudaSetDevice");
+  FrameParams fp = make_params(*view, width, height, bg, 1);
+  fp.win_y0 = row0;
+  fp.win_rows = rows;
+  fp.out_h = rows;
+  return render_to_host(h, fp, rgb_out, stats, t0);
 }
 
 SPLAT_API int splat_cuda_render_cells(splat_cuda_handle* h, const splat_view_desc* view, uint32_t width,

@@ -279,9 +279,10 @@ __global__ void __launch_bounds__(NT, NT == 512 ? 2 : (NT == 256 ? 5 : 8)) k_ble
       sync();
       continue;
     }
-    const uint32_t W = tv->fp.w, H = tv->fp.h;
+    // Rows [Y0, Y1) of the frame are rendered; output row = frame row - Y0.
+    const uint32_t W = tv->fp.w, Y0 = tv->fp.win_y0, Y1 = min(tv->fp.h, Y0 + tv->fp.win_rows);
     const Record* __restrict__ rec = tv->rec;
-    const uint32_t ox = (local % tiles_x) * TW, oy = (local / tiles_x) * TH;
+    const uint32_t ox = (local % tiles_x) * TW, oy = (local / tiles_x + tv->fp.win_ty0) * TH;
     const uint32_t px = ox + lx;
 
     // EXACT: dx = lane + ((g*4) + ((ox16 + 0.5) - x)), dy = (py + 0.5) - y
@@ -298,7 +299,7 @@ __global__ void __launch_bounds__(NT, NT == 512 ? 2 : (NT == 256 ? 5 : 8)) k_ble
     for (int k = 0; k < PPT; k++) {
       T[k] = 1.0f;
       cr[k] = cg[k] = cb[k] = 0.0f;
-      done[k] = !(px < W && oy + ly0 + k < H);
+      done[k] = !(px < W && oy + ly0 + k >= Y0 && oy + ly0 + k < Y1);
       all_done = all_done && done[k];
     }
 
@@ -448,9 +449,10 @@ __global__ void __launch_bounds__(NT, NT == 512 ? 2 : (NT == 256 ? 5 : 8)) k_ble
       const uint32_t qb = to_u8(__fadd_rn(cb[k], __fmul_rn(T[k], bg2)));
       if (fused || rows) {
         sm.px[ly * TW + lx] = qr | (qg << 8) | (qb << 16);
-      } else if (px < W && py < H) {
-        // f == 1: the frame; other factors: the full-resolution scratch frame.
-        uint8_t* o = (f == 1 ? out : tv->full) + ((size_t)py * W + px) * 3;
+      } else if (px < W && py >= Y0 && py < Y1) {
+        // f == 1: the frame (window); other factors: the full-resolution
+        // scratch frame (whole frames only: Y0 = 0).
+        uint8_t* o = (f == 1 ? out : tv->full) + ((size_t)(py - Y0) * W + px) * 3;
         o[0] = (uint8_t)qr;
         o[1] = (uint8_t)qg;
         o[2] = (uint8_t)qb;
@@ -460,14 +462,14 @@ __global__ void __launch_bounds__(NT, NT == 512 ? 2 : (NT == 256 ? 5 : 8)) k_ble
       sync();
       for (uint32_t e = gt; e < TH * kRowWords; e += G) {
         const uint32_t ly = e / kRowWords, b0 = 4u * (e % kRowWords), py = oy + ly;  // b0: byte of the row
-        if (py < H) {
+        if (py >= Y0 && py < Y1) {
           uint32_t v = 0u;
 #pragma unroll
           for (uint32_t r = 0; r < 4; r++) {
             const uint32_t bb = b0 + r;
             v |= ((sm.px[ly * TW + bb / 3u] >> (8u * (bb % 3u))) & 255u) << (8u * r);
           }
-          *reinterpret_cast<uint32_t*>(out + ((size_t)py * W + ox) * 3 + b0) = v;
+          *reinterpret_cast<uint32_t*>(out + ((size_t)(py - Y0) * W + ox) * 3 + b0) = v;
         }
       }
     }

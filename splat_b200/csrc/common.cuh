@@ -42,6 +42,10 @@ struct FrameParams {
   uint32_t tiles_x, tiles_y;
   uint32_t downsample;      // 1 = none
   uint32_t out_w, out_h;    // floor(w/f), floor(h/f)
+  // Rows [win_y0, win_y0 + win_rows) of the w x h frame are rendered (the
+  // whole frame: 0, h); the tile grid then covers tile rows [win_ty0,
+  // win_ty0 + tiles_y) and the output holds the window's rows (f = 1).
+  uint32_t win_y0, win_rows, win_ty0, pad;
 };
 
 // Device-resident scene, FP32 storage (layout chosen for coalesced loads).

@@ -232,9 +232,13 @@ __device__ __forceinline__ void project_splat(const FrameParams& fp, const Scene
       r.r2 = make_float4(col[2], __uint_as_float(bx0 | (x1 << 16)), __uint_as_float(by0 | (y1 << 16)), tz);
       rec[i] = r;
       b.depth_bits = __float_as_uint(tz);
-      if (bx0 < x1 && by0 < y1) {
-        const uint32_t tx0 = bx0 >> fp.tile_sx, ty0 = by0 >> fp.tile_sy;
-        const uint32_t tx1 = (x1 + fp.tile_w - 1) >> fp.tile_sx, ty1 = (y1 + fp.tile_h - 1) >> fp.tile_sy;
+      // Tile rows clipped to the rendered window and counted from its first
+      // tile row (the whole frame: unchanged).
+      const uint32_t wty0 = max(by0 >> fp.tile_sy, fp.win_ty0);
+      const uint32_t wty1 = min((y1 + fp.tile_h - 1) >> fp.tile_sy, fp.win_ty0 + fp.tiles_y);
+      if (bx0 < x1 && by0 < y1 && wty0 < wty1) {
+        const uint32_t tx0 = bx0 >> fp.tile_sx, ty0 = wty0 - fp.win_ty0;
+        const uint32_t tx1 = (x1 + fp.tile_w - 1) >> fp.tile_sx, ty1 = wty1 - fp.win_ty0;
         b.rect_lo = tx0 | (ty0 << 16);
         b.rect_hi = tx1 | (ty1 << 16);
         b.count = (tx1 - tx0) * (ty1 - ty0);

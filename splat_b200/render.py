@@ -181,6 +181,25 @@ class CudaRenderer(Renderer):
         N.check(rc, self._h, "render_cells")
         return (out, RenderStats.from_c(st)) if stats else out
 
+    def render_rows(self, view: View, width: int, height: int, background, row0: int, rows: int,
+                    out: np.ndarray = None, stats: bool = False):
+        """Rows [row0, row0 + rows) of the width x height frame, bit for bit
+        as `render` draws them (splat_cuda_render_rows): only the tile rows
+        of the window are binned, sorted and blended. Returns a (rows, width,
+        3) u8 array (`out` if given, C-contiguous)."""
+        _pixel_count(width, height)
+        if out is None:
+            out = np.empty((rows, width, 3), np.uint8)
+        if out.shape != (rows, width, 3) or out.dtype != np.uint8 or not out.flags["C_CONTIGUOUS"]:
+            raise ValueError("out must be a C-contiguous (rows, width, 3) uint8 array")
+        bg = _f32(background)
+        st = N.RenderStatsC()
+        rc = N.lib().splat_cuda_render_rows(self._h, ctypes.byref(_view_desc(view)), width, height,
+                                            bg.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), row0, rows,
+                                            out.ctypes.data_as(ctypes.c_void_p), out.nbytes, ctypes.byref(st))
+        N.check(rc, self._h, "render_rows")
+        return (out, RenderStats.from_c(st)) if stats else out
+
     # --- device-side entry points --------------------------------------------
     def render_into(self, view: View, width: int, height: int, background, out_ptr: int, out_bytes: int,
                     downsample: int = 1) -> RenderStats:

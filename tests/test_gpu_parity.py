@@ -356,6 +356,32 @@ def test_device_path_matches_host_path():
     r.close()
 
 
+@pytest.mark.parametrize("exact", [False, True])
+@pytest.mark.parametrize("cfg", [(16, 16, 512), (8, 8, 256), (32, 16, 256)])
+def test_row_windows_match_the_whole_frame(exact, cfg):
+    """splat_cuda_render_rows: any window of rows (tile-aligned or not, one
+    row, the whole frame) equals those rows of the whole frame bit for bit,
+    and windows that split the frame (multi.row_windows, as ranks would draw
+    them) stitch back into it."""
+    from splat_b200 import multi
+
+    s = scene("clusters3")
+    w, h = 333, 191
+    r = CudaRenderer(s)
+    r.set_blend_config(*cfg)
+    for v in orbit_views(s, 2):
+        full, _ = cuda_frame(r, v, w, h, (0.1, 0.2, 0.3), exact=exact)
+        for row0, rows in [(0, h), (16, 32), (5, 50), (190, 1), (47, 144)]:
+            got = r.render_rows(v, w, h, (0.1, 0.2, 0.3), row0, rows)
+            assert np.array_equal(got, full[row0:row0 + rows]), (row0, rows)
+        for world in (2, 3, 4):
+            parts = [r.render_rows(v, w, h, (0.1, 0.2, 0.3), r0, n) for r0, n in multi.row_windows(h, world) if n]
+            assert np.array_equal(np.concatenate(parts), full)
+    with pytest.raises(N.SplatError, match="exceed the frame height"):
+        r.render_rows(orbit_views(s, 1)[0], w, h, (0, 0, 0), 150, 50)
+    r.close()
+
+
 @pytest.mark.parametrize("size,f,cfg", [((1920, 1080), 1, (16, 16, 512)), ((1920, 1080), 1, (32, 16, 256)),
                                         ((1920, 1080), 1, (8, 8, 256)), ((333, 191), 1, (16, 16, 512)),
                                         ((320, 192), 2, (16, 16, 512)), ((333, 191), 3, (16, 16, 512))])
