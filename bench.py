@@ -199,6 +199,16 @@ def scene_load(scene, dev):
     return out
 
 
+def profile_traffic(config, stage):
+    """The dominant kernel's DRAM bytes per launch measured by ncu for this
+    workload (profiles/traffic.json) and where they come from, or None."""
+    try:
+        entry = json.load(open(os.path.join(ROOT, "profiles", "traffic.json"))).get(config, {})
+        return entry.get(stage), entry.get("source")
+    except Exception:
+        return None, None
+
+
 def measured_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -426,14 +436,7 @@ def run_ours(args):
         times = {"project": stage["project_ms"], "sort": stage["sort_ms"], "raster": stage["raster_ms"]}
         dom = max(times, key=times.get)
         achieved = bytes_stage[dom] / (times[dom] / 1e3) / 1e9
-        traffic = traffic_src = None
-        prof = os.path.join(ROOT, "profiles", "traffic.json")
-        if os.path.exists(prof):
-            try:
-                entry = json.load(open(prof)).get(args.config, {})
-                traffic, traffic_src = entry.get(dom), entry.get("source")
-            except Exception:
-                traffic = traffic_src = None
+        traffic, traffic_src = profile_traffic(args.config, dom)
         load = scene_load(source, dev) if cfg["precision"] == "fp32" else None
         cpu = None
         if not args.no_cpu_baseline:
@@ -681,7 +684,8 @@ def run_learned(args):
             "gsplat_tiles_per_s": P * value / world / 1e9,
             "stages_ms": stage,
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                         "frac": achieved / peak, "traffic": profile_traffic("learned", dom)[0],
+                         "traffic_source": profile_traffic("learned", dom)[1], "peak_kind": peak_kind,
                          "algorithmic_bytes": bytes_stage[dom]},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e, "unit": "frames/s", "h2d_bytes_per_step": 56,
