@@ -176,9 +176,10 @@ int splat_cuda_render(splat_cuda_handle* h, const splat_view_desc* view, uint32_
  * first): the projection covers the whole frame, the tile binning, sorts and
  * blend only the tile rows that meet the window. One frame split into row
  * windows over several devices (each with the scene) is the frame's
- * tile-ownership split without a record exchange. No downsample. The
- * reference has no counterpart: its backends render whole frames
- * (Renderer::render, src/render/mod.rs:89-96). */
+ * tile-ownership split without a record exchange. No downsample. In stats,
+ * `visible` counts the splats visible in the whole frame and `overlaps` the
+ * window's (splat, tile) pairs. The reference has no counterpart: its
+ * backends render whole frames (Renderer::render, src/render/mod.rs:89-96). */
 int splat_cuda_render_rows(splat_cuda_handle* h, const splat_view_desc* view, uint32_t width, uint32_t height,
                            const float bg[3], uint32_t row0, uint32_t rows, uint8_t* rgb_out, size_t out_bytes,
                            splat_render_stats* stats);
