@@ -462,6 +462,10 @@ int create_impl(const splat_scene_desc* d, int device, splat_cuda_handle** out, 
   }
   int rc = ensure_pairs(h, std::max<uint64_t>(4 * n, 1u << 16));
   if (rc) return bail(rc);
+  // A cudaMemcpy from pageable memory may return before its DMA has landed,
+  // and the handle's stream does not wait for the legacy stream that carries
+  // it: the scene must be on the device before the first kernel reads it.
+  if (upload && (e = cudaDeviceSynchronize()) != cudaSuccess) return bail(cuda_fail(h, e, "upload scene"));
   *out = h;
   return SPLAT_OK;
 }
@@ -783,6 +787,13 @@ SPLAT_API int splat_cuda_create_learned(const splat_scene_desc* d, const uint16_
       splat_cuda_destroy(h);
       return rc;
     }
+  }
+  const cudaError_t se = cudaDeviceSynchronize();  // the uploads have landed (see create_impl)
+  if (se != cudaSuccess) {
+    rc = cuda_fail(h, se, "upload latents");
+    g_create_error = h->err;
+    splat_cuda_destroy(h);
+    return rc;
   }
   *out = h;
   return SPLAT_OK;

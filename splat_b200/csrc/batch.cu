@@ -196,6 +196,9 @@ int plan(splat_cuda_batch* b) {
     BK(cudaMemcpy(b->ltable, b->ltasks.data(), b->ltasks.size() * sizeof(ViewTask), cudaMemcpyHostToDevice),
        "upload learned views");
   }
+  // A cudaMemcpy from pageable memory may return before its DMA lands; the
+  // batch's stream does not wait for the legacy stream that carries it.
+  BK(cudaDeviceSynchronize(), "upload views");
   const size_t nt = std::max<uint32_t>(b->n_tiles, 1);
   BK(cudaMalloc(&b->totals, nt * sizeof(uint32_t)), "cudaMalloc totals");
   BK(cudaMalloc(&b->ranges, nt * sizeof(uint2)), "cudaMalloc ranges");

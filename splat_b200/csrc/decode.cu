@@ -490,7 +490,9 @@ int decode_to_handle(const Decoded& dec, uint32_t precision, int device, splat_c
   if (dec.n) {
     uint8_t* body = nullptr;
     cudaError_t e = cudaMalloc(&body, std::max<size_t>(dec.body_bytes, 1));
-    if (e == cudaSuccess) e = cudaMemcpy(body, dec.body, dec.body_bytes, cudaMemcpyHostToDevice);
+    // On the decode's own stream: a cudaMemcpy from pageable memory may return
+    // before its DMA lands, and that stream does not wait for the legacy one.
+    if (e == cudaSuccess) e = cudaMemcpyAsync(body, dec.body, dec.body_bytes, cudaMemcpyHostToDevice, h->stream);
     if (e == cudaSuccess) {
       const unsigned grid = (unsigned)std::min<uint64_t>((dec.n + 255) / 256, 16u * (uint64_t)h->num_sms);
       if (precision == SPLAT_PRECISION_FP32)

@@ -784,7 +784,10 @@ SPLAT_API int splat_cuda_learner_create(const splat_cuda_handle* h, const splat_
     const double th = golden * i;
     dirs[i] = make_float4((float)(r * std::cos(th)), (float)y, (float)(r * std::sin(th)), 0.0f);
   }
-  if ((e = cudaMemcpy(L->dirs, dirs.data(), dirs.size() * sizeof(float4), cudaMemcpyHostToDevice)) != cudaSuccess)
+  // Uploads go on the learner's stream (which does not wait for the legacy
+  // stream that a plain cudaMemcpy from pageable memory may still be using).
+  if ((e = cudaMemcpyAsync(L->dirs, dirs.data(), dirs.size() * sizeof(float4), cudaMemcpyHostToDevice, L->stream)) !=
+      cudaSuccess)
     return bail(lcuda(L, e, "upload directions"));
 
   TrainArgs& a = L->args;
@@ -833,7 +836,7 @@ SPLAT_API int splat_cuda_learner_create(const splat_cuda_handle* h, const splat_
   for (auto& v : proj) v = (float)(rng.normal() * 2.0 / std::sqrt((double)coefs));
   float* dproj = nullptr;
   if ((rc = dalloc((void**)&dproj, proj.size() * 4, "init"))) return bail(rc);
-  e = cudaMemcpy(dproj, proj.data(), proj.size() * 4, cudaMemcpyHostToDevice);
+  e = cudaMemcpyAsync(dproj, proj.data(), proj.size() * 4, cudaMemcpyHostToDevice, L->stream);
   if (e == cudaSuccess) {
     k_init_latents<<<std::min<uint64_t>((L->n + 255) / 256, 4096), 256, 0, L->stream>>>(a, L->sh_degree, dproj,
                                                                                           L->lat32, L->lat16);
@@ -852,12 +855,12 @@ SPLAT_API int splat_cuda_learner_set_params(splat_cuda_learner* L, const float* 
   LCK(cudaSetDevice(L->device), "cudaSetDevice");
   LCK(cudaStreamSynchronize(L->stream), "learner stream");
   if (params) {
-    LCK(cudaMemcpy(L->p32, params, mlp::kParams * 4, cudaMemcpyHostToDevice), "upload parameters");
+    LCK(cudaMemcpyAsync(L->p32, params, mlp::kParams * 4, cudaMemcpyHostToDevice, L->stream), "upload parameters");
     k_to_half<<<(mlp::kParams + 255) / 256, 256, 0, L->stream>>>(L->p32, L->p16, mlp::kParams);
     LCK(cudaGetLastError(), "parameters");
   }
   if (latents) {
-    LCK(cudaMemcpy(L->lat32, latents, L->n * 64, cudaMemcpyHostToDevice), "upload latents");
+    LCK(cudaMemcpyAsync(L->lat32, latents, L->n * 64, cudaMemcpyHostToDevice, L->stream), "upload latents");
     k_to_half<<<(uint32_t)std::min<uint64_t>((L->n * 16 + 255) / 256, 8192), 256, 0, L->stream>>>(L->lat32, L->lat16,
                                                                                                    L->n * 16);
     LCK(cudaGetLastError(), "latents");
