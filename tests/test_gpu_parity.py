@@ -377,6 +377,12 @@ def test_row_windows_match_the_whole_frame(exact, cfg):
         for world in (2, 3, 4):
             parts = [r.render_rows(v, w, h, (0.1, 0.2, 0.3), r0, n) for r0, n in multi.row_windows(h, world) if n]
             assert np.array_equal(np.concatenate(parts), full)
+        # a window into mapped pinned memory (written by the kernels directly)
+        import torch
+
+        pinned = torch.full((64, w, 3), 7, dtype=torch.uint8).pin_memory().numpy()
+        r.render_rows(v, w, h, (0.1, 0.2, 0.3), 32, 64, out=pinned)
+        assert np.array_equal(pinned, full[32:96])
     with pytest.raises(N.SplatError, match="exceed the frame height"):
         r.render_rows(orbit_views(s, 1)[0], w, h, (0, 0, 0), 150, 50)
     r.close()
