@@ -101,31 +101,69 @@ from splat_b200.multi import dist_env, max_over_ranks, shard  # noqa: E402
 
 
 class Clocks:
-    """Samples nvidia-smi clocks and throttle reasons every 200 ms during the
-    timed region (one-shot queries, so nothing sits in a pipe buffer)."""
+    """Samples the SM clock, its maximum and the clock-event (throttle)
+    reasons of the GPU every `period` seconds while the timed region runs,
+    through NVML (read-only queries), so that even a timed region of a few
+    milliseconds gets several samples; nvidia-smi one-shot queries are the
+    fallback when NVML cannot be loaded."""
 
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    BITS = [0x8, 0x40, 0x20, 0x4]  # nvmlClocksEventReason{HwSlowdown, HwThermalSlowdown, SwThermalSlowdown, SwPowerCap}
     Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
-    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
-    def __init__(self, index):
+    def __init__(self, index, period=0.002):
         self.index = index
-        self.rows = []
+        self.period = period
+        self.rows = []  # (sm_mhz, max_mhz, reasons bitmask)
         self.stop = threading.Event()
+        self.source = "nvml"
+        self.nvml = None
+        try:
+            import pynvml
+            import torch
+
+            pynvml.nvmlInit()
+            try:
+                p = torch.cuda.get_device_properties(index)
+                bus = f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0"
+                self.handle = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+            except Exception:
+                self.handle = pynvml.nvmlDeviceGetHandleByIndex(index)
+            self.nvml = pynvml
+        except Exception:
+            self.source = "nvidia-smi"
+
+    def _sample_nvml(self):
+        n = self.nvml
+        sm = n.nvmlDeviceGetClockInfo(self.handle, n.NVML_CLOCK_SM)
+        mx = n.nvmlDeviceGetMaxClockInfo(self.handle, n.NVML_CLOCK_SM)
+        rs = n.nvmlDeviceGetCurrentClocksEventReasons(self.handle)
+        self.rows.append((float(sm), float(mx), int(rs)))
+
+    def _sample_smi(self):
+        out = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                              "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+        for line in out.stdout.strip().splitlines():
+            c = [x.strip() for x in line.split(",")]
+            if len(c) >= 7:
+                bits = sum(b for b, v in zip(self.BITS, c[3:7]) if v.lower().startswith("active"))
+                try:
+                    self.rows.append((float(c[0]), float(c[1]), bits))
+                except ValueError:
+                    pass
 
     def _poll(self):
         while not self.stop.is_set():
             try:
-                out = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
-                for line in out.stdout.strip().splitlines():
-                    self.rows.append([c.strip() for c in line.split(",")])
+                self._sample_nvml() if self.nvml else self._sample_smi()
             except Exception:
                 pass
-            self.stop.wait(0.2)
+            self.stop.wait(self.period if self.nvml else 0.2)
 
     def __enter__(self):
+        self.t0 = time.perf_counter()
         self.t = threading.Thread(target=self._poll, daemon=True)
         self.t.start()
         return self
@@ -133,24 +171,22 @@ class Clocks:
     def __exit__(self, *a):
         self.stop.set()
         self.t.join(timeout=10)
+        self.seconds = time.perf_counter() - self.t0
 
     def summary(self):
-        def num(v):
-            try:
-                return float(v)
-            except ValueError:
-                return None
-
-        rows = [r for r in self.rows if len(r) >= 7]
-        sm = [num(r[0]) for r in rows if num(r[0]) is not None]
-        mx = [num(r[1]) for r in rows if num(r[1]) is not None]
-        reasons = set()
-        for r in rows:
-            for k, nm in enumerate(self.NAMES):
-                if r[3 + k].lower().startswith("active"):
-                    reasons.add(nm)
+        sm = [r[0] for r in self.rows]
+        mx = [r[1] for r in self.rows]
+        reasons = sorted({nm for r in self.rows for nm, b in zip(self.NAMES, self.BITS) if r[2] & b})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(rows)}
+                "reasons": reasons, "samples": len(self.rows), "source": self.source,
+                "window_s": round(getattr(self, "seconds", 0.0), 4)}
+
+
+def bench_config(cfg, n, w, h, world):
+    """The workload's config dict, the same in both arms of the benchmark."""
+    return {"workload": cfg["workload"], "splats": n, "width": w, "height": h, "tile": 16,
+            "storage": cfg["precision"], "parallelism": f"view-parallel x{world}",
+            "l2": f"inputs larger than L2 (scene {n * cfg['s_in'] / 1e6:.0f} MB > 126 MB)"}
 
 
 def make_workload(n, cfg):
@@ -286,7 +322,7 @@ def run_reference(args):
         "impl": "reference", "metric": cfg["metric"], "value": fps, "unit": "frames/s", "n_gpus": 0,
         "steps": len(times), "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": cfg["workload"], "splats": args.splats, "width": W, "height": H},
+        "config": bench_config(cfg, args.splats, W, H, world),
         "cpu_baseline": {"value": fps, "unit": "frames/s", "cores": threads, "kind": "port",
                          "sample": f"{len(times)} frames of the orbit (full {W}x{H} frames)"},
         "e2e": {"value": fps, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -312,6 +348,29 @@ def fp64_errors(device_frames, source_scene, decoded_scene, views, w, h):
                         "max_abs": int(np.max(np.abs(img.astype(int) - ref.astype(int))))}
         rows.append(row)
     return rows
+
+
+def home_frame_check(r, scene, home, w, h, host):
+    """The reference bench's PSNR (src/bench.rs:51-59, 153-170): the home
+    frame of the orbit, drawn by the device (default and exact blends, into
+    pinned host memory through splat_cuda_render) against the reference's
+    `cpu` backend (the oracle's restatement)."""
+    from oracle import oracle as O
+    from splat_b200 import _native as Nat
+
+    cpu = O.CpuTiled(scene, threads=0)
+    want, _ = cpu.render(home, w, h, (0, 0, 0))
+    cpu.close()
+    r.render_into(home, w, h, (0, 0, 0), host.data_ptr(), host.numel())
+    fast = host.numpy().reshape(h, w, 3).copy()
+    r.set_option(Nat.SPLAT_OPT_EXACT_BLEND, 1)
+    r.render_into(home, w, h, (0, 0, 0), host.data_ptr(), host.numel())
+    exact = host.numpy().reshape(h, w, 3).copy()
+    r.set_option(Nat.SPLAT_OPT_EXACT_BLEND, 0)
+    return {"frame": "home (orbit frame 0)", "psnr_db": O.psnr(fast, want),
+            "max_abs": int(np.max(np.abs(fast.astype(int) - want.astype(int)))),
+            "exact_blend_identical": bool(np.array_equal(exact, want)),
+            "against": "cpu backend (C++ restatement of src/render/cpu.rs), same scene and view"}
 
 
 def run_ours(args):
@@ -447,14 +506,13 @@ def run_ours(args):
             cpu_naive = {"value": nfps, "unit": "frames/s", "cores": 1, "kind": "port",
                          "sample": f"{nframes} full {W}x{H} frames of the orbit",
                          "backend": "cpu-naive (src/render/naive.rs), one thread"}
+        home_check = home_frame_check(r, f32_scene, home, W, H, host) if cfg["precision"] == "fp32" else None
         line = {
             "metric": cfg["metric"], "value": value, "unit": "frames/s", "n_gpus": world, "steps": K,
             "warmup": args.warmup, "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": cfg["workload"], "splats": N, "width": W, "height": H, "tile": 16,
-                       "storage": cfg["precision"], "visible": V, "pairs": P,
-                       "parallelism": f"view-parallel x{world}",
-                       "l2": f"inputs larger than L2 (scene {N * cfg['s_in'] / 1e6:.0f} MB > 126 MB)"},
+            "config": bench_config(cfg, N, W, H, world),
+            "frame": {"visible": V, "pairs": P},
             "gsplat_tiles_per_s": P * value / world / 1e9,
             "stages_ms": stage,
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -473,6 +531,8 @@ def run_ours(args):
         }
         if errors is not None:
             line["error_vs_fp64_naive"] = errors
+        if home_check is not None:
+            line["psnr_vs_cpu"] = home_check
         if load is not None:
             line["scene_load"] = load
         if cpu is not None:

@@ -196,9 +196,6 @@ int plan(splat_cuda_batch* b) {
     BK(cudaMemcpy(b->ltable, b->ltasks.data(), b->ltasks.size() * sizeof(ViewTask), cudaMemcpyHostToDevice),
        "upload learned views");
   }
-  // A cudaMemcpy from pageable memory may return before its DMA lands; the
-  // batch's stream does not wait for the legacy stream that carries it.
-  BK(cudaDeviceSynchronize(), "upload views");
   const size_t nt = std::max<uint32_t>(b->n_tiles, 1);
   BK(cudaMalloc(&b->totals, nt * sizeof(uint32_t)), "cudaMalloc totals");
   BK(cudaMalloc(&b->ranges, nt * sizeof(uint2)), "cudaMalloc ranges");
@@ -206,6 +203,10 @@ int plan(splat_cuda_batch* b) {
   // Padding tiles between views are never written by the column scan: their
   // totals stay zero (empty ranges).
   BK(cudaMemset(b->totals, 0, nt * sizeof(uint32_t)), "clear totals");
+  // A cudaMemcpy from pageable memory may return before its DMA lands, and a
+  // device memset is asynchronous; the batch's stream does not wait for the
+  // legacy stream that carries both, so they must land before its first use.
+  BK(cudaDeviceSynchronize(), "upload views");
   b->counters_bytes = frame_counters_bytes(nv, std::max<uint32_t>(b->n_chunks, 1));
   BK(cudaMalloc(&b->counters, b->counters_bytes), "cudaMalloc counters");
   BK(cudaMallocHost(&b->counters_host, b->counters_bytes), "cudaMallocHost counters");

@@ -751,10 +751,13 @@ SPLAT_API int splat_cuda_learner_create(const splat_cuda_handle* h, const splat_
   const uint32_t per = (tiles + slots - 1) / slots;
   L->grid = (tiles + per - 1) / per;
   const uint64_t nl = L->n * 16;
+  // Zeroed on the learner's own stream: it is non-blocking, so a memset on
+  // the legacy stream could still land after the packing kernel and the
+  // uploads below have written these buffers.
   auto dalloc = [&](void** p, size_t bytes, const char* what) -> int {
     cudaError_t er = cudaMalloc(p, bytes);
     if (er != cudaSuccess) return lcuda(L, er, what);
-    er = cudaMemset(*p, 0, bytes);
+    er = cudaMemsetAsync(*p, 0, bytes, L->stream);
     if (er != cudaSuccess) return lcuda(L, er, what);
     return SPLAT_OK;
   };
