@@ -42,7 +42,9 @@ typedef enum splat_status {
   SPLAT_OK = 0,
   SPLAT_ERR_INVALID_ARG = 1,   /* null pointer, bad size, frame > MAX_DIM, ... */
   SPLAT_ERR_OOM = 2,           /* device or pinned-host allocation failed */
-  SPLAT_ERR_CAPACITY = 3,      /* more (splat, tile) pairs than the pair limit */
+  SPLAT_ERR_CAPACITY = 3,      /* one tile holds more (splat, tile) pairs than
+                                  the pair buffers can (frames that only need
+                                  more pairs in total are drawn in windows) */
   SPLAT_ERR_DEVICE = 4,        /* CUDA error (text in splat_cuda_last_error) */
   SPLAT_ERR_TIMEOUT = 5,       /* a bounded device-side wait gave up */
   SPLAT_ERR_UNSUPPORTED = 6    /* option or precision not available */
@@ -165,8 +167,14 @@ int splat_cuda_create_from_ply(const void* data, size_t bytes, uint32_t precisio
  * height above SPLAT_MAX_DIM is rejected (src/render/mod.rs:35-41). Pair
  * buffers grow and the frame is re-rendered when a view needs more (splat,
  * tile) pairs than allocated (the reference's grow-and-retry,
- * src/render/gpu.rs:1040-1056). Blocks until the frame is in rgb_out.
- * Replaces Renderer::render (src/render/mod.rs:89-96). */
+ * src/render/gpu.rs:1040-1056). A view that needs more pairs than the pair
+ * limit (SPLAT_OPT_PAIR_LIMIT, default 2^30 - 1) or than device memory
+ * holds is drawn in windows of whole tiles whose pairs fit, each with the
+ * full projection: the frame is complete and identical to a one-pass frame
+ * (the reference's gpu backend keeps the front-most pairs instead,
+ * src/render/gpu.rs:1253-1289), `overlaps` counts all its pairs. Blocks
+ * until the frame is in rgb_out. Replaces Renderer::render
+ * (src/render/mod.rs:89-96). */
 int splat_cuda_render(splat_cuda_handle* h, const splat_view_desc* view, uint32_t width, uint32_t height,
                       const float bg[3], uint32_t downsample, uint8_t* rgb_out, size_t out_bytes,
                       splat_render_stats* stats);
@@ -210,7 +218,10 @@ int splat_cuda_render_cells(splat_cuda_handle* h, const splat_view_desc* view, u
 
 /* Waits for the frames enqueued by splat_cuda_render_device, fills the stats
  * of the last one and reports whether it overflowed the pair buffers
- * (*regrown = 1: the buffers have been grown; enqueue the frame again). */
+ * (*regrown = 1: the buffers have been grown; enqueue the frame again). A
+ * last frame that needs more pairs than the pair limit (or device memory)
+ * allows is drawn again in windows of tiles into its destination before
+ * this call returns (*regrown = 0, complete stats). */
 int splat_cuda_finish(splat_cuda_handle* h, splat_render_stats* stats, int* regrown);
 
 /* Uses `stream` (a cudaStream_t on the handle's device; NULL restores the
@@ -241,6 +252,27 @@ void* splat_cuda_get_stream(splat_cuda_handle* h);
                                       image does not depend on it; the keys of
                                       splat_cuda_debug_dump use its tiles. */
 #define SPLAT_OPT_SCENE_SPLATS 8u    /* read-only: gaussians in the scene */
+#define SPLAT_OPT_PAIR_LIMIT 9u      /* largest pair-buffer capacity (pairs; 1024 ..
+                                        2^30 - 1, the default); frames that need
+                                        more are drawn in windows of tiles. The
+                                        reference's test-only max_cap
+                                        (src/render/gpu.rs:1273). */
+/* Fault injection, for tests of the error paths; nothing faults on the GPU.
+ * value = kind | microseconds << 8 (0 clears); each injection fires once.
+ *   SPLAT_FAULT_ALLOC      the handle's next device allocation reports out of
+ *                          memory without calling the allocator: the call
+ *                          returns SPLAT_ERR_OOM and the handle stays usable
+ *                          (pair-buffer growth absorbs it by trying a smaller
+ *                          capacity).
+ *   SPLAT_FAULT_LOST_WAIT  the tensor-core waits of the next frame (learned
+ *                          colour) or training call also wait for a completion
+ *                          that never arrives, giving up after `microseconds`:
+ *                          the call returns SPLAT_ERR_TIMEOUT, the kernel frees
+ *                          its tensor memory, a training step is dropped, and
+ *                          the next call runs normally. */
+#define SPLAT_OPT_INJECT_FAULT 10u
+#define SPLAT_FAULT_ALLOC 1u
+#define SPLAT_FAULT_LOST_WAIT 2u
 int splat_cuda_set_option(splat_cuda_handle* h, uint32_t option, uint64_t value);
 int splat_cuda_get_option(splat_cuda_handle* h, uint32_t option, uint64_t* value);
 
@@ -451,6 +483,10 @@ int splat_cuda_learner_step_debug(splat_cuda_learner* l, float* grad_params, flo
 int splat_cuda_learner_directions(const splat_cuda_learner* l, float* dirs);
 /* SPLAT_LEARN_* and SPLAT_OPT_KERNEL_LAUNCHES. */
 int splat_cuda_learner_get_option(const splat_cuda_learner* l, uint32_t option, uint64_t* value);
+/* SPLAT_OPT_INJECT_FAULT with SPLAT_FAULT_LOST_WAIT (a test of the timeout
+ * path: the steps of the next train or step_debug call give up on a wait and
+ * are dropped; that call returns SPLAT_ERR_TIMEOUT). */
+int splat_cuda_learner_set_option(splat_cuda_learner* l, uint32_t option, uint64_t value);
 const char* splat_cuda_learner_last_error(const splat_cuda_learner* l);
 int splat_cuda_learner_destroy(splat_cuda_learner* l);
 

@@ -74,6 +74,17 @@ template <class T> void dfree(T*& p) {
   p = nullptr;
 }
 
+// cudaMalloc for the handle's per-frame buffers; an injected allocation
+// failure (SPLAT_FAULT_ALLOC) makes the next one report out of memory
+// without calling the allocator.
+template <class T> cudaError_t dmalloc(splat_cuda_handle* h, T** p, size_t bytes) {
+  if (h->inject_alloc) {
+    h->inject_alloc = false;
+    return cudaErrorMemoryAllocation;
+  }
+  return cudaMalloc(p, bytes);
+}
+
 void free_pairs(splat_cuda_handle* h) {
   for (int b = 0; b < 2; b++) dfree(h->pairs[b]);
   h->cap = 0;
@@ -83,9 +94,26 @@ int ensure_pairs(splat_cuda_handle* h, uint64_t cap) {
   if (cap <= h->cap) return SPLAT_OK;
   if (cap > kMaxPairs) return fail(h, SPLAT_ERR_CAPACITY, "more than 2^30 - 1 gaussian/tile pairs");
   free_pairs(h);
-  for (int b = 0; b < 2; b++) CK(cudaMalloc(&h->pairs[b], cap * sizeof(uint64_t)), "cudaMalloc pairs");
+  for (int b = 0; b < 2; b++) CK(dmalloc(h, &h->pairs[b], cap * sizeof(uint64_t)), "cudaMalloc pairs");
   h->cap = cap;
   return SPLAT_OK;
+}
+
+// Grows the pair buffers towards `want` pairs (at most the pair limit). When
+// the device cannot hold that many, smaller capacities are tried, halving,
+// down to the current one; frames that then do not fit are drawn in windows
+// of tiles. Fails only when not even the current capacity can be restored.
+int grow_pairs(splat_cuda_handle* h, uint64_t want) {
+  want = std::min(want, h->pair_limit);
+  const uint64_t old = h->cap;
+  if (want <= old) return SPLAT_OK;
+  for (uint64_t c = want; c > old; c /= 2) {
+    const int rc = ensure_pairs(h, c);
+    if (rc == SPLAT_OK) return SPLAT_OK;
+    if (rc != SPLAT_ERR_OOM) return rc;
+    cudaGetLastError();  // the failed allocation is not a sticky error
+  }
+  return ensure_pairs(h, std::max<uint64_t>(old, 1));
 }
 
 int ensure_size(splat_cuda_handle* h, uint64_t tiles, uint32_t rows, size_t out_bytes, size_t full_bytes) {
@@ -94,33 +122,33 @@ int ensure_size(splat_cuda_handle* h, uint64_t tiles, uint32_t rows, size_t out_
     dfree(h->totals);
     dfree(h->order);
     h->ranges_cap = 0;
-    CK(cudaMalloc(&h->ranges, tiles * sizeof(uint2)), "cudaMalloc ranges");
-    CK(cudaMalloc(&h->totals, tiles * sizeof(uint32_t)), "cudaMalloc totals");
-    CK(cudaMalloc(&h->order, kTileClasses * tiles * sizeof(uint32_t)), "cudaMalloc tile classes");
+    CK(dmalloc(h, &h->ranges, tiles * sizeof(uint2)), "cudaMalloc ranges");
+    CK(dmalloc(h, &h->totals, tiles * sizeof(uint32_t)), "cudaMalloc totals");
+    CK(dmalloc(h, &h->order, kTileClasses * tiles * sizeof(uint32_t)), "cudaMalloc tile classes");
     h->ranges_cap = tiles;
   }
   const size_t words = (size_t)rows * tiles;
   if (words > h->counts_cap) {
     dfree(h->counts);
     h->counts_cap = 0;
-    CK(cudaMalloc(&h->counts, words * sizeof(uint32_t)), "cudaMalloc counts");
+    CK(dmalloc(h, &h->counts, words * sizeof(uint32_t)), "cudaMalloc counts");
     h->counts_cap = words;
   }
   const uint32_t chunks = (uint32_t)((tiles + kScanChunk - 1) / kScanChunk);
   if (chunks > h->chunks_cap || !h->st) {
     dfree(h->st);
     h->chunks_cap = 0;
-    CK(cudaMalloc(&h->st, frame_counters_bytes(1, std::max(chunks, 1u))), "cudaMalloc frame counters");
+    CK(dmalloc(h, &h->st, frame_counters_bytes(1, std::max(chunks, 1u))), "cudaMalloc frame counters");
     h->chunks_cap = std::max(chunks, 1u);
   }
   if (out_bytes > h->out_cap) {
     dfree(h->out_dev);
-    CK(cudaMalloc(&h->out_dev, out_bytes), "cudaMalloc frame");
+    CK(dmalloc(h, &h->out_dev, out_bytes), "cudaMalloc frame");
     h->out_cap = out_bytes;
   }
   if (full_bytes > h->full_cap) {
     dfree(h->full_dev);
-    CK(cudaMalloc(&h->full_dev, full_bytes), "cudaMalloc full-resolution frame");
+    CK(dmalloc(h, &h->full_dev, full_bytes), "cudaMalloc full-resolution frame");
     h->full_cap = full_bytes;
   }
   return SPLAT_OK;
@@ -182,6 +210,9 @@ FrameParams make_params(const splat_view_desc& v, uint32_t w, uint32_t hgt, cons
   p.out_h = hgt / f;
   p.win_y0 = 0;
   p.win_rows = hgt;
+  p.out_y0 = 0;
+  p.win_x0 = 0;
+  p.win_cols = w;
   return p;
 }
 
@@ -196,7 +227,8 @@ void set_tile_shape(FrameParams& p, uint32_t tile_w, uint32_t tile_h) {
   p.tile_h = tile_h;
   p.tile_sx = (uint32_t)__builtin_ctz(tile_w);
   p.tile_sy = (uint32_t)__builtin_ctz(tile_h);
-  p.tiles_x = (p.w + tile_w - 1) / tile_w;
+  p.win_tx0 = p.win_x0 / tile_w;
+  p.tiles_x = (p.win_x0 + p.win_cols + tile_w - 1) / tile_w - p.win_tx0;
   p.win_ty0 = p.win_y0 / tile_h;
   p.tiles_y = (p.win_y0 + p.win_rows + tile_h - 1) / tile_h - p.win_ty0;
 }
@@ -224,6 +256,8 @@ int enqueue_frame(splat_cuda_handle* h, const FrameParams& fp_in, uint8_t* dev_o
   ViewTask t{};
   t.fp = fp;
   t.s = scene_dev(h);
+  t.s.lost_wait_us = h->inject_lost_us;  // fault injection: this frame only
+  h->inject_lost_us = 0;
   t.rec = h->rec;
   t.bin = h->bin;
   t.counts = h->counts;
@@ -254,10 +288,16 @@ int enqueue_frame(splat_cuda_handle* h, const FrameParams& fp_in, uint8_t* dev_o
   if (h->stage_events) CK(cudaEventRecord(h->ev[3], s), "event");
   CK(cudaMemcpyAsync(h->st_host, h->st, frame_counters_bytes(1, 0), cudaMemcpyDeviceToHost, s), "copy frame state");
   h->last_fp = fp;
+  h->last_req = fp_in;
+  h->last_out = dev_out;
+  h->last_mapped = host_mapped;
   return SPLAT_OK;
 }
 
-// Waits for the enqueued frame and interprets its state.
+// Waits for the enqueued frame and interprets its state. *regrown: 0 the
+// frame is complete; 1 it needed more pairs than the buffers held, which
+// have grown to hold them (draw it again); 2 it needs more pairs than the
+// buffers can hold (the pair limit, or device memory): draw it in windows.
 int finish_frame(splat_cuda_handle* h, splat_render_stats* stats, int* regrown) {
   *regrown = 0;
   CK(cudaStreamSynchronize(h->stream), "frame");
@@ -280,14 +320,88 @@ int finish_frame(splat_cuda_handle* h, splat_render_stats* stats, int* regrown) 
     cudaMemsetAsync(h->st, 0, sizeof(DevState), h->stream);
     return fail(h, SPLAT_ERR_TIMEOUT, "a tensor-core wait in the learned-colour projection gave up");
   }
-  if (st.total_pairs > h->cap) {
-    const uint64_t want = std::max<uint64_t>(st.total_pairs + st.total_pairs / 4, h->cap + 1);
-    int rc = ensure_pairs(h, std::min<uint64_t>(want, std::max<uint64_t>(st.total_pairs, kMaxPairs)));
-    if (rc) return rc;
-    *regrown = 1;
-  }
   h->have_frame = true;
+  if (st.total_pairs > h->cap) {
+    const uint64_t total = st.total_pairs;
+    const int rc = grow_pairs(h, std::max<uint64_t>(total + total / 4, h->cap + 1));
+    if (rc) return rc;
+    *regrown = h->cap >= total ? 1 : 2;
+  }
   return SPLAT_OK;
+}
+
+// Draws the frame `req` (a whole frame or a window of rows) into `target`
+// as windows of whole tiles whose pairs fit the buffers: bands of tile rows
+// sized from the frame's pair count, a band that still overflows split in
+// two (by tile rows, then by tile columns), each window a complete
+// projection plus the binning, sorts and blend of its own tiles, written in
+// place into the frame. Every pixel sees the same splats in the same order
+// as in one pass, so the frame is identical to the one-pass frame. stats:
+// the visible splats of the frame, the pairs and stage times summed over
+// the windows. Fails (SPLAT_ERR_CAPACITY) only if a single tile holds more
+// pairs than the buffers can.
+int render_windows(splat_cuda_handle* h, FrameParams req, uint8_t* target, bool mapped, splat_render_stats* stats) {
+  struct Win {
+    uint32_t y0, y1, x0, x1;
+  };
+  const uint32_t tw = h->blend.tile_w, th = h->blend.tile_h;
+  const uint32_t y0 = req.win_y0, y1 = req.win_y0 + req.win_rows;
+  const uint32_t ty0 = y0 / th, nty = (y1 + th - 1) / th - ty0;
+  const uint64_t per = std::max<uint64_t>(h->cap - h->cap / 4, 1);
+  const uint64_t bands = std::min<uint64_t>(nty, std::max<uint64_t>(2, (h->st_host->total_pairs + per - 1) / per));
+  std::vector<Win> todo;
+  for (uint64_t b = bands; b-- > 0;) {
+    const uint32_t a = std::max(y0, (uint32_t)((ty0 + b * nty / bands) * th));
+    const uint32_t e = std::min(y1, (uint32_t)((ty0 + (b + 1) * nty / bands) * th));
+    if (e > a) todo.push_back({a, e, 0u, req.w});
+  }
+  splat_render_stats sum{};
+  int rc = SPLAT_OK;
+  uint32_t passes = 0;
+  while (!todo.empty()) {
+    const Win w = todo.back();
+    todo.pop_back();
+    FrameParams fp = req;
+    fp.win_y0 = w.y0;
+    fp.win_rows = w.y1 - w.y0;
+    fp.win_x0 = w.x0;
+    fp.win_cols = w.x1 - w.x0;
+    if ((rc = enqueue_frame(h, fp, target, mapped))) break;
+    splat_render_stats ws{};
+    int rg = 0;
+    if ((rc = finish_frame(h, &ws, &rg))) break;
+    if (rg == 1 && ++passes < 64) {  // the buffers grew: this window again
+      todo.push_back(w);
+      continue;
+    }
+    if (rg) {  // split: by tile rows while there are several, then by tile columns
+      const uint32_t r0 = w.y0 / th, nr = (w.y1 + th - 1) / th - r0;
+      const uint32_t c0 = w.x0 / tw, nc = (w.x1 + tw - 1) / tw - c0;
+      if (nr > 1) {
+        const uint32_t m = (r0 + nr / 2) * th;
+        todo.push_back({m, w.y1, w.x0, w.x1});
+        todo.push_back({w.y0, m, w.x0, w.x1});
+      } else if (nc > 1) {
+        const uint32_t m = (c0 + nc / 2) * tw;
+        todo.push_back({w.y0, w.y1, m, w.x1});
+        todo.push_back({w.y0, w.y1, w.x0, m});
+      } else {
+        rc = fail(h, SPLAT_ERR_CAPACITY, "one tile holds more (splat, tile) pairs than the pair buffers can");
+        break;
+      }
+      continue;
+    }
+    sum.visible = ws.visible;
+    sum.overlaps += ws.overlaps;
+    sum.project_ms += ws.project_ms;
+    sum.sort_ms += ws.sort_ms;
+    sum.raster_ms += ws.raster_ms;
+  }
+  h->last_req = req;
+  h->last_out = target;
+  h->last_mapped = mapped;
+  if (rc == SPLAT_OK && stats) *stats = sum;
+  return rc;
 }
 
 int check_view_args(splat_cuda_handle* h, const splat_view_desc* view, uint32_t w, uint32_t hgt, const float* bg) {
@@ -502,7 +616,14 @@ SPLAT_API int splat_cuda_finish(splat_cuda_handle* h, splat_render_stats* stats,
   if (!regrown) regrown = &dummy;
   if (stats) std::memset(stats, 0, sizeof(*stats));
   CK(cudaSetDevice(h->device), "cudaSetDevice");
-  return finish_frame(h, stats, regrown);
+  int rc = finish_frame(h, stats, regrown);
+  if (rc == SPLAT_OK && *regrown == 2) {
+    // More pairs than the buffers can hold: the frame is drawn again, in
+    // windows, into the same destination before this call returns.
+    *regrown = 0;
+    rc = render_windows(h, h->last_req, h->last_out, h->last_mapped, stats);
+  }
+  return rc;
 }
 
 namespace {
@@ -534,6 +655,14 @@ int render_to_host(splat_cuda_handle* h, const FrameParams& fp, uint8_t* rgb_out
          "copy frame");
     int regrown = 0;
     if ((rc = finish_frame(h, stats, &regrown))) return rc;
+    if (regrown == 2) {  // more pairs than the buffers can hold: windows of tiles
+      if ((rc = render_windows(h, fp, mapped ? mapped : h->out_dev, mapped != nullptr, stats))) return rc;
+      if (bytes && !mapped)
+        CK(cudaMemcpyAsync(direct ? rgb_out : h->stage, h->out_dev, bytes, cudaMemcpyDeviceToHost, h->stream),
+           "copy frame");
+      CK(cudaStreamSynchronize(h->stream), "frame");
+      regrown = 0;
+    }
     if (!regrown) {
       if (!direct && bytes) std::memcpy(rgb_out, h->stage, bytes);
       if (stats)
@@ -576,6 +705,7 @@ SPLAT_API int splat_cuda_render_rows(splat_cuda_handle* h, const splat_view_desc
   FrameParams fp = make_params(*view, width, height, bg, 1);
   fp.win_y0 = row0;
   fp.win_rows = rows;
+  fp.out_y0 = row0;
   fp.out_h = rows;
   return render_to_host(h, fp, rgb_out, stats, t0);
 }
@@ -606,7 +736,7 @@ SPLAT_API int splat_cuda_render_cells(splat_cuda_handle* h, const splat_view_des
     if (h->cells_dev) cudaFree(h->cells_dev);
     h->cells_dev = nullptr;
     h->cells_cap = 0;
-    CK(cudaMalloc(&h->cells_dev, need), "cudaMalloc cells");
+    CK(dmalloc(h, &h->cells_dev, need), "cudaMalloc cells");
     h->cells_cap = need;
   }
   const bool direct = need && is_pinned_host(cells_out);
@@ -625,6 +755,15 @@ SPLAT_API int splat_cuda_render_cells(splat_cuda_handle* h, const splat_view_des
          "copy cells");
     int regrown = 0;
     if ((rc = finish_frame(h, stats, &regrown))) return rc;
+    if (regrown == 2) {  // more pairs than the buffers can hold: windows of tiles
+      if ((rc = render_windows(h, fp, h->out_dev, false, stats))) return rc;
+      CK(launch_cells(h->out_dev, fp.out_w, nc, nr, mode, h->cells_dev, h->stream, &h->launches), "cells kernel");
+      if (need)
+        CK(cudaMemcpyAsync(direct ? cells_out : h->stage, h->cells_dev, need, cudaMemcpyDeviceToHost, h->stream),
+           "copy cells");
+      CK(cudaStreamSynchronize(h->stream), "frame");
+      regrown = 0;
+    }
     if (!regrown) {
       if (!direct && need) std::memcpy(cells_out, h->stage, need);
       if (stats)
@@ -651,10 +790,20 @@ SPLAT_API int splat_cuda_set_option(splat_cuda_handle* h, uint32_t option, uint6
       h->exact = value != 0;
       return SPLAT_OK;
     case SPLAT_OPT_PAIR_CAPACITY: {
-      if (value == 0 || value > kMaxPairs) return fail(h, SPLAT_ERR_INVALID_ARG, "pair capacity out of range");
+      if (value == 0 || value > h->pair_limit)
+        return fail(h, SPLAT_ERR_INVALID_ARG, "pair capacity out of range (1 .. the pair limit)");
       // Shrinking is allowed: reallocate at exactly `value`.
       free_pairs(h);
       return ensure_pairs(h, value);
+    }
+    case SPLAT_OPT_PAIR_LIMIT: {
+      if (value < 1024 || value > kMaxPairs) return fail(h, SPLAT_ERR_INVALID_ARG, "pair limit out of range");
+      h->pair_limit = value;
+      if (h->cap > value) {  // the buffers shrink to the new limit
+        free_pairs(h);
+        return ensure_pairs(h, value);
+      }
+      return SPLAT_OK;
     }
     case SPLAT_OPT_STAGE_EVENTS:
       h->stage_events = value != 0;
@@ -670,6 +819,15 @@ SPLAT_API int splat_cuda_set_option(splat_cuda_handle* h, uint32_t option, uint6
       h->blend = c;
       return SPLAT_OK;
     }
+    case SPLAT_OPT_INJECT_FAULT:
+      switch (value & 0xFFu) {
+        case 0: h->inject_alloc = false; h->inject_lost_us = 0; return SPLAT_OK;
+        case SPLAT_FAULT_ALLOC: h->inject_alloc = true; return SPLAT_OK;
+        case SPLAT_FAULT_LOST_WAIT:
+          h->inject_lost_us = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(value >> 8, 10000000ull));
+          return SPLAT_OK;
+        default: return fail(h, SPLAT_ERR_UNSUPPORTED, "unknown fault kind");
+      }
     case SPLAT_OPT_DEBUG_CAPTURE: {
       h->debug_capture = value != 0;
       if (h->debug_capture && h->n && !h->dbg_proj) {
@@ -688,6 +846,7 @@ SPLAT_API int splat_cuda_get_option(splat_cuda_handle* h, uint32_t option, uint6
   switch (option) {
     case SPLAT_OPT_EXACT_BLEND: *value = h->exact; return SPLAT_OK;
     case SPLAT_OPT_PAIR_CAPACITY: *value = h->cap; return SPLAT_OK;
+    case SPLAT_OPT_PAIR_LIMIT: *value = h->pair_limit; return SPLAT_OK;
     case SPLAT_OPT_STAGE_EVENTS: *value = h->stage_events; return SPLAT_OK;
     case SPLAT_OPT_DEBUG_CAPTURE: *value = h->debug_capture; return SPLAT_OK;
     case SPLAT_OPT_FP64_CONICS: *value = h->have_frame ? h->st_host->fp64_conics : 0; return SPLAT_OK;
@@ -697,6 +856,9 @@ SPLAT_API int splat_cuda_get_option(splat_cuda_handle* h, uint32_t option, uint6
       return SPLAT_OK;
     case SPLAT_OPT_SCENE_SPLATS:
       *value = h->n;
+      return SPLAT_OK;
+    case SPLAT_OPT_INJECT_FAULT:
+      *value = h->inject_alloc ? SPLAT_FAULT_ALLOC : h->inject_lost_us ? (SPLAT_FAULT_LOST_WAIT | ((uint64_t)h->inject_lost_us << 8)) : 0;
       return SPLAT_OK;
     default: return fail(h, SPLAT_ERR_UNSUPPORTED, "unknown option");
   }

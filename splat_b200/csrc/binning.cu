@@ -357,108 +357,18 @@ __global__ void __launch_bounds__(kTileThreads) k_sort_mid(const uint2* __restri
   }
 }
 
-// Sorts the pairs of each tile longer than kMidSortCap, in
-// global memory (the pair buffer and the second pair buffer as ping-pong),
-// one CTA per tile: each pass of the tile sort runs over chunks of kLongChunk
-// words staged through shared memory, digit starts carried across chunks.
-constexpr int kLongChunk = 4096;
-
-struct LongSmem {
-  TileSortSmem t;
-  uint32_t run[256];  // running start of each digit across chunks
-  uint32_t key[kLongChunk];
-};
-
+// Sorts the pairs of each tile longer than kMidSortCap in global memory (the
+// pair buffer, the second pair buffer as ping-pong), one CTA per tile
+// (long_tile_sort: chunked LSD passes, ties ordered by splat index).
 __global__ void __launch_bounds__(kTileThreads) k_sort_long(const uint2* __restrict__ ranges,
                                                             const uint32_t* __restrict__ long_list,
                                                             uint64_t* __restrict__ w0, uint64_t* __restrict__ w1,
                                                             uint64_t cap, const DevState* st) {  // class 0
-  __shared__ LongSmem sm;
-  constexpr int kChunks = kLongChunk / (32 * kTileWarps);
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  __shared__ ChunkSortSmem sm;
   const uint32_t nlong = st->cls[0];
   for (uint32_t li = blockIdx.x; li < nlong; li += gridDim.x) {
     const uint2 r = ranges[long_list[li]];  // within the capacity (k_tile_ranges)
-    const uint32_t b = r.x, n = r.y - r.x;
-    uint32_t a = 0xFFFFFFFFu, o = 0u;
-    for (uint32_t e = tid; e < n; e += kTileThreads) {
-      const uint32_t k = (uint32_t)(w0[b + e] >> 32);
-      a &= k;
-      o |= k;
-    }
-    uint32_t and_all, or_all;
-    block_and_or(a, o, sm.t, and_all, or_all);
-    const uint32_t vary = and_all ^ or_all;
-    uint64_t* src = w0 + b;
-    uint64_t* dst = w1 + b;
-    for (int d = 0; d < 4; d++) {
-      const int shift = 32 + 8 * d;
-      if (((vary >> (8 * d)) & 255u) == 0u) continue;
-      // Digit starts over the whole tile.
-      clear_counts(sm.t);
-      __syncthreads();
-      for (uint32_t e = tid; e < n; e += kTileThreads) atomicAdd(&sm.t.wh[warp][(src[e] >> shift) & 255u], 1u);
-      __syncthreads();
-      digit_offsets(sm.t);
-      sm.run[tid] = sm.t.dstart[tid];
-      __syncthreads();
-      // Stable scatter, chunk by chunk in order.
-      for (uint32_t c0 = 0; c0 < n; c0 += kLongChunk) {
-        const uint32_t cn = min((uint32_t)kLongChunk, n - c0);
-        for (uint32_t e = tid; e < cn; e += kTileThreads) sm.key[e] = (uint32_t)(src[c0 + e] >> 32);
-        clear_counts(sm.t);
-        __syncthreads();
-        const uint32_t seg = (cn + kTileWarps - 1) / kTileWarps;
-        const uint32_t seg0 = min(cn, (uint32_t)warp * seg), seg1 = min(cn, seg0 + seg);
-        uint32_t k[kChunks], dr[kChunks];
-        warp_rank<kChunks>(sm.key, seg0, seg1, 8 * d, sm.t, k, dr);
-        __syncthreads();
-        // Exclusive per-warp offsets per digit; the chunk's count per digit.
-        uint32_t running = 0;
-#pragma unroll
-        for (int w = 0; w < kTileWarps; w++) {
-          const uint32_t t = sm.t.wh[w][tid];
-          sm.t.wh[w][tid] = running;
-          running += t;
-        }
-        __syncthreads();
-#pragma unroll
-        for (int c = 0; c < kChunks; c++) {
-          if (dr[c] != 0xFFFFFFFFu) {
-            const uint32_t dig = dr[c] & 255u;
-            dst[sm.run[dig] + sm.t.wh[warp][dig] + (dr[c] >> 8)] = src[c0 + seg0 + (uint32_t)c * 32 + lane];
-          }
-        }
-        __syncthreads();
-        sm.run[tid] += running;
-        __syncthreads();
-      }
-      uint64_t* t = src;
-      src = dst;
-      dst = t;
-    }
-    if (src != w0 + b) {
-      for (uint32_t e = tid; e < n; e += kTileThreads) w0[b + e] = src[e];
-    }
-    __syncthreads();
-    // fix_ties: runs of equal depth ordered by splat index.
-    for (uint32_t e = tid + 1; e < n; e += kTileThreads) {
-      const uint32_t kk = (uint32_t)(w0[b + e] >> 32);
-      if (kk == (uint32_t)(w0[b + e - 1] >> 32) && (e == 1 || (uint32_t)(w0[b + e - 2] >> 32) != kk)) {
-        uint32_t r1 = e + 1;
-        while (r1 < n && (uint32_t)(w0[b + r1] >> 32) == kk) r1++;
-        for (uint32_t i = e; i < r1; i++) {  // insertion sort of [e-1, r1) by splat index
-          const uint64_t x = w0[b + i];
-          uint32_t j = i;
-          while (j > e - 1 && (uint32_t)w0[b + j - 1] > (uint32_t)x) {
-            w0[b + j] = w0[b + j - 1];
-            j--;
-          }
-          w0[b + j] = x;
-        }
-      }
-    }
-    __syncthreads();
+    long_tile_sort(w0 + r.x, w1 + r.x, r.y - r.x, sm);
   }
 }
 

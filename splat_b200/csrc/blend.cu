@@ -279,10 +279,12 @@ __global__ void __launch_bounds__(NT, NT == 512 ? 2 : (NT == 256 ? 5 : 8)) k_ble
       sync();
       continue;
     }
-    // Rows [Y0, Y1) of the frame are rendered; output row = frame row - Y0.
+    // Rows [Y0, Y1) and columns [X0, X1) of the frame are rendered; output
+    // row = frame row - OY.
     const uint32_t W = tv->fp.w, Y0 = tv->fp.win_y0, Y1 = min(tv->fp.h, Y0 + tv->fp.win_rows);
+    const uint32_t X0 = tv->fp.win_x0, X1 = min(W, X0 + tv->fp.win_cols), OY = tv->fp.out_y0;
     const Record* __restrict__ rec = tv->rec;
-    const uint32_t ox = (local % tiles_x) * TW, oy = (local / tiles_x + tv->fp.win_ty0) * TH;
+    const uint32_t ox = (local % tiles_x + tv->fp.win_tx0) * TW, oy = (local / tiles_x + tv->fp.win_ty0) * TH;
     const uint32_t px = ox + lx;
 
     // EXACT: dx = lane + ((g*4) + ((ox16 + 0.5) - x)), dy = (py + 0.5) - y
@@ -299,7 +301,7 @@ __global__ void __launch_bounds__(NT, NT == 512 ? 2 : (NT == 256 ? 5 : 8)) k_ble
     for (int k = 0; k < PPT; k++) {
       T[k] = 1.0f;
       cr[k] = cg[k] = cb[k] = 0.0f;
-      done[k] = !(px < W && oy + ly0 + k >= Y0 && oy + ly0 + k < Y1);
+      done[k] = !(px >= X0 && px < X1 && oy + ly0 + k >= Y0 && oy + ly0 + k < Y1);
       all_done = all_done && done[k];
     }
 
@@ -440,7 +442,8 @@ __global__ void __launch_bounds__(NT, NT == 512 ? 2 : (NT == 256 ? 5 : 8)) k_ble
     // frames keep the per-pixel byte stores (a separate instantiation: the
     // word path costs the device-frame kernel about 4 %).
     constexpr uint32_t kRowWords = (TW * 3) / 4;  // TW is a multiple of 8
-    const bool rows = ROWS && f == 1 && W % 4u == 0 && ox + TW <= W && (reinterpret_cast<uintptr_t>(out) & 3u) == 0;
+    const bool rows = ROWS && f == 1 && W % 4u == 0 && ox >= X0 && ox + TW <= X1 &&
+                      (reinterpret_cast<uintptr_t>(out) & 3u) == 0;
 #pragma unroll
     for (int k = 0; k < PPT; k++) {
       const uint32_t ly = ly0 + k, py = oy + ly;
@@ -449,10 +452,10 @@ __global__ void __launch_bounds__(NT, NT == 512 ? 2 : (NT == 256 ? 5 : 8)) k_ble
       const uint32_t qb = to_u8(__fadd_rn(cb[k], __fmul_rn(T[k], bg2)));
       if (fused || rows) {
         sm.px[ly * TW + lx] = qr | (qg << 8) | (qb << 16);
-      } else if (px < W && py >= Y0 && py < Y1) {
+      } else if (px >= X0 && px < X1 && py >= Y0 && py < Y1) {
         // f == 1: the frame (window); other factors: the full-resolution
-        // scratch frame (whole frames only: Y0 = 0).
-        uint8_t* o = (f == 1 ? out : tv->full) + ((size_t)(py - Y0) * W + px) * 3;
+        // scratch frame (whole frames: OY = 0).
+        uint8_t* o = (f == 1 ? out : tv->full) + ((size_t)(py - OY) * W + px) * 3;
         o[0] = (uint8_t)qr;
         o[1] = (uint8_t)qg;
         o[2] = (uint8_t)qb;
@@ -469,7 +472,7 @@ __global__ void __launch_bounds__(NT, NT == 512 ? 2 : (NT == 256 ? 5 : 8)) k_ble
             const uint32_t bb = b0 + r;
             v |= ((sm.px[ly * TW + bb / 3u] >> (8u * (bb % 3u))) & 255u) << (8u * r);
           }
-          *reinterpret_cast<uint32_t*>(out + ((size_t)(py - Y0) * W + ox) * 3 + b0) = v;
+          *reinterpret_cast<uint32_t*>(out + ((size_t)(py - OY) * W + ox) * 3 + b0) = v;
         }
       }
     }

@@ -42,10 +42,15 @@ struct FrameParams {
   uint32_t tiles_x, tiles_y;
   uint32_t downsample;      // 1 = none
   uint32_t out_w, out_h;    // floor(w/f), floor(h/f)
-  // Rows [win_y0, win_y0 + win_rows) of the w x h frame are rendered (the
-  // whole frame: 0, h); the tile grid then covers tile rows [win_ty0,
-  // win_ty0 + tiles_y) and the output holds the window's rows (f = 1).
-  uint32_t win_y0, win_rows, win_ty0, pad;
+  // The window of the w x h frame that is rendered: rows [win_y0, win_y0 +
+  // win_rows), columns [win_x0, win_x0 + win_cols) (the whole frame: 0, h,
+  // 0, w); the tile grid then covers tile rows [win_ty0, win_ty0 + tiles_y)
+  // and tile columns [win_tx0, win_tx0 + tiles_x). Frame row y is output row
+  // y - out_y0 (row windows into a buffer of their own rows: out_y0 =
+  // win_y0; windows drawn into the whole frame: 0). A window that does not
+  // start at column 0 or end at the frame's edge is aligned to tiles.
+  uint32_t win_y0, win_rows, win_ty0, out_y0;
+  uint32_t win_x0, win_cols, win_tx0, pad;
 };
 
 // Device-resident scene, FP32 storage (layout chosen for coalesced loads).
@@ -68,7 +73,11 @@ struct SceneDev {
   const uint4* lat16;
   const uint16_t* mlp16;
   uint32_t learned;
-  uint32_t pad;
+  // Fault injection (tests of the timeout path): when nonzero, each CTA of
+  // the learned-colour projection also waits, at its first tensor-core wait,
+  // for a completion that never arrives, giving up after this many
+  // microseconds, as a lost completion would make it do.
+  uint32_t lost_wait_us;
 };
 
 // A projected splat as the blend reads it: 48 bytes, three float4.

@@ -32,6 +32,7 @@ struct splat_cuda_handle {
   splat::BinInfo* bin = nullptr;
   // pair buffers: per-tile buckets and the long-tile sort's scratch
   uint64_t cap = 0;
+  uint64_t pair_limit = splat::kMaxPairs;  // largest capacity; beyond it frames are drawn in windows
   uint64_t* pairs[2] = {nullptr, nullptr};
   // per-size buffers
   uint2* ranges = nullptr;
@@ -62,10 +63,18 @@ struct splat_cuda_handle {
   // options
   bool exact = false;
   bool stage_events = true;
+  // fault injection (SPLAT_OPT_INJECT_FAULT), each fires once
+  bool inject_alloc = false;    // the next device allocation fails as out of memory
+  uint32_t inject_lost_us = 0;  // the next frame's tensor-core waits meet a lost completion
   uint32_t launches = 0;  // kernels this handle has launched (wraps at 2^32)
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
-  // last frame
+  // last frame: the tile grid it was drawn with; the frame as requested,
+  // its destination and whether that is mapped host memory (for a frame
+  // that splat_cuda_finish has to draw again in windows)
   splat::FrameParams last_fp{};
+  splat::FrameParams last_req{};
+  uint8_t* last_out = nullptr;
+  bool last_mapped = false;
   bool have_frame = false;
   std::string err;
 };

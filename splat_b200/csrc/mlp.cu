@@ -64,6 +64,7 @@ struct TrainSmem {
   float b3[16];
   float db3[16];
   uint64_t mbar;
+  uint64_t lost;  // never arrived on: the injected lost completion (StepState::lost_wait_us)
   uint32_t tmem;
 };
 
@@ -75,7 +76,8 @@ struct StepState {
   unsigned long long loss_steps;
   float last_loss;
   unsigned int adam_done;     // CTAs of k_adam finished with the step
-  unsigned int error;         // a bounded wait gave up
+  unsigned int error;         // a bounded wait gave up (the step is dropped)
+  unsigned int lost_wait_us;  // fault injection: see SceneDev::lost_wait_us
 };
 
 enum class Src { kExplicit, kScene };
@@ -219,7 +221,10 @@ __global__ void __launch_bounds__(kTrainThreads) k_train(TrainArgs a) {
     S.b3[tid] = __half2float(__ushort_as_half(a.p16[mlp::kB3 + tid]));
     S.db3[tid] = 0.0f;
   }
-  if (tid == 0) umma::mbar_init(umma::smem_u32(&S.mbar), 1);
+  if (tid == 0) {
+    umma::mbar_init(umma::smem_u32(&S.mbar), 1);
+    umma::mbar_init(umma::smem_u32(&S.lost), 1);
+  }
   if (tid < 32) umma::tmem_alloc(&S.tmem, kTrainTmemCols);
   umma::fence_before_sync();
   __syncthreads();
@@ -238,11 +243,24 @@ __global__ void __launch_bounds__(kTrainThreads) k_train(TrainArgs a) {
   }
 
   uint32_t phase = 0;
-  bool timed_out = false, aborted = false;
+  bool timed_out = false, aborted = false, inflight = false;
   float loss = 0.0f;
+  // Fault injection (tests of the timeout path): the first wait also waits
+  // for a completion that never arrives, for at most lost_wait_us.
+  uint64_t lost_ns = 1000ull * *reinterpret_cast<volatile unsigned int*>(&a.st->lost_wait_us);
+  // Waits for the MMAs committed to `mbar`; after a wait that gave up, the
+  // phase stays the one still in flight, which the exit path waits for.
   auto wait_mma = [&]() {
-    if (!umma::mbar_wait(mbar, phase)) timed_out = true;
-    phase ^= 1u;
+    if (umma::mbar_wait(mbar, phase)) {
+      phase ^= 1u;
+      inflight = false;
+    } else {
+      timed_out = true;
+    }
+    if (lost_ns) {
+      if (!umma::mbar_wait(umma::smem_u32(&S.lost), 0, lost_ns)) timed_out = true;
+      lost_ns = 0;
+    }
     umma::fence_after_sync();
   };
   auto sync_or_abort = [&]() -> bool {
@@ -296,6 +314,7 @@ __global__ void __launch_bounds__(kTrainThreads) k_train(TrainArgs a) {
       mlp::gemm_k(tmem + kTS, sR, 8, umma::smem_u32(S.w1f), 64, 2, mlp::kIdN64);
       umma::commit(mbar);
     }
+    inflight = true;
     wait_mma();
     const uint64_t mask1 = mlp::hidden_epilogue(tmem, kTS, nullptr, S.R, tid);
     if (sync_or_abort()) { aborted = true; break; }
@@ -304,6 +323,7 @@ __global__ void __launch_bounds__(kTrainThreads) k_train(TrainArgs a) {
       mlp::gemm_k(tmem + kTS, sR, 0, umma::smem_u32(S.w2f), 64, 4, mlp::kIdN64);
       umma::commit(mbar);
     }
+    inflight = true;
     wait_mma();
     // Layer 2's epilogue with layer 3 and its backward on the CUDA cores:
     // h2 = fp16(relu(z2 + b2)) to Q chunks 0-7, z3 = W3 h2 + b3, rgb, loss,
@@ -376,6 +396,7 @@ __global__ void __launch_bounds__(kTrainThreads) k_train(TrainArgs a) {
                   umma::desc_mnmajor(sD3, mlp::kRows, 0, 16 * s), mlp::kIdWgN16, (first && s == 0) ? 0u : 1u);
       umma::commit(mbar);
     }
+    inflight = true;
     wait_mma();
     masked_epilogue(tmem, kTS, mask1, S.Q, 16, tid);  // dz1
     if (sync_or_abort()) { aborted = true; break; }
@@ -387,6 +408,7 @@ __global__ void __launch_bounds__(kTrainThreads) k_train(TrainArgs a) {
                   umma::desc_mnmajor(sR, mlp::kRows, 0, 16 * s), mlp::kIdWgN96, (first && s == 0) ? 0u : 1u);
       umma::commit(mbar);
     }
+    inflight = true;
     wait_mma();
     {
       float g[16];
@@ -437,7 +459,7 @@ __global__ void __launch_bounds__(kTrainThreads) k_train(TrainArgs a) {
   }
   if (aborted) {
     if (tid == 0) atomicExch(&a.st->error, 1u);
-    umma::mbar_wait(mbar, phase, 100000000ull);  // the MMAs still in flight, if any
+    if (inflight) umma::mbar_wait(mbar, phase, 100000000ull);  // the MMAs still in flight
   }
   umma::fence_before_sync();
   __syncthreads();
@@ -487,7 +509,23 @@ __global__ void __launch_bounds__(kAdamThreads) k_adam(float* __restrict__ p32, 
   const float inv = 1.0f / (kLossScale * (float)active);
   const float t = (float)(step + 1);
   const float c1 = 1.0f - powf(a.b1, t), c2 = 1.0f - powf(a.b2, t);
-  if (blockIdx.x < kAdamParamCtas) {
+  // A step whose training kernel gave up on a wait is dropped: its partial
+  // gradients are cleared and nothing is updated or counted.
+  const bool dropped = *reinterpret_cast<volatile unsigned int*>(&st->error) != 0u;
+  if (dropped) {
+    if (blockIdx.x < kAdamParamCtas) {
+      const uint32_t i = blockIdx.x * kAdamThreads + threadIdx.x;
+      if (i < mlp::kParams) grad[i] = 0.0f;
+    } else {
+      const uint64_t key = epoch_key(a.seed, step / a.steps_per_epoch);
+      for (uint32_t q = (blockIdx.x - kAdamParamCtas) * kAdamThreads + threadIdx.x; q < active;
+           q += (gridDim.x - kAdamParamCtas) * kAdamThreads) {
+        const uint64_t splat = mlp::shuffle_index(k * a.batch + q, a.samples, key, a.bits) / a.n_dirs;
+        float4* g4 = reinterpret_cast<float4*>(lat_grad + splat * 16);
+        for (int c = 0; c < 4; c++) g4[c] = make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+    }
+  } else if (blockIdx.x < kAdamParamCtas) {
     const uint32_t i = blockIdx.x * kAdamThreads + threadIdx.x;
     if (i < mlp::kParams) {
       const float g = grad[i] * inv;
@@ -546,6 +584,11 @@ __global__ void __launch_bounds__(kAdamThreads) k_adam(float* __restrict__ p32, 
     __threadfence();
     if (atomicAdd(&st->adam_done, 1u) == gridDim.x - 1) {
       __threadfence();
+      if (dropped) {
+        st->loss_step = 0.0;
+        st->adam_done = 0;
+        return;
+      }
       const double ls = *reinterpret_cast<volatile double*>(&st->loss_step) / (3.0 * (double)active);
       st->loss_step = 0.0;
       st->loss_sum += ls;
@@ -658,6 +701,7 @@ struct splat_cuda_learner {
   StepState* st = nullptr;
   cudaGraphExec_t graph = nullptr;  // kGraphSteps steps
   uint32_t launches = 0;
+  uint32_t inject_lost_us = 0;  // SPLAT_FAULT_LOST_WAIT for the next call
   std::string err;
 };
 
@@ -694,9 +738,17 @@ cudaError_t enqueue_step(splat_cuda_learner* L, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+// Waits for the learner's stream and reads the step state. A step whose
+// training kernel gave up on a wait was dropped (k_adam); the error is
+// reported once and cleared, so that the next call trains again. An
+// injected lost completion fires for one call only.
 int sync_state(splat_cuda_learner* L, StepState* out) {
   LCK(cudaStreamSynchronize(L->stream), "training step");
   LCK(cudaMemcpy(out, L->st, sizeof(StepState), cudaMemcpyDeviceToHost), "read step state");
+  if (out->lost_wait_us || out->error) {
+    LCK(cudaMemsetAsync(&L->st->error, 0, 2 * sizeof(unsigned int), L->stream), "clear step error");
+    LCK(cudaStreamSynchronize(L->stream), "clear step error");
+  }
   if (out->error) return lfail(L, SPLAT_ERR_TIMEOUT, "a tensor-core wait in the training kernel gave up");
   return SPLAT_OK;
 }
@@ -879,9 +931,22 @@ SPLAT_API int splat_cuda_learner_set_params(splat_cuda_learner* L, const float* 
   return SPLAT_OK;
 }
 
+// Arms an injected lost completion (SPLAT_FAULT_LOST_WAIT) for the steps the
+// call enqueues next; sync_state clears it.
+int arm_injection(splat_cuda_learner* L) {
+  if (!L->inject_lost_us) return SPLAT_OK;
+  LCK(cudaMemcpyAsync(&L->st->lost_wait_us, &L->inject_lost_us, sizeof(unsigned int), cudaMemcpyHostToDevice,
+                      L->stream),
+      "fault injection");
+  LCK(cudaStreamSynchronize(L->stream), "fault injection");
+  L->inject_lost_us = 0;
+  return SPLAT_OK;
+}
+
 SPLAT_API int splat_cuda_learner_train(splat_cuda_learner* L, uint64_t steps, splat_learn_stats* stats) {
   if (!L) return SPLAT_ERR_INVALID_ARG;
   LCK(cudaSetDevice(L->device), "cudaSetDevice");
+  if (int rc = arm_injection(L)) return rc;
   LCK(cudaMemsetAsync(&L->st->loss_sum, 0, sizeof(double) + sizeof(unsigned long long), L->stream), "reset loss");
   if (!L->graph && steps >= kGraphSteps) {
     cudaGraph_t g = nullptr;
@@ -935,6 +1000,7 @@ SPLAT_API int splat_cuda_learner_train(splat_cuda_learner* L, uint64_t steps, sp
 SPLAT_API int splat_cuda_learner_step_debug(splat_cuda_learner* L, float* grad_params, float* grad_latents) {
   if (!L) return SPLAT_ERR_INVALID_ARG;
   LCK(cudaSetDevice(L->device), "cudaSetDevice");
+  if (int rc = arm_injection(L)) return rc;
   LCK(launch_train<Src::kScene>(L->args, L->grid, L->sh_degree, L->stream), "training kernel");
   L->launches += 1;
   StepState st;
@@ -991,6 +1057,24 @@ SPLAT_API int splat_cuda_learner_get_option(const splat_cuda_learner* L, uint32_
     case SPLAT_LEARN_SHUFFLE_BITS: *value = L->bits; return SPLAT_OK;
     case SPLAT_LEARN_TRAIN_CTAS: *value = L->grid; return SPLAT_OK;
     default: return SPLAT_ERR_UNSUPPORTED;
+  }
+}
+
+SPLAT_API int splat_cuda_learner_set_option(splat_cuda_learner* L, uint32_t option, uint64_t value) {
+  if (!L) return SPLAT_ERR_INVALID_ARG;
+  switch (option) {
+    case SPLAT_OPT_INJECT_FAULT:
+      if ((value & 0xFFu) == SPLAT_FAULT_LOST_WAIT) {
+        L->inject_lost_us = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(value >> 8, 10000000ull));
+        return SPLAT_OK;
+      }
+      if (value == 0) {
+        L->inject_lost_us = 0;
+        return SPLAT_OK;
+      }
+      return lfail(L, SPLAT_ERR_UNSUPPORTED, "the learner injects SPLAT_FAULT_LOST_WAIT only");
+    default:
+      return lfail(L, SPLAT_ERR_UNSUPPORTED, "unknown option");
   }
 }
 

@@ -232,13 +232,15 @@ __device__ __forceinline__ void project_splat(const FrameParams& fp, const Scene
       r.r2 = make_float4(col[2], __uint_as_float(bx0 | (x1 << 16)), __uint_as_float(by0 | (y1 << 16)), tz);
       rec[i] = r;
       b.depth_bits = __float_as_uint(tz);
-      // Tile rows clipped to the rendered window and counted from its first
-      // tile row (the whole frame: unchanged).
+      // Tile rows and columns clipped to the rendered window and counted
+      // from its first tile row and column (the whole frame: unchanged).
       const uint32_t wty0 = max(by0 >> fp.tile_sy, fp.win_ty0);
       const uint32_t wty1 = min((y1 + fp.tile_h - 1) >> fp.tile_sy, fp.win_ty0 + fp.tiles_y);
-      if (bx0 < x1 && by0 < y1 && wty0 < wty1) {
-        const uint32_t tx0 = bx0 >> fp.tile_sx, ty0 = wty0 - fp.win_ty0;
-        const uint32_t tx1 = (x1 + fp.tile_w - 1) >> fp.tile_sx, ty1 = wty1 - fp.win_ty0;
+      const uint32_t wtx0 = max(bx0 >> fp.tile_sx, fp.win_tx0);
+      const uint32_t wtx1 = min((x1 + fp.tile_w - 1) >> fp.tile_sx, fp.win_tx0 + fp.tiles_x);
+      if (bx0 < x1 && by0 < y1 && wty0 < wty1 && wtx0 < wtx1) {
+        const uint32_t tx0 = wtx0 - fp.win_tx0, ty0 = wty0 - fp.win_ty0;
+        const uint32_t tx1 = wtx1 - fp.win_tx0, ty1 = wty1 - fp.win_ty0;
         b.rect_lo = tx0 | (ty0 << 16);
         b.rect_hi = tx1 | (ty1 << 16);
         b.count = (tx1 - tx0) * (ty1 - ty0);
@@ -333,6 +335,7 @@ struct LearnedSmem {
   mlp::ForwardTiles t;
   ViewTask vt;  // the current tile's view
   uint64_t mbar;
+  uint64_t lost;  // never arrived on: the injected lost completion (SceneDev::lost_wait_us)
   uint32_t tmem;
 };
 // At most 7 CTAs fit an SM by shared memory (228 KB, 1 KB reserved per CTA),
@@ -352,7 +355,10 @@ __global__ void __launch_bounds__(kLearnedThreads, 7)
   LearnedSmem& S = *reinterpret_cast<LearnedSmem*>(smem_raw);
   const uint32_t tid = threadIdx.x;
   if (!BATCH && blockIdx.x == 0 && tid == 0) *table = t0;
-  if (tid == 0) umma::mbar_init(umma::smem_u32(&S.mbar), 1);
+  if (tid == 0) {
+    umma::mbar_init(umma::smem_u32(&S.mbar), 1);
+    umma::mbar_init(umma::smem_u32(&S.lost), 1);
+  }
   if (tid < 32) umma::tmem_alloc(&S.tmem, kLearnedTmemCols);
   umma::fence_before_sync();
   __syncthreads();
@@ -360,10 +366,21 @@ __global__ void __launch_bounds__(kLearnedThreads, 7)
   const uint32_t tmem = S.tmem, mbar = umma::smem_u32(&S.mbar);
   const uint32_t act = umma::smem_u32(S.t.act);
   uint32_t phase = 0;
-  bool timed_out = false, aborted = false;
+  bool timed_out = false, aborted = false, inflight = false;
+  uint64_t lost_ns = BATCH ? 0ull : 1000ull * t0.s.lost_wait_us;
+  // Waits for the MMAs committed to `mbar`; after a wait that gave up, the
+  // phase stays the one still in flight, which the exit path waits for.
   auto wait_mma = [&]() {
-    if (!umma::mbar_wait(mbar, phase)) timed_out = true;
-    phase ^= 1u;
+    if (umma::mbar_wait(mbar, phase)) {
+      phase ^= 1u;
+      inflight = false;
+    } else {
+      timed_out = true;
+    }
+    if (lost_ns) {
+      if (!umma::mbar_wait(umma::smem_u32(&S.lost), 0, lost_ns)) timed_out = true;
+      lost_ns = 0;
+    }
     umma::fence_after_sync();
   };
   auto sync_or_abort = [&]() -> bool {
@@ -415,6 +432,7 @@ __global__ void __launch_bounds__(kLearnedThreads, 7)
       mlp::gemm_k(tmem, act, 0, umma::smem_u32(S.t.w1f), 64, 2, mlp::kIdN64);
       umma::commit(mbar);
     }
+    inflight = true;
     wait_mma();
     mlp::relu_epilogue(tmem, 0, nullptr, S.t.act, tid);  // h1 over x (layer 1 is done)
     if (sync_or_abort()) { aborted = true; break; }
@@ -423,6 +441,7 @@ __global__ void __launch_bounds__(kLearnedThreads, 7)
       mlp::gemm_k(tmem, act, 0, umma::smem_u32(S.t.w2f), 64, 4, mlp::kIdN64);
       umma::commit(mbar);
     }
+    inflight = true;
     wait_mma();
     mlp::relu_epilogue(tmem, 0, S.t.b2, S.t.act, tid);  // h2 over h1 (layer 2 is done)
     if (sync_or_abort()) { aborted = true; break; }
@@ -431,6 +450,7 @@ __global__ void __launch_bounds__(kLearnedThreads, 7)
       mlp::gemm_k(tmem, act, 0, umma::smem_u32(S.t.w3f), 16, 4, mlp::kIdN16);
       umma::commit(mbar);
     }
+    inflight = true;
     wait_mma();
     float z[16];
     umma::tmem_ld16(umma::tmem_warp_addr(tmem, 0), z);
@@ -450,7 +470,7 @@ __global__ void __launch_bounds__(kLearnedThreads, 7)
   if (!aborted && __syncthreads_or(timed_out)) aborted = true;
   if (aborted) {
     if (tid == 0) atomicExch(&fc.st->error, 1u);
-    umma::mbar_wait(mbar, phase, 100000000ull);  // an MMA still in flight, if any
+    if (inflight) umma::mbar_wait(mbar, phase, 100000000ull);  // the MMA still in flight
   }
   umma::fence_before_sync();
   __syncthreads();

@@ -77,17 +77,30 @@ __device__ __forceinline__ DepthQuant make_quant(uint32_t min_bits, uint32_t max
   return DepthQuant{dmin, range > 0.0f ? 65535.0f / range : 0.0f};
 }
 
-// Orders each run of items with equal quantised key by their full word
-// (insertion sort by the run's first thread; runs are short except for
-// degenerate depth distributions). q(item) gives the quantised key, w(item)
-// the 64-bit word (depth bits, splat index) the run is ordered by.
+// Runs of equal quantised key up to this length are ordered by one thread
+// (insertion sort: at most kMaxInsertRun^2 / 2 steps); a tile holding a
+// longer run is sorted again as a whole by bitonic_sort (degenerate depth
+// distributions: a plane seen head-on gives every pair of a tile one depth).
+constexpr uint32_t kMaxInsertRun = 32;
+
+// Orders each run of at most kMaxInsertRun items with equal quantised key by
+// their full word, the run's first thread sorting it. q(item) gives the
+// quantised key, w(item) the 64-bit word (depth bits, splat index) the run is
+// ordered by. Returns true in a thread that found a longer run, which it
+// leaves as it is (the caller then sorts the whole tile with bitonic_sort).
 template <class Item, class Q, class W>
-__device__ __forceinline__ void sort_runs(Item* items, uint32_t n, uint32_t tid, uint32_t nthreads, Q&& q, W&& w) {
+__device__ __forceinline__ bool sort_short_runs(Item* items, uint32_t n, uint32_t tid, uint32_t nthreads, Q&& q,
+                                                W&& w) {
+  bool long_run = false;
   for (uint32_t e = tid + 1; e < n; e += nthreads) {
     const uint32_t qq = q(items[e]);
     if (qq == q(items[e - 1]) && (e == 1 || q(items[e - 2]) != qq)) {
       uint32_t r1 = e + 1;
-      while (r1 < n && q(items[r1]) == qq) r1++;
+      while (r1 < n && r1 - (e - 1) <= kMaxInsertRun && q(items[r1]) == qq) r1++;
+      if (r1 - (e - 1) > kMaxInsertRun) {
+        long_run = true;
+        continue;
+      }
       for (uint32_t i = e; i < r1; i++) {
         const Item x = items[i];
         const uint64_t wx = w(x);
@@ -98,6 +111,34 @@ __device__ __forceinline__ void sort_runs(Item* items, uint32_t n, uint32_t tid,
         }
         items[j] = x;
       }
+    }
+  }
+  return long_run;
+}
+
+// Bitonic sort of words[0, n) (n <= cap, cap a power of two, the array
+// holding cap words) by the full word, ascending, by `nthreads` threads
+// (thread tid) with sync() between the steps: words[n, m) are padded with
+// ~0 up to the power of two m >= n. A tile holds each splat at most once, so
+// its words are distinct and the order is exactly (depth, splat index).
+template <class Sync>
+__device__ __forceinline__ void bitonic_sort(uint64_t* words, uint32_t n, uint32_t tid, uint32_t nthreads,
+                                             Sync&& sync) {
+  uint32_t m = 1;
+  while (m < n) m <<= 1;
+  for (uint32_t e = n + tid; e < m; e += nthreads) words[e] = ~0ull;
+  sync();
+  for (uint32_t k = 2; k <= m; k <<= 1) {
+    for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+      for (uint32_t i = tid; i < m / 2; i += nthreads) {
+        const uint32_t lo = 2 * i - (i & (j - 1)), hi = lo + j;
+        const uint64_t a = words[lo], b = words[hi];
+        if ((a > b) == ((lo & k) == 0)) {
+          words[lo] = b;
+          words[hi] = a;
+        }
+      }
+      sync();
     }
   }
 }
@@ -170,6 +211,109 @@ __device__ __forceinline__ void clear_counts(TileSortSmem& sm) {
   for (int w = 0; w < kTileWarps; w++) sm.wh[w][threadIdx.x] = 0u;
 }
 
+// Long tiles (more pairs than shared memory holds): stable LSD passes in
+// global memory, each over chunks of kSortChunk words staged through shared
+// memory, digit starts carried across chunks, ping-pong between the tile's
+// words and a scratch range of the same length.
+constexpr int kSortChunk = 4096;
+
+struct ChunkSortSmem {
+  TileSortSmem t;
+  uint32_t run[256];  // running start of each digit across chunks
+  uint32_t key[kSortChunk];
+};
+
+// Stable LSD passes over the bytes of the 64-bit words whose bit is set in
+// `bytes` (bit b: byte b, least significant first; byte 4 is the low byte of
+// the depth bits), from src into dst and back. Returns the buffer holding
+// the result. One CTA of kTileThreads threads.
+__device__ __forceinline__ uint64_t* chunked_lsd(uint64_t* src, uint64_t* dst, uint32_t n, uint32_t bytes,
+                                                 ChunkSortSmem& sm) {
+  constexpr int kChunks = kSortChunk / (32 * kTileWarps);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  for (int byte = 0; byte < 8; byte++) {
+    if (!((bytes >> byte) & 1u)) continue;
+    const int shift = 8 * byte, half = byte >> 2, dshift = 8 * (byte & 3);
+    // Digit starts over the whole tile.
+    clear_counts(sm.t);
+    __syncthreads();
+    for (uint32_t e = tid; e < n; e += kTileThreads) atomicAdd(&sm.t.wh[warp][(src[e] >> shift) & 255u], 1u);
+    __syncthreads();
+    digit_offsets(sm.t);
+    sm.run[tid] = sm.t.dstart[tid];
+    __syncthreads();
+    // Stable scatter, chunk by chunk in order.
+    for (uint32_t c0 = 0; c0 < n; c0 += kSortChunk) {
+      const uint32_t cn = min((uint32_t)kSortChunk, n - c0);
+      for (uint32_t e = tid; e < cn; e += kTileThreads) sm.key[e] = (uint32_t)(src[c0 + e] >> (32 * half));
+      clear_counts(sm.t);
+      __syncthreads();
+      const uint32_t seg = (cn + kTileWarps - 1) / kTileWarps;
+      const uint32_t seg0 = min(cn, (uint32_t)warp * seg), seg1 = min(cn, seg0 + seg);
+      uint32_t k[kChunks], dr[kChunks];
+      warp_rank<kChunks>(sm.key, seg0, seg1, dshift, sm.t, k, dr);
+      __syncthreads();
+      // Exclusive per-warp offsets per digit; the chunk's count per digit.
+      uint32_t running = 0;
+#pragma unroll
+      for (int w = 0; w < kTileWarps; w++) {
+        const uint32_t t = sm.t.wh[w][tid];
+        sm.t.wh[w][tid] = running;
+        running += t;
+      }
+      __syncthreads();
+#pragma unroll
+      for (int c = 0; c < kChunks; c++) {
+        if (dr[c] != 0xFFFFFFFFu) {
+          const uint32_t dig = dr[c] & 255u;
+          dst[sm.run[dig] + sm.t.wh[warp][dig] + (dr[c] >> 8)] = src[c0 + seg0 + (uint32_t)c * 32 + lane];
+        }
+      }
+      __syncthreads();
+      sm.run[tid] += running;
+      __syncthreads();
+    }
+    uint64_t* t = src;
+    src = dst;
+    dst = t;
+  }
+  return src;
+}
+
+// Sorts words[0, n) in place by the full word (depth bits, then splat
+// index: the reference's sort_hi32 + fix_ties order), scratch[0, n) as the
+// ping-pong range. The depth bytes that vary over the tile are sorted first;
+// if that leaves two equal depths next to each other, the tile is sorted
+// again over the varying bytes of the splat index and then of the depth
+// (LSD over the whole word), so ties never cost more than linear passes.
+__device__ __forceinline__ void long_tile_sort(uint64_t* words, uint64_t* scratch, uint32_t n, ChunkSortSmem& sm) {
+  const int tid = threadIdx.x;
+  uint32_t ah = 0xFFFFFFFFu, oh = 0u, al = 0xFFFFFFFFu, ol = 0u;
+  for (uint32_t e = tid; e < n; e += kTileThreads) {
+    const uint64_t w = words[e];
+    ah &= (uint32_t)(w >> 32);
+    oh |= (uint32_t)(w >> 32);
+    al &= (uint32_t)w;
+    ol |= (uint32_t)w;
+  }
+  uint32_t and_hi, or_hi, and_lo, or_lo;
+  block_and_or(ah, oh, sm.t, and_hi, or_hi);
+  block_and_or(al, ol, sm.t, and_lo, or_lo);
+  const uint32_t vary_hi = and_hi ^ or_hi, vary_lo = and_lo ^ or_lo;
+  uint32_t depth_bytes = 0, index_bytes = 0;
+  for (int b = 0; b < 4; b++) {
+    if ((vary_hi >> (8 * b)) & 255u) depth_bytes |= 1u << (4 + b);
+    if ((vary_lo >> (8 * b)) & 255u) index_bytes |= 1u << b;
+  }
+  uint64_t* res = chunked_lsd(words, scratch, n, depth_bytes, sm);
+  bool tie = false;
+  for (uint32_t e = tid + 1; e < n; e += kTileThreads) tie |= (res[e] >> 32) == (res[e - 1] >> 32);
+  if (__syncthreads_or(tie)) res = chunked_lsd(res, res == words ? scratch : words, n, index_bytes | depth_bytes, sm);
+  if (res != words)
+    for (uint32_t e = tid; e < n; e += kTileThreads) words[e] = res[e];
+  __syncthreads();
+}
+
 // CTA sort of one tile's n <= kMidSortCap words (already in shared memory,
 // their depth-bit range [mn, mx] known): one counting pass on the depth
 // quantised to 12 bits over that range, q = min(4095, (d - dmin) * 4095 /
@@ -187,7 +331,7 @@ struct CountSortSmem {
   uint32_t wsum[kTileWarps];
 };
 
-__device__ __forceinline__ void smem_count_sort(const uint64_t* words, uint32_t n, uint32_t mn, uint32_t mx,
+__device__ __forceinline__ void smem_count_sort(uint64_t* words, uint32_t n, uint32_t mn, uint32_t mx,
                                                 uint32_t* hist /* kCountBuckets / 2 words */, uint16_t* slot,
                                                 CountSortSmem& sm) {
   static_assert(kCountBuckets == 16 * kTileThreads, "16 counters per thread");
@@ -246,8 +390,12 @@ __device__ __forceinline__ void smem_count_sort(const uint64_t* words, uint32_t 
     slot[(atomicAdd(&hist[q >> 1], 1u << sh) >> sh) & 0xFFFFu] = (uint16_t)e;
   }
   __syncthreads();
-  sort_runs(
+  const bool long_run = sort_short_runs(
       slot, n, tid, kTileThreads, [&](uint16_t i) { return quant(words[i]); }, [&](uint16_t i) { return words[i]; });
+  if (__syncthreads_or(long_run)) {
+    bitonic_sort(words, n, tid, kTileThreads, [] { __syncthreads(); });
+    for (uint32_t e = tid; e < n; e += kTileThreads) slot[e] = (uint16_t)e;
+  }
   __syncthreads();
 }
 
@@ -364,8 +512,9 @@ __device__ __forceinline__ void warp_sort_tile(uint64_t* __restrict__ words, uin
     if (j < m && e < n) scratch[e] = w[j];
   }
   __syncwarp();
-  sort_runs(
+  const bool long_run = sort_short_runs(
       scratch, n, lane, 32, [&](uint64_t x) { return quant(x); }, [](uint64_t x) { return x; });
+  if (__any_sync(0xffffffffu, long_run)) bitonic_sort(scratch, n, lane, 32, [] { __syncwarp(); });
   __syncwarp();
   for (uint32_t e = lane; e < n; e += 32) words[e] = scratch[e];
   __syncwarp();

@@ -74,6 +74,9 @@ class Learner:
         self._check(N.lib().splat_cuda_learner_get_option(self._h, opt, ctypes.byref(v)), "get_option")
         return int(v.value)
 
+    def set_option(self, opt: int, value: int):
+        self._check(N.lib().splat_cuda_learner_set_option(self._h, opt, int(value)), "set_option")
+
     @property
     def steps_per_epoch(self) -> int:
         return self.option(N.LEARN_STEPS_PER_EPOCH)

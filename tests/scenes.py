@@ -192,3 +192,25 @@ def needles(n=20_000, seed=5, length=4.0, thickness=1e-4) -> Scene:
     s.opacities = rng.uniform(0.3, 1.0, n).astype(np.float32)
     s.colors = rng.uniform(0.0, 1.0, (n, 3)).astype(np.float32)
     return s.finalize()
+
+
+def planes(n_big=20_000, n_small=20_000, seed=13, depths=(5.0, 6.0)) -> Scene:
+    """Splats on planes facing a camera at the origin that looks along +z
+    (View.looking_along_z): every splat of a plane has the same depth bits
+    (t.z = 0 x + 0 y + 1 z exactly), so each tile's pairs fall into a few
+    runs of equal depth that only the splat index orders (the reference's
+    fix_ties, src/render/cpu.rs:396-414). Large splats crowd the centre, so
+    central tiles hold tens of thousands of pairs, outer tiles hundreds."""
+    rng = np.random.default_rng(seed)
+    n = n_big + n_small
+    z = np.asarray(depths, np.float32)[rng.integers(0, len(depths), n)]
+    xy = np.concatenate([rng.normal(0.0, 0.4, (n_big, 2)), rng.uniform(-3.0, 3.0, (n_small, 2))])
+    s = Scene()
+    s.positions = np.stack([xy[:, 0] * z / 5.0, xy[:, 1] * z / 5.0, z], 1).astype(np.float32)
+    sig = np.concatenate([rng.uniform(0.25, 0.6, n_big), rng.uniform(0.01, 0.05, n_small)])
+    s.scales = np.stack([sig, sig * rng.uniform(0.5, 1.0, n), np.full(n, 0.01)], 1).astype(np.float32)
+    ang = rng.uniform(0, np.pi, n)
+    s.rotations = np.stack([np.zeros(n), np.zeros(n), np.sin(ang / 2), np.cos(ang / 2)], 1).astype(np.float32)
+    s.opacities = rng.uniform(0.05, 0.6, n).astype(np.float32)
+    s.colors = rng.uniform(0.0, 1.0, (n, 3)).astype(np.float32)
+    return s.finalize()

@@ -66,6 +66,39 @@ def test_no_alloc_sort_matches_render_order():
         assert np.array_equal(got, want), f"tile {t}: {np.sum(got != want)} of {len(want)} pairs out of order"
 
 
+def _words(rng, n, depth_levels):
+    """n distinct pair words: depth bits from `depth_levels` distinct positive
+    floats (few levels: long runs of equal depth), splat indices distinct."""
+    depths = np.sort(rng.uniform(0.5, 40.0, depth_levels).astype(np.float32)).view(np.uint32)
+    d = depths[rng.integers(0, depth_levels, n)].astype(np.uint64)
+    idx = rng.choice(1 << 24, n, replace=False).astype(np.uint64)
+    return (d << np.uint64(32)) | idx
+
+
+@pytest.mark.parametrize("n,levels", [(4097, 3), (300_000, 1000), (300_000, 1), (MAX_PAIRS, 50_000),
+                                      (MAX_PAIRS, 2)])
+def test_no_alloc_sort_matches_full_word_order(n, levels):
+    """Tiles longer than one shared-memory chunk (the carried digit starts),
+    depth bytes that do not vary (skipped passes), the size limit, and runs
+    of equal depth up to the whole tile: the result is the words in
+    ascending order (depth bits, then splat index), equal to a sort of the
+    words on the host; three calls in a row reuse the scratch array."""
+    import torch
+
+    lib = N.lib()
+    rng = np.random.default_rng(n + levels)
+    for call in range(3):
+        words = _words(rng, n, levels)
+        dev = torch.from_numpy(words.view(np.int64)).cuda()
+        rc = lib.splat_cuda_sort_tile_noalloc(ctypes.c_void_p(dev.data_ptr()), n,
+                                              ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+        assert rc == N.SPLAT_OK
+        torch.cuda.synchronize()
+        got = dev.cpu().numpy().view(np.uint64)
+        want = np.sort(words)
+        assert np.array_equal(got, want), f"call {call}: {np.sum(got != want)} of {n} words out of order"
+
+
 def test_no_alloc_sort_rejects_more_than_its_scratch():
     rc = N.lib().splat_cuda_sort_tile_noalloc(ctypes.c_void_p(0), MAX_PAIRS + 1, None)
     assert rc == N.SPLAT_ERR_INVALID_ARG
