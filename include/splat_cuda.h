@@ -271,6 +271,12 @@ void* splat_cuda_get_stream(splat_cuda_handle* h);
  *                          its tensor memory, a training step is dropped, and
  *                          the next call runs normally. */
 #define SPLAT_OPT_INJECT_FAULT 10u
+#define SPLAT_OPT_COUNT_EVALS 11u  /* 1: the blend (16x16 tiles, 512 threads, not
+                                      exact) also counts its pixel/splat
+                                      evaluations; a measurement mode */
+#define SPLAT_OPT_BLEND_EVALS 12u  /* read-only: pixel/splat evaluations of the
+                                      last completed frame (0 unless counted):
+                                      the blend's work after early termination */
 #define SPLAT_FAULT_ALLOC 1u
 #define SPLAT_FAULT_LOST_WAIT 2u
 int splat_cuda_set_option(splat_cuda_handle* h, uint32_t option, uint64_t value);
@@ -475,6 +481,16 @@ int splat_cuda_learner_set_params(splat_cuda_learner* l, const float* params, co
  * (what splat_cuda_create_learned takes). */
 int splat_cuda_learner_params(splat_cuda_learner* l, float* params, float* latents, uint16_t* params_f16,
                               uint16_t* latents_f16);
+/* Checkpoint of the training state: the fp32 parameter and latent masters,
+ * their Adam moments, the latent rows' update stamps, the step count (Adam's
+ * bias correction and the position in the epoch's shuffle) and the loss
+ * record, as one byte blob with a header. A learner for the same scene and
+ * configuration (splats, directions, batch, seed, SH degree; checked on
+ * load) that loads it trains on from where the saver stopped, step for step.
+ * No counterpart in the reference (which renders only). */
+size_t splat_cuda_learner_state_bytes(const splat_cuda_learner* l);
+int splat_cuda_learner_save_state(splat_cuda_learner* l, void* out, size_t bytes);
+int splat_cuda_learner_load_state(splat_cuda_learner* l, const void* data, size_t bytes);
 /* One step that also reports its gradient before Adam applies it: d loss /
  * d params (SPLAT_MLP_PARAMS) and d loss / d latents (n * 16, zero for rows
  * the step did not sample); either may be NULL. */

@@ -35,6 +35,8 @@ SPLAT_OPT_PAIR_LIMIT = 9
 SPLAT_OPT_INJECT_FAULT = 10
 SPLAT_FAULT_ALLOC = 1
 SPLAT_FAULT_LOST_WAIT = 2
+SPLAT_OPT_COUNT_EVALS = 11
+SPLAT_OPT_BLEND_EVALS = 12
 
 SPLAT_CELLS_TRUECOLOR = 0
 SPLAT_CELLS_ANSI256 = 1
@@ -55,7 +57,8 @@ EXPORTS = [
     "splat_cuda_create_learned", "splat_cuda_learner_create", "splat_cuda_learner_create_error",
     "splat_cuda_learner_train", "splat_cuda_learner_set_params", "splat_cuda_learner_params",
     "splat_cuda_learner_step_debug", "splat_cuda_learner_directions", "splat_cuda_learner_get_option",
-    "splat_cuda_learner_set_option",
+    "splat_cuda_learner_set_option", "splat_cuda_learner_state_bytes", "splat_cuda_learner_save_state",
+    "splat_cuda_learner_load_state",
     "splat_cuda_learner_last_error", "splat_cuda_learner_destroy", "splat_cuda_mlp_gradient",
     "splat_cuda_create_from_splat", "splat_cuda_create_from_ply", "splat_cuda_render_cells",
 ]
@@ -184,6 +187,10 @@ def lib():
         L.splat_cuda_learner_directions.argtypes = [vp, vp]
         L.splat_cuda_learner_get_option.argtypes = [vp, u32, ctypes.POINTER(u64)]
         L.splat_cuda_learner_set_option.argtypes = [vp, u32, u64]
+        L.splat_cuda_learner_state_bytes.argtypes = [vp]
+        L.splat_cuda_learner_state_bytes.restype = ctypes.c_size_t
+        L.splat_cuda_learner_save_state.argtypes = [vp, vp, ctypes.c_size_t]
+        L.splat_cuda_learner_load_state.argtypes = [vp, vp, ctypes.c_size_t]
         L.splat_cuda_learner_last_error.argtypes = [vp]
         L.splat_cuda_learner_last_error.restype = ctypes.c_char_p
         L.splat_cuda_learner_destroy.argtypes = [vp]

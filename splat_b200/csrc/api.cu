@@ -217,8 +217,84 @@ FrameParams make_params(const splat_view_desc& v, uint32_t w, uint32_t hgt, cons
 }
 
 SceneDev scene_dev(const splat_cuda_handle* h) {
-  return SceneDev{h->pos_op, h->cov_a, h->cov_b, h->color, h->sh, h->pos_k, h->geom16, h->sh16, h->n, h->sh_degree,
-                  h->precision == SPLAT_PRECISION_FP16 ? 1u : 0u, h->lat16, h->mlp16, h->lat16 ? 1u : 0u, 0u};
+  SceneDev s{};
+  s.pos_op = h->pos_op;
+  s.cov_a = h->cov_a;
+  s.cov_b = h->cov_b;
+  s.color = h->color;
+  s.sh = h->sh;
+  s.pos_k = h->pos_k;
+  s.geom16 = h->geom16;
+  s.sh16 = h->sh16;
+  s.n = h->n;
+  s.sh_degree = h->sh_degree;
+  s.fp16 = h->precision == SPLAT_PRECISION_FP16 ? 1u : 0u;
+  s.lat16 = h->lat16;
+  s.mlp16 = h->mlp16;
+  s.learned = h->lat16 ? 1u : 0u;
+  s.order = h->bin_order;
+  s.lost_wait_us = 0u;
+  return s;
+}
+
+// The binning order (SceneDev::order): the splats sorted by the 3D Morton
+// code of their position (10 bits per axis over the positions' bounding
+// box; non-finite positions first), equal codes in scene order. Computed once
+// per scene from the device copy of the positions.
+int build_binning_order(splat_cuda_handle* h) {
+  const uint64_t n = h->n;
+  if (n < 2) return SPLAT_OK;
+  std::vector<float4> pos(n);
+  const float4* src = h->precision == SPLAT_PRECISION_FP16 ? h->pos_k : h->pos_op;
+  cudaError_t e = cudaMemcpy(pos.data(), src, n * sizeof(float4), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_fail(h, e, "read positions");
+  float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (const float4& p : pos) {
+    const float c[3] = {p.x, p.y, p.z};
+    for (int k = 0; k < 3; k++)
+      if (std::isfinite(c[k])) {
+        lo[k] = std::min(lo[k], c[k]);
+        hi[k] = std::max(hi[k], c[k]);
+      }
+  }
+  auto spread = [](uint32_t v) {  // 10 bits -> every third bit of 30
+    v &= 1023u;
+    v = (v | (v << 16)) & 0x030000FFu;
+    v = (v | (v << 8)) & 0x0300F00Fu;
+    v = (v | (v << 4)) & 0x030C30C3u;
+    v = (v | (v << 2)) & 0x09249249u;
+    return v;
+  };
+  std::vector<uint64_t> key(n), tmp(n);
+  for (uint64_t i = 0; i < n; i++) {
+    const float c[3] = {pos[i].x, pos[i].y, pos[i].z};
+    uint32_t code = 0;
+    bool finite = true;
+    for (int k = 0; k < 3; k++) {
+      finite = finite && std::isfinite(c[k]);
+      const float ext = hi[k] - lo[k];
+      const float t = ext > 0.0f ? (c[k] - lo[k]) / ext : 0.0f;
+      const uint32_t q = finite ? (uint32_t)std::min(1023.0f, std::max(0.0f, t * 1023.0f)) : 0u;
+      code |= spread(q) << k;
+    }
+    key[i] = ((uint64_t)(finite ? code + 1 : 0) << 32) | i;
+  }
+  // LSD radix sort of the codes (bits 32..62), stable: equal codes keep scene order.
+  for (int shift = 32; shift < 63; shift += 11) {
+    std::vector<uint32_t> cnt(2049, 0);
+    for (uint64_t k : key) cnt[((k >> shift) & 2047u) + 1]++;
+    for (int d = 0; d < 2048; d++) cnt[d + 1] += cnt[d];
+    for (uint64_t k : key) tmp[cnt[(k >> shift) & 2047u]++] = k;
+    key.swap(tmp);
+  }
+  std::vector<uint32_t> order(n);
+  for (uint64_t i = 0; i < n; i++) order[i] = (uint32_t)key[i];
+  if (!h->bin_order && (e = cudaMalloc(&h->bin_order, n * sizeof(uint32_t))) != cudaSuccess)
+    return cuda_fail(h, e, "cudaMalloc binning order");
+  if ((e = cudaMemcpy(h->bin_order, order.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice)) != cudaSuccess)
+    return cuda_fail(h, e, "upload binning order");
+  if ((e = cudaDeviceSynchronize()) != cudaSuccess) return cuda_fail(h, e, "upload binning order");
+  return SPLAT_OK;
 }
 
 // Tile shape of a frame: sets tile_w/h, their logs and the tile grid.
@@ -282,7 +358,7 @@ int enqueue_frame(splat_cuda_handle* h, const FrameParams& fp_in, uint8_t* dev_o
      "binning kernels");
   if (h->stage_events) CK(cudaEventRecord(h->ev[2], s), "event");
   CK(launch_blend(h->table, 1, (uint32_t)tiles, h->pairs[0], h->ranges, h->order, h->exact, h->blend, fc.st,
-                  h->num_sms, s, &h->launches, host_mapped),
+                  h->num_sms, s, &h->launches, host_mapped, h->count_evals),
      "blend kernel");
   if (scratch) CK(launch_downsample(fp, h->full_dev, dev_out, s, &h->launches), "downsample kernel");
   if (h->stage_events) CK(cudaEventRecord(h->ev[3], s), "event");
@@ -580,6 +656,7 @@ int create_impl(const splat_scene_desc* d, int device, splat_cuda_handle** out, 
   // and the handle's stream does not wait for the legacy stream that carries
   // it: the scene must be on the device before the first kernel reads it.
   if (upload && (e = cudaDeviceSynchronize()) != cudaSuccess) return bail(cuda_fail(h, e, "upload scene"));
+  if (upload && (rc = build_binning_order(h))) return bail(rc);
   *out = h;
   return SPLAT_OK;
 }
@@ -808,6 +885,11 @@ SPLAT_API int splat_cuda_set_option(splat_cuda_handle* h, uint32_t option, uint6
     case SPLAT_OPT_STAGE_EVENTS:
       h->stage_events = value != 0;
       return SPLAT_OK;
+    case SPLAT_OPT_COUNT_EVALS:
+      h->count_evals = value != 0;
+      return SPLAT_OK;
+    case SPLAT_OPT_BLEND_EVALS:
+      return fail(h, SPLAT_ERR_INVALID_ARG, "SPLAT_OPT_BLEND_EVALS is read-only");
     case SPLAT_OPT_FP64_CONICS:
       return fail(h, SPLAT_ERR_INVALID_ARG, "SPLAT_OPT_FP64_CONICS is read-only");
     case SPLAT_OPT_KERNEL_LAUNCHES:
@@ -848,6 +930,8 @@ SPLAT_API int splat_cuda_get_option(splat_cuda_handle* h, uint32_t option, uint6
     case SPLAT_OPT_PAIR_CAPACITY: *value = h->cap; return SPLAT_OK;
     case SPLAT_OPT_PAIR_LIMIT: *value = h->pair_limit; return SPLAT_OK;
     case SPLAT_OPT_STAGE_EVENTS: *value = h->stage_events; return SPLAT_OK;
+    case SPLAT_OPT_COUNT_EVALS: *value = h->count_evals; return SPLAT_OK;
+    case SPLAT_OPT_BLEND_EVALS: *value = h->have_frame ? h->st_host->evals : 0; return SPLAT_OK;
     case SPLAT_OPT_DEBUG_CAPTURE: *value = h->debug_capture; return SPLAT_OK;
     case SPLAT_OPT_FP64_CONICS: *value = h->have_frame ? h->st_host->fp64_conics : 0; return SPLAT_OK;
     case SPLAT_OPT_KERNEL_LAUNCHES: *value = h->launches; return SPLAT_OK;
@@ -990,6 +1074,7 @@ SPLAT_API int splat_cuda_destroy(splat_cuda_handle* h) {
   dfree(h->table);
   dfree(h->dbg_proj);
   dfree(h->dbg_color);
+  dfree(h->bin_order);
   if (h->st_host) cudaFreeHost(h->st_host);
   if (h->stage) cudaFreeHost(h->stage);
   for (auto& ev : h->ev)

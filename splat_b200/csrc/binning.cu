@@ -38,33 +38,49 @@ namespace {
 
 constexpr int kBinThreads = 512;
 
-// Calls f(tile, splat, depth bits) for every pair of the splats [s0, s1): a
-// lane expands its own splat when it has at most 32 pairs, larger splats are
-// expanded by the whole warp.
-template <class F>
-__device__ __forceinline__ void for_each_pair(const BinInfo* __restrict__ bin, uint64_t s0, uint64_t s1,
-                                              uint32_t tiles_x, F&& f) {
+// Calls f(tile, splat, depth bits, active) for every pair of the splats at
+// positions [s0, s1) of the binning order (SceneDev::order; null: scene
+// order). Splats with at most 32 pairs are expanded by their own lane, the
+// warp's lanes in lockstep (round r emits pair r of every lane's splat,
+// `active` false for lanes with fewer pairs, whose tile is kNoTile), so that
+// lanes on the same tile can share one bucket atomic; larger splats are
+// expanded by the whole warp (distinct tiles, all lanes active, `active`
+// passed as a compile-time true through fw).
+constexpr uint32_t kNoTile = 0xFFFFFFFFu;
+
+template <class F, class FW>
+__device__ __forceinline__ void for_each_pair(const BinInfo* __restrict__ bin, const uint32_t* __restrict__ order,
+                                              uint64_t s0, uint64_t s1, uint32_t tiles_x, F&& f, FW&& fw) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   constexpr uint64_t kStride = (uint64_t)kBinThreads;
   // The lane's splat of the warp's next group of 32 is loaded while the
   // current group's pairs are expanded.
   const BinInfo culled{kCulled, 0u, 0u, 0u};
+  auto splat_at = [&](uint64_t k) -> uint32_t { return order ? __ldg(order + k) : (uint32_t)k; };
   uint64_t wb = s0 + (uint64_t)warp * 32;
-  BinInfo nb = wb + lane < s1 ? bin[wb + lane] : culled;
+  uint32_t ni = wb + lane < s1 ? splat_at(wb + lane) : 0u;
+  BinInfo nb = wb + lane < s1 ? bin[ni] : culled;
   for (; wb < s1; wb += kStride) {
-    const uint64_t i = wb + lane;
+    const uint64_t k = wb + lane;
     const BinInfo b = nb;
-    nb = i + kStride < s1 ? bin[i + kStride] : culled;
+    const uint32_t i = ni;
+    if (k + kStride < s1) {
+      ni = splat_at(k + kStride);
+      nb = bin[ni];
+    } else {
+      nb = culled;
+    }
     const uint32_t cnt = b.rect_lo != kCulled ? b.count : 0u;
-    if (cnt <= 32) {
-      const uint32_t tx0 = b.rect_lo & 0xFFFFu, ty0 = b.rect_lo >> 16, tx1 = b.rect_hi & 0xFFFFu;
-      uint32_t tx = tx0, ty = ty0;
-      for (uint32_t p = 0; p < cnt; p++) {
-        f(ty * tiles_x + tx, (uint32_t)i, b.depth_bits);
-        if (++tx == tx1) {
-          tx = tx0;
-          ty++;
-        }
+    const uint32_t mine = cnt <= 32 ? cnt : 0u;
+    const uint32_t rounds = __reduce_max_sync(0xffffffffu, mine);
+    const uint32_t tx0 = b.rect_lo & 0xFFFFu, ty0 = b.rect_lo >> 16, tx1 = b.rect_hi & 0xFFFFu;
+    uint32_t tx = tx0, ty = ty0;
+    for (uint32_t r = 0; r < rounds; r++) {
+      const bool act = r < mine;
+      f(act ? ty * tiles_x + tx : kNoTile, i, b.depth_bits, act);
+      if (act && ++tx == tx1) {
+        tx = tx0;
+        ty++;
       }
     }
     uint32_t big = __ballot_sync(0xffffffffu, cnt > 32);
@@ -73,11 +89,11 @@ __device__ __forceinline__ void for_each_pair(const BinInfo* __restrict__ bin, u
       big &= big - 1u;
       const uint32_t b_lo = __shfl_sync(0xffffffffu, b.rect_lo, L), b_hi = __shfl_sync(0xffffffffu, b.rect_hi, L);
       const uint32_t b_cnt = __shfl_sync(0xffffffffu, cnt, L), b_d = __shfl_sync(0xffffffffu, b.depth_bits, L);
-      const uint32_t b_i = __shfl_sync(0xffffffffu, (uint32_t)i, L);
-      const uint32_t tx0 = b_lo & 0xFFFFu, ty0 = b_lo >> 16, wdt = (b_hi & 0xFFFFu) - tx0;
-      for (uint32_t k = lane; k < b_cnt; k += 32) {
-        const uint32_t row = k / wdt;
-        f((ty0 + row) * tiles_x + tx0 + (k - row * wdt), b_i, b_d);
+      const uint32_t b_i = __shfl_sync(0xffffffffu, i, L);
+      const uint32_t btx0 = b_lo & 0xFFFFu, bty0 = b_lo >> 16, wdt = (b_hi & 0xFFFFu) - btx0;
+      for (uint32_t q = lane; q < b_cnt; q += 32) {
+        const uint32_t row = q / wdt;
+        fw((bty0 + row) * tiles_x + btx0 + (q - row * wdt), b_i, b_d);
       }
     }
   }
@@ -86,6 +102,7 @@ __device__ __forceinline__ void for_each_pair(const BinInfo* __restrict__ bin, u
 // The per-view fields the count and scatter CTAs need.
 struct BinView {
   const BinInfo* bin;
+  const uint32_t* order;  // the binning order (null: scene order)
   uint32_t* row;  // this CTA's row of the view's count matrix
   uint64_t s0, s1;
   uint32_t tiles_x, tiles, tile0;
@@ -96,6 +113,7 @@ __device__ __forceinline__ BinView bin_view(const ViewTask* __restrict__ table, 
   const ViewTask* t = table + v;
   BinView b;
   b.bin = t->bin;
+  b.order = t->s.order;
   b.tiles_x = t->fp.tiles_x;
   b.tiles = t->fp.tiles_x * t->fp.tiles_y;
   b.tile0 = t->tile0;
@@ -117,12 +135,16 @@ __global__ void __launch_bounds__(kBinThreads) k_bin_count(const ViewTask* __res
     for (uint32_t t = threadIdx.x; t < b.tiles; t += kBinThreads) s_row[t] = 0u;
     __syncthreads();
   }
-  for_each_pair(b.bin, b.s0, b.s1, b.tiles_x, [&](uint32_t t, uint32_t, uint32_t) {
-    if (SMEM)
-      atomicAdd(&s_row[t], 1u);
-    else
-      atomicAdd(&b.row[t], 1u);
-  });
+  uint32_t* const cnt = SMEM ? s_row : b.row;
+  const int lane = threadIdx.x & 31;
+  for_each_pair(
+      b.bin, b.order, b.s0, b.s1, b.tiles_x,
+      [&](uint32_t t, uint32_t, uint32_t, bool act) {
+        // Lanes on the same tile add their pairs with one atomic.
+        const uint32_t peers = __match_any_sync(0xffffffffu, t);
+        if (act && lane == __ffs(peers) - 1) atomicAdd(&cnt[t], (uint32_t)__popc(peers));
+      },
+      [&](uint32_t t, uint32_t, uint32_t) { atomicAdd(&cnt[t], 1u); });
   if (SMEM) {
     __syncthreads();
     for (uint32_t t = threadIdx.x; t < b.tiles; t += kBinThreads) b.row[t] = s_row[t];
@@ -268,14 +290,28 @@ __global__ void __launch_bounds__(kBinThreads) k_bin_scatter(const ViewTask* __r
     for (uint32_t t = threadIdx.x; t < b.tiles; t += kBinThreads) s_row[t] = vr[t].x + b.row[t];
     __syncthreads();
   }
-  for_each_pair(b.bin, b.s0, b.s1, b.tiles_x, [&](uint32_t t, uint32_t i, uint32_t depth_bits) {
-    uint64_t pos;
-    if (SMEM)
-      pos = atomicAdd(&s_row[t], 1u);
-    else
-      pos = (uint64_t)vr[t].x + atomicAdd(&b.row[t], 1u);
-    if (pos < cap) pairs[pos] = ((uint64_t)depth_bits << 32) | i;
-  });
+  const int lane = threadIdx.x & 31;
+  const uint32_t lt = (1u << lane) - 1u;
+  for_each_pair(
+      b.bin, b.order, b.s0, b.s1, b.tiles_x,
+      [&](uint32_t t, uint32_t i, uint32_t depth_bits, bool act) {
+        // Lanes on the same tile take consecutive positions from one atomic,
+        // so their stores land next to each other.
+        const uint32_t peers = __match_any_sync(0xffffffffu, t);
+        const int leader = __ffs(peers) - 1;
+        uint32_t base = 0u;
+        if (act && lane == leader) base = SMEM ? atomicAdd(&s_row[t], (uint32_t)__popc(peers))
+                                               : atomicAdd(&b.row[t], (uint32_t)__popc(peers));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (act) {
+          const uint64_t pos = (SMEM ? 0ull : (uint64_t)vr[t].x) + base + __popc(peers & lt);
+          if (pos < cap) pairs[pos] = ((uint64_t)depth_bits << 32) | i;
+        }
+      },
+      [&](uint32_t t, uint32_t i, uint32_t depth_bits) {
+        const uint64_t pos = SMEM ? atomicAdd(&s_row[t], 1u) : (uint64_t)vr[t].x + atomicAdd(&b.row[t], 1u);
+        if (pos < cap) pairs[pos] = ((uint64_t)depth_bits << 32) | i;
+      });
 }
 
 // Tiles of at most kWarpSortCap pairs (classes 4 and 5, the heavier class

@@ -221,7 +221,10 @@ struct __align__(16) GroupSmem {
   uint32_t work;
 };
 
-template <bool EXACT, int TW, int TH, int NT, bool ROWS>
+// COUNT: also counts the pixel/splat evaluations (the blend's unit of work
+// after early termination) into st->evals; a separate instantiation, used
+// only when SPLAT_OPT_COUNT_EVALS asks for it.
+template <bool EXACT, int TW, int TH, int NT, bool ROWS, bool COUNT = false>
 __global__ void __launch_bounds__(NT, NT == 512 ? 2 : (NT == 256 ? 5 : 8)) k_blend(const ViewTask* __restrict__ table, uint32_t n_views, uint32_t n_tiles,
                                               const uint64_t* __restrict__ pairs, const uint2* __restrict__ ranges,
                                               const uint32_t* __restrict__ order, DevState* st) {
@@ -295,6 +298,7 @@ __global__ void __launch_bounds__(NT, NT == 512 ? 2 : (NT == 256 ? 5 : 8)) k_ble
     const float ox05 = (float)ox + 0.5f, oy05 = (float)oy + 0.5f;
 
     float T[PPT], cr[PPT], cg[PPT], cb[PPT];
+    uint32_t evals = 0;
     bool done[PPT];
     bool all_done = true;
 #pragma unroll
@@ -376,6 +380,7 @@ __global__ void __launch_bounds__(NT, NT == 512 ? 2 : (NT == 256 ? 5 : 8)) k_ble
             const float al0 = splat_alpha<EXACT>(in0, a0, b0, fx05, gbase, lanef, rowc, lxf, lyf);
             const float al1 = splat_alpha<EXACT>(in1, a1, b1, fx05, gbase, lanef, rowc, lxf, lyf);
             float r_, g_, b_;
+            if (COUNT) evals += 2;
             staged_colour<EXACT>(b0, bt.c[j0], r_, g_, b_);
             accumulate<EXACT>(al0, r_, g_, b_, T[0], cr[0], cg[0], cb[0]);
             const bool sat0 = T[0] < kTMin;
@@ -392,6 +397,7 @@ __global__ void __launch_bounds__(NT, NT == 512 ? 2 : (NT == 256 ? 5 : 8)) k_ble
             const bool in0 = !EXACT || ((bt.mx[j0] & xbit) && (bt.my[j0] & ybit));
             const float al0 = splat_alpha<EXACT>(in0, a0, b0, fx05, gbase, lanef, rowc, lxf, lyf);
             float r_, g_, b_;
+            if (COUNT) evals += 1;
             staged_colour<EXACT>(b0, bt.c[j0], r_, g_, b_);
             accumulate<EXACT>(al0, r_, g_, b_, T[0], cr[0], cg[0], cb[0]);
             if (T[0] < kTMin) done[0] = true;
@@ -413,6 +419,7 @@ __global__ void __launch_bounds__(NT, NT == 512 ? 2 : (NT == 256 ? 5 : 8)) k_ble
                 const bool in = !EXACT || ((mx & xbit) && ((my >> ly) & 1u));
                 const float al = splat_alpha<EXACT>(in, a, b, fx05, gbase, lanef, (float)(oy + ly) + 0.5f,
                                                     (float)lx, (float)ly);
+                if (COUNT) evals += 1;
                 if (al > 0.0f) {
                   accumulate<EXACT>(al, red, green, blue, T[q], cr[q], cg[q], cb[q]);
                   if (T[q] < kTMin) done[q] = true;
@@ -430,6 +437,12 @@ __global__ void __launch_bounds__(NT, NT == 512 ? 2 : (NT == 256 ? 5 : 8)) k_ble
       if (count(!all_done) == 0) break;
     }
 
+    if (COUNT) {
+      uint32_t e = evals;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
+      if (lane == 0 && e) atomicAdd(&st->evals, (unsigned long long)e);
+    }
     // C + T * bg, quantised (the reference adds unfused: c + (t * bg)).
     const uint32_t f = tv->fp.downsample;
     uint8_t* __restrict__ out = tv->out;
@@ -534,12 +547,12 @@ bool blend_config_supported(const BlendConfig& c) {
 
 namespace {
 
-template <bool EXACT, int TW, int TH, int NT, bool ROWS>
+template <bool EXACT, int TW, int TH, int NT, bool ROWS, bool COUNT = false>
 cudaError_t launch_blend_t(const ViewTask* table, uint32_t n_views, uint32_t n_tiles, const uint64_t* pairs,
                            const uint2* ranges, const uint32_t* order, DevState* st, int num_sms,
                            cudaStream_t stream) {
   using S = BlendShape<TW, TH, NT>;
-  const auto kernel = k_blend<EXACT, TW, TH, NT, ROWS>;
+  const auto kernel = k_blend<EXACT, TW, TH, NT, ROWS, COUNT>;
   const int smem = (int)(S::NG * sizeof(GroupSmem<TW, TH, NT>));
   // Resident CTAs per SM, looked up once per instantiation.
   static std::atomic<int> occ{0};
@@ -561,15 +574,19 @@ cudaError_t launch_blend_t(const ViewTask* table, uint32_t n_views, uint32_t n_t
 template <bool EXACT>
 cudaError_t launch_blend_e(const ViewTask* table, uint32_t n_views, uint32_t n_tiles, const uint64_t* pairs,
                            const uint2* ranges, const uint32_t* order, const BlendConfig& c, DevState* st,
-                           int num_sms, cudaStream_t s, bool rows) {
-  // The row-word variant for mapped host frames exists for the default
-  // blend (16x16 tiles, 512 threads); other shapes write such frames byte by
-  // byte, which is as correct.
+                           int num_sms, cudaStream_t s, bool rows, bool count) {
+  // The row-word variant for mapped host frames and the evaluation-counting
+  // variant exist for the default blend (16x16 tiles, 512 threads); other
+  // shapes write mapped frames byte by byte, which is as correct, and do not
+  // count.
 #define SPLAT_BLEND(TW, TH, NT)                                                                        \
   if (c.tile_w == TW && c.tile_h == TH && c.threads == NT) {                                           \
-    if constexpr (!EXACT && TW == 16 && TH == 16 && NT == 512)                                         \
+    if constexpr (!EXACT && TW == 16 && TH == 16 && NT == 512) {                                       \
+      if (count) return launch_blend_t<EXACT, TW, TH, NT, false, true>(table, n_views, n_tiles, pairs, \
+                                                                       ranges, order, st, num_sms, s); \
       if (rows) return launch_blend_t<EXACT, TW, TH, NT, true>(table, n_views, n_tiles, pairs, ranges, \
                                                                order, st, num_sms, s);                 \
+    }                                                                                                  \
     return launch_blend_t<EXACT, TW, TH, NT, false>(table, n_views, n_tiles, pairs, ranges, order, st, \
                                                     num_sms, s);                                       \
   }
@@ -590,11 +607,13 @@ cudaError_t launch_blend_e(const ViewTask* table, uint32_t n_views, uint32_t n_t
 
 cudaError_t launch_blend(const ViewTask* table, uint32_t n_views, uint32_t n_tiles, const uint64_t* pairs,
                          const uint2* ranges, const uint32_t* order, bool exact, const BlendConfig& cfg, DevState* st,
-                         int num_sms, cudaStream_t stream, uint32_t* launches, bool host_rows) {
+                         int num_sms, cudaStream_t stream, uint32_t* launches, bool host_rows, bool count) {
   if (n_tiles == 0) return cudaSuccess;
   const cudaError_t e =
-      exact ? launch_blend_e<true>(table, n_views, n_tiles, pairs, ranges, order, cfg, st, num_sms, stream, host_rows)
-            : launch_blend_e<false>(table, n_views, n_tiles, pairs, ranges, order, cfg, st, num_sms, stream, host_rows);
+      exact ? launch_blend_e<true>(table, n_views, n_tiles, pairs, ranges, order, cfg, st, num_sms, stream, host_rows,
+                                   count)
+            : launch_blend_e<false>(table, n_views, n_tiles, pairs, ranges, order, cfg, st, num_sms, stream,
+                                    host_rows, count);
   if (e == cudaSuccess) *launches += 1;
   return e;
 }

@@ -73,6 +73,11 @@ struct SceneDev {
   const uint4* lat16;
   const uint16_t* mlp16;
   uint32_t learned;
+  // The order in which the binning visits the splats: a static permutation
+  // of the scene that follows a 3D Morton curve through the splat positions,
+  // so that the splats one CTA bins lie close together on screen and its
+  // pairs fall into few tiles, in runs (null: scene order).
+  const uint32_t* order;
   // Fault injection (tests of the timeout path): when nonzero, each CTA of
   // the learned-colour projection also waits, at its first tensor-core wait,
   // for a completion that never arrives, giving up after this many
@@ -129,6 +134,7 @@ struct DevState {
   unsigned int mid_next;           // the mid sort's next work item
   unsigned int cls[kTileClasses];  // tiles per class (tile_class)
   unsigned int pad;
+  unsigned long long evals;        // pixel/splat evaluations of the blend (when counted)
 };
 
 // The cleared counters of a frame or batch of n_views views over n_chunks
@@ -231,7 +237,8 @@ cudaError_t launch_binning(const ViewTask* table, const BinLaunch& bl, uint32_t*
 // host_rows: the views' frames are mapped pinned host memory (see k_blend).
 cudaError_t launch_blend(const ViewTask* table, uint32_t n_views, uint32_t n_tiles, const uint64_t* pairs,
                          const uint2* ranges, const uint32_t* order, bool exact, const BlendConfig& cfg, DevState* st,
-                         int num_sms, cudaStream_t stream, uint32_t* launches, bool host_rows = false);
+                         int num_sms, cudaStream_t stream, uint32_t* launches, bool host_rows = false,
+                         bool count = false);
 // Half-block terminal cells (SPLAT_CELLS_*) of a frame of width w.
 cudaError_t launch_cells(const uint8_t* frame, uint32_t w, uint32_t cols, uint32_t rows, uint32_t mode, uint8_t* cells,
                          cudaStream_t stream, uint32_t* launches);

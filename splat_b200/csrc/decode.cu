@@ -510,6 +510,11 @@ int decode_to_handle(const Decoded& dec, uint32_t precision, int device, splat_c
       splat_cuda_destroy(h);
       return e == cudaErrorMemoryAllocation ? SPLAT_ERR_OOM : SPLAT_ERR_DEVICE;
     }
+    if ((rc = build_binning_order(h))) {
+      set_create_error(h->err);
+      splat_cuda_destroy(h);
+      return rc;
+    }
   }
   *out = h;
   return SPLAT_OK;

@@ -27,6 +27,7 @@ struct splat_cuda_handle {
   uint16_t* sh16 = nullptr;  // FP16 storage: base colour + SH planes
   uint4* lat16 = nullptr;     // learned colour: 16 fp16 latents per splat
   uint16_t* mlp16 = nullptr;  // learned colour: the MLP's fp16 parameters
+  uint32_t* bin_order = nullptr;  // the binning order (SceneDev::order)
   // per-splat frame buffers
   splat::Record* rec = nullptr;
   splat::BinInfo* bin = nullptr;
@@ -63,6 +64,7 @@ struct splat_cuda_handle {
   // options
   bool exact = false;
   bool stage_events = true;
+  bool count_evals = false;  // SPLAT_OPT_COUNT_EVALS
   // fault injection (SPLAT_OPT_INJECT_FAULT), each fires once
   bool inject_alloc = false;    // the next device allocation fails as out of memory
   uint32_t inject_lost_us = 0;  // the next frame's tensor-core waits meet a lost completion
@@ -94,5 +96,7 @@ SceneDev scene_dev(const splat_cuda_handle* h);
 int create_unfilled(const splat_scene_desc* d, int device, splat_cuda_handle** out, std::string* err);
 // Sets the text splat_cuda_create_error reports on this thread.
 void set_create_error(const std::string& msg);
+// Computes the scene's binning order from its positions on the device.
+int build_binning_order(splat_cuda_handle* h);
 
 }  // namespace splat

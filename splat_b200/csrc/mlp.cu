@@ -905,6 +905,113 @@ SPLAT_API int splat_cuda_learner_create(const splat_cuda_handle* h, const splat_
   return SPLAT_OK;
 }
 
+namespace {
+
+// Learner checkpoint layout: this header, then the fp32 parameter masters and
+// their two Adam moments (kParams floats each), the latent masters and their
+// moments (n * 16 floats each) and the latent rows' stamps (n u32): the state
+// that the next step reads, so that training resumes where it stopped.
+struct LearnerStateHeader {
+  char magic[8];  // "SPLATLRN"
+  uint32_t version, header_bytes;
+  uint64_t n;
+  uint32_t directions, batch;
+  uint64_t seed;
+  uint32_t sh_degree, params;
+  uint64_t step;        // completed steps (the Adam bias correction and the shuffle position)
+  double loss_sum;      // the loss record of the current call
+  uint64_t loss_steps;
+  float last_loss, pad;
+};
+constexpr uint32_t kStateVersion = 1;
+
+size_t state_bytes(const splat_cuda_learner* L) {
+  return sizeof(LearnerStateHeader) + 3ull * mlp::kParams * 4 + 3ull * L->n * 64 + L->n * 4;
+}
+
+}  // namespace
+
+SPLAT_API size_t splat_cuda_learner_state_bytes(const splat_cuda_learner* L) { return L ? state_bytes(L) : 0; }
+
+SPLAT_API int splat_cuda_learner_save_state(splat_cuda_learner* L, void* out, size_t bytes) {
+  if (!L || !out) return SPLAT_ERR_INVALID_ARG;
+  if (bytes < state_bytes(L)) return lfail(L, SPLAT_ERR_INVALID_ARG, "buffer smaller than splat_cuda_learner_state_bytes");
+  LCK(cudaSetDevice(L->device), "cudaSetDevice");
+  LCK(cudaStreamSynchronize(L->stream), "learner stream");
+  StepState st{};
+  LCK(cudaMemcpy(&st, L->st, sizeof(st), cudaMemcpyDeviceToHost), "read step state");
+  LearnerStateHeader hd{};
+  std::memcpy(hd.magic, "SPLATLRN", 8);
+  hd.version = kStateVersion;
+  hd.header_bytes = sizeof(LearnerStateHeader);
+  hd.n = L->n;
+  hd.directions = L->n_dirs;
+  hd.batch = L->batch;
+  hd.seed = L->seed;
+  hd.sh_degree = L->sh_degree;
+  hd.params = mlp::kParams;
+  hd.step = st.step;
+  hd.loss_sum = st.loss_sum;
+  hd.loss_steps = st.loss_steps;
+  hd.last_loss = st.last_loss;
+  uint8_t* o = static_cast<uint8_t*>(out);
+  std::memcpy(o, &hd, sizeof(hd));
+  o += sizeof(hd);
+  const size_t pb = mlp::kParams * 4, lb = L->n * 64;
+  for (const auto& part : {std::make_pair((const void*)L->p32, pb), std::make_pair((const void*)L->pm, pb),
+                           std::make_pair((const void*)L->pv, pb), std::make_pair((const void*)L->lat32, lb),
+                           std::make_pair((const void*)L->lm, lb), std::make_pair((const void*)L->lv, lb),
+                           std::make_pair((const void*)L->stamp, (size_t)L->n * 4)}) {
+    LCK(cudaMemcpy(o, part.first, part.second, cudaMemcpyDeviceToHost), "read learner state");
+    o += part.second;
+  }
+  return SPLAT_OK;
+}
+
+SPLAT_API int splat_cuda_learner_load_state(splat_cuda_learner* L, const void* data, size_t bytes) {
+  if (!L || !data) return SPLAT_ERR_INVALID_ARG;
+  LearnerStateHeader hd{};
+  if (bytes < sizeof(hd)) return lfail(L, SPLAT_ERR_INVALID_ARG, "not a learner state (too short)");
+  std::memcpy(&hd, data, sizeof(hd));
+  if (std::memcmp(hd.magic, "SPLATLRN", 8) != 0 || hd.header_bytes != sizeof(hd))
+    return lfail(L, SPLAT_ERR_INVALID_ARG, "not a learner state");
+  if (hd.version != kStateVersion) return lfail(L, SPLAT_ERR_UNSUPPORTED, "unsupported learner state version");
+  if (hd.n != L->n || hd.directions != L->n_dirs || hd.batch != L->batch || hd.seed != L->seed ||
+      hd.sh_degree != L->sh_degree || hd.params != mlp::kParams)
+    return lfail(L, SPLAT_ERR_INVALID_ARG,
+                 "learner state of another scene or configuration (splats, directions, batch, seed, SH degree)");
+  if (bytes < state_bytes(L)) return lfail(L, SPLAT_ERR_INVALID_ARG, "learner state truncated");
+  LCK(cudaSetDevice(L->device), "cudaSetDevice");
+  LCK(cudaStreamSynchronize(L->stream), "learner stream");
+  const uint8_t* p = static_cast<const uint8_t*>(data) + sizeof(hd);
+  const size_t pb = mlp::kParams * 4, lb = L->n * 64;
+  for (const auto& part : {std::make_pair((void*)L->p32, pb), std::make_pair((void*)L->pm, pb),
+                           std::make_pair((void*)L->pv, pb), std::make_pair((void*)L->lat32, lb),
+                           std::make_pair((void*)L->lm, lb), std::make_pair((void*)L->lv, lb),
+                           std::make_pair((void*)L->stamp, (size_t)L->n * 4)}) {
+    LCK(cudaMemcpy(part.first, p, part.second, cudaMemcpyHostToDevice), "upload learner state");
+    p += part.second;
+  }
+  // A cudaMemcpy from pageable memory may return before its DMA lands, and
+  // the learner's non-blocking stream does not wait for the legacy stream
+  // that carries it.
+  LCK(cudaDeviceSynchronize(), "upload learner state");
+  k_to_half<<<(mlp::kParams + 255) / 256, 256, 0, L->stream>>>(L->p32, L->p16, mlp::kParams);
+  k_to_half<<<(uint32_t)std::min<uint64_t>((L->n * 16 + 255) / 256, 8192), 256, 0, L->stream>>>(L->lat32, L->lat16,
+                                                                                                 L->n * 16);
+  LCK(cudaGetLastError(), "learner state");
+  StepState st{};
+  st.step = hd.step;
+  st.loss_sum = hd.loss_sum;
+  st.loss_steps = hd.loss_steps;
+  st.last_loss = hd.last_loss;
+  LCK(cudaMemcpyAsync(L->st, &st, sizeof(st), cudaMemcpyHostToDevice, L->stream), "upload step state");
+  LCK(cudaMemsetAsync(L->grad, 0, mlp::kParams * 4, L->stream), "clear gradients");
+  LCK(cudaMemsetAsync(L->lgrad, 0, L->n * 64, L->stream), "clear gradients");
+  LCK(cudaStreamSynchronize(L->stream), "learner state");  // &st is a local
+  return SPLAT_OK;
+}
+
 SPLAT_API int splat_cuda_learner_set_params(splat_cuda_learner* L, const float* params, const float* latents) {
   if (!L) return SPLAT_ERR_INVALID_ARG;
   LCK(cudaSetDevice(L->device), "cudaSetDevice");

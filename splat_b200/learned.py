@@ -109,6 +109,27 @@ class Learner:
         lat = None if latents is None else np.ascontiguousarray(latents, np.float32).reshape(self.n, N.MLP_LATENT)
         self._check(N.lib().splat_cuda_learner_set_params(self._h, _ptr(p), _ptr(lat)), "set_params")
 
+    def save_state(self) -> bytes:
+        """The training state (parameters, latents, Adam moments, step count)
+        as bytes; `load_state` on a learner of the same scene and
+        configuration resumes from it."""
+        n = N.lib().splat_cuda_learner_state_bytes(self._h)
+        buf = ctypes.create_string_buffer(n)
+        self._check(N.lib().splat_cuda_learner_save_state(self._h, buf, n), "save_state")
+        return buf.raw
+
+    def load_state(self, state: bytes):
+        buf = ctypes.create_string_buffer(bytes(state), len(state))
+        self._check(N.lib().splat_cuda_learner_load_state(self._h, buf, len(state)), "load_state")
+
+    def save(self, path: str):
+        with open(path, "wb") as f:
+            f.write(self.save_state())
+
+    def load(self, path: str):
+        with open(path, "rb") as f:
+            self.load_state(f.read())
+
     def step_debug(self):
         """One step; returns its gradient (d params, d latents (n, 16))."""
         g = np.zeros(N.MLP_PARAMS, np.float32)
