@@ -458,6 +458,17 @@ def run_ours(args):
     stage = {k: v / nv for k, v in sums.items()}
     V, P = vis / nv, ovl / nv
 
+    # The blend's work: pixel/splat evaluations after early termination
+    # (a counting instantiation of the blend, outside the timed region).
+    r.set_option(Nat.SPLAT_OPT_COUNT_EVALS, 1)
+    evals = 0
+    for v in views:
+        r.render_device(v, W, H, (0, 0, 0), out.data_ptr(), nbytes)
+        r.finish()
+        evals += r.get_option(Nat.SPLAT_OPT_BLEND_EVALS)
+    r.set_option(Nat.SPLAT_OPT_COUNT_EVALS, 0)
+    E = evals / nv
+
     # End to end through the public C ABI: splat_cuda_render into pinned host memory.
     host = torch.empty(W * H * 3, dtype=torch.uint8).pin_memory()
     for v in warm[:3]:
@@ -533,6 +544,15 @@ def run_ours(args):
             line["error_vs_fp64_naive"] = errors
         if home_check is not None:
             line["psnr_vs_cpu"] = home_check
+        issue = profile_traffic(args.config, "blend_issue")[0]
+        line["blend_work"] = {
+            "evaluations_per_frame": E, "evaluations_per_pair": E / P if P else None,
+            "bound_pairs_x_256": P * 256, "evaluations_per_s": E / (stage["raster_ms"] / 1e3),
+            "note": "pixel/splat evaluations of the default blend after early termination (counted on the device "
+                    "over the orbit, outside the timed region); the blend is bound by instruction issue, not HBM",
+        }
+        if issue:
+            line["blend_work"]["issue"] = issue
         if load is not None:
             line["scene_load"] = load
         if cpu is not None:

@@ -80,7 +80,14 @@ def lattice_scene(n_side: int = 14, scale: float = 0.03, opacity: float = 0.9) -
     return s.finalize()
 
 
-def cluster_scene(n: int = 1_200_000, seed: int = 0x5EED0001, sh_degree: int = 3, clusters: int = 64) -> Scene:
+def cluster_scene(n: int = 1_200_000, seed: int = 0x5EED0001, sh_degree: int = 3, clusters: int = 64,
+                  sh_code_dim: int = 0) -> Scene:
+    """sh_code_dim = k > 0: the higher SH coefficients are not independent
+    but generated from a k-dimensional code per splat, rest = B z with z ~
+    N(0, I_k) and B a fixed (seeded) basis scaled so that each coefficient
+    still has standard deviation 0.08 - a scene whose view-dependent colour
+    carries k numbers per splat (as correlated SH of captured scenes does)
+    instead of 45."""
     s = Scene()
     cl = (splitmix_u64(stream_seed(seed, 0), n) % np.uint64(clusters)).astype(np.int64)
     centres = (f32(-5.0) + f32(10.0) * uniform(stream_seed(seed, 1), clusters * 3)).reshape(clusters, 3)
@@ -97,8 +104,15 @@ def cluster_scene(n: int = 1_200_000, seed: int = 0x5EED0001, sh_degree: int = 3
     s.sh_degree = sh_degree
     per = (sh_degree + 1) ** 2 - 1
     rest = np.empty((n, per, 3), np.float32)
-    for c in range(per):
-        rest[:, c, :] = (f32(0.08) * normal(stream_seed(seed, 7 + c), 3 * n)).reshape(n, 3)
+    if sh_code_dim > 0 and per > 0:
+        k = int(sh_code_dim)
+        z = normal(stream_seed(seed, 7), k * n).reshape(n, k)
+        basis = normal(stream_seed(seed, 8), k * per * 3).reshape(k, per * 3)
+        basis *= f32(0.08) / np.sqrt(np.sum(basis * basis, axis=0, keepdims=True) + f32(1e-12))
+        rest[:] = (z @ basis).astype(np.float32).reshape(n, per, 3)
+    else:
+        for c in range(per):
+            rest[:, c, :] = (f32(0.08) * normal(stream_seed(seed, 7 + c), 3 * n)).reshape(n, 3)
     s.sh_rest = rest
     return s.finalize()
 
