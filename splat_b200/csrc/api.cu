@@ -393,8 +393,11 @@ int finish_frame(splat_cuda_handle* h, splat_render_stats* stats, int* regrown) 
     }
   }
   if (st.error) {
+    const unsigned code = st.error;
     cudaMemsetAsync(h->st, 0, sizeof(DevState), h->stream);
-    return fail(h, SPLAT_ERR_TIMEOUT, "a tensor-core wait in the learned-colour projection gave up");
+    return fail(h, SPLAT_ERR_TIMEOUT,
+                code == 2u ? "the projection's bulk copies did not complete in time"
+                           : "a tensor-core wait in the learned-colour projection gave up");
   }
   h->have_frame = true;
   if (st.total_pairs > h->cap) {
@@ -627,8 +630,10 @@ int create_impl(const splat_scene_desc* d, int device, splat_cuda_handle** out, 
     std::vector<float> col(upload ? 3 * n : 0);
     for (uint64_t i = 0; upload && i < n; i++)
       for (int ch = 0; ch < 3; ch++) col[ch * n + i] = d->colors[3 * i + ch];
+    // 16 bytes of slack after every array: the projection's bulk copies
+    // round a plane's slice out to 16-byte boundaries.
     auto up = [&](void** dst, const void* src, size_t bytes, const char* what) -> int {
-      cudaError_t er = cudaMalloc(dst, bytes);
+      cudaError_t er = cudaMalloc(dst, bytes + 16);
       if (er != cudaSuccess) return cuda_fail(h, er, what);
       if (!upload) return SPLAT_OK;
       er = cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice);

@@ -60,12 +60,36 @@ __device__ __forceinline__ void l2_prefetch(const void* p) {
 // LEARNED: the colour comes from the learned-colour MLP afterwards; the
 // record's colour is left 0 and `dir` receives normalize_or_zero(p - eye),
 // the direction the SH colour would be evaluated at.
-template <int DEG, bool F16, bool LEARNED = false>
+// Where the FP32 scene values of splat i are read: global memory (through
+// the read-only path), or a CTA's copy in shared memory (k_project_tma).
+struct GlobalScene {
+  const SceneDev& s;
+  __device__ __forceinline__ float4 pos(uint64_t i) const { return __ldg(&s.pos_op[i]); }
+  __device__ __forceinline__ float4 cov_a(uint64_t i) const { return __ldg(&s.cov_a[i]); }
+  __device__ __forceinline__ float4 cov_b(uint64_t i) const { return __ldg(&s.cov_b[i]); }
+  __device__ __forceinline__ float color(int ch, uint64_t i) const { return __ldg(s.color + (uint64_t)ch * s.n + i); }
+  __device__ __forceinline__ float sh(int plane, uint64_t i) const {
+    return __ldg(s.sh + (uint64_t)plane * s.n + i);
+  }
+  static constexpr bool kGlobal = true;
+};
+
+template <class Src>
+__device__ __forceinline__ Src scene_source(const SceneDev& s, const Src* given) {
+  if constexpr (Src::kGlobal)
+    return Src{s};
+  else
+    return *given;
+}
+
+template <int DEG, bool F16, bool LEARNED = false, class Src = GlobalScene>
 __device__ __forceinline__ void project_splat(const FrameParams& fp, const SceneDev& s, uint64_t i,
                                               Record* __restrict__ rec, BinInfo* __restrict__ bin,
                                               float* __restrict__ dbg_proj, float* __restrict__ dbg_color,
-                                              bool& vis, bool& used_fp64, float* dir = nullptr) {
-  if constexpr (!LEARNED && DEG > 0) {
+                                              bool& vis, bool& used_fp64, float* dir = nullptr,
+                                              const Src* given = nullptr) {
+  const Src src = scene_source<Src>(s, given);
+  if constexpr (!LEARNED && DEG > 0 && Src::kGlobal) {
     // The warp's 32 entries of every SH plane are brought into L2 now; the
     // loads that read them come after the geometry and the culling tests.
     const uint32_t lane = threadIdx.x & 31;
@@ -93,7 +117,7 @@ __device__ __forceinline__ void project_splat(const FrameParams& fp, const Scene
       g16 = __ldg(&s.geom16[i]);
       opacity = fminf(fmaxf(h2f(g16.w >> 16), 0.0f), 1.0f);  // Scene::finalize's clamp; NaN -> 0
     } else {
-      const float4 po = __ldg(&s.pos_op[i]);
+      const float4 po = src.pos(i);
       px = po.x;
       py = po.y;
       pz = po.z;
@@ -137,8 +161,8 @@ __device__ __forceinline__ void project_splat(const FrameParams& fp, const Scene
         q[3] = h2f(g16.w & 0xFFFFu);
         covariance_from<float>(sc, q[0], q[1], q[2], q[3], cov);
       } else {
-        const float4 ca = __ldg(&s.cov_a[i]);
-        const float4 cb = __ldg(&s.cov_b[i]);
+        const float4 ca = src.cov_a(i);
+        const float4 cb = src.cov_b(i);
         cov[0] = ca.x;
         cov[1] = ca.y;
         cov[2] = ca.z;
@@ -189,9 +213,9 @@ __device__ __forceinline__ void project_splat(const FrameParams& fp, const Scene
           col[1] = h2f(__ldg(s.sh16 + s.n + i));
           col[2] = h2f(__ldg(s.sh16 + 2 * s.n + i));
         } else {
-          col[0] = __ldg(s.color + i);
-          col[1] = __ldg(s.color + s.n + i);
-          col[2] = __ldg(s.color + 2 * s.n + i);
+          col[0] = src.color(0, i);
+          col[1] = src.color(1, i);
+          col[2] = src.color(2, i);
         }
         if constexpr (DEG > 0) {
           // normalize_or_zero(p - eye)
@@ -207,8 +231,7 @@ __device__ __forceinline__ void project_splat(const FrameParams& fp, const Scene
             sh::eval_sh<DEG>([&](int coef, int ch) { return h2f(__ldg(s.sh16 + (uint64_t)((coef + 1) * 3 + ch) * s.n + i)); },
                          nx, ny, nz, col);
           else
-            sh::eval_sh<DEG>([&](int coef, int ch) { return __ldg(s.sh + (uint64_t)(coef * 3 + ch) * s.n + i); }, nx, ny,
-                         nz, col);
+            sh::eval_sh<DEG>([&](int coef, int ch) { return src.sh(coef * 3 + ch, i); }, nx, ny, nz, col);
         }
         col[0] = fmaxf(col[0], 0.0f);
         col[1] = fmaxf(col[1], 0.0f);
@@ -291,6 +314,112 @@ __global__ void __launch_bounds__(256) k_project(ViewTask t, ViewTask* __restric
   const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   bool vis = false, used_fp64 = false;
   if (i < t.s.n) project_splat<DEG, F16>(t.fp, t.s, i, t.rec, t.bin, dbg_proj, dbg_color, vis, used_fp64);
+  count_visible(vis, used_fp64, fc, 0);
+}
+
+// FP32 scenes: the same projection with each CTA's slice of every scene
+// array (positions, covariance, colour and SH planes: 232 bytes per splat at
+// degree 3) brought into shared memory by bulk asynchronous copies (TMA,
+// cp.async.bulk) that complete on one mbarrier, so that every byte the CTA
+// reads is in flight at once and the threads wait once instead of on each
+// load. A plane's slice need not start on the 16 bytes a bulk copy needs: the
+// copy starts at the 16-byte boundary below it (the plane buffers carry 16
+// bytes of slack at their end for the rounded-up last copy) and the slice is
+// read at its offset. The arithmetic is project_splat's, unchanged.
+constexpr uint32_t kTmaSplats = 256;
+constexpr uint32_t kTmaPlaneFloats = kTmaSplats + 8;  // the slice, its offset and the rounding
+
+template <int DEG>
+struct TmaLayout {
+  static constexpr uint32_t kShPlanes = ((DEG + 1) * (DEG + 1) - 1) * 3;
+  static constexpr uint32_t kPlanes = 3 + kShPlanes;  // colour, then SH
+  static constexpr size_t kBytes = 3 * kTmaSplats * sizeof(float4) + kPlanes * kTmaPlaneFloats * sizeof(float) + 16;
+};
+
+struct SmemScene {
+  const float4* p_pos;
+  const float4* p_ca;
+  const float4* p_cb;
+  const float* planes;  // kTmaPlaneFloats floats per plane
+  const uint32_t* off;  // per plane: the slice's offset in its copy
+  uint64_t base;
+  __device__ __forceinline__ float4 pos(uint64_t i) const { return p_pos[i - base]; }
+  __device__ __forceinline__ float4 cov_a(uint64_t i) const { return p_ca[i - base]; }
+  __device__ __forceinline__ float4 cov_b(uint64_t i) const { return p_cb[i - base]; }
+  __device__ __forceinline__ float color(int ch, uint64_t i) const {
+    return planes[ch * kTmaPlaneFloats + off[ch] + (i - base)];
+  }
+  __device__ __forceinline__ float sh(int plane, uint64_t i) const {
+    return planes[(3 + plane) * kTmaPlaneFloats + off[3 + plane] + (i - base)];
+  }
+  static constexpr bool kGlobal = false;
+};
+
+__device__ __forceinline__ void bulk_copy(void* smem_dst, const void* gmem_src, uint32_t bytes, uint32_t mbar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          umma::smem_u32(smem_dst)),
+      "l"(gmem_src), "r"(bytes), "r"(mbar)
+      : "memory");
+}
+
+template <int DEG>
+__global__ void __launch_bounds__(kTmaSplats) k_project_tma(ViewTask t, ViewTask* __restrict__ table,
+                                                            float* __restrict__ dbg_proj, float* __restrict__ dbg_color,
+                                                            FrameCounters fc) {
+  using L = TmaLayout<DEG>;
+  extern __shared__ __align__(128) uint8_t smem_raw[];
+  float4* s_pos = reinterpret_cast<float4*>(smem_raw);
+  float4* s_ca = s_pos + kTmaSplats;
+  float4* s_cb = s_ca + kTmaSplats;
+  float* s_planes = reinterpret_cast<float*>(s_cb + kTmaSplats);
+  __shared__ uint32_t s_off[L::kPlanes];
+  __shared__ __align__(8) uint64_t s_mbar;
+  const uint32_t tid = threadIdx.x;
+  if (blockIdx.x == 0 && tid == 0) *table = t;
+  const uint64_t n = t.s.n, base = (uint64_t)blockIdx.x * kTmaSplats;
+  const uint32_t cnt = (uint32_t)min((uint64_t)kTmaSplats, n - base);
+  const uint32_t mbar = umma::smem_u32(&s_mbar);
+  // Copy sizes: whole float4 records; plane slices rounded out to 16 bytes.
+  auto plane_src = [&](uint32_t p) -> const float* {
+    return p < 3 ? t.s.color + (uint64_t)p * n : t.s.sh + (uint64_t)(p - 3) * n;
+  };
+  if (tid < L::kPlanes) {
+    const uint64_t first = (uint64_t)(plane_src(tid) - (tid < 3 ? t.s.color : t.s.sh)) + base;
+    s_off[tid] = (uint32_t)(first & 3u);
+  }
+  if (tid == 0) {
+    umma::mbar_init(mbar, 1);
+    uint32_t bytes = 3 * cnt * (uint32_t)sizeof(float4);
+    for (uint32_t p = 0; p < L::kPlanes; p++) {
+      const uintptr_t a = reinterpret_cast<uintptr_t>(plane_src(p) + base);
+      const uintptr_t lo = a & ~(uintptr_t)15, hi = (a + cnt * sizeof(float) + 15) & ~(uintptr_t)15;
+      bytes += (uint32_t)(hi - lo);
+    }
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
+  }
+  __syncthreads();
+  // The copies, spread over the first warps' lanes.
+  if (tid < 3) {
+    const float4* src = tid == 0 ? t.s.pos_op : tid == 1 ? t.s.cov_a : t.s.cov_b;
+    bulk_copy(s_pos + tid * kTmaSplats, src + base, cnt * (uint32_t)sizeof(float4), mbar);
+  } else if (tid >= 32 && tid < 32 + L::kPlanes) {
+    const uint32_t p = tid - 32;
+    const uintptr_t a = reinterpret_cast<uintptr_t>(plane_src(p) + base);
+    const uintptr_t lo = a & ~(uintptr_t)15, hi = (a + cnt * sizeof(float) + 15) & ~(uintptr_t)15;
+    bulk_copy(s_planes + p * kTmaPlaneFloats, reinterpret_cast<const void*>(lo), (uint32_t)(hi - lo), mbar);
+  }
+  bool vis = false, used_fp64 = false;
+  if (!umma::mbar_wait(mbar, 0)) {
+    // Copies that did not land in time: the frame reports an error, and the
+    // CTA leaves only once they have (bounded) or given up on them.
+    if (tid == 0) atomicExch(&fc.st->error, 2u);
+    umma::mbar_wait(mbar, 0, 100000000ull);
+  } else if (tid < cnt) {
+    const SmemScene src{s_pos, s_ca, s_cb, s_planes, s_off, base};
+    project_splat<DEG, false, false, SmemScene>(t.fp, t.s, base + tid, t.rec, t.bin, dbg_proj, dbg_color, vis,
+                                                used_fp64, nullptr, &src);
+  }
   count_visible(vis, used_fp64, fc, 0);
 }
 
@@ -503,12 +632,27 @@ cudaError_t launch_project(const ViewTask& t, ViewTask* table, float* dbg_proj, 
   }
   // An empty scene still stores the view table.
   const unsigned grid = t.s.n ? (unsigned)((t.s.n + 255) / 256) : 1u;
-#define SPLAT_PROJECT(D)                                                                          \
-  do {                                                                                            \
-    if (t.s.fp16)                                                                                 \
-      k_project<D, true><<<grid, 256, 0, stream>>>(t, table, dbg_proj, dbg_color, fc);            \
-    else                                                                                          \
-      k_project<D, false><<<grid, 256, 0, stream>>>(t, table, dbg_proj, dbg_color, fc);           \
+  static_assert(kTmaSplats == 256, "one CTA of the TMA projection per 256 splats");
+#define SPLAT_PROJECT(D)                                                                                        \
+  do {                                                                                                          \
+    if (t.s.fp16 || t.s.n == 0) {                                                                               \
+      if (t.s.fp16)                                                                                             \
+        k_project<D, true><<<grid, 256, 0, stream>>>(t, table, dbg_proj, dbg_color, fc);                        \
+      else                                                                                                      \
+        k_project<D, false><<<grid, 256, 0, stream>>>(t, table, dbg_proj, dbg_color, fc);                       \
+    } else {                                                                                                    \
+      /* raised once per device, outside capture: a scene's first frame is never captured */                 \
+      static bool attr_set[64] = {};                                                                            \
+      int dev = 0;                                                                                              \
+      if (cudaGetDevice(&dev) != cudaSuccess) dev = 0;                                                          \
+      if (!attr_set[dev & 63]) {                                                                                \
+        const cudaError_t ae = cudaFuncSetAttribute(k_project_tma<D>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                                    (int)TmaLayout<D>::kBytes);                                 \
+        if (ae != cudaSuccess) return ae;                                                                       \
+        attr_set[dev & 63] = true;                                                                              \
+      }                                                                                                         \
+      k_project_tma<D><<<grid, kTmaSplats, TmaLayout<D>::kBytes, stream>>>(t, table, dbg_proj, dbg_color, fc);  \
+    }                                                                                                           \
   } while (0)
   switch (t.s.sh_degree) {
     case 0: SPLAT_PROJECT(0); break;
