@@ -100,12 +100,37 @@ def parse():
 from splat_b200.multi import dist_env, max_over_ranks, shard  # noqa: E402
 
 
+_CLOCK_SAMPLER = r"""
+import json, signal, sys, time
+import pynvml
+pynvml.nvmlInit()
+bus, index, period = sys.argv[1], int(sys.argv[2]), float(sys.argv[3])
+try:
+    h = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+except Exception:
+    h = pynvml.nvmlDeviceGetHandleByIndex(index)
+rows, stop = [], []
+signal.signal(signal.SIGTERM, lambda *a: stop.append(1))
+print("ready", flush=True)
+while not stop:
+    try:
+        rows.append((pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM),
+                     pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM),
+                     pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)))
+    except Exception:
+        pass
+    time.sleep(period)
+print(json.dumps(rows), flush=True)
+"""
+
+
 class Clocks:
     """Samples the SM clock, its maximum and the clock-event (throttle)
-    reasons of the GPU every `period` seconds while the timed region runs,
-    through NVML (read-only queries), so that even a timed region of a few
-    milliseconds gets several samples; nvidia-smi one-shot queries are the
-    fallback when NVML cannot be loaded."""
+    reasons of the GPU about every millisecond while the timed region runs.
+    The sampler is a separate process querying NVML (read-only), so it takes
+    nothing from the process that launches the frames and gets many samples
+    even from a timed region of a few milliseconds; nvidia-smi one-shot
+    queries from a thread are the fallback when NVML is not usable."""
 
     NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
     BITS = [0x8, 0x40, 0x20, 0x4]  # nvmlClocksEventReason{HwSlowdown, HwThermalSlowdown, SwThermalSlowdown, SwPowerCap}
@@ -113,70 +138,72 @@ class Clocks:
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, index, period=0.002):
+    def __init__(self, index, period=0.001):
         self.index = index
         self.period = period
         self.rows = []  # (sm_mhz, max_mhz, reasons bitmask)
         self.stop = threading.Event()
-        self.source = "nvml"
-        self.nvml = None
+        self.proc = None
+        self.source = "nvml (sampler process)"
+
+    def _bus(self):
         try:
-            import pynvml
             import torch
 
-            pynvml.nvmlInit()
-            try:
-                p = torch.cuda.get_device_properties(index)
-                bus = f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0"
-                self.handle = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
-            except Exception:
-                self.handle = pynvml.nvmlDeviceGetHandleByIndex(index)
-            self.nvml = pynvml
+            p = torch.cuda.get_device_properties(self.index)
+            return f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0"
         except Exception:
-            self.source = "nvidia-smi"
+            return ""
 
-    def _sample_nvml(self):
-        n = self.nvml
-        sm = n.nvmlDeviceGetClockInfo(self.handle, n.NVML_CLOCK_SM)
-        mx = n.nvmlDeviceGetMaxClockInfo(self.handle, n.NVML_CLOCK_SM)
-        rs = n.nvmlDeviceGetCurrentClocksEventReasons(self.handle)
-        self.rows.append((float(sm), float(mx), int(rs)))
-
-    def _sample_smi(self):
-        out = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                              "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
-        for line in out.stdout.strip().splitlines():
-            c = [x.strip() for x in line.split(",")]
-            if len(c) >= 7:
-                bits = sum(b for b, v in zip(self.BITS, c[3:7]) if v.lower().startswith("active"))
-                try:
-                    self.rows.append((float(c[0]), float(c[1]), bits))
-                except ValueError:
-                    pass
-
-    def _poll(self):
+    def _poll_smi(self):
         while not self.stop.is_set():
             try:
-                self._sample_nvml() if self.nvml else self._sample_smi()
+                out = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                for line in out.stdout.strip().splitlines():
+                    c = [x.strip() for x in line.split(",")]
+                    bits = sum(b for b, v in zip(self.BITS, c[3:7]) if v.lower().startswith("active"))
+                    self.rows.append((float(c[0]), float(c[1]), bits))
             except Exception:
                 pass
-            self.stop.wait(self.period if self.nvml else 0.2)
+            self.stop.wait(0.2)
 
     def __enter__(self):
+        try:
+            self.proc = subprocess.Popen([sys.executable, "-c", _CLOCK_SAMPLER, self._bus(), str(self.index),
+                                          str(self.period)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                                         text=True)
+            if self.proc.stdout.readline().strip() != "ready":
+                raise RuntimeError("clock sampler did not start")
+        except Exception:
+            if self.proc:
+                self.proc.kill()
+            self.proc = None
+            self.source = "nvidia-smi"
+            self.t = threading.Thread(target=self._poll_smi, daemon=True)
+            self.t.start()
         self.t0 = time.perf_counter()
-        self.t = threading.Thread(target=self._poll, daemon=True)
-        self.t.start()
         return self
 
     def __exit__(self, *a):
-        self.stop.set()
-        self.t.join(timeout=10)
         self.seconds = time.perf_counter() - self.t0
+        if self.proc:
+            import signal
+
+            self.proc.send_signal(signal.SIGTERM)
+            try:
+                out, _ = self.proc.communicate(timeout=30)
+                self.rows = [tuple(r) for r in json.loads(out.strip().splitlines()[-1])]
+            except Exception:
+                self.proc.kill()
+        else:
+            self.stop.set()
+            self.t.join(timeout=10)
 
     def summary(self):
-        sm = [r[0] for r in self.rows]
-        mx = [r[1] for r in self.rows]
-        reasons = sorted({nm for r in self.rows for nm, b in zip(self.NAMES, self.BITS) if r[2] & b})
+        sm = [float(r[0]) for r in self.rows]
+        mx = [float(r[1]) for r in self.rows]
+        reasons = sorted({nm for r in self.rows for nm, b in zip(self.NAMES, self.BITS) if int(r[2]) & b})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": reasons, "samples": len(self.rows), "source": self.source,
                 "window_s": round(getattr(self, "seconds", 0.0), 4)}
@@ -563,6 +590,37 @@ def run_ours(args):
         torch.distributed.destroy_process_group()
 
 
+def learned_quality_correlated(args, W, H, dev):
+    """The learned colour's quality where the SH carries structure: the same
+    1.2M-splat geometry with the 45 higher coefficients generated from a
+    4-dimensional code per splat (synth.cluster_scene(sh_code_dim=4)),
+    trained as the main workload, PSNR against exact SH over orbit frames."""
+    from oracle import oracle as O
+    from splat_b200 import Frame, synth
+    from splat_b200.learned import LearnConfig, Learner, learned_renderer
+    from splat_b200.render import CudaRenderer
+
+    scene = synth.cluster_scene(args.splats, seed=0x5EED0001, sh_degree=3, sh_code_dim=4)
+    cam = synth.orbit_camera(scene)
+    _, _, timed = synth.orbit_views(cam, ORBIT, 5)
+    exact = CudaRenderer(scene, device=dev)
+    learner = Learner(exact, LearnConfig(directions=256, batch=65536, lr=1e-3, seed=1))
+    ts = learner.train(max(1, int(round(args.learn_epochs * learner.steps_per_epoch))))
+    p16, lat16 = learner.params_f16()
+    learner.close()
+    r = learned_renderer(scene.to_fp16(), lat16, p16, device=dev)
+    ps = []
+    fe, fl = Frame(), Frame()
+    for v in timed[: max(1, args.psnr_frames // 4)]:
+        exact.render(v, W, H, (0, 0, 0), fe)
+        r.render(v, W, H, (0, 0, 0), fl)
+        ps.append(O.psnr(fl.pixels, fe.pixels))
+    r.close()
+    exact.close()
+    return {"mean_db": float(np.mean(ps)), "min_db": float(np.min(ps)), "frames": len(ps), "epochs": ts.epochs,
+            "scene": "the workload's geometry; SH rest coefficients from a 4-dim code per splat (std 0.08 each)"}
+
+
 def run_learned(args):
     """Learned colour: train on the device, then time the learned renderer
     (and the exact-SH plain renderer of the same scene) over the orbit."""
@@ -718,6 +776,7 @@ def run_learned(args):
             ps_l.append(O.psnr(fl.pixels, fe.pixels))
             ps_b.append(O.psnr(fb.pixels, fe.pixels))
             mx_l.append(int(np.abs(fl.pixels.astype(int) - fe.pixels.astype(int)).max()))
+        correlated = learned_quality_correlated(args, W, H, dev)
         peak, peak_kind = measured_peaks()
         try:
             tpeak = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["bf16_tflops_sustained"])
@@ -754,6 +813,7 @@ def run_learned(args):
             "psnr_vs_exact_sh": {"mean_db": float(np.mean(ps_l)), "min_db": float(np.min(ps_l)),
                                  "max_abs": int(max(mx_l)), "frames": len(ps_l)},
             "psnr_base_colour_vs_exact_sh": {"mean_db": float(np.mean(ps_b)), "min_db": float(np.min(ps_b))},
+            "psnr_vs_exact_sh_correlated": correlated,
             "training": {"epochs": ts.epochs, "steps": ts.steps, "samples": int(samples), "ms": ts.ms,
                          "samples_per_s": samples / (ts.ms / 1e3), "final_loss": ts.last_loss,
                          "mean_loss_last_call": ts.mean_loss, "train_ctas": train_ctas,

@@ -354,7 +354,7 @@ int enqueue_frame(splat_cuda_handle* h, const FrameParams& fp_in, uint8_t* dev_o
   bl.counts_all = h->counts;
   bl.counts_bytes = (size_t)rows * tiles * sizeof(uint32_t);
   CK(launch_binning(h->table, bl, h->totals, h->ranges, h->order, h->pairs[0], h->pairs[1], h->cap,
-                    fc, h->num_sms, h->max_smem, s, &h->launches),
+                    fc, h->num_sms, h->max_smem, s, &h->launches, !blend_sorts_tiles(h->blend)),
      "binning kernels");
   if (h->stage_events) CK(cudaEventRecord(h->ev[2], s), "event");
   CK(launch_blend(h->table, 1, (uint32_t)tiles, h->pairs[0], h->ranges, h->order, h->exact, h->blend, fc.st,

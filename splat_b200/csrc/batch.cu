@@ -254,7 +254,7 @@ int enqueue(splat_cuda_batch* b, cudaStream_t s) {
   bl.counts_all = b->counts;
   bl.counts_bytes = b->counts_words * sizeof(uint32_t);
   BK(launch_binning(b->table, bl, b->totals, b->ranges, b->order, b->pairs[0], b->pairs[1], b->cap,
-                    fc, b->num_sms, b->max_smem, s, &b->launches),
+                    fc, b->num_sms, b->max_smem, s, &b->launches, !blend_sorts_tiles(b->cfg)),
      "binning kernels");
   BK(stage_event(b, 2, s), "event");
   BK(launch_blend(b->table, nv, b->n_tiles, b->pairs[0], b->ranges, b->order, b->exact, b->cfg, fc.st,

@@ -47,6 +47,9 @@ constexpr int kBinThreads = 512;
 // expanded by the whole warp (distinct tiles, all lanes active, `active`
 // passed as a compile-time true through fw).
 constexpr uint32_t kNoTile = 0xFFFFFFFFu;
+// false: each lane expands its own splat's pairs at its own pace, one bucket
+// atomic per pair (fw), as for the larger splats.
+constexpr bool kAggregateBuckets = true;
 
 template <class F, class FW>
 __device__ __forceinline__ void for_each_pair(const BinInfo* __restrict__ bin, const uint32_t* __restrict__ order,
@@ -72,15 +75,25 @@ __device__ __forceinline__ void for_each_pair(const BinInfo* __restrict__ bin, c
     }
     const uint32_t cnt = b.rect_lo != kCulled ? b.count : 0u;
     const uint32_t mine = cnt <= 32 ? cnt : 0u;
-    const uint32_t rounds = __reduce_max_sync(0xffffffffu, mine);
     const uint32_t tx0 = b.rect_lo & 0xFFFFu, ty0 = b.rect_lo >> 16, tx1 = b.rect_hi & 0xFFFFu;
     uint32_t tx = tx0, ty = ty0;
-    for (uint32_t r = 0; r < rounds; r++) {
-      const bool act = r < mine;
-      f(act ? ty * tiles_x + tx : kNoTile, i, b.depth_bits, act);
-      if (act && ++tx == tx1) {
-        tx = tx0;
-        ty++;
+    if constexpr (kAggregateBuckets) {
+      const uint32_t rounds = __reduce_max_sync(0xffffffffu, mine);
+      for (uint32_t r = 0; r < rounds; r++) {
+        const bool act = r < mine;
+        f(act ? ty * tiles_x + tx : kNoTile, i, b.depth_bits, act);
+        if (act && ++tx == tx1) {
+          tx = tx0;
+          ty++;
+        }
+      }
+    } else {
+      for (uint32_t r = 0; r < mine; r++) {
+        fw(ty * tiles_x + tx, i, b.depth_bits);
+        if (++tx == tx1) {
+          tx = tx0;
+          ty++;
+        }
       }
     }
     uint32_t big = __ballot_sync(0xffffffffu, cnt > 32);
@@ -419,7 +432,7 @@ uint32_t bin_rows(uint64_t n, int num_sms) {
 cudaError_t launch_binning(const ViewTask* table, const BinLaunch& bl, uint32_t* totals, uint2* ranges,
                            uint32_t* order, uint64_t* pairs, uint64_t* pairs_alt,
                            uint64_t cap, const FrameCounters& fc, int num_sms, size_t max_smem, cudaStream_t stream,
-                           uint32_t* launches) {
+                           uint32_t* launches, bool tile_sorts) {
   if (bl.n_tiles == 0) return cudaSuccess;
   const size_t smem = (size_t)bl.max_tiles * sizeof(uint32_t);
   const bool use_smem = smem <= max_smem;
@@ -464,10 +477,13 @@ cudaError_t launch_binning(const ViewTask* table, const BinLaunch& bl, uint32_t*
   const int os = std::max(occ_small.load(std::memory_order_relaxed), 1);
   const int om = std::max(occ_mid.load(std::memory_order_relaxed), 1);
   const int ol = std::max(occ_long.load(std::memory_order_relaxed), 1);
-  k_sort_small<<<num_sms * os, 256, 0, stream>>>(ranges, order, bl.n_tiles, pairs, fc.st);
-  k_sort_mid<<<num_sms * om, kTileThreads, sizeof(MidSmem), stream>>>(ranges, order, bl.n_tiles, pairs, fc.st);
+  if (tile_sorts) {
+    k_sort_small<<<num_sms * os, 256, 0, stream>>>(ranges, order, bl.n_tiles, pairs, fc.st);
+    k_sort_mid<<<num_sms * om, kTileThreads, sizeof(MidSmem), stream>>>(ranges, order, bl.n_tiles, pairs, fc.st);
+    *launches += 2;
+  }
   k_sort_long<<<num_sms * ol, kTileThreads, 0, stream>>>(ranges, order, pairs, pairs_alt, cap, fc.st);
-  *launches += 7;
+  *launches += 5;
   return cudaGetLastError();
 }
 

@@ -39,6 +39,7 @@
 #include <cstddef>
 
 #include "common.cuh"
+#include "tilesort.cuh"
 
 namespace splat {
 namespace {
@@ -81,26 +82,37 @@ __device__ __forceinline__ uint32_t to_u8(float v) {
 }
 
 
-// Default path staging: the splat's centre in tile pixel coordinates (xs,
-// ys; exact differences, the same whatever the tile shape), its conic times
-// log2 e (A, B, C: power = A dx^2 + B dx dy + C dy^2 in log2 units), lop =
-// log2 opacity and cap = min(lop, log2 0.99). Then pw' = power + lop and
-// alpha = 2^min(pw', cap) is min(opacity exp(power), 0.99) with power <= 0
-// enforced, and the alpha test is pw' >= log2(1/255).
-// a = (xs, ys, A, B), b = (C, lop, cap, red), c = (green, blue).
+// Default path staging. With the splat's centre in tile pixel coordinates
+// (xs, ys; exact differences, the same whatever the tile shape), its conic
+// times log2 e (A, B, C: power = A dx^2 + B dx dy + C dy^2 in log2 units,
+// dx = x - xs, dy = y - ys) and lop = log2 opacity, the exponent
+// pw' = power + lop is expanded once per splat into a quadratic in the
+// pixel's own tile coordinates (x, y):
+//   pw' = A x^2 + B x y + C y^2 + D x + E y + F,
+//   D = -2 A xs - B ys, E = -2 C ys - B xs, F = A xs^2 + B xs ys + C ys^2 + lop,
+// so that a pixel evaluates it in five fused multiply-adds. alpha =
+// 2^min(pw', cap) with cap = min(lop, log2 0.99) is min(opacity exp(power),
+// 0.99) with power <= 0 enforced, and the alpha test is pw' >= log2(1/255).
+// The expansion's terms stay within the ellipse's own scale wherever the
+// splat contributes (a pixel in reach is within its k-sigma extent), so the
+// f32 cancellation it adds is about 1e-6 in log2 units.
+// a = (A, B, C, D), b = (E, F, cap, red), c = (green, blue).
 __device__ __forceinline__ void stage_splat(const Record& r, float ox05, float oy05, float4& a, float4& b, float2& c) {
   const float lop = __log2f(r.r1.y);
-  a = make_float4(r.r0.x - ox05, r.r0.y - oy05, r.r0.z * kLog2e, r.r0.w * kLog2e);
-  b = make_float4(r.r1.x * kLog2e, lop, fminf(lop, kLog2AlphaMax), r.r1.z);
+  const float xs = r.r0.x - ox05, ys = r.r0.y - oy05;
+  const float A = r.r0.z * kLog2e, B = r.r0.w * kLog2e, C = r.r1.x * kLog2e;
+  const float D = -2.0f * A * xs - B * ys, E = -2.0f * C * ys - B * xs;
+  const float F = (A * xs * xs + B * xs * ys) + (C * ys * ys + lop);
+  a = make_float4(A, B, C, D);
+  b = make_float4(E, F, fminf(lop, kLog2AlphaMax), r.r1.z);
   c = make_float2(r.r1.w, r.r2.x);
 }
 
-// Default path alpha from the staged splat (stage_splat) at a pixel offset
-// (dx, dy), adx = A dx: pw' = dx (B dy + A dx) + (C dy dy + lop), clamped;
-// 0 when below the alpha threshold. Every blend shape evaluates this same
-// expression, so images do not depend on the shape.
-__device__ __forceinline__ float fast_alpha(const float4& a, const float4& b, float dx, float adx, float dy) {
-  const float pw = fminf(fmaf(dx, fmaf(a.w, dy, adx), fmaf(b.x * dy, dy, b.y)), b.z);
+// Default path alpha from the staged splat (stage_splat) at the pixel's tile
+// coordinates (x, y); 0 when below the alpha threshold. Every blend shape
+// evaluates this same expression, so images do not depend on the shape.
+__device__ __forceinline__ float fast_alpha(const float4& a, const float4& b, float x, float y) {
+  const float pw = fminf(fmaf(x, fmaf(a.x, x, fmaf(a.y, y, a.w)), fmaf(y, fmaf(a.z, y, b.x), b.y)), b.z);
   return pw >= kLog2AlphaMin ? ex2_approx(pw) : 0.0f;
 }
 
@@ -124,9 +136,7 @@ __device__ __forceinline__ float splat_alpha(bool inbox, const float4& a, const 
     // extent rounded outwards and pixels are sampled at their centres), so
     // the alpha test alone excludes it here; the exact path also tests the
     // bbox, as the reference does.
-    const float dx = lxf - a.x;
-    const float dy = lyf - a.y;
-    return fast_alpha(a, b, dx, a.z * dx, dy);
+    return fast_alpha(a, b, lxf, lyf);
   }
 }
 
@@ -209,24 +219,146 @@ struct __align__(16) StagedBatch {
   uint32_t my[G];
 };
 
+// The default shape (16x16 tiles, two groups of 256 threads per CTA) sorts
+// each tile of at most kMidSortCap pairs itself, before blending it (the
+// other shapes leave that to k_sort_small / k_sort_mid).
+template <int TW, int TH, int NT>
+constexpr bool kSortsTiles = TW == 16 && TH == 16 && NT == 512;
+
 // Shared memory of one tile group: two staged batches (the group blends one
 // while it stages the next), the warps' lists of batch entries, the tile's
-// quantised pixels for the fused downsample, the group's tile.
+// quantised pixels for the fused downsample, the group's tile and its pair-
+// count class. Groups that sort their tiles overlay the tile's words (and,
+// before them, the sort's counters) on the blend's arrays, which are idle
+// while the tile is sorted, and keep the sorted order in `slot`.
 template <int TW, int TH, int NT>
 struct __align__(16) GroupSmem {
   using S = BlendShape<TW, TH, NT>;
-  StagedBatch<S::G> bt[2];
-  uint16_t list[S::GW][S::G];
-  uint32_t px[S::P];
-  uint32_t work;
+  static constexpr bool kSort = kSortsTiles<TW, TH, NT>;
+  struct Blend {
+    StagedBatch<S::G> bt[2];
+    uint16_t list[S::GW][S::G];
+    uint32_t px[S::P];
+  };
+  union {
+    Blend b;
+    uint64_t words[kSort ? kMidSortCap : 1];
+  };
+  uint16_t slot[kSort ? kMidSortCap : 1];
+  uint32_t red[2][S::GW];
+  uint32_t wsum[S::GW];
+  uint32_t work, cls;
 };
+
+// The per-tile depth sort of a tile of n <= kMidSortCap pairs by its group
+// of 256 threads (thread t), in place in global memory: the counting pass of
+// smem_count_sort (a 12-bit monotone quantisation of the depth over the
+// tile's range, positions from shared-memory atomics on 16-bit packed
+// counters), runs of equal key ordered by the full word (a longer run than
+// one thread orders sends the whole tile through a bitonic sort), then the
+// words gathered into shared memory in that order and written back. The
+// result is the reference's (depth, scene index) order, as k_sort_small /
+// k_sort_mid produce it. sync() is the group's barrier, any(p) its vote.
+template <class Sm, class Sync, class Any>
+__device__ __forceinline__ void group_sort_tile(uint64_t* w, uint32_t n, Sm& sm, uint32_t t, Sync&& sync,
+                                                Any&& any) {
+  constexpr uint32_t kThreads = 256;
+  static_assert(kCountBuckets == 16 * kThreads, "16 counters per thread");
+  const uint32_t lane = t & 31, warp = t >> 5;
+  uint32_t* hist = reinterpret_cast<uint32_t*>(sm.words);
+  uint32_t mn = 0xFFFFFFFFu, mx = 0u;
+  for (uint32_t e = t; e < n; e += kThreads) {
+    const uint32_t d = (uint32_t)(w[e] >> 32);
+    mn = min(mn, d);
+    mx = max(mx, d);
+  }
+  for (uint32_t b = t; b < kCountBuckets / 2; b += kThreads) hist[b] = 0u;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+    mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  }
+  if (lane == 0) {
+    sm.red[0][warp] = mn;
+    sm.red[1][warp] = mx;
+  }
+  sync();
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    mn = min(mn, sm.red[0][k]);
+    mx = max(mx, sm.red[1][k]);
+  }
+  const float dmin = __uint_as_float(mn), range = __uint_as_float(mx) - dmin;
+  const float scale = range > 0.0f ? (float)(kCountBuckets - 1) / range : 0.0f;
+  auto quant = [&](uint64_t x) -> uint32_t {
+    const float q = (__uint_as_float((uint32_t)(x >> 32)) - dmin) * scale;
+    return q >= (float)(kCountBuckets - 1) ? kCountBuckets - 1 : (uint32_t)q;
+  };
+  for (uint32_t e = t; e < n; e += kThreads) {
+    const uint32_t q = quant(w[e]);
+    atomicAdd(&hist[q >> 1], 1u << (16 * (q & 1u)));
+  }
+  sync();
+  // Exclusive scan of the 4096 counters, 16 per thread.
+  uint32_t c[16], sum = 0;
+  uint4* h4 = reinterpret_cast<uint4*>(hist + 8 * t);
+#pragma unroll
+  for (int k = 0; k < 2; k++) {
+    const uint4 v = h4[k];
+    const uint32_t w4[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      c[8 * k + 2 * j] = w4[j] & 0xFFFFu;
+      c[8 * k + 2 * j + 1] = w4[j] >> 16;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 16; k++) sum += c[k];
+  uint32_t x = sum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) sm.wsum[warp] = x;
+  sync();
+  uint32_t run = x - sum;
+  for (uint32_t k = 0; k < warp; k++) run += sm.wsum[k];
+  uint32_t pk[8];
+#pragma unroll
+  for (int j = 0; j < 8; j++) {
+    const uint32_t lo = run;
+    run += c[2 * j];
+    pk[j] = lo | (run << 16);
+    run += c[2 * j + 1];
+  }
+  h4[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+  h4[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+  sync();
+  for (uint32_t e = t; e < n; e += kThreads) {
+    const uint32_t q = quant(w[e]), sh = 16 * (q & 1u);
+    sm.slot[(atomicAdd(&hist[q >> 1], 1u << sh) >> sh) & 0xFFFFu] = (uint16_t)e;
+  }
+  sync();
+  const bool long_run = sort_short_runs(
+      sm.slot, n, t, kThreads, [&](uint16_t i) { return quant(w[i]); }, [&](uint16_t i) { return w[i]; });
+  const bool any_long = any(long_run);  // also the barrier after the runs
+  for (uint32_t e = t; e < n; e += kThreads) sm.words[e] = w[sm.slot[e]];
+  sync();
+  if (any_long) bitonic_sort(sm.words, n, t, kThreads, sync);
+  for (uint32_t e = t; e < n; e += kThreads) w[e] = sm.words[e];
+  sync();  // the group's staging reads the sorted words next
+}
 
 // COUNT: also counts the pixel/splat evaluations (the blend's unit of work
 // after early termination) into st->evals; a separate instantiation, used
 // only when SPLAT_OPT_COUNT_EVALS asks for it.
+//
+// The pair words are read with ordinary (coherent) loads: groups of the
+// default shape sort their tile in place before they stage it.
 template <bool EXACT, int TW, int TH, int NT, bool ROWS, bool COUNT = false>
 __global__ void __launch_bounds__(NT, NT == 512 ? 2 : (NT == 256 ? 5 : 8)) k_blend(const ViewTask* __restrict__ table, uint32_t n_views, uint32_t n_tiles,
-                                              const uint64_t* __restrict__ pairs, const uint2* __restrict__ ranges,
+                                              uint64_t* pairs, const uint2* __restrict__ ranges,
                                               const uint32_t* __restrict__ order, DevState* st) {
   using S = BlendShape<TW, TH, NT>;
   using Smem = GroupSmem<TW, TH, NT>;
@@ -260,16 +392,18 @@ __global__ void __launch_bounds__(NT, NT == 512 ? 2 : (NT == 256 ? 5 : 8)) k_ble
   __syncthreads();
   for (;;) {
     if (gt == 0) {
-      uint32_t w = atomicAdd(&st->blend_next, 1u), tl = 0xFFFFFFFFu;
+      uint32_t w = atomicAdd(&st->blend_next, 1u), tl = 0xFFFFFFFFu, cl = kTileClasses;
 #pragma unroll
       for (int k = 0; k < kTileClasses; k++) {
         if (w < s_cls[k]) {
           tl = order[(size_t)k * n_tiles + w];
+          cl = (uint32_t)k;
           break;
         }
         w -= s_cls[k];
       }
       sm.work = tl;
+      sm.cls = cl;
     }
     sync();
     const uint32_t tile = sm.work;
@@ -311,6 +445,12 @@ __global__ void __launch_bounds__(NT, NT == 512 ? 2 : (NT == 256 ? 5 : 8)) k_ble
 
     const uint2 range = ranges[tile];
     const uint32_t begin = range.x, n = range.y > range.x ? range.y - range.x : 0u;
+    if constexpr (Smem::kSort) {
+      // Tiles of classes 1-5 (2 .. kMidSortCap pairs) are sorted here; longer
+      // ones were sorted by k_sort_long.
+      if (sm.cls >= 1 && sm.cls <= 5 && n >= 2)
+        group_sort_tile(pairs + begin, n, sm, (uint32_t)gt, sync, [&](bool p) { return count(p) != 0; });
+    }
     // Batch k is staged into buffer k & 1 by the group while it blends batch
     // k - 1 from the other buffer; the barrier that ends batch k - 1 (the
     // early-exit vote) publishes it. The records of batch k + 1 are in
@@ -339,14 +479,14 @@ __global__ void __launch_bounds__(NT, NT == 512 ? 2 : (NT == 256 ? 5 : 8)) k_ble
     if (n > 0) {
       if ((uint32_t)gt < n) {
         nr = rec[(uint32_t)pairs[begin + gt]];
-        stage(sm.bt[0]);
+        stage(sm.b.bt[0]);
       }
       has = (uint32_t)gt + G < n;
       if (has) nr = rec[(uint32_t)pairs[begin + G + gt]];
       sync();
     }
     for (uint32_t start = 0, buf = 0; start < n; start += G, buf ^= 1u) {
-      const StagedBatch<G>& bt = sm.bt[buf];
+      const StagedBatch<G>& bt = sm.b.bt[buf];
       const uint32_t cnt = min((uint32_t)G, n - start);
       // This warp's list of batch entries whose bbox meets its block.
       uint32_t len = 0;
@@ -355,7 +495,7 @@ __global__ void __launch_bounds__(NT, NT == 512 ? 2 : (NT == 256 ? 5 : 8)) k_ble
           const uint32_t e = c0 + lane;
           const bool hit = e < cnt && (bt.mx[e] & wxbits) && (bt.my[e] & wybits);
           const uint32_t bal = __ballot_sync(0xffffffffu, hit);
-          if (hit) sm.list[gw][len + __popc(bal & ((1u << lane) - 1u))] = (uint16_t)e;
+          if (hit) sm.b.list[gw][len + __popc(bal & ((1u << lane) - 1u))] = (uint16_t)e;
           len += __popc(bal);
         }
         __syncwarp();
@@ -368,7 +508,7 @@ __global__ void __launch_bounds__(NT, NT == 512 ? 2 : (NT == 256 ? 5 : 8)) k_ble
           // when the first one saturated the pixel.
           const float rowc = (float)(oy + ly0) + 0.5f, lxf = (float)lx, lyf = (float)ly0;
           const uint32_t ybit = 1u << ly0, xbit = 1u << lx;
-          const uint16_t* lst = sm.list[gw];
+          const uint16_t* lst = sm.b.list[gw];
           uint32_t k = 0;
           for (; k + 1 < len; k += 2) {
             const uint32_t jj = *reinterpret_cast<const uint32_t*>(lst + k);  // k even: 4-byte aligned
@@ -406,7 +546,7 @@ __global__ void __launch_bounds__(NT, NT == 512 ? 2 : (NT == 256 ? 5 : 8)) k_ble
         } else {
           const uint32_t xbit = 1u << lx;
           for (uint32_t k = 0; k < len && !all_done; k++) {
-            const uint32_t j = sm.list[gw][k];
+            const uint32_t j = sm.b.list[gw][k];
             const float4 a = bt.a[j], b = bt.b[j];
             const uint32_t mx = bt.mx[j], my = bt.my[j];
             float red, green, blue;
@@ -431,7 +571,7 @@ __global__ void __launch_bounds__(NT, NT == 512 ? 2 : (NT == 256 ? 5 : 8)) k_ble
         }
       }
       const uint32_t nxt = start + 2 * G + gt;
-      if (has) stage(sm.bt[buf ^ 1u]);  // batch start + G
+      if (has) stage(sm.b.bt[buf ^ 1u]);  // batch start + G
       has = nxt < n;
       if (has) nr = rec[(uint32_t)pairs[begin + nxt]];
       if (count(!all_done) == 0) break;
@@ -464,7 +604,7 @@ __global__ void __launch_bounds__(NT, NT == 512 ? 2 : (NT == 256 ? 5 : 8)) k_ble
       const uint32_t qg = to_u8(__fadd_rn(cg[k], __fmul_rn(T[k], bg1)));
       const uint32_t qb = to_u8(__fadd_rn(cb[k], __fmul_rn(T[k], bg2)));
       if (fused || rows) {
-        sm.px[ly * TW + lx] = qr | (qg << 8) | (qb << 16);
+        sm.b.px[ly * TW + lx] = qr | (qg << 8) | (qb << 16);
       } else if (px >= X0 && px < X1 && py >= Y0 && py < Y1) {
         // f == 1: the frame (window); other factors: the full-resolution
         // scratch frame (whole frames: OY = 0).
@@ -483,7 +623,7 @@ __global__ void __launch_bounds__(NT, NT == 512 ? 2 : (NT == 256 ? 5 : 8)) k_ble
 #pragma unroll
           for (uint32_t r = 0; r < 4; r++) {
             const uint32_t bb = b0 + r;
-            v |= ((sm.px[ly * TW + bb / 3u] >> (8u * (bb % 3u))) & 255u) << (8u * r);
+            v |= ((sm.b.px[ly * TW + bb / 3u] >> (8u * (bb % 3u))) & 255u) << (8u * r);
           }
           *reinterpret_cast<uint32_t*>(out + ((size_t)(py - OY) * W + ox) * 3 + b0) = v;
         }
@@ -499,7 +639,7 @@ __global__ void __launch_bounds__(NT, NT == 512 ? 2 : (NT == 256 ? 5 : 8)) k_ble
           uint32_t acc[3] = {0u, 0u, 0u};
           for (uint32_t sy = 0; sy < f; sy++)
             for (uint32_t sx = 0; sx < f; sx++) {
-              const uint32_t p = sm.px[(byl * f + sy) * TW + bxl * f + sx];
+              const uint32_t p = sm.b.px[(byl * f + sy) * TW + bxl * f + sx];
               acc[0] += p & 255u;
               acc[1] += (p >> 8) & 255u;
               acc[2] += (p >> 16) & 255u;
@@ -539,6 +679,8 @@ __global__ void k_downsample(FrameParams fp, const uint8_t* __restrict__ full, u
 
 }  // namespace
 
+bool blend_sorts_tiles(const BlendConfig& c) { return c.tile_w == 16 && c.tile_h == 16 && c.threads == 512; }
+
 bool blend_config_supported(const BlendConfig& c) {
   const bool shape = (c.tile_w == 8 && c.tile_h == 8) || (c.tile_w == 16 && c.tile_h == 16) ||
                      (c.tile_w == 32 && c.tile_h == 16);
@@ -548,7 +690,7 @@ bool blend_config_supported(const BlendConfig& c) {
 namespace {
 
 template <bool EXACT, int TW, int TH, int NT, bool ROWS, bool COUNT = false>
-cudaError_t launch_blend_t(const ViewTask* table, uint32_t n_views, uint32_t n_tiles, const uint64_t* pairs,
+cudaError_t launch_blend_t(const ViewTask* table, uint32_t n_views, uint32_t n_tiles, uint64_t* pairs,
                            const uint2* ranges, const uint32_t* order, DevState* st, int num_sms,
                            cudaStream_t stream) {
   using S = BlendShape<TW, TH, NT>;
@@ -572,7 +714,7 @@ cudaError_t launch_blend_t(const ViewTask* table, uint32_t n_views, uint32_t n_t
 }
 
 template <bool EXACT>
-cudaError_t launch_blend_e(const ViewTask* table, uint32_t n_views, uint32_t n_tiles, const uint64_t* pairs,
+cudaError_t launch_blend_e(const ViewTask* table, uint32_t n_views, uint32_t n_tiles, uint64_t* pairs,
                            const uint2* ranges, const uint32_t* order, const BlendConfig& c, DevState* st,
                            int num_sms, cudaStream_t s, bool rows, bool count) {
   // The row-word variant for mapped host frames and the evaluation-counting
@@ -605,7 +747,7 @@ cudaError_t launch_blend_e(const ViewTask* table, uint32_t n_views, uint32_t n_t
 
 }  // namespace
 
-cudaError_t launch_blend(const ViewTask* table, uint32_t n_views, uint32_t n_tiles, const uint64_t* pairs,
+cudaError_t launch_blend(const ViewTask* table, uint32_t n_views, uint32_t n_tiles, uint64_t* pairs,
                          const uint2* ranges, const uint32_t* order, bool exact, const BlendConfig& cfg, DevState* st,
                          int num_sms, cudaStream_t stream, uint32_t* launches, bool host_rows, bool count) {
   if (n_tiles == 0) return cudaSuccess;

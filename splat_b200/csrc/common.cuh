@@ -201,6 +201,9 @@ struct BlendConfig {
   uint32_t tile_w, tile_h, threads;
 };
 bool blend_config_supported(const BlendConfig& c);
+// Whether the blend of this configuration sorts the tiles of at most
+// kMidSortCap pairs itself (then the binning launches no small/mid sorts).
+bool blend_sorts_tiles(const BlendConfig& c);
 
 // Launchers (each returns the cudaGetLastError of its launches and adds the
 // number of kernels it launched to *launches).
@@ -229,13 +232,15 @@ struct BinLaunch {
   uint32_t* counts_all;   // all count matrices (for the zeroing)
   size_t counts_bytes;
 };
+// tile_sorts: launch the sorts of tiles of at most kMidSortCap pairs (false
+// when the blend sorts them itself, blend_sorts_tiles).
 cudaError_t launch_binning(const ViewTask* table, const BinLaunch& bl, uint32_t* totals, uint2* ranges,
                            uint32_t* order, uint64_t* pairs, uint64_t* pairs_alt,
                            uint64_t cap, const FrameCounters& fc, int num_sms, size_t max_smem, cudaStream_t stream,
-                           uint32_t* launches);
+                           uint32_t* launches, bool tile_sorts = true);
 // (d) blend + downsample over the depth-sorted buckets of every view.
 // host_rows: the views' frames are mapped pinned host memory (see k_blend).
-cudaError_t launch_blend(const ViewTask* table, uint32_t n_views, uint32_t n_tiles, const uint64_t* pairs,
+cudaError_t launch_blend(const ViewTask* table, uint32_t n_views, uint32_t n_tiles, uint64_t* pairs,
                          const uint2* ranges, const uint32_t* order, bool exact, const BlendConfig& cfg, DevState* st,
                          int num_sms, cudaStream_t stream, uint32_t* launches, bool host_rows = false,
                          bool count = false);

@@ -163,7 +163,10 @@ def test_batch_configs_and_tuner():
         assert np.array_equal(got[i], want[i]), f"tuned view {i}"
     n0 = b.get_option(N.SPLAT_OPT_KERNEL_LAUNCHES)
     b.render()
-    assert b.get_option(N.SPLAT_OPT_KERNEL_LAUNCHES) - n0 == 9
+    # project, count, column scan, ranges, scatter, long sort, blend; plus the
+    # small and mid tile sorts unless the blend sorts them (16x16 tiles, 512 threads)
+    want_launches = 7 if tuple(b.config) == (16, 16, 512) else 9
+    assert b.get_option(N.SPLAT_OPT_KERNEL_LAUNCHES) - n0 == want_launches
     b.close()
     for r in rends:
         r.close()
