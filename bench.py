@@ -444,8 +444,15 @@ def run_ours(args):
         for i in range(args.steps):
             r.render_device(views[i % len(views)], W, H, (0, 0, 0), out.data_ptr(), nbytes)
             s, _ = r.finish()
+        # The last profiled frame again, with the blend counting its evaluations
+        # (launched after the profiled frames: outside a capture of their launches).
+        r.set_option(Nat.SPLAT_OPT_COUNT_EVALS, 1)
+        r.render_device(views[(args.steps - 1) % len(views)], W, H, (0, 0, 0), out.data_ptr(), nbytes)
+        r.finish()
+        evals = r.get_option(Nat.SPLAT_OPT_BLEND_EVALS)
         if rank == 0:
-            print(json.dumps({"profile_frames": args.steps, "visible": s.visible, "pairs": s.overlaps}), flush=True)
+            print(json.dumps({"profile_frames": args.steps, "visible": s.visible, "pairs": s.overlaps,
+                              "last_frame_blend_evaluations": evals}), flush=True)
         r.close()
         return
 
