@@ -514,6 +514,15 @@ def run_ours(args):
     e2e_s = time.perf_counter() - t0
     te_max = max_over_ranks(e2e_s, dev)
     e2e = frames_total / te_max
+    # Where an end-to-end frame's time goes: the device stages (frames written
+    # through the host buffer's device mapping) and the call's wall time.
+    e2e_stages = {"project_ms": 0.0, "sort_ms": 0.0, "raster_ms": 0.0, "call_ms": 0.0}
+    for v in views:
+        st_e = r.render_into(v, W, H, (0, 0, 0), host.data_ptr(), host.numel())
+        e2e_stages["project_ms"] += st_e.project_ms / len(views)
+        e2e_stages["sort_ms"] += st_e.sort_ms / len(views)
+        e2e_stages["raster_ms"] += st_e.raster_ms / len(views)
+        e2e_stages["call_ms"] += st_e.total_ms / len(views)
 
     errors = None
     if rank == 0 and cfg["precision"] == "fp16" and args.error_frames > 0:
@@ -570,7 +579,8 @@ def run_ours(args):
                     "d2h_bytes_per_step": W * H * 3 + 32,
                     "note": "input per step: the 56-byte view, passed as kernel parameters (the scene stays "
                             "resident); output: the u8 frame, written by the blend straight into the caller's "
-                            "pinned host buffer through its device mapping, plus the 32-byte frame state"},
+                            "pinned host buffer through its device mapping, plus the 32-byte frame state",
+                    "stages_ms": e2e_stages},
             "clocks": clk.summary(),
             "gpu_launches": launches,
         }
