@@ -318,6 +318,7 @@ namespace {
 int enqueue_frame(splat_cuda_handle* h, const FrameParams& fp_in, uint8_t* dev_out, bool host_mapped = false) {
   FrameParams fp = fp_in;
   set_tile_shape(fp, h->blend.tile_w, h->blend.tile_h);
+  fp.flags = h->debug_capture ? kFrameKeepSortedPairs : 0u;  // splat_cuda_debug_dump reads the sorted pairs
   const uint64_t tiles = (uint64_t)fp.tiles_x * fp.tiles_y;
   const uint32_t f = fp.downsample;
   const bool scratch = f > 1 && (fp.tile_w % f != 0 || fp.tile_h % f != 0);

@@ -287,7 +287,9 @@ int record(splat_cuda_batch* b) {
 // Kernels per batch (the launch count one graph replay adds).
 uint32_t kernels_per_batch(const splat_cuda_batch* b) {
   if (!b->n_tiles) return 0u;
-  return 8u + (b->proj_ctas ? 1u : 0u) + (b->learned_tiles ? 1u : 0u);
+  // count, column scan, ranges, scatter, long sort, blend, and the small and
+  // mid tile sorts unless the blend sorts those tiles itself
+  return (blend_sorts_tiles(b->cfg) ? 6u : 8u) + (b->proj_ctas ? 1u : 0u) + (b->learned_tiles ? 1u : 0u);
 }
 
 const DevState& host_state(const splat_cuda_batch* b) { return *static_cast<const DevState*>(b->counters_host); }

@@ -49,7 +49,7 @@ constexpr int kBinThreads = 512;
 constexpr uint32_t kNoTile = 0xFFFFFFFFu;
 // false: each lane expands its own splat's pairs at its own pace, one bucket
 // atomic per pair (fw), as for the larger splats.
-constexpr bool kAggregateBuckets = true;
+constexpr bool kAggregateBuckets = false;
 
 template <class F, class FW>
 __device__ __forceinline__ void for_each_pair(const BinInfo* __restrict__ bin, const uint32_t* __restrict__ order,

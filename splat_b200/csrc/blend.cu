@@ -259,9 +259,15 @@ struct __align__(16) GroupSmem {
 // words gathered into shared memory in that order and written back. The
 // result is the reference's (depth, scene index) order, as k_sort_small /
 // k_sort_mid produce it. sync() is the group's barrier, any(p) its vote.
+//
+// Unless write_back is set (or a long run sent the tile through the bitonic
+// sort), the tile's words stay where they are and the order is left in
+// sm.slot: the group stages word slot[k] as the k-th; the function returns
+// true then. write_back (the frame keeps its sorted pairs for inspection)
+// gathers the words into shared memory in order and writes them back.
 template <class Sm, class Sync, class Any>
-__device__ __forceinline__ void group_sort_tile(uint64_t* w, uint32_t n, Sm& sm, uint32_t t, Sync&& sync,
-                                                Any&& any) {
+__device__ __forceinline__ bool group_sort_tile(uint64_t* w, uint32_t n, Sm& sm, uint32_t t, Sync&& sync, Any&& any,
+                                                bool write_back) {
   constexpr uint32_t kThreads = 256;
   static_assert(kCountBuckets == 16 * kThreads, "16 counters per thread");
   const uint32_t lane = t & 31, warp = t >> 5;
@@ -343,11 +349,13 @@ __device__ __forceinline__ void group_sort_tile(uint64_t* w, uint32_t n, Sm& sm,
   const bool long_run = sort_short_runs(
       sm.slot, n, t, kThreads, [&](uint16_t i) { return quant(w[i]); }, [&](uint16_t i) { return w[i]; });
   const bool any_long = any(long_run);  // also the barrier after the runs
+  if (!any_long && !write_back) return true;
   for (uint32_t e = t; e < n; e += kThreads) sm.words[e] = w[sm.slot[e]];
   sync();
   if (any_long) bitonic_sort(sm.words, n, t, kThreads, sync);
   for (uint32_t e = t; e < n; e += kThreads) w[e] = sm.words[e];
   sync();  // the group's staging reads the sorted words next
+  return false;
 }
 
 // COUNT: also counts the pixel/splat evaluations (the blend's unit of work
@@ -445,12 +453,16 @@ __global__ void __launch_bounds__(NT, NT == 512 ? 2 : (NT == 256 ? 5 : 8)) k_ble
 
     const uint2 range = ranges[tile];
     const uint32_t begin = range.x, n = range.y > range.x ? range.y - range.x : 0u;
+    bool use_slot = false;
     if constexpr (Smem::kSort) {
       // Tiles of classes 1-5 (2 .. kMidSortCap pairs) are sorted here; longer
       // ones were sorted by k_sort_long.
-      if (sm.cls >= 1 && sm.cls <= 5 && n >= 2)
-        group_sort_tile(pairs + begin, n, sm, (uint32_t)gt, sync, [&](bool p) { return count(p) != 0; });
+      use_slot = sm.cls >= 1 && sm.cls <= 5 && n >= 2 &&
+                 group_sort_tile(pairs + begin, n, sm, (uint32_t)gt, sync, [&](bool p) { return count(p) != 0; },
+                                 (tv->fp.flags & kFrameKeepSortedPairs) != 0u);
     }
+    // The k-th pair word of the tile in depth order.
+    auto word_at = [&](uint32_t k) -> uint64_t { return pairs[begin + (use_slot ? (uint32_t)sm.slot[k] : k)]; };
     // Batch k is staged into buffer k & 1 by the group while it blends batch
     // k - 1 from the other buffer; the barrier that ends batch k - 1 (the
     // early-exit vote) publishes it. The records of batch k + 1 are in
@@ -478,11 +490,11 @@ __global__ void __launch_bounds__(NT, NT == 512 ? 2 : (NT == 256 ? 5 : 8)) k_ble
     };
     if (n > 0) {
       if ((uint32_t)gt < n) {
-        nr = rec[(uint32_t)pairs[begin + gt]];
+        nr = rec[(uint32_t)word_at(gt)];
         stage(sm.b.bt[0]);
       }
       has = (uint32_t)gt + G < n;
-      if (has) nr = rec[(uint32_t)pairs[begin + G + gt]];
+      if (has) nr = rec[(uint32_t)word_at(G + gt)];
       sync();
     }
     for (uint32_t start = 0, buf = 0; start < n; start += G, buf ^= 1u) {
@@ -573,7 +585,7 @@ __global__ void __launch_bounds__(NT, NT == 512 ? 2 : (NT == 256 ? 5 : 8)) k_ble
       const uint32_t nxt = start + 2 * G + gt;
       if (has) stage(sm.b.bt[buf ^ 1u]);  // batch start + G
       has = nxt < n;
-      if (has) nr = rec[(uint32_t)pairs[begin + nxt]];
+      if (has) nr = rec[(uint32_t)word_at(nxt)];
       if (count(!all_done) == 0) break;
     }
 

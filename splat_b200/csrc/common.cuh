@@ -50,8 +50,13 @@ struct FrameParams {
   // win_y0; windows drawn into the whole frame: 0). A window that does not
   // start at column 0 or end at the frame's edge is aligned to tiles.
   uint32_t win_y0, win_rows, win_ty0, out_y0;
-  uint32_t win_x0, win_cols, win_tx0, pad;
+  uint32_t win_x0, win_cols, win_tx0;
+  uint32_t flags;  // kFrame* bits
 };
+// The frame's pair buffer keeps every tile's pairs in depth order after the
+// blend (for inspection; otherwise tiles the blend sorts itself may be left
+// in bucket order, their order held in shared memory only).
+constexpr uint32_t kFrameKeepSortedPairs = 1u;
 
 // Device-resident scene, FP32 storage (layout chosen for coalesced loads).
 struct SceneDev {
