@@ -91,6 +91,10 @@ def parse():
     p.add_argument("--psnr-frames", type=int, default=40, help="learned: orbit frames compared with exact SH")
     p.add_argument("--profile", action="store_true",
                    help="render --warmup then --steps frames and exit (a short command for ncu captures)")
+    p.add_argument("--profile-io", action="store_true",
+                   help="decode the workload's PLY and .splat bytes on the device (FP32 and FP16 storage) and draw "
+                        "its home frame as terminal cells (half blocks, downsample 2; truecolor and ANSI-256), "
+                        "--steps times each, then exit (a short command for ncu captures of k_decode_* and k_cells)")
     a = p.parse_args()
     if a.steps is None:
         a.steps = {"plain": 4000, "fp16": 1000, "batch": 20, "learned": 4000}[a.config]
@@ -1088,8 +1092,36 @@ def run_batch(args):
         torch.distributed.destroy_process_group()
 
 
+def run_profile_io(args):
+    """The scene-file decoders and the terminal-cell kernel on the plain
+    workload (see --profile-io)."""
+    import torch
+
+    from oracle import scene_io as IO
+    from splat_b200 import _native as Nat
+    from splat_b200.render import CudaRenderer, from_ply_bytes, from_splat_bytes
+
+    torch.cuda.set_device(0)
+    cfg = CONFIGS["plain"]
+    scene, _, _, home, _, _ = make_workload(args.splats, cfg)
+    ply, spl = IO.write_ply(scene), IO.write_splat(scene)
+    for _ in range(args.steps):
+        for data, loader in ((ply, from_ply_bytes), (spl, from_splat_bytes)):
+            for prec in (Nat.SPLAT_PRECISION_FP32, Nat.SPLAT_PRECISION_FP16):
+                loader(data, precision=prec).close()
+    r = CudaRenderer(scene)
+    for _ in range(args.steps):
+        for mode in (Nat.SPLAT_CELLS_TRUECOLOR, Nat.SPLAT_CELLS_ANSI256):
+            r.render_cells(home, cfg["w"], cfg["h"], (0, 0, 0), downsample=2, mode=mode)
+    r.close()
+    print(json.dumps({"profile_io": args.steps, "ply_bytes": len(ply), "splat_bytes": len(spl)}), flush=True)
+
+
 def main():
     args = parse()
+    if args.profile_io:
+        run_profile_io(args)
+        return
     if args.config == "batch":
         if args.impl == "reference":
             run_batch_reference(args)

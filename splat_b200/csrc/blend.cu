@@ -82,8 +82,9 @@ __device__ __forceinline__ uint32_t to_u8(float v) {
 }
 
 
-// Default path staging. With the splat's centre in tile pixel coordinates
-// (xs, ys; exact differences, the same whatever the tile shape), its conic
+// Default path staging. With the splat's centre in the pixel coordinates
+// of the 32 x 16 block of the frame that holds the tile (xs, ys; the same
+// block whatever the tile shape), its conic
 // times log2 e (A, B, C: power = A dx^2 + B dx dy + C dy^2 in log2 units,
 // dx = x - xs, dy = y - ys) and lop = log2 opacity, the exponent
 // pw' = power + lop is expanded once per splat into a quadratic in the
@@ -108,9 +109,10 @@ __device__ __forceinline__ void stage_splat(const Record& r, float ox05, float o
   c = make_float2(r.r1.w, r.r2.x);
 }
 
-// Default path alpha from the staged splat (stage_splat) at the pixel's tile
-// coordinates (x, y); 0 when below the alpha threshold. Every blend shape
-// evaluates this same expression, so images do not depend on the shape.
+// Default path alpha from the staged splat (stage_splat) at the pixel's
+// coordinates (x, y) in the 32 x 16 block; 0 when below the alpha threshold.
+// Every blend shape evaluates this same expression with the same operands,
+// so images do not depend on the shape.
 __device__ __forceinline__ float fast_alpha(const float4& a, const float4& b, float x, float y) {
   const float pw = fminf(fmaf(x, fmaf(a.x, x, fmaf(a.y, y, a.w)), fmaf(y, fmaf(a.z, y, b.x), b.y)), b.z);
   return pw >= kLog2AlphaMin ? ex2_approx(pw) : 0.0f;
@@ -437,7 +439,13 @@ __global__ void __launch_bounds__(NT, NT == 512 ? 2 : (NT == 256 ? 5 : 8)) k_ble
     // (src/render/cpu.rs:658-671).
     const float fx05 = __fadd_rn((float)(px & ~15u), 0.5f);
     const float gbase = (float)(px & 12u), lanef = (float)(px & 3u);
-    const float ox05 = (float)ox + 0.5f, oy05 = (float)oy + 0.5f;
+    // Default path: the staged exponent is a quadratic in pixel coordinates
+    // relative to the 32 x 16 block of the frame that holds the tile (qx0,
+    // qy0), the same block for every tile shape, so that a pixel's
+    // arithmetic and image do not depend on the shape.
+    const uint32_t qx0 = ox & ~31u, qy0 = oy & ~15u;
+    const float ox05 = (float)qx0 + 0.5f, oy05 = (float)qy0 + 0.5f;
+    const float qxf = (float)(px - qx0);
 
     float T[PPT], cr[PPT], cg[PPT], cb[PPT];
     uint32_t evals = 0;
@@ -518,7 +526,7 @@ __global__ void __launch_bounds__(NT, NT == 512 ? 2 : (NT == 256 ? 5 : 8)) k_ble
           // below the alpha test contributes alpha = 0, which leaves C and T
           // unchanged bit for bit; the second splat is dropped (alpha = 0)
           // when the first one saturated the pixel.
-          const float rowc = (float)(oy + ly0) + 0.5f, lxf = (float)lx, lyf = (float)ly0;
+          const float rowc = (float)(oy + ly0) + 0.5f, lxf = qxf, lyf = (float)(oy + ly0 - qy0);
           const uint32_t ybit = 1u << ly0, xbit = 1u << lx;
           const uint16_t* lst = sm.b.list[gw];
           uint32_t k = 0;
@@ -570,7 +578,7 @@ __global__ void __launch_bounds__(NT, NT == 512 ? 2 : (NT == 256 ? 5 : 8)) k_ble
                 const uint32_t ly = ly0 + q;
                 const bool in = !EXACT || ((mx & xbit) && ((my >> ly) & 1u));
                 const float al = splat_alpha<EXACT>(in, a, b, fx05, gbase, lanef, (float)(oy + ly) + 0.5f,
-                                                    (float)lx, (float)ly);
+                                                    qxf, (float)(oy + ly - qy0));
                 if (COUNT) evals += 1;
                 if (al > 0.0f) {
                   accumulate<EXACT>(al, red, green, blue, T[q], cr[q], cg[q], cb[q]);
