@@ -615,7 +615,8 @@ def learned_quality_correlated(args, W, H, dev):
     """The learned colour's quality where the SH carries structure: the same
     1.2M-splat geometry with the 45 higher coefficients generated from a
     4-dimensional code per splat (synth.cluster_scene(sh_code_dim=4)),
-    trained as the main workload, PSNR against exact SH over orbit frames."""
+    trained as the main workload for twice its epochs, PSNR against exact
+    SH over orbit frames."""
     from oracle import oracle as O
     from splat_b200 import Frame, synth
     from splat_b200.learned import LearnConfig, Learner, learned_renderer
@@ -626,7 +627,7 @@ def learned_quality_correlated(args, W, H, dev):
     _, _, timed = synth.orbit_views(cam, ORBIT, 5)
     exact = CudaRenderer(scene, device=dev)
     learner = Learner(exact, LearnConfig(directions=256, batch=65536, lr=1e-3, seed=1))
-    ts = learner.train(max(1, int(round(args.learn_epochs * learner.steps_per_epoch))))
+    ts = learner.train(max(1, int(round(2 * args.learn_epochs * learner.steps_per_epoch))))
     p16, lat16 = learner.params_f16()
     learner.close()
     r = learned_renderer(scene.to_fp16(), lat16, p16, device=dev)

@@ -94,7 +94,8 @@ int ensure_pairs(splat_cuda_handle* h, uint64_t cap) {
   if (cap <= h->cap) return SPLAT_OK;
   if (cap > kMaxPairs) return fail(h, SPLAT_ERR_CAPACITY, "more than 2^30 - 1 gaussian/tile pairs");
   free_pairs(h);
-  for (int b = 0; b < 2; b++) CK(dmalloc(h, &h->pairs[b], cap * sizeof(uint64_t)), "cudaMalloc pairs");
+  // Two words of slack: the blend's bulk copy of a tile rounds its end up to 16 bytes.
+  for (int b = 0; b < 2; b++) CK(dmalloc(h, &h->pairs[b], (cap + 2) * sizeof(uint64_t)), "cudaMalloc pairs");
   h->cap = cap;
   return SPLAT_OK;
 }
@@ -397,8 +398,9 @@ int finish_frame(splat_cuda_handle* h, splat_render_stats* stats, int* regrown) 
     const unsigned code = st.error;
     cudaMemsetAsync(h->st, 0, sizeof(DevState), h->stream);
     return fail(h, SPLAT_ERR_TIMEOUT,
-                code == 2u ? "the projection's bulk copies did not complete in time"
-                           : "a tensor-core wait in the learned-colour projection gave up");
+                code == 2u   ? "the projection's bulk copies did not complete in time"
+                : code == 3u ? "the blend's bulk copy of a tile's pairs did not complete in time"
+                             : "a tensor-core wait in the learned-colour projection gave up");
   }
   h->have_frame = true;
   if (st.total_pairs > h->cap) {

@@ -120,7 +120,8 @@ int ensure_pairs(splat_cuda_batch* b, uint64_t cap) {
   if (cap > kMaxPairs) return bfail(b, SPLAT_ERR_CAPACITY, "more than 2^30 - 1 gaussian/tile pairs in the batch");
   for (auto& p : b->pairs) dfree(p);
   b->cap = 0;
-  for (auto& p : b->pairs) BK(cudaMalloc(&p, cap * sizeof(uint64_t)), "cudaMalloc pairs");
+  // Two words of slack: the blend's bulk copy of a tile rounds its end up to 16 bytes.
+  for (auto& p : b->pairs) BK(cudaMalloc(&p, (cap + 2) * sizeof(uint64_t)), "cudaMalloc pairs");
   b->cap = cap;
   return SPLAT_OK;
 }

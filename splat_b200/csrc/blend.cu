@@ -40,6 +40,7 @@
 
 #include "common.cuh"
 #include "tilesort.cuh"
+#include "umma.cuh"
 
 namespace splat {
 namespace {
@@ -242,45 +243,77 @@ struct __align__(16) GroupSmem {
     uint16_t list[S::GW][S::G];
     uint32_t px[S::P];
   };
+  // The tile's words as the bulk copy brings them in (with one word of
+  // alignment slack in front and one behind) and the counting sort's 4096
+  // 16-bit counters, overlaid on the blend's arrays while the tile is sorted.
+  struct Sort {
+    uint64_t words[kSort ? kMidSortCap + 2 : 1];
+    uint32_t hist[kSort ? kCountBuckets / 2 : 1];
+  };
   union {
     Blend b;
-    uint64_t words[kSort ? kMidSortCap : 1];
+    Sort srt;
   };
   uint16_t slot[kSort ? kMidSortCap : 1];
   uint32_t red[2][S::GW];
   uint32_t wsum[S::GW];
+  uint64_t mbar;  // completion of the tile's bulk copy
   uint32_t work, cls;
 };
 
 // The per-tile depth sort of a tile of n <= kMidSortCap pairs by its group
-// of 256 threads (thread t), in place in global memory: the counting pass of
-// smem_count_sort (a 12-bit monotone quantisation of the depth over the
-// tile's range, positions from shared-memory atomics on 16-bit packed
-// counters), runs of equal key ordered by the full word (a longer run than
-// one thread orders sends the whole tile through a bitonic sort), then the
-// words gathered into shared memory in that order and written back. The
-// result is the reference's (depth, scene index) order, as k_sort_small /
-// k_sort_mid produce it. sync() is the group's barrier, any(p) its vote.
-//
-// Unless write_back is set (or a long run sent the tile through the bitonic
-// sort), the tile's words stay where they are and the order is left in
-// sm.slot: the group stages word slot[k] as the k-th; the function returns
-// true then. write_back (the frame keeps its sorted pairs for inspection)
-// gathers the words into shared memory in order and writes them back.
+// of 256 threads (thread t). The tile's words (w, in the pair buffer) come
+// into shared memory by one bulk asynchronous copy (TMA, cp.async.bulk,
+// completing on the group's mbarrier; the copy starts at the 16-byte boundary
+// at or below the tile and the pair buffer has slack for its rounded-up
+// end), and the sort reads them there: the counting pass of smem_count_sort
+// (a 12-bit monotone quantisation of the depth over the tile's range,
+// positions from shared-memory atomics on 16-bit packed counters), then runs
+// of equal key ordered by the full word (a run longer than one thread orders
+// sends the whole tile through a bitonic sort). The result is the
+// reference's (depth, scene index) order, as k_sort_small / k_sort_mid
+// produce it; it is left in sm.slot (the group stages word w[slot[k]] as the
+// k-th: the function returns true) unless the words had to be reordered
+// (the bitonic sort) or write_back asks for them (the frame keeps its sorted
+// pairs for inspection): then they are written back to w in order and the
+// function returns false. A copy that does not land within the bounded wait
+// sets the frame's error flag; the sort then reads the words from w. sync()
+// is the group's barrier, any(p) its vote, phase the mbarrier's parity.
 template <class Sm, class Sync, class Any>
 __device__ __forceinline__ bool group_sort_tile(uint64_t* w, uint32_t n, Sm& sm, uint32_t t, Sync&& sync, Any&& any,
-                                                bool write_back) {
+                                                bool write_back, uint32_t& phase, DevState* st) {
   constexpr uint32_t kThreads = 256;
   static_assert(kCountBuckets == 16 * kThreads, "16 counters per thread");
   const uint32_t lane = t & 31, warp = t >> 5;
-  uint32_t* hist = reinterpret_cast<uint32_t*>(sm.words);
+  uint32_t* hist = sm.srt.hist;
+  const uint32_t mbar = (uint32_t)__cvta_generic_to_shared(&sm.mbar);
+  const uint32_t off = (uint32_t)((reinterpret_cast<uintptr_t>(w) >> 3) & 1u);  // words below the 16-byte boundary
+  if (t == 0) {
+    const uint32_t bytes = ((n + off) * 8u + 15u) & ~15u;
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            (uint32_t)__cvta_generic_to_shared(sm.srt.words)),
+        "l"(w - off), "r"(bytes), "r"(mbar)
+        : "memory");
+  }
+  for (uint32_t b = t; b < kCountBuckets / 2; b += kThreads) hist[b] = 0u;
+  bool landed = umma::mbar_wait(mbar, phase);
+  if (!any(!landed)) {
+    landed = true;
+  } else {  // the whole group takes the same path: wait (bounded) for the copy, read w
+    if (t == 0) atomicExch(&st->error, 3u);
+    umma::mbar_wait(mbar, phase, 100000000ull);
+    landed = false;
+  }
+  phase ^= 1u;
+  const uint64_t* src = landed ? sm.srt.words + off : w;
   uint32_t mn = 0xFFFFFFFFu, mx = 0u;
   for (uint32_t e = t; e < n; e += kThreads) {
-    const uint32_t d = (uint32_t)(w[e] >> 32);
+    const uint32_t d = (uint32_t)(src[e] >> 32);
     mn = min(mn, d);
     mx = max(mx, d);
   }
-  for (uint32_t b = t; b < kCountBuckets / 2; b += kThreads) hist[b] = 0u;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
@@ -303,7 +336,7 @@ __device__ __forceinline__ bool group_sort_tile(uint64_t* w, uint32_t n, Sm& sm,
     return q >= (float)(kCountBuckets - 1) ? kCountBuckets - 1 : (uint32_t)q;
   };
   for (uint32_t e = t; e < n; e += kThreads) {
-    const uint32_t q = quant(w[e]);
+    const uint32_t q = quant(src[e]);
     atomicAdd(&hist[q >> 1], 1u << (16 * (q & 1u)));
   }
   sync();
@@ -344,18 +377,22 @@ __device__ __forceinline__ bool group_sort_tile(uint64_t* w, uint32_t n, Sm& sm,
   h4[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
   sync();
   for (uint32_t e = t; e < n; e += kThreads) {
-    const uint32_t q = quant(w[e]), sh = 16 * (q & 1u);
+    const uint32_t q = quant(src[e]), sh = 16 * (q & 1u);
     sm.slot[(atomicAdd(&hist[q >> 1], 1u << sh) >> sh) & 0xFFFFu] = (uint16_t)e;
   }
   sync();
   const bool long_run = sort_short_runs(
-      sm.slot, n, t, kThreads, [&](uint16_t i) { return quant(w[i]); }, [&](uint16_t i) { return w[i]; });
+      sm.slot, n, t, kThreads, [&](uint16_t i) { return quant(src[i]); }, [&](uint16_t i) { return src[i]; });
   const bool any_long = any(long_run);  // also the barrier after the runs
   if (!any_long && !write_back) return true;
-  for (uint32_t e = t; e < n; e += kThreads) sm.words[e] = w[sm.slot[e]];
-  sync();
-  if (any_long) bitonic_sort(sm.words, n, t, kThreads, sync);
-  for (uint32_t e = t; e < n; e += kThreads) w[e] = sm.words[e];
+  if (!landed) return true;  // degraded (the frame reports the error): long runs stay unordered
+  uint64_t* sw = sm.srt.words + off;
+  if (any_long) {
+    bitonic_sort(sw, n, t, kThreads, sync);
+    for (uint32_t e = t; e < n; e += kThreads) w[e] = sw[e];
+  } else {
+    for (uint32_t e = t; e < n; e += kThreads) w[e] = sw[sm.slot[e]];
+  }
   sync();  // the group's staging reads the sorted words next
   return false;
 }
@@ -399,6 +436,10 @@ __global__ void __launch_bounds__(NT, NT == 512 ? 2 : (NT == 256 ? 5 : 8)) k_ble
   // the order k_tile_ranges appended it.
   __shared__ uint32_t s_cls[kTileClasses];
   if (tid < kTileClasses) s_cls[tid] = st->cls[tid];
+  if constexpr (Smem::kSort) {
+    if (gt == 0) umma::mbar_init((uint32_t)__cvta_generic_to_shared(&sm.mbar), 1);
+  }
+  uint32_t sort_phase = 0;  // parity of the group's next bulk-copy completion
   __syncthreads();
   for (;;) {
     if (gt == 0) {
@@ -467,7 +508,7 @@ __global__ void __launch_bounds__(NT, NT == 512 ? 2 : (NT == 256 ? 5 : 8)) k_ble
       // ones were sorted by k_sort_long.
       use_slot = sm.cls >= 1 && sm.cls <= 5 && n >= 2 &&
                  group_sort_tile(pairs + begin, n, sm, (uint32_t)gt, sync, [&](bool p) { return count(p) != 0; },
-                                 (tv->fp.flags & kFrameKeepSortedPairs) != 0u);
+                                 (tv->fp.flags & kFrameKeepSortedPairs) != 0u, sort_phase, st);
     }
     // The k-th pair word of the tile in depth order.
     auto word_at = [&](uint32_t k) -> uint64_t { return pairs[begin + (use_slot ? (uint32_t)sm.slot[k] : k)]; };
@@ -672,7 +713,11 @@ __global__ void __launch_bounds__(NT, NT == 512 ? 2 : (NT == 256 ? 5 : 8)) k_ble
         }
       }
     }
-    sync();  // the group's shared memory is reused by its next tile
+    // The group's shared memory is reused by its next tile; a tile sort's bulk
+    // copy writes it through the async proxy, after the blend's generic
+    // accesses (each thread's ordered by its proxy fence, all by the barrier).
+    if constexpr (Smem::kSort) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    sync();
   }
 }
 

@@ -283,9 +283,12 @@ __device__ __forceinline__ uint64_t* chunked_lsd(uint64_t* src, uint64_t* dst, u
 // Sorts words[0, n) in place by the full word (depth bits, then splat
 // index: the reference's sort_hi32 + fix_ties order), scratch[0, n) as the
 // ping-pong range. The depth bytes that vary over the tile are sorted first;
-// if that leaves two equal depths next to each other, the tile is sorted
-// again over the varying bytes of the splat index and then of the depth
-// (LSD over the whole word), so ties never cost more than linear passes.
+// runs of equal depth that this leaves (a few equal floats among thousands
+// of depths are common) are then ordered by splat index by their first
+// thread when at most kMaxInsertRun long; if any run is longer, the tile is
+// sorted again over the varying bytes of the splat index and then of the
+// depth (LSD over the whole word), so ties never cost more than linear
+// passes.
 __device__ __forceinline__ void long_tile_sort(uint64_t* words, uint64_t* scratch, uint32_t n, ChunkSortSmem& sm) {
   const int tid = threadIdx.x;
   uint32_t ah = 0xFFFFFFFFu, oh = 0u, al = 0xFFFFFFFFu, ol = 0u;
@@ -306,9 +309,11 @@ __device__ __forceinline__ void long_tile_sort(uint64_t* words, uint64_t* scratc
     if ((vary_lo >> (8 * b)) & 255u) index_bytes |= 1u << b;
   }
   uint64_t* res = chunked_lsd(words, scratch, n, depth_bytes, sm);
-  bool tie = false;
-  for (uint32_t e = tid + 1; e < n; e += kTileThreads) tie |= (res[e] >> 32) == (res[e - 1] >> 32);
-  if (__syncthreads_or(tie)) res = chunked_lsd(res, res == words ? scratch : words, n, index_bytes | depth_bytes, sm);
+  const bool long_run = sort_short_runs(
+      res, n, (uint32_t)tid, kTileThreads, [](uint64_t x) { return (uint32_t)(x >> 32); },
+      [](uint64_t x) { return x; });
+  if (__syncthreads_or(long_run))
+    res = chunked_lsd(res, res == words ? scratch : words, n, index_bytes | depth_bytes, sm);
   if (res != words)
     for (uint32_t e = tid; e < n; e += kTileThreads) words[e] = res[e];
   __syncthreads();
