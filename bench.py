@@ -115,15 +115,16 @@ except Exception:
     h = pynvml.nvmlDeviceGetHandleByIndex(index)
 rows, stop = [], []
 signal.signal(signal.SIGTERM, lambda *a: stop.append(1))
+mx = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)  # a property of the part: read once
 print("ready", flush=True)
 while not stop:
     try:
-        rows.append((pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM),
-                     pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM),
+        rows.append((pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM), mx,
                      pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)))
     except Exception:
         pass
-    time.sleep(period)
+    if period > 0:
+        time.sleep(period)
 print(json.dumps(rows), flush=True)
 """
 
@@ -142,7 +143,7 @@ class Clocks:
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, index, period=0.001):
+    def __init__(self, index, period=0.0):
         self.index = index
         self.period = period
         self.rows = []  # (sm_mhz, max_mhz, reasons bitmask)

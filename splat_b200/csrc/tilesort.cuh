@@ -223,66 +223,56 @@ struct ChunkSortSmem {
   uint32_t key[kSortChunk];
 };
 
-// One stable LSD pass from src into dst over the 8-bit digit at `shift` of
-// a 32-bit key of each word (keyof), chunk by chunk through shared memory
-// with the digit starts carried across chunks. One CTA of kTileThreads
-// threads.
-template <class KeyOf>
-__device__ __forceinline__ void lsd_pass(const uint64_t* src, uint64_t* dst, uint32_t n, KeyOf&& keyof, int shift,
-                                         ChunkSortSmem& sm) {
-  constexpr int kChunks = kSortChunk / (32 * kTileWarps);
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  // Digit starts over the whole tile.
-  clear_counts(sm.t);
-  __syncthreads();
-  for (uint32_t e = tid; e < n; e += kTileThreads) atomicAdd(&sm.t.wh[warp][(keyof(src[e]) >> shift) & 255u], 1u);
-  __syncthreads();
-  digit_offsets(sm.t);
-  sm.run[tid] = sm.t.dstart[tid];
-  __syncthreads();
-  // Stable scatter, chunk by chunk in order.
-  for (uint32_t c0 = 0; c0 < n; c0 += kSortChunk) {
-    const uint32_t cn = min((uint32_t)kSortChunk, n - c0);
-    for (uint32_t e = tid; e < cn; e += kTileThreads) sm.key[e] = keyof(src[c0 + e]);
-    clear_counts(sm.t);
-    __syncthreads();
-    const uint32_t seg = (cn + kTileWarps - 1) / kTileWarps;
-    const uint32_t seg0 = min(cn, (uint32_t)warp * seg), seg1 = min(cn, seg0 + seg);
-    uint32_t k[kChunks], dr[kChunks];
-    warp_rank<kChunks>(sm.key, seg0, seg1, shift, sm.t, k, dr);
-    __syncthreads();
-    // Exclusive per-warp offsets per digit; the chunk's count per digit.
-    uint32_t running = 0;
-#pragma unroll
-    for (int w = 0; w < kTileWarps; w++) {
-      const uint32_t t = sm.t.wh[w][tid];
-      sm.t.wh[w][tid] = running;
-      running += t;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int c = 0; c < kChunks; c++) {
-      if (dr[c] != 0xFFFFFFFFu) {
-        const uint32_t dig = dr[c] & 255u;
-        dst[sm.run[dig] + sm.t.wh[warp][dig] + (dr[c] >> 8)] = src[c0 + seg0 + (uint32_t)c * 32 + lane];
-      }
-    }
-    __syncthreads();
-    sm.run[tid] += running;
-    __syncthreads();
-  }
-}
-
 // Stable LSD passes over the bytes of the 64-bit words whose bit is set in
 // `bytes` (bit b: byte b, least significant first; byte 4 is the low byte of
 // the depth bits), from src into dst and back. Returns the buffer holding
-// the result.
+// the result. One CTA of kTileThreads threads.
 __device__ __forceinline__ uint64_t* chunked_lsd(uint64_t* src, uint64_t* dst, uint32_t n, uint32_t bytes,
                                                  ChunkSortSmem& sm) {
+  constexpr int kChunks = kSortChunk / (32 * kTileWarps);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   for (int byte = 0; byte < 8; byte++) {
     if (!((bytes >> byte) & 1u)) continue;
-    const int half = byte >> 2;
-    lsd_pass(src, dst, n, [half](uint64_t w) { return (uint32_t)(w >> (32 * half)); }, 8 * (byte & 3), sm);
+    const int shift = 8 * byte, half = byte >> 2, dshift = 8 * (byte & 3);
+    // Digit starts over the whole tile.
+    clear_counts(sm.t);
+    __syncthreads();
+    for (uint32_t e = tid; e < n; e += kTileThreads) atomicAdd(&sm.t.wh[warp][(src[e] >> shift) & 255u], 1u);
+    __syncthreads();
+    digit_offsets(sm.t);
+    sm.run[tid] = sm.t.dstart[tid];
+    __syncthreads();
+    // Stable scatter, chunk by chunk in order.
+    for (uint32_t c0 = 0; c0 < n; c0 += kSortChunk) {
+      const uint32_t cn = min((uint32_t)kSortChunk, n - c0);
+      for (uint32_t e = tid; e < cn; e += kTileThreads) sm.key[e] = (uint32_t)(src[c0 + e] >> (32 * half));
+      clear_counts(sm.t);
+      __syncthreads();
+      const uint32_t seg = (cn + kTileWarps - 1) / kTileWarps;
+      const uint32_t seg0 = min(cn, (uint32_t)warp * seg), seg1 = min(cn, seg0 + seg);
+      uint32_t k[kChunks], dr[kChunks];
+      warp_rank<kChunks>(sm.key, seg0, seg1, dshift, sm.t, k, dr);
+      __syncthreads();
+      // Exclusive per-warp offsets per digit; the chunk's count per digit.
+      uint32_t running = 0;
+#pragma unroll
+      for (int w = 0; w < kTileWarps; w++) {
+        const uint32_t t = sm.t.wh[w][tid];
+        sm.t.wh[w][tid] = running;
+        running += t;
+      }
+      __syncthreads();
+#pragma unroll
+      for (int c = 0; c < kChunks; c++) {
+        if (dr[c] != 0xFFFFFFFFu) {
+          const uint32_t dig = dr[c] & 255u;
+          dst[sm.run[dig] + sm.t.wh[warp][dig] + (dr[c] >> 8)] = src[c0 + seg0 + (uint32_t)c * 32 + lane];
+        }
+      }
+      __syncthreads();
+      sm.run[tid] += running;
+      __syncthreads();
+    }
     uint64_t* t = src;
     src = dst;
     dst = t;
@@ -290,81 +280,40 @@ __device__ __forceinline__ uint64_t* chunked_lsd(uint64_t* src, uint64_t* dst, u
   return src;
 }
 
-// Min and max of x over the CTA.
-__device__ __forceinline__ void block_min_max(uint32_t mn, uint32_t mx, TileSortSmem& sm, uint32_t& mn_all,
-                                              uint32_t& mx_all) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-  for (int s = 16; s > 0; s >>= 1) {
-    mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, s));
-    mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, s));
-  }
-  if (lane == 0) {
-    sm.red[0][warp] = mn;
-    sm.red[1][warp] = mx;
-  }
-  __syncthreads();
-  mn_all = 0xFFFFFFFFu;
-  mx_all = 0u;
-#pragma unroll
-  for (int w = 0; w < kTileWarps; w++) {
-    mn_all = min(mn_all, sm.red[0][w]);
-    mx_all = max(mx_all, sm.red[1][w]);
-  }
-  __syncthreads();
-}
-
 // Sorts words[0, n) in place by the full word (depth bits, then splat
 // index: the reference's sort_hi32 + fix_ties order), scratch[0, n) as the
-// ping-pong range. Two stable LSD passes on the depth quantised to 16 bits
-// over the tile's range (DepthQuant: monotone, so the passes order the words
-// up to runs of equal key), then each run of equal key ordered by the full
-// word by its first thread when at most kMaxInsertRun long. If a run is
-// longer (depths crowded into one key: a plane seen head-on), the tile is
-// sorted again by LSD passes over the varying bytes of the splat index and
-// then of the depth bits, so neither case costs more than linear passes.
+// ping-pong range. The depth bytes that vary over the tile are sorted first;
+// runs of equal depth that this leaves (a few equal floats among thousands
+// of depths are common) are then ordered by splat index by their first
+// thread when at most kMaxInsertRun long; if any run is longer, the tile is
+// sorted again over the varying bytes of the splat index and then of the
+// depth (LSD over the whole word), so ties never cost more than linear
+// passes.
 __device__ __forceinline__ void long_tile_sort(uint64_t* words, uint64_t* scratch, uint32_t n, ChunkSortSmem& sm) {
   const int tid = threadIdx.x;
-  uint32_t mn = 0xFFFFFFFFu, mx = 0u;
+  uint32_t ah = 0xFFFFFFFFu, oh = 0u, al = 0xFFFFFFFFu, ol = 0u;
   for (uint32_t e = tid; e < n; e += kTileThreads) {
-    const uint32_t d = (uint32_t)(words[e] >> 32);
-    mn = min(mn, d);
-    mx = max(mx, d);
+    const uint64_t w = words[e];
+    ah &= (uint32_t)(w >> 32);
+    oh |= (uint32_t)(w >> 32);
+    al &= (uint32_t)w;
+    ol |= (uint32_t)w;
   }
-  block_min_max(mn, mx, sm.t, mn, mx);
-  const DepthQuant quant = make_quant(mn, mx);
-  uint64_t* res = words;
-  uint64_t* other = scratch;
-  if (mx != mn) {
-    for (int b = 0; b < 2; b++) {
-      lsd_pass(res, other, n, quant, 8 * b, sm);
-      uint64_t* t = res;
-      res = other;
-      other = t;
-    }
+  uint32_t and_hi, or_hi, and_lo, or_lo;
+  block_and_or(ah, oh, sm.t, and_hi, or_hi);
+  block_and_or(al, ol, sm.t, and_lo, or_lo);
+  const uint32_t vary_hi = and_hi ^ or_hi, vary_lo = and_lo ^ or_lo;
+  uint32_t depth_bytes = 0, index_bytes = 0;
+  for (int b = 0; b < 4; b++) {
+    if ((vary_hi >> (8 * b)) & 255u) depth_bytes |= 1u << (4 + b);
+    if ((vary_lo >> (8 * b)) & 255u) index_bytes |= 1u << b;
   }
-  const bool long_run =
-      sort_short_runs(res, n, (uint32_t)tid, kTileThreads, quant, [](uint64_t x) { return x; });
-  if (__syncthreads_or(long_run)) {
-    uint32_t ah = 0xFFFFFFFFu, oh = 0u, al = 0xFFFFFFFFu, ol = 0u;
-    for (uint32_t e = tid; e < n; e += kTileThreads) {
-      const uint64_t w = res[e];
-      ah &= (uint32_t)(w >> 32);
-      oh |= (uint32_t)(w >> 32);
-      al &= (uint32_t)w;
-      ol |= (uint32_t)w;
-    }
-    uint32_t and_hi, or_hi, and_lo, or_lo;
-    block_and_or(ah, oh, sm.t, and_hi, or_hi);
-    block_and_or(al, ol, sm.t, and_lo, or_lo);
-    const uint32_t vary_hi = and_hi ^ or_hi, vary_lo = and_lo ^ or_lo;
-    uint32_t bytes = 0;
-    for (int b = 0; b < 4; b++) {
-      if ((vary_hi >> (8 * b)) & 255u) bytes |= 1u << (4 + b);
-      if ((vary_lo >> (8 * b)) & 255u) bytes |= 1u << b;
-    }
-    res = chunked_lsd(res, other, n, bytes, sm);
-  }
+  uint64_t* res = chunked_lsd(words, scratch, n, depth_bytes, sm);
+  const bool long_run = sort_short_runs(
+      res, n, (uint32_t)tid, kTileThreads, [](uint64_t x) { return (uint32_t)(x >> 32); },
+      [](uint64_t x) { return x; });
+  if (__syncthreads_or(long_run))
+    res = chunked_lsd(res, res == words ? scratch : words, n, index_bytes | depth_bytes, sm);
   if (res != words)
     for (uint32_t e = tid; e < n; e += kTileThreads) words[e] = res[e];
   __syncthreads();
