@@ -432,7 +432,7 @@ __global__ void __launch_bounds__(NT, NT == 512 ? 2 : (NT == 256 ? 5 : 8)) k_ble
   const uint32_t wxbits = 0xFFu << (wbx * 8);
   const uint32_t wybits = ((1u << S::BH) - 1u) << (wby * S::BH);
 
-  // Tiles are taken heaviest class first (tile_class), each class's list in
+  // Tiles are taken by pair-count class (tile_class), each class's list in
   // the order k_tile_ranges appended it.
   __shared__ uint32_t s_cls[kTileClasses];
   if (tid < kTileClasses) s_cls[tid] = st->cls[tid];
@@ -445,7 +445,12 @@ __global__ void __launch_bounds__(NT, NT == 512 ? 2 : (NT == 256 ? 5 : 8)) k_ble
     if (gt == 0) {
       uint32_t w = atomicAdd(&st->blend_next, 1u), tl = 0xFFFFFFFFu, cl = kTileClasses;
 #pragma unroll
-      for (int k = 0; k < kTileClasses; k++) {
+      for (int i = 0; i < kTileClasses; i++) {
+        // Frames in mapped host memory (ROWS) take the empty and the lightest
+        // tiles first: their rows then cross the bus while the heavy tiles
+        // compute, instead of in one burst at the end of the frame (classes
+        // 6, 5, 0, 1, 2, 3, 4); device frames take the heaviest first.
+        const int k = ROWS ? (i < 2 ? kTileClasses - 1 - i : i - 2) : i;
         if (w < s_cls[k]) {
           tl = order[(size_t)k * n_tiles + w];
           cl = (uint32_t)k;
