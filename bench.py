@@ -143,7 +143,7 @@ class Clocks:
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, index, period=0.0):
+    def __init__(self, index, period=0.0002):
         self.index = index
         self.period = period
         self.rows = []  # (sm_mhz, max_mhz, reasons bitmask)
