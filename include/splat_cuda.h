@@ -192,6 +192,48 @@ int splat_cuda_render_rows(splat_cuda_handle* h, const splat_view_desc* view, ui
                            const float bg[3], uint32_t row0, uint32_t rows, uint8_t* rgb_out, size_t out_bytes,
                            splat_render_stats* stats);
 
+/*
+ * One frame over several devices that each hold a SHARD of the splats (a
+ * contiguous run of the scene, shards in scene order), with one exchange of
+ * projected splats: tile ownership by row windows. No counterpart in the
+ * reference, whose backends render whole frames from the whole scene
+ * (Renderer::render, src/render/mod.rs:89-96).
+ *
+ * 1. Each device projects its shard (handle h, created from the shard's
+ *    splats) for the whole width x height frame with
+ *    splat_cuda_shard_records. Windows k = 0 .. n_windows - 1 are the pixel
+ *    rows [row_bounds[k], row_bounds[k + 1]) (bounds nondecreasing, at most
+ *    height; n_windows at most 64). Every visible splat whose pixel bbox
+ *    meets a window's rows goes to that window as one record of
+ *    SPLAT_RECORD_BYTES bytes; the records are written to DEVICE memory
+ *    `send` (16-byte aligned) window after window, each window's records in
+ *    scene order, and counts[k] receives window k's count. If the records
+ *    do not fit send_capacity (records), nothing is written, counts are
+ *    filled in and the call returns SPLAT_ERR_CAPACITY (size the buffer from
+ *    them and call again). *visible (may be NULL) receives the shard's
+ *    visible splats. Blocks until the records are written.
+ * 2. The records of window k are exchanged (an all-to-all: sender r's k-th
+ *    run to the owner of window k) and concatenated in shard order.
+ * 3. The owner draws its window with splat_cuda_render_records: `records`
+ *    holds n_records of them (DEVICE memory on h's device, 16-byte aligned,
+ *    in shard order as received; at most 2^32 - 1); rows [row0, row0 +
+ *    rows) of the frame go to `out`, host memory or device memory of h's
+ *    device (rows * width * 3 bytes). The window equals those rows of
+ *    splat_cuda_render of the whole scene, bit for bit, when row0 and rows
+ *    are those of a window given to every sender. h may be any handle on
+ *    the device (its own scene is not read). Stats: `visible` counts the
+ *    records, `overlaps` the window's (splat, tile) pairs. Pair buffers grow
+ *    and frames past the pair limit are drawn in windows of tiles, as in
+ *    splat_cuda_render. Blocks until the rows are in `out`.
+ */
+#define SPLAT_RECORD_BYTES 48u
+int splat_cuda_shard_records(splat_cuda_handle* h, const splat_view_desc* view, uint32_t width, uint32_t height,
+                             uint32_t n_windows, const uint32_t* row_bounds, void* send, uint64_t send_capacity,
+                             uint64_t* counts, uint64_t* visible);
+int splat_cuda_render_records(splat_cuda_handle* h, const splat_view_desc* view, uint32_t width, uint32_t height,
+                              const float bg[3], const void* records, uint64_t n_records, uint32_t row0,
+                              uint32_t rows, uint8_t* out, size_t out_bytes, splat_render_stats* stats);
+
 /* As splat_cuda_render, but the frame goes to DEVICE memory dev_out (on the
  * handle's device) and the call only enqueues work on the handle's stream: it
  * does not wait for the GPU. Call splat_cuda_finish before using the stats;

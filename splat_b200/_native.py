@@ -38,6 +38,8 @@ SPLAT_FAULT_LOST_WAIT = 2
 SPLAT_OPT_COUNT_EVALS = 11
 SPLAT_OPT_BLEND_EVALS = 12
 
+SPLAT_RECORD_BYTES = 48
+
 SPLAT_CELLS_TRUECOLOR = 0
 SPLAT_CELLS_ANSI256 = 1
 
@@ -47,6 +49,7 @@ _STATUS_NAMES = {0: "OK", 1: "INVALID_ARG", 2: "OOM", 3: "CAPACITY", 4: "DEVICE"
 EXPORTS = [
     "splat_cuda_abi_version", "splat_cuda_backend_name", "splat_cuda_create", "splat_cuda_create_error",
     "splat_cuda_render", "splat_cuda_render_rows", "splat_cuda_render_device", "splat_cuda_finish",
+    "splat_cuda_shard_records", "splat_cuda_render_records",
     "splat_cuda_set_stream",
     "splat_cuda_get_stream", "splat_cuda_set_option", "splat_cuda_get_option", "splat_cuda_debug_dump",
     "splat_cuda_destroy", "splat_cuda_last_error", "splat_cuda_sort_tile_noalloc",
@@ -144,6 +147,10 @@ def lib():
                                              ctypes.c_size_t, ctypes.POINTER(RenderStatsC)]
         L.splat_cuda_render_device.argtypes = [vp, ctypes.POINTER(ViewDesc), u32, u32, f32p, u32, vp,
                                                ctypes.c_size_t]
+        L.splat_cuda_shard_records.argtypes = [vp, ctypes.POINTER(ViewDesc), u32, u32, u32, ctypes.POINTER(u32),
+                                               vp, u64, ctypes.POINTER(u64), ctypes.POINTER(u64)]
+        L.splat_cuda_render_records.argtypes = [vp, ctypes.POINTER(ViewDesc), u32, u32, f32p, vp, u64, u32, u32,
+                                                vp, ctypes.c_size_t, ctypes.POINTER(RenderStatsC)]
         L.splat_cuda_finish.argtypes = [vp, ctypes.POINTER(RenderStatsC), ctypes.POINTER(ctypes.c_int)]
         L.splat_cuda_set_stream.argtypes = [vp, vp]
         L.splat_cuda_get_stream.argtypes = [vp]

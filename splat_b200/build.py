@@ -33,6 +33,7 @@ SOURCES = {
     "mlp.cu": [],
     "decode.cu": ["--fmad=false"],
     "term.cu": [],
+    "shard.cu": [],
 }
 HEADERS = [os.path.join(CSRC, "common.cuh"), os.path.join(CSRC, "tilesort.cuh"), os.path.join(CSRC, "handle.h"),
            os.path.join(CSRC, "umma.cuh"), os.path.join(CSRC, "mlp.cuh"), os.path.join(CSRC, "sh.cuh"),

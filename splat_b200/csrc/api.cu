@@ -155,6 +155,15 @@ int ensure_size(splat_cuda_handle* h, uint64_t tiles, uint32_t rows, size_t out_
   return SPLAT_OK;
 }
 
+bool is_device_memory(const void* p, int device) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice && a.device == device;
+}
+
 bool is_pinned_host(const void* p) {
   cudaPointerAttributes a{};
   if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
@@ -315,7 +324,9 @@ void set_tile_shape(FrameParams& p, uint32_t tile_w, uint32_t tile_h) {
 namespace {
 
 // Enqueues one frame into dev_out (no host synchronisation); host_mapped:
-// dev_out is the device address of mapped pinned host memory.
+// dev_out is the device address of mapped pinned host memory. While
+// h->rx is set (splat_cuda_render_records) the frame draws the h->rx_n
+// records at h->rx_rec: their binning input replaces the projection.
 int enqueue_frame(splat_cuda_handle* h, const FrameParams& fp_in, uint8_t* dev_out, bool host_mapped = false) {
   FrameParams fp = fp_in;
   set_tile_shape(fp, h->blend.tile_w, h->blend.tile_h);
@@ -324,7 +335,8 @@ int enqueue_frame(splat_cuda_handle* h, const FrameParams& fp_in, uint8_t* dev_o
   const uint32_t f = fp.downsample;
   const bool scratch = f > 1 && (fp.tile_w % f != 0 || fp.tile_h % f != 0);
   const size_t full_bytes = scratch ? (size_t)fp.w * fp.h * 3 : 0;
-  const uint32_t rows = bin_rows(h->n, h->num_sms);
+  const bool records = h->rx;
+  const uint32_t rows = bin_rows(records ? h->rx_n : h->n, h->num_sms);
   int rc = ensure_size(h, tiles, rows, 0, full_bytes);
   if (rc) return rc;
   const uint32_t chunks = (uint32_t)((tiles + kScanChunk - 1) / kScanChunk);
@@ -342,10 +354,19 @@ int enqueue_frame(splat_cuda_handle* h, const FrameParams& fp_in, uint8_t* dev_o
   t.out = dev_out;
   t.full = scratch ? h->full_dev : nullptr;
   t.rows = rows;
+  if (records) {
+    t.s.n = h->rx_n;
+    t.s.order = nullptr;  // the records' order is the scene order
+    t.rec = const_cast<Record*>(h->rx_rec);
+    t.bin = h->rx_bin;
+  }
   if (h->stage_events) CK(cudaEventRecord(h->ev[0], s), "event");
-  CK(launch_project(t, h->table, h->debug_capture ? h->dbg_proj : nullptr, h->debug_capture ? h->dbg_color : nullptr,
-                    fc, s, &h->launches),
-     "project kernel");
+  if (records)
+    CK(launch_records_bin(t, h->table, fc, s, &h->launches), "records kernel");
+  else
+    CK(launch_project(t, h->table, h->debug_capture ? h->dbg_proj : nullptr,
+                      h->debug_capture ? h->dbg_color : nullptr, fc, s, &h->launches),
+       "project kernel");
   if (h->stage_events) CK(cudaEventRecord(h->ev[1], s), "event");
   BinLaunch bl{};
   bl.n_views = 1;
@@ -713,12 +734,31 @@ SPLAT_API int splat_cuda_finish(splat_cuda_handle* h, splat_render_stats* stats,
 
 namespace {
 
-// A frame (or a window of rows) into caller-owned host memory: bytes =
-// out_w * out_h * 3 of fp.
+// A frame (or a window of rows) into caller-owned host memory (or, with
+// device_ok, device memory of the handle's device, written in place): bytes
+// = out_w * out_h * 3 of fp.
 int render_to_host(splat_cuda_handle* h, const FrameParams& fp, uint8_t* rgb_out, splat_render_stats* stats,
-                   std::chrono::steady_clock::time_point t0) {
+                   std::chrono::steady_clock::time_point t0, bool device_ok = false) {
   int rc = SPLAT_OK;
   const size_t bytes = (size_t)fp.out_w * fp.out_h * 3;
+  if (bytes && device_ok && is_device_memory(rgb_out, h->device)) {
+    for (int attempt = 0; attempt < 8; attempt++) {
+      if ((rc = enqueue_frame(h, fp, rgb_out))) return rc;
+      int regrown = 0;
+      if ((rc = finish_frame(h, stats, &regrown))) return rc;
+      if (regrown == 2) {
+        if ((rc = render_windows(h, fp, rgb_out, false, stats))) return rc;
+        CK(cudaStreamSynchronize(h->stream), "frame");
+        regrown = 0;
+      }
+      if (!regrown) {
+        if (stats)
+          stats->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        return SPLAT_OK;
+      }
+    }
+    return fail(h, SPLAT_ERR_CAPACITY, "pair buffers kept overflowing");
+  }
   if ((rc = ensure_size(h, 0, 0, bytes, 0))) return rc;
   // Pinned output the device can address: the blend (or the downsample)
   // writes the frame straight into it, overlapped with the frame's own
@@ -793,6 +833,121 @@ SPLAT_API int splat_cuda_render_rows(splat_cuda_handle* h, const splat_view_desc
   fp.out_y0 = row0;
   fp.out_h = rows;
   return render_to_host(h, fp, rgb_out, stats, t0);
+}
+
+SPLAT_API int splat_cuda_shard_records(splat_cuda_handle* h, const splat_view_desc* view, uint32_t width,
+                                       uint32_t height, uint32_t n_windows, const uint32_t* row_bounds, void* send,
+                                       uint64_t send_capacity, uint64_t* counts, uint64_t* visible) {
+  if (visible) *visible = 0;
+  const float bg[3] = {0.0f, 0.0f, 0.0f};
+  int rc = check_view_args(h, view, width, height, bg);
+  if (rc) return rc;
+  if (n_windows == 0 || n_windows > kMaxShardWindows || !row_bounds || !counts)
+    return fail(h, SPLAT_ERR_INVALID_ARG, "1 to 64 row windows, their n + 1 bounds and a counts array of n");
+  ShardWindows w{};
+  w.n = n_windows;
+  for (uint32_t k = 0; k <= n_windows; k++) {
+    if (row_bounds[k] > height || (k && row_bounds[k] < row_bounds[k - 1]))
+      return fail(h, SPLAT_ERR_INVALID_ARG, "row window bounds must be nondecreasing and at most the frame height");
+    w.bound[k] = row_bounds[k];
+  }
+  if (send_capacity && (!send || (reinterpret_cast<uintptr_t>(send) & 15u)))
+    return fail(h, SPLAT_ERR_INVALID_ARG, "the send buffer must be 16-byte aligned device memory");
+  for (uint32_t k = 0; k < n_windows; k++) counts[k] = 0;
+  if (width == 0 || height == 0 || h->n == 0) return SPLAT_OK;
+  CK(cudaSetDevice(h->device), "cudaSetDevice");
+  const size_t scratch = shard_scratch_bytes(h->n, n_windows);
+  if (scratch > h->shard_scratch_cap) {
+    dfree(h->shard_scratch);
+    h->shard_scratch_cap = 0;
+    CK(dmalloc(h, reinterpret_cast<uint8_t**>(&h->shard_scratch), scratch), "cudaMalloc record selection");
+    h->shard_scratch_cap = scratch;
+  }
+  const size_t totals_bytes = kMaxShardWindows * sizeof(unsigned long long);
+  if (!h->shard_totals) CK(dmalloc(h, &h->shard_totals, totals_bytes), "cudaMalloc record totals");
+  if (!h->shard_totals_host) CK(cudaMallocHost(&h->shard_totals_host, totals_bytes), "cudaMallocHost record totals");
+  if ((rc = ensure_size(h, 0, 0, 0, 0))) return rc;  // the frame counters
+  FrameParams fp = make_params(*view, width, height, bg, 1);
+  set_tile_shape(fp, h->blend.tile_w, h->blend.tile_h);
+  cudaStream_t s = h->stream;
+  CK(cudaMemsetAsync(h->st, 0, frame_counters_bytes(1, 0), s), "clear frame state");
+  const FrameCounters fc = frame_counters_at(h->st, 1);
+  ViewTask t{};
+  t.fp = fp;
+  t.s = scene_dev(h);
+  t.s.lost_wait_us = h->inject_lost_us;
+  h->inject_lost_us = 0;
+  t.rec = h->rec;
+  t.bin = h->bin;
+  CK(launch_project(t, h->table, nullptr, nullptr, fc, s, &h->launches), "project kernel");
+  CK(launch_shard_count(h->rec, h->bin, h->n, w, h->shard_scratch, h->shard_totals, s, &h->launches),
+     "record selection kernels");
+  CK(cudaMemcpyAsync(h->shard_totals_host, h->shard_totals, n_windows * sizeof(unsigned long long),
+                     cudaMemcpyDeviceToHost, s),
+     "copy record totals");
+  CK(cudaMemcpyAsync(h->st_host, h->st, sizeof(DevState), cudaMemcpyDeviceToHost, s), "copy frame state");
+  CK(cudaStreamSynchronize(s), "record selection");
+  if (h->st_host->error) {
+    const unsigned code = h->st_host->error;
+    cudaMemsetAsync(h->st, 0, sizeof(DevState), s);
+    return fail(h, SPLAT_ERR_TIMEOUT,
+                code == 2u ? "the projection's bulk copies did not complete in time"
+                           : "a tensor-core wait in the learned-colour projection gave up");
+  }
+  uint64_t total = 0;
+  for (uint32_t k = 0; k < n_windows; k++) total += (counts[k] = h->shard_totals_host[k]);
+  if (visible) *visible = h->st_host->visible;
+  if (total > send_capacity)
+    return fail(h, SPLAT_ERR_CAPACITY,
+                "the send buffer holds " + std::to_string(send_capacity) + " records, the windows take " +
+                    std::to_string(total) + " (counts are filled in)");
+  if (total) {
+    CK(launch_shard_scatter(h->rec, h->bin, h->n, w, h->shard_scratch, static_cast<Record*>(send), send_capacity, s,
+                            &h->launches),
+       "record scatter kernel");
+    CK(cudaStreamSynchronize(s), "record scatter");
+  }
+  return SPLAT_OK;
+}
+
+SPLAT_API int splat_cuda_render_records(splat_cuda_handle* h, const splat_view_desc* view, uint32_t width,
+                                        uint32_t height, const float bg[3], const void* records, uint64_t n_records,
+                                        uint32_t row0, uint32_t rows, uint8_t* out, size_t out_bytes,
+                                        splat_render_stats* stats) {
+  const auto t0 = std::chrono::steady_clock::now();
+  if (stats) std::memset(stats, 0, sizeof(*stats));
+  int rc = check_view_args(h, view, width, height, bg);
+  if (rc) return rc;
+  if ((uint64_t)row0 + rows > height)
+    return fail(h, SPLAT_ERR_INVALID_ARG, "rows [row0, row0 + rows) exceed the frame height");
+  const size_t need = (size_t)width * rows * 3;
+  if (need && (!out || out_bytes < need))
+    return fail(h, SPLAT_ERR_INVALID_ARG, "output buffer smaller than width*rows*3 bytes");
+  if (n_records && (!records || (reinterpret_cast<uintptr_t>(records) & 15u)))
+    return fail(h, SPLAT_ERR_INVALID_ARG, "the records must be 16-byte aligned device memory");
+  if (n_records > 0xFFFFFFFFull) return fail(h, SPLAT_ERR_INVALID_ARG, "more than 2^32 - 1 records");
+  if (need == 0) return SPLAT_OK;
+  CK(cudaSetDevice(h->device), "cudaSetDevice");
+  const uint64_t slots = std::max<uint64_t>(n_records, 1);
+  if (slots > h->rx_bin_cap) {
+    dfree(h->rx_bin);
+    h->rx_bin_cap = 0;
+    CK(dmalloc(h, &h->rx_bin, slots * sizeof(BinInfo)), "cudaMalloc record binning input");
+    h->rx_bin_cap = slots;
+  }
+  FrameParams fp = make_params(*view, width, height, bg, 1);
+  fp.win_y0 = row0;
+  fp.win_rows = rows;
+  fp.out_y0 = row0;
+  fp.out_h = rows;
+  h->rx = true;
+  h->rx_rec = static_cast<const Record*>(records);
+  h->rx_n = n_records;
+  rc = render_to_host(h, fp, out, stats, t0, true);
+  h->rx = false;
+  h->rx_rec = nullptr;
+  h->rx_n = 0;
+  return rc;
 }
 
 SPLAT_API int splat_cuda_render_cells(splat_cuda_handle* h, const splat_view_desc* view, uint32_t width,
@@ -1071,6 +1226,10 @@ SPLAT_API int splat_cuda_destroy(splat_cuda_handle* h) {
   dfree(h->cells_dev);
   dfree(h->rec);
   dfree(h->bin);
+  dfree(h->rx_bin);
+  dfree(h->shard_scratch);
+  dfree(h->shard_totals);
+  if (h->shard_totals_host) cudaFreeHost(h->shard_totals_host);
   free_pairs(h);
   dfree(h->ranges);
   dfree(h->counts);

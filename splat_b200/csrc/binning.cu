@@ -46,7 +46,7 @@ constexpr int kBinThreads = 512;
 // lanes on the same tile can share one bucket atomic; larger splats are
 // expanded by the whole warp (distinct tiles, all lanes active, `active`
 // passed as a compile-time true through fw).
-constexpr uint32_t kNoTile = 0xFFFFFFFFu;
+[[maybe_unused]] constexpr uint32_t kNoTile = 0xFFFFFFFFu;
 // false: each lane expands its own splat's pairs at its own pace, one bucket
 // atomic per pair (fw), as for the larger splats.
 constexpr bool kAggregateBuckets = false;

@@ -106,6 +106,30 @@ struct __align__(16) BinInfo {
   uint32_t rect_lo, rect_hi, depth_bits, count;
 };
 
+// The tile rectangle of a splat whose pixel bbox (pixel_bbox,
+// src/render/cpu.rs:96-102) is [bx0, x1) x [by0, y1): its tile rows and
+// columns clipped to the frame's rendered window and counted from the
+// window's first tile row and column (the whole frame: unchanged). A bbox
+// that holds no pixel of the window gives the empty rectangle (no pairs).
+__device__ __forceinline__ void window_rect(const FrameParams& fp, uint32_t bx0, uint32_t x1, uint32_t by0,
+                                            uint32_t y1, BinInfo& b) {
+  const uint32_t wty0 = max(by0 >> fp.tile_sy, fp.win_ty0);
+  const uint32_t wty1 = min((y1 + fp.tile_h - 1) >> fp.tile_sy, fp.win_ty0 + fp.tiles_y);
+  const uint32_t wtx0 = max(bx0 >> fp.tile_sx, fp.win_tx0);
+  const uint32_t wtx1 = min((x1 + fp.tile_w - 1) >> fp.tile_sx, fp.win_tx0 + fp.tiles_x);
+  if (bx0 < x1 && by0 < y1 && wty0 < wty1 && wtx0 < wtx1) {
+    const uint32_t tx0 = wtx0 - fp.win_tx0, ty0 = wty0 - fp.win_ty0;
+    const uint32_t tx1 = wtx1 - fp.win_tx0, ty1 = wty1 - fp.win_ty0;
+    b.rect_lo = tx0 | (ty0 << 16);
+    b.rect_hi = tx1 | (ty1 << 16);
+    b.count = (tx1 - tx0) * (ty1 - ty0);
+  } else {
+    b.rect_lo = 0u;  // visible, but its bbox holds no pixel of the window: no pairs
+    b.rect_hi = 0u;
+    b.count = 0u;
+  }
+}
+
 // Per-tile depth sort sizes: tiles up to kWarpSortCap pairs are sorted by one
 // warp, up to kMidSortCap by one CTA in shared memory, longer ones in chunks.
 constexpr uint32_t kWarpSortCap = 512;
@@ -249,6 +273,33 @@ cudaError_t launch_blend(const ViewTask* table, uint32_t n_views, uint32_t n_til
                          const uint2* ranges, const uint32_t* order, bool exact, const BlendConfig& cfg, DevState* st,
                          int num_sms, cudaStream_t stream, uint32_t* launches, bool host_rows = false,
                          bool count = false);
+// Splat-sharded frames (shard.cu). Row windows of a frame, [bound[k],
+// bound[k + 1]) for k < n, at most kMaxShardWindows of them.
+constexpr uint32_t kMaxShardWindows = 64;
+struct ShardWindows {
+  uint32_t n;
+  uint32_t bound[kMaxShardWindows + 1];
+};
+// Device scratch of the record selection of n splats over w.n windows.
+size_t shard_scratch_bytes(uint64_t n, uint32_t windows);
+// The sender side: counts, for every window, the projected splats (rec and
+// bin of a whole-frame projection of n splats) whose pixel bbox meets its
+// rows, into totals[0 .. w.n) (device memory), keeping in `scratch` the
+// offsets the scatter uses.
+cudaError_t launch_shard_count(const Record* rec, const BinInfo* bin, uint64_t n, const ShardWindows& w,
+                               void* scratch, unsigned long long* totals, cudaStream_t stream, uint32_t* launches);
+// ... then writes each such splat's record to every window its rows meet:
+// window k's records from send + (totals of the windows before k) on, in
+// scene order; positions at or past cap are not written.
+cudaError_t launch_shard_scatter(const Record* rec, const BinInfo* bin, uint64_t n, const ShardWindows& w,
+                                 const void* scratch, Record* send, uint64_t cap, cudaStream_t stream,
+                                 uint32_t* launches);
+// The receiver side: the binning input of t.s.n records (t.rec, received in
+// scene order) for the view's window, in place of the projection; CTA 0
+// also stores t as table[0].
+cudaError_t launch_records_bin(const ViewTask& t, ViewTask* table, const FrameCounters& fc, cudaStream_t stream,
+                               uint32_t* launches);
+
 // Half-block terminal cells (SPLAT_CELLS_*) of a frame of width w.
 cudaError_t launch_cells(const uint8_t* frame, uint32_t w, uint32_t cols, uint32_t rows, uint32_t mode, uint8_t* cells,
                          cudaStream_t stream, uint32_t* launches);

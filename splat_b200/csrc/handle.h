@@ -31,6 +31,18 @@ struct splat_cuda_handle {
   // per-splat frame buffers
   splat::Record* rec = nullptr;
   splat::BinInfo* bin = nullptr;
+  // splat-sharded frames: the records a splat_cuda_render_records call draws
+  // (caller-owned device memory, set for the duration of the call) and their
+  // binning input; the record selection's scratch and host copy of its totals
+  bool rx = false;
+  const splat::Record* rx_rec = nullptr;
+  uint64_t rx_n = 0;
+  splat::BinInfo* rx_bin = nullptr;
+  uint64_t rx_bin_cap = 0;
+  void* shard_scratch = nullptr;
+  size_t shard_scratch_cap = 0;
+  unsigned long long* shard_totals = nullptr;       // device, kMaxShardWindows
+  unsigned long long* shard_totals_host = nullptr;  // pinned, kMaxShardWindows
   // pair buffers: per-tile buckets and the long-tile sort's scratch
   uint64_t cap = 0;
   uint64_t pair_limit = splat::kMaxPairs;  // largest capacity; beyond it frames are drawn in windows

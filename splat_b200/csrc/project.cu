@@ -255,23 +255,7 @@ __device__ __forceinline__ void project_splat(const FrameParams& fp, const Scene
       r.r2 = make_float4(col[2], __uint_as_float(bx0 | (x1 << 16)), __uint_as_float(by0 | (y1 << 16)), tz);
       rec[i] = r;
       b.depth_bits = __float_as_uint(tz);
-      // Tile rows and columns clipped to the rendered window and counted
-      // from its first tile row and column (the whole frame: unchanged).
-      const uint32_t wty0 = max(by0 >> fp.tile_sy, fp.win_ty0);
-      const uint32_t wty1 = min((y1 + fp.tile_h - 1) >> fp.tile_sy, fp.win_ty0 + fp.tiles_y);
-      const uint32_t wtx0 = max(bx0 >> fp.tile_sx, fp.win_tx0);
-      const uint32_t wtx1 = min((x1 + fp.tile_w - 1) >> fp.tile_sx, fp.win_tx0 + fp.tiles_x);
-      if (bx0 < x1 && by0 < y1 && wty0 < wty1 && wtx0 < wtx1) {
-        const uint32_t tx0 = wtx0 - fp.win_tx0, ty0 = wty0 - fp.win_ty0;
-        const uint32_t tx1 = wtx1 - fp.win_tx0, ty1 = wty1 - fp.win_ty0;
-        b.rect_lo = tx0 | (ty0 << 16);
-        b.rect_hi = tx1 | (ty1 << 16);
-        b.count = (tx1 - tx0) * (ty1 - ty0);
-      } else {
-        b.rect_lo = 0u;  // visible, but its bbox holds no pixel: no pairs
-        b.rect_hi = 0u;
-        b.count = 0u;
-      }
+      window_rect(fp, bx0, x1, by0, y1, b);
       vis = true;
       out_x = x;
       out_y = y;

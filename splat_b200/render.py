@@ -200,6 +200,79 @@ class CudaRenderer(Renderer):
         N.check(rc, self._h, "render_rows")
         return (out, RenderStats.from_c(st)) if stats else out
 
+    # --- splat-sharded frames ---------------------------------------------------
+    def shard_records(self, view: View, width: int, height: int, row_bounds, send=None):
+        """The record exchange's sender side (splat_cuda_shard_records): this
+        renderer's scene is one shard of the splats; its splats are projected
+        for the whole frame and each visible one goes, as a
+        SPLAT_RECORD_BYTES-byte record, to every row window [row_bounds[k],
+        row_bounds[k + 1]) its pixel bbox meets. Returns (records, counts,
+        visible): a uint8 CUDA tensor of sum(counts) records, window after
+        window, each window's in scene order (`send`, a uint8 CUDA tensor, is
+        used when large enough), the records per window and the shard's
+        visible splats."""
+        import torch
+
+        _pixel_count(width, height)
+        bounds = np.ascontiguousarray(row_bounds, np.uint32)
+        nw = len(bounds) - 1
+        counts = np.zeros(max(nw, 1), np.uint64)
+        vis = ctypes.c_uint64(0)
+        rb = N.SPLAT_RECORD_BYTES
+        if send is None:
+            send = torch.empty(max(self.n, 1) * rb + 16, dtype=torch.uint8, device=f"cuda:{self.device}")
+        for _ in range(2):
+            base = send.data_ptr()
+            off = (-base) % 16  # the records start 16-byte aligned
+            cap = max(send.numel() - off, 0) // rb
+            rc = N.lib().splat_cuda_shard_records(
+                self._h, ctypes.byref(_view_desc(view)), width, height, nw,
+                bounds.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)), base + off if cap else None, cap,
+                counts.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), ctypes.byref(vis))
+            if rc == N.SPLAT_ERR_CAPACITY:
+                send = torch.empty(int(counts[:nw].sum()) * rb + 16, dtype=torch.uint8, device=send.device)
+                continue
+            N.check(rc, self._h, "shard_records")
+            total = int(counts[:nw].sum())
+            return send[off:off + total * rb], [int(c) for c in counts[:nw]], int(vis.value)
+        raise N.SplatError(N.SPLAT_ERR_CAPACITY, "shard_records: the send buffer did not grow")
+
+    def render_records(self, view: View, width: int, height: int, background, records, row0: int, rows: int,
+                       out=None, stats: bool = False):
+        """Rows [row0, row0 + rows) of the frame drawn from received records
+        (splat_cuda_render_records): `records` is a uint8 CUDA tensor of
+        whole records on this renderer's device (the senders' runs for this
+        window, concatenated in shard order). `out`: a (rows, width, 3)
+        uint8 numpy array (host) or CUDA tensor (written in place); a new
+        numpy array when None."""
+        import torch
+
+        _pixel_count(width, height)
+        rb = N.SPLAT_RECORD_BYTES
+        if records.numel() % rb:
+            raise ValueError("records must hold whole records of SPLAT_RECORD_BYTES bytes")
+        n = records.numel() // rb
+        if n and records.data_ptr() % 16:
+            records = records.clone()  # the records must start 16-byte aligned
+        if out is None:
+            out = np.empty((rows, width, 3), np.uint8)
+        if isinstance(out, torch.Tensor):
+            if tuple(out.shape) != (rows, width, 3) or out.dtype != torch.uint8 or not out.is_contiguous():
+                raise ValueError("out must be a contiguous (rows, width, 3) uint8 tensor")
+            ptr, nbytes = out.data_ptr(), out.numel()
+        else:
+            if out.shape != (rows, width, 3) or out.dtype != np.uint8 or not out.flags["C_CONTIGUOUS"]:
+                raise ValueError("out must be a C-contiguous (rows, width, 3) uint8 array")
+            ptr, nbytes = out.ctypes.data, out.nbytes
+        bg = _f32(background)
+        st = N.RenderStatsC()
+        rc = N.lib().splat_cuda_render_records(self._h, ctypes.byref(_view_desc(view)), width, height,
+                                               bg.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                               records.data_ptr() if n else None, n, row0, rows, ptr, nbytes,
+                                               ctypes.byref(st))
+        N.check(rc, self._h, "render_records")
+        return (out, RenderStats.from_c(st)) if stats else out
+
     # --- device-side entry points --------------------------------------------
     def render_into(self, view: View, width: int, height: int, background, out_ptr: int, out_bytes: int,
                     downsample: int = 1) -> RenderStats:

@@ -121,6 +121,16 @@ class Scene:
         self.cov3d = covariance(self.scales, self.rotations) if n else np.zeros((0, 6), np.float32)
         return self
 
+    def shard(self, s0: int, s1: int) -> "Scene":
+        """Splats [s0, s1) of this finalized scene as a scene of their own
+        (one device's share of a frame split by splats)."""
+        self._flush()
+        out = Scene()
+        for name in ("positions", "scales", "rotations", "opacities", "colors", "sh_rest", "cov3d"):
+            setattr(out, name, np.ascontiguousarray(getattr(self, name)[s0:s1]))
+        out.sh_degree = self.sh_degree
+        return out
+
     def bounds(self):
         """Robust centre/radius (``scene.rs:212-258``): per-axis median and
         min(p90, 2 * p50) of the distances, on a subsample of <= ~200k points."""
@@ -180,6 +190,11 @@ class HalfScene:
 
     def __len__(self):
         return len(self.positions)
+
+    def shard(self, s0: int, s1: int) -> "HalfScene":
+        """Splats [s0, s1) as a scene of their own (one device's share)."""
+        return HalfScene(self.positions[s0:s1], self.scales[s0:s1], self.rotations[s0:s1], self.opacities[s0:s1],
+                         self.sh[s0:s1], self.sh_degree)
 
     def decoded(self) -> dict:
         """The stored values widened back to f32 (exact), as arrays named like
