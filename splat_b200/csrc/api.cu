@@ -129,11 +129,12 @@ int ensure_size(splat_cuda_handle* h, uint64_t tiles, uint32_t rows, size_t out_
     h->ranges_cap = tiles;
   }
   const size_t words = (size_t)rows * tiles;
-  if (words > h->counts_cap) {
+  if (words > h->counts_cap) {  // with room for windows and record counts that vary
+    const size_t cap = words + words / 4;
     dfree(h->counts);
     h->counts_cap = 0;
-    CK(dmalloc(h, &h->counts, words * sizeof(uint32_t)), "cudaMalloc counts");
-    h->counts_cap = words;
+    CK(dmalloc(h, &h->counts, cap * sizeof(uint32_t)), "cudaMalloc counts");
+    h->counts_cap = cap;
   }
   const uint32_t chunks = (uint32_t)((tiles + kScanChunk - 1) / kScanChunk);
   if (chunks > h->chunks_cap || !h->st) {
@@ -336,7 +337,7 @@ int enqueue_frame(splat_cuda_handle* h, const FrameParams& fp_in, uint8_t* dev_o
   const bool scratch = f > 1 && (fp.tile_w % f != 0 || fp.tile_h % f != 0);
   const size_t full_bytes = scratch ? (size_t)fp.w * fp.h * 3 : 0;
   const bool records = h->rx;
-  const uint32_t rows = bin_rows(records ? h->rx_n : h->n, h->num_sms);
+  const uint32_t rows = bin_rows(records ? h->rx_n : h->n, h->num_sms, 1024);
   int rc = ensure_size(h, tiles, rows, 0, full_bytes);
   if (rc) return rc;
   const uint32_t chunks = (uint32_t)((tiles + kScanChunk - 1) / kScanChunk);
@@ -929,11 +930,12 @@ SPLAT_API int splat_cuda_render_records(splat_cuda_handle* h, const splat_view_d
   if (need == 0) return SPLAT_OK;
   CK(cudaSetDevice(h->device), "cudaSetDevice");
   const uint64_t slots = std::max<uint64_t>(n_records, 1);
-  if (slots > h->rx_bin_cap) {
+  if (slots > h->rx_bin_cap) {  // with room for the next frames' counts to vary
+    const uint64_t cap = slots + slots / 4;
     dfree(h->rx_bin);
     h->rx_bin_cap = 0;
-    CK(dmalloc(h, &h->rx_bin, slots * sizeof(BinInfo)), "cudaMalloc record binning input");
-    h->rx_bin_cap = slots;
+    CK(dmalloc(h, &h->rx_bin, cap * sizeof(BinInfo)), "cudaMalloc record binning input");
+    h->rx_bin_cap = cap;
   }
   FrameParams fp = make_params(*view, width, height, bg, 1);
   fp.win_y0 = row0;

@@ -423,9 +423,9 @@ __global__ void __launch_bounds__(kTileThreads) k_sort_long(const uint2* __restr
 
 }  // namespace
 
-uint32_t bin_rows(uint64_t n, int num_sms) {
-  // About 4096 splats per CTA, at most two CTAs per SM.
-  const uint64_t r = (n + 4095) / 4096;
+uint32_t bin_rows(uint64_t n, int num_sms, uint32_t per_cta) {
+  // About per_cta splats per CTA, at most two CTAs per SM.
+  const uint64_t r = (n + per_cta - 1) / per_cta;
   return (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(r, 2ull * (uint64_t)num_sms));
 }
 

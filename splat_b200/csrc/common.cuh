@@ -247,8 +247,11 @@ cudaError_t launch_project_batch(const ViewTask* table, uint32_t n_views, uint32
 // view's index in the batch.
 cudaError_t launch_project_learned_batch(ViewTask* table, uint32_t n_views, uint64_t total_tiles,
                                          const FrameCounters& fc, cudaStream_t stream, uint32_t* launches);
-// Count-matrix rows (CTAs of the count and scatter launches) for n splats.
-uint32_t bin_rows(uint64_t n, int num_sms);
+// Count-matrix rows (CTAs of the count and scatter launches) for n splats:
+// about per_cta splats each, at most two CTAs per SM. A single view takes
+// 1024 per CTA (small scenes and windows of records still fill the GPU); the
+// views of a batch, which fill it together, 4096.
+uint32_t bin_rows(uint64_t n, int num_sms, uint32_t per_cta = 4096);
 // (b) binning into per-tile buckets and (c) the per-tile depth sorts, over
 // all views of the table: count matrix, tile totals, ranges, mid/long lists.
 struct BinLaunch {
