@@ -16,6 +16,13 @@ Workloads (--config):
          over the same 1080p orbit; PSNR against the exact-SH plain path, and
          the plain path's frames/s from the same run.
   batch  96 views of mixed resolution over three scenes, one CUDA graph.
+  sharded
+         the plain workload's frame drawn from splats sharded over the ranks:
+         each rank holds a contiguous share of the scene and owns a window of
+         tile rows; the projected splats cross in one all-to-all (NCCL) and
+         the windows are gathered on the device. With one process, --shards
+         ranks run one after another on the one GPU (the exchange becomes a
+         concatenation): the line then also states each rank's part.
 A step is one frame.
 
   value  frames/s with the scene resident in HBM and the frame written to
@@ -64,6 +71,10 @@ CONFIGS = {
                 "s_in": 64,  # f32 position + k, f16 scale/rotation/opacity, 16 f16 latents
                 "workload": "1.2M gaussians of the SH3 workload with colour from 16 FP16 latents + a shared "
                             "19-64-64-3 MLP (FP16 geometry), 1920x1080, 16x16 tiles, 40-view orbit"},
+    "sharded": {"metric": "frames/s at 1920x1080, 1.2M SH3 splats, one frame from splats sharded over the ranks",
+                "w": 1920, "h": 1080, "precision": "fp32", "s_in": 232,
+                "workload": "1.2M SH-degree-3 gaussians (64 seeded clusters), 1920x1080, 16x16 tiles, 40-view "
+                            "orbit; splats sharded in contiguous runs, one window of tile rows per rank"},
     "fp16": {"metric": "frames/s at 3840x2160, 1.2M SH3 splats, FP16 storage", "w": 3840, "h": 2160,
              "precision": "fp16",
              "s_in": 124,  # f32 position; f16 scale, rotation, opacity, 48 SH coefficients
@@ -85,6 +96,7 @@ def parse():
     p.add_argument("--error-frames", type=int, default=2,
                    help="fp16: frames whose error against the FP64 naive rasterizer is stated")
     p.add_argument("--splats", type=int, default=N_SPLATS)
+    p.add_argument("--shards", type=int, default=4, help="sharded, one process: ranks emulated one after another")
     p.add_argument("--cpu-sample-s", type=float, default=15.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--learn-epochs", type=float, default=30.0, help="learned: training epochs before rendering")
@@ -97,7 +109,7 @@ def parse():
                         "--steps times each, then exit (a short command for ncu captures of k_decode_* and k_cells)")
     a = p.parse_args()
     if a.steps is None:
-        a.steps = {"plain": 4000, "fp16": 1000, "batch": 20, "learned": 4000}[a.config]
+        a.steps = {"plain": 4000, "fp16": 1000, "batch": 20, "learned": 4000, "sharded": 500}[a.config]
     return a
 
 
@@ -610,6 +622,153 @@ def run_ours(args):
     r.close()
     if world > 1:
         torch.distributed.destroy_process_group()
+
+
+def run_sharded(args):
+    """The frame of the plain workload from splats sharded over the ranks
+    (splat_cuda_shard_records -> all-to-all of the records ->
+    splat_cuda_render_records -> all_gather of the windows). Timed with CUDA
+    events on the current stream around whole frames (the library's calls
+    block, so the span holds every rank part and exchange), max over ranks."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    from splat_b200 import _native as Nat
+    from splat_b200 import multi
+    from splat_b200.render import CudaRenderer, Frame
+
+    rank, world, local = dist_env()
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+    cfg = CONFIGS["sharded"]
+    W, H, RB = cfg["w"], cfg["h"], Nat.SPLAT_RECORD_BYTES
+    scene, _, _, home, warm, timed = make_workload(args.splats, cfg)
+    S = world if world > 1 else max(1, args.shards)
+    mine = [rank] if world > 1 else list(range(S))
+    n = len(scene)
+    shards = {q: CudaRenderer(scene.shard(*multi.shard_range(n, q, S)), device=dev) for q in mine}
+    wins = multi.row_windows(H, S)
+    bounds = [r0 for r0, _ in wins] + [H]
+    most = max(rows for _, rows in wins)
+    outs = {q: torch.zeros((most, W, 3), dtype=torch.uint8, device=dev) for q in mine}
+    sends = {q: torch.empty(max(n // S, 1) * RB * 2, dtype=torch.uint8, device=dev) for q in mine}
+    gathered = [torch.empty((most, W, 3), dtype=torch.uint8, device=dev) for _ in range(S)]
+    parts = {"select_ms": [], "draw_ms": [], "sent_bytes": []}
+
+    def frame(v, record=False):
+        res = {}
+        for q in mine:
+            t0 = time.perf_counter()
+            res[q] = shards[q].shard_records(v, W, H, bounds, send=sends[q])
+            if record:
+                parts["select_ms"].append(1e3 * (time.perf_counter() - t0))
+                parts["sent_bytes"].append(sum(res[q][1]) * RB)
+            if res[q][0].numel() > sends[q].numel():
+                sends[q] = res[q][0]
+        for q in mine:
+            row0, rows = wins[q]
+            if world > 1:
+                recs, _ = multi.exchange_records(res[q][0], res[q][1], RB, world)
+            else:
+                runs = []
+                for p in mine:
+                    send, counts, _ = res[p]
+                    off = sum(counts[:q]) * RB
+                    runs.append(send[off:off + counts[q] * RB])
+                recs = torch.cat(runs)
+            t0 = time.perf_counter()
+            if rows:
+                shards[q].render_records(v, W, H, (0, 0, 0), recs, row0, rows, out=outs[q][:rows])
+            if record:
+                parts["draw_ms"].append(1e3 * (time.perf_counter() - t0))
+        if world > 1:
+            dist.all_gather(gathered, outs[rank])
+        else:
+            for q in mine:
+                gathered[q].copy_(outs[q])
+
+    def assemble():
+        f = np.empty((H, W, 3), np.uint8)
+        for (r0, rows), g in zip(wins, gathered):
+            if rows:
+                f[r0:r0 + rows] = g[:rows].cpu().numpy()
+        return f
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for v in [home] + warm[: max(args.warmup, 3)] + timed[:8]:  # record buffers settle here
+        frame(v)
+    torch.cuda.synchronize()
+    match = None
+    if rank == 0:  # the home frame against the one-device frame of the whole scene
+        frame(home)
+        torch.cuda.synchronize()
+        whole = CudaRenderer(scene, device=dev)
+        f = Frame()
+        whole.render(home, W, H, (0, 0, 0), f)
+        whole.close()
+        match = bool(np.array_equal(assemble(), f.pixels))
+    elif world > 1:
+        frame(home)
+    views = timed
+    K = args.steps
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = sum(r.get_option(Nat.SPLAT_OPT_KERNEL_LAUNCHES) for r in shards.values())
+    barrier()
+    with Clocks(dev) as clk:
+        start.record()
+        for i in range(K):
+            frame(views[i % len(views)])
+        end.record()
+        barrier()
+    launches = sum(r.get_option(Nat.SPLAT_OPT_KERNEL_LAUNCHES) for r in shards.values()) - launches0
+    ms = max_over_ranks(start.elapsed_time(end), dev)
+    value = K / (ms / 1e3)
+    # End to end: each frame then also reaches pinned host memory on rank 0.
+    host = torch.empty((H, W, 3), dtype=torch.uint8).pin_memory()
+    barrier()
+    t0 = time.perf_counter()
+    for i in range(min(K, 200)):
+        frame(views[i % len(views)])
+        if rank == 0:
+            for (r0, rows), g in zip(wins, gathered):
+                if rows:
+                    host[r0:r0 + rows].copy_(g[:rows], non_blocking=True)
+            torch.cuda.synchronize()
+    e2e = min(K, 200) / max_over_ranks(time.perf_counter() - t0, dev)
+    for v in views[:8]:
+        frame(v, record=True)
+    if rank == 0:
+        line = {
+            "metric": cfg["metric"], "value": value, "unit": "frames/s", "n_gpus": world, "steps": K,
+            "warmup": args.warmup, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": dict(bench_config(cfg, n, W, H, world), parallelism=f"splat-sharded x{S}"
+                           + ("" if world > 1 else " (emulated one after another on one GPU)")),
+            "matches_whole_frame": match,
+            "parts": {"select_ms_per_rank": float(np.median(parts["select_ms"])),
+                      "draw_ms_per_window": float(np.median(parts["draw_ms"])),
+                      "records_bytes_per_rank": float(np.median(parts["sent_bytes"])),
+                      "note": "wall time of the blocking calls (this process's ranks), medians over 8 views"},
+            "e2e": {"value": e2e, "unit": "frames/s", "h2d_bytes_per_step": 56 * S, "d2h_bytes_per_step": W * H * 3,
+                    "note": "each frame also copied from the gathered windows to pinned host memory on rank 0"},
+            "clocks": clk.summary(),
+            "gpu_launches": launches,
+        }
+        print(json.dumps(line), flush=True)
+    for r in shards.values():
+        r.close()
+    if world > 1:
+        dist.destroy_process_group()
 
 
 def learned_quality_correlated(args, W, H, dev):
@@ -1133,6 +1292,8 @@ def main():
         run_reference(args)
     elif args.config == "learned":
         run_learned(args)
+    elif args.config == "sharded":
+        run_sharded(args)
     else:
         run_ours(args)
 

@@ -903,8 +903,8 @@ SPLAT_API int splat_cuda_shard_records(splat_cuda_handle* h, const splat_view_de
                 "the send buffer holds " + std::to_string(send_capacity) + " records, the windows take " +
                     std::to_string(total) + " (counts are filled in)");
   if (total) {
-    CK(launch_shard_scatter(h->rec, h->bin, h->n, w, h->shard_scratch, static_cast<Record*>(send), send_capacity, s,
-                            &h->launches),
+    CK(launch_shard_scatter(h->rec, h->bin, h->n, w, h->shard_scratch, h->shard_totals, static_cast<Record*>(send),
+                            send_capacity, s, &h->launches),
        "record scatter kernel");
     CK(cudaStreamSynchronize(s), "record scatter");
   }

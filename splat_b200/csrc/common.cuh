@@ -295,8 +295,8 @@ cudaError_t launch_shard_count(const Record* rec, const BinInfo* bin, uint64_t n
 // window k's records from send + (totals of the windows before k) on, in
 // scene order; positions at or past cap are not written.
 cudaError_t launch_shard_scatter(const Record* rec, const BinInfo* bin, uint64_t n, const ShardWindows& w,
-                                 const void* scratch, Record* send, uint64_t cap, cudaStream_t stream,
-                                 uint32_t* launches);
+                                 const void* scratch, const unsigned long long* totals, Record* send, uint64_t cap,
+                                 cudaStream_t stream, uint32_t* launches);
 // The receiver side: the binning input of t.s.n records (t.rec, received in
 // scene order) for the view's window, in place of the projection; CTA 0
 // also stores t as table[0].

@@ -26,9 +26,17 @@ namespace splat {
 namespace {
 
 constexpr uint32_t kShardThreads = 256;
-constexpr uint32_t kShardPerCta = 4096;  // splats per CTA of the count and scatter launches
+constexpr uint32_t kShardWarps = kShardThreads / 32;
+// Each warp of the count and scatter launches walks one chunk of kShardChunk
+// consecutive splats, 32 at a time, in scene order: the scatter orders each
+// window's records within a chunk by ballots alone (no block barrier), and
+// the chunks' counts, scanned in chunk order, place the chunks.
+constexpr uint32_t kShardChunk = 256;
 
-uint32_t shard_ctas(uint64_t n) { return (uint32_t)std::max<uint64_t>(1, (n + kShardPerCta - 1) / kShardPerCta); }
+__host__ __device__ __forceinline__ uint64_t shard_chunks(uint64_t n) {
+  return n ? (n + kShardChunk - 1) / kShardChunk : 1;
+}
+uint32_t shard_ctas(uint64_t n) { return (uint32_t)((shard_chunks(n) + kShardWarps - 1) / kShardWarps); }
 
 // The pixel rows [y0, y1) of splat i's bbox, if it is visible and its bbox
 // holds a pixel of the frame (the projection ran over the whole frame).
@@ -46,100 +54,102 @@ __device__ __forceinline__ bool meets(const ShardWindows& w, uint32_t k, uint32_
   return w.bound[k] < y1 && w.bound[k + 1] > y0;
 }
 
-// Records per (CTA, window): cnt[cta * w.n + k].
+// Records per (window, chunk): cnt[k * chunks + chunk].
 __global__ void __launch_bounds__(kShardThreads) k_shard_count(const Record* __restrict__ rec,
                                                                const BinInfo* __restrict__ bin, uint64_t n,
                                                                const ShardWindows w, uint32_t* __restrict__ cnt) {
-  __shared__ uint32_t c[kMaxShardWindows];
-  const uint32_t tid = threadIdx.x, lane = tid & 31;
-  for (uint32_t k = tid; k < w.n; k += kShardThreads) c[k] = 0u;
-  __syncthreads();
-  const uint64_t s0 = (uint64_t)blockIdx.x * kShardPerCta, s1 = n < s0 + kShardPerCta ? n : s0 + kShardPerCta;
-  // Whole warps walk the range (s1 - s0 rounded up), so every ballot is full.
-  for (uint64_t i = s0 + tid; i < s0 + ((s1 - s0 + 31) & ~31ull); i += kShardThreads) {
+  __shared__ uint32_t c[kShardWarps][kMaxShardWindows];
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint64_t chunk = (uint64_t)blockIdx.x * kShardWarps + warp;
+  if (chunk >= shard_chunks(n)) return;  // whole warps: no block barrier follows
+  for (uint32_t k = lane; k < w.n; k += 32) c[warp][k] = 0u;
+  __syncwarp();
+  const uint64_t s0 = chunk * kShardChunk, s1 = n < s0 + kShardChunk ? n : s0 + kShardChunk;
+  for (uint64_t b0 = s0; b0 < s1; b0 += 32) {
+    const uint64_t i = b0 + lane;
     uint32_t y0 = 0, y1 = 0;
     const bool v = i < s1 && splat_rows(rec, bin, i, y0, y1);
     for (uint32_t k = 0; k < w.n; k++) {
       const uint32_t m = __ballot_sync(0xffffffffu, v && meets(w, k, y0, y1));
-      if (lane == 0 && m) atomicAdd(&c[k], (uint32_t)__popc(m));
+      if (lane == 0) c[warp][k] += (uint32_t)__popc(m);
     }
   }
-  __syncthreads();
-  for (uint32_t k = tid; k < w.n; k += kShardThreads) cnt[(uint64_t)blockIdx.x * w.n + k] = c[k];
+  __syncwarp();
+  const uint64_t chunks = shard_chunks(n);
+  for (uint32_t k = lane; k < w.n; k += 32) cnt[k * chunks + chunk] = c[warp][k];
 }
 
-// One CTA: per window, the exclusive scan of the CTAs' counts, offset by the
-// totals of the windows before it, into off[cta * w.n + k]; totals[k].
-__global__ void __launch_bounds__(1024) k_shard_scan(const uint32_t* __restrict__ cnt, uint32_t ctas,
-                                                     const ShardWindows w, unsigned long long* __restrict__ off,
+// CTA k: the exclusive scan of window k's chunk counts into off[k * chunks +
+// chunk] and their sum into totals[k] (the windows are scanned side by side;
+// the scatter adds the earlier windows' totals).
+__global__ void __launch_bounds__(1024) k_shard_scan(const uint32_t* __restrict__ cnt, uint32_t chunks,
+                                                     unsigned long long* __restrict__ off,
                                                      unsigned long long* __restrict__ totals) {
   __shared__ unsigned long long wsum[32];
-  const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  unsigned long long base = 0;  // records of the windows before k
-  for (uint32_t k = 0; k < w.n; k++) {
-    unsigned long long carry = base;
-    for (uint32_t c0 = 0; c0 < ctas; c0 += 1024) {
-      const uint32_t c = c0 + tid;
-      const unsigned long long v = c < ctas ? cnt[(uint64_t)c * w.n + k] : 0ull;
-      unsigned long long x = v;
+  const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, k = blockIdx.x;
+  const uint32_t* src = cnt + (uint64_t)k * chunks;
+  unsigned long long* dst = off + (uint64_t)k * chunks;
+  unsigned long long carry = 0;
+  for (uint32_t c0 = 0; c0 < chunks; c0 += 1024) {
+    const uint32_t c = c0 + tid;
+    const unsigned long long v = c < chunks ? src[c] : 0ull;
+    unsigned long long x = v;
 #pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= (uint32_t)o) x += y;
-      }
-      if (lane == 31) wsum[warp] = x;
-      __syncthreads();
-      unsigned long long before = 0, all = 0;
-      for (uint32_t q = 0; q < 32; q++) {
-        if (q < warp) before += wsum[q];
-        all += wsum[q];
-      }
-      if (c < ctas) off[(uint64_t)c * w.n + k] = carry + before + x - v;
-      carry += all;
-      __syncthreads();  // wsum is rewritten by the next chunk
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= (uint32_t)o) x += y;
     }
-    if (tid == 0) totals[k] = carry - base;
-    base = carry;
+    if (lane == 31) wsum[warp] = x;
+    __syncthreads();
+    unsigned long long before = 0, all = 0;
+    for (uint32_t q = 0; q < 32; q++) {
+      if (q < warp) before += wsum[q];
+      all += wsum[q];
+    }
+    if (c < chunks) dst[c] = carry + before + x - v;
+    carry += all;
+    __syncthreads();  // wsum is rewritten by the next block of chunks
   }
+  if (tid == 0) totals[k] = carry;
 }
 
-// Writes the records: each CTA walks its splats in rounds of 256, in scene
-// order, and places the round's records of window k after those of the
-// earlier rounds (a block-wide ballot scan per window).
+// Writes the records: each warp walks its chunk 32 splats at a time, in
+// scene order, and places each window's records of the 32 after those
+// already written (a ballot prefix; the window cursors live in the warp's
+// shared-memory row).
 __global__ void __launch_bounds__(kShardThreads) k_shard_scatter(const Record* __restrict__ rec,
                                                                  const BinInfo* __restrict__ bin, uint64_t n,
                                                                  const ShardWindows w,
                                                                  const unsigned long long* __restrict__ off,
+                                                                 const unsigned long long* __restrict__ totals,
                                                                  Record* __restrict__ send, uint64_t cap) {
-  __shared__ unsigned long long cur[kMaxShardWindows];
-  __shared__ uint32_t wcnt[kShardThreads / 32];
-  const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  for (uint32_t k = tid; k < w.n; k += kShardThreads) cur[k] = off[(uint64_t)blockIdx.x * w.n + k];
-  __syncthreads();
-  const uint64_t s0 = (uint64_t)blockIdx.x * kShardPerCta, s1 = n < s0 + kShardPerCta ? n : s0 + kShardPerCta;
-  for (uint64_t r0 = s0; r0 < s1; r0 += kShardThreads) {
-    const uint64_t i = r0 + tid;
+  __shared__ unsigned long long cur[kShardWarps][kMaxShardWindows];
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint64_t chunk = (uint64_t)blockIdx.x * kShardWarps + warp, chunks = shard_chunks(n);
+  if (chunk >= chunks) return;
+  for (uint32_t k = lane; k < w.n; k += 32) {
+    unsigned long long base = 0;  // the records of the windows before k
+    for (uint32_t j = 0; j < k; j++) base += totals[j];
+    cur[warp][k] = base + off[k * chunks + chunk];
+  }
+  __syncwarp();
+  const uint64_t s0 = chunk * kShardChunk, s1 = n < s0 + kShardChunk ? n : s0 + kShardChunk;
+  const uint32_t below = (1u << lane) - 1u;
+  for (uint64_t b0 = s0; b0 < s1; b0 += 32) {
+    const uint64_t i = b0 + lane;
     uint32_t y0 = 0, y1 = 0;
     const bool v = i < s1 && splat_rows(rec, bin, i, y0, y1);
     Record r{};
     if (v) r = rec[i];
     for (uint32_t k = 0; k < w.n; k++) {
       const bool hit = v && meets(w, k, y0, y1);
-      if (!__syncthreads_or(hit)) continue;  // uniform: no record of this round goes to k
       const uint32_t m = __ballot_sync(0xffffffffu, hit);
-      if (lane == 0) wcnt[warp] = (uint32_t)__popc(m);
-      __syncthreads();
-      uint32_t before = 0, all = 0;
-#pragma unroll
-      for (uint32_t q = 0; q < kShardThreads / 32; q++) {
-        if (q < warp) before += wcnt[q];
-        all += wcnt[q];
-      }
-      const unsigned long long pos = cur[k] + before + (uint32_t)__popc(m & ((1u << lane) - 1u));
+      if (m == 0u) continue;  // uniform over the warp
+      const unsigned long long pos = cur[warp][k] + (uint32_t)__popc(m & below);
       if (hit && pos < cap) send[pos] = r;
-      __syncthreads();  // every thread has read cur[k] and wcnt
-      if (tid == 0) cur[k] += all;
-      // cur[k] is read again only after the next round's __syncthreads_or.
+      __syncwarp();  // every lane has read cur[warp][k]
+      if (lane == 0) cur[warp][k] += (uint32_t)__popc(m);
+      __syncwarp();
     }
   }
 }
@@ -163,13 +173,13 @@ __global__ void __launch_bounds__(256) k_records_bin(const ViewTask t, ViewTask*
   }
 }
 
-// Scratch layout: offsets (u64, ctas x windows), then counts (u32, same).
+// Scratch layout: offsets (u64, chunks x windows), then counts (u32, same).
 struct ShardScratch {
   unsigned long long* off;
   uint32_t* cnt;
 };
 ShardScratch shard_scratch_at(void* p, uint64_t n, uint32_t windows) {
-  const size_t cells = (size_t)shard_ctas(n) * windows;
+  const size_t cells = (size_t)shard_chunks(n) * windows;
   ShardScratch s;
   s.off = static_cast<unsigned long long*>(p);
   s.cnt = reinterpret_cast<uint32_t*>(s.off + cells);
@@ -179,24 +189,23 @@ ShardScratch shard_scratch_at(void* p, uint64_t n, uint32_t windows) {
 }  // namespace
 
 size_t shard_scratch_bytes(uint64_t n, uint32_t windows) {
-  return (size_t)shard_ctas(n) * windows * (sizeof(unsigned long long) + sizeof(uint32_t));
+  return (size_t)shard_chunks(n) * windows * (sizeof(unsigned long long) + sizeof(uint32_t));
 }
 
 cudaError_t launch_shard_count(const Record* rec, const BinInfo* bin, uint64_t n, const ShardWindows& w,
                                void* scratch, unsigned long long* totals, cudaStream_t stream, uint32_t* launches) {
-  const uint32_t ctas = shard_ctas(n);
   const ShardScratch s = shard_scratch_at(scratch, n, w.n);
-  k_shard_count<<<ctas, kShardThreads, 0, stream>>>(rec, bin, n, w, s.cnt);
-  k_shard_scan<<<1, 1024, 0, stream>>>(s.cnt, ctas, w, s.off, totals);
+  k_shard_count<<<shard_ctas(n), kShardThreads, 0, stream>>>(rec, bin, n, w, s.cnt);
+  k_shard_scan<<<w.n, 1024, 0, stream>>>(s.cnt, (uint32_t)shard_chunks(n), s.off, totals);
   *launches += 2;
   return cudaGetLastError();
 }
 
 cudaError_t launch_shard_scatter(const Record* rec, const BinInfo* bin, uint64_t n, const ShardWindows& w,
-                                 const void* scratch, Record* send, uint64_t cap, cudaStream_t stream,
-                                 uint32_t* launches) {
+                                 const void* scratch, const unsigned long long* totals, Record* send, uint64_t cap,
+                                 cudaStream_t stream, uint32_t* launches) {
   const ShardScratch s = shard_scratch_at(const_cast<void*>(scratch), n, w.n);
-  k_shard_scatter<<<shard_ctas(n), kShardThreads, 0, stream>>>(rec, bin, n, w, s.off, send, cap);
+  k_shard_scatter<<<shard_ctas(n), kShardThreads, 0, stream>>>(rec, bin, n, w, s.off, totals, send, cap);
   *launches += 1;
   return cudaGetLastError();
 }
