@@ -761,11 +761,15 @@ int render_to_host(splat_cuda_handle* h, const FrameParams& fp, uint8_t* rgb_out
     return fail(h, SPLAT_ERR_CAPACITY, "pair buffers kept overflowing");
   }
   if ((rc = ensure_size(h, 0, 0, bytes, 0))) return rc;
-  // Pinned output the device can address: the blend (or the downsample)
-  // writes the frame straight into it, overlapped with the frame's own
-  // compute, instead of a copy after the frame. Other pinned memory gets one
-  // copy; pageable memory goes through the handle's pinned staging buffer.
-  uint8_t* const mapped = bytes ? mapped_host(rgb_out) : nullptr;
+  // Pinned output the device can address: the default blend writes the
+  // frame straight into it as whole words of tile rows, overlapped with the
+  // frame's own compute, instead of a copy after the frame. Other blend
+  // configurations, the exact blend and downsampled frames (whose stores
+  // would cross the host link byte by byte) draw into device memory and copy
+  // the frame, as other pinned memory does; pageable memory goes through the
+  // handle's pinned staging buffer.
+  const bool rows_ok = fp.downsample == 1 && blend_writes_host_rows(h->blend, h->exact);
+  uint8_t* const mapped = bytes && rows_ok ? mapped_host(rgb_out) : nullptr;
   const bool direct = bytes && (mapped || is_pinned_host(rgb_out));
   if (!direct && bytes > h->stage_cap) {
     if (h->stage) cudaFreeHost(h->stage);

@@ -750,6 +750,7 @@ __global__ void k_downsample(FrameParams fp, const uint8_t* __restrict__ full, u
 }  // namespace
 
 bool blend_sorts_tiles(const BlendConfig& c) { return c.tile_w == 16 && c.tile_h == 16 && c.threads == 512; }
+bool blend_writes_host_rows(const BlendConfig& c, bool exact) { return !exact && blend_sorts_tiles(c); }
 
 bool blend_config_supported(const BlendConfig& c) {
   const bool shape = (c.tile_w == 8 && c.tile_h == 8) || (c.tile_w == 16 && c.tile_h == 16) ||

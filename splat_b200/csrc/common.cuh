@@ -233,6 +233,11 @@ bool blend_config_supported(const BlendConfig& c);
 // Whether the blend of this configuration sorts the tiles of at most
 // kMidSortCap pairs itself (then the binning launches no small/mid sorts).
 bool blend_sorts_tiles(const BlendConfig& c);
+// Whether the blend of this configuration has the row-word variant for
+// frames in mapped host memory (whole 4-byte words of tile rows; the other
+// variants store bytes, which over the host link are an order of magnitude
+// slower than drawing into device memory and copying the frame).
+bool blend_writes_host_rows(const BlendConfig& c, bool exact);
 
 // Launchers (each returns the cudaGetLastError of its launches and adds the
 // number of kernels it launched to *launches).
