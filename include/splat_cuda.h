@@ -105,7 +105,9 @@ typedef struct splat_view_desc {
 } splat_view_desc;
 
 /* RenderStats (src/render/mod.rs:72-83). For this tiled backend `overlaps`
- * counts (splat, tile) pairs. Stage times are device times from CUDA events
+ * counts the (splat, tile) pairs drawn: the tiles of each splat's pixel bbox
+ * that its alpha = 1/255 ellipse reaches (every bbox tile, as the
+ * reference's cpu backend pairs them, with SPLAT_OPT_BBOX_PAIRS). Stage times are device times from CUDA events
  * (project = projection + SH + pair emission, sort = radix sort + tile ranges,
  * raster = blend + downsample); total_ms is host wall time of the call. */
 typedef struct splat_render_stats {
@@ -319,6 +321,15 @@ void* splat_cuda_get_stream(splat_cuda_handle* h);
 #define SPLAT_OPT_BLEND_EVALS 12u  /* read-only: pixel/splat evaluations of the
                                       last completed frame (0 unless counted):
                                       the blend's work after early termination */
+#define SPLAT_OPT_BBOX_PAIRS 13u  /* 1: pair each splat with every tile of its
+                                      pixel bbox, as the reference's tiled
+                                      backends do (src/render/cpu.rs:251-277);
+                                      0 (default): a tile whose pixel centres
+                                      all lie outside the splat's alpha = 1/255
+                                      ellipse gets no pair (its contribution
+                                      there is zero: the image is the same,
+                                      `overlaps` counts the pairs drawn). The
+                                      keys of splat_cuda_debug_dump follow it. */
 #define SPLAT_FAULT_ALLOC 1u
 #define SPLAT_FAULT_LOST_WAIT 2u
 int splat_cuda_set_option(splat_cuda_handle* h, uint32_t option, uint64_t value);

@@ -37,6 +37,7 @@ SPLAT_FAULT_ALLOC = 1
 SPLAT_FAULT_LOST_WAIT = 2
 SPLAT_OPT_COUNT_EVALS = 11
 SPLAT_OPT_BLEND_EVALS = 12
+SPLAT_OPT_BBOX_PAIRS = 13
 
 SPLAT_RECORD_BYTES = 48
 

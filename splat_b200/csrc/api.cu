@@ -331,7 +331,8 @@ namespace {
 int enqueue_frame(splat_cuda_handle* h, const FrameParams& fp_in, uint8_t* dev_out, bool host_mapped = false) {
   FrameParams fp = fp_in;
   set_tile_shape(fp, h->blend.tile_w, h->blend.tile_h);
-  fp.flags = h->debug_capture ? kFrameKeepSortedPairs : 0u;  // splat_cuda_debug_dump reads the sorted pairs
+  fp.flags = (h->debug_capture ? kFrameKeepSortedPairs : 0u) |  // splat_cuda_debug_dump reads the sorted pairs
+             (h->bbox_pairs ? kFrameBboxPairs : 0u);
   const uint64_t tiles = (uint64_t)fp.tiles_x * fp.tiles_y;
   const uint32_t f = fp.downsample;
   const bool scratch = f > 1 && (fp.tile_w % f != 0 || fp.tile_h % f != 0);
@@ -1054,6 +1055,9 @@ SPLAT_API int splat_cuda_set_option(splat_cuda_handle* h, uint32_t option, uint6
     case SPLAT_OPT_STAGE_EVENTS:
       h->stage_events = value != 0;
       return SPLAT_OK;
+    case SPLAT_OPT_BBOX_PAIRS:
+      h->bbox_pairs = value != 0;
+      return SPLAT_OK;
     case SPLAT_OPT_COUNT_EVALS:
       h->count_evals = value != 0;
       return SPLAT_OK;
@@ -1100,6 +1104,7 @@ SPLAT_API int splat_cuda_get_option(splat_cuda_handle* h, uint32_t option, uint6
     case SPLAT_OPT_PAIR_LIMIT: *value = h->pair_limit; return SPLAT_OK;
     case SPLAT_OPT_STAGE_EVENTS: *value = h->stage_events; return SPLAT_OK;
     case SPLAT_OPT_COUNT_EVALS: *value = h->count_evals; return SPLAT_OK;
+    case SPLAT_OPT_BBOX_PAIRS: *value = h->bbox_pairs; return SPLAT_OK;
     case SPLAT_OPT_BLEND_EVALS: *value = h->have_frame ? h->st_host->evals : 0; return SPLAT_OK;
     case SPLAT_OPT_DEBUG_CAPTURE: *value = h->debug_capture; return SPLAT_OK;
     case SPLAT_OPT_FP64_CONICS: *value = h->have_frame ? h->st_host->fp64_conics : 0; return SPLAT_OK;

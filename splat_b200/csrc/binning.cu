@@ -38,27 +38,21 @@ namespace {
 
 constexpr int kBinThreads = 512;
 
-// Calls f(tile, splat, depth bits, active) for every pair of the splats at
+// Calls fw(tile, splat, depth bits) for every pair of the splats at
 // positions [s0, s1) of the binning order (SceneDev::order; null: scene
-// order). Splats with at most 32 pairs are expanded by their own lane, the
-// warp's lanes in lockstep (round r emits pair r of every lane's splat,
-// `active` false for lanes with fewer pairs, whose tile is kNoTile), so that
-// lanes on the same tile can share one bucket atomic; larger splats are
-// expanded by the whole warp (distinct tiles, all lanes active, `active`
-// passed as a compile-time true through fw).
-[[maybe_unused]] constexpr uint32_t kNoTile = 0xFFFFFFFFu;
-// false: each lane expands its own splat's pairs at its own pace, one bucket
-// atomic per pair (fw), as for the larger splats.
-constexpr bool kAggregateBuckets = false;
-
-template <class F, class FW>
+// order): row by row, the tiles of each row's span (row_span). Splats with
+// at most 32 pairs are expanded by their own lane; larger splats by the
+// whole warp, 32 tiles of a row at a time.
+template <class FW>
 __device__ __forceinline__ void for_each_pair(const BinInfo* __restrict__ bin, const uint32_t* __restrict__ order,
-                                              uint64_t s0, uint64_t s1, uint32_t tiles_x, F&& f, FW&& fw) {
+                                              uint64_t s0, uint64_t s1, uint32_t tiles_x, uint32_t tiles_y,
+                                              FW&& fw) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   constexpr uint64_t kStride = (uint64_t)kBinThreads;
+  const int tx_lim = (int)tiles_x, ty_lim = (int)tiles_y;
   // The lane's splat of the warp's next group of 32 is loaded while the
   // current group's pairs are expanded.
-  const BinInfo culled{kCulled, 0u, 0u, 0u};
+  const BinInfo culled{kCulled, 0u, 0u, 0u, {0u, 0u, 0u, 0u}};
   auto splat_at = [&](uint64_t k) -> uint32_t { return order ? __ldg(order + k) : (uint32_t)k; };
   uint64_t wb = s0 + (uint64_t)warp * 32;
   uint32_t ni = wb + lane < s1 ? splat_at(wb + lane) : 0u;
@@ -75,38 +69,67 @@ __device__ __forceinline__ void for_each_pair(const BinInfo* __restrict__ bin, c
     }
     const uint32_t cnt = b.rect_lo != kCulled ? b.count : 0u;
     const uint32_t mine = cnt <= 32 ? cnt : 0u;
-    const uint32_t tx0 = b.rect_lo & 0xFFFFu, ty0 = b.rect_lo >> 16, tx1 = b.rect_hi & 0xFFFFu;
-    uint32_t tx = tx0, ty = ty0;
-    if constexpr (kAggregateBuckets) {
-      const uint32_t rounds = __reduce_max_sync(0xffffffffu, mine);
-      for (uint32_t r = 0; r < rounds; r++) {
-        const bool act = r < mine;
-        f(act ? ty * tiles_x + tx : kNoTile, i, b.depth_bits, act);
-        if (act && ++tx == tx1) {
-          tx = tx0;
-          ty++;
-        }
-      }
-    } else {
-      for (uint32_t r = 0; r < mine; r++) {
-        fw(ty * tiles_x + tx, i, b.depth_bits);
-        if (++tx == tx1) {
-          tx = tx0;
-          ty++;
-        }
+    if (mine) {
+      const TileRect t = bin_rect(b);
+      // Rows max(0, -ty0) .. r1 of the rectangle lie in the window.
+      const int r1 = min(t.ty1, ty_lim) - t.ty0;
+      int row = max(0, -t.ty0), a, e;
+      row_span(b, t, (uint32_t)row, tx_lim, a, e);
+      for (uint32_t q = 0; q < mine; q++) {
+        while (a == e && row + 1 < r1) row_span(b, t, (uint32_t)++row, tx_lim, a, e);
+        if (a == e) break;  // (count is the sum of the spans: not reached)
+        fw((uint32_t)(t.ty0 + row) * tiles_x + (uint32_t)a, i, b.depth_bits);
+        a++;
       }
     }
     uint32_t big = __ballot_sync(0xffffffffu, cnt > 32);
     while (big) {
       const int L = __ffs(big) - 1;
       big &= big - 1u;
-      const uint32_t b_lo = __shfl_sync(0xffffffffu, b.rect_lo, L), b_hi = __shfl_sync(0xffffffffu, b.rect_hi, L);
-      const uint32_t b_cnt = __shfl_sync(0xffffffffu, cnt, L), b_d = __shfl_sync(0xffffffffu, b.depth_bits, L);
-      const uint32_t b_i = __shfl_sync(0xffffffffu, i, L);
-      const uint32_t btx0 = b_lo & 0xFFFFu, bty0 = b_lo >> 16, wdt = (b_hi & 0xFFFFu) - btx0;
-      for (uint32_t q = lane; q < b_cnt; q += 32) {
-        const uint32_t row = q / wdt;
-        fw((bty0 + row) * tiles_x + btx0 + (q - row * wdt), b_i, b_d);
+      BinInfo w;
+      w.rect_lo = __shfl_sync(0xffffffffu, b.rect_lo, L);
+      w.rect_hi = __shfl_sync(0xffffffffu, b.rect_hi, L);
+#pragma unroll
+      for (int q = 0; q < 4; q++) w.skip[q] = __shfl_sync(0xffffffffu, b.skip[q], L);
+      const uint32_t b_d = __shfl_sync(0xffffffffu, b.depth_bits, L), b_i = __shfl_sync(0xffffffffu, i, L);
+      const uint32_t b_cnt = __shfl_sync(0xffffffffu, cnt, L);
+      const TileRect t = bin_rect(w);
+      const int r0 = max(0, -t.ty0), r1 = min(t.ty1, ty_lim) - t.ty0;
+      const int cx0 = max(t.tx0, 0), wdt = min(t.tx1, tx_lim) - cx0;
+      // Lane r < kSkipRows holds row r's span (empty outside the window) and
+      // the pairs up to its end; rows past kSkipRows are whole.
+      int ra = 0, re = 0;
+      if (lane >= r0 && lane < min(r1, (int)kSkipRows)) row_span(w, t, (uint32_t)lane, tx_lim, ra, re);
+      const uint32_t wr = (uint32_t)(re - ra);
+      uint32_t incl = wr;
+#pragma unroll
+      for (int o = 1; o < (int)kSkipRows; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+      }
+      const uint32_t head = __shfl_sync(0xffffffffu, incl, kSkipRows - 1);
+      const int rf0 = max(r0, (int)kSkipRows);  // the first whole row inside the window
+      // The warp's lanes take 32 consecutive pairs at a time: a pair among
+      // the first rows finds its row by binary search over those lanes.
+      for (uint32_t q0 = 0; q0 < b_cnt; q0 += 32) {
+        const uint32_t q = q0 + (uint32_t)lane;
+        uint32_t lo = 0;
+#pragma unroll
+        for (uint32_t step = kSkipRows / 2; step >= 1; step >>= 1) {
+          if (__shfl_sync(0xffffffffu, incl, lo + step - 1) <= q) lo += step;
+        }
+        const int a_r = __shfl_sync(0xffffffffu, ra, lo);
+        const uint32_t ex = __shfl_sync(0xffffffffu, incl - wr, lo);
+        int row, col;
+        if (q < head) {
+          row = (int)lo;
+          col = a_r + (int)(q - ex);
+        } else {
+          const int q2 = (int)(q - head);
+          row = rf0 + q2 / wdt;
+          col = cx0 + q2 % wdt;
+        }
+        if (q < b_cnt) fw((uint32_t)(t.ty0 + row) * tiles_x + (uint32_t)col, b_i, b_d);
       }
     }
   }
@@ -118,7 +141,7 @@ struct BinView {
   const uint32_t* order;  // the binning order (null: scene order)
   uint32_t* row;  // this CTA's row of the view's count matrix
   uint64_t s0, s1;
-  uint32_t tiles_x, tiles, tile0;
+  uint32_t tiles_x, tiles_y, tiles, tile0;
 };
 
 __device__ __forceinline__ BinView bin_view(const ViewTask* __restrict__ table, uint32_t n_views) {
@@ -128,6 +151,7 @@ __device__ __forceinline__ BinView bin_view(const ViewTask* __restrict__ table, 
   b.bin = t->bin;
   b.order = t->s.order;
   b.tiles_x = t->fp.tiles_x;
+  b.tiles_y = t->fp.tiles_y;
   b.tiles = t->fp.tiles_x * t->fp.tiles_y;
   b.tile0 = t->tile0;
   const uint32_t r = blockIdx.x - t->bin_cta0, rows = t->rows;
@@ -149,15 +173,7 @@ __global__ void __launch_bounds__(kBinThreads) k_bin_count(const ViewTask* __res
     __syncthreads();
   }
   uint32_t* const cnt = SMEM ? s_row : b.row;
-  const int lane = threadIdx.x & 31;
-  for_each_pair(
-      b.bin, b.order, b.s0, b.s1, b.tiles_x,
-      [&](uint32_t t, uint32_t, uint32_t, bool act) {
-        // Lanes on the same tile add their pairs with one atomic.
-        const uint32_t peers = __match_any_sync(0xffffffffu, t);
-        if (act && lane == __ffs(peers) - 1) atomicAdd(&cnt[t], (uint32_t)__popc(peers));
-      },
-      [&](uint32_t t, uint32_t, uint32_t) { atomicAdd(&cnt[t], 1u); });
+  for_each_pair(b.bin, b.order, b.s0, b.s1, b.tiles_x, b.tiles_y, [&](uint32_t t, uint32_t, uint32_t) { atomicAdd(&cnt[t], 1u); });
   if (SMEM) {
     __syncthreads();
     for (uint32_t t = threadIdx.x; t < b.tiles; t += kBinThreads) b.row[t] = s_row[t];
@@ -303,28 +319,10 @@ __global__ void __launch_bounds__(kBinThreads) k_bin_scatter(const ViewTask* __r
     for (uint32_t t = threadIdx.x; t < b.tiles; t += kBinThreads) s_row[t] = vr[t].x + b.row[t];
     __syncthreads();
   }
-  const int lane = threadIdx.x & 31;
-  const uint32_t lt = (1u << lane) - 1u;
-  for_each_pair(
-      b.bin, b.order, b.s0, b.s1, b.tiles_x,
-      [&](uint32_t t, uint32_t i, uint32_t depth_bits, bool act) {
-        // Lanes on the same tile take consecutive positions from one atomic,
-        // so their stores land next to each other.
-        const uint32_t peers = __match_any_sync(0xffffffffu, t);
-        const int leader = __ffs(peers) - 1;
-        uint32_t base = 0u;
-        if (act && lane == leader) base = SMEM ? atomicAdd(&s_row[t], (uint32_t)__popc(peers))
-                                               : atomicAdd(&b.row[t], (uint32_t)__popc(peers));
-        base = __shfl_sync(0xffffffffu, base, leader);
-        if (act) {
-          const uint64_t pos = (SMEM ? 0ull : (uint64_t)vr[t].x) + base + __popc(peers & lt);
-          if (pos < cap) pairs[pos] = ((uint64_t)depth_bits << 32) | i;
-        }
-      },
-      [&](uint32_t t, uint32_t i, uint32_t depth_bits) {
-        const uint64_t pos = SMEM ? atomicAdd(&s_row[t], 1u) : (uint64_t)vr[t].x + atomicAdd(&b.row[t], 1u);
-        if (pos < cap) pairs[pos] = ((uint64_t)depth_bits << 32) | i;
-      });
+  for_each_pair(b.bin, b.order, b.s0, b.s1, b.tiles_x, b.tiles_y, [&](uint32_t t, uint32_t i, uint32_t depth_bits) {
+    const uint64_t pos = SMEM ? atomicAdd(&s_row[t], 1u) : (uint64_t)vr[t].x + atomicAdd(&b.row[t], 1u);
+    if (pos < cap) pairs[pos] = ((uint64_t)depth_bits << 32) | i;
+  });
 }
 
 // Tiles of at most kWarpSortCap pairs (classes 4 and 5, the heavier class

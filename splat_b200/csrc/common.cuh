@@ -57,6 +57,11 @@ struct FrameParams {
 // blend (for inspection; otherwise tiles the blend sorts itself may be left
 // in bucket order, their order held in shared memory only).
 constexpr uint32_t kFrameKeepSortedPairs = 1u;
+// The frame pairs each splat with every tile of its pixel bbox, as the
+// reference does (src/render/cpu.rs:251-277). Otherwise a tile whose pixel
+// centres all lie outside the splat's alpha = 1/255 ellipse (its blend
+// contribution there is zero) gets no pair; see window_rect.
+constexpr uint32_t kFrameBboxPairs = 2u;
 
 // Device-resident scene, FP32 storage (layout chosen for coalesced loads).
 struct SceneDev {
@@ -99,33 +104,168 @@ struct __align__(16) Record {
 };
 
 // Per-splat binning input written by the projection: the tile rectangle of
-// its pixel bbox (tx0 | ty0 << 16, tx1 | ty1 << 16), depth bits, pair count.
-// rect_lo == kCulled marks a culled splat; a visible splat whose bbox holds
-// no pixel has count 0.
+// its pixel bbox in the window's tile coordinates, not clipped to the window
+// (each coordinate + kRectBias in 16 bits: tx0 | ty0 << 16, tx1 | ty1 <<
+// 16), depth bits, the number of its pairs inside the window, and per row
+// r < kSkipRows of the rectangle the tiles at its left and right ends that
+// the splat does not reach (byte r of `skip`: left | right << 4): row r
+// pairs the splat with tiles [tx0 + left, tx1 - right), clipped to the
+// window. The skips do not depend on the window, so a frame drawn in windows
+// has the pairs of the frame drawn at once. rect_lo == kCulled marks a
+// culled splat; a visible splat whose bbox holds no pixel has count 0.
 struct __align__(16) BinInfo {
   uint32_t rect_lo, rect_hi, depth_bits, count;
+  uint32_t skip[4];
 };
+constexpr uint32_t kSkipRows = 16;
+constexpr int kRectBias = 32768;
+
+struct TileRect {
+  int tx0, ty0, tx1, ty1;
+};
+__device__ __forceinline__ TileRect bin_rect(const BinInfo& b) {
+  return {(int)(b.rect_lo & 0xFFFFu) - kRectBias, (int)(b.rect_lo >> 16) - kRectBias,
+          (int)(b.rect_hi & 0xFFFFu) - kRectBias, (int)(b.rect_hi >> 16) - kRectBias};
+}
+
+// Row r's tile span [a, e) of the rectangle, clipped to the window's tile
+// columns [0, tiles_x) (empty: a == e).
+__device__ __forceinline__ void row_span(const BinInfo& b, const TileRect& t, uint32_t r, int tiles_x, int& a,
+                                         int& e) {
+  // The word by selects, not by a dynamic index (which would put b in local memory).
+  const uint32_t word = r < 8u ? (r < 4u ? b.skip[0] : b.skip[1]) : (r < 12u ? b.skip[2] : b.skip[3]);
+  const uint32_t sk = r < kSkipRows ? (word >> (8u * (r & 3u))) & 255u : 0u;
+  a = max(t.tx0 + (int)(sk & 15u), 0);
+  e = min(t.tx1 - (int)(sk >> 4), tiles_x);
+  if (a > e) a = e;
+}
+
+// Hardware approximations as inline PTX: the same instruction, hence the
+// same result, in every translation unit whatever its contraction flags.
+__device__ __forceinline__ float lg2_hw(float x) {
+  float y;
+  asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float rcp_hw(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float sqrt_hw(float x) {
+  float y;
+  asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// For each row of a splat's tile rectangle, the tiles at its two ends whose
+// pixel centres all lie outside the splat's alpha = 1/255 ellipse, from the
+// splat's record r (centre, -conic/2 terms, opacity): with the conic (a, b,
+// c) and K = 2 ln(255 opacity), alpha >= 1/255 exactly where
+// Q = a dx^2 + 2 b dx dy + c dy^2 <= K (the same K that sizes the pixel bbox,
+// k^2). In the band of a tile row's pixel-centre rows [Y0, Y1] the ellipse
+// reaches x from min L(dy) to max U(dy), U/L(dy) = (-b dy +/- sqrt(a K -
+// det dy^2)) / a (det = ac - b^2), extremes at the ellipse's leftmost and
+// rightmost points (dy = +/- b sqrt(K c / det) / c) clamped into the band;
+// a tile column whose pixel-centre x range misses [x + L, x + U] holds no
+// pixel the splat reaches. K is widened by 0.2 % + 0.002 and the x range by
+// 0.01 px (the hardware square roots and reciprocals err by a few units in
+// the last place), so no tile a pixel needs is dropped; the blend's images do
+// not change (a dropped tile's pixels would all have failed the alpha test).
+// Every operation rounds explicitly, so the projection and the records'
+// binning input (different translation units and contraction flags) compute
+// the same skips. A 1 x 1 rectangle is left whole; rows past kSkipRows keep
+// their full width; skips saturate at 15 tiles.
+__device__ __forceinline__ void ellipse_skips(const FrameParams& fp, const Record& r, uint32_t ftx0, uint32_t ftx1,
+                                              uint32_t fty0, uint32_t fty1, BinInfo& b) {
+  const uint32_t width = ftx1 - ftx0, rows_all = fty1 - fty0;
+  if (width == 1u && rows_all == 1u) return;  // the centre's own tile
+  const float a = __fmul_rn(-2.0f, r.r0.z), bb = -r.r0.w, c = __fmul_rn(-2.0f, r.r1.x);
+  // det = ac - b^2 with b^2's rounding error carried (two-product): no
+  // cancellation for thin ellipses.
+  const float p = __fmul_rn(bb, bb), pe = __fmaf_rn(bb, bb, -p);
+  const float det = __fsub_rn(__fmaf_rn(a, c, -p), pe);
+  // K = 2 ln 2 (log2 op + log2 255), widened.
+  const float K0 = __fmul_rn(1.38629436f, __fadd_rn(lg2_hw(r.r1.y), 7.99435344f));
+  const float K = __fadd_rn(__fmul_rn(K0, 1.002f), 0.002f);
+  if (!(det > 0.0f && a > 0.0f && c > 0.0f && K > 0.0f)) return;
+  const float inv_det = rcp_hw(det), inv_a = rcp_hw(a);
+  const float aK = __fmul_rn(a, K);
+  const float ey = sqrt_hw(__fmul_rn(aK, inv_det));                          // vertical half-extent
+  const float xm = sqrt_hw(__fmul_rn(__fmul_rn(c, K), inv_det));             // horizontal half-extent
+  const float dyr = __fmul_rn(__fmul_rn(-bb, xm), rcp_hw(c));                // dy of the rightmost point
+  const float tw = (float)fp.tile_w, th = (float)fp.tile_h, inv_tw = 1.0f / (float)fp.tile_w;  // exact: powers of 2
+  const uint32_t rows = min(rows_all, kSkipRows);
+  for (uint32_t q = 0; q < rows; q++) {
+    const float ty = (float)(fty0 + q);
+    const float dy0 = __fsub_rn(__fadd_rn(__fmul_rn(ty, th), 0.5f), r.r0.y);
+    const float dy1 = __fadd_rn(dy0, th - 1.0f);
+    uint32_t left = 15u, right = 15u;  // no ellipse in the band: the whole row (up to 15 tiles a side)
+    if (dy1 >= -ey && dy0 <= ey) {
+      const float lo = fmaxf(dy0, -ey), hi = fminf(dy1, ey);
+      const float yr = fminf(fmaxf(dyr, lo), hi), yl = fminf(fmaxf(-dyr, lo), hi);
+      const float sr = sqrt_hw(fmaxf(__fsub_rn(aK, __fmul_rn(det, __fmul_rn(yr, yr))), 0.0f));
+      const float sl = sqrt_hw(fmaxf(__fsub_rn(aK, __fmul_rn(det, __fmul_rn(yl, yl))), 0.0f));
+      const float U = __fmul_rn(__fadd_rn(__fmul_rn(-bb, yr), sr), inv_a);
+      const float L = __fmul_rn(__fsub_rn(__fmul_rn(-bb, yl), sl), inv_a);
+      // Tile columns whose pixel centres [tx tw + 0.5, tx tw + tw - 0.5] meet [x + L, x + U].
+      const float xl = __fsub_rn(__fadd_rn(r.r0.x, L), 0.01f), xu = __fadd_rn(__fadd_rn(r.r0.x, U), 0.01f);
+      const float ta = ceilf(__fmul_rn(__fsub_rn(xl, tw - 0.5f), inv_tw));
+      const float tb = floorf(__fmul_rn(__fsub_rn(xu, 0.5f), inv_tw));
+      left = (uint32_t)fminf(fmaxf(__fsub_rn(ta, (float)ftx0), 0.0f), 15.0f);
+      right = (uint32_t)fminf(fmaxf(__fsub_rn((float)(ftx1 - 1u), tb), 0.0f), 15.0f);
+    }
+    left = min(left, width);
+    right = min(right, width - left);
+    const uint32_t byte = (left | (right << 4)) << (8u * (q & 3u));
+    if (q < 4u)
+      b.skip[0] |= byte;
+    else if (q < 8u)
+      b.skip[1] |= byte;
+    else if (q < 12u)
+      b.skip[2] |= byte;
+    else
+      b.skip[3] |= byte;
+  }
+}
 
 // The tile rectangle of a splat whose pixel bbox (pixel_bbox,
-// src/render/cpu.rs:96-102) is [bx0, x1) x [by0, y1): its tile rows and
-// columns clipped to the frame's rendered window and counted from the
-// window's first tile row and column (the whole frame: unchanged). A bbox
-// that holds no pixel of the window gives the empty rectangle (no pairs).
+// src/render/cpu.rs:96-102) is [bx0, x1) x [by0, y1), counted from the
+// window's first tile row and column (the whole frame: unchanged), and the
+// number of its pairs inside the window. A bbox that holds no pixel of the
+// window gives no pairs. Unless the frame asks for the bbox pairs
+// (kFrameBboxPairs), the rows' end tiles the splat's ellipse does not reach
+// are skipped (ellipse_skips, from the splat's record r, over the whole
+// rectangle).
 __device__ __forceinline__ void window_rect(const FrameParams& fp, uint32_t bx0, uint32_t x1, uint32_t by0,
-                                            uint32_t y1, BinInfo& b) {
-  const uint32_t wty0 = max(by0 >> fp.tile_sy, fp.win_ty0);
-  const uint32_t wty1 = min((y1 + fp.tile_h - 1) >> fp.tile_sy, fp.win_ty0 + fp.tiles_y);
-  const uint32_t wtx0 = max(bx0 >> fp.tile_sx, fp.win_tx0);
-  const uint32_t wtx1 = min((x1 + fp.tile_w - 1) >> fp.tile_sx, fp.win_tx0 + fp.tiles_x);
+                                            uint32_t y1, const Record& r, BinInfo& b) {
+  const uint32_t ftx0 = bx0 >> fp.tile_sx, ftx1 = (x1 + fp.tile_w - 1) >> fp.tile_sx;
+  const uint32_t fty0 = by0 >> fp.tile_sy, fty1 = (y1 + fp.tile_h - 1) >> fp.tile_sy;
+  const uint32_t wty0 = max(fty0, fp.win_ty0), wty1 = min(fty1, fp.win_ty0 + fp.tiles_y);
+  const uint32_t wtx0 = max(ftx0, fp.win_tx0), wtx1 = min(ftx1, fp.win_tx0 + fp.tiles_x);
+  b.skip[0] = b.skip[1] = b.skip[2] = b.skip[3] = 0u;
   if (bx0 < x1 && by0 < y1 && wty0 < wty1 && wtx0 < wtx1) {
-    const uint32_t tx0 = wtx0 - fp.win_tx0, ty0 = wty0 - fp.win_ty0;
-    const uint32_t tx1 = wtx1 - fp.win_tx0, ty1 = wty1 - fp.win_ty0;
-    b.rect_lo = tx0 | (ty0 << 16);
-    b.rect_hi = tx1 | (ty1 << 16);
-    b.count = (tx1 - tx0) * (ty1 - ty0);
+    TileRect t;
+    t.tx0 = (int)ftx0 - (int)fp.win_tx0;
+    t.ty0 = (int)fty0 - (int)fp.win_ty0;
+    t.tx1 = (int)ftx1 - (int)fp.win_tx0;
+    t.ty1 = (int)fty1 - (int)fp.win_ty0;
+    b.rect_lo = (uint32_t)(t.tx0 + kRectBias) | ((uint32_t)(t.ty0 + kRectBias) << 16);
+    b.rect_hi = (uint32_t)(t.tx1 + kRectBias) | ((uint32_t)(t.ty1 + kRectBias) << 16);
+    if (!(fp.flags & kFrameBboxPairs)) ellipse_skips(fp, r, ftx0, ftx1, fty0, fty1, b);
+    // The pairs inside the window: its rows of the rectangle (r0 .. r1), each
+    // row's span clipped to its columns; rows past kSkipRows are whole.
+    const int r0 = (int)(wty0 - fty0), r1 = (int)(wty1 - fty0), cols = (int)(wtx1 - wtx0);
+    uint32_t count = 0;
+    for (int q = r0; q < min(r1, (int)kSkipRows); q++) {
+      int a, e;
+      row_span(b, t, (uint32_t)q, (int)fp.tiles_x, a, e);
+      count += (uint32_t)(e - a);
+    }
+    count += (uint32_t)(max(r1 - max(r0, (int)kSkipRows), 0) * cols);
+    b.count = count;
   } else {
-    b.rect_lo = 0u;  // visible, but its bbox holds no pixel of the window: no pairs
-    b.rect_hi = 0u;
+    b.rect_lo = b.rect_hi = (uint32_t)kRectBias | ((uint32_t)kRectBias << 16);  // visible, no pixel of the window
     b.count = 0u;
   }
 }

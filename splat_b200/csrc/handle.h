@@ -77,6 +77,7 @@ struct splat_cuda_handle {
   bool exact = false;
   bool stage_events = true;
   bool count_evals = false;  // SPLAT_OPT_COUNT_EVALS
+  bool bbox_pairs = false;   // SPLAT_OPT_BBOX_PAIRS
   // fault injection (SPLAT_OPT_INJECT_FAULT), each fires once
   bool inject_alloc = false;    // the next device allocation fails as out of memory
   uint32_t inject_lost_us = 0;  // the next frame's tensor-core waits meet a lost completion

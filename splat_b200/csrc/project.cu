@@ -124,7 +124,7 @@ __device__ __forceinline__ void project_splat(const FrameParams& fp, const Scene
       opacity = po.w;
       k = 0.0f;
     }
-    BinInfo b{kCulled, 0u, 0u, 0u};
+    BinInfo b{kCulled, 0u, 0u, 0u, {0u, 0u, 0u, 0u}};
     float out_x = 0.f, out_y = 0.f, out_ex = 0.f, out_ey = 0.f, out_depth = 0.f, c0 = 0.f, c1 = 0.f, c2 = 0.f;
     float col[3] = {0.f, 0.f, 0.f};
     do {
@@ -255,7 +255,7 @@ __device__ __forceinline__ void project_splat(const FrameParams& fp, const Scene
       r.r2 = make_float4(col[2], __uint_as_float(bx0 | (x1 << 16)), __uint_as_float(by0 | (y1 << 16)), tz);
       rec[i] = r;
       b.depth_bits = __float_as_uint(tz);
-      window_rect(fp, bx0, x1, by0, y1, b);
+      window_rect(fp, bx0, x1, by0, y1, r, b);
       vis = true;
       out_x = x;
       out_y = y;

@@ -159,11 +159,11 @@ __global__ void __launch_bounds__(256) k_records_bin(const ViewTask t, ViewTask*
   const uint64_t i = (uint64_t)blockIdx.x * 256 + threadIdx.x;
   const bool v = i < t.s.n;
   if (v) {
-    const float4 r2 = t.rec[i].r2;
-    const uint32_t xb = __float_as_uint(r2.y), yb = __float_as_uint(r2.z);
+    const Record r = t.rec[i];
+    const uint32_t xb = __float_as_uint(r.r2.y), yb = __float_as_uint(r.r2.z);
     BinInfo b;
-    b.depth_bits = __float_as_uint(r2.w);
-    window_rect(t.fp, xb & 0xFFFFu, xb >> 16, yb & 0xFFFFu, yb >> 16, b);
+    b.depth_bits = __float_as_uint(r.r2.w);
+    window_rect(t.fp, xb & 0xFFFFu, xb >> 16, yb & 0xFFFFu, yb >> 16, r, b);
     t.bin[i] = b;
   }
   const uint32_t c = (uint32_t)__syncthreads_count(v);

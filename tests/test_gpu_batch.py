@@ -45,6 +45,7 @@ def test_blend_configs_match_cpu_backend(oracle, cfg):
     r = CudaRenderer(s)
     r.set_blend_config(*cfg)
     r.set_option(N.SPLAT_OPT_DEBUG_CAPTURE, 1)
+    r.set_option(N.SPLAT_OPT_BBOX_PAIRS, 1)  # the reference's pairs: every tile of the pixel bbox
     cpu = oracle.CpuTiled(s)
     for i, (w, h) in enumerate([(333, 190), (64, 48), (17, 9)]):
         v = _view(s, 0.7 * i, 0.2, 0.6 + 0.4 * i)

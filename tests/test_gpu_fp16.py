@@ -66,6 +66,7 @@ def test_fp16_projection_bit_exact_on_decoded_values(oracle, degree, size):
     r = CudaRenderer(half)
     assert r.precision == N.SPLAT_PRECISION_FP16
     r.set_option(N.SPLAT_OPT_DEBUG_CAPTURE, 1)
+    r.set_option(N.SPLAT_OPT_BBOX_PAIRS, 1)  # the reference's pairs: every tile of the pixel bbox
     for view in _views(s):
         r.render(view, w, h, (0.1, 0.2, 0.3), Frame())
         d = r.debug_dump(w, h)

@@ -46,6 +46,7 @@ def test_headline_workload_matches_oracle(oracle, workload):
     scene, views = workload
     r = CudaRenderer(scene)
     r.set_option(N.SPLAT_OPT_DEBUG_CAPTURE, 1)
+    r.set_option(N.SPLAT_OPT_BBOX_PAIRS, 1)  # the reference's pairs: every tile of the pixel bbox
     cpu = oracle.CpuTiled(scene)
     bg = (0.0, 0.0, 0.0)
     try:

@@ -61,6 +61,7 @@ def test_frame_past_the_pair_limit_is_complete(oracle):
     s = screen_filling(n)
     v = plane_view()
     r = CudaRenderer(s)
+    r.set_option(N.SPLAT_OPT_BBOX_PAIRS, 1)  # the reference's pairs: every tile of the pixel bbox
     r.set_option(N.SPLAT_OPT_PAIR_LIMIT, 1 << 18)
     assert r.get_option(N.SPLAT_OPT_PAIR_LIMIT) == 1 << 18
     cpu = oracle.CpuTiled(s)
@@ -98,6 +99,7 @@ def test_reference_pair_limit_scenario_full_size():
     s = screen_filling(n)
     v = plane_view()
     r = CudaRenderer(s)
+    r.set_option(N.SPLAT_OPT_BBOX_PAIRS, 1)  # the reference's pairs: every tile of the pixel bbox
     try:
         f = Frame()
         st = r.render(v, w, h, (0.0, 0.0, 0.0), f)
@@ -182,6 +184,7 @@ def test_a_tile_beyond_the_limit_is_an_error():
     s = screen_filling(3000)
     v = plane_view()
     r = CudaRenderer(s)
+    r.set_option(N.SPLAT_OPT_BBOX_PAIRS, 1)  # the reference's pairs: every tile of the pixel bbox
     try:
         r.set_option(N.SPLAT_OPT_PAIR_LIMIT, 2048)
         with pytest.raises(N.SplatError) as e:

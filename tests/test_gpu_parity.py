@@ -86,6 +86,7 @@ def test_projection_and_keys_bit_exact(oracle, name, size):
     w, h = size
     r = CudaRenderer(s)
     r.set_option(N.SPLAT_OPT_DEBUG_CAPTURE, 1)
+    r.set_option(N.SPLAT_OPT_BBOX_PAIRS, 1)  # the reference's pairs: every tile of the pixel bbox
     for view in orbit_views(s, 3):
         r.render(view, w, h, (0.1, 0.2, 0.3), Frame())
         d = r.debug_dump(w, h)
@@ -209,6 +210,7 @@ def test_pair_buffers_grow_and_rerender(oracle):
 def test_stats_match_cpu_backend(oracle):
     s = scene("clusters3")
     r = CudaRenderer(s)
+    r.set_option(N.SPLAT_OPT_BBOX_PAIRS, 1)  # the reference's pairs: every tile of the pixel bbox
     cpu = oracle.CpuTiled(s)
     for v in orbit_views(s, 3):
         _, st = cuda_frame(r, v, 320, 180)

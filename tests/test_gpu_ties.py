@@ -40,6 +40,7 @@ def test_equal_depth_runs_order_by_splat_index(oracle, planes, tile):
     v = View.looking_along_z([0.0, 0.0, 0.0])
     r = CudaRenderer(s)
     r.set_option(N.SPLAT_OPT_DEBUG_CAPTURE, 1)
+    r.set_option(N.SPLAT_OPT_BBOX_PAIRS, 1)  # the reference's pairs: every tile of the pixel bbox
     r.set_blend_config(tile[0], tile[1], 256)
     cpu = oracle.CpuTiled(s)
     try:
