@@ -45,11 +45,9 @@ constexpr int kBinThreads = 512;
 // whole warp, 32 tiles of a row at a time.
 template <class FW>
 __device__ __forceinline__ void for_each_pair(const BinInfo* __restrict__ bin, const uint32_t* __restrict__ order,
-                                              uint64_t s0, uint64_t s1, uint32_t tiles_x, uint32_t tiles_y,
-                                              FW&& fw) {
+                                              uint64_t s0, uint64_t s1, uint32_t tiles_x, FW&& fw) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   constexpr uint64_t kStride = (uint64_t)kBinThreads;
-  const int tx_lim = (int)tiles_x, ty_lim = (int)tiles_y;
   // The lane's splat of the warp's next group of 32 is loaded while the
   // current group's pairs are expanded.
   const BinInfo culled{kCulled, 0u, 0u, 0u, {0u, 0u, 0u, 0u}};
@@ -69,16 +67,28 @@ __device__ __forceinline__ void for_each_pair(const BinInfo* __restrict__ bin, c
     }
     const uint32_t cnt = b.rect_lo != kCulled ? b.count : 0u;
     const uint32_t mine = cnt <= 32 ? cnt : 0u;
-    if (mine) {
-      const TileRect t = bin_rect(b);
-      // Rows max(0, -ty0) .. r1 of the rectangle lie in the window.
-      const int r1 = min(t.ty1, ty_lim) - t.ty0;
-      int row = max(0, -t.ty0), a, e;
-      row_span(b, t, (uint32_t)row, tx_lim, a, e);
+    const uint32_t tx0 = b.rect_lo & 0xFFFFu, ty0 = b.rect_lo >> 16, tx1 = b.rect_hi & 0xFFFFu;
+    const uint32_t wdt0 = tx1 - tx0, area = wdt0 * ((b.rect_hi >> 16) - ty0);
+    if (mine && area <= kMaskTiles) {
+      // The rectangle's kept tiles, one bit each (row-major): the common
+      // case, one code path whether tiles are skipped or not. k / wdt0 for
+      // k < 32 as a multiply and shift.
+      const uint32_t inv = (65535u + wdt0) / wdt0;
+      uint32_t m = b.skip[0];
+      while (m) {
+        const uint32_t kb = (uint32_t)__ffs(m) - 1u;
+        m &= m - 1u;
+        const uint32_t row = (kb * inv) >> 16;
+        fw((ty0 + row) * tiles_x + tx0 + (kb - row * wdt0), i, b.depth_bits);
+      }
+    } else if (mine) {  // a larger rectangle culled to at most 32 pairs: each row's span
+      const uint32_t rows = (b.rect_hi >> 16) - ty0;
+      uint32_t row = 0, a, e;
+      row_span(b, 0, tx0, tx1, a, e);
       for (uint32_t q = 0; q < mine; q++) {
-        while (a == e && row + 1 < r1) row_span(b, t, (uint32_t)++row, tx_lim, a, e);
+        while (a == e && row + 1 < rows) row_span(b, ++row, tx0, tx1, a, e);
         if (a == e) break;  // (count is the sum of the spans: not reached)
-        fw((uint32_t)(t.ty0 + row) * tiles_x + (uint32_t)a, i, b.depth_bits);
+        fw((ty0 + row) * tiles_x + a, i, b.depth_bits);
         a++;
       }
     }
@@ -93,14 +103,20 @@ __device__ __forceinline__ void for_each_pair(const BinInfo* __restrict__ bin, c
       for (int q = 0; q < 4; q++) w.skip[q] = __shfl_sync(0xffffffffu, b.skip[q], L);
       const uint32_t b_d = __shfl_sync(0xffffffffu, b.depth_bits, L), b_i = __shfl_sync(0xffffffffu, i, L);
       const uint32_t b_cnt = __shfl_sync(0xffffffffu, cnt, L);
-      const TileRect t = bin_rect(w);
-      const int r0 = max(0, -t.ty0), r1 = min(t.ty1, ty_lim) - t.ty0;
-      const int cx0 = max(t.tx0, 0), wdt = min(t.tx1, tx_lim) - cx0;
-      // Lane r < kSkipRows holds row r's span (empty outside the window) and
-      // the pairs up to its end; rows past kSkipRows are whole.
-      int ra = 0, re = 0;
-      if (lane >= r0 && lane < min(r1, (int)kSkipRows)) row_span(w, t, (uint32_t)lane, tx_lim, ra, re);
-      const uint32_t wr = (uint32_t)(re - ra);
+      const uint32_t btx0 = w.rect_lo & 0xFFFFu, bty0 = w.rect_lo >> 16;
+      const uint32_t btx1 = w.rect_hi & 0xFFFFu, brows = (w.rect_hi >> 16) - bty0, wdt = btx1 - btx0;
+      if (!has_skips(w)) {
+        for (uint32_t q = lane; q < b_cnt; q += 32) {
+          const uint32_t row = q / wdt;
+          fw((bty0 + row) * tiles_x + btx0 + (q - row * wdt), b_i, b_d);
+        }
+        continue;
+      }
+      // Lane r < kSkipRows holds row r's span and the pairs up to its end;
+      // rows past kSkipRows are whole.
+      uint32_t ra = 0, re = 0;
+      if ((uint32_t)lane < min(brows, kSkipRows)) row_span(w, (uint32_t)lane, btx0, btx1, ra, re);
+      const uint32_t wr = re - ra;
       uint32_t incl = wr;
 #pragma unroll
       for (int o = 1; o < (int)kSkipRows; o <<= 1) {
@@ -108,7 +124,6 @@ __device__ __forceinline__ void for_each_pair(const BinInfo* __restrict__ bin, c
         if (lane >= o) incl += y;
       }
       const uint32_t head = __shfl_sync(0xffffffffu, incl, kSkipRows - 1);
-      const int rf0 = max(r0, (int)kSkipRows);  // the first whole row inside the window
       // The warp's lanes take 32 consecutive pairs at a time: a pair among
       // the first rows finds its row by binary search over those lanes.
       for (uint32_t q0 = 0; q0 < b_cnt; q0 += 32) {
@@ -118,18 +133,17 @@ __device__ __forceinline__ void for_each_pair(const BinInfo* __restrict__ bin, c
         for (uint32_t step = kSkipRows / 2; step >= 1; step >>= 1) {
           if (__shfl_sync(0xffffffffu, incl, lo + step - 1) <= q) lo += step;
         }
-        const int a_r = __shfl_sync(0xffffffffu, ra, lo);
-        const uint32_t ex = __shfl_sync(0xffffffffu, incl - wr, lo);
-        int row, col;
+        const uint32_t a_r = __shfl_sync(0xffffffffu, ra, lo), ex = __shfl_sync(0xffffffffu, incl - wr, lo);
+        uint32_t row, col;
         if (q < head) {
-          row = (int)lo;
-          col = a_r + (int)(q - ex);
+          row = lo;
+          col = a_r + (q - ex);
         } else {
-          const int q2 = (int)(q - head);
-          row = rf0 + q2 / wdt;
-          col = cx0 + q2 % wdt;
+          const uint32_t q2 = q - head;
+          row = kSkipRows + q2 / wdt;
+          col = btx0 + q2 % wdt;
         }
-        if (q < b_cnt) fw((uint32_t)(t.ty0 + row) * tiles_x + (uint32_t)col, b_i, b_d);
+        if (q < b_cnt) fw((bty0 + row) * tiles_x + col, b_i, b_d);
       }
     }
   }
@@ -141,7 +155,7 @@ struct BinView {
   const uint32_t* order;  // the binning order (null: scene order)
   uint32_t* row;  // this CTA's row of the view's count matrix
   uint64_t s0, s1;
-  uint32_t tiles_x, tiles_y, tiles, tile0;
+  uint32_t tiles_x, tiles, tile0;
 };
 
 __device__ __forceinline__ BinView bin_view(const ViewTask* __restrict__ table, uint32_t n_views) {
@@ -151,7 +165,6 @@ __device__ __forceinline__ BinView bin_view(const ViewTask* __restrict__ table, 
   b.bin = t->bin;
   b.order = t->s.order;
   b.tiles_x = t->fp.tiles_x;
-  b.tiles_y = t->fp.tiles_y;
   b.tiles = t->fp.tiles_x * t->fp.tiles_y;
   b.tile0 = t->tile0;
   const uint32_t r = blockIdx.x - t->bin_cta0, rows = t->rows;
@@ -173,7 +186,7 @@ __global__ void __launch_bounds__(kBinThreads) k_bin_count(const ViewTask* __res
     __syncthreads();
   }
   uint32_t* const cnt = SMEM ? s_row : b.row;
-  for_each_pair(b.bin, b.order, b.s0, b.s1, b.tiles_x, b.tiles_y, [&](uint32_t t, uint32_t, uint32_t) { atomicAdd(&cnt[t], 1u); });
+  for_each_pair(b.bin, b.order, b.s0, b.s1, b.tiles_x, [&](uint32_t t, uint32_t, uint32_t) { atomicAdd(&cnt[t], 1u); });
   if (SMEM) {
     __syncthreads();
     for (uint32_t t = threadIdx.x; t < b.tiles; t += kBinThreads) b.row[t] = s_row[t];
@@ -319,7 +332,7 @@ __global__ void __launch_bounds__(kBinThreads) k_bin_scatter(const ViewTask* __r
     for (uint32_t t = threadIdx.x; t < b.tiles; t += kBinThreads) s_row[t] = vr[t].x + b.row[t];
     __syncthreads();
   }
-  for_each_pair(b.bin, b.order, b.s0, b.s1, b.tiles_x, b.tiles_y, [&](uint32_t t, uint32_t i, uint32_t depth_bits) {
+  for_each_pair(b.bin, b.order, b.s0, b.s1, b.tiles_x, [&](uint32_t t, uint32_t i, uint32_t depth_bits) {
     const uint64_t pos = SMEM ? atomicAdd(&s_row[t], 1u) : (uint64_t)vr[t].x + atomicAdd(&b.row[t], 1u);
     if (pos < cap) pairs[pos] = ((uint64_t)depth_bits << 32) | i;
   });

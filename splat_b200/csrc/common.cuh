@@ -104,40 +104,38 @@ struct __align__(16) Record {
 };
 
 // Per-splat binning input written by the projection: the tile rectangle of
-// its pixel bbox in the window's tile coordinates, not clipped to the window
-// (each coordinate + kRectBias in 16 bits: tx0 | ty0 << 16, tx1 | ty1 <<
-// 16), depth bits, the number of its pairs inside the window, and per row
-// r < kSkipRows of the rectangle the tiles at its left and right ends that
-// the splat does not reach (byte r of `skip`: left | right << 4): row r
-// pairs the splat with tiles [tx0 + left, tx1 - right), clipped to the
-// window. The skips do not depend on the window, so a frame drawn in windows
-// has the pairs of the frame drawn at once. rect_lo == kCulled marks a
-// culled splat; a visible splat whose bbox holds no pixel has count 0.
+// its pixel bbox clipped to the rendered window and counted from the
+// window's first tile row and column (tx0 | ty0 << 16, tx1 | ty1 << 16),
+// depth bits, its pair count, and which tiles of the rectangle it pairs
+// with. A rectangle of at most kMaskTiles tiles: bit k of skip[0] for its
+// k-th tile in row-major order. A larger one: per row r < kSkipRows the
+// tiles at the row's two ends that the splat does not reach (byte r of
+// `skip`: left | right << 4, each at most 15; kSkipEmpty: none of the row),
+// row r pairing with tiles [tx0 + left, tx1 - right); all zero: the whole
+// rectangle. rect_lo == kCulled marks a culled splat; a visible splat whose
+// bbox holds no pixel has count 0.
 struct __align__(16) BinInfo {
   uint32_t rect_lo, rect_hi, depth_bits, count;
   uint32_t skip[4];
 };
 constexpr uint32_t kSkipRows = 16;
-constexpr int kRectBias = 32768;
+constexpr uint32_t kSkipEmpty = 0xFFu;
+constexpr uint32_t kMaskTiles = 32;
 
-struct TileRect {
-  int tx0, ty0, tx1, ty1;
-};
-__device__ __forceinline__ TileRect bin_rect(const BinInfo& b) {
-  return {(int)(b.rect_lo & 0xFFFFu) - kRectBias, (int)(b.rect_lo >> 16) - kRectBias,
-          (int)(b.rect_hi & 0xFFFFu) - kRectBias, (int)(b.rect_hi >> 16) - kRectBias};
+__host__ __device__ __forceinline__ uint32_t low_bits(uint32_t n) { return n >= 32u ? ~0u : (1u << n) - 1u; }
+
+__device__ __forceinline__ bool has_skips(const BinInfo& b) {
+  return (b.skip[0] | b.skip[1] | b.skip[2] | b.skip[3]) != 0u;
 }
 
-// Row r's tile span [a, e) of the rectangle, clipped to the window's tile
-// columns [0, tiles_x) (empty: a == e).
-__device__ __forceinline__ void row_span(const BinInfo& b, const TileRect& t, uint32_t r, int tiles_x, int& a,
-                                         int& e) {
+// Row r's tile span [a, e) of the rectangle [tx0, tx1) (empty: a == e).
+__device__ __forceinline__ void row_span(const BinInfo& b, uint32_t r, uint32_t tx0, uint32_t tx1, uint32_t& a,
+                                         uint32_t& e) {
   // The word by selects, not by a dynamic index (which would put b in local memory).
   const uint32_t word = r < 8u ? (r < 4u ? b.skip[0] : b.skip[1]) : (r < 12u ? b.skip[2] : b.skip[3]);
   const uint32_t sk = r < kSkipRows ? (word >> (8u * (r & 3u))) & 255u : 0u;
-  a = max(t.tx0 + (int)(sk & 15u), 0);
-  e = min(t.tx1 - (int)(sk >> 4), tiles_x);
-  if (a > e) a = e;
+  a = sk == kSkipEmpty ? tx1 : tx0 + (sk & 15u);
+  e = sk == kSkipEmpty ? tx1 : tx1 - (sk >> 4);
 }
 
 // Hardware approximations as inline PTX: the same instruction, hence the
@@ -172,14 +170,22 @@ __device__ __forceinline__ float sqrt_hw(float x) {
 // 0.01 px (the hardware square roots and reciprocals err by a few units in
 // the last place), so no tile a pixel needs is dropped; the blend's images do
 // not change (a dropped tile's pixels would all have failed the alpha test).
-// Every operation rounds explicitly, so the projection and the records'
-// binning input (different translation units and contraction flags) compute
-// the same skips. A 1 x 1 rectangle is left whole; rows past kSkipRows keep
-// their full width; skips saturate at 15 tiles.
-__device__ __forceinline__ void ellipse_skips(const FrameParams& fp, const Record& r, uint32_t ftx0, uint32_t ftx1,
-                                              uint32_t fty0, uint32_t fty1, BinInfo& b) {
-  const uint32_t width = ftx1 - ftx0, rows_all = fty1 - fty0;
-  if (width == 1u && rows_all == 1u) return;  // the centre's own tile
+//
+// The spans are those of the whole bbox rectangle [ftx0, ftx1) x [fty0,
+// fty1) (its rows past kSkipRows, and every row of a 1 x 1 rectangle, whole;
+// at most 15 tiles dropped at either end), intersected with the window's
+// part [wtx0, wtx1) x [wty0, wty1): a frame drawn in windows has exactly the
+// pairs of the frame drawn at once. Every operation rounds explicitly, so
+// the projection and the records' binning input (different translation
+// units and contraction flags) compute the same skips. Sets b.skip and
+// returns the pair count.
+__device__ __forceinline__ uint32_t ellipse_skips(const FrameParams& fp, const Record& r, uint32_t ftx0, uint32_t ftx1,
+                                                  uint32_t fty0, uint32_t fty1, uint32_t wtx0, uint32_t wtx1,
+                                                  uint32_t wty0, uint32_t wty1, BinInfo& b) {
+  const uint32_t wcols = wtx1 - wtx0, wrows = wty1 - wty0, all = wcols * wrows;
+  const bool masked = all <= kMaskTiles;
+  if (masked) b.skip[0] = low_bits(all);  // whole, unless narrowed below
+  if (ftx1 - ftx0 == 1u && fty1 - fty0 == 1u) return all;  // the centre's own tile
   const float a = __fmul_rn(-2.0f, r.r0.z), bb = -r.r0.w, c = __fmul_rn(-2.0f, r.r1.x);
   // det = ac - b^2 with b^2's rounding error carried (two-product): no
   // cancellation for thin ellipses.
@@ -188,55 +194,74 @@ __device__ __forceinline__ void ellipse_skips(const FrameParams& fp, const Recor
   // K = 2 ln 2 (log2 op + log2 255), widened.
   const float K0 = __fmul_rn(1.38629436f, __fadd_rn(lg2_hw(r.r1.y), 7.99435344f));
   const float K = __fadd_rn(__fmul_rn(K0, 1.002f), 0.002f);
-  if (!(det > 0.0f && a > 0.0f && c > 0.0f && K > 0.0f)) return;
+  if (!(det > 0.0f && a > 0.0f && c > 0.0f && K > 0.0f)) return all;
   const float inv_det = rcp_hw(det), inv_a = rcp_hw(a);
   const float aK = __fmul_rn(a, K);
   const float ey = sqrt_hw(__fmul_rn(aK, inv_det));                          // vertical half-extent
   const float xm = sqrt_hw(__fmul_rn(__fmul_rn(c, K), inv_det));             // horizontal half-extent
   const float dyr = __fmul_rn(__fmul_rn(-bb, xm), rcp_hw(c));                // dy of the rightmost point
   const float tw = (float)fp.tile_w, th = (float)fp.tile_h, inv_tw = 1.0f / (float)fp.tile_w;  // exact: powers of 2
-  const uint32_t rows = min(rows_all, kSkipRows);
+  const uint32_t dy0 = wty0 - fty0;  // bbox rows above the window
+  const uint32_t rows = min(wrows, kSkipRows);
+  uint32_t count = (wrows - rows) * wcols;
+  uint32_t mask = masked ? low_bits(all) & ~low_bits(rows * wcols) : 0u;  // rows past kSkipRows: whole
   for (uint32_t q = 0; q < rows; q++) {
-    const float ty = (float)(fty0 + q);
-    const float dy0 = __fsub_rn(__fadd_rn(__fmul_rn(ty, th), 0.5f), r.r0.y);
-    const float dy1 = __fadd_rn(dy0, th - 1.0f);
-    uint32_t left = 15u, right = 15u;  // no ellipse in the band: the whole row (up to 15 tiles a side)
-    if (dy1 >= -ey && dy0 <= ey) {
-      const float lo = fmaxf(dy0, -ey), hi = fminf(dy1, ey);
-      const float yr = fminf(fmaxf(dyr, lo), hi), yl = fminf(fmaxf(-dyr, lo), hi);
-      const float sr = sqrt_hw(fmaxf(__fsub_rn(aK, __fmul_rn(det, __fmul_rn(yr, yr))), 0.0f));
-      const float sl = sqrt_hw(fmaxf(__fsub_rn(aK, __fmul_rn(det, __fmul_rn(yl, yl))), 0.0f));
-      const float U = __fmul_rn(__fadd_rn(__fmul_rn(-bb, yr), sr), inv_a);
-      const float L = __fmul_rn(__fsub_rn(__fmul_rn(-bb, yl), sl), inv_a);
-      // Tile columns whose pixel centres [tx tw + 0.5, tx tw + tw - 0.5] meet [x + L, x + U].
-      const float xl = __fsub_rn(__fadd_rn(r.r0.x, L), 0.01f), xu = __fadd_rn(__fadd_rn(r.r0.x, U), 0.01f);
-      const float ta = ceilf(__fmul_rn(__fsub_rn(xl, tw - 0.5f), inv_tw));
-      const float tb = floorf(__fmul_rn(__fsub_rn(xu, 0.5f), inv_tw));
-      left = (uint32_t)fminf(fmaxf(__fsub_rn(ta, (float)ftx0), 0.0f), 15.0f);
-      right = (uint32_t)fminf(fmaxf(__fsub_rn((float)(ftx1 - 1u), tb), 0.0f), 15.0f);
+    const uint32_t rb = q + dy0;  // the row of the whole rectangle
+    uint32_t sa = ftx0, se = ftx1;  // its span, whole past kSkipRows
+    if (rb < kSkipRows) {
+      const float ty = (float)(fty0 + rb);
+      const float band0 = __fsub_rn(__fadd_rn(__fmul_rn(ty, th), 0.5f), r.r0.y);
+      const float band1 = __fadd_rn(band0, th - 1.0f);
+      if (band1 >= -ey && band0 <= ey) {
+        const float lo = fmaxf(band0, -ey), hi = fminf(band1, ey);
+        const float yr = fminf(fmaxf(dyr, lo), hi), yl = fminf(fmaxf(-dyr, lo), hi);
+        const float sr = sqrt_hw(fmaxf(__fsub_rn(aK, __fmul_rn(det, __fmul_rn(yr, yr))), 0.0f));
+        const float sl = sqrt_hw(fmaxf(__fsub_rn(aK, __fmul_rn(det, __fmul_rn(yl, yl))), 0.0f));
+        const float U = __fmul_rn(__fadd_rn(__fmul_rn(-bb, yr), sr), inv_a);
+        const float L = __fmul_rn(__fsub_rn(__fmul_rn(-bb, yl), sl), inv_a);
+        // Tile columns whose pixel centres [tx tw + 0.5, tx tw + tw - 0.5] meet [x + L, x + U].
+        const float xl = __fsub_rn(__fadd_rn(r.r0.x, L), 0.01f), xu = __fadd_rn(__fadd_rn(r.r0.x, U), 0.01f);
+        const float ta = ceilf(__fmul_rn(__fsub_rn(xl, tw - 0.5f), inv_tw));
+        const float tb = floorf(__fmul_rn(__fsub_rn(xu, 0.5f), inv_tw));
+        const uint32_t left = (uint32_t)fminf(fmaxf(__fsub_rn(ta, (float)ftx0), 0.0f), 15.0f);
+        uint32_t right = (uint32_t)fminf(fmaxf(__fsub_rn((float)(ftx1 - 1u), tb), 0.0f), 15.0f);
+        if (left == 15u && right == 15u) right = 14u;  // 15 | 15 << 4 is kSkipEmpty
+        sa = ftx0 + left;
+        se = max(sa, ftx1 - min(right, ftx1 - ftx0));
+      } else {
+        sa = se = ftx1;  // the ellipse misses the band
+      }
     }
-    left = min(left, width);
-    right = min(right, width - left);
-    const uint32_t byte = (left | (right << 4)) << (8u * (q & 3u));
+    // The span inside the window's columns.
+    const uint32_t ca = min(max(sa, wtx0), wtx1), ce = max(min(se, wtx1), ca);
+    count += ce - ca;
+    if (masked) {
+      mask |= low_bits(ce - ca) << (q * wcols + (ca - wtx0));
+      continue;
+    }
+    const uint32_t byte = ce == ca ? kSkipEmpty : (ca - wtx0) | ((wtx1 - ce) << 4);
+    const uint32_t sh = 8u * (q & 3u);
     if (q < 4u)
-      b.skip[0] |= byte;
+      b.skip[0] |= byte << sh;
     else if (q < 8u)
-      b.skip[1] |= byte;
+      b.skip[1] |= byte << sh;
     else if (q < 12u)
-      b.skip[2] |= byte;
+      b.skip[2] |= byte << sh;
     else
-      b.skip[3] |= byte;
+      b.skip[3] |= byte << sh;
   }
+  if (masked) b.skip[0] = mask;
+  return count;
 }
 
 // The tile rectangle of a splat whose pixel bbox (pixel_bbox,
-// src/render/cpu.rs:96-102) is [bx0, x1) x [by0, y1), counted from the
-// window's first tile row and column (the whole frame: unchanged), and the
-// number of its pairs inside the window. A bbox that holds no pixel of the
-// window gives no pairs. Unless the frame asks for the bbox pairs
-// (kFrameBboxPairs), the rows' end tiles the splat's ellipse does not reach
-// are skipped (ellipse_skips, from the splat's record r, over the whole
-// rectangle).
+// src/render/cpu.rs:96-102) is [bx0, x1) x [by0, y1): its tile rows and
+// columns clipped to the frame's rendered window and counted from the
+// window's first tile row and column (the whole frame: unchanged). A bbox
+// that holds no pixel of the window gives the empty rectangle (no pairs).
+// Unless the frame asks for the bbox pairs (kFrameBboxPairs), the rows' end
+// tiles the splat's ellipse does not reach are skipped (ellipse_skips, from
+// the splat's record r).
 __device__ __forceinline__ void window_rect(const FrameParams& fp, uint32_t bx0, uint32_t x1, uint32_t by0,
                                             uint32_t y1, const Record& r, BinInfo& b) {
   const uint32_t ftx0 = bx0 >> fp.tile_sx, ftx1 = (x1 + fp.tile_w - 1) >> fp.tile_sx;
@@ -245,27 +270,20 @@ __device__ __forceinline__ void window_rect(const FrameParams& fp, uint32_t bx0,
   const uint32_t wtx0 = max(ftx0, fp.win_tx0), wtx1 = min(ftx1, fp.win_tx0 + fp.tiles_x);
   b.skip[0] = b.skip[1] = b.skip[2] = b.skip[3] = 0u;
   if (bx0 < x1 && by0 < y1 && wty0 < wty1 && wtx0 < wtx1) {
-    TileRect t;
-    t.tx0 = (int)ftx0 - (int)fp.win_tx0;
-    t.ty0 = (int)fty0 - (int)fp.win_ty0;
-    t.tx1 = (int)ftx1 - (int)fp.win_tx0;
-    t.ty1 = (int)fty1 - (int)fp.win_ty0;
-    b.rect_lo = (uint32_t)(t.tx0 + kRectBias) | ((uint32_t)(t.ty0 + kRectBias) << 16);
-    b.rect_hi = (uint32_t)(t.tx1 + kRectBias) | ((uint32_t)(t.ty1 + kRectBias) << 16);
-    if (!(fp.flags & kFrameBboxPairs)) ellipse_skips(fp, r, ftx0, ftx1, fty0, fty1, b);
-    // The pairs inside the window: its rows of the rectangle (r0 .. r1), each
-    // row's span clipped to its columns; rows past kSkipRows are whole.
-    const int r0 = (int)(wty0 - fty0), r1 = (int)(wty1 - fty0), cols = (int)(wtx1 - wtx0);
-    uint32_t count = 0;
-    for (int q = r0; q < min(r1, (int)kSkipRows); q++) {
-      int a, e;
-      row_span(b, t, (uint32_t)q, (int)fp.tiles_x, a, e);
-      count += (uint32_t)(e - a);
+    const uint32_t tx0 = wtx0 - fp.win_tx0, ty0 = wty0 - fp.win_ty0;
+    const uint32_t tx1 = wtx1 - fp.win_tx0, ty1 = wty1 - fp.win_ty0;
+    b.rect_lo = tx0 | (ty0 << 16);
+    b.rect_hi = tx1 | (ty1 << 16);
+    const uint32_t area = (tx1 - tx0) * (ty1 - ty0);
+    if (fp.flags & kFrameBboxPairs) {
+      b.count = area;
+      if (area <= kMaskTiles) b.skip[0] = low_bits(area);
+    } else {
+      b.count = ellipse_skips(fp, r, ftx0, ftx1, fty0, fty1, wtx0, wtx1, wty0, wty1, b);
     }
-    count += (uint32_t)(max(r1 - max(r0, (int)kSkipRows), 0) * cols);
-    b.count = count;
   } else {
-    b.rect_lo = b.rect_hi = (uint32_t)kRectBias | ((uint32_t)kRectBias << 16);  // visible, no pixel of the window
+    b.rect_lo = 0u;  // visible, but its bbox holds no pixel of the window: no pairs
+    b.rect_hi = 0u;
     b.count = 0u;
   }
 }
