@@ -352,6 +352,7 @@ int enqueue_frame(splat_cuda_handle* h, const FrameParams& fp_in, uint8_t* dev_o
   h->inject_lost_us = 0;
   t.rec = h->rec;
   t.bin = h->bin;
+  t.skip = h->skip;
   t.counts = h->counts;
   t.out = dev_out;
   t.full = scratch ? h->full_dev : nullptr;
@@ -361,6 +362,7 @@ int enqueue_frame(splat_cuda_handle* h, const FrameParams& fp_in, uint8_t* dev_o
     t.s.order = nullptr;  // the records' order is the scene order
     t.rec = const_cast<Record*>(h->rx_rec);
     t.bin = h->rx_bin;
+    t.skip = h->rx_skip;
   }
   if (h->stage_events) CK(cudaEventRecord(h->ev[0], s), "event");
   if (records)
@@ -636,7 +638,8 @@ int create_impl(const splat_scene_desc* d, int device, splat_cuda_handle** out, 
     if ((rc = up((void**)&h->sh16, sh.data(), (size_t)planes * n * sizeof(uint16_t), "upload FP16 SH")))
       return bail(rc);
     if ((e = cudaMalloc(&h->rec, n * sizeof(Record))) != cudaSuccess) return bail(cuda_fail(h, e, "cudaMalloc records"));
-    if ((e = cudaMalloc(&h->bin, n * sizeof(BinInfo))) != cudaSuccess) return bail(cuda_fail(h, e, "cudaMalloc bins"));
+    if ((e = cudaMalloc(&h->bin, n * sizeof(BinInfo))) != cudaSuccess ||
+        (e = cudaMalloc(&h->skip, n * sizeof(BinSkip))) != cudaSuccess) return bail(cuda_fail(h, e, "cudaMalloc bins"));
   } else if (n) {
     // Upload in the device layout: float4 (pos, opacity), float4 + float4 for
     // the covariance (with k = sqrt(2 ln(opacity / ALPHA_MIN)), the bbox
@@ -678,7 +681,8 @@ int create_impl(const splat_scene_desc* d, int device, splat_cuda_handle** out, 
       if ((rc = up((void**)&h->sh, sh.data(), (size_t)rest * 3 * n * sizeof(float), "upload SH"))) return bail(rc);
     }
     if ((e = cudaMalloc(&h->rec, n * sizeof(Record))) != cudaSuccess) return bail(cuda_fail(h, e, "cudaMalloc records"));
-    if ((e = cudaMalloc(&h->bin, n * sizeof(BinInfo))) != cudaSuccess) return bail(cuda_fail(h, e, "cudaMalloc bins"));
+    if ((e = cudaMalloc(&h->bin, n * sizeof(BinInfo))) != cudaSuccess ||
+        (e = cudaMalloc(&h->skip, n * sizeof(BinSkip))) != cudaSuccess) return bail(cuda_fail(h, e, "cudaMalloc bins"));
 
   }
   int rc = ensure_pairs(h, std::max<uint64_t>(4 * n, 1u << 16));
@@ -885,6 +889,7 @@ SPLAT_API int splat_cuda_shard_records(splat_cuda_handle* h, const splat_view_de
   h->inject_lost_us = 0;
   t.rec = h->rec;
   t.bin = h->bin;
+  t.skip = h->skip;
   CK(launch_project(t, h->table, nullptr, nullptr, fc, s, &h->launches), "project kernel");
   CK(launch_shard_count(h->rec, h->bin, h->n, w, h->shard_scratch, h->shard_totals, s, &h->launches),
      "record selection kernels");
@@ -938,8 +943,10 @@ SPLAT_API int splat_cuda_render_records(splat_cuda_handle* h, const splat_view_d
   if (slots > h->rx_bin_cap) {  // with room for the next frames' counts to vary
     const uint64_t cap = slots + slots / 4;
     dfree(h->rx_bin);
+    dfree(h->rx_skip);
     h->rx_bin_cap = 0;
     CK(dmalloc(h, &h->rx_bin, cap * sizeof(BinInfo)), "cudaMalloc record binning input");
+    CK(dmalloc(h, &h->rx_skip, cap * sizeof(BinSkip)), "cudaMalloc record binning input");
     h->rx_bin_cap = cap;
   }
   FrameParams fp = make_params(*view, width, height, bg, 1);
@@ -1237,7 +1244,9 @@ SPLAT_API int splat_cuda_destroy(splat_cuda_handle* h) {
   dfree(h->cells_dev);
   dfree(h->rec);
   dfree(h->bin);
+  dfree(h->skip);
   dfree(h->rx_bin);
+  dfree(h->rx_skip);
   dfree(h->shard_scratch);
   dfree(h->shard_totals);
   if (h->shard_totals_host) cudaFreeHost(h->shard_totals_host);

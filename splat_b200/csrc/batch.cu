@@ -43,6 +43,7 @@ struct splat_cuda_batch {
   // per-view buffers (independent of the tile configuration)
   Record* rec = nullptr;
   BinInfo* bin = nullptr;
+  BinSkip* skip = nullptr;  // kept-tile lists of the wide rectangles
   std::vector<uint64_t> splat_off;  // first record of each view
   // plan (depends on the tile configuration)
   std::vector<ViewTask> tasks;
@@ -150,6 +151,7 @@ int plan(splat_cuda_batch* b) {
     t.s = scene_dev(h);
     t.rec = b->rec + b->splat_off[i];
     t.bin = b->bin + b->splat_off[i];
+    t.skip = b->skip + b->splat_off[i];
     t.out = v.dev_out;
     t.full = nullptr;
     t.rows = bin_rows(h->n, b->num_sms);
@@ -328,6 +330,7 @@ void destroy(splat_cuda_batch* b) {
   for (auto& p : b->pairs) dfree(p);
   dfree(b->rec);
   dfree(b->bin);
+  dfree(b->skip);
   for (auto& e : b->ev)
     if (e) cudaEventDestroy(e);
   for (auto& e : b->stage)
@@ -394,6 +397,8 @@ SPLAT_API int splat_cuda_batch_create(splat_cuda_handle* const* scenes, uint32_t
     return bail(bcuda(b, e, "cudaMalloc records"));
   if ((e = cudaMalloc(&b->bin, std::max<uint64_t>(splats, 1) * sizeof(BinInfo))) != cudaSuccess)
     return bail(bcuda(b, e, "cudaMalloc bins"));
+  if ((e = cudaMalloc(&b->skip, std::max<uint64_t>(splats, 1) * sizeof(BinSkip))) != cudaSuccess)
+    return bail(bcuda(b, e, "cudaMalloc bin skips"));
   int rc = ensure_pairs(b, std::max<uint64_t>(4 * splats, 1u << 16));
   if (rc) return bail(rc);
   if ((rc = prepare(b))) return bail(rc);

@@ -44,13 +44,14 @@ constexpr int kBinThreads = 512;
 // at most 32 pairs are expanded by their own lane; larger splats by the
 // whole warp, 32 tiles of a row at a time.
 template <class FW>
-__device__ __forceinline__ void for_each_pair(const BinInfo* __restrict__ bin, const uint32_t* __restrict__ order,
-                                              uint64_t s0, uint64_t s1, uint32_t tiles_x, FW&& fw) {
+__device__ __forceinline__ void for_each_pair(const BinInfo* __restrict__ bin, const BinSkip* __restrict__ skip,
+                                              const uint32_t* __restrict__ order, uint64_t s0, uint64_t s1,
+                                              uint32_t tiles_x, FW&& fw) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   constexpr uint64_t kStride = (uint64_t)kBinThreads;
   // The lane's splat of the warp's next group of 32 is loaded while the
   // current group's pairs are expanded.
-  const BinInfo culled{kCulled, 0u, 0u, 0u, {0u, 0u, 0u, 0u}};
+  const BinInfo culled{kCulled, 0u, 0u, 0u};
   auto splat_at = [&](uint64_t k) -> uint32_t { return order ? __ldg(order + k) : (uint32_t)k; };
   uint64_t wb = s0 + (uint64_t)warp * 32;
   uint32_t ni = wb + lane < s1 ? splat_at(wb + lane) : 0u;
@@ -65,29 +66,29 @@ __device__ __forceinline__ void for_each_pair(const BinInfo* __restrict__ bin, c
     } else {
       nb = culled;
     }
-    const uint32_t cnt = b.rect_lo != kCulled ? b.count : 0u;
-    const uint32_t mine = cnt <= 32 ? cnt : 0u;
     const uint32_t tx0 = b.rect_lo & 0xFFFFu, ty0 = b.rect_lo >> 16, tx1 = b.rect_hi & 0xFFFFu;
-    const uint32_t wdt0 = tx1 - tx0, area = wdt0 * ((b.rect_hi >> 16) - ty0);
-    if (mine && area <= kMaskTiles) {
+    const uint32_t wdt0 = tx1 - tx0, rows = (b.rect_hi >> 16) - ty0;
+    const bool small = b.rect_lo != kCulled && wdt0 * rows <= kMaskTiles;
+    const uint32_t cnt = b.rect_lo == kCulled ? 0u : (small ? (uint32_t)__popc(b.cm) : b.cm);
+    if (small) {
       // The rectangle's kept tiles, one bit each (row-major): the common
-      // case, one code path whether tiles are skipped or not. k / wdt0 for
-      // k < 32 as a multiply and shift.
-      const uint32_t inv = (65535u + wdt0) / wdt0;
-      uint32_t m = b.skip[0];
+      // case, one code path whether tiles are skipped or not. kb / wdt0 for
+      // kb < 32 as a multiply and shift.
+      const uint32_t inv = (65535u + wdt0) / max(wdt0, 1u);
+      uint32_t m = b.cm;
       while (m) {
         const uint32_t kb = (uint32_t)__ffs(m) - 1u;
         m &= m - 1u;
         const uint32_t row = (kb * inv) >> 16;
         fw((ty0 + row) * tiles_x + tx0 + (kb - row * wdt0), i, b.depth_bits);
       }
-    } else if (mine) {  // a larger rectangle culled to at most 32 pairs: each row's span
-      const uint32_t rows = (b.rect_hi >> 16) - ty0;
+    } else if (cnt && cnt <= 32) {  // a larger rectangle culled to at most 32 pairs: each row's span
+      const BinSkip sk = skip[i];
       uint32_t row = 0, a, e;
-      row_span(b, 0, tx0, tx1, a, e);
-      for (uint32_t q = 0; q < mine; q++) {
-        while (a == e && row + 1 < rows) row_span(b, ++row, tx0, tx1, a, e);
-        if (a == e) break;  // (count is the sum of the spans: not reached)
+      row_span(sk, 0, tx0, tx1, a, e);
+      for (uint32_t q = 0; q < cnt; q++) {
+        while (a == e && row + 1 < rows) row_span(sk, ++row, tx0, tx1, a, e);
+        if (a == e) break;  // (the count is the sum of the spans: not reached)
         fw((ty0 + row) * tiles_x + a, i, b.depth_bits);
         a++;
       }
@@ -96,15 +97,12 @@ __device__ __forceinline__ void for_each_pair(const BinInfo* __restrict__ bin, c
     while (big) {
       const int L = __ffs(big) - 1;
       big &= big - 1u;
-      BinInfo w;
-      w.rect_lo = __shfl_sync(0xffffffffu, b.rect_lo, L);
-      w.rect_hi = __shfl_sync(0xffffffffu, b.rect_hi, L);
-#pragma unroll
-      for (int q = 0; q < 4; q++) w.skip[q] = __shfl_sync(0xffffffffu, b.skip[q], L);
+      const uint32_t b_lo = __shfl_sync(0xffffffffu, b.rect_lo, L), b_hi = __shfl_sync(0xffffffffu, b.rect_hi, L);
       const uint32_t b_d = __shfl_sync(0xffffffffu, b.depth_bits, L), b_i = __shfl_sync(0xffffffffu, i, L);
       const uint32_t b_cnt = __shfl_sync(0xffffffffu, cnt, L);
-      const uint32_t btx0 = w.rect_lo & 0xFFFFu, bty0 = w.rect_lo >> 16;
-      const uint32_t btx1 = w.rect_hi & 0xFFFFu, brows = (w.rect_hi >> 16) - bty0, wdt = btx1 - btx0;
+      const BinSkip w = skip[b_i];  // the same words for every lane
+      const uint32_t btx0 = b_lo & 0xFFFFu, bty0 = b_lo >> 16;
+      const uint32_t btx1 = b_hi & 0xFFFFu, brows = (b_hi >> 16) - bty0, wdt = btx1 - btx0;
       if (!has_skips(w)) {
         for (uint32_t q = lane; q < b_cnt; q += 32) {
           const uint32_t row = q / wdt;
@@ -152,6 +150,7 @@ __device__ __forceinline__ void for_each_pair(const BinInfo* __restrict__ bin, c
 // The per-view fields the count and scatter CTAs need.
 struct BinView {
   const BinInfo* bin;
+  const BinSkip* skip;
   const uint32_t* order;  // the binning order (null: scene order)
   uint32_t* row;  // this CTA's row of the view's count matrix
   uint64_t s0, s1;
@@ -163,6 +162,7 @@ __device__ __forceinline__ BinView bin_view(const ViewTask* __restrict__ table, 
   const ViewTask* t = table + v;
   BinView b;
   b.bin = t->bin;
+  b.skip = t->skip;
   b.order = t->s.order;
   b.tiles_x = t->fp.tiles_x;
   b.tiles = t->fp.tiles_x * t->fp.tiles_y;
@@ -186,7 +186,7 @@ __global__ void __launch_bounds__(kBinThreads) k_bin_count(const ViewTask* __res
     __syncthreads();
   }
   uint32_t* const cnt = SMEM ? s_row : b.row;
-  for_each_pair(b.bin, b.order, b.s0, b.s1, b.tiles_x, [&](uint32_t t, uint32_t, uint32_t) { atomicAdd(&cnt[t], 1u); });
+  for_each_pair(b.bin, b.skip, b.order, b.s0, b.s1, b.tiles_x, [&](uint32_t t, uint32_t, uint32_t) { atomicAdd(&cnt[t], 1u); });
   if (SMEM) {
     __syncthreads();
     for (uint32_t t = threadIdx.x; t < b.tiles; t += kBinThreads) b.row[t] = s_row[t];
@@ -332,7 +332,7 @@ __global__ void __launch_bounds__(kBinThreads) k_bin_scatter(const ViewTask* __r
     for (uint32_t t = threadIdx.x; t < b.tiles; t += kBinThreads) s_row[t] = vr[t].x + b.row[t];
     __syncthreads();
   }
-  for_each_pair(b.bin, b.order, b.s0, b.s1, b.tiles_x, [&](uint32_t t, uint32_t i, uint32_t depth_bits) {
+  for_each_pair(b.bin, b.skip, b.order, b.s0, b.s1, b.tiles_x, [&](uint32_t t, uint32_t i, uint32_t depth_bits) {
     const uint64_t pos = SMEM ? atomicAdd(&s_row[t], 1u) : (uint64_t)vr[t].x + atomicAdd(&b.row[t], 1u);
     if (pos < cap) pairs[pos] = ((uint64_t)depth_bits << 32) | i;
   });

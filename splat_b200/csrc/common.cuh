@@ -106,16 +106,21 @@ struct __align__(16) Record {
 // Per-splat binning input written by the projection: the tile rectangle of
 // its pixel bbox clipped to the rendered window and counted from the
 // window's first tile row and column (tx0 | ty0 << 16, tx1 | ty1 << 16),
-// depth bits, its pair count, and which tiles of the rectangle it pairs
-// with. A rectangle of at most kMaskTiles tiles: bit k of skip[0] for its
-// k-th tile in row-major order. A larger one: per row r < kSkipRows the
-// tiles at the row's two ends that the splat does not reach (byte r of
-// `skip`: left | right << 4, each at most 15; kSkipEmpty: none of the row),
-// row r pairing with tiles [tx0 + left, tx1 - right); all zero: the whole
-// rectangle. rect_lo == kCulled marks a culled splat; a visible splat whose
-// bbox holds no pixel has count 0.
+// depth bits, and which tiles of the rectangle it pairs with: for a
+// rectangle of at most kMaskTiles tiles, `cm` has bit k set for its k-th
+// tile in row-major order (its pair count is the number of bits); for a
+// larger one, `cm` is its pair count and the splat's BinSkip says which
+// tiles are kept. rect_lo == kCulled marks a culled splat; a visible splat
+// whose bbox holds no pixel has no pairs (empty rectangle, cm = 0).
 struct __align__(16) BinInfo {
-  uint32_t rect_lo, rect_hi, depth_bits, count;
+  uint32_t rect_lo, rect_hi, depth_bits, cm;
+};
+// The kept tiles of a rectangle of more than kMaskTiles tiles, written only
+// for those: per row r < kSkipRows, the tiles at the row's two ends that the
+// splat does not reach (byte r: left | right << 4, each at most 15;
+// kSkipEmpty: none of the row), row r pairing with tiles [tx0 + left,
+// tx1 - right); all zero: the whole rectangle.
+struct __align__(16) BinSkip {
   uint32_t skip[4];
 };
 constexpr uint32_t kSkipRows = 16;
@@ -124,15 +129,24 @@ constexpr uint32_t kMaskTiles = 32;
 
 __host__ __device__ __forceinline__ uint32_t low_bits(uint32_t n) { return n >= 32u ? ~0u : (1u << n) - 1u; }
 
-__device__ __forceinline__ bool has_skips(const BinInfo& b) {
-  return (b.skip[0] | b.skip[1] | b.skip[2] | b.skip[3]) != 0u;
+__device__ __forceinline__ uint32_t rect_area(const BinInfo& b) {
+  return ((b.rect_hi & 0xFFFFu) - (b.rect_lo & 0xFFFFu)) * ((b.rect_hi >> 16) - (b.rect_lo >> 16));
+}
+// The splat's pair count (0 for a culled splat).
+__device__ __forceinline__ uint32_t bin_count(const BinInfo& b) {
+  if (b.rect_lo == kCulled) return 0u;
+  return rect_area(b) <= kMaskTiles ? (uint32_t)__popc(b.cm) : b.cm;
+}
+
+__device__ __forceinline__ bool has_skips(const BinSkip& k) {
+  return (k.skip[0] | k.skip[1] | k.skip[2] | k.skip[3]) != 0u;
 }
 
 // Row r's tile span [a, e) of the rectangle [tx0, tx1) (empty: a == e).
-__device__ __forceinline__ void row_span(const BinInfo& b, uint32_t r, uint32_t tx0, uint32_t tx1, uint32_t& a,
+__device__ __forceinline__ void row_span(const BinSkip& k, uint32_t r, uint32_t tx0, uint32_t tx1, uint32_t& a,
                                          uint32_t& e) {
-  // The word by selects, not by a dynamic index (which would put b in local memory).
-  const uint32_t word = r < 8u ? (r < 4u ? b.skip[0] : b.skip[1]) : (r < 12u ? b.skip[2] : b.skip[3]);
+  // The word by selects, not by a dynamic index (which would put k in local memory).
+  const uint32_t word = r < 8u ? (r < 4u ? k.skip[0] : k.skip[1]) : (r < 12u ? k.skip[2] : k.skip[3]);
   const uint32_t sk = r < kSkipRows ? (word >> (8u * (r & 3u))) & 255u : 0u;
   a = sk == kSkipEmpty ? tx1 : tx0 + (sk & 15u);
   e = sk == kSkipEmpty ? tx1 : tx1 - (sk >> 4);
@@ -177,15 +191,15 @@ __device__ __forceinline__ float sqrt_hw(float x) {
 // part [wtx0, wtx1) x [wty0, wty1): a frame drawn in windows has exactly the
 // pairs of the frame drawn at once. Every operation rounds explicitly, so
 // the projection and the records' binning input (different translation
-// units and contraction flags) compute the same skips. Sets b.skip and
-// returns the pair count.
-__device__ __forceinline__ uint32_t ellipse_skips(const FrameParams& fp, const Record& r, uint32_t ftx0, uint32_t ftx1,
-                                                  uint32_t fty0, uint32_t fty1, uint32_t wtx0, uint32_t wtx1,
-                                                  uint32_t wty0, uint32_t wty1, BinInfo& b) {
+// units and contraction flags) compute the same skips. Sets b.cm (the mask,
+// or the pair count) and, for a rectangle of more than kMaskTiles tiles, k.
+__device__ __forceinline__ void ellipse_skips(const FrameParams& fp, const Record& r, uint32_t ftx0, uint32_t ftx1,
+                                              uint32_t fty0, uint32_t fty1, uint32_t wtx0, uint32_t wtx1,
+                                              uint32_t wty0, uint32_t wty1, BinInfo& b, BinSkip& k) {
   const uint32_t wcols = wtx1 - wtx0, wrows = wty1 - wty0, all = wcols * wrows;
   const bool masked = all <= kMaskTiles;
-  if (masked) b.skip[0] = low_bits(all);  // whole, unless narrowed below
-  if (ftx1 - ftx0 == 1u && fty1 - fty0 == 1u) return all;  // the centre's own tile
+  b.cm = masked ? low_bits(all) : all;  // whole, unless narrowed below
+  if (ftx1 - ftx0 == 1u && fty1 - fty0 == 1u) return;  // the centre's own tile
   const float a = __fmul_rn(-2.0f, r.r0.z), bb = -r.r0.w, c = __fmul_rn(-2.0f, r.r1.x);
   // det = ac - b^2 with b^2's rounding error carried (two-product): no
   // cancellation for thin ellipses.
@@ -194,7 +208,7 @@ __device__ __forceinline__ uint32_t ellipse_skips(const FrameParams& fp, const R
   // K = 2 ln 2 (log2 op + log2 255), widened.
   const float K0 = __fmul_rn(1.38629436f, __fadd_rn(lg2_hw(r.r1.y), 7.99435344f));
   const float K = __fadd_rn(__fmul_rn(K0, 1.002f), 0.002f);
-  if (!(det > 0.0f && a > 0.0f && c > 0.0f && K > 0.0f)) return all;
+  if (!(det > 0.0f && a > 0.0f && c > 0.0f && K > 0.0f)) return;
   const float inv_det = rcp_hw(det), inv_a = rcp_hw(a);
   const float aK = __fmul_rn(a, K);
   const float ey = sqrt_hw(__fmul_rn(aK, inv_det));                          // vertical half-extent
@@ -242,16 +256,15 @@ __device__ __forceinline__ uint32_t ellipse_skips(const FrameParams& fp, const R
     const uint32_t byte = ce == ca ? kSkipEmpty : (ca - wtx0) | ((wtx1 - ce) << 4);
     const uint32_t sh = 8u * (q & 3u);
     if (q < 4u)
-      b.skip[0] |= byte << sh;
+      k.skip[0] |= byte << sh;
     else if (q < 8u)
-      b.skip[1] |= byte << sh;
+      k.skip[1] |= byte << sh;
     else if (q < 12u)
-      b.skip[2] |= byte << sh;
+      k.skip[2] |= byte << sh;
     else
-      b.skip[3] |= byte << sh;
+      k.skip[3] |= byte << sh;
   }
-  if (masked) b.skip[0] = mask;
-  return count;
+  b.cm = masked ? mask : count;
 }
 
 // The tile rectangle of a splat whose pixel bbox (pixel_bbox,
@@ -261,31 +274,31 @@ __device__ __forceinline__ uint32_t ellipse_skips(const FrameParams& fp, const R
 // that holds no pixel of the window gives the empty rectangle (no pairs).
 // Unless the frame asks for the bbox pairs (kFrameBboxPairs), the rows' end
 // tiles the splat's ellipse does not reach are skipped (ellipse_skips, from
-// the splat's record r).
-__device__ __forceinline__ void window_rect(const FrameParams& fp, uint32_t bx0, uint32_t x1, uint32_t by0,
-                                            uint32_t y1, const Record& r, BinInfo& b) {
+// the splat's record r). Returns whether k is needed (a rectangle of more
+// than kMaskTiles tiles: the caller stores it).
+__device__ __forceinline__ bool window_rect(const FrameParams& fp, uint32_t bx0, uint32_t x1, uint32_t by0,
+                                            uint32_t y1, const Record& r, BinInfo& b, BinSkip& k) {
   const uint32_t ftx0 = bx0 >> fp.tile_sx, ftx1 = (x1 + fp.tile_w - 1) >> fp.tile_sx;
   const uint32_t fty0 = by0 >> fp.tile_sy, fty1 = (y1 + fp.tile_h - 1) >> fp.tile_sy;
   const uint32_t wty0 = max(fty0, fp.win_ty0), wty1 = min(fty1, fp.win_ty0 + fp.tiles_y);
   const uint32_t wtx0 = max(ftx0, fp.win_tx0), wtx1 = min(ftx1, fp.win_tx0 + fp.tiles_x);
-  b.skip[0] = b.skip[1] = b.skip[2] = b.skip[3] = 0u;
+  k.skip[0] = k.skip[1] = k.skip[2] = k.skip[3] = 0u;
   if (bx0 < x1 && by0 < y1 && wty0 < wty1 && wtx0 < wtx1) {
     const uint32_t tx0 = wtx0 - fp.win_tx0, ty0 = wty0 - fp.win_ty0;
     const uint32_t tx1 = wtx1 - fp.win_tx0, ty1 = wty1 - fp.win_ty0;
     b.rect_lo = tx0 | (ty0 << 16);
     b.rect_hi = tx1 | (ty1 << 16);
     const uint32_t area = (tx1 - tx0) * (ty1 - ty0);
-    if (fp.flags & kFrameBboxPairs) {
-      b.count = area;
-      if (area <= kMaskTiles) b.skip[0] = low_bits(area);
-    } else {
-      b.count = ellipse_skips(fp, r, ftx0, ftx1, fty0, fty1, wtx0, wtx1, wty0, wty1, b);
-    }
-  } else {
-    b.rect_lo = 0u;  // visible, but its bbox holds no pixel of the window: no pairs
-    b.rect_hi = 0u;
-    b.count = 0u;
+    if (fp.flags & kFrameBboxPairs)
+      b.cm = area <= kMaskTiles ? low_bits(area) : area;
+    else
+      ellipse_skips(fp, r, ftx0, ftx1, fty0, fty1, wtx0, wtx1, wty0, wty1, b, k);
+    return area > kMaskTiles;
   }
+  b.rect_lo = 0u;  // visible, but its bbox holds no pixel of the window: no pairs
+  b.rect_hi = 0u;
+  b.cm = 0u;
+  return false;
 }
 
 // Per-tile depth sort sizes: tiles up to kWarpSortCap pairs are sorted by one
@@ -354,6 +367,7 @@ struct ViewTask {
   SceneDev s;
   Record* rec;          // n records of this view
   BinInfo* bin;         // n tile rectangles of this view
+  BinSkip* skip;        // n kept-tile lists (for rectangles of more than kMaskTiles tiles)
   uint32_t* counts;     // rows x tiles count matrix
   uint8_t* out;         // device frame, out_w * out_h * 3 bytes
   uint8_t* full;        // full-resolution scratch for a downsample factor
@@ -363,7 +377,7 @@ struct ViewTask {
   uint32_t proj_cta0;   // first CTA of the view in the projection launch
   uint32_t bin_cta0;    // ... in the count and scatter launches
   uint32_t col_cta0;    // ... in the column-scan launch
-  uint32_t pad[1];      // learned-colour batch table: the view's batch index
+  uint32_t pad[3];      // pad[0], learned-colour batch table: the view's batch index
 };
 
 // The view whose `field` (a first-CTA or first-tile member) is the largest

@@ -31,6 +31,7 @@ struct splat_cuda_handle {
   // per-splat frame buffers
   splat::Record* rec = nullptr;
   splat::BinInfo* bin = nullptr;
+  splat::BinSkip* skip = nullptr;  // kept-tile lists of the wide rectangles
   // splat-sharded frames: the records a splat_cuda_render_records call draws
   // (caller-owned device memory, set for the duration of the call) and their
   // binning input; the record selection's scratch and host copy of its totals
@@ -38,6 +39,7 @@ struct splat_cuda_handle {
   const splat::Record* rx_rec = nullptr;
   uint64_t rx_n = 0;
   splat::BinInfo* rx_bin = nullptr;
+  splat::BinSkip* rx_skip = nullptr;
   uint64_t rx_bin_cap = 0;
   void* shard_scratch = nullptr;
   size_t shard_scratch_cap = 0;

@@ -85,7 +85,8 @@ __device__ __forceinline__ Src scene_source(const SceneDev& s, const Src* given)
 template <int DEG, bool F16, bool LEARNED = false, class Src = GlobalScene>
 __device__ __forceinline__ void project_splat(const FrameParams& fp, const SceneDev& s, uint64_t i,
                                               Record* __restrict__ rec, BinInfo* __restrict__ bin,
-                                              float* __restrict__ dbg_proj, float* __restrict__ dbg_color,
+                                              BinSkip* __restrict__ skip, float* __restrict__ dbg_proj,
+                                              float* __restrict__ dbg_color,
                                               bool& vis, bool& used_fp64, float* dir = nullptr,
                                               const Src* given = nullptr) {
   const Src src = scene_source<Src>(s, given);
@@ -124,7 +125,9 @@ __device__ __forceinline__ void project_splat(const FrameParams& fp, const Scene
       opacity = po.w;
       k = 0.0f;
     }
-    BinInfo b{kCulled, 0u, 0u, 0u, {0u, 0u, 0u, 0u}};
+    BinInfo b{kCulled, 0u, 0u, 0u};
+    BinSkip bk;
+    bool wide = false;  // bk is stored
     float out_x = 0.f, out_y = 0.f, out_ex = 0.f, out_ey = 0.f, out_depth = 0.f, c0 = 0.f, c1 = 0.f, c2 = 0.f;
     float col[3] = {0.f, 0.f, 0.f};
     do {
@@ -255,7 +258,7 @@ __device__ __forceinline__ void project_splat(const FrameParams& fp, const Scene
       r.r2 = make_float4(col[2], __uint_as_float(bx0 | (x1 << 16)), __uint_as_float(by0 | (y1 << 16)), tz);
       rec[i] = r;
       b.depth_bits = __float_as_uint(tz);
-      window_rect(fp, bx0, x1, by0, y1, r, b);
+      wide = window_rect(fp, bx0, x1, by0, y1, r, b, bk);
       vis = true;
       out_x = x;
       out_y = y;
@@ -264,6 +267,7 @@ __device__ __forceinline__ void project_splat(const FrameParams& fp, const Scene
       out_depth = tz;
     } while (false);
     bin[i] = b;
+    if (wide) skip[i] = bk;
     if (dbg_proj) {
       float* d = dbg_proj + 8 * i;
       d[0] = out_x; d[1] = out_y; d[2] = out_ex; d[3] = out_ey; d[4] = out_depth; d[5] = c0; d[6] = c1; d[7] = c2;
@@ -297,7 +301,7 @@ __global__ void __launch_bounds__(256) k_project(ViewTask t, ViewTask* __restric
   if (blockIdx.x == 0 && threadIdx.x == 0) *table = t;
   const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   bool vis = false, used_fp64 = false;
-  if (i < t.s.n) project_splat<DEG, F16>(t.fp, t.s, i, t.rec, t.bin, dbg_proj, dbg_color, vis, used_fp64);
+  if (i < t.s.n) project_splat<DEG, F16>(t.fp, t.s, i, t.rec, t.bin, t.skip, dbg_proj, dbg_color, vis, used_fp64);
   count_visible(vis, used_fp64, fc, 0);
 }
 
@@ -401,7 +405,7 @@ __global__ void __launch_bounds__(kTmaSplats) k_project_tma(ViewTask t, ViewTask
     umma::mbar_wait(mbar, 0, 100000000ull);
   } else if (tid < cnt) {
     const SmemScene src{s_pos, s_ca, s_cb, s_planes, s_off, base};
-    project_splat<DEG, false, false, SmemScene>(t.fp, t.s, base + tid, t.rec, t.bin, dbg_proj, dbg_color, vis,
+    project_splat<DEG, false, false, SmemScene>(t.fp, t.s, base + tid, t.rec, t.bin, t.skip, dbg_proj, dbg_color, vis,
                                                 used_fp64, nullptr, &src);
   }
   count_visible(vis, used_fp64, fc, 0);
@@ -422,14 +426,14 @@ __global__ void __launch_bounds__(256) k_project_batch(const ViewTask* __restric
   bool vis = false, used_fp64 = false;
   if (i < s_t.s.n) {
     switch (s_t.s.sh_degree * 2 + (s_t.s.fp16 ? 1 : 0)) {
-      case 0: project_splat<0, false>(s_t.fp, s_t.s, i, s_t.rec, s_t.bin, nullptr, nullptr, vis, used_fp64); break;
-      case 1: project_splat<0, true>(s_t.fp, s_t.s, i, s_t.rec, s_t.bin, nullptr, nullptr, vis, used_fp64); break;
-      case 2: project_splat<1, false>(s_t.fp, s_t.s, i, s_t.rec, s_t.bin, nullptr, nullptr, vis, used_fp64); break;
-      case 3: project_splat<1, true>(s_t.fp, s_t.s, i, s_t.rec, s_t.bin, nullptr, nullptr, vis, used_fp64); break;
-      case 4: project_splat<2, false>(s_t.fp, s_t.s, i, s_t.rec, s_t.bin, nullptr, nullptr, vis, used_fp64); break;
-      case 5: project_splat<2, true>(s_t.fp, s_t.s, i, s_t.rec, s_t.bin, nullptr, nullptr, vis, used_fp64); break;
-      case 6: project_splat<3, false>(s_t.fp, s_t.s, i, s_t.rec, s_t.bin, nullptr, nullptr, vis, used_fp64); break;
-      default: project_splat<3, true>(s_t.fp, s_t.s, i, s_t.rec, s_t.bin, nullptr, nullptr, vis, used_fp64); break;
+      case 0: project_splat<0, false>(s_t.fp, s_t.s, i, s_t.rec, s_t.bin, s_t.skip, nullptr, nullptr, vis, used_fp64); break;
+      case 1: project_splat<0, true>(s_t.fp, s_t.s, i, s_t.rec, s_t.bin, s_t.skip, nullptr, nullptr, vis, used_fp64); break;
+      case 2: project_splat<1, false>(s_t.fp, s_t.s, i, s_t.rec, s_t.bin, s_t.skip, nullptr, nullptr, vis, used_fp64); break;
+      case 3: project_splat<1, true>(s_t.fp, s_t.s, i, s_t.rec, s_t.bin, s_t.skip, nullptr, nullptr, vis, used_fp64); break;
+      case 4: project_splat<2, false>(s_t.fp, s_t.s, i, s_t.rec, s_t.bin, s_t.skip, nullptr, nullptr, vis, used_fp64); break;
+      case 5: project_splat<2, true>(s_t.fp, s_t.s, i, s_t.rec, s_t.bin, s_t.skip, nullptr, nullptr, vis, used_fp64); break;
+      case 6: project_splat<3, false>(s_t.fp, s_t.s, i, s_t.rec, s_t.bin, s_t.skip, nullptr, nullptr, vis, used_fp64); break;
+      default: project_splat<3, true>(s_t.fp, s_t.s, i, s_t.rec, s_t.bin, s_t.skip, nullptr, nullptr, vis, used_fp64); break;
     }
   }
   count_visible(vis, used_fp64, fc, v);
@@ -536,7 +540,7 @@ __global__ void __launch_bounds__(kLearnedThreads, 7)
     if (i < n) {
       l0 = __ldg(t.s.lat16 + 2 * i);  // in flight during the projection
       l1 = __ldg(t.s.lat16 + 2 * i + 1);
-      project_splat<0, true, true>(t.fp, t.s, i, t.rec, t.bin, dbg_proj, nullptr, vis, used_fp64, dir);
+      project_splat<0, true, true>(t.fp, t.s, i, t.rec, t.bin, t.skip, dbg_proj, nullptr, vis, used_fp64, dir);
     }
     mlp::store_input(S.t.act, 0, tid, l0, l1, dir[0], dir[1], dir[2]);
     if (sync_or_abort()) { aborted = true; break; }

@@ -42,8 +42,7 @@ uint32_t shard_ctas(uint64_t n) { return (uint32_t)((shard_chunks(n) + kShardWar
 // holds a pixel of the frame (the projection ran over the whole frame).
 __device__ __forceinline__ bool splat_rows(const Record* __restrict__ rec, const BinInfo* __restrict__ bin, uint64_t i,
                                            uint32_t& y0, uint32_t& y1) {
-  const BinInfo b = bin[i];
-  if (b.rect_lo == kCulled || b.count == 0u) return false;
+  if (bin_count(bin[i]) == 0u) return false;
   const uint32_t yb = __float_as_uint(rec[i].r2.z);
   y0 = yb & 0xFFFFu;
   y1 = yb >> 16;
@@ -162,8 +161,9 @@ __global__ void __launch_bounds__(256) k_records_bin(const ViewTask t, ViewTask*
     const Record r = t.rec[i];
     const uint32_t xb = __float_as_uint(r.r2.y), yb = __float_as_uint(r.r2.z);
     BinInfo b;
+    BinSkip k;
     b.depth_bits = __float_as_uint(r.r2.w);
-    window_rect(t.fp, xb & 0xFFFFu, xb >> 16, yb & 0xFFFFu, yb >> 16, r, b);
+    if (window_rect(t.fp, xb & 0xFFFFu, xb >> 16, yb & 0xFFFFu, yb >> 16, r, b, k)) t.skip[i] = k;
     t.bin[i] = b;
   }
   const uint32_t c = (uint32_t)__syncthreads_count(v);
