@@ -314,7 +314,7 @@ __global__ void __launch_bounds__(256) k_project(ViewTask t, ViewTask* __restric
 // copy starts at the 16-byte boundary below it (the plane buffers carry 16
 // bytes of slack at their end for the rounded-up last copy) and the slice is
 // read at its offset. The arithmetic is project_splat's, unchanged.
-constexpr uint32_t kTmaSplats = 256;
+constexpr uint32_t kTmaSplats = 128;  // 32 KB of slices per CTA (SH3): 7 CTAs per SM
 constexpr uint32_t kTmaPlaneFloats = kTmaSplats + 8;  // the slice, its offset and the rounding
 
 template <int DEG>
@@ -620,7 +620,7 @@ cudaError_t launch_project(const ViewTask& t, ViewTask* table, float* dbg_proj, 
   }
   // An empty scene still stores the view table.
   const unsigned grid = t.s.n ? (unsigned)((t.s.n + 255) / 256) : 1u;
-  static_assert(kTmaSplats == 256, "one CTA of the TMA projection per 256 splats");
+  const unsigned grid_tma = t.s.n ? (unsigned)((t.s.n + kTmaSplats - 1) / kTmaSplats) : 1u;
 #define SPLAT_PROJECT(D)                                                                                        \
   do {                                                                                                          \
     if (t.s.fp16 || t.s.n == 0) {                                                                               \
@@ -639,7 +639,7 @@ cudaError_t launch_project(const ViewTask& t, ViewTask* table, float* dbg_proj, 
         if (ae != cudaSuccess) return ae;                                                                       \
         attr_set[dev & 63] = true;                                                                              \
       }                                                                                                         \
-      k_project_tma<D><<<grid, kTmaSplats, TmaLayout<D>::kBytes, stream>>>(t, table, dbg_proj, dbg_color, fc);  \
+      k_project_tma<D><<<grid_tma, kTmaSplats, TmaLayout<D>::kBytes, stream>>>(t, table, dbg_proj, dbg_color, fc);  \
     }                                                                                                           \
   } while (0)
   switch (t.s.sh_degree) {
