@@ -73,8 +73,10 @@ __device__ __forceinline__ void for_each_pair(const BinInfo* __restrict__ bin, c
     if (small) {
       // The rectangle's kept tiles, one bit each (row-major): the common
       // case, one code path whether tiles are skipped or not. kb / wdt0 for
-      // kb < 32 as a multiply and shift.
-      const uint32_t inv = (65535u + wdt0) / max(wdt0, 1u);
+      // kb < 32 as a multiply and shift: inv = floor(65536 / wdt0) + 1 from
+      // the hardware reciprocal (exact for powers of two; otherwise
+      // 65536 / wdt0 lies at least 1/32 from an integer, far beyond its error).
+      const uint32_t inv = (uint32_t)(rcp_hw((float)max(wdt0, 1u)) * 65536.0f) + 1u;
       uint32_t m = b.cm;
       while (m) {
         const uint32_t kb = (uint32_t)__ffs(m) - 1u;
