@@ -40,9 +40,9 @@ constexpr int kBinThreads = 512;
 
 // Calls fw(tile, splat, depth bits) for every pair of the splats at
 // positions [s0, s1) of the binning order (SceneDev::order; null: scene
-// order): row by row, the tiles of each row's span (row_span). Splats with
-// at most 32 pairs are expanded by their own lane; larger splats by the
-// whole warp, 32 tiles of a row at a time.
+// order). A splat whose rectangle holds at most kMaskTiles tiles is expanded
+// by its own lane from its bit mask; a larger one by the whole warp, row by
+// row of its spans (row_span).
 template <class FW>
 __device__ __forceinline__ void for_each_pair(const BinInfo* __restrict__ bin, const BinSkip* __restrict__ skip,
                                               const uint32_t* __restrict__ order, uint64_t s0, uint64_t s1,
@@ -84,18 +84,10 @@ __device__ __forceinline__ void for_each_pair(const BinInfo* __restrict__ bin, c
         const uint32_t row = (kb * inv) >> 16;
         fw((ty0 + row) * tiles_x + tx0 + (kb - row * wdt0), i, b.depth_bits);
       }
-    } else if (cnt && cnt <= 32) {  // a larger rectangle culled to at most 32 pairs: each row's span
-      const BinSkip sk = skip[i];
-      uint32_t row = 0, a, e;
-      row_span(sk, 0, tx0, tx1, a, e);
-      for (uint32_t q = 0; q < cnt; q++) {
-        while (a == e && row + 1 < rows) row_span(sk, ++row, tx0, tx1, a, e);
-        if (a == e) break;  // (the count is the sum of the spans: not reached)
-        fw((ty0 + row) * tiles_x + a, i, b.depth_bits);
-        a++;
-      }
     }
-    uint32_t big = __ballot_sync(0xffffffffu, cnt > 32);
+    // Larger rectangles (at most 32 pairs or not) go through the whole warp,
+    // so that no lane runs a long per-row loop while the others wait.
+    uint32_t big = __ballot_sync(0xffffffffu, !small && cnt > 0);
     while (big) {
       const int L = __ffs(big) - 1;
       big &= big - 1u;
