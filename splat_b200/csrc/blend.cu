@@ -220,7 +220,56 @@ struct __align__(16) StagedBatch {
   float2 c[G];  // see staged_colour
   uint32_t mx[G];
   uint32_t my[G];
+  uint32_t wm[G];  // the warp blocks the splat reaches (block_mask)
 };
+
+// The warp blocks of the tile at (ox, oy) that hold a pixel centre the
+// splat (record r) reaches: bit w for the group's warp w (block column
+// w % WCOLS, row w / WCOLS, 8 x BH pixels), among those its bbox masks
+// (mx, my) meet. As the projection bounds the tiles (ellipse_skips): with
+// the conic (a, b, c) and K = 2 ln(255 opacity), alpha >= 1/255 where
+// a dx^2 + 2 b dx dy + c dy^2 <= K; per block row, the ellipse's x range in
+// the row's band of pixel-centre rows, from its leftmost and rightmost
+// points clamped into the band (K widened by 0.2 % + 0.002, the range by
+// 0.01 px). A block left out holds only pixels whose alpha test fails, so
+// leaving it out of the warp's list changes no pixel. A splat the test
+// cannot bound keeps every block its bbox meets.
+template <class S>
+__device__ __forceinline__ uint32_t block_mask(const Record& r, uint32_t ox, uint32_t oy, uint32_t mx, uint32_t my) {
+  constexpr int BROWS = S::GW / S::WCOLS;
+  uint32_t box = 0;  // the blocks the bbox meets
+#pragma unroll
+  for (int by = 0; by < BROWS; by++)
+    if (my & (((1u << S::BH) - 1u) << (by * S::BH)))
+#pragma unroll
+      for (int bx = 0; bx < S::WCOLS; bx++)
+        if (mx & (0xFFu << (bx * 8))) box |= 1u << (by * S::WCOLS + bx);
+  if (__popc(box) <= 1) return box;
+  const float a = -2.0f * r.r0.z, bb = -r.r0.w, c = -2.0f * r.r1.x;
+  const float p = bb * bb, det = fmaf(a, c, -p) - fmaf(bb, bb, -p);
+  const float K = fmaf(1.38629436f * (lg2_hw(r.r1.y) + 7.99435344f), 1.002f, 0.002f);
+  if (!(det > 0.0f && a > 0.0f && c > 0.0f && K > 0.0f)) return box;
+  const float inv_det = rcp_hw(det), inv_a = rcp_hw(a), aK = a * K;
+  const float ey = sqrt_hw(aK * inv_det), xm = sqrt_hw(c * K * inv_det);
+  const float dyr = -bb * xm * rcp_hw(c);
+  uint32_t m = 0;
+#pragma unroll
+  for (int by = 0; by < BROWS; by++) {
+    if (!((box >> (by * S::WCOLS)) & ((1u << S::WCOLS) - 1u))) continue;
+    const float band0 = (float)(oy + by * S::BH) + 0.5f - r.r0.y, band1 = band0 + (float)(S::BH - 1);
+    if (band1 < -ey || band0 > ey) continue;
+    const float lo = fmaxf(band0, -ey), hi = fminf(band1, ey);
+    const float yr = fminf(fmaxf(dyr, lo), hi), yl = fminf(fmaxf(-dyr, lo), hi);
+    const float sr = sqrt_hw(fmaxf(aK - det * yr * yr, 0.0f)), sl = sqrt_hw(fmaxf(aK - det * yl * yl, 0.0f));
+    const float xu = r.r0.x + (sr - bb * yr) * inv_a + 0.01f, xl = r.r0.x - (sl + bb * yl) * inv_a - 0.01f;
+#pragma unroll
+    for (int bx = 0; bx < S::WCOLS; bx++) {
+      const float c0 = (float)(ox + bx * 8) + 0.5f;
+      if (c0 + 7.0f >= xl && c0 <= xu) m |= 1u << (by * S::WCOLS + bx);
+    }
+  }
+  return m & box;
+}
 
 // The default shape (16x16 tiles, two groups of 256 threads per CTA) sorts
 // each tile of at most kMidSortCap pairs itself, before blending it (the
@@ -429,8 +478,6 @@ __global__ void __launch_bounds__(NT, NT == 512 ? 2 : (NT == 256 ? 5 : 8)) k_ble
   const uint32_t wbx = gw % S::WCOLS, wby = gw / S::WCOLS;
   const uint32_t lx = wbx * 8 + (lane & 7);
   const uint32_t ly0 = wby * S::BH + (lane >> 3) * PPT;
-  const uint32_t wxbits = 0xFFu << (wbx * 8);
-  const uint32_t wybits = ((1u << S::BH) - 1u) << (wby * S::BH);
 
   // Tiles are taken by pair-count class (tile_class), each class's list in
   // the order k_tile_ranges appended it.
@@ -529,6 +576,7 @@ __global__ void __launch_bounds__(NT, NT == 512 ? 2 : (NT == 256 ? 5 : 8)) k_ble
       const int y0 = min(max((int)(by & 0xFFFFu) - (int)oy, 0), TH), y1 = min(max((int)(by >> 16) - (int)oy, 0), TH);
       d.mx[gt] = x1 > x0 ? bit_range(x0, x1) : 0u;
       d.my[gt] = y1 > y0 ? bit_range(y0, y1) : 0u;
+      d.wm[gt] = block_mask<S>(nr, ox, oy, d.mx[gt], d.my[gt]);
       if (EXACT) {
         d.a[gt] = nr.r0;
         d.b[gt] = nr.r1;
@@ -559,7 +607,7 @@ __global__ void __launch_bounds__(NT, NT == 512 ? 2 : (NT == 256 ? 5 : 8)) k_ble
       if (__any_sync(0xffffffffu, !all_done)) {
         for (uint32_t c0 = 0; c0 < cnt; c0 += 32) {
           const uint32_t e = c0 + lane;
-          const bool hit = e < cnt && (bt.mx[e] & wxbits) && (bt.my[e] & wybits);
+          const bool hit = e < cnt && ((bt.wm[e] >> gw) & 1u);
           const uint32_t bal = __ballot_sync(0xffffffffu, hit);
           if (hit) sm.b.list[gw][len + __popc(bal & ((1u << lane) - 1u))] = (uint16_t)e;
           len += __popc(bal);
