@@ -2,7 +2,9 @@
 // sort of tiles too long to sort inside the blend CTA.
 //
 // Every visible splat duplicates into one pair per tile of its pixel bbox
-// (src/render/cpu.rs:251-277). The reference buckets pairs with a counting
+// (src/render/cpu.rs:251-277) that its alpha = 1/255 ellipse reaches (every
+// bbox tile with kFrameBboxPairs; the projection marks the tiles in the
+// splat's BinInfo / BinSkip). The reference buckets pairs with a counting
 // sort by tile (cpu.rs:149-199): per-group tile histograms, a prefix over
 // (tile, group), then a scatter. The same scheme here, with CTAs as groups:
 //

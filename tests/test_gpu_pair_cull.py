@@ -84,8 +84,9 @@ def _pairs(r, view, w, h, bbox):
     return d
 
 
-def test_left_out_pairs_miss_the_ellipse():
-    s = scenes.clusters(20_000, seed=7, sh_degree=3)
+@pytest.mark.parametrize("name", ["clusters", "needles"])
+def test_left_out_pairs_miss_the_ellipse(name):
+    s = scenes.clusters(20_000, seed=7, sh_degree=3) if name == "clusters" else scenes.needles(20_000, seed=5)
     w, h = 640, 360
     r = CudaRenderer(s)
     r.set_option(N.SPLAT_OPT_DEBUG_CAPTURE, 1)
@@ -111,7 +112,9 @@ def test_left_out_pairs_miss_the_ellipse():
                 left = np.setdiff1d(fv, cv)
                 gone_t += [t] * len(left)
                 gone_i += list(left)
-            assert kept == len(cut["keys"]) and kept < len(full["keys"])
+            assert kept == len(cut["keys"]) and kept <= len(full["keys"])
+            if not gone_i:
+                continue
             # every left-out pair: the tile's pixel-centre rectangle misses the ellipse
             p = cut["proj"].astype(np.float64)
             gi = np.array(gone_i, np.int64)
