@@ -168,7 +168,7 @@ int plan(splat_cuda_batch* b) {
       b->ltasks.back().proj_cta0 = (uint32_t)b->learned_tiles;
       b->learned_tiles += (h->n + 127) / 128;
     } else {
-      proj += (h->n + 255) / 256;
+      proj += (h->n + kProjectSplatsPerCta - 1) / kProjectSplatsPerCta;
     }
     bins += t.rows;
     cols += (tiles + 31) / 32;

@@ -417,6 +417,8 @@ bool blend_writes_host_rows(const BlendConfig& c, bool exact);
 // or of every view of the table (batch).
 cudaError_t launch_project(const ViewTask& t, ViewTask* table, float* dbg_proj, float* dbg_color,
                            const FrameCounters& fc, cudaStream_t stream, uint32_t* launches);
+// (Each CTA of the batch projection takes kProjectSplatsPerCta splats of one view.)
+constexpr uint32_t kProjectSplatsPerCta = 128;
 cudaError_t launch_project_batch(const ViewTask* table, uint32_t n_views, uint32_t total_ctas,
                                  const FrameCounters& fc, cudaStream_t stream, uint32_t* launches);
 // The learned-colour views of a batch: `table` holds n_views copies of them

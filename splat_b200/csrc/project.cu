@@ -314,7 +314,7 @@ __global__ void __launch_bounds__(256) k_project(ViewTask t, ViewTask* __restric
 // copy starts at the 16-byte boundary below it (the plane buffers carry 16
 // bytes of slack at their end for the rounded-up last copy) and the slice is
 // read at its offset. The arithmetic is project_splat's, unchanged.
-constexpr uint32_t kTmaSplats = 128;  // 32 KB of slices per CTA (SH3): 7 CTAs per SM
+constexpr uint32_t kTmaSplats = kProjectSplatsPerCta;  // 128: 32 KB of slices per CTA (SH3), 7 CTAs per SM
 constexpr uint32_t kTmaPlaneFloats = kTmaSplats + 8;  // the slice, its offset and the rounding
 
 template <int DEG>
@@ -351,23 +351,23 @@ __device__ __forceinline__ void bulk_copy(void* smem_dst, const void* gmem_src, 
       : "memory");
 }
 
+// One CTA's slice of kTmaSplats splats from `base` of the FP32 view t,
+// staged through shared memory (smem_raw: TmaLayout<DEG>::kBytes; s_off:
+// TmaLayout<DEG>::kPlanes words; s_mbar: an mbarrier used once) and
+// projected: the body of k_project_tma and, per CTA, of k_project_batch.
 template <int DEG>
-__global__ void __launch_bounds__(kTmaSplats) k_project_tma(ViewTask t, ViewTask* __restrict__ table,
-                                                            float* __restrict__ dbg_proj, float* __restrict__ dbg_color,
-                                                            FrameCounters fc) {
+__device__ __forceinline__ void project_slice_tma(const ViewTask& t, uint64_t base, uint8_t* smem_raw, uint32_t* s_off,
+                                                  uint64_t* s_mbar, float* dbg_proj, float* dbg_color,
+                                                  const FrameCounters& fc, bool& vis, bool& used_fp64) {
   using L = TmaLayout<DEG>;
-  extern __shared__ __align__(128) uint8_t smem_raw[];
   float4* s_pos = reinterpret_cast<float4*>(smem_raw);
   float4* s_ca = s_pos + kTmaSplats;
   float4* s_cb = s_ca + kTmaSplats;
   float* s_planes = reinterpret_cast<float*>(s_cb + kTmaSplats);
-  __shared__ uint32_t s_off[L::kPlanes];
-  __shared__ __align__(8) uint64_t s_mbar;
   const uint32_t tid = threadIdx.x;
-  if (blockIdx.x == 0 && tid == 0) *table = t;
-  const uint64_t n = t.s.n, base = (uint64_t)blockIdx.x * kTmaSplats;
+  const uint64_t n = t.s.n;
   const uint32_t cnt = (uint32_t)min((uint64_t)kTmaSplats, n - base);
-  const uint32_t mbar = umma::smem_u32(&s_mbar);
+  const uint32_t mbar = umma::smem_u32(s_mbar);
   // Copy sizes: whole float4 records; plane slices rounded out to 16 bytes.
   auto plane_src = [&](uint32_t p) -> const float* {
     return p < 3 ? t.s.color + (uint64_t)p * n : t.s.sh + (uint64_t)(p - 3) * n;
@@ -397,7 +397,6 @@ __global__ void __launch_bounds__(kTmaSplats) k_project_tma(ViewTask t, ViewTask
     const uintptr_t lo = a & ~(uintptr_t)15, hi = (a + cnt * sizeof(float) + 15) & ~(uintptr_t)15;
     bulk_copy(s_planes + p * kTmaPlaneFloats, reinterpret_cast<const void*>(lo), (uint32_t)(hi - lo), mbar);
   }
-  bool vis = false, used_fp64 = false;
   if (!umma::mbar_wait(mbar, 0)) {
     // Copies that did not land in time: the frame reports an error, and the
     // CTA leaves only once they have (bounded) or given up on them.
@@ -408,31 +407,51 @@ __global__ void __launch_bounds__(kTmaSplats) k_project_tma(ViewTask t, ViewTask
     project_splat<DEG, false, false, SmemScene>(t.fp, t.s, base + tid, t.rec, t.bin, t.skip, dbg_proj, dbg_color, vis,
                                                 used_fp64, nullptr, &src);
   }
+}
+
+template <int DEG>
+__global__ void __launch_bounds__(kTmaSplats) k_project_tma(ViewTask t, ViewTask* __restrict__ table,
+                                                            float* __restrict__ dbg_proj, float* __restrict__ dbg_color,
+                                                            FrameCounters fc) {
+  extern __shared__ __align__(128) uint8_t smem_raw[];
+  __shared__ uint32_t s_off[TmaLayout<DEG>::kPlanes];
+  __shared__ __align__(8) uint64_t s_mbar;
+  if (blockIdx.x == 0 && threadIdx.x == 0) *table = t;
+  bool vis = false, used_fp64 = false;
+  project_slice_tma<DEG>(t, (uint64_t)blockIdx.x * kTmaSplats, smem_raw, s_off, &s_mbar, dbg_proj, dbg_color, fc, vis,
+                         used_fp64);
   count_visible(vis, used_fp64, fc, 0);
 }
 
-// Every view of the table: CTA c projects 256 splats of the view whose
-// proj_cta0 is the largest one <= c (views of different scenes, SH degrees
-// and storage precisions in one launch).
-__global__ void __launch_bounds__(256) k_project_batch(const ViewTask* __restrict__ table, uint32_t n_views,
-                                                       FrameCounters fc) {
+// Every view of the table: CTA c projects kTmaSplats splats of the view
+// whose proj_cta0 is the largest one <= c (views of different scenes, SH
+// degrees and storage precisions in one launch); FP32 views through the
+// bulk-copy staging of k_project_tma (shared memory sized for degree 3).
+__global__ void __launch_bounds__(kTmaSplats) k_project_batch(const ViewTask* __restrict__ table, uint32_t n_views,
+                                                              FrameCounters fc) {
+  extern __shared__ __align__(128) uint8_t smem_raw[];
   __shared__ ViewTask s_t;
+  __shared__ uint32_t s_off[TmaLayout<3>::kPlanes];
+  __shared__ __align__(8) uint64_t s_mbar;
   const uint32_t v = find_view(table, n_views, blockIdx.x, offsetof(ViewTask, proj_cta0));
-  static_assert(sizeof(ViewTask) % 16 == 0, "ViewTask copies as uint4");
+  static_assert(sizeof(ViewTask) % 16 == 0 && sizeof(ViewTask) / 16 <= kTmaSplats, "ViewTask copies as uint4");
   if (threadIdx.x < sizeof(ViewTask) / 16)
     reinterpret_cast<uint4*>(&s_t)[threadIdx.x] = __ldg(reinterpret_cast<const uint4*>(table + v) + threadIdx.x);
   __syncthreads();
-  const uint64_t i = (uint64_t)(blockIdx.x - s_t.proj_cta0) * blockDim.x + threadIdx.x;
+  const uint64_t base = (uint64_t)(blockIdx.x - s_t.proj_cta0) * kTmaSplats, i = base + threadIdx.x;
   bool vis = false, used_fp64 = false;
-  if (i < s_t.s.n) {
-    switch (s_t.s.sh_degree * 2 + (s_t.s.fp16 ? 1 : 0)) {
-      case 0: project_splat<0, false>(s_t.fp, s_t.s, i, s_t.rec, s_t.bin, s_t.skip, nullptr, nullptr, vis, used_fp64); break;
-      case 1: project_splat<0, true>(s_t.fp, s_t.s, i, s_t.rec, s_t.bin, s_t.skip, nullptr, nullptr, vis, used_fp64); break;
-      case 2: project_splat<1, false>(s_t.fp, s_t.s, i, s_t.rec, s_t.bin, s_t.skip, nullptr, nullptr, vis, used_fp64); break;
-      case 3: project_splat<1, true>(s_t.fp, s_t.s, i, s_t.rec, s_t.bin, s_t.skip, nullptr, nullptr, vis, used_fp64); break;
-      case 4: project_splat<2, false>(s_t.fp, s_t.s, i, s_t.rec, s_t.bin, s_t.skip, nullptr, nullptr, vis, used_fp64); break;
-      case 5: project_splat<2, true>(s_t.fp, s_t.s, i, s_t.rec, s_t.bin, s_t.skip, nullptr, nullptr, vis, used_fp64); break;
-      case 6: project_splat<3, false>(s_t.fp, s_t.s, i, s_t.rec, s_t.bin, s_t.skip, nullptr, nullptr, vis, used_fp64); break;
+  if (!s_t.s.fp16) {  // base < n: the view has a CTA per kTmaSplats of its splats
+    switch (s_t.s.sh_degree) {
+      case 0: project_slice_tma<0>(s_t, base, smem_raw, s_off, &s_mbar, nullptr, nullptr, fc, vis, used_fp64); break;
+      case 1: project_slice_tma<1>(s_t, base, smem_raw, s_off, &s_mbar, nullptr, nullptr, fc, vis, used_fp64); break;
+      case 2: project_slice_tma<2>(s_t, base, smem_raw, s_off, &s_mbar, nullptr, nullptr, fc, vis, used_fp64); break;
+      default: project_slice_tma<3>(s_t, base, smem_raw, s_off, &s_mbar, nullptr, nullptr, fc, vis, used_fp64); break;
+    }
+  } else if (i < s_t.s.n) {
+    switch (s_t.s.sh_degree) {
+      case 0: project_splat<0, true>(s_t.fp, s_t.s, i, s_t.rec, s_t.bin, s_t.skip, nullptr, nullptr, vis, used_fp64); break;
+      case 1: project_splat<1, true>(s_t.fp, s_t.s, i, s_t.rec, s_t.bin, s_t.skip, nullptr, nullptr, vis, used_fp64); break;
+      case 2: project_splat<2, true>(s_t.fp, s_t.s, i, s_t.rec, s_t.bin, s_t.skip, nullptr, nullptr, vis, used_fp64); break;
       default: project_splat<3, true>(s_t.fp, s_t.s, i, s_t.rec, s_t.bin, s_t.skip, nullptr, nullptr, vis, used_fp64); break;
     }
   }
@@ -667,7 +686,7 @@ cudaError_t launch_project_learned_batch(ViewTask* table, uint32_t n_views, uint
 cudaError_t launch_project_batch(const ViewTask* table, uint32_t n_views, uint32_t total_ctas,
                                  const FrameCounters& fc, cudaStream_t stream, uint32_t* launches) {
   if (total_ctas == 0) return cudaSuccess;
-  k_project_batch<<<total_ctas, 256, 0, stream>>>(table, n_views, fc);
+  k_project_batch<<<total_ctas, kTmaSplats, TmaLayout<3>::kBytes, stream>>>(table, n_views, fc);
   *launches += 1;
   return cudaGetLastError();
 }
