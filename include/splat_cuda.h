@@ -421,9 +421,11 @@ const char* splat_cuda_batch_create_error(void);
 int splat_cuda_batch_set_config(splat_cuda_batch* b, const splat_blend_config* config);
 int splat_cuda_batch_get_config(const splat_cuda_batch* b, splat_blend_config* config);
 /* The tuner: times `reps` graph launches of every supported configuration
- * (after one warm-up launch each), keeps the fastest and re-records the
- * batch with it. Writes up to `capacity` results (all configurations tried,
- * in the order tried) and their number to *n_results. */
+ * (after one warm-up launch each), twice over the list, keeps each
+ * configuration's faster time and the fastest configuration, and re-records
+ * the batch with it. Writes up to `capacity` results (every configuration
+ * tried, in the order tried, with its time) and their number to
+ * *n_results. */
 int splat_cuda_batch_autotune(splat_cuda_batch* b, uint32_t reps, splat_tune_result* results, uint32_t capacity,
                               uint32_t* n_results);
 /* Launches the recorded graph on the batch's stream; does not wait. */

@@ -487,28 +487,43 @@ SPLAT_API int splat_cuda_batch_autotune(splat_cuda_batch* b, uint32_t reps, spla
   const BlendConfig start = b->cfg;
   BlendConfig best = start;
   double best_ms = -1.0;
+  // Two rounds over the candidates, each keeping its faster time: a
+  // configuration timed while the clock dipped gets a second chance.
+  constexpr uint32_t kCand = sizeof(kCandidates) / sizeof(kCandidates[0]);
+  double per_ms[kCand];
+  bool fits[kCand];
+  for (uint32_t k = 0; k < kCand; k++) {
+    fits[k] = true;
+    for (const auto& v : b->views) fits[k] = fits[k] && downsample_fits(v, kCandidates[k]);
+    per_ms[k] = -1.0;
+  }
+  for (int round = 0; round < 2; round++) {
+    for (uint32_t k = 0; k < kCand; k++) {
+      if (!fits[k]) continue;
+      b->cfg = kCandidates[k];
+      int rc = prepare(b);
+      if (rc) return rc;
+      BK(cudaGraphLaunch(b->exec, b->own_stream), "graph launch");  // warm-up
+      BK(cudaEventRecord(b->ev[0], b->own_stream), "event");
+      for (uint32_t r = 0; r < reps; r++) BK(cudaGraphLaunch(b->exec, b->own_stream), "graph launch");
+      BK(cudaEventRecord(b->ev[1], b->own_stream), "event");
+      BK(cudaEventSynchronize(b->ev[1]), "tuning");
+      b->launches += (reps + 1) * kernels_per_batch(b);
+      float ms = 0.0f;
+      BK(cudaEventElapsedTime(&ms, b->ev[0], b->ev[1]), "event time");
+      const double per = ms / reps;
+      if (per_ms[k] < 0.0 || per < per_ms[k]) per_ms[k] = per;
+    }
+  }
   uint32_t count = 0;
-  for (const BlendConfig& c : kCandidates) {
-    bool fits = true;
-    for (const auto& v : b->views) fits = fits && downsample_fits(v, c);
-    if (!fits) continue;
-    b->cfg = c;
-    int rc = prepare(b);
-    if (rc) return rc;
-    BK(cudaGraphLaunch(b->exec, b->own_stream), "graph launch");  // warm-up
-    BK(cudaEventRecord(b->ev[0], b->own_stream), "event");
-    for (uint32_t r = 0; r < reps; r++) BK(cudaGraphLaunch(b->exec, b->own_stream), "graph launch");
-    BK(cudaEventRecord(b->ev[1], b->own_stream), "event");
-    BK(cudaEventSynchronize(b->ev[1]), "tuning");
-    b->launches += (reps + 1) * kernels_per_batch(b);
-    float ms = 0.0f;
-    BK(cudaEventElapsedTime(&ms, b->ev[0], b->ev[1]), "event time");
-    const double per = ms / reps;
+  for (uint32_t k = 0; k < kCand; k++) {
+    if (!fits[k]) continue;
+    const BlendConfig& c = kCandidates[k];
     if (results && count < capacity)
-      results[count] = splat_tune_result{splat_blend_config{c.tile_w, c.tile_h, c.threads}, 0u, per};
+      results[count] = splat_tune_result{splat_blend_config{c.tile_w, c.tile_h, c.threads}, 0u, per_ms[k]};
     count++;
-    if (best_ms < 0.0 || per < best_ms) {
-      best_ms = per;
+    if (best_ms < 0.0 || per_ms[k] < best_ms) {
+      best_ms = per_ms[k];
       best = c;
     }
   }
