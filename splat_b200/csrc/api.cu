@@ -861,8 +861,8 @@ SPLAT_API int splat_cuda_shard_records(splat_cuda_handle* h, const splat_view_de
       return fail(h, SPLAT_ERR_INVALID_ARG, "row window bounds must be nondecreasing and at most the frame height");
     w.bound[k] = row_bounds[k];
   }
-  if (send_capacity && (!send || (reinterpret_cast<uintptr_t>(send) & 15u)))
-    return fail(h, SPLAT_ERR_INVALID_ARG, "the send buffer must be 16-byte aligned device memory");
+  if (send_capacity && (!send || (reinterpret_cast<uintptr_t>(send) & 15u) || !is_device_memory(send, h->device)))
+    return fail(h, SPLAT_ERR_INVALID_ARG, "the send buffer must be 16-byte aligned device memory of the handle's device");
   for (uint32_t k = 0; k < n_windows; k++) counts[k] = 0;
   if (width == 0 || height == 0 || h->n == 0) return SPLAT_OK;
   CK(cudaSetDevice(h->device), "cudaSetDevice");
@@ -934,8 +934,8 @@ SPLAT_API int splat_cuda_render_records(splat_cuda_handle* h, const splat_view_d
   const size_t need = (size_t)width * rows * 3;
   if (need && (!out || out_bytes < need))
     return fail(h, SPLAT_ERR_INVALID_ARG, "output buffer smaller than width*rows*3 bytes");
-  if (n_records && (!records || (reinterpret_cast<uintptr_t>(records) & 15u)))
-    return fail(h, SPLAT_ERR_INVALID_ARG, "the records must be 16-byte aligned device memory");
+  if (n_records && (!records || (reinterpret_cast<uintptr_t>(records) & 15u) || !is_device_memory(records, h->device)))
+    return fail(h, SPLAT_ERR_INVALID_ARG, "the records must be 16-byte aligned device memory of the handle's device");
   if (n_records > 0xFFFFFFFFull) return fail(h, SPLAT_ERR_INVALID_ARG, "more than 2^32 - 1 records");
   if (need == 0) return SPLAT_OK;
   CK(cudaSetDevice(h->device), "cudaSetDevice");
