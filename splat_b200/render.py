@@ -261,8 +261,6 @@ class CudaRenderer(Renderer):
                 raise ValueError("out must be a contiguous (rows, width, 3) uint8 tensor")
             if out.is_cuda and out.device.index != self.device:
                 raise ValueError(f"out is on {out.device}, the renderer on cuda:{self.device}")
-            if not out.is_cuda and not out.is_pinned():
-                raise ValueError("a CPU tensor out must be pinned (or pass a numpy array)")
             ptr, nbytes = out.data_ptr(), out.numel()
         else:
             if out.shape != (rows, width, 3) or out.dtype != np.uint8 or not out.flags["C_CONTIGUOUS"]:
